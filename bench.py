@@ -1,0 +1,341 @@
+"""Benchmark of the hydro step: cell-updates/s of luna-cpp's FiniteVolume<3> step (time_step + step) on a 128^3 static
+Voronoi mesh, FP64 against FP32, on N GPUs (one process per GPU; replicas: the step does not shard).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--nx 128] [--impl luna|reference]
+    python -m torch.distributed.run --nproc-per-node N bench.py --gpus N ...
+
+Workload: 128^3 generators on a unit periodic lattice with uniform jitter +-0.1 spacing (mt19937_64 seed 1), ideal gas
+gamma 5/3, point blast (rho 1, v 0, p 1e-5, E = 1 in the cells whose centroid lies within 2 cell widths of the centre),
+MUSCL-Hancock + HLLC with the face-centroid limiter, CFL 0.3. Synthetic inputs of the configuration's shape (the
+reference uses no dataset). One step = time_step(0.3) (primitives, sweep, CFL reduction, the read of dt) + step(dt)
+(face fluxes, update). The working set (~3 GB) is larger than L2 (126 MB), so no flush is needed between steps.
+Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s at 128^3 3D Voronoi (FP64 vs FP32)"
+UNIT = "cell-updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--nx", type=int, default=128)
+    ap.add_argument("--impl", default="luna", choices=["luna", "reference"])
+    ap.add_argument("--cpu-sample-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def algorithmic_bytes(faces_per_cell: float, gradient_bytes: int = 120) -> dict:
+    """Algorithmic HBM bytes per cell update of the static step (each array read once per phase, neighbour gathers
+    counted once, no stored flux rows), per phase:
+      G (gradient sweep): Q 40 + V 8 + centroid 24 + position 24 + CSR start 4 + list entries 4 * 2F/N
+                          + face rows 56 F/N (owner+neighbour 8, area 24, centroid 24) + gradient row written
+      F (fluxes+update):  face rows 56 F/N + Q read 40 + gradient row read + centroid 24 + position 24 + V 8 + Q 40
+    With F/N = 7.95 and FP64 gradient rows (120 B): 728.8 + 701.2 = 1430 B. The kernel split: the sweep is phase G; the
+    flux kernel reads the face rows and the cell rows (phase F without the Q traffic); the update reads Q and writes Q."""
+    fpc = faces_per_cell
+    g = 40 + 8 + 24 + 24 + 4 + 4 * 2 * fpc + 56 * fpc + gradient_bytes
+    f = 56 * fpc + 40 + gradient_bytes + 24 + 24 + 8 + 40
+    return {"step": g + f, "sweep": g, "fluxes": 56 * fpc + gradient_bytes + 24 + 24 + 8 + 40, "update": 80.0 + 4 + 4 * 2 * fpc,
+            "primitives": 40 + 8 + 56}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_cell():
+    """DRAM bytes per cell per launch from the committed ncu summary (profiles/ncu_traffic_*.txt), or None."""
+    out = {}
+    pdir = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(pdir):
+        return out
+    for name in sorted(os.listdir(pdir)):
+        if not (name.startswith("ncu_traffic") and name.endswith(".txt")):
+            continue
+        for line in open(os.path.join(pdir, name)):
+            m = re.match(r"\s*bytes_per_cell\s+(\w+)\s+(\w+)\s*=\s*([0-9.eE+-]+)", line)
+            if m:
+                out[(m.group(1), m.group(2))] = float(m.group(3))
+    return out
+
+
+class Clocks:
+    """nvidia-smi samples of the SM clock and throttle reasons during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if parts[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def build_workload(nx: int, threads: int):
+    from luna_cpp_b200.mesh import build_mesh, jittered_points
+    from luna_cpp_b200.problems import point_blast
+
+    mesh = build_mesh(jittered_points((nx, nx, nx), jitter=0.1, seed=1), threads=threads)
+    return mesh, point_blast(mesh)
+
+
+def cpu_baseline(mesh, q0, steps: int, threads: int):
+    """The CPU oracle (a restatement of the reference's step; the reference itself needs Kokkos and voronoi-cpp, absent
+    here) on the same mesh and state, all its steps timed after one warm-up step."""
+    from oracle import oracle as O
+
+    used = O.threads(threads)
+    fv = O.OracleFV(mesh)
+    fv.set_state(q0)
+    fv.step(fv.time_step(0.3))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        fv.step(fv.time_step(0.3))
+    t = time.perf_counter() - t0
+    return {"value": mesh.n_cells * steps / t, "unit": UNIT, "cores": used, "kind": "port",
+            "sample": f"{steps} oracle steps (after 1 warm-up) of the same {mesh.n_cells}-cell mesh and state",
+            "ms_per_step": 1e3 * t / steps}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the CPU implementation of the path (the oracle port: the reference's own build needs Kokkos and
+    voronoi-cpp), all host threads, on the same workload; rank 0 only."""
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    mesh, q0 = build_workload(args.nx, threads)
+    from oracle import oracle as O
+
+    used = O.threads(threads)
+    fv = O.OracleFV(mesh)
+    fv.set_state(q0)
+    for _ in range(args.warmup):
+        fv.step(fv.time_step(0.3))
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        fv.step(fv.time_step(0.3))
+    t = time.perf_counter() - t0
+    value = mesh.n_cells * args.steps / t
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"3D static Voronoi {args.nx}^3 jittered (0.1) point blast, MUSCL-Hancock + HLLC, "
+                                   "face-centroid limiter, CFL 0.3, FP64", "n_cells": mesh.n_cells,
+                       "n_faces": mesh.n_faces, "parallelism": "replicas"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": "port",
+                             "sample": f"{args.steps} full oracle steps after {args.warmup} warm-up steps"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def timed_steps(fv, steps, torch):
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record()
+    for _ in range(steps):
+        fv.step(fv.time_step(0.3))
+    end.record()
+    torch.cuda.synchronize()
+    return start.elapsed_time(end)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import torch
+
+    from luna_cpp_b200 import hydro
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    threads = max(1, (os.cpu_count() or 1) // world)
+    mesh, q0 = build_workload(args.nx, threads)
+    N, F = mesh.n_cells, mesh.n_faces
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    results = {}
+    for prec in ("fp32", "fp64"):
+        fv = hydro.FiniteVolume(mesh, precision=prec)
+        fv.set_stream(stream)
+        fv.set_state(q0)
+        for _ in range(args.warmup):
+            fv.step(fv.time_step(0.3))
+        fv.set_timing(True)
+        fv.timings(reset=True)
+        barrier()
+        clocks = Clocks(local)
+        with clocks:
+            ms = timed_steps(fv, args.steps, torch)
+        barrier()
+        phases = fv.timings(reset=True)
+        fv.set_timing(False)
+        ms = max_over_ranks(ms)
+        results[prec] = {"ms": ms, "phases": phases, "clocks": clocks.summary(), "fallbacks": fv.fallbacks(), "fv": fv}
+
+    # End to end through the public API with host buffers: each step copies Q in from pinned host memory, steps, and
+    # copies Q back out.
+    fv = results["fp64"]["fv"]
+    host_q = torch.from_numpy(q0.copy()).pin_memory()
+    host_out = torch.empty_like(host_q).pin_memory()
+    e2e_steps = max(3, args.steps // 2)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        hydro.check(hydro.lib().luna_fv_set_state(fv.handle, host_q.data_ptr(), 0))
+        fv.step(fv.time_step(0.3))
+        hydro.check(hydro.lib().luna_fv_get_state(fv.handle, host_out.data_ptr(), 0))
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    barrier()
+
+    if rank == 0:
+        ab = algorithmic_bytes(F / N)
+        peak, peak_kind = measured_peaks()
+        r64 = results["fp64"]
+        phases = r64["phases"]
+        dominant = max(("sweep", "fluxes", "update", "primitives"), key=lambda k: phases[k][0])
+        dom_ms, dom_launches = phases[dominant]
+        avg_s = dom_ms / max(dom_launches, 1) / 1e3
+        achieved = ab[dominant] * N / avg_s / 1e9
+        tpc = traffic_per_cell()
+        traffic = tpc.get(("fp64", dominant))
+        step_s = r64["ms"] / args.steps / 1e3
+        launches = sum(v[1] for v in phases.values())
+        value = world * N * args.steps / (r64["ms"] / 1e3)
+        fp32_value = world * N * args.steps / (results["fp32"]["ms"] / 1e3)
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": r64["ms"] / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic",
+            "config": {
+                "workload": f"3D static Voronoi {args.nx}^3 jittered (0.1) point blast, MUSCL-Hancock + HLLC, "
+                            "face-centroid limiter, CFL 0.3, FP64 (time_step + step)",
+                "n_cells": N, "n_faces": F, "faces_per_cell": F / N, "parallelism": f"replicas x{world}",
+                "l2": "inputs larger than L2 (working set ~3 GB > 126 MB), no flush",
+            },
+            "face_fluxes_per_s": world * F * args.steps / (r64["ms"] / 1e3),
+            "fp32": {"value": fp32_value, "ms_per_step": results["fp32"]["ms"] / args.steps,
+                     "speedup_vs_fp64": fp32_value / value,
+                     "phases_ms_per_step": {k: v[0] / args.steps for k, v in results["fp32"]["phases"].items()}},
+            "phases_ms_per_step": {k: v[0] / args.steps for k, v in phases.items()},
+            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
+                         "algorithmic_bytes_per_cell": ab[dominant],
+                         "traffic": None if traffic is None else traffic * N},
+            "step_roofline": {"algorithmic_bytes_per_cell": ab["step"],
+                              "achieved": ab["step"] * N / step_s / 1e9, "peak": peak, "unit": "GB/s",
+                              "frac": ab["step"] * N / step_s / 1e9 / peak},
+            "clocks": r64["clocks"],
+            "e2e": {"value": world * N * e2e_steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(q0.nbytes),
+                    "d2h_bytes_per_step": int(q0.nbytes), "steps": e2e_steps},
+            "gpu_launches": int(launches),
+            "fallbacks_last_step": r64["fallbacks"],
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(mesh, q0, args.cpu_sample_steps, os.cpu_count() or 1)
+        print(json.dumps(line), flush=True)
+    for r in results.values():
+        r["fv"].close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,138 @@
+/* libluna_b200: luna-cpp's per-step finite-volume hydro update on a periodic Voronoi mesh, on one B200 (sm_100a).
+ *
+ * The C ABI a drop-in for luna-cpp's hydro::FiniteVolume<D, Exec, Riemann, Precision> (src/hydro/finite_volume.hpp):
+ * the same call order (time_step(courant) -> dt, then step(dt); a moving mesh remeshes between the two flux passes of a
+ * step), the same mesh arrays (voronoi-cpp's face lists as emitted), the same extensive conserved state Q[N][D + 2].
+ * Plain pointers and sizes only; no exceptions cross the boundary: every call returns a luna_status and the message of
+ * the last failure on this thread is in luna_last_error(). The library owns all device memory of a luna_fv; the caller's
+ * mesh arrays may be freed after luna_fv_create / luna_fv_set_mesh. A luna_fv is thread-compatible, not thread-safe.
+ * All kernels of a luna_fv run on its stream; the only host synchronisations are the reads of dt, of the fallback count
+ * and of states copied to host memory.
+ */
+#ifndef LUNA_B200_H
+#define LUNA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define LUNA_API __attribute__((visibility("default")))
+#else
+#define LUNA_API
+#endif
+
+typedef enum {
+    LUNA_OK = 0,
+    LUNA_EINVAL = 1,      /* bad argument (the reference throws std::invalid_argument / logic_error) */
+    LUNA_ENOMEM = 2,      /* a device or host allocation failed */
+    LUNA_ECUDA = 3,       /* a CUDA call failed (message in luna_last_error) */
+    LUNA_ENONFINITE = 4,  /* a kernel found a non-finite dt, flux or state (error word set) */
+    LUNA_ETIMEOUT = 5,    /* a bounded device-side wait gave up */
+    LUNA_ESTATE = 6       /* call out of order (e.g. step_moving_end without begin) */
+} luna_status;
+
+enum { LUNA_UPDATE_PER_CELL = 0, LUNA_UPDATE_PER_FACE = 1 };            /* hydro::Update (finite_volume.hpp:25) */
+enum { LUNA_LIMITER_FACE_CENTROID = 0, LUNA_LIMITER_NONE = 1 };         /* hydro::Limiter (finite_volume.hpp:29) */
+enum { LUNA_STATIC_MESH = 0, LUNA_MOVING = 1 };                         /* hydro::Motion (finite_volume.hpp:31) */
+enum { LUNA_HLLC = 0, LUNA_HLL = 1 };                                   /* Riemann parameter (euler.hpp:444, :546) */
+/* Precision policies (precision.hpp:26-54): LUNA_FP64 is Precision<> (double throughout); LUNA_FP32 is the reference's
+ * `riemann32` preset Precision<double, float, double, float> (hydro_sedov.cpp:422): gradients, limiter, face-state change
+ * and the Riemann solve in float in the face's frame; geometry, primitives (pressure recovery), flux rows and the
+ * per-cell accumulation in double. */
+enum { LUNA_FP64 = 0, LUNA_FP32 = 1 };
+
+/* hydro::Gas (euler.hpp:82-101): gamma and the RAMSES floors. */
+typedef struct {
+    double gamma;
+    double smallr; /* 1e-10 in the reference */
+    double smallc; /* 1e-10 in the reference */
+} luna_gas;
+
+/* voronoi-cpp's mesh arrays as FiniteVolume::refresh() reads them (finite_volume.hpp:353-364), row-major, D = dim.
+ * cell_face entries carry the owner bit: f if the cell owns face f, ~f otherwise (Geometry::owned_at, :318). */
+typedef struct {
+    int dim;                          /* 2 or 3 */
+    int64_t n_cells, n_faces;
+    const int32_t* owner;             /* [F] */
+    const int32_t* neighbour;         /* [F] */
+    const int32_t* cell_face_start;   /* [N + 1] */
+    const int32_t* cell_face;         /* [2F] */
+    const double* area;               /* [F][D], owner -> neighbour */
+    const double* face_centroid;      /* [F][D], relative to the owner's generator */
+    const double* centroid;           /* [N][D], relative to the cell's generator */
+    const double* volume;             /* [N] */
+    const double* positions;          /* [N][D], generators in [0, box) */
+    double box[3];                    /* periodic box sides */
+    int on_device;                    /* 1: the pointers are device pointers of the current device */
+} luna_mesh_desc;
+
+typedef struct luna_fv luna_fv;
+
+/* FiniteVolume(exec, mesh, gas, order, update, limiter, motion) (finite_volume.hpp:79-107) with the Riemann and
+ * Precision template parameters as arguments. order 0 or 1 (else LUNA_EINVAL, as the reference's invalid_argument).
+ * A moving mesh requires order 1 and the per-face update. */
+LUNA_API luna_status luna_fv_create(const luna_mesh_desc* mesh, const luna_gas* gas, int order, int update, int limiter,
+                                    int motion, int riemann, int precision, luna_fv** out);
+LUNA_API luna_status luna_fv_destroy(luna_fv* fv);
+
+/* The stream all kernels of fv run on (cudaStream_t; NULL = the legacy default stream). */
+LUNA_API luna_status luna_fv_set_stream(luna_fv* fv, void* stream);
+
+/* state() (finite_volume.hpp:145-148): the device array Q[N][D + 2]; the caller may write it, so the primitive rows are
+ * recomputed by the next time_step(). */
+LUNA_API luna_status luna_fv_state(luna_fv* fv, double** dev_q);
+LUNA_API luna_status luna_fv_set_state(luna_fv* fv, const double* q, int on_device);
+LUNA_API luna_status luna_fv_get_state(luna_fv* fv, double* q, int on_device);
+
+/* time_step(courant) (finite_volume.hpp:190-201): primitives, the sweep (limited gradients, point velocities), the CFL
+ * reduction; writes dt (AREPO's rule, finite_volume.hpp:1040-1104). Synchronises on the read of dt. */
+LUNA_API luna_status luna_fv_time_step(luna_fv* fv, double courant, double* dt_out);
+/* step(dt) (finite_volume.hpp:205-226) on a static mesh: face fluxes and the cell update. Asynchronous. */
+LUNA_API luna_status luna_fv_step(luna_fv* fv, double dt);
+/* fallbacks() (finite_volume.hpp:230-238): face sides of the last step that fell back to the cell's state. */
+LUNA_API luna_status luna_fv_fallbacks(luna_fv* fv, int64_t* out);
+/* The error word of the kernels since the last call (bit 0: non-finite dt term, bit 1: non-finite state after an update,
+ * bit 2: a list entry out of range); cleared by the read. */
+LUNA_API luna_status luna_fv_error_word(luna_fv* fv, uint32_t* out);
+
+/* The moving step (step_moving, finite_volume.hpp:1497-1519), split around the caller's remesh because the mesh update
+ * belongs to the mesh library: begin snaps the points to the mesh grid (2^-30 of the longest side), keeps the
+ * centroids of t^n, applies the t^n fluxes at dt/2 and drifts the points; it writes the new generator positions
+ * [N][D] (host or device memory) for the caller's remesh. end takes the t^n+1 mesh (same cells, same order) and
+ * applies its fluxes at dt/2. */
+LUNA_API luna_status luna_fv_step_moving_begin(luna_fv* fv, double dt, double* positions_out, int on_device);
+LUNA_API luna_status luna_fv_step_moving_end(luna_fv* fv, const luna_mesh_desc* new_mesh);
+/* A static mesh replaced by another of the same cells (checkpoint restore; FiniteVolume::mesh_moved). */
+LUNA_API luna_status luna_fv_set_mesh(luna_fv* fv, const luna_mesh_desc* mesh);
+/* positions() / point_velocities() (finite_volume.hpp:150-158): [N][D], host or device memory. */
+LUNA_API luna_status luna_fv_positions(luna_fv* fv, double* out, int on_device);
+LUNA_API luna_status luna_fv_point_velocities(luna_fv* fv, double* out, int on_device);
+/* The primitive rows [N][D + 4] (W, c, r) and the limited gradients [N][D + 2][D] (double) of the last sweep. */
+LUNA_API luna_status luna_fv_prims(luna_fv* fv, double* out, int on_device);
+LUNA_API luna_status luna_fv_gradients(luna_fv* fv, double* out, int on_device);
+
+/* Per-phase device time (hydro::Timings, finite_volume.hpp:36-39, without its fences): with timing on, CUDA events on
+ * fv's stream bracket every kernel; luna_fv_timings synchronises, adds the elapsed times since the last reset and counts
+ * the launches per phase. Phases: 0 primitives, 1 sweep (gradients, limiter, point velocities, CFL reduction),
+ * 2 fluxes, 3 update, 4 drift (the moving step's snapping and drift). */
+typedef struct {
+    double ms[5];
+    int64_t launches[5];
+} luna_timings;
+LUNA_API luna_status luna_fv_set_timing(luna_fv* fv, int on);
+LUNA_API luna_status luna_fv_timings(luna_fv* fv, luna_timings* out, int reset);
+
+LUNA_API const char* luna_status_string(luna_status s);
+LUNA_API const char* luna_last_error(void);
+/* Device bytes held by fv (all its buffers). */
+LUNA_API luna_status luna_fv_device_bytes(luna_fv* fv, int64_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,93 @@
+"""In-tree build of the native libraries: ``python -m luna_cpp_b200.build [hydro|mesh|oracle|all]``.
+
+- ``libluna_b200.so``: the hydro step, CUDA for sm_100a only (nvcc -gencode arch=compute_100a,code=sm_100a), C ABI in
+  include/luna_b200.h;
+- ``libluna_mesh.so``: the periodic Voronoi mesh builder (host C++, OpenMP);
+- ``oracle/liboracle.so``: the CPU oracle the tests check against (plain C, no multiply-add contraction).
+The libraries are built next to their sources so they travel with the tree.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+INCLUDE = os.path.join(ROOT, "include")
+ORACLE = os.path.join(ROOT, "oracle")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _nvcc() -> str:
+    for c in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if c and os.path.exists(c):
+            return c
+    raise RuntimeError("nvcc not found")
+
+
+def _run(cmd, cwd=None):
+    print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True, cwd=cwd)
+
+
+def _stale(target, sources):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(s) > t for s in sources)
+
+
+def _sources(directory, exts):
+    out = []
+    for dirpath, _, files in os.walk(directory):
+        for f in files:
+            if os.path.splitext(f)[1] in exts:
+                out.append(os.path.join(dirpath, f))
+    return sorted(out)
+
+
+def build_mesh(force=False):
+    target = os.path.join(PKG, "libluna_mesh.so")
+    srcs = [os.path.join(CSRC, "mesh", "voronoi_build.cpp")]
+    if force or _stale(target, srcs + [os.path.join(CSRC, "mesh", "luna_mesh.h")]):
+        _run(["g++", "-O3", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-Wall", "-o", target] + srcs)
+    return target
+
+
+def build_oracle(force=False):
+    target = os.path.join(ORACLE, "liboracle.so")
+    srcs = [os.path.join(ORACLE, f) for f in sorted(os.listdir(ORACLE)) if f.endswith(".c")]
+    if force or _stale(target, srcs + [os.path.join(ORACLE, "luna_oracle.h")]):
+        _run(["gcc", "-O2", "-std=c11", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-shared", "-Wall",
+              "-Wno-maybe-uninitialized", "-o", target] + srcs + ["-lm"])
+    return target
+
+
+def build_hydro(force=False, extra=()):
+    target = os.path.join(PKG, "libluna_b200.so")
+    hydro = os.path.join(CSRC, "hydro")
+    cu = [s for s in _sources(hydro, {".cu"})]
+    deps = _sources(hydro, {".cu", ".cuh", ".h", ".hpp"}) + _sources(INCLUDE, {".h"})
+    if not cu:
+        return None
+    if force or _stale(target, deps):
+        _run([_nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
+              "-Xcompiler", "-fvisibility=hidden", "-shared", "-I", INCLUDE, "-I", hydro, "-o", target, *extra, *cu,
+              "-lcudart"])
+    return target
+
+
+def build_all(force=False):
+    build_mesh(force)
+    build_oracle(force)
+    build_hydro(force)
+
+
+if __name__ == "__main__":
+    what = sys.argv[1] if len(sys.argv) > 1 else "all"
+    force = "--force" in sys.argv
+    {"all": build_all, "hydro": build_hydro, "mesh": build_mesh, "oracle": build_oracle}[what](force)

@@ -1,0 +1,682 @@
+// Kernels of the hydro step on a periodic Voronoi mesh (luna-cpp's FiniteVolume<D>, src/hydro/finite_volume.hpp).
+//
+// Data layout in HBM (the library's own copies, made once per mesh):
+//   cells  q[N][V] (extensive Q), prims[N][8] (W, c, r, pad: two 32-B sectors a row), gradient rows [N][GS] of G
+//          (GS = 16 in 3D: 15 used, 128 B in double / 64 B in float), vol[N], cen[N][D] (relative to the generator),
+//          pos[N][D] (generators)
+//   faces  owner[F], neighbour[F], area[F][D], mag[F] (|A|, computed once per mesh), fcen[F][D] (relative to the
+//          owner's generator), flux rows [F][V] (per-face update)
+//   lists  start[N + 1], list[2F] (voronoi-cpp's lists with the owner bit: ~f marks a face the cell does not own)
+#pragma once
+
+#include <cstdint>
+
+#include "physics.cuh"
+
+namespace luna {
+
+constexpr int PS = 8;  // doubles per primitive row: W (V), c, r, pad
+template <int D>
+constexpr int grad_stride() {
+    return D == 3 ? 16 : 8;
+}
+
+template <int D>
+struct MeshDev {
+    const int32_t* __restrict__ owner;
+    const int32_t* __restrict__ neighbour;
+    const int32_t* __restrict__ start;
+    const int32_t* __restrict__ list;
+    const double* __restrict__ area;
+    const double* __restrict__ mag;
+    const double* __restrict__ fcen;
+    const double* __restrict__ cen;
+    const double* __restrict__ vol;
+    const double* __restrict__ pos;
+    double side[3], inv[3];
+    int32_t n, f;
+
+    // tet_mesh::wrap (voronoi-cpp): the nearest periodic image of a separation.
+    __device__ __forceinline__ double wrap(double d, int a) const { return d - side[a] * rint(d * inv[a]); }
+    // Geometry::separation (finite_volume.hpp:282-285).
+    __device__ __forceinline__ void separation(int i, int j, double* d) const {
+#pragma unroll
+        for (int a = 0; a < D; ++a) d[a] = wrap(pos[D * j + a] - pos[D * i + a], a);
+    }
+    // Geometry::face_offset (finite_volume.hpp:322-326): face centroid of f relative to the centroid of cell i.
+    __device__ __forceinline__ void face_offset(int f, int i, double* out) const {
+        const int o = owner[f];
+        double rel[D];
+        if (o == i) {
+#pragma unroll
+            for (int a = 0; a < D; ++a) rel[a] = fcen[D * f + a];
+        } else {
+            double s[D];
+            separation(i, o, s);
+#pragma unroll
+            for (int a = 0; a < D; ++a) rel[a] = fcen[D * f + a] + s[a];
+        }
+#pragma unroll
+        for (int a = 0; a < D; ++a) out[a] = rel[a] - cen[D * i + a];
+    }
+};
+
+__device__ __forceinline__ int list_face(int32_t e) { return e >= 0 ? e : ~e; }
+
+// Counters a step's kernels write; read back with dt (one copy).
+struct Counters {
+    unsigned long long dt_bits;       // min over the time-step terms, as the bits of a positive double
+    unsigned long long fallbacks[2];  // face sides that took the cell's state (pass 0, moving pass 1)
+    unsigned long long error;         // bit 0 non-finite dt term, bit 1 non-finite state, bit 2 index out of range
+};
+
+__device__ __forceinline__ void block_min_to(double value, unsigned long long* target) {
+    __shared__ double warp_min[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) value = fmin(value, __shfl_xor_sync(0xffffffffu, value, o));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) warp_min[warp] = value;
+    __syncthreads();
+    if (warp == 0) {
+        const int warps = (blockDim.x + 31) >> 5;
+        value = lane < warps ? warp_min[lane] : 1.0e300;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) value = fmin(value, __shfl_xor_sync(0xffffffffu, value, o));
+        // Positive doubles order as their bit patterns; NaN (skipped by fmin) and +inf never win.
+        if (lane == 0 && value > 0.0 && value < 1.0e300) atomicMin(target, static_cast<unsigned long long>(__double_as_longlong(value)));
+    }
+}
+
+__device__ __forceinline__ void block_sum_to(unsigned long long value, unsigned long long* target) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) value += __shfl_xor_sync(0xffffffffu, value, o);
+    if ((threadIdx.x & 31) == 0 && value) atomicAdd(target, value);
+}
+
+// primitives() (finite_volume.hpp:403-415): W = primitive(Q / V), c = sqrt(gamma P / rho), r = radius(V).
+template <int D>
+__global__ void __launch_bounds__(256) k_primitives(MeshDev<D> m, const double* __restrict__ q, double* __restrict__ prims, GasDev gas) {
+    constexpr int V = D + 2;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.n) return;
+    const double inv = 1.0 / m.vol[i];
+    double U[V], W[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) U[v] = q[V * i + v] * inv;
+    primitive<D>(U, gas, W);
+    double* p = prims + PS * i;
+#pragma unroll
+    for (int v = 0; v < V; ++v) p[v] = W[v];
+    p[V] = sqrt(gas.gamma * W[D + 1] / W[0]);
+    p[V + 1] = radius<D>(m.vol[i]);
+}
+
+// |A| per face, once per mesh (the magnitudes the reference caches, finite_volume.hpp:1598-1601).
+template <int D>
+__global__ void k_magnitudes(const double* __restrict__ area, double* __restrict__ mag, int f_count) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= f_count) return;
+    double a[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) a[k] = area[D * f + k];
+    mag[f] = sqrt(dot<D>(a, a));
+}
+
+// Sweep::solve (finite_volume.hpp:591-615): M = L L^T by Cholesky, then every variable's fit; the gradient is x[1..D].
+template <int D, class G>
+__device__ __forceinline__ void cholesky_solve(G (&M)[D + 1][D + 1], G (&b)[D + 2][D + 1], G* grad) {
+    constexpr int U = D + 1, V = D + 2;
+    G L[U][U];
+#pragma unroll
+    for (int p = 0; p < U; ++p)
+#pragma unroll
+        for (int s = 0; s < U; ++s) L[p][s] = G(0);
+#pragma unroll
+    for (int p = 0; p < U; ++p)
+#pragma unroll
+        for (int s = 0; s <= p; ++s) {
+            G sum = M[s][p];
+#pragma unroll
+            for (int k = 0; k < s; ++k) sum -= L[p][k] * L[s][k];
+            L[p][s] = p == s ? sqrt(sum) : sum / L[s][s];
+        }
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        G z[U], x[U];
+#pragma unroll
+        for (int p = 0; p < U; ++p) {
+            G sum = b[v][p];
+#pragma unroll
+            for (int k = 0; k < p; ++k) sum -= L[p][k] * z[k];
+            z[p] = sum / L[p][p];
+        }
+#pragma unroll
+        for (int p = U - 1; p >= 0; --p) {
+            G sum = z[p];
+#pragma unroll
+            for (int k = p + 1; k < U; ++k) sum -= L[k][p] * x[k];
+            x[p] = sum / L[p][p];
+        }
+#pragma unroll
+        for (int a = 0; a < D; ++a) grad[D * v + a] = x[1 + a];
+    }
+}
+
+template <class G>
+__device__ __forceinline__ G finite_max();
+template <>
+__device__ __forceinline__ double finite_max<double>() {
+    return 1.7976931348623157e308;
+}
+template <>
+__device__ __forceinline__ float finite_max<float>() {
+    return 3.40282347e38f;
+}
+
+// The sweep of time_step(), one thread a cell (Sweep<Moving, Grad>::operator(), finite_volume.hpp:463-569): walk 1 over
+// the cell's list sums the area-weighted least-squares fit with intercept (M, b), the neighbours' range, the surface,
+// the smallest face and (moving) the largest face angle; faces below 1e-6 of the surface leave the range (a third walk,
+// rare); the fit is solved by Cholesky; walk 2 clips the gradient at each face centroid in list order. Moving: the point
+// velocity with AREPO's regularisation. The CFL terms (TimeStep, finite_volume.hpp:1040-1104) ride in walk 1: each owned
+// face's two terms and the cell's term, reduced per block into one atomicMin.
+// G: double (Precision<>) or float (Grad32: exact = false, ranges of W_j - W_i rounded once).
+template <int D, bool Moving, bool Grad, class G, bool Limit>
+__global__ void __launch_bounds__(128) k_sweep(MeshDev<D> m, const double* __restrict__ prims, G* __restrict__ grad_out,
+                                               double* __restrict__ w_out, double courant, Counters* __restrict__ ctr) {
+    constexpr int V = D + 2, U = D + 1, GS = grad_stride<D>();
+    constexpr bool exact = sizeof(G) == sizeof(double);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double smallest_dt = 1.0e300;
+    if (i < m.n) {
+        const double* pi = prims + PS * i;
+        double Wi[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) Wi[v] = pi[v];
+        const double ci = pi[V], ri = pi[V + 1];
+        double surface = 0, smallest = __longlong_as_double(0x7ff0000000000000ll), max_angle = 0;
+        G lo[V], hi[V];
+        G M[U][U], b[V][U];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            lo[v] = finite_max<G>();
+            hi[v] = -finite_max<G>();
+#pragma unroll
+            for (int p = 0; p < U; ++p) b[v][p] = G(0);
+        }
+#pragma unroll
+        for (int p = 0; p < U; ++p)
+#pragma unroll
+            for (int s = 0; s < U; ++s) M[p][s] = G(0);
+        double centroid[D];
+#pragma unroll
+        for (int a = 0; a < D; ++a) centroid[a] = m.cen[D * i + a];
+        const int first = m.start[i], end = m.start[i + 1];
+        for (int k = first; k < end; ++k) {
+            const int32_t e = m.list[k];
+            const int f = list_face(e);
+            const int j = e >= 0 ? m.neighbour[f] : m.owner[f];
+            const double* pj = prims + PS * j;
+            double Wj[V];
+#pragma unroll
+            for (int v = 0; v < V; ++v) Wj[v] = pj[v];
+            double d[D];
+            m.separation(i, j, d);
+            const double magnitude = m.mag[f];
+            surface += magnitude;
+            smallest = fmin(smallest, magnitude);
+            const double d2 = dot<D>(d, d);
+            if constexpr (Moving) max_angle = fmax(max_angle, face_angle<D>(magnitude) / (0.5 * sqrt(d2)));
+            if (e >= 0) {  // FaceStep (finite_volume.hpp:1074-1090) for the faces this cell owns
+                const double dist = sqrt(d2);
+                double dv[D];
+#pragma unroll
+                for (int a = 0; a < D; ++a) dv[a] = Wj[1 + a] - Wi[1 + a];
+                const double vsig = ci + pj[V] - dot<D>(dv, d) / dist;
+                if (vsig > 0) {
+                    smallest_dt = fmin(smallest_dt, courant * ((dist + ri) / vsig));
+                    smallest_dt = fmin(smallest_dt, courant * ((dist + pj[V + 1]) / vsig));
+                }
+            }
+            if constexpr (Grad) {
+                G X[U];
+                X[0] = G(1);
+#pragma unroll
+                for (int p = 1; p < U; ++p) X[p] = static_cast<G>(d[p - 1] + m.cen[D * j + p - 1] - centroid[p - 1]);
+                const G w = static_cast<G>(magnitude);
+#pragma unroll
+                for (int p = 0; p < U; ++p)
+#pragma unroll
+                    for (int s = p; s < U; ++s) M[p][s] += w * X[p] * X[s];
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    const double dW = Wj[v] - Wi[v];
+#pragma unroll
+                    for (int p = 0; p < U; ++p) b[v][p] += w * X[p] * static_cast<G>(dW);
+                    const G value = exact ? static_cast<G>(Wj[v]) : static_cast<G>(dW);
+                    lo[v] = fmin(lo[v], value);
+                    hi[v] = fmax(hi[v], value);
+                }
+            }
+        }
+        // CellStep (finite_volume.hpp:1040-1052).
+        double wi[D];
+#pragma unroll
+        for (int a = 0; a < D; ++a) wi[a] = Wi[1 + a];
+        if constexpr (Moving) {
+            const double factor = 2.25, speed = 0.5;
+            double fraction = 0;
+            if (max_angle > 0.75 * factor) fraction = max_angle > factor ? speed : speed * (max_angle - 0.75 * factor) / (0.25 * factor);
+            const double cd = sqrt(dot<D>(centroid, centroid));
+            if (cd > 0 && fraction > 0) {
+                const double s = fraction * ci / cd;
+#pragma unroll
+                for (int a = 0; a < D; ++a) wi[a] = wi[a] + centroid[a] * s;
+            }
+#pragma unroll
+            for (int a = 0; a < D; ++a) w_out[D * i + a] = wi[a];
+        }
+        {
+            double rel[D];
+#pragma unroll
+            for (int a = 0; a < D; ++a) rel[a] = Wi[1 + a] - (Moving ? wi[a] : 0.0);
+            smallest_dt = fmin(smallest_dt, courant * (ri / (ci + sqrt(dot<D>(rel, rel)))));
+        }
+        if constexpr (Grad) {
+            const double tiny = 1e-6 * surface;
+            const bool any_tiny = smallest < tiny;
+            if (any_tiny) {  // neighbour_range (finite_volume.hpp:572-588)
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    lo[v] = finite_max<G>();
+                    hi[v] = -finite_max<G>();
+                }
+                for (int k = first; k < end; ++k) {
+                    const int32_t e = m.list[k];
+                    const int f = list_face(e);
+                    if (m.mag[f] < tiny) continue;
+                    const int j = e >= 0 ? m.neighbour[f] : m.owner[f];
+                    const double* pj = prims + PS * j;
+#pragma unroll
+                    for (int v = 0; v < V; ++v) {
+                        const G value = exact ? static_cast<G>(pj[v]) : static_cast<G>(pj[v] - Wi[v]);
+                        lo[v] = fmin(lo[v], value);
+                        hi[v] = fmax(hi[v], value);
+                    }
+                }
+            }
+            G g[V * D];
+            cholesky_solve<D, G>(M, b, g);
+            if constexpr (Limit) {
+                for (int k = first; k < end; ++k) {
+                    const int f = list_face(m.list[k]);
+                    if (any_tiny && m.mag[f] < tiny) continue;
+                    double offset[D];
+                    m.face_offset(f, i, offset);
+                    G rg[D];
+#pragma unroll
+                    for (int a = 0; a < D; ++a) rg[a] = static_cast<G>(offset[a]);
+#pragma unroll
+                    for (int v = 0; v < V; ++v) {
+                        G* gv = g + D * v;
+                        const G dp = dot<D>(gv, rg);
+                        if constexpr (exact) {
+                            if (dp > 0 && Wi[v] + dp > hi[v]) {
+                                const G s = hi[v] > Wi[v] ? (hi[v] - Wi[v]) / dp : G(0);
+#pragma unroll
+                                for (int a = 0; a < D; ++a) gv[a] = gv[a] * s;
+                            } else if (dp < 0 && Wi[v] + dp < lo[v]) {
+                                const G s = lo[v] < Wi[v] ? (lo[v] - Wi[v]) / dp : G(0);
+#pragma unroll
+                                for (int a = 0; a < D; ++a) gv[a] = gv[a] * s;
+                            }
+                        } else {
+                            if (dp > 0 && dp > hi[v]) {
+                                const G s = hi[v] > 0 ? hi[v] / dp : G(0);
+#pragma unroll
+                                for (int a = 0; a < D; ++a) gv[a] = gv[a] * s;
+                            } else if (dp < 0 && dp < lo[v]) {
+                                const G s = lo[v] < 0 ? lo[v] / dp : G(0);
+#pragma unroll
+                                for (int a = 0; a < D; ++a) gv[a] = gv[a] * s;
+                            }
+                        }
+                    }
+                }
+            }
+            G* out = grad_out + static_cast<int64_t>(GS) * i;
+#pragma unroll
+            for (int c = 0; c < V * D; ++c) out[c] = g[c];
+        }
+    }
+    block_min_to(smallest_dt, &ctr->dt_bits);
+    if (i < m.n && !(smallest_dt == smallest_dt)) atomicOr(&ctr->error, 1ull);
+}
+
+// What a flux pass needs beyond the mesh: the state rows and the moving step's extra rows.
+template <int D, class G>
+struct FluxArgs {
+    const double* __restrict__ q;
+    const double* __restrict__ prims;
+    const G* __restrict__ grad;
+    const int32_t* __restrict__ steps;      // moving: grid steps per point over the step
+    const double* __restrict__ old_cen;     // moving: centroids of t^n
+    double dt;                              // the flux's dt (FaceFlux::dt)
+    double unit;                            // moving: grid step / dt
+    GasDev gas;
+};
+
+// FaceFlux::side at order 1 (finite_volume.hpp:1306-1329): W + g . r - dt/2 A(W) g, or W if rho or P fall to <= 0.
+template <int D, class G>
+__device__ __forceinline__ void face_side(const FluxArgs<D, G>& x, int i, const double* r, double dt, double* Wf, int& fallbacks) {
+    constexpr int V = D + 2, GS = grad_stride<D>();
+    const double* p = x.prims + PS * i;
+    const G* gr = x.grad + static_cast<int64_t>(GS) * i;
+    double W[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) W[v] = p[v];
+    G g[V * D];
+#pragma unroll
+    for (int c = 0; c < V * D; ++c) g[c] = gr[c];
+    if constexpr (sizeof(G) == sizeof(double)) {
+        double A[V];
+        half_step_rate<D, double>(W, g, x.gas.gamma, A);
+#pragma unroll
+        for (int v = 0; v < V; ++v) Wf[v] = W[v] - 0.5 * dt * A[v];
+#pragma unroll
+        for (int v = 0; v < V; ++v) Wf[v] += dot<D>(g + D * v, r);
+    } else {
+        float Wg[V], rate[V], rg[D];
+#pragma unroll
+        for (int v = 0; v < V; ++v) Wg[v] = static_cast<float>(W[v]);
+        half_step_rate<D, float>(Wg, g, static_cast<float>(x.gas.gamma), rate);
+#pragma unroll
+        for (int a = 0; a < D; ++a) rg[a] = static_cast<float>(r[a]);
+        const float h = 0.5f * static_cast<float>(dt);
+#pragma unroll
+        for (int v = 0; v < V; ++v) Wf[v] = W[v] + static_cast<double>(dot<D>(g + D * v, rg) - h * rate[v]);
+    }
+    if (Wf[0] > 0 && Wf[D + 1] > 0) return;
+    ++fallbacks;
+#pragma unroll
+    for (int v = 0; v < V; ++v) Wf[v] = W[v];
+}
+
+// MovingFlux<false>::pass_side (finite_volume.hpp:1457-1467): W + g . r on the mesh of t^n, no half step.
+template <int D, class G>
+__device__ __forceinline__ void pass1_side(const FluxArgs<D, G>& x, int i, const double* r, double* Wf, int& fallbacks) {
+    constexpr int V = D + 2, GS = grad_stride<D>();
+    const double* p = x.prims + PS * i;
+    const G* gr = x.grad + static_cast<int64_t>(GS) * i;
+    double W[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) W[v] = p[v];
+    G g[V * D];
+#pragma unroll
+    for (int c = 0; c < V * D; ++c) g[c] = gr[c];
+    if constexpr (sizeof(G) == sizeof(double)) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) Wf[v] = W[v] + dot<D>(g + D * v, r);
+    } else {
+        float rg[D];
+#pragma unroll
+        for (int a = 0; a < D; ++a) rg[a] = static_cast<float>(r[a]);
+#pragma unroll
+        for (int v = 0; v < V; ++v) Wf[v] = W[v] + static_cast<double>(dot<D>(g + D * v, rg));
+    }
+    if (Wf[0] > 0 && Wf[D + 1] > 0) return;
+    ++fallbacks;
+#pragma unroll
+    for (int v = 0; v < V; ++v) Wf[v] = W[v];
+}
+
+// FaceFlux::solve (finite_volume.hpp:1400-1413): along the unit normal n; RF: in float in the face's frame.
+template <int D, bool RF, int Riemann>
+__device__ __forceinline__ void riemann_solve(const double* L, const double* R, const double* n, const double* wf, const GasDev& gas,
+                                              double* F, bool moving) {
+    constexpr int V = D + 2;
+    if constexpr (!RF) {
+        if constexpr (Riemann == 1)
+            hll_flux<D>(L, R, n, wf, gas, F, moving);
+        else
+            hllc_flux<D, double>(L, R, n, wf, gas.gamma, gas.inverse_gm1, F, moving);
+    } else {
+        float Lf[V], Rf[V], nf[D], Ff[V], zero[D];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            Lf[v] = static_cast<float>(v >= 1 && v <= D ? L[v] - wf[v - 1] : L[v]);
+            Rf[v] = static_cast<float>(v >= 1 && v <= D ? R[v] - wf[v - 1] : R[v]);
+        }
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+            nf[a] = static_cast<float>(n[a]);
+            zero[a] = 0.0f;
+        }
+        hllc_flux<D, float>(Lf, Rf, nf, zero, static_cast<float>(gas.gamma), gas.inverse_gm1_float, Ff, false);
+#pragma unroll
+        for (int v = 0; v < V; ++v) F[v] = static_cast<double>(Ff[v]);
+        if (moving) to_lab<D, double>(F, wf);
+    }
+}
+
+// FaceFlux::face_velocity (finite_volume.hpp:1380-1397): the mean point velocity plus a correction along d, |c| <= 0.9|d|.
+template <int D>
+__device__ __forceinline__ void face_velocity(const MeshDev<D>& m, int f, int o, int j, const double* wL, const double* wR, double* out) {
+    double d[D], c[D], dw[D];
+    m.separation(o, j, d);
+    const double dist = sqrt(dot<D>(d, d));
+    const double inv_dist = 1.0 / dist;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        c[a] = m.fcen[D * f + a] - d[a] * 0.5;
+        dw[a] = wL[a] - wR[a];
+    }
+    double facv = dot<D>(c, dw) * inv_dist;
+    const double limit = 0.9 * dist, c2 = dot<D>(c, c);
+    if (c2 > limit * limit) facv *= limit / sqrt(c2);
+    const double s = facv * inv_dist;
+#pragma unroll
+    for (int a = 0; a < D; ++a) out[a] = (wL[a] + wR[a]) * 0.5 + d[a] * s;
+}
+
+// The flux through face f times |A| (FaceFlux::operator(), finite_volume.hpp:1415-1434; MovingFlux::operator(),
+// :1469-1490). Pass: -1 static, 0 moving on the mesh of t^n, 1 moving on the mesh of t^n+1.
+template <int D, int Order, int Pass, class G, bool RF, int Riemann>
+__device__ __forceinline__ void face_flux(const MeshDev<D>& m, const FluxArgs<D, G>& x, int f, double* F, int& fb_o, int& fb_j) {
+    constexpr int V = D + 2;
+    const int o = m.owner[f], j = m.neighbour[f];
+    double a[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) a[k] = m.area[D * f + k];
+    const double magnitude = sqrt(dot<D>(a, a));
+    if (magnitude == 0) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) F[v] = 0;
+        return;
+    }
+    double L[V], R[V], n[D], wf[D];
+    const double inv = 1.0 / magnitude;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        n[k] = a[k] * inv;
+        wf[k] = 0;
+    }
+    if constexpr (Pass < 0) {
+        if constexpr (Order == 0) {
+            double U[V];
+            const double io = 1.0 / m.vol[o], ij = 1.0 / m.vol[j];
+#pragma unroll
+            for (int v = 0; v < V; ++v) U[v] = x.q[V * o + v] * io;
+            primitive<D>(U, x.gas, L);
+#pragma unroll
+            for (int v = 0; v < V; ++v) U[v] = x.q[V * j + v] * ij;
+            primitive<D>(U, x.gas, R);
+        } else {
+            double ro[D], rj[D];
+            m.face_offset(f, o, ro);
+            m.face_offset(f, j, rj);
+            face_side<D, G>(x, o, ro, x.dt, L, fb_o);
+            face_side<D, G>(x, j, rj, x.dt, R, fb_j);
+        }
+    } else {
+        double wo[D], wj[D];
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            wo[k] = static_cast<double>(x.steps[D * o + k]) * x.unit;
+            wj[k] = static_cast<double>(x.steps[D * j + k]) * x.unit;
+        }
+        face_velocity<D>(m, f, o, j, wo, wj, wf);
+        double ro[D], rj[D];
+        m.face_offset(f, o, ro);
+        m.face_offset(f, j, rj);
+        if constexpr (Pass == 0) {
+            pass1_side<D, G>(x, o, ro, L, fb_o);
+            pass1_side<D, G>(x, j, rj, R, fb_j);
+        } else {
+            double r2[D];
+#pragma unroll
+            for (int k = 0; k < D; ++k) r2[k] = ro[k] + m.cen[D * o + k] - x.old_cen[D * o + k] + wo[k] * (0.5 * x.dt);
+            face_side<D, G>(x, o, r2, x.dt, L, fb_o);
+#pragma unroll
+            for (int k = 0; k < D; ++k) r2[k] = rj[k] + m.cen[D * j + k] - x.old_cen[D * j + k] + wj[k] * (0.5 * x.dt);
+            face_side<D, G>(x, j, r2, x.dt, R, fb_j);
+        }
+    }
+    riemann_solve<D, RF, Riemann>(L, R, n, wf, x.gas, F, Pass >= 0);
+#pragma unroll
+    for (int v = 0; v < V; ++v) F[v] *= magnitude;
+}
+
+// apply()'s flux pass (finite_volume.hpp:1591-1602): one flux row per face.
+template <int D, int Order, int Pass, class G, bool RF, int Riemann>
+__global__ void __launch_bounds__(128) k_flux(MeshDev<D> m, FluxArgs<D, G> x, double* __restrict__ flux,
+                                              unsigned long long* __restrict__ fallbacks) {
+    constexpr int V = D + 2;
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    int count = 0;
+    if (f < m.f) {
+        double F[V];
+        face_flux<D, Order, Pass, G, RF, Riemann>(m, x, f, F, count, count);
+#pragma unroll
+        for (int v = 0; v < V; ++v) flux[V * static_cast<int64_t>(f) + v] = F[v];
+    }
+    block_sum_to(static_cast<unsigned long long>(count), fallbacks);
+}
+
+// apply()'s update (finite_volume.hpp:1603-1615): Q_i -= dt sum_k sign_k F_k in list order; NextPrims: the next
+// primitive rows (a moving step's second pass; here every per-face step, which makes the next primitives() pass free).
+template <int D, bool NextPrims>
+__global__ void __launch_bounds__(256) k_update(MeshDev<D> m, double* __restrict__ q, const double* __restrict__ flux, double dt,
+                                                double* __restrict__ prims, GasDev gas, Counters* __restrict__ ctr) {
+    constexpr int V = D + 2;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.n) return;
+    double sum[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) sum[v] = 0;
+    const int first = m.start[i], end = m.start[i + 1];
+    for (int k = first; k < end; ++k) {
+        const int32_t e = m.list[k];
+        const int f = list_face(e);
+        const double sign = e >= 0 ? 1.0 : -1.0;
+        const double* row = flux + V * static_cast<int64_t>(f);
+#pragma unroll
+        for (int v = 0; v < V; ++v) sum[v] += sign * row[v];
+    }
+    double next[V];
+    bool finite = true;
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        next[v] = q[V * i + v] - dt * sum[v];
+        q[V * i + v] = next[v];
+        finite = finite && isfinite(next[v]);
+    }
+    if (!finite) atomicOr(&ctr->error, 2ull);
+    if constexpr (NextPrims) {
+        const double inv = 1.0 / m.vol[i];
+        double U[V], W[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) U[v] = next[v] * inv;
+        primitive<D>(U, gas, W);
+        double* p = prims + PS * i;
+#pragma unroll
+        for (int v = 0; v < V; ++v) p[v] = W[v];
+        p[V] = sqrt(gas.gamma * W[D + 1] / W[0]);
+        p[V + 1] = radius<D>(m.vol[i]);
+    }
+}
+
+// apply()'s per-cell loop (finite_volume.hpp:1543-1562): each cell computes the fluxes of its faces itself, in list order.
+template <int D, int Order, class G, bool RF, int Riemann>
+__global__ void __launch_bounds__(128) k_fluxes_and_update(MeshDev<D> m, FluxArgs<D, G> x, double* __restrict__ next, double dt,
+                                                           Counters* __restrict__ ctr) {
+    constexpr int V = D + 2;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int count = 0;
+    if (i < m.n) {
+        double sum[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) sum[v] = 0;
+        for (int k = m.start[i]; k < m.start[i + 1]; ++k) {
+            const int32_t e = m.list[k];
+            const int f = list_face(e);
+            int fo = 0, fj = 0;
+            double F[V];
+            face_flux<D, Order, -1, G, RF, Riemann>(m, x, f, F, fo, fj);
+            const bool owned = e >= 0;
+            count += owned ? fo : fj;
+            const double sign = owned ? 1.0 : -1.0;
+#pragma unroll
+            for (int v = 0; v < V; ++v) sum[v] += sign * F[v];
+        }
+        bool finite = true;
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            next[V * i + v] = x.q[V * i + v] - dt * sum[v];
+            finite = finite && isfinite(next[V * i + v]);
+        }
+        if (!finite) atomicOr(&ctr->error, 2ull);
+    }
+    block_sum_to(static_cast<unsigned long long>(count), &ctr->fallbacks[0]);
+}
+
+// The moving step's start (finite_volume.hpp:1506-1514): keep the centroids of t^n, snap the points to the mesh grid,
+// their move over dt as whole grid steps.
+template <int D>
+__global__ void k_keep_centroids(int n, const double* __restrict__ cen, double* __restrict__ old_cen, double* __restrict__ x,
+                                 const double* __restrict__ w, int32_t* __restrict__ steps, double dt, double step, double per_step,
+                                 long long p0, long long p1, long long p2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const long long period[3] = {p0, p1, p2};
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        old_cen[D * i + a] = cen[D * i + a];
+        const long long p = period[a];
+        long long k0 = llround(x[D * i + a] * per_step);
+        k0 = ((k0 % p) + p) % p;
+        long long k1 = llround((x[D * i + a] + dt * w[D * i + a]) * per_step);
+        k1 = ((k1 % p) + p) % p;
+        x[D * i + a] = static_cast<double>(k0) * step;
+        long long d = k1 - k0;
+        if (d > p / 2) d -= p;
+        if (d < -(p / 2)) d += p;
+        steps[D * i + a] = static_cast<int32_t>(d);
+    }
+}
+
+// move()'s drift on the grid (finite_volume.hpp:1219-1231).
+template <int D>
+__global__ void k_drift(int n, double* __restrict__ x, const int32_t* __restrict__ steps, double step, double per_step, long long p0,
+                        long long p1, long long p2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const long long period[3] = {p0, p1, p2};
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        const long long k = llround(x[D * i + a] * per_step) + steps[D * i + a];
+        const long long p = period[a];
+        x[D * i + a] = static_cast<double>(((k % p) + p) % p) * step;
+    }
+}
+
+}  // namespace luna

@@ -1,0 +1,732 @@
+// libluna_b200: the C ABI of include/luna_b200.h over the sm_100a kernels of kernels.cuh.
+//
+// A luna_fv mirrors luna-cpp's FiniteVolume<D> (src/hydro/finite_volume.hpp:47-239): it owns Q and its rows, copies the
+// caller's mesh arrays once per mesh, and runs time_step() (primitives, the sweep with the CFL reduction riding in it) and
+// step() (face fluxes, then the per-cell update in list order, which also writes the next step's primitive rows).
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "kernels.cuh"
+#include "luna_b200.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+luna_status set_error(luna_status s, const std::string& what) {
+    g_last_error = what;
+    return s;
+}
+
+#define LUNA_CUDA(call)                                                                                           \
+    do {                                                                                                          \
+        cudaError_t err_ = (call);                                                                                \
+        if (err_ != cudaSuccess) return set_error(LUNA_ECUDA, std::string(#call) + ": " + cudaGetErrorString(err_)); \
+    } while (0)
+
+#define LUNA_TRY(call)                      \
+    do {                                    \
+        luna_status st_ = (call);           \
+        if (st_ != LUNA_OK) return st_;     \
+    } while (0)
+
+// A device allocation that frees itself.
+template <class T>
+struct DevArray {
+    T* ptr = nullptr;
+    size_t count = 0;
+    DevArray() = default;
+    DevArray(const DevArray&) = delete;
+    DevArray& operator=(const DevArray&) = delete;
+    ~DevArray() { release(); }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        count = 0;
+    }
+    luna_status alloc(size_t n, const char* what) {
+        if (n == count && ptr) return LUNA_OK;
+        release();
+        if (n == 0) return LUNA_OK;
+        cudaError_t e = cudaMalloc(&ptr, n * sizeof(T));
+        if (e != cudaSuccess) {
+            ptr = nullptr;
+            cudaGetLastError();
+            return set_error(e == cudaErrorMemoryAllocation ? LUNA_ENOMEM : LUNA_ECUDA,
+                             std::string("cudaMalloc(") + what + "): " + cudaGetErrorString(e));
+        }
+        count = n;
+        return LUNA_OK;
+    }
+    size_t bytes() const { return count * sizeof(T); }
+};
+
+constexpr int kBlockCells = 128;
+constexpr int kBlockFaces = 128;
+
+int blocks(int64_t n, int per) { return static_cast<int>((n + per - 1) / per); }
+
+}  // namespace
+
+struct luna_fv {
+    int dim = 3, order = 1, update = LUNA_UPDATE_PER_FACE, limiter = LUNA_LIMITER_FACE_CENTROID, motion = LUNA_STATIC_MESH,
+        riemann = LUNA_HLLC, precision = LUNA_FP64;
+    int64_t n = 0, f = 0;
+    luna::GasDev gas{};
+    double box[3] = {1, 1, 1};
+    cudaStream_t stream = nullptr;
+
+    // mesh
+    DevArray<int32_t> owner, neighbour, start, list;
+    DevArray<double> area, mag, fcen, cen, vol, pos;
+    // state and rows
+    DevArray<double> q, next, prims, grad64, flux, w, x, old_cen;
+    DevArray<float> grad32;
+    DevArray<int32_t> steps;
+    DevArray<luna::Counters> counters;
+    luna::Counters* host_counters = nullptr;  // pinned
+
+    // Per-phase timing: event pairs recorded around each launch, reduced on request.
+    bool timing = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> event_pool;
+    std::vector<std::pair<int, size_t>> pending;  // (phase, pool index) recorded since the last reduction
+    double phase_ms[5] = {0, 0, 0, 0, 0};
+    int64_t phase_launches[5] = {0, 0, 0, 0, 0};
+
+    bool prims_ready = false, swept = false, moving_pending = false;
+    double pending_dt = 0;
+    double grid_step = 0, per_step = 0;
+    long long period[3] = {1, 1, 1};
+
+    ~luna_fv() {
+        if (host_counters) cudaFreeHost(host_counters);
+        for (auto& e : event_pool) {
+            cudaEventDestroy(e.first);
+            cudaEventDestroy(e.second);
+        }
+    }
+
+    // Opens a timed launch of `phase`; returns the pool slot (or -1 with timing off). close_timed records its end.
+    long open_timed(int phase) {
+        if (!timing) return -1;
+        const size_t slot = pending.size();
+        if (slot >= event_pool.size()) {
+            cudaEvent_t a, b;
+            if (cudaEventCreate(&a) != cudaSuccess) return -1;
+            if (cudaEventCreate(&b) != cudaSuccess) {
+                cudaEventDestroy(a);
+                return -1;
+            }
+            event_pool.push_back({a, b});
+        }
+        cudaEventRecord(event_pool[slot].first, stream);
+        pending.push_back({phase, slot});
+        return static_cast<long>(slot);
+    }
+    void close_timed(long slot) {
+        if (slot >= 0) cudaEventRecord(event_pool[static_cast<size_t>(slot)].second, stream);
+    }
+
+    template <int D>
+    luna::MeshDev<D> mesh_dev() const {
+        luna::MeshDev<D> m;
+        m.owner = owner.ptr;
+        m.neighbour = neighbour.ptr;
+        m.start = start.ptr;
+        m.list = list.ptr;
+        m.area = area.ptr;
+        m.mag = mag.ptr;
+        m.fcen = fcen.ptr;
+        m.cen = cen.ptr;
+        m.vol = vol.ptr;
+        m.pos = pos.ptr;
+        for (int a = 0; a < 3; ++a) {
+            m.side[a] = box[a];
+            m.inv[a] = box[a] > 0 ? 1.0 / box[a] : 0.0;
+        }
+        m.n = static_cast<int32_t>(n);
+        m.f = static_cast<int32_t>(f);
+        return m;
+    }
+};
+
+namespace {
+
+template <class T>
+luna_status upload(DevArray<T>& dst, const T* src, size_t count, bool on_device, cudaStream_t s, const char* what) {
+    LUNA_TRY(dst.alloc(count, what));
+    if (count == 0) return LUNA_OK;
+    if (!src) return set_error(LUNA_EINVAL, std::string("mesh array ") + what + " is null");
+    LUNA_CUDA(cudaMemcpyAsync(dst.ptr, src, count * sizeof(T), on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+    return LUNA_OK;
+}
+
+luna_status validate_mesh(const luna_mesh_desc* m, int dim, int64_t n) {
+    if (!m) return set_error(LUNA_EINVAL, "mesh is null");
+    if (m->dim != 2 && m->dim != 3) return set_error(LUNA_EINVAL, "mesh dim must be 2 or 3");
+    if (dim && m->dim != dim) return set_error(LUNA_EINVAL, "mesh dim differs from the solver's");
+    if (m->n_cells <= 0 || m->n_cells >= (int64_t(1) << 31)) return set_error(LUNA_EINVAL, "n_cells out of range");
+    if (n && m->n_cells != n) return set_error(LUNA_EINVAL, "a new mesh must have the same cells");
+    if (m->n_faces < 0 || 2 * m->n_faces >= (int64_t(1) << 31)) return set_error(LUNA_EINVAL, "n_faces out of range");
+    for (int a = 0; a < m->dim; ++a)
+        if (!(m->box[a] > 0)) return set_error(LUNA_EINVAL, "box sides must be positive");
+    if (!m->on_device) {  // host lists: checked here, once per mesh (device lists are the caller's responsibility)
+        const int64_t N = m->n_cells, F = m->n_faces;
+        if (!m->cell_face_start || !m->cell_face || !m->owner || !m->neighbour) return set_error(LUNA_EINVAL, "mesh lists are null");
+        if (m->cell_face_start[0] != 0 || m->cell_face_start[N] != 2 * F) return set_error(LUNA_EINVAL, "cell_face_start must run 0 .. 2F");
+        for (int64_t i = 0; i < N; ++i)
+            if (m->cell_face_start[i + 1] < m->cell_face_start[i]) return set_error(LUNA_EINVAL, "cell_face_start not monotone");
+        for (int64_t k = 0; k < 2 * F; ++k) {
+            const int32_t e = m->cell_face[k];
+            const int32_t face = e >= 0 ? e : ~e;
+            if (face >= F) return set_error(LUNA_EINVAL, "cell_face entry out of range");
+        }
+        for (int64_t k = 0; k < F; ++k)
+            if (m->owner[k] < 0 || m->owner[k] >= N || m->neighbour[k] < 0 || m->neighbour[k] >= N)
+                return set_error(LUNA_EINVAL, "owner/neighbour out of range");
+    }
+    return LUNA_OK;
+}
+
+luna_status load_mesh(luna_fv* fv, const luna_mesh_desc* m) {
+    const int D = m->dim;
+    const size_t N = static_cast<size_t>(m->n_cells), F = static_cast<size_t>(m->n_faces);
+    const bool dev = m->on_device != 0;
+    cudaStream_t s = fv->stream;
+    LUNA_TRY(upload(fv->owner, m->owner, F, dev, s, "owner"));
+    LUNA_TRY(upload(fv->neighbour, m->neighbour, F, dev, s, "neighbour"));
+    LUNA_TRY(upload(fv->start, m->cell_face_start, N + 1, dev, s, "cell_face_start"));
+    LUNA_TRY(upload(fv->list, m->cell_face, 2 * F, dev, s, "cell_face"));
+    LUNA_TRY(upload(fv->area, m->area, F * D, dev, s, "area"));
+    LUNA_TRY(upload(fv->fcen, m->face_centroid, F * D, dev, s, "face_centroid"));
+    LUNA_TRY(upload(fv->cen, m->centroid, N * D, dev, s, "centroid"));
+    LUNA_TRY(upload(fv->vol, m->volume, N, dev, s, "volume"));
+    LUNA_TRY(upload(fv->pos, m->positions, N * D, dev, s, "positions"));
+    LUNA_TRY(fv->mag.alloc(F, "magnitudes"));
+    fv->f = static_cast<int64_t>(F);
+    for (int a = 0; a < 3; ++a) fv->box[a] = a < D ? m->box[a] : 0.0;
+    if (F > 0) {
+        if (D == 3)
+            luna::k_magnitudes<3><<<blocks(F, 256), 256, 0, s>>>(fv->area.ptr, fv->mag.ptr, static_cast<int>(F));
+        else
+            luna::k_magnitudes<2><<<blocks(F, 256), 256, 0, s>>>(fv->area.ptr, fv->mag.ptr, static_cast<int>(F));
+        LUNA_CUDA(cudaGetLastError());
+    }
+    if (fv->update == LUNA_UPDATE_PER_FACE) LUNA_TRY(fv->flux.alloc(F * (D + 2) > 0 ? F * (D + 2) : 1, "flux rows"));
+    // Lists in device memory are trusted as voronoi-cpp's; the sweep does not re-check them.
+    return LUNA_OK;
+}
+
+template <int D>
+luna_status run_primitives(luna_fv* fv) {
+    {
+        const long timed_ = fv->open_timed(0);
+        luna::k_primitives<D><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->q.ptr, fv->prims.ptr, fv->gas);
+        fv->close_timed(timed_);
+    }
+    LUNA_CUDA(cudaGetLastError());
+    return LUNA_OK;
+}
+
+template <int D, bool Moving, bool Grad, class G>
+luna_status launch_sweep(luna_fv* fv, G* grad, double courant) {
+    const auto m = fv->mesh_dev<D>();
+    if (fv->limiter == LUNA_LIMITER_NONE)
+        {
+            const long timed_ = fv->open_timed(1);
+            luna::k_sweep<D, Moving, Grad, G, false><<<blocks(fv->n, kBlockCells), kBlockCells, 0, fv->stream>>>(m, fv->prims.ptr, grad, fv->w.ptr, courant,
+                                                                                                               fv->counters.ptr);
+            fv->close_timed(timed_);
+        }
+    else
+        {
+            const long timed_ = fv->open_timed(1);
+            luna::k_sweep<D, Moving, Grad, G, true><<<blocks(fv->n, kBlockCells), kBlockCells, 0, fv->stream>>>(m, fv->prims.ptr, grad, fv->w.ptr, courant,
+                                                                                                              fv->counters.ptr);
+            fv->close_timed(timed_);
+        }
+    LUNA_CUDA(cudaGetLastError());
+    return LUNA_OK;
+}
+
+// sweep() (finite_volume.hpp:1107-1149): the dt word is reset, then one kernel writes gradients, point velocities and dt.
+template <int D>
+luna_status run_sweep(luna_fv* fv, double courant) {
+    const unsigned long long init = 0x7fefffffffffffffull;  // DBL_MAX: the Min reducer's identity
+    LUNA_CUDA(cudaMemcpyAsync(&fv->counters.ptr->dt_bits, &init, sizeof(init), cudaMemcpyHostToDevice, fv->stream));
+    const bool moving = fv->motion == LUNA_MOVING, grad = fv->order == 1;
+    if (fv->precision == LUNA_FP32) {
+        if (moving) return launch_sweep<D, true, true, float>(fv, fv->grad32.ptr, courant);
+        return grad ? launch_sweep<D, false, true, float>(fv, fv->grad32.ptr, courant) : launch_sweep<D, false, false, float>(fv, fv->grad32.ptr, courant);
+    }
+    if (moving) return launch_sweep<D, true, true, double>(fv, fv->grad64.ptr, courant);
+    return grad ? launch_sweep<D, false, true, double>(fv, fv->grad64.ptr, courant) : launch_sweep<D, false, false, double>(fv, fv->grad64.ptr, courant);
+}
+
+luna_status read_counters(luna_fv* fv) {
+    LUNA_CUDA(cudaMemcpyAsync(fv->host_counters, fv->counters.ptr, sizeof(luna::Counters), cudaMemcpyDeviceToHost, fv->stream));
+    LUNA_CUDA(cudaStreamSynchronize(fv->stream));
+    return LUNA_OK;
+}
+
+template <int D>
+luna_status prepare_sweep(luna_fv* fv, double courant) {
+    if (!fv->prims_ready) LUNA_TRY(run_primitives<D>(fv));
+    fv->prims_ready = false;
+    return run_sweep<D>(fv, courant);
+}
+
+template <int D, int Order, int Pass, class G, bool RF, int Riemann>
+luna_status launch_flux(luna_fv* fv, const luna::FluxArgs<D, G>& x) {
+    if (fv->f == 0) return LUNA_OK;
+    {
+        const long timed_ = fv->open_timed(2);
+        luna::k_flux<D, Order, Pass, G, RF, Riemann><<<blocks(fv->f, kBlockFaces), kBlockFaces, 0, fv->stream>>>(
+            fv->mesh_dev<D>(), x, fv->flux.ptr, &fv->counters.ptr->fallbacks[Pass == 1 ? 1 : 0]);
+        fv->close_timed(timed_);
+    }
+    LUNA_CUDA(cudaGetLastError());
+    return LUNA_OK;
+}
+
+template <int D, int Order, int Pass, class G>
+luna_status dispatch_flux(luna_fv* fv, const luna::FluxArgs<D, G>& x) {
+    if (fv->precision == LUNA_FP32) return launch_flux<D, Order, Pass, G, true, 0>(fv, x);
+    if (fv->riemann == LUNA_HLL) return launch_flux<D, Order, Pass, G, false, 1>(fv, x);
+    return launch_flux<D, Order, Pass, G, false, 0>(fv, x);
+}
+
+template <int D, int Order, class G, bool RF, int Riemann>
+luna_status launch_per_cell(luna_fv* fv, const luna::FluxArgs<D, G>& x, double dt) {
+    double* out = Order == 0 ? fv->next.ptr : fv->q.ptr;
+    {
+        const long timed_ = fv->open_timed(2);
+        luna::k_fluxes_and_update<D, Order, G, RF, Riemann><<<blocks(fv->n, kBlockCells), kBlockCells, 0, fv->stream>>>(fv->mesh_dev<D>(), x, out, dt,
+                                                                                                                     fv->counters.ptr);
+        fv->close_timed(timed_);
+    }
+    LUNA_CUDA(cudaGetLastError());
+    if (Order == 0) std::swap(fv->q.ptr, fv->next.ptr);
+    return LUNA_OK;
+}
+
+template <int D, class G>
+luna::FluxArgs<D, G> flux_args(luna_fv* fv, const G* grad, double dt) {
+    luna::FluxArgs<D, G> x;
+    x.q = fv->q.ptr;
+    x.prims = fv->prims.ptr;
+    x.grad = grad;
+    x.steps = fv->steps.ptr;
+    x.old_cen = fv->old_cen.ptr;
+    x.dt = dt;
+    x.unit = 0;
+    x.gas = fv->gas;
+    return x;
+}
+
+// apply() for a static mesh (finite_volume.hpp:1538-1631).
+template <int D, class G>
+luna_status run_apply(luna_fv* fv, const G* grad, double dt) {
+    const auto x = flux_args<D, G>(fv, grad, dt);
+    if (fv->update == LUNA_UPDATE_PER_CELL) {
+        if (fv->order == 0) {
+            if (fv->precision == LUNA_FP32) return launch_per_cell<D, 0, G, true, 0>(fv, x, dt);
+            return fv->riemann == LUNA_HLL ? launch_per_cell<D, 0, G, false, 1>(fv, x, dt) : launch_per_cell<D, 0, G, false, 0>(fv, x, dt);
+        }
+        if (fv->precision == LUNA_FP32) return launch_per_cell<D, 1, G, true, 0>(fv, x, dt);
+        return fv->riemann == LUNA_HLL ? launch_per_cell<D, 1, G, false, 1>(fv, x, dt) : launch_per_cell<D, 1, G, false, 0>(fv, x, dt);
+    }
+    if (fv->order == 0)
+        LUNA_TRY((dispatch_flux<D, 0, -1, G>(fv, x)));
+    else
+        LUNA_TRY((dispatch_flux<D, 1, -1, G>(fv, x)));
+    {
+        const long timed_ = fv->open_timed(3);
+        luna::k_update<D, true><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->q.ptr, fv->flux.ptr, dt, fv->prims.ptr, fv->gas,
+                                                                            fv->counters.ptr);
+        fv->close_timed(timed_);
+    }
+    LUNA_CUDA(cudaGetLastError());
+    fv->prims_ready = true;  // the update wrote the next primitive rows
+    return LUNA_OK;
+}
+
+template <int D>
+luna_status step_static(luna_fv* fv, double dt) {
+    if (!fv->swept) LUNA_TRY(prepare_sweep<D>(fv, 1.0));
+    fv->swept = false;
+    LUNA_CUDA(cudaMemsetAsync(&fv->counters.ptr->fallbacks[0], 0, 2 * sizeof(unsigned long long), fv->stream));
+    if (fv->precision == LUNA_FP32) return run_apply<D, float>(fv, fv->grad32.ptr, dt);
+    return run_apply<D, double>(fv, fv->grad64.ptr, dt);
+}
+
+template <int D>
+luna_status moving_begin(luna_fv* fv, double dt) {
+    if (!fv->swept) LUNA_TRY(prepare_sweep<D>(fv, 1.0));
+    fv->swept = false;
+    LUNA_CUDA(cudaMemsetAsync(&fv->counters.ptr->fallbacks[0], 0, 2 * sizeof(unsigned long long), fv->stream));
+    {
+        const long timed_ = fv->open_timed(4);
+        luna::k_keep_centroids<D><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(static_cast<int>(fv->n), fv->cen.ptr, fv->old_cen.ptr, fv->x.ptr, fv->w.ptr,
+                                                                               fv->steps.ptr, dt, fv->grid_step, fv->per_step, fv->period[0],
+                                                                               fv->period[1], fv->period[2]);
+        fv->close_timed(timed_);
+    }
+    LUNA_CUDA(cudaGetLastError());
+    fv->pending_dt = dt;
+    if (fv->precision == LUNA_FP32) {
+        auto x = flux_args<D, float>(fv, fv->grad32.ptr, 0.0);
+        x.unit = fv->grid_step / dt;
+        LUNA_TRY((launch_flux<D, 1, 0, float, true, 0>(fv, x)));
+    } else {
+        auto x = flux_args<D, double>(fv, fv->grad64.ptr, 0.0);
+        x.unit = fv->grid_step / dt;
+        if (fv->riemann == LUNA_HLL)
+            LUNA_TRY((launch_flux<D, 1, 0, double, false, 1>(fv, x)));
+        else
+            LUNA_TRY((launch_flux<D, 1, 0, double, false, 0>(fv, x)));
+    }
+    {
+        const long timed_ = fv->open_timed(3);
+        luna::k_update<D, false><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->q.ptr, fv->flux.ptr, 0.5 * dt, fv->prims.ptr, fv->gas,
+                                                                             fv->counters.ptr);
+        fv->close_timed(timed_);
+    }
+    LUNA_CUDA(cudaGetLastError());
+    {
+        const long timed_ = fv->open_timed(4);
+        luna::k_drift<D><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(static_cast<int>(fv->n), fv->x.ptr, fv->steps.ptr, fv->grid_step, fv->per_step,
+                                                                     fv->period[0], fv->period[1], fv->period[2]);
+        fv->close_timed(timed_);
+    }
+    LUNA_CUDA(cudaGetLastError());
+    fv->moving_pending = true;
+    return LUNA_OK;
+}
+
+template <int D>
+luna_status moving_end(luna_fv* fv) {
+    const double dt = fv->pending_dt;
+    if (fv->precision == LUNA_FP32) {
+        auto x = flux_args<D, float>(fv, fv->grad32.ptr, 2 * dt);
+        x.unit = fv->grid_step / dt;
+        LUNA_TRY((launch_flux<D, 1, 1, float, true, 0>(fv, x)));
+    } else {
+        auto x = flux_args<D, double>(fv, fv->grad64.ptr, 2 * dt);
+        x.unit = fv->grid_step / dt;
+        if (fv->riemann == LUNA_HLL)
+            LUNA_TRY((launch_flux<D, 1, 1, double, false, 1>(fv, x)));
+        else
+            LUNA_TRY((launch_flux<D, 1, 1, double, false, 0>(fv, x)));
+    }
+    {
+        const long timed_ = fv->open_timed(3);
+        luna::k_update<D, true><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->q.ptr, fv->flux.ptr, 0.5 * dt, fv->prims.ptr, fv->gas,
+                                                                            fv->counters.ptr);
+        fv->close_timed(timed_);
+    }
+    LUNA_CUDA(cudaGetLastError());
+    fv->prims_ready = true;
+    fv->moving_pending = false;
+    return LUNA_OK;
+}
+
+luna_status copy_out(const double* src, double* dst, size_t count, int on_device, cudaStream_t s) {
+    if (!dst) return set_error(LUNA_EINVAL, "output is null");
+    LUNA_CUDA(cudaMemcpyAsync(dst, src, count * sizeof(double), on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+    LUNA_CUDA(cudaStreamSynchronize(s));
+    return LUNA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+LUNA_API const char* luna_status_string(luna_status s) {
+    switch (s) {
+        case LUNA_OK: return "ok";
+        case LUNA_EINVAL: return "invalid argument";
+        case LUNA_ENOMEM: return "out of memory";
+        case LUNA_ECUDA: return "CUDA error";
+        case LUNA_ENONFINITE: return "non-finite value";
+        case LUNA_ETIMEOUT: return "device wait timed out";
+        case LUNA_ESTATE: return "call out of order";
+    }
+    return "unknown status";
+}
+
+LUNA_API const char* luna_last_error(void) { return g_last_error.c_str(); }
+
+LUNA_API luna_status luna_fv_create(const luna_mesh_desc* mesh, const luna_gas* gas, int order, int update, int limiter, int motion, int riemann,
+                                    int precision, luna_fv** out) {
+    if (!out) return set_error(LUNA_EINVAL, "out is null");
+    *out = nullptr;
+    if (!gas || !(gas->gamma > 1.0)) return set_error(LUNA_EINVAL, "gas: gamma must be > 1");
+    if (order != 0 && order != 1) return set_error(LUNA_EINVAL, "hydro::FiniteVolume: order 0 or 1");
+    if (update != LUNA_UPDATE_PER_CELL && update != LUNA_UPDATE_PER_FACE) return set_error(LUNA_EINVAL, "update: per_cell or per_face");
+    if (limiter != LUNA_LIMITER_FACE_CENTROID && limiter != LUNA_LIMITER_NONE) return set_error(LUNA_EINVAL, "limiter: face_centroid or none");
+    if (motion != LUNA_STATIC_MESH && motion != LUNA_MOVING) return set_error(LUNA_EINVAL, "motion: static_mesh or moving");
+    if (riemann != LUNA_HLLC && riemann != LUNA_HLL) return set_error(LUNA_EINVAL, "riemann: HLLC or HLL");
+    if (precision != LUNA_FP64 && precision != LUNA_FP32) return set_error(LUNA_EINVAL, "precision: FP64 or FP32");
+    if (precision == LUNA_FP32 && riemann == LUNA_HLL)
+        return set_error(LUNA_EINVAL, "the FP32 policy takes HLLC (the reference's reduced presets are HLLC only)");
+    if (motion == LUNA_MOVING && (order != 1 || update != LUNA_UPDATE_PER_FACE))
+        return set_error(LUNA_EINVAL, "a moving mesh runs order 1 with the per-face update");
+    LUNA_TRY(validate_mesh(mesh, 0, 0));
+    luna_fv* fv = new (std::nothrow) luna_fv();
+    if (!fv) return set_error(LUNA_ENOMEM, "luna_fv");
+    fv->dim = mesh->dim;
+    fv->order = order;
+    fv->update = update;
+    fv->limiter = limiter;
+    fv->motion = motion;
+    fv->riemann = riemann;
+    fv->precision = precision;
+    fv->n = mesh->n_cells;
+    fv->gas.gamma = gas->gamma;
+    fv->gas.smallr = gas->smallr;
+    fv->gas.smallc = gas->smallc;
+    fv->gas.inverse_gm1 = 1.0 / (gas->gamma - 1.0);
+    fv->gas.inverse_gm1_float = 1.0f / (static_cast<float>(gas->gamma) - 1.0f);
+    auto fail = [&](luna_status s) {
+        delete fv;
+        return s;
+    };
+    const int D = fv->dim, V = D + 2;
+    const size_t N = static_cast<size_t>(fv->n);
+    if (cudaMallocHost(&fv->host_counters, sizeof(luna::Counters)) != cudaSuccess) {
+        cudaGetLastError();
+        fv->host_counters = nullptr;
+        return fail(set_error(LUNA_ENOMEM, "pinned counters"));
+    }
+    luna_status s;
+    if ((s = fv->counters.alloc(1, "counters")) != LUNA_OK) return fail(s);
+    if (cudaMemsetAsync(fv->counters.ptr, 0, sizeof(luna::Counters), fv->stream) != cudaSuccess) return fail(set_error(LUNA_ECUDA, "memset counters"));
+    if ((s = fv->q.alloc(N * V, "Q")) != LUNA_OK) return fail(s);
+    if (cudaMemsetAsync(fv->q.ptr, 0, N * V * sizeof(double), fv->stream) != cudaSuccess) return fail(set_error(LUNA_ECUDA, "memset Q"));
+    if (order == 0 && update == LUNA_UPDATE_PER_CELL && (s = fv->next.alloc(N * V, "Q next")) != LUNA_OK) return fail(s);
+    if ((s = fv->prims.alloc(N * luna::PS, "primitive rows")) != LUNA_OK) return fail(s);
+    const size_t GS = D == 3 ? luna::grad_stride<3>() : luna::grad_stride<2>();
+    if (order == 1) {
+        if (precision == LUNA_FP32) {
+            if ((s = fv->grad32.alloc(N * GS, "gradient rows")) != LUNA_OK) return fail(s);
+        } else if ((s = fv->grad64.alloc(N * GS, "gradient rows")) != LUNA_OK) {
+            return fail(s);
+        }
+    }
+    if ((s = fv->w.alloc(N * D, "point velocities")) != LUNA_OK) return fail(s);
+    if (cudaMemsetAsync(fv->w.ptr, 0, N * D * sizeof(double), fv->stream) != cudaSuccess) return fail(set_error(LUNA_ECUDA, "memset w"));
+    if ((s = load_mesh(fv, mesh)) != LUNA_OK) return fail(s);
+    if (motion == LUNA_MOVING) {
+        if ((s = fv->x.alloc(N * D, "positions")) != LUNA_OK) return fail(s);
+        if ((s = fv->old_cen.alloc(N * D, "old centroids")) != LUNA_OK) return fail(s);
+        if ((s = fv->steps.alloc(N * D, "grid steps")) != LUNA_OK) return fail(s);
+        if (cudaMemcpyAsync(fv->x.ptr, fv->pos.ptr, N * D * sizeof(double), cudaMemcpyDeviceToDevice, fv->stream) != cudaSuccess)
+            return fail(set_error(LUNA_ECUDA, "copy positions"));
+        double longest = mesh->box[0];
+        for (int a = 1; a < D; ++a) longest = longest > mesh->box[a] ? longest : mesh->box[a];
+        fv->grid_step = std::ldexp(longest, -30);
+        fv->per_step = 1.0 / fv->grid_step;
+        for (int a = 0; a < D; ++a) fv->period[a] = std::llround(mesh->box[a] / fv->grid_step);
+    }
+    if (cudaStreamSynchronize(fv->stream) != cudaSuccess) return fail(set_error(LUNA_ECUDA, cudaGetErrorString(cudaGetLastError())));
+    *out = fv;
+    return LUNA_OK;
+}
+
+LUNA_API luna_status luna_fv_destroy(luna_fv* fv) {
+    if (!fv) return LUNA_OK;
+    cudaStreamSynchronize(fv->stream);
+    delete fv;
+    return LUNA_OK;
+}
+
+LUNA_API luna_status luna_fv_set_stream(luna_fv* fv, void* stream) {
+    if (!fv) return set_error(LUNA_EINVAL, "fv is null");
+    LUNA_CUDA(cudaStreamSynchronize(fv->stream));
+    fv->stream = static_cast<cudaStream_t>(stream);
+    return LUNA_OK;
+}
+
+LUNA_API luna_status luna_fv_state(luna_fv* fv, double** dev_q) {
+    if (!fv || !dev_q) return set_error(LUNA_EINVAL, "null argument");
+    fv->prims_ready = false;
+    fv->swept = false;
+    *dev_q = fv->q.ptr;
+    return LUNA_OK;
+}
+
+LUNA_API luna_status luna_fv_set_state(luna_fv* fv, const double* q, int on_device) {
+    if (!fv || !q) return set_error(LUNA_EINVAL, "null argument");
+    const size_t bytes = static_cast<size_t>(fv->n) * (fv->dim + 2) * sizeof(double);
+    LUNA_CUDA(cudaMemcpyAsync(fv->q.ptr, q, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, fv->stream));
+    if (!on_device) LUNA_CUDA(cudaStreamSynchronize(fv->stream));
+    fv->prims_ready = false;
+    fv->swept = false;
+    return LUNA_OK;
+}
+
+LUNA_API luna_status luna_fv_get_state(luna_fv* fv, double* q, int on_device) {
+    if (!fv) return set_error(LUNA_EINVAL, "fv is null");
+    return copy_out(fv->q.ptr, q, static_cast<size_t>(fv->n) * (fv->dim + 2), on_device, fv->stream);
+}
+
+LUNA_API luna_status luna_fv_time_step(luna_fv* fv, double courant, double* dt_out) {
+    if (!fv || !dt_out) return set_error(LUNA_EINVAL, "null argument");
+    if (fv->moving_pending) return set_error(LUNA_ESTATE, "time_step inside a moving step (call luna_fv_step_moving_end first)");
+    LUNA_TRY(fv->dim == 3 ? prepare_sweep<3>(fv, courant) : prepare_sweep<2>(fv, courant));
+    LUNA_TRY(read_counters(fv));
+    fv->swept = true;
+    double dt;
+    std::memcpy(&dt, &fv->host_counters->dt_bits, sizeof(dt));
+    *dt_out = dt;
+    if (fv->host_counters->error & 1ull) return set_error(LUNA_ENONFINITE, "a time-step term is not finite");
+    return LUNA_OK;
+}
+
+LUNA_API luna_status luna_fv_step(luna_fv* fv, double dt) {
+    if (!fv) return set_error(LUNA_EINVAL, "fv is null");
+    if (fv->motion == LUNA_MOVING) return set_error(LUNA_ESTATE, "a moving mesh steps with luna_fv_step_moving_begin/end");
+    if (!(dt >= 0)) return set_error(LUNA_EINVAL, "dt must be >= 0");
+    return fv->dim == 3 ? step_static<3>(fv, dt) : step_static<2>(fv, dt);
+}
+
+LUNA_API luna_status luna_fv_fallbacks(luna_fv* fv, int64_t* out) {
+    if (!fv || !out) return set_error(LUNA_EINVAL, "null argument");
+    LUNA_TRY(read_counters(fv));
+    *out = static_cast<int64_t>(fv->host_counters->fallbacks[0] + fv->host_counters->fallbacks[1]);
+    return LUNA_OK;
+}
+
+LUNA_API luna_status luna_fv_error_word(luna_fv* fv, uint32_t* out) {
+    if (!fv || !out) return set_error(LUNA_EINVAL, "null argument");
+    LUNA_TRY(read_counters(fv));
+    *out = static_cast<uint32_t>(fv->host_counters->error);
+    LUNA_CUDA(cudaMemsetAsync(&fv->counters.ptr->error, 0, sizeof(unsigned long long), fv->stream));
+    return LUNA_OK;
+}
+
+LUNA_API luna_status luna_fv_step_moving_begin(luna_fv* fv, double dt, double* positions_out, int on_device) {
+    if (!fv) return set_error(LUNA_EINVAL, "fv is null");
+    if (fv->motion != LUNA_MOVING) return set_error(LUNA_ESTATE, "not a moving mesh");
+    if (fv->moving_pending) return set_error(LUNA_ESTATE, "a moving step is already open");
+    if (!(dt > 0)) return set_error(LUNA_EINVAL, "dt must be > 0");
+    LUNA_TRY(fv->dim == 3 ? moving_begin<3>(fv, dt) : moving_begin<2>(fv, dt));
+    if (positions_out) LUNA_TRY(copy_out(fv->x.ptr, positions_out, static_cast<size_t>(fv->n) * fv->dim, on_device, fv->stream));
+    return LUNA_OK;
+}
+
+LUNA_API luna_status luna_fv_step_moving_end(luna_fv* fv, const luna_mesh_desc* new_mesh) {
+    if (!fv) return set_error(LUNA_EINVAL, "fv is null");
+    if (!fv->moving_pending) return set_error(LUNA_ESTATE, "luna_fv_step_moving_end without begin");
+    LUNA_TRY(validate_mesh(new_mesh, fv->dim, fv->n));
+    LUNA_TRY(load_mesh(fv, new_mesh));
+    return fv->dim == 3 ? moving_end<3>(fv) : moving_end<2>(fv);
+}
+
+LUNA_API luna_status luna_fv_set_mesh(luna_fv* fv, const luna_mesh_desc* mesh) {
+    if (!fv) return set_error(LUNA_EINVAL, "fv is null");
+    if (fv->moving_pending) return set_error(LUNA_ESTATE, "inside a moving step (use luna_fv_step_moving_end)");
+    LUNA_TRY(validate_mesh(mesh, fv->dim, fv->n));
+    LUNA_TRY(load_mesh(fv, mesh));
+    if (fv->motion == LUNA_MOVING)
+        LUNA_CUDA(cudaMemcpyAsync(fv->x.ptr, fv->pos.ptr, static_cast<size_t>(fv->n) * fv->dim * sizeof(double), cudaMemcpyDeviceToDevice, fv->stream));
+    fv->prims_ready = false;
+    fv->swept = false;
+    LUNA_CUDA(cudaStreamSynchronize(fv->stream));
+    return LUNA_OK;
+}
+
+LUNA_API luna_status luna_fv_positions(luna_fv* fv, double* out, int on_device) {
+    if (!fv) return set_error(LUNA_EINVAL, "fv is null");
+    const double* src = fv->motion == LUNA_MOVING ? fv->x.ptr : fv->pos.ptr;
+    return copy_out(src, out, static_cast<size_t>(fv->n) * fv->dim, on_device, fv->stream);
+}
+
+LUNA_API luna_status luna_fv_point_velocities(luna_fv* fv, double* out, int on_device) {
+    if (!fv) return set_error(LUNA_EINVAL, "fv is null");
+    return copy_out(fv->w.ptr, out, static_cast<size_t>(fv->n) * fv->dim, on_device, fv->stream);
+}
+
+LUNA_API luna_status luna_fv_prims(luna_fv* fv, double* out, int on_device) {
+    if (!fv || !out) return set_error(LUNA_EINVAL, "null argument");
+    const int width = fv->dim + 4;
+    LUNA_CUDA(cudaMemcpy2DAsync(out, width * sizeof(double), fv->prims.ptr, luna::PS * sizeof(double), width * sizeof(double),
+                                static_cast<size_t>(fv->n), on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, fv->stream));
+    LUNA_CUDA(cudaStreamSynchronize(fv->stream));
+    return LUNA_OK;
+}
+
+LUNA_API luna_status luna_fv_gradients(luna_fv* fv, double* out, int on_device) {
+    if (!fv || !out) return set_error(LUNA_EINVAL, "null argument");
+    if (fv->order != 1) return set_error(LUNA_ESTATE, "order 0 has no gradients");
+    const int D = fv->dim, width = (D + 2) * D;
+    const size_t GS = D == 3 ? luna::grad_stride<3>() : luna::grad_stride<2>();
+    const size_t N = static_cast<size_t>(fv->n);
+    if (fv->precision == LUNA_FP64) {
+        LUNA_CUDA(cudaMemcpy2DAsync(out, width * sizeof(double), fv->grad64.ptr, GS * sizeof(double), width * sizeof(double), N,
+                                    on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, fv->stream));
+        LUNA_CUDA(cudaStreamSynchronize(fv->stream));
+        return LUNA_OK;
+    }
+    if (on_device) return set_error(LUNA_EINVAL, "FP32 gradients are copied to host memory only");
+    float* tmp = nullptr;
+    LUNA_CUDA(cudaMallocHost(&tmp, N * GS * sizeof(float)));
+    cudaError_t e = cudaMemcpyAsync(tmp, fv->grad32.ptr, N * GS * sizeof(float), cudaMemcpyDeviceToHost, fv->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(fv->stream);
+    if (e == cudaSuccess)
+        for (size_t i = 0; i < N; ++i)
+            for (int c = 0; c < width; ++c) out[i * width + c] = static_cast<double>(tmp[i * GS + c]);
+    cudaFreeHost(tmp);
+    if (e != cudaSuccess) return set_error(LUNA_ECUDA, cudaGetErrorString(e));
+    return LUNA_OK;
+}
+
+LUNA_API luna_status luna_fv_set_timing(luna_fv* fv, int on) {
+    if (!fv) return set_error(LUNA_EINVAL, "fv is null");
+    fv->timing = on != 0;
+    return LUNA_OK;
+}
+
+LUNA_API luna_status luna_fv_timings(luna_fv* fv, luna_timings* out, int reset) {
+    if (!fv || !out) return set_error(LUNA_EINVAL, "null argument");
+    LUNA_CUDA(cudaStreamSynchronize(fv->stream));
+    for (const auto& p : fv->pending) {
+        float ms = 0;
+        LUNA_CUDA(cudaEventElapsedTime(&ms, fv->event_pool[p.second].first, fv->event_pool[p.second].second));
+        fv->phase_ms[p.first] += ms;
+        fv->phase_launches[p.first] += 1;
+    }
+    fv->pending.clear();
+    for (int k = 0; k < 5; ++k) {
+        out->ms[k] = fv->phase_ms[k];
+        out->launches[k] = fv->phase_launches[k];
+        if (reset) {
+            fv->phase_ms[k] = 0;
+            fv->phase_launches[k] = 0;
+        }
+    }
+    return LUNA_OK;
+}
+
+LUNA_API luna_status luna_fv_device_bytes(luna_fv* fv, int64_t* out) {
+    if (!fv || !out) return set_error(LUNA_EINVAL, "null argument");
+    size_t b = 0;
+    b += fv->owner.bytes() + fv->neighbour.bytes() + fv->start.bytes() + fv->list.bytes();
+    b += fv->area.bytes() + fv->mag.bytes() + fv->fcen.bytes() + fv->cen.bytes() + fv->vol.bytes() + fv->pos.bytes();
+    b += fv->q.bytes() + fv->next.bytes() + fv->prims.bytes() + fv->grad64.bytes() + fv->grad32.bytes() + fv->flux.bytes();
+    b += fv->w.bytes() + fv->x.bytes() + fv->old_cen.bytes() + fv->steps.bytes() + fv->counters.bytes();
+    *out = static_cast<int64_t>(b);
+    return LUNA_OK;
+}
+
+}  // extern "C"

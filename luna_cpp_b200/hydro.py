@@ -1,0 +1,265 @@
+"""The host-side mirror of luna-cpp's ``hydro::FiniteVolume<D>`` (src/hydro/finite_volume.hpp:47-239) over the C ABI of
+``libluna_b200.so`` (include/luna_b200.h).
+
+Same call order as the reference's drivers (``dt = fv.time_step(courant); fv.step(dt)``), same constructor options
+(order, update loop, limiter, motion; the Riemann solver and the precision policy as arguments), same extensive state
+Q[N][D + 2]. Errors come back as ``LunaError`` carrying the library's status and message, where the reference throws
+``std::invalid_argument`` / ``std::logic_error``. There is no CPU path: without the CUDA library or a GPU, construction
+fails.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native
+
+STATUS = {0: "ok", 1: "invalid argument", 2: "out of memory", 3: "CUDA error", 4: "non-finite value",
+          5: "device wait timed out", 6: "call out of order"}
+
+UPDATE = {"per_cell": 0, "per_face": 1}
+LIMITER = {"face_centroid": 0, "none": 1}
+MOTION = {"static_mesh": 0, "static": 0, "moving": 1}
+RIEMANN = {"hllc": 0, "hll": 1}
+PRECISION = {"fp64": 0, "double": 0, "fp32": 1, "riemann32": 1}
+
+
+class LunaError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+@dataclass
+class Gas:
+    """hydro::Gas (euler.hpp:82-101)."""
+
+    gamma: float = 5.0 / 3.0
+    smallr: float = 1e-10
+    smallc: float = 1e-10
+
+
+class _Gas(ctypes.Structure):
+    _fields_ = [("gamma", ctypes.c_double), ("smallr", ctypes.c_double), ("smallc", ctypes.c_double)]
+
+
+class MeshDesc(ctypes.Structure):
+    """luna_mesh_desc (include/luna_b200.h)."""
+
+    _fields_ = [("dim", ctypes.c_int), ("n_cells", ctypes.c_int64), ("n_faces", ctypes.c_int64),
+                ("owner", ctypes.c_void_p), ("neighbour", ctypes.c_void_p), ("cell_face_start", ctypes.c_void_p),
+                ("cell_face", ctypes.c_void_p), ("area", ctypes.c_void_p), ("face_centroid", ctypes.c_void_p),
+                ("centroid", ctypes.c_void_p), ("volume", ctypes.c_void_p), ("positions", ctypes.c_void_p),
+                ("box", ctypes.c_double * 3), ("on_device", ctypes.c_int)]
+
+
+# Every entry point of include/luna_b200.h with its ctypes signature.
+P, I, D64, I64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int64
+SIGNATURES = {
+    "luna_fv_create": ([P, P, I, I, I, I, I, I, P], I),
+    "luna_fv_destroy": ([P], I),
+    "luna_fv_set_stream": ([P, P], I),
+    "luna_fv_state": ([P, P], I),
+    "luna_fv_set_state": ([P, P, I], I),
+    "luna_fv_get_state": ([P, P, I], I),
+    "luna_fv_time_step": ([P, D64, P], I),
+    "luna_fv_step": ([P, D64], I),
+    "luna_fv_fallbacks": ([P, P], I),
+    "luna_fv_error_word": ([P, P], I),
+    "luna_fv_step_moving_begin": ([P, D64, P, I], I),
+    "luna_fv_step_moving_end": ([P, P], I),
+    "luna_fv_set_mesh": ([P, P], I),
+    "luna_fv_positions": ([P, P, I], I),
+    "luna_fv_point_velocities": ([P, P, I], I),
+    "luna_fv_prims": ([P, P, I], I),
+    "luna_fv_gradients": ([P, P, I], I),
+    "luna_status_string": ([I], ctypes.c_char_p),
+    "luna_last_error": ([], ctypes.c_char_p),
+    "luna_fv_device_bytes": ([P, P], I),
+    "luna_fv_set_timing": ([P, I], I),
+    "luna_fv_timings": ([P, P, I], I),
+}
+
+PHASES = ("primitives", "sweep", "fluxes", "update", "drift")
+
+
+class _Timings(ctypes.Structure):
+    _fields_ = [("ms", ctypes.c_double * 5), ("launches", ctypes.c_int64 * 5)]
+
+
+def lib():
+    L = _native.load("hydro")
+    if not getattr(L, "_typed", False):
+        for name, (args, res) in SIGNATURES.items():
+            if hasattr(L, name):
+                fn = getattr(L, name)
+                fn.argtypes = args
+                fn.restype = res
+        L._typed = True
+    return L
+
+
+def check(status: int):
+    if status != 0:
+        raise LunaError(status, lib().luna_last_error().decode())
+
+
+def mesh_desc(mesh, keep: list) -> MeshDesc:
+    """A luna_mesh_desc over the host arrays of a luna_cpp_b200.mesh.Mesh (kept alive through ``keep``)."""
+    arrays = [np.ascontiguousarray(mesh.owner, dtype=np.int32), np.ascontiguousarray(mesh.neighbour, dtype=np.int32),
+              np.ascontiguousarray(mesh.cell_face_start, dtype=np.int32),
+              np.ascontiguousarray(mesh.cell_face, dtype=np.int32), np.ascontiguousarray(mesh.area, dtype=np.float64),
+              np.ascontiguousarray(mesh.face_centroid, dtype=np.float64),
+              np.ascontiguousarray(mesh.centroid, dtype=np.float64), np.ascontiguousarray(mesh.volume, dtype=np.float64),
+              np.ascontiguousarray(mesh.positions, dtype=np.float64)]
+    keep.append(arrays)
+    d = MeshDesc()
+    d.dim = mesh.dim
+    d.n_cells = mesh.n_cells
+    d.n_faces = mesh.n_faces
+    (d.owner, d.neighbour, d.cell_face_start, d.cell_face, d.area, d.face_centroid, d.centroid, d.volume,
+     d.positions) = [a.ctypes.data for a in arrays]
+    for a in range(3):
+        d.box[a] = mesh.box[a] if a < len(mesh.box) else 0.0
+    d.on_device = 0
+    return d
+
+
+class FiniteVolume:
+    """hydro::FiniteVolume<D, Cuda, Riemann, Precision> on one GPU (the current device)."""
+
+    def __init__(self, mesh, gas: Gas | None = None, order: int = 1, update: str = "per_face",
+                 limiter: str = "face_centroid", motion: str = "static_mesh", riemann: str = "hllc",
+                 precision: str = "fp64"):
+        self.mesh = mesh
+        self.dim = mesh.dim
+        self.V = mesh.dim + 2
+        self.n = mesh.n_cells
+        self.gas = gas or Gas()
+        g = _Gas(self.gas.gamma, self.gas.smallr, self.gas.smallc)
+        keep: list = []
+        desc = mesh_desc(mesh, keep)
+        h = ctypes.c_void_p()
+        check(lib().luna_fv_create(ctypes.byref(desc), ctypes.byref(g), order, UPDATE[update], LIMITER[limiter],
+                                   MOTION[motion], RIEMANN[riemann], PRECISION[precision], ctypes.byref(h)))
+        self._h = h
+        self.order, self.update, self.limiter, self.motion = order, update, limiter, motion
+        self.riemann, self.precision = riemann, precision
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().luna_fv_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    # ---- state ----
+    def state_ptr(self) -> int:
+        """state(): the device pointer of Q[N][V]; the primitive rows are recomputed by the next time_step()."""
+        p = ctypes.c_void_p()
+        check(lib().luna_fv_state(self._h, ctypes.byref(p)))
+        return int(p.value)
+
+    def set_state(self, q) -> None:
+        """Q from host (numpy) or device memory (a CUDA torch tensor, contiguous float64 [N, V])."""
+        if hasattr(q, "is_cuda") and q.is_cuda:
+            check(lib().luna_fv_set_state(self._h, ctypes.c_void_p(q.data_ptr()), 1))
+            return
+        a = np.ascontiguousarray(q, dtype=np.float64)
+        if a.shape != (self.n, self.V):
+            raise ValueError(f"state must be [{self.n}, {self.V}]")
+        check(lib().luna_fv_set_state(self._h, a.ctypes.data, 0))
+
+    def get_state(self, out=None):
+        if out is not None and hasattr(out, "is_cuda") and out.is_cuda:
+            check(lib().luna_fv_get_state(self._h, ctypes.c_void_p(out.data_ptr()), 1))
+            return out
+        a = np.empty((self.n, self.V), dtype=np.float64) if out is None else out
+        check(lib().luna_fv_get_state(self._h, a.ctypes.data, 0))
+        return a
+
+    # ---- the step ----
+    def time_step(self, courant: float = 0.3) -> float:
+        dt = ctypes.c_double()
+        check(lib().luna_fv_time_step(self._h, courant, ctypes.byref(dt)))
+        return dt.value
+
+    def step(self, dt: float) -> None:
+        check(lib().luna_fv_step(self._h, dt))
+
+    def step_moving(self, dt: float, remesh) -> object:
+        """One moving step: the t^n fluxes, the drift, ``remesh(positions) -> Mesh`` (the mesh library's update), the
+        t^n+1 fluxes. Returns the new mesh."""
+        pos = np.empty((self.n, self.dim), dtype=np.float64)
+        check(lib().luna_fv_step_moving_begin(self._h, dt, pos.ctypes.data, 0))
+        new_mesh = remesh(pos)
+        keep: list = []
+        desc = mesh_desc(new_mesh, keep)
+        check(lib().luna_fv_step_moving_end(self._h, ctypes.byref(desc)))
+        self.mesh = new_mesh
+        return new_mesh
+
+    def set_mesh(self, mesh) -> None:
+        keep: list = []
+        desc = mesh_desc(mesh, keep)
+        check(lib().luna_fv_set_mesh(self._h, ctypes.byref(desc)))
+        self.mesh = mesh
+
+    def fallbacks(self) -> int:
+        out = ctypes.c_int64()
+        check(lib().luna_fv_fallbacks(self._h, ctypes.byref(out)))
+        return int(out.value)
+
+    def error_word(self) -> int:
+        out = ctypes.c_uint32()
+        check(lib().luna_fv_error_word(self._h, ctypes.byref(out)))
+        return int(out.value)
+
+    # ---- rows ----
+    def prims(self) -> np.ndarray:
+        a = np.empty((self.n, self.V + 2), dtype=np.float64)
+        check(lib().luna_fv_prims(self._h, a.ctypes.data, 0))
+        return a
+
+    def gradients(self) -> np.ndarray:
+        a = np.empty((self.n, self.V * self.dim), dtype=np.float64)
+        check(lib().luna_fv_gradients(self._h, a.ctypes.data, 0))
+        return a
+
+    def point_velocities(self) -> np.ndarray:
+        a = np.empty((self.n, self.dim), dtype=np.float64)
+        check(lib().luna_fv_point_velocities(self._h, a.ctypes.data, 0))
+        return a
+
+    def positions(self) -> np.ndarray:
+        a = np.empty((self.n, self.dim), dtype=np.float64)
+        check(lib().luna_fv_positions(self._h, a.ctypes.data, 0))
+        return a
+
+    def set_stream(self, stream_ptr: int) -> None:
+        check(lib().luna_fv_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
+    def set_timing(self, on: bool = True) -> None:
+        check(lib().luna_fv_set_timing(self._h, 1 if on else 0))
+
+    def timings(self, reset: bool = True) -> dict:
+        """{phase: (ms, launches)} since the last reset (hydro::Timings)."""
+        t = _Timings()
+        check(lib().luna_fv_timings(self._h, ctypes.byref(t), 1 if reset else 0))
+        return {name: (t.ms[k], int(t.launches[k])) for k, name in enumerate(PHASES)}
+
+    def device_bytes(self) -> int:
+        out = ctypes.c_int64()
+        check(lib().luna_fv_device_bytes(self._h, ctypes.byref(out)))
+        return int(out.value)

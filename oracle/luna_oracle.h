@@ -1,0 +1,81 @@
+/* CPU oracle of luna-cpp's per-step finite-volume hydro update: TEST INFRASTRUCTURE ONLY.
+ *
+ * A plain C restatement of the reference's algorithm (src/hydro/euler.hpp, src/hydro/finite_volume.hpp), used by the
+ * tests as the checker of the CUDA path and by bench.py as the timed CPU baseline. Nothing in the product links it.
+ * Each function cites the reference lines it follows. Arithmetic is IEEE double in the reference's operation order,
+ * compiled without multiply-add contraction.
+ *
+ * Pinned by: LUNA's HLL/HLLC golden fluxes (src/test/hydro_test.cpp:48-80, to 1e-14), the flux invariants
+ * (hydro_test.cpp:106-132), and the mesh invariants (uniform state, conservation, determinism; hydro_test.cpp:185-274).
+ * The whole 3D step depends on voronoi-cpp's mesh, which is absent: its parity with the reference is pinned only through
+ * those invariants (see the tests).
+ */
+#ifndef LUNA_ORACLE_H
+#define LUNA_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    double gamma, smallr, smallc, inverse_gm1;
+    float inverse_gm1_float;
+} lo_gas;
+
+/* voronoi-cpp's arrays (finite_volume.hpp:257-327), host pointers. */
+typedef struct {
+    int dim;
+    int64_t n, f;
+    const int32_t *owner, *neighbour, *start, *list;
+    const double *area, *face_centroid, *centroid, *volume, *positions;
+    double box[3];
+} lo_mesh;
+
+typedef struct lo_fv lo_fv;
+
+void lo_gas_init(lo_gas* gas, double gamma);
+
+/* euler.hpp: per-state functions (D = 2 or 3, states of D + 2 entries). */
+void lo_primitive(int D, const double* U, const lo_gas* gas, double* W);
+void lo_conserved(int D, const double* W, const lo_gas* gas, double* U);
+void lo_half_step(int D, const double* W, const double* g /* [V][D] */, double dt, const lo_gas* gas, double* out);
+void lo_hllc_flux(int D, const double* L, const double* R, const double* n, const double* w, const lo_gas* gas, double* F);
+void lo_hll_flux(int D, const double* L, const double* R, const double* n, const double* w, const lo_gas* gas, double* F);
+/* The float Riemann solve (T = float), as FaceFlux::solve runs it for a float policy (finite_volume.hpp:1400-1413). */
+void lo_hllc_flux_float(int D, const float* L, const float* R, const float* n, const lo_gas* gas, float* F);
+
+/* FiniteVolume<D> (static or moving mesh, order 0/1, per-face or per-cell update, face-centroid limiter or none,
+ * HLLC (riemann 0) or HLL (1)). grad_float: the Grad32 policy (gradients, limiter, face-state change in float). */
+lo_fv* lo_fv_create(const lo_mesh* mesh, const lo_gas* gas, int order, int per_face, int limiter_none, int riemann,
+                    int moving, int grad_float, int riemann_float);
+void lo_fv_destroy(lo_fv* fv);
+double* lo_fv_state(lo_fv* fv); /* Q [N][V], extensive; writing it marks the primitives stale */
+void lo_fv_state_changed(lo_fv* fv);
+double lo_fv_time_step(lo_fv* fv, double courant);
+void lo_fv_step(lo_fv* fv, double dt);
+int64_t lo_fv_fallbacks(const lo_fv* fv);
+int lo_fv_threads(int threads); /* sets the OpenMP thread count (<= 0: all); returns the count in use */
+/* Rows of the last sweep: prims [N][V + 2] (W, c, r) and gradients [N][V * D] (double). */
+const double* lo_fv_prims(const lo_fv* fv);
+const double* lo_fv_gradients(const lo_fv* fv);
+/* Moving mesh: point velocities of the last sweep [N][D]; positions [N][D]. */
+const double* lo_fv_point_velocities(const lo_fv* fv);
+/* Moving step in two halves around the caller's remesh (step_moving, finite_volume.hpp:1497-1519):
+ * begin snaps the points, keeps the centroids, applies the t^n fluxes (half dt) and writes the new positions
+ * [N][D] (on the grid) into positions_out; the caller builds the mesh of those positions and passes it to end. */
+void lo_fv_step_moving_begin(lo_fv* fv, double dt, double* positions_out);
+void lo_fv_step_moving_end(lo_fv* fv, const lo_mesh* new_mesh);
+/* The adjoint of one static step at fixed dt (step_adjoint, finite_volume.hpp:2201-2231): qbar <- J^T qbar, with the
+ * forward state Q^n in the object. */
+void lo_fv_step_adjoint(lo_fv* fv, double dt, double* qbar);
+
+/* The snapping grid of a box (voronoi-cpp's exact_predicates): step = 2^-30 of the longest side. */
+double lo_grid_step(int D, const double* box);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

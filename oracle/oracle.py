@@ -1,0 +1,208 @@
+"""Python binding of the CPU oracle (``liboracle.so``): TEST INFRASTRUCTURE ONLY.
+
+Only the tests, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use this module, as the checker of the CUDA
+path; the product never imports it. See ``luna_oracle.h`` for what the oracle restates and how it is pinned.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+
+
+class _Gas(ctypes.Structure):
+    _fields_ = [("gamma", ctypes.c_double), ("smallr", ctypes.c_double), ("smallc", ctypes.c_double),
+                ("inverse_gm1", ctypes.c_double), ("inverse_gm1_float", ctypes.c_float)]
+
+
+class _Mesh(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int), ("n", ctypes.c_int64), ("f", ctypes.c_int64),
+                ("owner", ctypes.c_void_p), ("neighbour", ctypes.c_void_p), ("start", ctypes.c_void_p),
+                ("list", ctypes.c_void_p), ("area", ctypes.c_void_p), ("face_centroid", ctypes.c_void_p),
+                ("centroid", ctypes.c_void_p), ("volume", ctypes.c_void_p), ("positions", ctypes.c_void_p),
+                ("box", ctypes.c_double * 3)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB):
+        from luna_cpp_b200 import build
+        build.build_oracle()
+    L = ctypes.CDLL(LIB)
+    P, D, I, V = ctypes.c_void_p, ctypes.c_double, ctypes.c_int, None
+    sig = {
+        "lo_gas_init": ([P, D], V),
+        "lo_primitive": ([I, P, P, P], V),
+        "lo_conserved": ([I, P, P, P], V),
+        "lo_half_step": ([I, P, P, D, P, P], V),
+        "lo_hllc_flux": ([I, P, P, P, P, P, P], V),
+        "lo_hll_flux": ([I, P, P, P, P, P, P], V),
+        "lo_hllc_flux_float": ([I, P, P, P, P, P], V),
+        "lo_fv_create": ([P, P, I, I, I, I, I, I, I], P),
+        "lo_fv_destroy": ([P], V),
+        "lo_fv_state": ([P], P),
+        "lo_fv_state_changed": ([P], V),
+        "lo_fv_time_step": ([P, D], D),
+        "lo_fv_step": ([P, D], V),
+        "lo_fv_fallbacks": ([P], ctypes.c_int64),
+        "lo_fv_threads": ([I], I),
+        "lo_fv_prims": ([P], P),
+        "lo_fv_gradients": ([P], P),
+        "lo_fv_point_velocities": ([P], P),
+        "lo_fv_step_moving_begin": ([P, D, P], V),
+        "lo_fv_step_moving_end": ([P, P], V),
+        "lo_grid_step": ([I, P], D),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    if hasattr(L, "lo_fv_step_adjoint"):
+        L.lo_fv_step_adjoint.argtypes = [P, D, P]
+        L.lo_fv_step_adjoint.restype = None
+    _lib = L
+    return L
+
+
+def gas(gamma: float = 5.0 / 3.0) -> _Gas:
+    g = _Gas()
+    lib().lo_gas_init(ctypes.byref(g), gamma)
+    return g
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def riemann(L, R, n, w=None, gamma=5.0 / 3.0, solver="hllc"):
+    """One flux of HLLC (or HLL) through a face of unit normal n moving with w."""
+    D = len(n)
+    Lr = np.ascontiguousarray(L, dtype=np.float64)
+    Rr = np.ascontiguousarray(R, dtype=np.float64)
+    nn = np.ascontiguousarray(n, dtype=np.float64)
+    ww = np.zeros(D) if w is None else np.ascontiguousarray(w, dtype=np.float64)
+    F = np.zeros(D + 2)
+    g = gas(gamma)
+    fn = lib().lo_hllc_flux if solver == "hllc" else lib().lo_hll_flux
+    fn(D, _ptr(Lr), _ptr(Rr), _ptr(nn), _ptr(ww), ctypes.byref(g), _ptr(F))
+    return F
+
+
+def conserved(W, gamma=5.0 / 3.0):
+    W = np.ascontiguousarray(W, dtype=np.float64)
+    U = np.zeros_like(W)
+    g = gas(gamma)
+    D = W.shape[-1] - 2
+    flat_W = W.reshape(-1, D + 2)
+    flat_U = U.reshape(-1, D + 2)
+    for k in range(flat_W.shape[0]):
+        lib().lo_conserved(D, _ptr(flat_W[k]), ctypes.byref(g), _ptr(flat_U[k]))
+    return U
+
+
+class OracleFV:
+    """The oracle's FiniteVolume<D> on one mesh (luna_cpp_b200.mesh.Mesh)."""
+
+    def __init__(self, mesh, gamma=5.0 / 3.0, order=1, per_face=True, limiter="face_centroid", riemann="hllc",
+                 moving=False, precision="double"):
+        self._keep = []
+        self.mesh = mesh
+        self.dim = mesh.dim
+        self.V = mesh.dim + 2
+        self._gas = gas(gamma)
+        m = self._desc(mesh)
+        grad_float = 1 if precision in ("grad32", "riemann32") else 0
+        riemann_float = 1 if precision == "riemann32" else 0
+        self._h = lib().lo_fv_create(ctypes.byref(m), ctypes.byref(self._gas), order, 1 if per_face else 0,
+                                      1 if limiter == "none" else 0, 1 if riemann == "hll" else 0,
+                                      1 if moving else 0, grad_float, riemann_float)
+
+    def _desc(self, mesh):
+        arrays = [np.ascontiguousarray(x) for x in (mesh.owner, mesh.neighbour, mesh.cell_face_start, mesh.cell_face,
+                                                     mesh.area, mesh.face_centroid, mesh.centroid, mesh.volume,
+                                                     mesh.positions)]
+        self._keep.append(arrays)
+        m = _Mesh()
+        m.dim = mesh.dim
+        m.n = mesh.n_cells
+        m.f = mesh.n_faces
+        (m.owner, m.neighbour, m.start, m.list, m.area, m.face_centroid, m.centroid, m.volume,
+         m.positions) = [a.ctypes.data for a in arrays]
+        for a in range(3):
+            m.box[a] = mesh.box[a] if a < len(mesh.box) else 0.0
+        self._mesh_struct = m
+        return m
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().lo_fv_destroy(h)
+            self._h = None
+
+    @property
+    def n(self):
+        return self.mesh.n_cells
+
+    def state(self) -> np.ndarray:
+        ptr = lib().lo_fv_state(self._h)
+        buf = (ctypes.c_double * (self.n * self.V)).from_address(ptr)
+        return np.frombuffer(buf, dtype=np.float64).reshape(self.n, self.V)
+
+    def set_state(self, q):
+        self.state()[:] = q
+
+    def get_state(self):
+        return self.state().copy()
+
+    def time_step(self, courant=0.3):
+        return lib().lo_fv_time_step(self._h, courant)
+
+    def step(self, dt):
+        lib().lo_fv_step(self._h, dt)
+
+    def fallbacks(self):
+        return int(lib().lo_fv_fallbacks(self._h))
+
+    def prims(self):
+        ptr = lib().lo_fv_prims(self._h)
+        buf = (ctypes.c_double * (self.n * (self.V + 2))).from_address(ptr)
+        return np.frombuffer(buf, dtype=np.float64).reshape(self.n, self.V + 2).copy()
+
+    def gradients(self):
+        ptr = lib().lo_fv_gradients(self._h)
+        buf = (ctypes.c_double * (self.n * self.V * self.dim)).from_address(ptr)
+        return np.frombuffer(buf, dtype=np.float64).reshape(self.n, self.V * self.dim).copy()
+
+    def point_velocities(self):
+        ptr = lib().lo_fv_point_velocities(self._h)
+        buf = (ctypes.c_double * (self.n * self.dim)).from_address(ptr)
+        return np.frombuffer(buf, dtype=np.float64).reshape(self.n, self.dim).copy()
+
+    def step_moving(self, dt, remesh):
+        """One moving step; remesh(positions) -> Mesh builds the t^n+1 mesh."""
+        pos = np.zeros((self.n, self.dim))
+        lib().lo_fv_step_moving_begin(self._h, dt, _ptr(pos))
+        new_mesh = remesh(pos)
+        self.mesh = new_mesh
+        m = self._desc(new_mesh)
+        lib().lo_fv_step_moving_end(self._h, ctypes.byref(m))
+        self._keep = self._keep[-1:]
+        return new_mesh
+
+    def step_adjoint(self, dt, qbar):
+        q = np.ascontiguousarray(qbar, dtype=np.float64).copy()
+        lib().lo_fv_step_adjoint(self._h, dt, _ptr(q))
+        return q
+
+
+def threads(n: int = 0) -> int:
+    return int(lib().lo_fv_threads(n))

@@ -1,0 +1,227 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle on the same meshes and states, plus the reference's
+mesh invariants (src/test/hydro_test.cpp) on the GPU. Tolerances: FP64 one step 1e-13 relative (max norm), 50 steps of
+the 32^3 blast 1e-12 relative L1 per conserved field; the FP32 policy against the oracle's same policy 1e-6 relative
+(max norm) after one step; conservation 1e-14; bits equal run to run."""
+import numpy as np
+import pytest
+
+from conftest import jittered_mesh, random_mesh
+from oracle import oracle as O
+from luna_cpp_b200 import hydro
+from luna_cpp_b200.problems import acoustic_wave, point_blast, rough_state, shear_layer
+
+pytestmark = pytest.mark.gpu
+
+
+def relative(a, b):
+    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+def rel_l1(a, b):
+    return np.abs(a - b).sum(0) / np.abs(b).sum(0)
+
+
+def pair(mesh, q0, **kw):
+    prec = kw.pop("precision", "fp64")
+    gpu = hydro.FiniteVolume(mesh, precision=prec, **kw)
+    ora = O.OracleFV(mesh, order=kw.get("order", 1), per_face=kw.get("update", "per_face") == "per_face",
+                     limiter=kw.get("limiter", "face_centroid"), riemann=kw.get("riemann", "hllc"),
+                     moving=kw.get("motion", "static_mesh") == "moving",
+                     precision="riemann32" if prec == "fp32" else "double")
+    gpu.set_state(q0)
+    ora.set_state(q0)
+    return gpu, ora
+
+
+@pytest.mark.parametrize("order", [0, 1])
+@pytest.mark.parametrize("update", ["per_face", "per_cell"])
+@pytest.mark.parametrize("riemann", ["hllc", "hll"])
+def test_one_step_fp64(cuda, order, update, riemann):
+    mesh = jittered_mesh(16)
+    q0 = rough_state(mesh.n_cells) * mesh.volume[:, None]
+    gpu, ora = pair(mesh, q0, order=order, update=update, riemann=riemann)
+    dt_g, dt_o = gpu.time_step(0.3), ora.time_step(0.3)
+    assert abs(dt_g - dt_o) <= 1e-14 * dt_o
+    assert relative(gpu.prims(), ora.prims()) < 1e-14
+    if order == 1:
+        assert relative(gpu.gradients(), ora.gradients()) < 1e-11
+    gpu.step(dt_o)
+    ora.step(dt_o)
+    assert relative(gpu.get_state(), ora.get_state()) < 1e-13
+    assert gpu.fallbacks() == ora.fallbacks()
+
+
+def test_limiter_none_and_uniform_random_mesh(cuda):
+    mesh = random_mesh(4096)
+    q0 = rough_state(mesh.n_cells) * mesh.volume[:, None]
+    gpu, ora = pair(mesh, q0, limiter="none")
+    for _ in range(2):
+        dt = ora.time_step(0.3)
+        assert abs(gpu.time_step(0.3) - dt) <= 1e-14 * dt
+        gpu.step(dt)
+        ora.step(dt)
+    assert relative(gpu.get_state(), ora.get_state()) < 1e-12
+
+
+def test_blast_32_fp64_50_steps(cuda):
+    """The plain-method configuration: 32^3 jittered (0.1) mesh, point blast, MUSCL-Hancock + HLLC, CFL 0.3, 50 steps,
+    FP64, against the oracle: relative L1 <= 1e-12 for every conserved field (each side takes its own dt)."""
+    mesh = jittered_mesh(32)
+    q0 = point_blast(mesh)
+    gpu, ora = pair(mesh, q0)
+    for _ in range(50):
+        gpu.step(gpu.time_step(0.3))
+        ora.step(ora.time_step(0.3))
+    g, o = gpu.get_state(), ora.get_state()
+    assert np.all(np.isfinite(g))
+    assert np.max(rel_l1(g, o)) < 1e-12
+    assert gpu.fallbacks() == ora.fallbacks()
+
+
+def test_fp32_policy_matches_oracle_policy(cuda):
+    mesh = jittered_mesh(16)
+    q0 = rough_state(mesh.n_cells) * mesh.volume[:, None]
+    gpu, ora = pair(mesh, q0, precision="fp32")
+    dt = ora.time_step(0.3)
+    assert abs(gpu.time_step(0.3) - dt) <= 1e-14 * dt
+    gpu.step(dt)
+    ora.step(dt)
+    assert relative(gpu.get_state(), ora.get_state()) < 1e-6
+
+
+def test_fp32_against_fp64_acoustic_wave(cuda):
+    """FP32 face arithmetic against FP64 on the smooth wave (amplitude 1e-6, 20 steps): relative L1 of the perturbation
+    of Q (Q minus the background) within 1e-5."""
+    mesh = jittered_mesh(16)
+    q0 = acoustic_wave(mesh, amplitude=1e-6)
+    res = {}
+    for prec in ("fp64", "fp32"):
+        fv = hydro.FiniteVolume(mesh, precision=prec)
+        fv.set_state(q0)
+        for _ in range(20):
+            fv.step(fv.time_step(0.3))
+        res[prec] = fv.get_state()
+    background = acoustic_wave(mesh, amplitude=0.0)
+    p64, p32 = res["fp64"] - background, res["fp32"] - background
+    assert np.abs(p32 - p64).sum() / np.abs(p64).sum() < 1e-5
+
+
+@pytest.mark.parametrize("order", [0, 1])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_uniform_state_stays_uniform(cuda, order, precision):
+    mesh = jittered_mesh(16)
+    W = np.array([1.3, 0.3, -0.2, 0.1, 0.7])
+    U = O.conserved(W)
+    fv = hydro.FiniteVolume(mesh, order=order, precision=precision)
+    fv.set_state(np.tile(U, (mesh.n_cells, 1)) * mesh.volume[:, None])
+    for _ in range(3):
+        fv.step(fv.time_step(0.3))
+    got = fv.get_state() / mesh.volume[:, None]
+    assert relative(got, np.tile(U, (mesh.n_cells, 1))) < (1e-13 if precision == "fp64" else 1e-6)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_conservation_and_determinism(cuda, precision):
+    mesh = jittered_mesh(16)
+    q0 = rough_state(mesh.n_cells) * mesh.volume[:, None]
+    outs = []
+    for _ in range(2):
+        fv = hydro.FiniteVolume(mesh, precision=precision)
+        fv.set_state(q0)
+        for _ in range(10):
+            fv.step(fv.time_step(0.3))
+        outs.append(fv.get_state())
+    assert np.array_equal(outs[0], outs[1])
+    before = q0.astype(np.longdouble).sum(0)
+    after = outs[0].astype(np.longdouble).sum(0)
+    assert abs(float((after[0] - before[0]) / before[0])) < 1e-14
+    assert abs(float((after[4] - before[4]) / before[4])) < 1e-14
+    scale = float(before[0]) * np.sqrt(float(before[4] / before[0]))
+    assert np.max(np.abs((after[1:4] - before[1:4]).astype(np.float64))) / scale < 1e-14
+
+
+def test_per_cell_and_per_face_agree(cuda):
+    mesh = jittered_mesh(16)
+    q0 = rough_state(mesh.n_cells) * mesh.volume[:, None]
+    outs = []
+    for update in ("per_face", "per_cell"):
+        fv = hydro.FiniteVolume(mesh, update=update)
+        fv.set_state(q0)
+        for _ in range(10):
+            fv.step(fv.time_step(0.3))
+        outs.append(fv.get_state())
+    assert relative(outs[1], outs[0]) < 1e-12
+
+
+def test_2d_shear_layer_matches_oracle(cuda):
+    mesh = jittered_mesh(32, dim=2)
+    a = np.random.default_rng(3).standard_normal(8)
+    q0 = shear_layer(mesh, a)
+    gpu, ora = pair(mesh, q0)
+    for _ in range(5):
+        dt = ora.time_step(0.3)
+        assert abs(gpu.time_step(0.3) - dt) <= 1e-14 * dt
+        gpu.step(dt)
+        ora.step(dt)
+    assert relative(gpu.get_state(), ora.get_state()) < 1e-12
+
+
+def test_moving_step_matches_oracle(cuda):
+    """step_moving on a moving mesh: the t^n fluxes, the drift on the 2^-30 grid, the remesh, the t^n+1 fluxes."""
+    from luna_cpp_b200.mesh import build_mesh
+
+    mesh = jittered_mesh(12)
+    step = 2.0 ** -30
+    mesh = build_mesh(np.round(mesh.positions / step) * step)  # generators on the snapping grid
+    q0 = point_blast(mesh, radius_cells=2.5)
+    gpu, ora = pair(mesh, q0, motion="moving")
+    remesh = lambda pos: build_mesh(pos)
+    for _ in range(3):
+        dt = ora.time_step(0.3)
+        assert abs(gpu.time_step(0.3) - dt) <= 1e-14 * dt
+        assert relative(gpu.point_velocities(), ora.point_velocities()) < 1e-13
+        mg = gpu.step_moving(dt, remesh)
+        mo = ora.step_moving(dt, remesh)
+        assert np.array_equal(mg.positions, mo.positions)
+    g, o = gpu.get_state(), ora.get_state()
+    assert relative(g, o) < 1e-12
+    before = q0.sum(0)
+    assert abs((g[:, 0].sum() - before[0]) / before[0]) < 1e-14
+    assert abs((g[:, 4].sum() - before[4]) / before[4]) < 1e-14
+
+
+def test_errors_are_status_codes(cuda):
+    mesh = jittered_mesh(8)
+    fv = hydro.FiniteVolume(mesh)
+    with pytest.raises(hydro.LunaError) as e:
+        fv.step(-1.0)
+    assert e.value.status == 1
+    with pytest.raises(hydro.LunaError) as e:
+        hydro.lib()
+        hydro.check(hydro.lib().luna_fv_step_moving_end(fv.handle, None))
+    assert e.value.status in (1, 6)
+    with pytest.raises(hydro.LunaError):
+        hydro.FiniteVolume(mesh, motion="moving", update="per_cell")
+
+
+def test_full_size_properties(cuda):
+    """The 128^3 blast (the benchmark's workload) at full size: 3 steps stay finite, conserve mass and energy to 1e-14,
+    and repeat bit for bit."""
+    mesh = jittered_mesh(128)
+    q0 = point_blast(mesh)
+    outs = []
+    for _ in range(2):
+        fv = hydro.FiniteVolume(mesh)
+        fv.set_state(q0)
+        for _ in range(3):
+            dt = fv.time_step(0.3)
+            assert dt > 0
+            fv.step(dt)
+        outs.append(fv.get_state())
+        fv.close()
+    assert np.all(np.isfinite(outs[0]))
+    assert np.array_equal(outs[0], outs[1])
+    before = q0.astype(np.longdouble).sum(0)
+    after = outs[0].astype(np.longdouble).sum(0)
+    assert abs(float((after[0] - before[0]) / before[0])) < 1e-14
+    assert abs(float((after[4] - before[4]) / before[4])) < 1e-13

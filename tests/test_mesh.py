@@ -1,0 +1,51 @@
+"""The periodic Voronoi builder emits voronoi-cpp's layout: CPU only."""
+import numpy as np
+import pytest
+
+from conftest import jittered_mesh, random_mesh
+from luna_cpp_b200.mesh import build_mesh, jittered_points
+
+
+@pytest.mark.parametrize("mesh_fn", [lambda: jittered_mesh(16), lambda: random_mesh(4096), lambda: jittered_mesh(32, 2)])
+def test_layout_and_closure(mesh_fn):
+    m = mesh_fn()
+    N, F, D = m.n_cells, m.n_faces, m.dim
+    assert np.isclose(m.volume.sum(), 1.0, rtol=0, atol=1e-12)
+    assert (m.volume > 0).all()
+    # Every cell's outward area vectors close (the discrete divergence of a constant vanishes).
+    S = np.zeros((N, D))
+    np.add.at(S, m.owner, m.area)
+    np.add.at(S, m.neighbour, -m.area)
+    assert np.abs(S).max() < 1e-14
+    # Lists: each face appears once owned (f) in its owner's list and once as ~f in its neighbour's.
+    assert m.cell_face_start[0] == 0 and m.cell_face_start[-1] == 2 * F
+    for i in range(0, N, max(1, N // 97)):
+        entries = m.cell_face[m.cell_face_start[i]:m.cell_face_start[i + 1]]
+        for e in entries:
+            f = e if e >= 0 else ~e
+            if e >= 0:
+                assert m.owner[f] == i
+            else:
+                assert m.neighbour[f] == i
+    assert (m.owner < m.neighbour).all()
+    assert m.inconsistent == 0
+
+
+def test_face_count_matches_reference_ratio():
+    """F/N = 7.95 on a jittered (0.1) 3D lattice, as the reference measures (README.md:301)."""
+    m = jittered_mesh(32)
+    assert abs(m.n_faces / m.n_cells - 7.95) < 0.05
+
+
+def test_jittered_points_law():
+    p = jittered_points((4, 4, 4), jitter=0.1, seed=1)
+    h = 0.25
+    lattice = (np.stack(np.meshgrid(np.arange(4), np.arange(4), np.arange(4), indexing="ij"), -1).reshape(-1, 3) + 0.5) * h
+    d = (p - lattice + 0.5) % 1.0 - 0.5
+    assert np.abs(d).max() <= 0.1 * h + 1e-15
+    assert np.array_equal(p, jittered_points((4, 4, 4), jitter=0.1, seed=1))
+
+
+def test_too_small_box_is_an_error():
+    with pytest.raises(ValueError):
+        build_mesh(np.array([[0.5, 0.5, 0.5], [0.1, 0.1, 0.1]]))
