@@ -39,6 +39,8 @@ def parse():
     ap.add_argument("--impl", default="luna", choices=["luna", "reference"])
     ap.add_argument("--cpu-sample-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "fp32"],
+                    help="which policies to time (the JSON line needs both; one is for profiling runs)")
     return ap.parse_args()
 
 
@@ -241,7 +243,7 @@ def main():
         return float(t.item())
 
     results = {}
-    for prec in ("fp32", "fp64"):
+    for prec in ("fp32", "fp64") if args.precision == "both" else (args.precision,):
         fv = hydro.FiniteVolume(mesh, precision=prec)
         fv.set_stream(stream)
         fv.set_state(q0)
@@ -259,6 +261,16 @@ def main():
         ms = max_over_ranks(ms)
         results[prec] = {"ms": ms, "phases": phases, "clocks": clocks.summary(), "fallbacks": fv.fallbacks(), "fv": fv}
 
+    if args.precision != "both":
+        for r in results.values():
+            r["fv"].close()
+        if rank == 0:
+            r = next(iter(results.values()))
+            print(json.dumps({"profiling_run": args.precision, "ms_per_step": r["ms"] / args.steps,
+                              "phases_ms_per_step": {k: v[0] / args.steps for k, v in r["phases"].items()}}), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     # End to end through the public API with host buffers: each step copies Q in from pinned host memory, steps, and
     # copies Q back out.
     fv = results["fp64"]["fv"]

@@ -42,8 +42,10 @@ enum { LUNA_HLLC = 0, LUNA_HLL = 1 };                                   /* Riema
 /* Precision policies (precision.hpp:26-54): LUNA_FP64 is Precision<> (double throughout); LUNA_FP32 is the reference's
  * `riemann32` preset Precision<double, float, double, float> (hydro_sedov.cpp:422): gradients, limiter, face-state change
  * and the Riemann solve in float in the face's frame; geometry, primitives (pressure recovery), flux rows and the
- * per-cell accumulation in double. */
-enum { LUNA_FP64 = 0, LUNA_FP32 = 1 };
+ * per-cell accumulation in double. LUNA_GRAD32 is the reference's Grad32 (precision.hpp:43): float gradients, limiter and
+ * face-state change, a double Riemann solve (it keeps perturbations far below float's resolution of the state, which
+ * a float Riemann solve cannot). The reduced policies take HLLC only, as the reference's presets. */
+enum { LUNA_FP64 = 0, LUNA_FP32 = 1, LUNA_GRAD32 = 2 };
 
 /* hydro::Gas (euler.hpp:82-101): gamma and the RAMSES floors. */
 typedef struct {
@@ -114,6 +116,13 @@ LUNA_API luna_status luna_fv_point_velocities(luna_fv* fv, double* out, int on_d
 /* The primitive rows [N][D + 4] (W, c, r) and the limited gradients [N][D + 2][D] (double) of the last sweep. */
 LUNA_API luna_status luna_fv_prims(luna_fv* fv, double* out, int on_device);
 LUNA_API luna_status luna_fv_gradients(luna_fv* fv, double* out, int on_device);
+
+/* step_adjoint(dt, qbar) (finite_volume.hpp:2201-2231): qbar [N][D + 2] holds Qbar after the step on entry and
+ * Qbar before it on return (J^T qbar at fixed dt; dt's dependence on Q is not differentiated). Q must be the state at
+ * the start of the step (the caller restores it from a checkpoint); it is left unchanged. A static mesh, order 1, the
+ * per-face loop and the FP64 policy (else LUNA_EINVAL, as the reference's logic_error, :1674-1679). No atomics: the
+ * same bits every run. */
+LUNA_API luna_status luna_fv_step_adjoint(luna_fv* fv, double dt, double* qbar, int on_device);
 
 /* Per-phase device time (hydro::Timings, finite_volume.hpp:36-39, without its fences): with timing on, CUDA events on
  * fv's stream bracket every kernel; luna_fv_timings synchronises, adds the elapsed times since the last reset and counts

@@ -15,6 +15,7 @@
 #include <utility>
 #include <vector>
 
+#include "adjoint.cuh"
 #include "kernels.cuh"
 #include "luna_b200.h"
 
@@ -93,6 +94,9 @@ struct luna_fv {
     DevArray<float> grad32;
     DevArray<int32_t> steps;
     DevArray<luna::Counters> counters;
+    // adjoint (allocated by the first luna_fv_step_adjoint)
+    DevArray<double> adj_fit, adj_face_bar, adj_wbar, adj_bbar, adj_boundbar, adj_qbar;
+    DevArray<int32_t> adj_flags, adj_bound_face;
     luna::Counters* host_counters = nullptr;  // pinned
 
     // Per-phase timing: event pairs recorded around each launch, reduced on request.
@@ -264,7 +268,7 @@ luna_status run_sweep(luna_fv* fv, double courant) {
     const unsigned long long init = 0x7fefffffffffffffull;  // DBL_MAX: the Min reducer's identity
     LUNA_CUDA(cudaMemcpyAsync(&fv->counters.ptr->dt_bits, &init, sizeof(init), cudaMemcpyHostToDevice, fv->stream));
     const bool moving = fv->motion == LUNA_MOVING, grad = fv->order == 1;
-    if (fv->precision == LUNA_FP32) {
+    if (fv->precision != LUNA_FP64) {
         if (moving) return launch_sweep<D, true, true, float>(fv, fv->grad32.ptr, courant);
         return grad ? launch_sweep<D, false, true, float>(fv, fv->grad32.ptr, courant) : launch_sweep<D, false, false, float>(fv, fv->grad32.ptr, courant);
     }
@@ -365,7 +369,7 @@ luna_status step_static(luna_fv* fv, double dt) {
     if (!fv->swept) LUNA_TRY(prepare_sweep<D>(fv, 1.0));
     fv->swept = false;
     LUNA_CUDA(cudaMemsetAsync(&fv->counters.ptr->fallbacks[0], 0, 2 * sizeof(unsigned long long), fv->stream));
-    if (fv->precision == LUNA_FP32) return run_apply<D, float>(fv, fv->grad32.ptr, dt);
+    if (fv->precision != LUNA_FP64) return run_apply<D, float>(fv, fv->grad32.ptr, dt);
     return run_apply<D, double>(fv, fv->grad64.ptr, dt);
 }
 
@@ -383,10 +387,13 @@ luna_status moving_begin(luna_fv* fv, double dt) {
     }
     LUNA_CUDA(cudaGetLastError());
     fv->pending_dt = dt;
-    if (fv->precision == LUNA_FP32) {
+    if (fv->precision != LUNA_FP64) {
         auto x = flux_args<D, float>(fv, fv->grad32.ptr, 0.0);
         x.unit = fv->grid_step / dt;
-        LUNA_TRY((launch_flux<D, 1, 0, float, true, 0>(fv, x)));
+        if (fv->precision == LUNA_FP32)
+            LUNA_TRY((launch_flux<D, 1, 0, float, true, 0>(fv, x)));
+        else
+            LUNA_TRY((launch_flux<D, 1, 0, float, false, 0>(fv, x)));
     } else {
         auto x = flux_args<D, double>(fv, fv->grad64.ptr, 0.0);
         x.unit = fv->grid_step / dt;
@@ -416,10 +423,13 @@ luna_status moving_begin(luna_fv* fv, double dt) {
 template <int D>
 luna_status moving_end(luna_fv* fv) {
     const double dt = fv->pending_dt;
-    if (fv->precision == LUNA_FP32) {
+    if (fv->precision != LUNA_FP64) {
         auto x = flux_args<D, float>(fv, fv->grad32.ptr, 2 * dt);
         x.unit = fv->grid_step / dt;
-        LUNA_TRY((launch_flux<D, 1, 1, float, true, 0>(fv, x)));
+        if (fv->precision == LUNA_FP32)
+            LUNA_TRY((launch_flux<D, 1, 1, float, true, 0>(fv, x)));
+        else
+            LUNA_TRY((launch_flux<D, 1, 1, float, false, 0>(fv, x)));
     } else {
         auto x = flux_args<D, double>(fv, fv->grad64.ptr, 2 * dt);
         x.unit = fv->grid_step / dt;
@@ -437,6 +447,59 @@ luna_status moving_end(luna_fv* fv) {
     LUNA_CUDA(cudaGetLastError());
     fv->prims_ready = true;
     fv->moving_pending = false;
+    return LUNA_OK;
+}
+
+// step_adjoint (finite_volume.hpp:2201-2231): the forward recompute (primitives, the sweep keeping its fit), then the
+// faces' Riemann adjoints, the cells' adjoints and the gather into Qbar.
+template <int D>
+luna_status run_adjoint(luna_fv* fv, double dt, double* qbar) {
+    constexpr int V = D + 2, U = D + 1;
+    using FL = luna::FitLayout<D>;
+    const size_t N = static_cast<size_t>(fv->n), F = static_cast<size_t>(fv->f);
+    LUNA_TRY(fv->adj_fit.alloc(N * FL::width, "adjoint fit rows"));
+    LUNA_TRY(fv->adj_flags.alloc(N * 2 * V, "adjoint flags"));
+    LUNA_TRY(fv->adj_face_bar.alloc(F > 0 ? F * 2 * V : 1, "adjoint face bars"));
+    LUNA_TRY(fv->adj_wbar.alloc(N * V, "adjoint W bars"));
+    LUNA_TRY(fv->adj_bbar.alloc(N * V * U, "adjoint b bars"));
+    LUNA_TRY(fv->adj_boundbar.alloc(N * V, "adjoint bound bars"));
+    LUNA_TRY(fv->adj_bound_face.alloc(N * V, "adjoint bound faces"));
+    const auto m = fv->mesh_dev<D>();
+    LUNA_TRY(run_primitives<D>(fv));
+    {
+        const long timed_ = fv->open_timed(1);
+        if (fv->limiter == LUNA_LIMITER_NONE)
+            luna::k_sweep_fit<D, false><<<blocks(N, kBlockCells), kBlockCells, 0, fv->stream>>>(m, fv->prims.ptr, fv->grad64.ptr, fv->adj_fit.ptr,
+                                                                                              fv->adj_flags.ptr);
+        else
+            luna::k_sweep_fit<D, true><<<blocks(N, kBlockCells), kBlockCells, 0, fv->stream>>>(m, fv->prims.ptr, fv->grad64.ptr, fv->adj_fit.ptr,
+                                                                                             fv->adj_flags.ptr);
+        fv->close_timed(timed_);
+    }
+    LUNA_CUDA(cudaGetLastError());
+    if (F > 0) {
+        const long timed_ = fv->open_timed(2);
+        if (fv->riemann == LUNA_HLL)
+            luna::k_faces_adjoint<D, 1><<<blocks(F, kBlockFaces), kBlockFaces, 0, fv->stream>>>(m, fv->prims.ptr, fv->grad64.ptr, qbar, dt, fv->gas,
+                                                                                              fv->adj_face_bar.ptr);
+        else
+            luna::k_faces_adjoint<D, 0><<<blocks(F, kBlockFaces), kBlockFaces, 0, fv->stream>>>(m, fv->prims.ptr, fv->grad64.ptr, qbar, dt, fv->gas,
+                                                                                              fv->adj_face_bar.ptr);
+        fv->close_timed(timed_);
+        LUNA_CUDA(cudaGetLastError());
+    }
+    {
+        const long timed_ = fv->open_timed(3);
+        luna::k_cell_adjoint<D><<<blocks(N, kBlockCells), kBlockCells, 0, fv->stream>>>(m, fv->prims.ptr, fv->grad64.ptr, fv->adj_face_bar.ptr,
+                                                                                        fv->adj_fit.ptr, fv->adj_flags.ptr, dt, fv->gas, fv->adj_wbar.ptr,
+                                                                                        fv->adj_bbar.ptr, fv->adj_boundbar.ptr, fv->adj_bound_face.ptr);
+        luna::k_gather_adjoint<D><<<blocks(N, kBlockCells), kBlockCells, 0, fv->stream>>>(m, fv->q.ptr, fv->adj_wbar.ptr, fv->adj_bbar.ptr,
+                                                                                          fv->adj_boundbar.ptr, fv->adj_bound_face.ptr, fv->gas, qbar);
+        fv->close_timed(timed_);
+    }
+    LUNA_CUDA(cudaGetLastError());
+    fv->prims_ready = true;  // Q is unchanged
+    fv->swept = false;
     return LUNA_OK;
 }
 
@@ -476,8 +539,8 @@ LUNA_API luna_status luna_fv_create(const luna_mesh_desc* mesh, const luna_gas* 
     if (limiter != LUNA_LIMITER_FACE_CENTROID && limiter != LUNA_LIMITER_NONE) return set_error(LUNA_EINVAL, "limiter: face_centroid or none");
     if (motion != LUNA_STATIC_MESH && motion != LUNA_MOVING) return set_error(LUNA_EINVAL, "motion: static_mesh or moving");
     if (riemann != LUNA_HLLC && riemann != LUNA_HLL) return set_error(LUNA_EINVAL, "riemann: HLLC or HLL");
-    if (precision != LUNA_FP64 && precision != LUNA_FP32) return set_error(LUNA_EINVAL, "precision: FP64 or FP32");
-    if (precision == LUNA_FP32 && riemann == LUNA_HLL)
+    if (precision != LUNA_FP64 && precision != LUNA_FP32 && precision != LUNA_GRAD32) return set_error(LUNA_EINVAL, "precision: FP64, FP32 or GRAD32");
+    if (precision != LUNA_FP64 && riemann == LUNA_HLL)
         return set_error(LUNA_EINVAL, "the FP32 policy takes HLLC (the reference's reduced presets are HLLC only)");
     if (motion == LUNA_MOVING && (order != 1 || update != LUNA_UPDATE_PER_FACE))
         return set_error(LUNA_EINVAL, "a moving mesh runs order 1 with the per-face update");
@@ -517,7 +580,7 @@ LUNA_API luna_status luna_fv_create(const luna_mesh_desc* mesh, const luna_gas* 
     if ((s = fv->prims.alloc(N * luna::PS, "primitive rows")) != LUNA_OK) return fail(s);
     const size_t GS = D == 3 ? luna::grad_stride<3>() : luna::grad_stride<2>();
     if (order == 1) {
-        if (precision == LUNA_FP32) {
+        if (precision != LUNA_FP64) {
             if ((s = fv->grad32.alloc(N * GS, "gradient rows")) != LUNA_OK) return fail(s);
         } else if ((s = fv->grad64.alloc(N * GS, "gradient rows")) != LUNA_OK) {
             return fail(s);
@@ -691,6 +754,23 @@ LUNA_API luna_status luna_fv_gradients(luna_fv* fv, double* out, int on_device) 
     return LUNA_OK;
 }
 
+LUNA_API luna_status luna_fv_step_adjoint(luna_fv* fv, double dt, double* qbar, int on_device) {
+    if (!fv || !qbar) return set_error(LUNA_EINVAL, "null argument");
+    if (fv->motion != LUNA_STATIC_MESH || fv->order != 1 || fv->update != LUNA_UPDATE_PER_FACE || fv->precision != LUNA_FP64)
+        return set_error(LUNA_EINVAL, "hydro::FiniteVolume::step_adjoint: a static mesh, order 1, the per-face loop, the FP64 policy");
+    if (fv->moving_pending) return set_error(LUNA_ESTATE, "inside a moving step");
+    const size_t count = static_cast<size_t>(fv->n) * (fv->dim + 2);
+    double* dev = qbar;
+    if (!on_device) {
+        LUNA_TRY(fv->adj_qbar.alloc(count, "adjoint Q bar"));
+        LUNA_CUDA(cudaMemcpyAsync(fv->adj_qbar.ptr, qbar, count * sizeof(double), cudaMemcpyHostToDevice, fv->stream));
+        dev = fv->adj_qbar.ptr;
+    }
+    LUNA_TRY(fv->dim == 3 ? run_adjoint<3>(fv, dt, dev) : run_adjoint<2>(fv, dt, dev));
+    if (!on_device) LUNA_TRY(copy_out(dev, qbar, count, 0, fv->stream));
+    return LUNA_OK;
+}
+
 LUNA_API luna_status luna_fv_set_timing(luna_fv* fv, int on) {
     if (!fv) return set_error(LUNA_EINVAL, "fv is null");
     fv->timing = on != 0;
@@ -725,6 +805,8 @@ LUNA_API luna_status luna_fv_device_bytes(luna_fv* fv, int64_t* out) {
     b += fv->area.bytes() + fv->mag.bytes() + fv->fcen.bytes() + fv->cen.bytes() + fv->vol.bytes() + fv->pos.bytes();
     b += fv->q.bytes() + fv->next.bytes() + fv->prims.bytes() + fv->grad64.bytes() + fv->grad32.bytes() + fv->flux.bytes();
     b += fv->w.bytes() + fv->x.bytes() + fv->old_cen.bytes() + fv->steps.bytes() + fv->counters.bytes();
+    b += fv->adj_fit.bytes() + fv->adj_face_bar.bytes() + fv->adj_wbar.bytes() + fv->adj_bbar.bytes() + fv->adj_boundbar.bytes();
+    b += fv->adj_qbar.bytes() + fv->adj_flags.bytes() + fv->adj_bound_face.bytes();
     *out = static_cast<int64_t>(b);
     return LUNA_OK;
 }

@@ -23,7 +23,7 @@ UPDATE = {"per_cell": 0, "per_face": 1}
 LIMITER = {"face_centroid": 0, "none": 1}
 MOTION = {"static_mesh": 0, "static": 0, "moving": 1}
 RIEMANN = {"hllc": 0, "hll": 1}
-PRECISION = {"fp64": 0, "double": 0, "fp32": 1, "riemann32": 1}
+PRECISION = {"fp64": 0, "double": 0, "fp32": 1, "riemann32": 1, "grad32": 2}
 
 
 class LunaError(RuntimeError):
@@ -79,6 +79,7 @@ SIGNATURES = {
     "luna_last_error": ([], ctypes.c_char_p),
     "luna_fv_device_bytes": ([P, P], I),
     "luna_fv_set_timing": ([P, I], I),
+    "luna_fv_step_adjoint": ([P, D64, P, I], I),
     "luna_fv_timings": ([P, P, I], I),
 }
 
@@ -245,6 +246,16 @@ class FiniteVolume:
     def positions(self) -> np.ndarray:
         a = np.empty((self.n, self.dim), dtype=np.float64)
         check(lib().luna_fv_positions(self._h, a.ctypes.data, 0))
+        return a
+
+    def step_adjoint(self, dt: float, qbar):
+        """J^T qbar of one step at fixed dt from the current state (which must be the step's start); numpy in, numpy out,
+        or a CUDA float64 tensor updated in place."""
+        if hasattr(qbar, "is_cuda") and qbar.is_cuda:
+            check(lib().luna_fv_step_adjoint(self._h, dt, ctypes.c_void_p(qbar.data_ptr()), 1))
+            return qbar
+        a = np.ascontiguousarray(qbar, dtype=np.float64).copy()
+        check(lib().luna_fv_step_adjoint(self._h, dt, a.ctypes.data, 0))
         return a
 
     def set_stream(self, stream_ptr: int) -> None:

@@ -993,3 +993,584 @@ void lo_fv_step_moving_end(lo_fv* fv, const lo_mesh* new_mesh) {
     apply(fv, 0.0, 0.5 * fv->pending_dt, 1);
     fv->prims_ready = fv->per_face; /* the per-face update wrote the next primitives (finite_volume.hpp:1628) */
 }
+
+/* ---------------------------------------------------------------------------------------------------------------------
+ * The adjoint of one static step (step_adjoint, finite_volume.hpp:2201-2231), double policy, order 1, per-face loop.
+ * ------------------------------------------------------------------------------------------------------------------- */
+
+/* primitive_adjoint (euler.hpp:143-162): Ubar = J^T Wbar, a floored density or energy takes its floor's derivative. */
+static void primitive_adjoint(int D, const double* U, const double* Wbar, const lo_gas* gas, double* Ubar) {
+    const int P = D + 1;
+    const double rho = fmax(U[0], gas->smallr), inv_rho = 1.0 / rho;
+    double v[3];
+    for (int k = 0; k < D; ++k) v[k] = U[1 + k] * inv_rho;
+    const double smalle = gas->smallc * gas->smallc / gas->gamma / (gas->gamma - 1.0);
+    /* primitive_branches (euler.hpp:121-127) */
+    double vb[3];
+    for (int k = 0; k < D; ++k) vb[k] = U[1 + k] * (1.0 / rho);
+    const int floors = (U[0] >= gas->smallr ? 0 : 1) | (U[P] - 0.5 * rho * dotd(D, vb, vb) >= smalle * rho ? 0 : 2);
+    const double ebar = (gas->gamma - 1.0) * Wbar[P];
+    double rhobar = Wbar[0], energybar = 0;
+    double vbar[3];
+    for (int k = 0; k < D; ++k) vbar[k] = Wbar[1 + k];
+    if (floors & 2) {
+        rhobar += smalle * ebar;
+    } else {
+        energybar = ebar;
+        rhobar -= 0.5 * dotd(D, v, v) * ebar;
+        const double s = rho * ebar;
+        for (int k = 0; k < D; ++k) vbar[k] = vbar[k] - v[k] * s;
+    }
+    double mbar[3];
+    for (int k = 0; k < D; ++k) mbar[k] = vbar[k] * inv_rho;
+    rhobar -= dotd(D, v, vbar) * inv_rho;
+    Ubar[0] = floors & 1 ? 0.0 : rhobar;
+    for (int k = 0; k < D; ++k) Ubar[1 + k] = mbar[k];
+    Ubar[P] = energybar;
+}
+
+/* half_step_adjoint (euler.hpp:241-272): adds J^T halfbar to Wbar and gbar. */
+static void half_step_adjoint(int D, const double* W, const double* g, double dt, const lo_gas* gas, const double* halfbar, double* Wbar,
+                              double* gbar) {
+    const int P = D + 1;
+    const double rho = W[0], inv_rho = 1.0 / W[0], rho_c2 = gas->gamma * W[P];
+    double Abar[VMAX];
+    for (int v = 0; v < D + 2; ++v) {
+        Wbar[v] += halfbar[v];
+        Abar[v] = -0.5 * dt * halfbar[v];
+    }
+    double inv_rhobar = 0, rho_c2bar = 0;
+    for (int d = 0; d < D; ++d) {
+        const double vn = W[1 + d];
+        Wbar[1 + d] += Abar[0] * g[0 * D + d];
+        gbar[0 * D + d] += Abar[0] * vn;
+        Wbar[0] += Abar[0] * g[(1 + d) * D + d];
+        gbar[(1 + d) * D + d] += Abar[0] * rho;
+        for (int k = 0; k < D; ++k) {
+            Wbar[1 + d] += Abar[1 + k] * g[(1 + k) * D + d];
+            gbar[(1 + k) * D + d] += Abar[1 + k] * vn;
+            if (k == d) {
+                inv_rhobar += Abar[1 + k] * g[P * D + d];
+                gbar[P * D + d] += Abar[1 + k] * inv_rho;
+            }
+        }
+        rho_c2bar += Abar[P] * g[(1 + d) * D + d];
+        gbar[(1 + d) * D + d] += Abar[P] * rho_c2;
+        Wbar[1 + d] += Abar[P] * g[P * D + d];
+        gbar[P * D + d] += Abar[P] * vn;
+    }
+    Wbar[0] -= inv_rho * inv_rho * inv_rhobar;
+    Wbar[P] += gas->gamma * rho_c2bar;
+}
+
+/* detail::side_with_adjoint (euler.hpp:375-398): adds J^T to Wbar; returns vn's bar. vbar_in is taken by value. */
+static double side_with_adjoint(int D, const double* W, const double* n, const lo_gas* gas, const side_d* s, const double* Fbar,
+                                const double* Ubar, double Ebar, const double* vbar_in, double* Wbar) {
+    const int P = D + 1;
+    const double m = W[0] * s->vn;
+    double vbar[3];
+    for (int k = 0; k < D; ++k) vbar[k] = vbar_in ? vbar_in[k] : 0.0;
+    Ebar += Fbar[P] * s->vn + Ubar[P];
+    double Pbar = Fbar[P] * s->vn, vnbar = Fbar[P] * (s->E + W[P]), mbar = Fbar[0], rhobar = Ubar[0];
+    for (int k = 0; k < D; ++k) {
+        Pbar += Fbar[1 + k] * n[k];
+        mbar += Fbar[1 + k] * s->v[k];
+        vbar[k] += Fbar[1 + k] * m + Ubar[1 + k] * W[0];
+        rhobar += Ubar[1 + k] * s->v[k];
+    }
+    rhobar += mbar * s->vn;
+    vnbar += mbar * W[0];
+    Pbar += Ebar * gas->inverse_gm1;
+    rhobar += Ebar * (0.5 * dotd(D, s->v, s->v));
+    const double e = Ebar * W[0];
+    for (int k = 0; k < D; ++k) vbar[k] = vbar[k] + s->v[k] * e;
+    Wbar[0] += rhobar;
+    for (int k = 0; k < D; ++k) Wbar[1 + k] += vbar[k];
+    Wbar[P] += Pbar;
+    return vnbar;
+}
+
+/* detail::side_adjoint (euler.hpp:402-413). */
+static void side_adjoint_full(int D, const double* W, const double* n, const lo_gas* gas, const side_d* s, const double* Fbar,
+                              const double* Ubar, double vnbar, double cbar, double* Wbar) {
+    const int P = D + 1;
+    vnbar += side_with_adjoint(D, W, n, gas, s, Fbar, Ubar, 0.0, NULL, Wbar);
+    for (int k = 0; k < D; ++k) Wbar[1 + k] += vnbar * n[k];
+    const double c2 = gas->gamma * W[P] / W[0];
+    if (c2 > 0) {
+        const double c2bar = cbar / (2 * s->c);
+        Wbar[P] += c2bar * gas->gamma / W[0];
+        Wbar[0] -= c2bar * c2 / W[0];
+    }
+}
+
+/* detail::to_lab_adjoint (euler.hpp:416-426). */
+static void to_lab_adjoint(int D, const double* Fbar, const double* w, double* G) {
+    const int P = D + 1;
+    for (int v = 0; v < D + 2; ++v) G[v] = Fbar[v];
+    G[0] += 0.5 * dotd(D, w, w) * Fbar[P];
+    for (int k = 0; k < D; ++k) {
+        G[0] += w[k] * Fbar[1 + k];
+        G[1 + k] += w[k] * Fbar[P];
+    }
+}
+
+/* HLL::flux_adjoint (euler.hpp:509-540) with HLL::branches (:468-477). */
+static void hll_flux_adjoint(int D, const double* L, const double* R, const double* n, const double* w, const lo_gas* gas,
+                             const double* Fbar_lab, double* Lbar, double* Rbar) {
+    const int P = D + 1;
+    const side_d l = side_full_d(D, L, n, w, gas), r = side_full_d(D, R, n, w, gas);
+    const double a = l.vn - l.c, b = r.vn - r.c, A = l.vn + l.c, B = r.vn + r.c;
+    const double SLm = fmin(a, b), SRm = fmax(A, B);
+    const int wave = SLm >= 0 ? 1 : SRm <= 0 ? 2 : 0;
+    const int pattern = (b < a ? 0 : 1) | (B > A ? 0 : 2);
+    (void)P;
+    const double SL = pattern & 1 ? l.vn - l.c : r.vn - r.c, SR = pattern & 2 ? l.vn + l.c : r.vn + r.c;
+    double Fbar[VMAX];
+    to_lab_adjoint(D, Fbar_lab, w, Fbar);
+    double lF[VMAX] = {0}, rF[VMAX] = {0}, lU[VMAX] = {0}, rU[VMAX] = {0};
+    double SLbar = 0, SRbar = 0;
+    if (wave == 1) {
+        for (int v = 0; v < D + 2; ++v) lF[v] = Fbar[v];
+    } else if (wave == 2) {
+        for (int v = 0; v < D + 2; ++v) rF[v] = Fbar[v];
+    } else {
+        const double inv_dS = 1.0 / (SR - SL);
+        for (int v = 0; v < D + 2; ++v) {
+            const double dU = r.U[v] - l.U[v], F = (SR * l.F[v] - SL * r.F[v] + SL * SR * dU) * inv_dS;
+            const double N = Fbar[v] * inv_dS;
+            SRbar += -Fbar[v] * F * inv_dS + N * (l.F[v] + SL * dU);
+            SLbar += Fbar[v] * F * inv_dS + N * (-r.F[v] + SR * dU);
+            lF[v] = SR * N;
+            rF[v] = -SL * N;
+            rU[v] = SL * SR * N;
+            lU[v] = -SL * SR * N;
+        }
+    }
+    double lvn = 0, lc = 0, rvn = 0, rc = 0;
+    if (pattern & 1) {
+        lvn += SLbar;
+        lc -= SLbar;
+    } else {
+        rvn += SLbar;
+        rc -= SLbar;
+    }
+    if (pattern & 2) {
+        lvn += SRbar;
+        lc += SRbar;
+    } else {
+        rvn += SRbar;
+        rc += SRbar;
+    }
+    side_adjoint_full(D, L, n, gas, &l, lF, lU, lvn, lc, Lbar);
+    side_adjoint_full(D, R, n, gas, &r, rF, rU, rvn, rc, Rbar);
+}
+
+/* HLLC::flux_adjoint (euler.hpp:738-832) with HLLC::waves (:651-680): only the case the forward took. */
+static void hllc_flux_adjoint(int D, const double* L, const double* R, const double* n, const double* w, const lo_gas* gas,
+                              const double* Fbar_lab, double* Lbar, double* Rbar) {
+    const int P = D + 1;
+    const double eps = 1e-20;
+    double rl[3], rr[3];
+    for (int k = 0; k < D; ++k) {
+        rl[k] = L[1 + k] - w[k];
+        rr[k] = R[1 + k] - w[k];
+    }
+    const double vnL = dotd(D, rl, n), vnR = dotd(D, rr, n);
+    const double inv_rhoL = 1.0 / L[0], inv_rhoR = 1.0 / R[0];
+    const double c2L = gas->gamma * L[P] * inv_rhoL, c2R = gas->gamma * R[P] * inv_rhoR;
+    const int ok = c2L >= 0 && c2R >= 0;
+    const double cL = c2L > 0 ? sqrt(c2L) : 0.0, cR = c2R > 0 ? sqrt(c2R) : 0.0;
+    const double sl = vnL - cL, sr = vnR - cR, tl = vnL + cL, tr = vnR + cR;
+    const double SL = fmin(sl, sr), SR = fmax(tl, tr);
+    const double denomL = L[0] * (SL - vnL), denomR = R[0] * (SR - vnR);
+    const double den_raw = denomL - denomR;
+    const double SM = (R[P] - L[P] + denomL * vnL - denomR * vnR) / nonzero_d(den_raw);
+    const int left = ok && (SL >= 0 || SM >= 0);
+    const int star = ok && SL < 0 && (SM >= 0 || SR > 0);
+    const double Sx = left ? SL : SR, denomx = left ? denomL : denomR;
+    const int pattern = (sr < sl ? 0 : 1) | (tr > tl ? 0 : 2) | (fabs(den_raw) < eps) << 7 | (star && fabs(Sx - SM) < eps) << 8 |
+                        (star && fabs(denomx) < eps) << 9;
+    double Fbar[VMAX];
+    to_lab_adjoint(D, Fbar_lab, w, Fbar);
+    double W[VMAX];
+    for (int v = 0; v < D + 2; ++v) W[v] = left ? L[v] : R[v];
+    const double vn = left ? vnL : vnR;
+    const side_d s = side_with_d(D, W, n, w, gas, vn);
+    double Wbar[VMAX] = {0, 0, 0, 0, 0};
+    double vnLbar = 0, vnRbar = 0;
+    if (!star) {
+        const double zero[VMAX] = {0, 0, 0, 0, 0};
+        const double r = side_with_adjoint(D, W, n, gas, &s, Fbar, zero, 0.0, NULL, Wbar);
+        if (left)
+            vnLbar += r;
+        else
+            vnRbar += r;
+    } else {
+        const double S = left ? SL : SR, denom = left ? denomL : denomR, inv_side = left ? inv_rhoL : inv_rhoR;
+        const double q = nonzero_d(S - SM), rho_star = denom / q, inv_denom = 1.0 / nonzero_d(denom);
+        const double a2 = SM - s.vn, a3 = SM + W[P] * inv_denom, E_star = s.E * inv_side + a2 * a3;
+        double v_star[3];
+        for (int k = 0; k < D; ++k) v_star[k] = s.v[k] + n[k] * a2;
+        double Sbar = 0, rho_starbar = 0, E_starbar = 0;
+        double sUbar[VMAX], v_starbar[3] = {0, 0, 0};
+        for (int v = 0; v < D + 2; ++v) {
+            const double U_star = v == 0 ? rho_star : v == P ? rho_star * E_star : rho_star * v_star[v - 1];
+            Sbar += Fbar[v] * (U_star - s.U[v]);
+            sUbar[v] = -S * Fbar[v];
+            const double U_starbar = S * Fbar[v];
+            if (v == 0) {
+                rho_starbar += U_starbar;
+            } else if (v == P) {
+                rho_starbar += U_starbar * E_star;
+                E_starbar = U_starbar * rho_star;
+            } else {
+                rho_starbar += U_starbar * v_star[v - 1];
+                v_starbar[v - 1] = U_starbar * rho_star;
+            }
+        }
+        const double a2bar = dotd(D, v_starbar, n) + E_starbar * a3, a3bar = E_starbar * a2;
+        double SMbar = a3bar + a2bar, vnbar = -a2bar;
+        const double inv_denombar = a3bar * W[P];
+        const double denombar = (pattern & 512 ? 0.0 : -inv_denom * inv_denom * inv_denombar) + rho_starbar / q;
+        const double qbar = pattern & 256 ? 0.0 : -rho_starbar * rho_star / q;
+        Sbar += qbar;
+        SMbar -= qbar;
+        const double sEbar = E_starbar * inv_side, inv_sidebar = E_starbar * s.E;
+        vnbar += side_with_adjoint(D, W, n, gas, &s, Fbar, sUbar, sEbar, v_starbar, Wbar);
+        Wbar[P] += a3bar * inv_denom;
+        const double den = nonzero_d(den_raw), numbar = SMbar / den, denbar = pattern & 128 ? 0.0 : -SMbar * SM / den;
+        double denomLbar = denbar + numbar * vnL, denomRbar = -denbar - numbar * vnR;
+        if (left)
+            denomLbar += denombar;
+        else
+            denomRbar += denombar;
+        vnLbar += numbar * denomL;
+        vnRbar -= numbar * denomR;
+        Rbar[P] += numbar;
+        Lbar[P] -= numbar;
+        if (left)
+            vnLbar += vnbar;
+        else
+            vnRbar += vnbar;
+        double invLbar = 0, invRbar = 0;
+        if (left)
+            invLbar += inv_sidebar;
+        else
+            invRbar += inv_sidebar;
+        double SLbar = denomLbar * L[0], SRbar = denomRbar * R[0];
+        if (left)
+            SLbar += Sbar;
+        else
+            SRbar += Sbar;
+        Lbar[0] += denomLbar * (SL - vnL);
+        vnLbar -= denomLbar * L[0];
+        Rbar[0] += denomRbar * (SR - vnR);
+        vnRbar -= denomRbar * R[0];
+        double cLbar = 0, cRbar = 0;
+        if (pattern & 1) {
+            vnLbar += SLbar;
+            cLbar -= SLbar;
+        } else {
+            vnRbar += SLbar;
+            cRbar -= SLbar;
+        }
+        if (pattern & 2) {
+            vnLbar += SRbar;
+            cLbar += SRbar;
+        } else {
+            vnRbar += SRbar;
+            cRbar += SRbar;
+        }
+        if (c2L > 0) {
+            const double c2bar = cLbar / (2 * cL);
+            Lbar[P] += c2bar * gas->gamma * inv_rhoL;
+            invLbar += c2bar * gas->gamma * L[P];
+        }
+        if (c2R > 0) {
+            const double c2bar = cRbar / (2 * cR);
+            Rbar[P] += c2bar * gas->gamma * inv_rhoR;
+            invRbar += c2bar * gas->gamma * R[P];
+        }
+        Lbar[0] -= inv_rhoL * inv_rhoL * invLbar;
+        Rbar[0] -= inv_rhoR * inv_rhoR * invRbar;
+    }
+    for (int v = 0; v < D + 2; ++v) {
+        Lbar[v] += left ? Wbar[v] : 0.0;
+        Rbar[v] += left ? 0.0 : Wbar[v];
+    }
+    for (int k = 0; k < D; ++k) {
+        Lbar[1 + k] += vnLbar * n[k];
+        Rbar[1 + k] += vnRbar * n[k];
+    }
+}
+
+/* The fit the sweep leaves for the adjoint (SweepFitHook<false>, finite_volume.hpp:1763-1926): M's Cholesky factor, M's
+ * row 0, the unlimited gradient g0, per variable the last clip (offset, bound, flags) and the face its bound came through. */
+typedef struct {
+    double Lc[UMAX][UMAX], M0[UMAX], g0[VMAX * 3], offset[VMAX * 3], bound[VMAX];
+    int clipped[VMAX], upper[VMAX], zero[VMAX], bound_face[VMAX];
+} fit_t;
+
+static void sweep_fit_cell(const lo_fv* fv, int64_t i, fit_t* fit) {
+    const int D = fv->D, V = fv->V, U = fv->U;
+    const double* Wi = fv->prims + (V + 2) * i;
+    double surface = 0, smallest = INFINITY;
+    double lo[VMAX], hi[VMAX];
+    int lo_f[VMAX], hi_f[VMAX];
+    for (int v = 0; v < V; ++v) {
+        lo[v] = DBL_MAX;
+        hi[v] = -DBL_MAX;
+        lo_f[v] = hi_f[v] = -1;
+    }
+    double M[UMAX][UMAX], b[VMAX][UMAX];
+    memset(M, 0, sizeof(M));
+    memset(b, 0, sizeof(b));
+    const double* centroid = fv->mesh.centroid + D * i;
+    const int32_t first = fv->mesh.start[i], end = fv->mesh.start[i + 1];
+    for (int32_t k = first; k < end; ++k) {
+        const int32_t e = fv->mesh.list[k];
+        const int f = list_face(e);
+        const int64_t j = e >= 0 ? fv->mesh.neighbour[f] : fv->mesh.owner[f];
+        const double* Wj = fv->prims + (V + 2) * j;
+        double d[3];
+        separation(fv, i, j, d);
+        const double magnitude = fv->mag[f];
+        surface += magnitude;
+        smallest = fmin(smallest, magnitude);
+        double X[UMAX];
+        X[0] = 1;
+        for (int p = 1; p < U; ++p) X[p] = d[p - 1] + fv->mesh.centroid[D * j + p - 1] - centroid[p - 1];
+        const double w = magnitude;
+        for (int p = 0; p < U; ++p)
+            for (int s = p; s < U; ++s) M[p][s] += w * X[p] * X[s];
+        for (int v = 0; v < V; ++v) {
+            const double dW = Wj[v] - Wi[v];
+            for (int p = 0; p < U; ++p) b[v][p] += w * X[p] * dW;
+            if (Wj[v] < lo[v]) lo[v] = Wj[v], lo_f[v] = f;
+            if (Wj[v] > hi[v]) hi[v] = Wj[v], hi_f[v] = f;
+        }
+    }
+    const double tiny = 1e-6 * surface;
+    const int any_tiny = smallest < tiny;
+    if (any_tiny) {
+        for (int v = 0; v < V; ++v) {
+            lo[v] = DBL_MAX;
+            hi[v] = -DBL_MAX;
+        }
+        for (int32_t k = first; k < end; ++k) {
+            const int32_t e = fv->mesh.list[k];
+            const int f = list_face(e);
+            const int64_t j = e >= 0 ? fv->mesh.neighbour[f] : fv->mesh.owner[f];
+            if (fv->mag[f] < tiny) continue;
+            const double* Wj = fv->prims + (V + 2) * j;
+            for (int v = 0; v < V; ++v) {
+                if (Wj[v] < lo[v]) lo[v] = Wj[v], lo_f[v] = f;
+                if (Wj[v] > hi[v]) hi[v] = Wj[v], hi_f[v] = f;
+            }
+        }
+    }
+    /* cholesky (finite_volume.hpp:677-687) */
+    memset(fit, 0, sizeof(*fit));
+    for (int p = 0; p < U; ++p)
+        for (int s = 0; s <= p; ++s) {
+            double sum = M[s][p];
+            for (int m = 0; m < s; ++m) sum -= fit->Lc[p][m] * fit->Lc[s][m];
+            fit->Lc[p][s] = p == s ? sqrt(sum) : sum / fit->Lc[s][s];
+        }
+    for (int p = 0; p < U; ++p) fit->M0[p] = M[0][p];
+    double grad[VMAX * 3];
+    solve_d(U, V, D, M, b, grad);
+    memcpy(fit->g0, grad, sizeof(double) * V * D);
+    int clip_f[VMAX];
+    for (int v = 0; v < V; ++v) {
+        fit->clipped[v] = fit->upper[v] = fit->zero[v] = 0;
+        clip_f[v] = -1;
+    }
+    if (!fv->limiter_none)
+        for (int32_t k = first; k < end; ++k) {
+            const int f = list_face(fv->mesh.list[k]);
+            if (any_tiny && fv->mag[f] < tiny) continue;
+            double offset[3];
+            face_offset(fv, f, i, offset);
+            for (int v = 0; v < V; ++v) {
+                double* g = grad + D * v;
+                const double dp = dotd(D, g, offset);
+                if (dp > 0 && Wi[v] + dp > hi[v]) {
+                    const double s = hi[v] > Wi[v] ? (hi[v] - Wi[v]) / dp : 0.0;
+                    for (int a = 0; a < D; ++a) g[a] = g[a] * s;
+                    fit->clipped[v] = 1, fit->upper[v] = 1, fit->zero[v] = !(hi[v] > Wi[v]), clip_f[v] = f;
+                } else if (dp < 0 && Wi[v] + dp < lo[v]) {
+                    const double s = lo[v] < Wi[v] ? (lo[v] - Wi[v]) / dp : 0.0;
+                    for (int a = 0; a < D; ++a) g[a] = g[a] * s;
+                    fit->clipped[v] = 1, fit->upper[v] = 0, fit->zero[v] = !(lo[v] < Wi[v]), clip_f[v] = f;
+                }
+            }
+        }
+    for (int v = 0; v < V; ++v) {
+        double offset[3] = {0, 0, 0};
+        if (fit->clipped[v]) face_offset(fv, clip_f[v], i, offset);
+        for (int a = 0; a < D; ++a) fit->offset[D * v + a] = offset[a];
+        fit->bound[v] = fit->upper[v] ? hi[v] : lo[v];
+        fit->bound_face[v] = fit->upper[v] ? hi_f[v] : lo_f[v];
+    }
+    memcpy(fv->grad + V * D * i, grad, sizeof(double) * V * D);
+}
+
+/* FaceFlux::side_value (finite_volume.hpp:1342-1347): the order-1 face state in double and whether it fell back. */
+static int side_value(const lo_fv* fv, int64_t i, const double* r, double dt, double* Wf) {
+    const int D = fv->D, V = fv->V;
+    const double* W = fv->prims + (V + 2) * i;
+    const double* g = fv->grad + V * D * i;
+    lo_half_step(D, W, g, dt, &fv->gas, Wf);
+    for (int v = 0; v < V; ++v) Wf[v] += dotd(D, g + D * v, r);
+    const int fallback = !(Wf[0] > 0 && Wf[D + 1] > 0);
+    if (fallback)
+        for (int v = 0; v < V; ++v) Wf[v] = W[v];
+    return fallback;
+}
+
+void lo_fv_step_adjoint(lo_fv* fv, double dt, double* qbar) {
+    const int D = fv->D, V = fv->V, U = fv->U;
+    const int64_t N = fv->n, F = fv->f;
+    primitives(fv);
+    fv->prims_ready = 1;
+    fv->swept = 0;
+    fit_t* fits = (fit_t*)malloc(sizeof(fit_t) * (size_t)N);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < N; ++i) sweep_fit_cell(fv, i, fits + i);
+    /* AdjointFaces (finite_volume.hpp:2078-2102): the bars of both face states, one row per face */
+    double* face_bar = (double*)calloc((size_t)F * 2 * V, sizeof(double));
+#pragma omp parallel for schedule(static)
+    for (int64_t f = 0; f < F; ++f) {
+        const double* a = fv->mesh.area + D * f;
+        const double magnitude = sqrt(dotd(D, a, a));
+        double Lbar[VMAX] = {0, 0, 0, 0, 0}, Rbar[VMAX] = {0, 0, 0, 0, 0};
+        if (magnitude != 0) {
+            const int64_t o = fv->mesh.owner[f], j = fv->mesh.neighbour[f];
+            double ro[3], rj[3], L[VMAX], R[VMAX], n[3], Fbar[VMAX], zero[3] = {0, 0, 0};
+            face_offset(fv, f, o, ro);
+            face_offset(fv, f, j, rj);
+            side_value(fv, o, ro, dt, L);
+            side_value(fv, j, rj, dt, R);
+            for (int v = 0; v < V; ++v) Fbar[v] = magnitude * dt * (qbar[V * j + v] - qbar[V * o + v]);
+            const double inv = 1.0 / magnitude;
+            for (int k = 0; k < D; ++k) n[k] = a[k] * inv;
+            if (fv->riemann == 1)
+                hll_flux_adjoint(D, L, R, n, zero, &fv->gas, Fbar, Lbar, Rbar);
+            else
+                hllc_flux_adjoint(D, L, R, n, zero, &fv->gas, Fbar, Lbar, Rbar);
+        }
+        for (int v = 0; v < V; ++v) {
+            face_bar[2 * V * f + v] = Lbar[v];
+            face_bar[2 * V * f + V + v] = Rbar[v];
+        }
+    }
+    /* AdjointCell (finite_volume.hpp:2107-2169) */
+    double* wbar = (double*)calloc((size_t)N * V, sizeof(double));
+    double* bbar = (double*)calloc((size_t)N * V * U, sizeof(double));
+    double* boundbar = (double*)calloc((size_t)N * V, sizeof(double));
+    int* bound_face = (int*)calloc((size_t)N * V, sizeof(int));
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < N; ++i) {
+        const double* Wi = fv->prims + (V + 2) * i;
+        const double* gi = fv->grad + V * D * i;
+        double Wi_bar[VMAX] = {0, 0, 0, 0, 0}, gi_bar[VMAX * 3];
+        memset(gi_bar, 0, sizeof(gi_bar));
+        for (int32_t k = fv->mesh.start[i]; k < fv->mesh.start[i + 1]; ++k) {
+            const int32_t e = fv->mesh.list[k];
+            const int f = list_face(e);
+            const double* a = fv->mesh.area + D * f;
+            if (dotd(D, a, a) == 0) continue;
+            const double* mine = face_bar + 2 * V * f + (e >= 0 ? 0 : V);
+            double r[3], Wf[VMAX];
+            face_offset(fv, f, i, r);
+            const int fallback = side_value(fv, i, r, dt, Wf);
+            if (fallback) {
+                for (int v = 0; v < V; ++v) Wi_bar[v] += mine[v];
+            } else {
+                for (int v = 0; v < V; ++v)
+                    for (int q = 0; q < D; ++q) gi_bar[D * v + q] = gi_bar[D * v + q] + r[q] * mine[v];
+                half_step_adjoint(D, Wi, gi, dt, &fv->gas, mine, Wi_bar, gi_bar);
+            }
+        }
+        const fit_t* ft = fits + i;
+        double xbar[VMAX][UMAX], bsol[VMAX][UMAX], self[VMAX], bnd[VMAX];
+        int face[VMAX];
+        for (int v = 0; v < V; ++v) {
+            const double* g0 = ft->g0 + D * v;
+            double g0bar[3];
+            for (int a = 0; a < D; ++a) g0bar[a] = gi_bar[D * v + a];
+            self[v] = 0;
+            bnd[v] = 0;
+            face[v] = -1;
+            if (ft->clipped[v] && ft->zero[v]) {
+                for (int a = 0; a < D; ++a) g0bar[a] = 0;
+            } else if (ft->clipped[v]) {
+                const double* o = ft->offset + D * v;
+                const double den = dotd(D, g0, o);
+                const double s = (ft->bound[v] - Wi[v]) / den, t = dotd(D, gi_bar + D * v, g0) / den;
+                for (int a = 0; a < D; ++a) g0bar[a] = gi_bar[D * v + a] * s - o[a] * (s * t);
+                bnd[v] = t;
+                face[v] = ft->bound_face[v];
+                self[v] -= t;
+            }
+            xbar[v][0] = 0;
+            for (int a = 0; a < D; ++a) xbar[v][1 + a] = g0bar[a];
+        }
+        /* solve_factored (finite_volume.hpp:688-702): b bar = M^-1 x bar */
+        for (int v = 0; v < V; ++v) {
+            double z[UMAX];
+            for (int p = 0; p < U; ++p) {
+                double sum = xbar[v][p];
+                for (int m = 0; m < p; ++m) sum -= ft->Lc[p][m] * z[m];
+                z[p] = sum / ft->Lc[p][p];
+            }
+            for (int p = U - 1; p >= 0; --p) {
+                double sum = z[p];
+                for (int m = p + 1; m < U; ++m) sum -= ft->Lc[m][p] * bsol[v][m];
+                bsol[v][p] = sum / ft->Lc[p][p];
+            }
+        }
+        for (int v = 0; v < V; ++v) {
+            for (int p = 0; p < U; ++p) self[v] -= ft->M0[p] * bsol[v][p];
+            wbar[V * i + v] = Wi_bar[v] + self[v];
+            for (int p = 0; p < U; ++p) bbar[(size_t)(U * V) * i + U * v + p] = bsol[v][p];
+            boundbar[V * i + v] = bnd[v];
+            bound_face[V * i + v] = face[v];
+        }
+    }
+    /* AdjointGather (finite_volume.hpp:2171-2195) */
+#pragma omp parallel for schedule(static)
+    for (int64_t j = 0; j < N; ++j) {
+        double W_bar[VMAX];
+        for (int v = 0; v < V; ++v) W_bar[v] = wbar[V * j + v];
+        const double* cj = fv->mesh.centroid + D * j;
+        for (int32_t k = fv->mesh.start[j]; k < fv->mesh.start[j + 1]; ++k) {
+            const int32_t e = fv->mesh.list[k];
+            const int f = list_face(e);
+            const int64_t i = e >= 0 ? fv->mesh.neighbour[f] : fv->mesh.owner[f];
+            double sep[3], between[3];
+            separation(fv, i, j, sep);
+            for (int a = 0; a < D; ++a) between[a] = sep[a] + cj[a] - fv->mesh.centroid[D * i + a];
+            const double w = fv->mag[f];
+            for (int v = 0; v < V; ++v) {
+                const double* bb = bbar + (size_t)(U * V) * i + U * v;
+                double sum = bb[0];
+                for (int p = 1; p < U; ++p) sum += between[p - 1] * bb[p];
+                W_bar[v] += w * sum + (bound_face[V * i + v] == f ? boundbar[V * i + v] : 0.0);
+            }
+        }
+        const double inv = 1.0 / fv->mesh.volume[j];
+        double Uj[VMAX], U_bar[VMAX];
+        for (int v = 0; v < V; ++v) Uj[v] = fv->q[V * j + v] * inv;
+        primitive_adjoint(D, Uj, W_bar, &fv->gas, U_bar);
+        for (int v = 0; v < V; ++v) qbar[V * j + v] += U_bar[v] * inv;
+    }
+    free(fits);
+    free(face_bar);
+    free(wbar);
+    free(bbar);
+    free(boundbar);
+    free(bound_face);
+}

@@ -27,7 +27,7 @@ def pair(mesh, q0, **kw):
     ora = O.OracleFV(mesh, order=kw.get("order", 1), per_face=kw.get("update", "per_face") == "per_face",
                      limiter=kw.get("limiter", "face_centroid"), riemann=kw.get("riemann", "hllc"),
                      moving=kw.get("motion", "static_mesh") == "moving",
-                     precision="riemann32" if prec == "fp32" else "double")
+                     precision={"fp32": "riemann32", "grad32": "grad32"}.get(prec, "double"))
     gpu.set_state(q0)
     ora.set_state(q0)
     return gpu, ora
@@ -78,10 +78,11 @@ def test_blast_32_fp64_50_steps(cuda):
     assert gpu.fallbacks() == ora.fallbacks()
 
 
-def test_fp32_policy_matches_oracle_policy(cuda):
+@pytest.mark.parametrize("precision", ["fp32", "grad32"])
+def test_reduced_policy_matches_oracle_policy(cuda, precision):
     mesh = jittered_mesh(16)
     q0 = rough_state(mesh.n_cells) * mesh.volume[:, None]
-    gpu, ora = pair(mesh, q0, precision="fp32")
+    gpu, ora = pair(mesh, q0, precision=precision)
     dt = ora.time_step(0.3)
     assert abs(gpu.time_step(0.3) - dt) <= 1e-14 * dt
     gpu.step(dt)
@@ -89,25 +90,33 @@ def test_fp32_policy_matches_oracle_policy(cuda):
     assert relative(gpu.get_state(), ora.get_state()) < 1e-6
 
 
-def test_fp32_against_fp64_acoustic_wave(cuda):
-    """FP32 face arithmetic against FP64 on the smooth wave (amplitude 1e-6, 20 steps): relative L1 of the perturbation
-    of Q (Q minus the background) within 1e-5."""
+@pytest.mark.parametrize("problem", ["wave", "blast"])
+def test_reduced_policies_against_fp64(cuda, problem):
+    """The reduced policies against FP64 (20 steps, each run its own dt): relative L1 of Q within 1e-5 for both. On the
+    1e-6 acoustic wave also the error of the perturbation (Q minus the background): the double Riemann solve of grad32
+    keeps it within 1e-5; the float Riemann solve of fp32 sees the O(1) face states at float's resolution (6e-8), i.e.
+    the 1e-6 perturbation to a few per cent, which is bounded here and stated, not hidden."""
     mesh = jittered_mesh(16)
-    q0 = acoustic_wave(mesh, amplitude=1e-6)
+    q0 = acoustic_wave(mesh, amplitude=1e-6) if problem == "wave" else point_blast(mesh, radius_cells=2.5)
     res = {}
-    for prec in ("fp64", "fp32"):
+    for prec in ("fp64", "fp32", "grad32"):
         fv = hydro.FiniteVolume(mesh, precision=prec)
         fv.set_state(q0)
         for _ in range(20):
             fv.step(fv.time_step(0.3))
         res[prec] = fv.get_state()
-    background = acoustic_wave(mesh, amplitude=0.0)
-    p64, p32 = res["fp64"] - background, res["fp32"] - background
-    assert np.abs(p32 - p64).sum() / np.abs(p64).sum() < 1e-5
+    for prec in ("fp32", "grad32"):
+        assert np.abs(res[prec] - res["fp64"]).sum() / np.abs(res["fp64"]).sum() < 1e-5
+    if problem == "wave":
+        background = acoustic_wave(mesh, amplitude=0.0)
+        p64 = res["fp64"] - background
+        pert = {prec: np.abs(res[prec] - res["fp64"]).sum() / np.abs(p64).sum() for prec in ("fp32", "grad32")}
+        assert pert["grad32"] < 1e-5
+        assert pert["fp32"] < 0.2
 
 
 @pytest.mark.parametrize("order", [0, 1])
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "grad32"])
 def test_uniform_state_stays_uniform(cuda, order, precision):
     mesh = jittered_mesh(16)
     W = np.array([1.3, 0.3, -0.2, 0.1, 0.7])
@@ -120,7 +129,7 @@ def test_uniform_state_stays_uniform(cuda, order, precision):
     assert relative(got, np.tile(U, (mesh.n_cells, 1))) < (1e-13 if precision == "fp64" else 1e-6)
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "grad32"])
 def test_conservation_and_determinism(cuda, precision):
     mesh = jittered_mesh(16)
     q0 = rough_state(mesh.n_cells) * mesh.volume[:, None]
