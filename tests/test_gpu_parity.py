@@ -14,7 +14,8 @@ pytestmark = pytest.mark.gpu
 
 
 def relative(a, b):
-    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+    scale = np.max(np.abs(b))
+    return float(np.max(np.abs(a - b)) / scale) if scale > 0 else float(np.max(np.abs(a - b)))
 
 
 def rel_l1(a, b):
