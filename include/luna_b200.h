@@ -135,6 +135,22 @@ typedef struct {
 LUNA_API luna_status luna_fv_set_timing(luna_fv* fv, int on);
 LUNA_API luna_status luna_fv_timings(luna_fv* fv, luna_timings* out, int reset);
 
+/* The flux-and-update pass of one static step (apply(), per-face loop) that allocates nothing, for callers that cannot
+ * allocate device memory themselves: code that must run with a fixed device footprint, or under a runtime or memory
+ * pool that owns every device allocation and hands the caller only finished buffers. It has no counterpart in the
+ * reference (whose steps always borrow scratch from the mesh or allocate it).
+ * The caller passes everything in device memory: the mesh arrays (mesh->on_device must be 1), Q [N][D + 2] (updated in
+ * place: Q -= dt * sum of the face fluxes, in list order), and at order 1 the primitive rows [N][8] (W, c, r, then
+ * padding) and the gradient rows (3D: [N][16], 2D: [N][8]; dW_v/dx_d at v * D + d, then padding) of the step's sweep.
+ * The per-face flux rows go to one fixed device array of 32 MiB inside the library, so a mesh may have at most
+ * 838,854 faces in 3D (1,048,568 in 2D); larger meshes are rejected with LUNA_EINVAL. Every GPU that loads the library
+ * holds that array until the process exits. Every call shares it and it keeps the last call's contents; calls that
+ * overlap on the GPU (other streams, other threads) race. The first call on a device looks up the array's device
+ * address (once per device, with that device current); make that first call before any stream capture.
+ * fallbacks_out (optional): the face sides that fell back to the cell's state; reading it synchronises the stream. */
+LUNA_API luna_status luna_apply_static_noalloc(const luna_mesh_desc* mesh, const luna_gas* gas, int order, int riemann, const double* prims,
+                                               const double* gradients, double* q, double dt, void* stream, int64_t* fallbacks_out);
+
 LUNA_API const char* luna_status_string(luna_status s);
 LUNA_API const char* luna_last_error(void);
 /* Device bytes held by fv (all its buffers). */

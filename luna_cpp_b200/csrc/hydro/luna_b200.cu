@@ -78,6 +78,11 @@ int blocks(int64_t n, int per) { return static_cast<int>((n + per - 1) / per); }
 
 }  // namespace
 
+namespace luna {
+// Other translation units of the library report through the same last-error slot as the entry points here.
+luna_status report_error(luna_status s, const std::string& what) { return set_error(s, what); }
+}  // namespace luna
+
 struct luna_fv {
     int dim = 3, order = 1, update = LUNA_UPDATE_PER_FACE, limiter = LUNA_LIMITER_FACE_CENTROID, motion = LUNA_STATIC_MESH,
         riemann = LUNA_HLLC, precision = LUNA_FP64;

@@ -80,6 +80,7 @@ SIGNATURES = {
     "luna_fv_device_bytes": ([P, P], I),
     "luna_fv_set_timing": ([P, I], I),
     "luna_fv_step_adjoint": ([P, D64, P, I], I),
+    "luna_apply_static_noalloc": ([P, P, I, I, P, P, P, D64, P, P], I),
     "luna_fv_timings": ([P, P, I], I),
 }
 
