@@ -173,185 +173,6 @@ __device__ __forceinline__ float finite_max<float>() {
     return 3.40282347e38f;
 }
 
-// The sweep of time_step(), one thread a cell (Sweep<Moving, Grad>::operator(), finite_volume.hpp:463-569): walk 1 over
-// the cell's list sums the area-weighted least-squares fit with intercept (M, b), the neighbours' range, the surface,
-// the smallest face and (moving) the largest face angle; faces below 1e-6 of the surface leave the range (a third walk,
-// rare); the fit is solved by Cholesky; walk 2 clips the gradient at each face centroid in list order. Moving: the point
-// velocity with AREPO's regularisation. The CFL terms (TimeStep, finite_volume.hpp:1040-1104) ride in walk 1: each owned
-// face's two terms and the cell's term, reduced per block into one atomicMin.
-// G: double (Precision<>) or float (Grad32: exact = false, ranges of W_j - W_i rounded once).
-template <int D, bool Moving, bool Grad, class G, bool Limit>
-__global__ void __launch_bounds__(128) k_sweep(MeshDev<D> m, const double* __restrict__ prims, G* __restrict__ grad_out,
-                                               double* __restrict__ w_out, double courant, Counters* __restrict__ ctr) {
-    constexpr int V = D + 2, U = D + 1, GS = grad_stride<D>();
-    constexpr bool exact = sizeof(G) == sizeof(double);
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double smallest_dt = 1.0e300;
-    if (i < m.n) {
-        const double* pi = prims + PS * i;
-        double Wi[V];
-#pragma unroll
-        for (int v = 0; v < V; ++v) Wi[v] = pi[v];
-        const double ci = pi[V], ri = pi[V + 1];
-        double surface = 0, smallest = __longlong_as_double(0x7ff0000000000000ll), max_angle = 0;
-        G lo[V], hi[V];
-        G M[U][U], b[V][U];
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-            lo[v] = finite_max<G>();
-            hi[v] = -finite_max<G>();
-#pragma unroll
-            for (int p = 0; p < U; ++p) b[v][p] = G(0);
-        }
-#pragma unroll
-        for (int p = 0; p < U; ++p)
-#pragma unroll
-            for (int s = 0; s < U; ++s) M[p][s] = G(0);
-        double centroid[D];
-#pragma unroll
-        for (int a = 0; a < D; ++a) centroid[a] = m.cen[D * i + a];
-        const int first = m.start[i], end = m.start[i + 1];
-        for (int k = first; k < end; ++k) {
-            const int32_t e = m.list[k];
-            const int f = list_face(e);
-            const int j = e >= 0 ? m.neighbour[f] : m.owner[f];
-            const double* pj = prims + PS * j;
-            double Wj[V];
-#pragma unroll
-            for (int v = 0; v < V; ++v) Wj[v] = pj[v];
-            double d[D];
-            m.separation(i, j, d);
-            const double magnitude = m.mag[f];
-            surface += magnitude;
-            smallest = fmin(smallest, magnitude);
-            const double d2 = dot<D>(d, d);
-            if constexpr (Moving) max_angle = fmax(max_angle, face_angle<D>(magnitude) / (0.5 * sqrt(d2)));
-            if (e >= 0) {  // FaceStep (finite_volume.hpp:1074-1090) for the faces this cell owns
-                const double dist = sqrt(d2);
-                double dv[D];
-#pragma unroll
-                for (int a = 0; a < D; ++a) dv[a] = Wj[1 + a] - Wi[1 + a];
-                const double vsig = ci + pj[V] - dot<D>(dv, d) / dist;
-                if (vsig > 0) {
-                    smallest_dt = fmin(smallest_dt, courant * ((dist + ri) / vsig));
-                    smallest_dt = fmin(smallest_dt, courant * ((dist + pj[V + 1]) / vsig));
-                }
-            }
-            if constexpr (Grad) {
-                G X[U];
-                X[0] = G(1);
-#pragma unroll
-                for (int p = 1; p < U; ++p) X[p] = static_cast<G>(d[p - 1] + m.cen[D * j + p - 1] - centroid[p - 1]);
-                const G w = static_cast<G>(magnitude);
-#pragma unroll
-                for (int p = 0; p < U; ++p)
-#pragma unroll
-                    for (int s = p; s < U; ++s) M[p][s] += w * X[p] * X[s];
-#pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    const double dW = Wj[v] - Wi[v];
-#pragma unroll
-                    for (int p = 0; p < U; ++p) b[v][p] += w * X[p] * static_cast<G>(dW);
-                    const G value = exact ? static_cast<G>(Wj[v]) : static_cast<G>(dW);
-                    lo[v] = fmin(lo[v], value);
-                    hi[v] = fmax(hi[v], value);
-                }
-            }
-        }
-        // CellStep (finite_volume.hpp:1040-1052).
-        double wi[D];
-#pragma unroll
-        for (int a = 0; a < D; ++a) wi[a] = Wi[1 + a];
-        if constexpr (Moving) {
-            const double factor = 2.25, speed = 0.5;
-            double fraction = 0;
-            if (max_angle > 0.75 * factor) fraction = max_angle > factor ? speed : speed * (max_angle - 0.75 * factor) / (0.25 * factor);
-            const double cd = sqrt(dot<D>(centroid, centroid));
-            if (cd > 0 && fraction > 0) {
-                const double s = fraction * ci / cd;
-#pragma unroll
-                for (int a = 0; a < D; ++a) wi[a] = wi[a] + centroid[a] * s;
-            }
-#pragma unroll
-            for (int a = 0; a < D; ++a) w_out[D * i + a] = wi[a];
-        }
-        {
-            double rel[D];
-#pragma unroll
-            for (int a = 0; a < D; ++a) rel[a] = Wi[1 + a] - (Moving ? wi[a] : 0.0);
-            smallest_dt = fmin(smallest_dt, courant * (ri / (ci + sqrt(dot<D>(rel, rel)))));
-        }
-        if constexpr (Grad) {
-            const double tiny = 1e-6 * surface;
-            const bool any_tiny = smallest < tiny;
-            if (any_tiny) {  // neighbour_range (finite_volume.hpp:572-588)
-#pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    lo[v] = finite_max<G>();
-                    hi[v] = -finite_max<G>();
-                }
-                for (int k = first; k < end; ++k) {
-                    const int32_t e = m.list[k];
-                    const int f = list_face(e);
-                    if (m.mag[f] < tiny) continue;
-                    const int j = e >= 0 ? m.neighbour[f] : m.owner[f];
-                    const double* pj = prims + PS * j;
-#pragma unroll
-                    for (int v = 0; v < V; ++v) {
-                        const G value = exact ? static_cast<G>(pj[v]) : static_cast<G>(pj[v] - Wi[v]);
-                        lo[v] = fmin(lo[v], value);
-                        hi[v] = fmax(hi[v], value);
-                    }
-                }
-            }
-            G g[V * D];
-            cholesky_solve<D, G>(M, b, g);
-            if constexpr (Limit) {
-                for (int k = first; k < end; ++k) {
-                    const int f = list_face(m.list[k]);
-                    if (any_tiny && m.mag[f] < tiny) continue;
-                    double offset[D];
-                    m.face_offset(f, i, offset);
-                    G rg[D];
-#pragma unroll
-                    for (int a = 0; a < D; ++a) rg[a] = static_cast<G>(offset[a]);
-#pragma unroll
-                    for (int v = 0; v < V; ++v) {
-                        G* gv = g + D * v;
-                        const G dp = dot<D>(gv, rg);
-                        if constexpr (exact) {
-                            if (dp > 0 && Wi[v] + dp > hi[v]) {
-                                const G s = hi[v] > Wi[v] ? (hi[v] - Wi[v]) / dp : G(0);
-#pragma unroll
-                                for (int a = 0; a < D; ++a) gv[a] = gv[a] * s;
-                            } else if (dp < 0 && Wi[v] + dp < lo[v]) {
-                                const G s = lo[v] < Wi[v] ? (lo[v] - Wi[v]) / dp : G(0);
-#pragma unroll
-                                for (int a = 0; a < D; ++a) gv[a] = gv[a] * s;
-                            }
-                        } else {
-                            if (dp > 0 && dp > hi[v]) {
-                                const G s = hi[v] > 0 ? hi[v] / dp : G(0);
-#pragma unroll
-                                for (int a = 0; a < D; ++a) gv[a] = gv[a] * s;
-                            } else if (dp < 0 && dp < lo[v]) {
-                                const G s = lo[v] < 0 ? lo[v] / dp : G(0);
-#pragma unroll
-                                for (int a = 0; a < D; ++a) gv[a] = gv[a] * s;
-                            }
-                        }
-                    }
-                }
-            }
-            G* out = grad_out + static_cast<int64_t>(GS) * i;
-#pragma unroll
-            for (int c = 0; c < V * D; ++c) out[c] = g[c];
-        }
-    }
-    block_min_to(smallest_dt, &ctr->dt_bits);
-    if (i < m.n && !(smallest_dt == smallest_dt)) atomicOr(&ctr->error, 1ull);
-}
-
 // What a flux pass needs beyond the mesh: the state rows and the moving step's extra rows.
 template <int D, class G>
 struct FluxArgs {

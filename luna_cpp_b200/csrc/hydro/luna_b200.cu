@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "adjoint.cuh"
+#include "geometry.cuh"
 #include "kernels.cuh"
 #include "luna_b200.h"
 
@@ -99,6 +100,10 @@ struct luna_fv {
     DevArray<float> grad32;
     DevArray<int32_t> steps;
     DevArray<luna::Counters> counters;
+    // the mesh reordered for the step (geometry.cuh), rebuilt by every load_mesh
+    DevArray<unsigned char> geo_entries, geo_factors, geo_dt, geo_faces;
+    DevArray<unsigned int> geo_face_tiny;
+    DevArray<double> geo_angle;
     // adjoint (allocated by the first luna_fv_step_adjoint)
     DevArray<double> adj_fit, adj_face_bar, adj_wbar, adj_bbar, adj_boundbar, adj_qbar;
     DevArray<int32_t> adj_flags, adj_bound_face;
@@ -143,6 +148,18 @@ struct luna_fv {
     }
     void close_timed(long slot) {
         if (slot >= 0) cudaEventRecord(event_pool[static_cast<size_t>(slot)].second, stream);
+    }
+
+    template <int D, class G>
+    luna::GeometryDev<D, G> geometry_dev() const {
+        luna::GeometryDev<D, G> g;
+        g.entries = reinterpret_cast<luna::EntryRow<G>*>(geo_entries.ptr);
+        g.face_tiny = geo_face_tiny.ptr;
+        g.factors = reinterpret_cast<G*>(geo_factors.ptr);
+        g.dt_rows = reinterpret_cast<luna::DtRow*>(geo_dt.ptr);
+        g.faces = reinterpret_cast<luna::FaceRow<G>*>(geo_faces.ptr);
+        g.max_angle = geo_angle.ptr;
+        return g;
     }
 
     template <int D>
@@ -206,6 +223,21 @@ luna_status validate_mesh(const luna_mesh_desc* m, int dim, int64_t n) {
     return LUNA_OK;
 }
 
+// The reordered rows of the current mesh (geometry.cuh::k_geometry), in the policy's gradient type.
+template <int D, class G>
+luna_status build_geometry(luna_fv* fv) {
+    const size_t N = static_cast<size_t>(fv->n), F = static_cast<size_t>(fv->f);
+    LUNA_TRY(fv->geo_entries.alloc(sizeof(luna::EntryRow<G>) * (2 * F > 0 ? 2 * F : 1), "entry rows"));
+    if (sizeof(G) != sizeof(double)) LUNA_TRY(fv->geo_face_tiny.alloc(2 * F > 0 ? 2 * F : 1, "entry face words"));
+    LUNA_TRY(fv->geo_factors.alloc(sizeof(G) * luna::factor_width<D>() * N, "fit factors"));
+    LUNA_TRY(fv->geo_dt.alloc(sizeof(luna::DtRow) * (F > 0 ? F : 1), "dt rows"));
+    LUNA_TRY(fv->geo_faces.alloc(sizeof(luna::FaceRow<G>) * (F > 0 ? F : 1), "face rows"));
+    LUNA_TRY(fv->geo_angle.alloc(N, "face angles"));
+    luna::k_geometry<D, G><<<blocks(N, 128), 128, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->geometry_dev<D, G>());
+    LUNA_CUDA(cudaGetLastError());
+    return LUNA_OK;
+}
+
 luna_status load_mesh(luna_fv* fv, const luna_mesh_desc* m) {
     const int D = m->dim;
     const size_t N = static_cast<size_t>(m->n_cells), F = static_cast<size_t>(m->n_faces);
@@ -232,7 +264,8 @@ luna_status load_mesh(luna_fv* fv, const luna_mesh_desc* m) {
     }
     if (fv->update == LUNA_UPDATE_PER_FACE) LUNA_TRY(fv->flux.alloc(F * (D + 2) > 0 ? F * (D + 2) : 1, "flux rows"));
     // Lists in device memory are trusted as voronoi-cpp's; the sweep does not re-check them.
-    return LUNA_OK;
+    return fv->precision == LUNA_FP64 ? (D == 3 ? build_geometry<3, double>(fv) : build_geometry<2, double>(fv))
+                                      : (D == 3 ? build_geometry<3, float>(fv) : build_geometry<2, float>(fv));
 }
 
 template <int D>
@@ -249,20 +282,17 @@ luna_status run_primitives(luna_fv* fv) {
 template <int D, bool Moving, bool Grad, class G>
 luna_status launch_sweep(luna_fv* fv, G* grad, double courant) {
     const auto m = fv->mesh_dev<D>();
-    if (fv->limiter == LUNA_LIMITER_NONE)
-        {
-            const long timed_ = fv->open_timed(1);
-            luna::k_sweep<D, Moving, Grad, G, false><<<blocks(fv->n, kBlockCells), kBlockCells, 0, fv->stream>>>(m, fv->prims.ptr, grad, fv->w.ptr, courant,
-                                                                                                               fv->counters.ptr);
-            fv->close_timed(timed_);
-        }
-    else
-        {
-            const long timed_ = fv->open_timed(1);
-            luna::k_sweep<D, Moving, Grad, G, true><<<blocks(fv->n, kBlockCells), kBlockCells, 0, fv->stream>>>(m, fv->prims.ptr, grad, fv->w.ptr, courant,
-                                                                                                              fv->counters.ptr);
-            fv->close_timed(timed_);
-        }
+    const auto geo = fv->geometry_dev<D, G>();
+    {
+        const long timed_ = fv->open_timed(1);
+        if (fv->limiter == LUNA_LIMITER_NONE)
+            luna::k_sweep_rows<D, Moving, Grad, G, false><<<blocks(fv->n, kBlockCells), kBlockCells, 0, fv->stream>>>(m, geo, fv->prims.ptr, grad,
+                                                                                                                fv->w.ptr, courant, fv->counters.ptr);
+        else
+            luna::k_sweep_rows<D, Moving, Grad, G, true><<<blocks(fv->n, kBlockCells), kBlockCells, 0, fv->stream>>>(m, geo, fv->prims.ptr, grad,
+                                                                                                               fv->w.ptr, courant, fv->counters.ptr);
+        fv->close_timed(timed_);
+    }
     LUNA_CUDA(cudaGetLastError());
     return LUNA_OK;
 }
@@ -305,6 +335,26 @@ luna_status launch_flux(luna_fv* fv, const luna::FluxArgs<D, G>& x) {
     }
     LUNA_CUDA(cudaGetLastError());
     return LUNA_OK;
+}
+
+template <int D, int Order, class G, bool RF, int Riemann>
+luna_status launch_flux_rows(luna_fv* fv, const luna::FluxArgs<D, G>& x) {
+    if (fv->f == 0) return LUNA_OK;
+    {
+        const long timed_ = fv->open_timed(2);
+        luna::k_flux_rows<D, Order, G, RF, Riemann><<<blocks(fv->f, kBlockFaces), kBlockFaces, 0, fv->stream>>>(
+            fv->mesh_dev<D>(), fv->geometry_dev<D, G>(), x, fv->flux.ptr, &fv->counters.ptr->fallbacks[0]);
+        fv->close_timed(timed_);
+    }
+    LUNA_CUDA(cudaGetLastError());
+    return LUNA_OK;
+}
+
+template <int D, int Order, class G>
+luna_status dispatch_flux_rows(luna_fv* fv, const luna::FluxArgs<D, G>& x) {
+    if (fv->precision == LUNA_FP32) return launch_flux_rows<D, Order, G, true, 0>(fv, x);
+    if (fv->riemann == LUNA_HLL) return launch_flux_rows<D, Order, G, false, 1>(fv, x);
+    return launch_flux_rows<D, Order, G, false, 0>(fv, x);
 }
 
 template <int D, int Order, int Pass, class G>
@@ -355,9 +405,9 @@ luna_status run_apply(luna_fv* fv, const G* grad, double dt) {
         return fv->riemann == LUNA_HLL ? launch_per_cell<D, 1, G, false, 1>(fv, x, dt) : launch_per_cell<D, 1, G, false, 0>(fv, x, dt);
     }
     if (fv->order == 0)
-        LUNA_TRY((dispatch_flux<D, 0, -1, G>(fv, x)));
+        LUNA_TRY((dispatch_flux_rows<D, 0, G>(fv, x)));
     else
-        LUNA_TRY((dispatch_flux<D, 1, -1, G>(fv, x)));
+        LUNA_TRY((dispatch_flux_rows<D, 1, G>(fv, x)));
     {
         const long timed_ = fv->open_timed(3);
         luna::k_update<D, true><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->q.ptr, fv->flux.ptr, dt, fv->prims.ptr, fv->gas,
@@ -812,6 +862,8 @@ LUNA_API luna_status luna_fv_device_bytes(luna_fv* fv, int64_t* out) {
     b += fv->w.bytes() + fv->x.bytes() + fv->old_cen.bytes() + fv->steps.bytes() + fv->counters.bytes();
     b += fv->adj_fit.bytes() + fv->adj_face_bar.bytes() + fv->adj_wbar.bytes() + fv->adj_bbar.bytes() + fv->adj_boundbar.bytes();
     b += fv->adj_qbar.bytes() + fv->adj_flags.bytes() + fv->adj_bound_face.bytes();
+    b += fv->geo_entries.bytes() + fv->geo_factors.bytes() + fv->geo_dt.bytes() + fv->geo_faces.bytes() + fv->geo_face_tiny.bytes();
+    b += fv->geo_angle.bytes();
     *out = static_cast<int64_t>(b);
     return LUNA_OK;
 }
