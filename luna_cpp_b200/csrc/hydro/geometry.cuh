@@ -4,13 +4,16 @@
 // costs three dependent loads (list -> face -> neighbour -> rows) plus the separation, the fit row X = [1, d + c_j - c_i]
 // and the face offset. Everything there except the neighbours' primitive rows depends on the mesh only, so this pass
 // computes it once, in the reference's arithmetic, into rows that the step streams in list order:
-//   entry rows [2F]  per list entry: w X_p (the fit's weighted row, p = 0..D), the face offset x_f - c_i, the neighbour,
+//   entries          per list entry: w X_p (the fit's weighted row, p = 0..D), the face offset x_f - c_i, the neighbour,
 //                    whether the cell owns the face, the face, and whether the face is below 1e-6 of the cell's surface;
-//   fit factors [N]  the Cholesky factor of the cell's normal matrix M = sum w X X^T (finite_volume.hpp:591-602);
+//                    sliced by 32 cells (a warp): entry k of the slice's lane l sits at (slice_base + k) * 32 + l, each
+//                    field in an array of its own, so a warp's load of entry k of its 32 cells is one contiguous run;
+//                    the entry's row of the cell's gradient operator c_k (see k_geometry) instead of the fit's sums;
 //   dt rows [F]      the separation d of the face's generators and |d| (the CFL face terms, finite_volume.hpp:1074-1090);
 //   face rows [F]    the unit normal A / |A|, |A|, both cells' face offsets and the two cells (FaceFlux, :1415-1434);
 //   cell angle [N]   the largest AREPO face angle of the cell (the moving mesh's regularisation, :509, :526-537).
 // The step then reads one streamed row per entry and gathers only the neighbour's primitive row: one dependent level.
+// Cells are swept in an order grouping lists of one length (see kOrderWindow).
 #pragma once
 
 #include <type_traits>
@@ -19,20 +22,10 @@
 
 namespace luna {
 
-// A list entry's row. wx[p] = w X_p with w = |A_f| (p = 0 .. D), off = face offset; bits: neighbour | owned << 31 in the
-// low word, face | tiny << 31 in the high word (double rows); float rows keep the face word in a separate array.
-struct alignas(64) EntryRow64 {
-    double wx[4];
-    double off[3];
-    unsigned long long bits;
-};
-struct alignas(32) EntryRow32 {
-    float wx[4];
-    float off[3];
-    unsigned int nbr_owned;
-};
 template <class G>
-using EntryRow = typename std::conditional<sizeof(G) == sizeof(double), EntryRow64, EntryRow32>::type;
+using Pair = typename std::conditional<sizeof(G) == sizeof(double), double2, float2>::type;
+
+constexpr unsigned int kOwnedBit = 0x80000000u, kTinyBit = 0x40000000u, kIndexMask = 0x3fffffffu;
 
 // A face's row for the flux pass: n = A / |A| (double in every policy: grad32 solves in double; riemann32 rounds it to
 // float itself, as FaceFlux::solve does), |A|, the cells, and the face offsets from each cell's centroid in G.
@@ -59,38 +52,48 @@ struct DtRow {
     double dist;
 };
 
-template <int D>
-constexpr int factor_width() {
-    return (D + 1) * (D + 2) / 2;  // the lower triangle of the (D+1)^2 factor
-}
+// Cells are swept in `order`: by list length within windows of kOrderWindow cells, so the 32 cells of a warp have lists
+// of nearly one length (lanes of a warp idle while the longest list runs) and stay close in the mesh.
+constexpr int kOrderWindow = 512;
 
 template <int D, class G>
 struct GeometryDev {
-    EntryRow<G>* __restrict__ entries;
-    unsigned int* __restrict__ face_tiny;  // float rows: face | tiny << 31 per entry
-    G* __restrict__ factors;               // [N][factor_width]
-    DtRow* __restrict__ dt_rows;           // [F]
-    FaceRow<G>* __restrict__ faces;        // [F]
-    double* __restrict__ max_angle;        // [N]
+    const int32_t* __restrict__ order;       // [N]: thread t sweeps cell order[t]
+    const int32_t* __restrict__ slice_base;  // [ceil(N / 32) + 1], in slots of 32 entries
+    unsigned int* __restrict__ nbr;          // neighbour | tiny << 30 | owned << 31
+    unsigned int* __restrict__ face;         // the face (owned entries: their dt row)
+    Pair<G>* __restrict__ c01;               // gradient operator row c_k, x and y
+    G* __restrict__ c2;                      // z (3D)
+    Pair<G>* __restrict__ off01;             // face offset x, y
+    G* __restrict__ off2;                    // z (3D)
+    DtRow* __restrict__ dt_rows;             // [F]
+    FaceRow<G>* __restrict__ faces;          // [F]
+    double* __restrict__ max_angle;          // [N]
 };
 
-// One thread a cell: the cell's geometry in list order, as Sweep::operator() computes it (finite_volume.hpp:486-520),
-// and the face rows of the faces it owns.
+// One thread a cell (in sweep order): the cell's geometry in list order. The least-squares fit of Sweep (an area-
+// weighted fit with intercept over the face neighbours, finite_volume.hpp:486-515, 591-615) is linear in the
+// neighbours' differences: x_v = M^-1 sum_k w_k X_k (W_kv - W_iv) with M = sum_k w_k X_k X_k^T, so the gradient is
+// g_v = sum_k c_k (W_kv - W_iv) with c_k = rows 1..D of M^-1 w_k X_k. M, its Cholesky factor and each c_k are formed
+// here in double, in the reference's order; the sweep then only sums c_k times the differences. Also the face rows of
+// the faces the cell owns, the dt rows and the largest face angle.
 template <int D, class G>
 __global__ void __launch_bounds__(128) k_geometry(MeshDev<D> m, GeometryDev<D, G> g) {
     constexpr int U = D + 1;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m.n) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m.n) return;
+    const int i = g.order[t];
     double centroid[D];
 #pragma unroll
     for (int a = 0; a < D; ++a) centroid[a] = m.cen[D * i + a];
     const int first = m.start[i], end = m.start[i + 1];
+    const int64_t slot0 = static_cast<int64_t>(g.slice_base[t >> 5]) * 32 + (t & 31);
     double surface = 0, smallest = __longlong_as_double(0x7ff0000000000000ll), max_angle = 0;
-    G M[U][U];
+    double M[U][U];
 #pragma unroll
     for (int p = 0; p < U; ++p)
 #pragma unroll
-        for (int s = 0; s < U; ++s) M[p][s] = G(0);
+        for (int s = 0; s < U; ++s) M[p][s] = 0;
     for (int k = first; k < end; ++k) {
         const int32_t e = m.list[k];
         const int f = list_face(e);
@@ -102,26 +105,36 @@ __global__ void __launch_bounds__(128) k_geometry(MeshDev<D> m, GeometryDev<D, G
         smallest = fmin(smallest, magnitude);
         const double d2 = dot<D>(d, d);
         max_angle = fmax(max_angle, face_angle<D>(magnitude) / (0.5 * sqrt(d2)));
-        G X[U];
-        X[0] = G(1);
+        double X[U];
+        X[0] = 1;
 #pragma unroll
-        for (int p = 1; p < U; ++p) X[p] = static_cast<G>(d[p - 1] + m.cen[D * j + p - 1] - centroid[p - 1]);
-        const G w = static_cast<G>(magnitude);
+        for (int p = 1; p < U; ++p) X[p] = d[p - 1] + m.cen[D * j + p - 1] - centroid[p - 1];
 #pragma unroll
         for (int p = 0; p < U; ++p)
 #pragma unroll
-            for (int s = p; s < U; ++s) M[p][s] += w * X[p] * X[s];
-        EntryRow<G>& row = g.entries[k];
-#pragma unroll
-        for (int p = 0; p < 4; ++p) row.wx[p] = p < U ? w * X[p] : G(0);
+            for (int s = p; s < U; ++s) M[p][s] += magnitude * X[p] * X[s];
         if (e >= 0) {
-            DtRow t;
+            DtRow r;
 #pragma unroll
-            for (int a = 0; a < 3; ++a) t.d[a] = a < D ? d[a] : 0.0;
-            t.dist = sqrt(d2);
-            g.dt_rows[f] = t;
+            for (int a = 0; a < 3; ++a) r.d[a] = a < D ? d[a] : 0.0;
+            r.dist = sqrt(d2);
+            g.dt_rows[f] = r;
         }
     }
+    double L[U][U];
+#pragma unroll
+    for (int p = 0; p < U; ++p)
+#pragma unroll
+        for (int s = 0; s < U; ++s) L[p][s] = 0;
+#pragma unroll
+    for (int p = 0; p < U; ++p)
+#pragma unroll
+        for (int s = 0; s <= p; ++s) {
+            double sum = M[s][p];
+#pragma unroll
+            for (int q = 0; q < s; ++q) sum -= L[p][q] * L[s][q];
+            L[p][s] = p == s ? sqrt(sum) : sum / L[s][s];
+        }
     const double tiny = 1e-6 * surface;
     const bool any_tiny = smallest < tiny;
     for (int k = first; k < end; ++k) {
@@ -129,29 +142,46 @@ __global__ void __launch_bounds__(128) k_geometry(MeshDev<D> m, GeometryDev<D, G
         const int f = list_face(e);
         const bool owned = e >= 0;
         const int j = owned ? m.neighbour[f] : m.owner[f];
+        const int64_t slot = slot0 + 32 * static_cast<int64_t>(k - first);
+        // c_k: M^-1 (w X_k) by the factor, rows 1..D
+        double d[D], z[U], x[U], wX[U];
+        m.separation(i, j, d);
+        const double magnitude = m.mag[f];
+        wX[0] = magnitude;
+#pragma unroll
+        for (int p = 1; p < U; ++p) wX[p] = magnitude * (d[p - 1] + m.cen[D * j + p - 1] - centroid[p - 1]);
+#pragma unroll
+        for (int p = 0; p < U; ++p) {
+            double sum = wX[p];
+#pragma unroll
+            for (int q = 0; q < p; ++q) sum -= L[p][q] * z[q];
+            z[p] = sum / L[p][p];
+        }
+#pragma unroll
+        for (int p = U - 1; p >= 0; --p) {
+            double sum = z[p];
+#pragma unroll
+            for (int q = p + 1; q < U; ++q) sum -= L[q][p] * x[q];
+            x[p] = sum / L[p][p];
+        }
+        g.c01[slot] = Pair<G>{static_cast<G>(x[1]), static_cast<G>(x[2])};
+        if constexpr (D == 3) g.c2[slot] = static_cast<G>(x[3]);
         double off[D];
         m.face_offset(f, i, off);
-        const bool tiny_face = any_tiny && m.mag[f] < tiny;
-        EntryRow<G>& row = g.entries[k];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) row.off[a] = a < D ? static_cast<G>(off[a]) : G(0);
-        const unsigned int low = static_cast<unsigned int>(j) | (owned ? 0x80000000u : 0u);
-        const unsigned int high = static_cast<unsigned int>(f) | (tiny_face ? 0x80000000u : 0u);
-        if constexpr (sizeof(G) == sizeof(double)) {
-            row.bits = static_cast<unsigned long long>(low) | (static_cast<unsigned long long>(high) << 32);
-        } else {
-            row.nbr_owned = low;
-            g.face_tiny[k] = high;
-        }
+        g.off01[slot] = Pair<G>{static_cast<G>(off[0]), static_cast<G>(off[1])};
+        if constexpr (D == 3) g.off2[slot] = static_cast<G>(off[2]);
+        const bool tiny_face = any_tiny && magnitude < tiny;
+        g.nbr[slot] = static_cast<unsigned int>(j) | (owned ? kOwnedBit : 0u) | (tiny_face ? kTinyBit : 0u);
+        g.face[slot] = static_cast<unsigned int>(f);
         if (owned) {  // the face row, written once by the owner
             double a[D];
 #pragma unroll
             for (int q = 0; q < D; ++q) a[q] = m.area[D * f + q];
-            const double magnitude = sqrt(dot<D>(a, a));
+            const double amag = sqrt(dot<D>(a, a));
             double offj[D];
             m.face_offset(f, j, offj);
             FaceRow<G> r;
-            const double inv = magnitude == 0 ? 0.0 : 1.0 / magnitude;
+            const double inv = amag == 0 ? 0.0 : 1.0 / amag;
 #pragma unroll
             for (int q = 0; q < 3; ++q) {
                 r.n[q] = q < D ? a[q] * inv : 0.0;
@@ -163,106 +193,105 @@ __global__ void __launch_bounds__(128) k_geometry(MeshDev<D> m, GeometryDev<D, G
                     r.offj[q] = q < D ? static_cast<float>(offj[q]) : 0.0f;
                 }
             }
-            r.mag = magnitude;
+            r.mag = amag;
             r.o = i;
             r.j = j;
             if constexpr (sizeof(G) == sizeof(double)) r.pad = 0;
             g.faces[f] = r;
         }
     }
-    // Sweep::solve's factorisation (finite_volume.hpp:591-602), the lower triangle row by row.
-    G L[U][U];
-#pragma unroll
-    for (int p = 0; p < U; ++p)
-#pragma unroll
-        for (int s = 0; s < U; ++s) L[p][s] = G(0);
-#pragma unroll
-    for (int p = 0; p < U; ++p)
-#pragma unroll
-        for (int s = 0; s <= p; ++s) {
-            G sum = M[s][p];
-#pragma unroll
-            for (int q = 0; q < s; ++q) sum -= L[p][q] * L[s][q];
-            L[p][s] = p == s ? sqrt(sum) : sum / L[s][s];
-        }
-    G* out = g.factors + static_cast<int64_t>(factor_width<D>()) * i;
-    int c = 0;
-#pragma unroll
-    for (int p = 0; p < U; ++p)
-#pragma unroll
-        for (int s = 0; s <= p; ++s) out[c++] = L[p][s];
     g.max_angle[i] = max_angle;
 }
 
-// The sweep over the reordered rows (Sweep<Moving, Grad>::operator(), finite_volume.hpp:463-569, same arithmetic):
-// walk 1 sums b = sum w X (W_j - W_i) and the neighbours' range (tiny faces left out), and the owned faces' CFL terms;
-// the fit is solved with the cell's stored factor; walk 2 clips at each face offset in list order. One streamed row and
-// one gathered primitive row per entry.
+// The sweep over the reordered rows (Sweep<Moving, Grad>::operator(), finite_volume.hpp:463-569): walk 1 sums the
+// gradient g_v = sum_k c_k (W_jv - W_iv) in list order, the neighbours' range (tiny faces left out) and the owned faces'
+// CFL terms; walk 2 clips at each face offset in list order. Per entry: streamed coalesced rows and one gathered
+// primitive row (two 256-bit loads).
 template <int D, bool Moving, bool Grad, class G, bool Limit>
 __global__ void __launch_bounds__(128) k_sweep_rows(MeshDev<D> m, GeometryDev<D, G> geo, const double* __restrict__ prims,
                                                     G* __restrict__ grad_out, double* __restrict__ w_out, double courant,
                                                     Counters* __restrict__ ctr) {
-    constexpr int V = D + 2, U = D + 1, GS = grad_stride<D>();
+    constexpr int V = D + 2, GS = grad_stride<D>();
     constexpr bool exact = sizeof(G) == sizeof(double);
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double smallest_dt = 1.0e300;
-    if (i < m.n) {
-        const double* pi = prims + PS * i;
+    if (t < m.n) {
+        const int i = geo.order[t];
+        double pi[8];
+        load_prim_row<D>(prims, i, pi);
         double Wi[V];
 #pragma unroll
         for (int v = 0; v < V; ++v) Wi[v] = pi[v];
         const double ci = pi[V], ri = pi[V + 1];
-        G lo[V], hi[V], b[V][U];
+        G lo[V], hi[V], g[V * D];
 #pragma unroll
         for (int v = 0; v < V; ++v) {
             lo[v] = finite_max<G>();
             hi[v] = -finite_max<G>();
 #pragma unroll
-            for (int p = 0; p < U; ++p) b[v][p] = G(0);
+            for (int a = 0; a < D; ++a) g[D * v + a] = G(0);
         }
-        const int first = m.start[i], end = m.start[i + 1];
-        for (int k = first; k < end; ++k) {
-            const EntryRow<G>& row = geo.entries[k];
-            unsigned int low, high;
-            if constexpr (exact) {
-                const unsigned long long bits = row.bits;
-                low = static_cast<unsigned int>(bits);
-                high = static_cast<unsigned int>(bits >> 32);
-            } else {
-                low = row.nbr_owned;
-                high = geo.face_tiny[k];
+        const int count = m.start[i + 1] - m.start[i];
+        const int64_t row0 = static_cast<int64_t>(geo.slice_base[t >> 5]) * 32;  // the warp's first slot
+        const int64_t slot0 = row0 + (t & 31);
+        // Lane 0 holds the warp's longest list (cells are ordered by list length within windows): it streams the warp's
+        // entry rows into L2 kPrefetch entries ahead with bulk prefetches, one per array and entry.
+        constexpr int kPrefetch = 4;
+        const bool leader = (threadIdx.x & 31) == 0;
+        auto prefetch_rows = [&](int k) {
+            const int64_t r = row0 + 32 * static_cast<int64_t>(k);
+            prefetch_l2(geo.nbr + r, 32 * sizeof(unsigned int));
+            prefetch_l2(geo.face + r, 32 * sizeof(unsigned int));
+            if constexpr (Grad) {
+                prefetch_l2(geo.c01 + r, 32 * sizeof(Pair<G>));
+                if constexpr (D == 3) prefetch_l2(geo.c2 + r, 32 * sizeof(G));
+                if constexpr (Limit) {
+                    prefetch_l2(geo.off01 + r, 32 * sizeof(Pair<G>));
+                    if constexpr (D == 3) prefetch_l2(geo.off2 + r, 32 * sizeof(G));
+                }
             }
-            const int j = static_cast<int>(low & 0x7fffffffu);
-            const bool owned = (low >> 31) != 0, tiny_face = (high >> 31) != 0;
-            const double* pj = prims + PS * j;
-            double Wj[V];
-#pragma unroll
-            for (int v = 0; v < V; ++v) Wj[v] = pj[v];
+        };
+        if (leader)
+            for (int k = 0; k < kPrefetch && k < count; ++k) prefetch_rows(k);
+        // The neighbour word one entry ahead: entry k's row gather issues as soon as its iteration starts.
+        unsigned int next = count > 0 ? geo.nbr[slot0] : 0u;
+        for (int k = 0; k < count; ++k) {
+            const int64_t slot = slot0 + 32 * static_cast<int64_t>(k);
+            if (leader && k + kPrefetch < count) prefetch_rows(k + kPrefetch);
+            const unsigned int word = next;
+            if (k + 1 < count) next = geo.nbr[slot + 32];
+            const int j = static_cast<int>(word & kIndexMask);
+            const bool owned = (word & kOwnedBit) != 0, tiny_face = (word & kTinyBit) != 0;
+            double pj[8];
+            load_prim_row<D>(prims, j, pj);
             if (owned) {  // FaceStep (finite_volume.hpp:1074-1090)
-                const DtRow t = geo.dt_rows[high & 0x7fffffffu];
+                const DtRow r = geo.dt_rows[geo.face[slot]];
                 double dv[D], d[D];
 #pragma unroll
                 for (int a = 0; a < D; ++a) {
-                    dv[a] = Wj[1 + a] - Wi[1 + a];
-                    d[a] = t.d[a];
+                    dv[a] = pj[1 + a] - Wi[1 + a];
+                    d[a] = r.d[a];
                 }
-                const double vsig = ci + pj[V] - dot<D>(dv, d) / t.dist;
+                const double vsig = ci + pj[V] - dot<D>(dv, d) / r.dist;
                 if (vsig > 0) {
-                    smallest_dt = fmin(smallest_dt, courant * ((t.dist + ri) / vsig));
-                    smallest_dt = fmin(smallest_dt, courant * ((t.dist + pj[V + 1]) / vsig));
+                    smallest_dt = fmin(smallest_dt, courant * ((r.dist + ri) / vsig));
+                    smallest_dt = fmin(smallest_dt, courant * ((r.dist + pj[V + 1]) / vsig));
                 }
             }
             if constexpr (Grad) {
-                G wx[U];
-#pragma unroll
-                for (int p = 0; p < U; ++p) wx[p] = row.wx[p];
+                const Pair<G> c01 = geo.c01[slot];
+                G c[D];
+                c[0] = c01.x;
+                c[1] = c01.y;
+                if constexpr (D == 3) c[2] = geo.c2[slot];
 #pragma unroll
                 for (int v = 0; v < V; ++v) {
-                    const double dW = Wj[v] - Wi[v];
+                    const double dW = pj[v] - Wi[v];
+                    const G dWg = static_cast<G>(dW);
 #pragma unroll
-                    for (int p = 0; p < U; ++p) b[v][p] += wx[p] * static_cast<G>(dW);
+                    for (int a = 0; a < D; ++a) g[D * v + a] += c[a] * dWg;
                     if (!tiny_face) {
-                        const G value = exact ? static_cast<G>(Wj[v]) : static_cast<G>(dW);
+                        const G value = exact ? static_cast<G>(pj[v]) : dWg;
                         lo[v] = fmin(lo[v], value);
                         hi[v] = fmax(hi[v], value);
                     }
@@ -296,49 +325,15 @@ __global__ void __launch_bounds__(128) k_sweep_rows(MeshDev<D> m, GeometryDev<D,
             smallest_dt = fmin(smallest_dt, courant * (ri / (ci + sqrt(dot<D>(rel, rel)))));
         }
         if constexpr (Grad) {
-            // Sweep::solve with the stored factor: forward and back substitution per variable.
-            G L[U][U];
-            const G* fr = geo.factors + static_cast<int64_t>(factor_width<D>()) * i;
-            {
-                int c = 0;
-#pragma unroll
-                for (int p = 0; p < U; ++p)
-#pragma unroll
-                    for (int s = 0; s <= p; ++s) L[p][s] = fr[c++];
-            }
-            G g[V * D];
-#pragma unroll
-            for (int v = 0; v < V; ++v) {
-                G z[U], x[U];
-#pragma unroll
-                for (int p = 0; p < U; ++p) {
-                    G sum = b[v][p];
-#pragma unroll
-                    for (int q = 0; q < p; ++q) sum -= L[p][q] * z[q];
-                    z[p] = sum / L[p][p];
-                }
-#pragma unroll
-                for (int p = U - 1; p >= 0; --p) {
-                    G sum = z[p];
-#pragma unroll
-                    for (int q = p + 1; q < U; ++q) sum -= L[q][p] * x[q];
-                    x[p] = sum / L[p][p];
-                }
-#pragma unroll
-                for (int a = 0; a < D; ++a) g[D * v + a] = x[1 + a];
-            }
             if constexpr (Limit) {
-                for (int k = first; k < end; ++k) {
-                    const EntryRow<G>& row = geo.entries[k];
-                    bool tiny_face;
-                    if constexpr (exact)
-                        tiny_face = (row.bits >> 63) != 0;
-                    else
-                        tiny_face = (geo.face_tiny[k] >> 31) != 0;
-                    if (tiny_face) continue;
+                for (int k = 0; k < count; ++k) {
+                    const int64_t slot = slot0 + 32 * static_cast<int64_t>(k);
+                    if (geo.nbr[slot] & kTinyBit) continue;
+                    const Pair<G> o01 = geo.off01[slot];
                     G rg[D];
-#pragma unroll
-                    for (int a = 0; a < D; ++a) rg[a] = row.off[a];
+                    rg[0] = o01.x;
+                    rg[1] = o01.y;
+                    if constexpr (D == 3) rg[2] = geo.off2[slot];
 #pragma unroll
                     for (int v = 0; v < V; ++v) {
                         G* gv = g + D * v;
@@ -373,7 +368,7 @@ __global__ void __launch_bounds__(128) k_sweep_rows(MeshDev<D> m, GeometryDev<D,
         }
     }
     block_min_to(smallest_dt, &ctr->dt_bits);
-    if (i < m.n && !(smallest_dt == smallest_dt)) atomicOr(&ctr->error, 1ull);
+    if (t < m.n && !(smallest_dt == smallest_dt)) atomicOr(&ctr->error, 1ull);
 }
 
 // The static flux pass over the face rows (FaceFlux::operator(), finite_volume.hpp:1415-1434): one streamed row per
@@ -385,7 +380,12 @@ __global__ void __launch_bounds__(128) k_flux_rows(MeshDev<D> m, GeometryDev<D, 
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     int count = 0;
     if (f < m.f) {
-        const FaceRow<G> r = geo.faces[f];
+        FaceRow<G> r;
+        {  // the 32-B aligned row in vector loads
+            double* words = reinterpret_cast<double*>(&r);
+#pragma unroll
+            for (int c = 0; c < static_cast<int>(sizeof(FaceRow<G>) / 8); c += 4) ldg256(reinterpret_cast<const double*>(geo.faces + f) + c, words + c);
+        }
         double F[V];
         if (r.mag == 0) {
 #pragma unroll

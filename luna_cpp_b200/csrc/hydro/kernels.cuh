@@ -63,6 +63,35 @@ struct MeshDev {
 
 __device__ __forceinline__ int list_face(int32_t e) { return e >= 0 ? e : ~e; }
 
+// One 256-bit read-only load (sm_100: a whole 32-B sector per lane, one request instead of four scalar ones).
+// p must be 32-B aligned and unwritten during the kernel.
+__device__ __forceinline__ void ldg256(const double* p, double* out) {
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(out[0]), "=d"(out[1]), "=d"(out[2]), "=d"(out[3]) : "l"(p));
+}
+__device__ __forceinline__ void ldg256(const float* p, float* out) {
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(out[0]), "=f"(out[1]), "=f"(out[2]), "=f"(out[3]), "=f"(out[4]), "=f"(out[5]), "=f"(out[6]), "=f"(out[7])
+        : "l"(p));
+}
+
+// A TMA bulk prefetch of [p, p + bytes) into L2 (p 16-B aligned, bytes a multiple of 16): one instruction per range,
+// no registers or shared memory held while the data is in flight.
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned int bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// A cell's primitive row (W, c, r, pad: 64 B, 64-B aligned) in two vector loads (3D), one (2D: W only).
+template <int D>
+__device__ __forceinline__ void load_prim_row(const double* prims, int i, double* row) {
+    const double* p = prims + 8 * static_cast<int64_t>(i);
+    ldg256(p, row);
+    if constexpr (D == 3) {
+        ldg256(p + 4, row + 4);
+    } else {
+        ldg256(p + 4, row + 4);
+    }
+}
+
 // Counters a step's kernels write; read back with dt (one copy).
 struct Counters {
     unsigned long long dt_bits;       // min over the time-step terms, as the bits of a positive double
@@ -187,17 +216,25 @@ struct FluxArgs {
 };
 
 // FaceFlux::side at order 1 (finite_volume.hpp:1306-1329): W + g . r - dt/2 A(W) g, or W if rho or P fall to <= 0.
+// A cell's gradient row (GS values of G, 32-B aligned) in vector loads.
+template <int D, class G>
+__device__ __forceinline__ void load_grad_row(const G* grad, int i, G* row) {
+    constexpr int GS = grad_stride<D>(), per = 32 / sizeof(G);
+    const G* p = grad + static_cast<int64_t>(GS) * i;
+#pragma unroll
+    for (int c = 0; c < GS; c += per) ldg256(p + c, row + c);
+}
+
 template <int D, class G>
 __device__ __forceinline__ void face_side(const FluxArgs<D, G>& x, int i, const double* r, double dt, double* Wf, int& fallbacks) {
     constexpr int V = D + 2, GS = grad_stride<D>();
-    const double* p = x.prims + PS * i;
-    const G* gr = x.grad + static_cast<int64_t>(GS) * i;
+    double prow[8];
+    load_prim_row<D>(x.prims, i, prow);
     double W[V];
 #pragma unroll
-    for (int v = 0; v < V; ++v) W[v] = p[v];
-    G g[V * D];
-#pragma unroll
-    for (int c = 0; c < V * D; ++c) g[c] = gr[c];
+    for (int v = 0; v < V; ++v) W[v] = prow[v];
+    G g[GS];
+    load_grad_row<D, G>(x.grad, i, g);
     if constexpr (sizeof(G) == sizeof(double)) {
         double A[V];
         half_step_rate<D, double>(W, g, x.gas.gamma, A);
@@ -226,14 +263,13 @@ __device__ __forceinline__ void face_side(const FluxArgs<D, G>& x, int i, const 
 template <int D, class G>
 __device__ __forceinline__ void pass1_side(const FluxArgs<D, G>& x, int i, const double* r, double* Wf, int& fallbacks) {
     constexpr int V = D + 2, GS = grad_stride<D>();
-    const double* p = x.prims + PS * i;
-    const G* gr = x.grad + static_cast<int64_t>(GS) * i;
+    double prow[8];
+    load_prim_row<D>(x.prims, i, prow);
     double W[V];
 #pragma unroll
-    for (int v = 0; v < V; ++v) W[v] = p[v];
-    G g[V * D];
-#pragma unroll
-    for (int c = 0; c < V * D; ++c) g[c] = gr[c];
+    for (int v = 0; v < V; ++v) W[v] = prow[v];
+    G g[GS];
+    load_grad_row<D, G>(x.grad, i, g);
     if constexpr (sizeof(G) == sizeof(double)) {
 #pragma unroll
         for (int v = 0; v < V; ++v) Wf[v] = W[v] + dot<D>(g + D * v, r);

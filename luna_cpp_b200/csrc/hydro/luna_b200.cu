@@ -12,6 +12,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <algorithm>
 #include <utility>
 #include <vector>
 
@@ -101,8 +102,9 @@ struct luna_fv {
     DevArray<int32_t> steps;
     DevArray<luna::Counters> counters;
     // the mesh reordered for the step (geometry.cuh), rebuilt by every load_mesh
-    DevArray<unsigned char> geo_entries, geo_factors, geo_dt, geo_faces;
-    DevArray<unsigned int> geo_face_tiny;
+    DevArray<unsigned char> geo_c01, geo_c2, geo_off01, geo_off2, geo_dt, geo_faces;
+    DevArray<unsigned int> geo_nbr, geo_face;
+    DevArray<int32_t> geo_slice_base, geo_order;
     DevArray<double> geo_angle;
     // adjoint (allocated by the first luna_fv_step_adjoint)
     DevArray<double> adj_fit, adj_face_bar, adj_wbar, adj_bbar, adj_boundbar, adj_qbar;
@@ -153,9 +155,14 @@ struct luna_fv {
     template <int D, class G>
     luna::GeometryDev<D, G> geometry_dev() const {
         luna::GeometryDev<D, G> g;
-        g.entries = reinterpret_cast<luna::EntryRow<G>*>(geo_entries.ptr);
-        g.face_tiny = geo_face_tiny.ptr;
-        g.factors = reinterpret_cast<G*>(geo_factors.ptr);
+        g.order = geo_order.ptr;
+        g.slice_base = geo_slice_base.ptr;
+        g.nbr = geo_nbr.ptr;
+        g.face = geo_face.ptr;
+        g.c01 = reinterpret_cast<luna::Pair<G>*>(geo_c01.ptr);
+        g.c2 = reinterpret_cast<G*>(geo_c2.ptr);
+        g.off01 = reinterpret_cast<luna::Pair<G>*>(geo_off01.ptr);
+        g.off2 = reinterpret_cast<G*>(geo_off2.ptr);
         g.dt_rows = reinterpret_cast<luna::DtRow*>(geo_dt.ptr);
         g.faces = reinterpret_cast<luna::FaceRow<G>*>(geo_faces.ptr);
         g.max_angle = geo_angle.ptr;
@@ -225,16 +232,41 @@ luna_status validate_mesh(const luna_mesh_desc* m, int dim, int64_t n) {
 
 // The reordered rows of the current mesh (geometry.cuh::k_geometry), in the policy's gradient type.
 template <int D, class G>
-luna_status build_geometry(luna_fv* fv) {
+luna_status build_geometry(luna_fv* fv, const std::vector<int32_t>& start) {
     const size_t N = static_cast<size_t>(fv->n), F = static_cast<size_t>(fv->f);
-    LUNA_TRY(fv->geo_entries.alloc(sizeof(luna::EntryRow<G>) * (2 * F > 0 ? 2 * F : 1), "entry rows"));
-    if (sizeof(G) != sizeof(double)) LUNA_TRY(fv->geo_face_tiny.alloc(2 * F > 0 ? 2 * F : 1, "entry face words"));
-    LUNA_TRY(fv->geo_factors.alloc(sizeof(G) * luna::factor_width<D>() * N, "fit factors"));
+    // The sweep order: cells by list length (longest first) within windows of kOrderWindow cells; then the slices of
+    // 32 threads, each as many slots as its longest list.
+    std::vector<int32_t> order(N);
+    for (size_t i = 0; i < N; ++i) order[i] = static_cast<int32_t>(i);
+    for (size_t w0 = 0; w0 < N; w0 += luna::kOrderWindow) {
+        const size_t w1 = std::min(N, w0 + static_cast<size_t>(luna::kOrderWindow));
+        std::stable_sort(order.begin() + w0, order.begin() + w1, [&](int32_t a, int32_t b) {
+            return start[a + 1] - start[a] > start[b + 1] - start[b];
+        });
+    }
+    const size_t S = (N + 31) / 32;
+    std::vector<int32_t> base(S + 1, 0);
+    for (size_t s = 0; s < S; ++s) {
+        int longest = 0;
+        for (size_t t = 32 * s; t < 32 * s + 32 && t < N; ++t) longest = std::max(longest, start[order[t] + 1] - start[order[t]]);
+        base[s + 1] = base[s] + longest;
+    }
+    const size_t slots = static_cast<size_t>(base[S]) * 32 > 0 ? static_cast<size_t>(base[S]) * 32 : 1;
+    LUNA_TRY(upload(fv->geo_order, order.data(), N, false, fv->stream, "sweep order"));
+    LUNA_TRY(upload(fv->geo_slice_base, base.data(), S + 1, false, fv->stream, "slice bases"));
+    LUNA_TRY(fv->geo_nbr.alloc(slots, "entry neighbours"));
+    LUNA_TRY(fv->geo_face.alloc(slots, "entry faces"));
+    LUNA_TRY(fv->geo_c01.alloc(sizeof(luna::Pair<G>) * slots, "entry gradient rows"));
+    LUNA_TRY(fv->geo_c2.alloc(sizeof(G) * slots, "entry gradient rows"));
+    LUNA_TRY(fv->geo_off01.alloc(sizeof(luna::Pair<G>) * slots, "entry offsets"));
+    LUNA_TRY(fv->geo_off2.alloc(sizeof(G) * slots, "entry offsets"));
     LUNA_TRY(fv->geo_dt.alloc(sizeof(luna::DtRow) * (F > 0 ? F : 1), "dt rows"));
     LUNA_TRY(fv->geo_faces.alloc(sizeof(luna::FaceRow<G>) * (F > 0 ? F : 1), "face rows"));
     LUNA_TRY(fv->geo_angle.alloc(N, "face angles"));
     luna::k_geometry<D, G><<<blocks(N, 128), 128, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->geometry_dev<D, G>());
     LUNA_CUDA(cudaGetLastError());
+    // The slice bases' host copy must outlive the asynchronous upload.
+    LUNA_CUDA(cudaStreamSynchronize(fv->stream));
     return LUNA_OK;
 }
 
@@ -264,8 +296,13 @@ luna_status load_mesh(luna_fv* fv, const luna_mesh_desc* m) {
     }
     if (fv->update == LUNA_UPDATE_PER_FACE) LUNA_TRY(fv->flux.alloc(F * (D + 2) > 0 ? F * (D + 2) : 1, "flux rows"));
     // Lists in device memory are trusted as voronoi-cpp's; the sweep does not re-check them.
-    return fv->precision == LUNA_FP64 ? (D == 3 ? build_geometry<3, double>(fv) : build_geometry<2, double>(fv))
-                                      : (D == 3 ? build_geometry<3, float>(fv) : build_geometry<2, float>(fv));
+    std::vector<int32_t> start(N + 1);
+    if (dev)
+        LUNA_CUDA(cudaMemcpy(start.data(), m->cell_face_start, (N + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    else
+        std::copy(m->cell_face_start, m->cell_face_start + N + 1, start.begin());
+    return fv->precision == LUNA_FP64 ? (D == 3 ? build_geometry<3, double>(fv, start) : build_geometry<2, double>(fv, start))
+                                      : (D == 3 ? build_geometry<3, float>(fv, start) : build_geometry<2, float>(fv, start));
 }
 
 template <int D>
@@ -862,7 +899,8 @@ LUNA_API luna_status luna_fv_device_bytes(luna_fv* fv, int64_t* out) {
     b += fv->w.bytes() + fv->x.bytes() + fv->old_cen.bytes() + fv->steps.bytes() + fv->counters.bytes();
     b += fv->adj_fit.bytes() + fv->adj_face_bar.bytes() + fv->adj_wbar.bytes() + fv->adj_bbar.bytes() + fv->adj_boundbar.bytes();
     b += fv->adj_qbar.bytes() + fv->adj_flags.bytes() + fv->adj_bound_face.bytes();
-    b += fv->geo_entries.bytes() + fv->geo_factors.bytes() + fv->geo_dt.bytes() + fv->geo_faces.bytes() + fv->geo_face_tiny.bytes();
+    b += fv->geo_c01.bytes() + fv->geo_c2.bytes() + fv->geo_off01.bytes() + fv->geo_off2.bytes() + fv->geo_nbr.bytes();
+    b += fv->geo_face.bytes() + fv->geo_slice_base.bytes() + fv->geo_order.bytes() + fv->geo_dt.bytes() + fv->geo_faces.bytes();
     b += fv->geo_angle.bytes();
     *out = static_cast<int64_t>(b);
     return LUNA_OK;
