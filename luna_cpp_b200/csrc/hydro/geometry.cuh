@@ -238,62 +238,84 @@ __global__ void __launch_bounds__(128) k_sweep_rows(MeshDev<D> m, GeometryDev<D,
         // entry rows into L2 kPrefetch entries ahead with bulk prefetches, one per array and entry.
         constexpr int kPrefetch = 4;
         const bool leader = (threadIdx.x & 31) == 0;
+        const unsigned long long once = l2_evict_first();
         auto prefetch_rows = [&](int k) {
             const int64_t r = row0 + 32 * static_cast<int64_t>(k);
-            prefetch_l2(geo.nbr + r, 32 * sizeof(unsigned int));
-            prefetch_l2(geo.face + r, 32 * sizeof(unsigned int));
+            prefetch_l2_hint(geo.nbr + r, 32 * sizeof(unsigned int), once);
+            prefetch_l2_hint(geo.face + r, 32 * sizeof(unsigned int), once);
             if constexpr (Grad) {
-                prefetch_l2(geo.c01 + r, 32 * sizeof(Pair<G>));
-                if constexpr (D == 3) prefetch_l2(geo.c2 + r, 32 * sizeof(G));
+                prefetch_l2_hint(geo.c01 + r, 32 * sizeof(Pair<G>), once);
+                if constexpr (D == 3) prefetch_l2_hint(geo.c2 + r, 32 * sizeof(G), once);
                 if constexpr (Limit) {
-                    prefetch_l2(geo.off01 + r, 32 * sizeof(Pair<G>));
-                    if constexpr (D == 3) prefetch_l2(geo.off2 + r, 32 * sizeof(G));
+                    prefetch_l2_hint(geo.off01 + r, 32 * sizeof(Pair<G>), once);
+                    if constexpr (D == 3) prefetch_l2_hint(geo.off2 + r, 32 * sizeof(G), once);
                 }
             }
         };
         if (leader)
             for (int k = 0; k < kPrefetch && k < count; ++k) prefetch_rows(k);
-        // The neighbour word one entry ahead: entry k's row gather issues as soon as its iteration starts.
-        unsigned int next = count > 0 ? geo.nbr[slot0] : 0u;
-        for (int k = 0; k < count; ++k) {
-            const int64_t slot = slot0 + 32 * static_cast<int64_t>(k);
-            if (leader && k + kPrefetch < count) prefetch_rows(k + kPrefetch);
-            const unsigned int word = next;
-            if (k + 1 < count) next = geo.nbr[slot + 32];
-            const int j = static_cast<int>(word & kIndexMask);
-            const bool owned = (word & kOwnedBit) != 0, tiny_face = (word & kTinyBit) != 0;
-            double pj[8];
-            load_prim_row<D>(prims, j, pj);
-            if (owned) {  // FaceStep (finite_volume.hpp:1074-1090)
-                const DtRow r = geo.dt_rows[geo.face[slot]];
-                double dv[D], d[D];
+        // kBatch entries at a time: all their loads are issued before any is used, so each thread keeps several
+        // gathers in flight (the entries of a list are independent; only the sums carry over, in list order).
+        constexpr int kBatch = 2;
+        for (int k0 = 0; k0 < count; k0 += kBatch) {
+            if (leader)
 #pragma unroll
-                for (int a = 0; a < D; ++a) {
-                    dv[a] = pj[1 + a] - Wi[1 + a];
-                    d[a] = r.d[a];
-                }
-                const double vsig = ci + pj[V] - dot<D>(dv, d) / r.dist;
-                if (vsig > 0) {
-                    smallest_dt = fmin(smallest_dt, courant * ((r.dist + ri) / vsig));
-                    smallest_dt = fmin(smallest_dt, courant * ((r.dist + pj[V + 1]) / vsig));
+                for (int b = 0; b < kBatch; ++b)
+                    if (k0 + b + kPrefetch < count) prefetch_rows(k0 + b + kPrefetch);
+            unsigned int word[kBatch], fword[kBatch];
+#pragma unroll
+            for (int b = 0; b < kBatch; ++b) {
+                const int64_t slot = slot0 + 32 * static_cast<int64_t>(k0 + b);
+                const bool valid = k0 + b < count;
+                word[b] = valid ? ldg_hint(geo.nbr + slot, once) : 0u;
+                fword[b] = valid && (word[b] & kOwnedBit) ? ldg_hint(geo.face + slot, once) : 0u;
+            }
+            double pj[kBatch][8], dtr[kBatch][4];
+            G c[kBatch][D];
+#pragma unroll
+            for (int b = 0; b < kBatch; ++b) {
+                const int64_t slot = slot0 + 32 * static_cast<int64_t>(k0 + b);
+                if (k0 + b < count) {
+                    load_prim_row<D>(prims, static_cast<int>(word[b] & kIndexMask), pj[b]);
+                    if (word[b] & kOwnedBit) ldg256_hint(reinterpret_cast<const double*>(geo.dt_rows + fword[b]), dtr[b], once);
+                    if constexpr (Grad) {
+                        const Pair<G> c01 = ldg_hint(geo.c01 + slot, once);
+                        c[b][0] = c01.x;
+                        c[b][1] = c01.y;
+                        if constexpr (D == 3) c[b][2] = ldg_hint(geo.c2 + slot, once);
+                    }
                 }
             }
-            if constexpr (Grad) {
-                const Pair<G> c01 = geo.c01[slot];
-                G c[D];
-                c[0] = c01.x;
-                c[1] = c01.y;
-                if constexpr (D == 3) c[2] = geo.c2[slot];
 #pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    const double dW = pj[v] - Wi[v];
-                    const G dWg = static_cast<G>(dW);
+            for (int b = 0; b < kBatch; ++b) {
+                if (k0 + b >= count) break;
+                const bool owned = (word[b] & kOwnedBit) != 0, tiny_face = (word[b] & kTinyBit) != 0;
+                if (owned) {  // FaceStep (finite_volume.hpp:1074-1090)
+                    double dv[D], d[D];
 #pragma unroll
-                    for (int a = 0; a < D; ++a) g[D * v + a] += c[a] * dWg;
-                    if (!tiny_face) {
-                        const G value = exact ? static_cast<G>(pj[v]) : dWg;
-                        lo[v] = fmin(lo[v], value);
-                        hi[v] = fmax(hi[v], value);
+                    for (int a = 0; a < D; ++a) {
+                        dv[a] = pj[b][1 + a] - Wi[1 + a];
+                        d[a] = dtr[b][a];
+                    }
+                    const double dist = dtr[b][3];
+                    const double vsig = ci + pj[b][V] - dot<D>(dv, d) / dist;
+                    if (vsig > 0) {
+                        // Both cells' terms (dist + r) / vsig: the smaller radius gives the smaller one, the same rounding.
+                        smallest_dt = fmin(smallest_dt, courant * ((dist + fmin(ri, pj[b][V + 1])) / vsig));
+                    }
+                }
+                if constexpr (Grad) {
+#pragma unroll
+                    for (int v = 0; v < V; ++v) {
+                        const double dW = pj[b][v] - Wi[v];
+                        const G dWg = static_cast<G>(dW);
+#pragma unroll
+                        for (int a = 0; a < D; ++a) g[D * v + a] += c[b][a] * dWg;
+                        if (!tiny_face) {
+                            const G value = exact ? static_cast<G>(pj[b][v]) : dWg;
+                            lo[v] = fmin(lo[v], value);
+                            hi[v] = fmax(hi[v], value);
+                        }
                     }
                 }
             }
@@ -326,37 +348,49 @@ __global__ void __launch_bounds__(128) k_sweep_rows(MeshDev<D> m, GeometryDev<D,
         }
         if constexpr (Grad) {
             if constexpr (Limit) {
-                for (int k = 0; k < count; ++k) {
-                    const int64_t slot = slot0 + 32 * static_cast<int64_t>(k);
-                    if (geo.nbr[slot] & kTinyBit) continue;
-                    const Pair<G> o01 = geo.off01[slot];
-                    G rg[D];
-                    rg[0] = o01.x;
-                    rg[1] = o01.y;
-                    if constexpr (D == 3) rg[2] = geo.off2[slot];
+                constexpr int kClipBatch = 4;
+                for (int k0 = 0; k0 < count; k0 += kClipBatch) {
+                    unsigned int word[kClipBatch];
+                    G rg[kClipBatch][D];
 #pragma unroll
-                    for (int v = 0; v < V; ++v) {
-                        G* gv = g + D * v;
-                        const G dp = dot<D>(gv, rg);
-                        if constexpr (exact) {
-                            if (dp > 0 && Wi[v] + dp > hi[v]) {
-                                const G s = hi[v] > Wi[v] ? (hi[v] - Wi[v]) / dp : G(0);
+                    for (int b = 0; b < kClipBatch; ++b) {
+                        const int64_t slot = slot0 + 32 * static_cast<int64_t>(k0 + b);
+                        if (k0 + b < count) {
+                            word[b] = ldg_hint(geo.nbr + slot, once);
+                            const Pair<G> o01 = ldg_hint(geo.off01 + slot, once);
+                            rg[b][0] = o01.x;
+                            rg[b][1] = o01.y;
+                            if constexpr (D == 3) rg[b][2] = ldg_hint(geo.off2 + slot, once);
+                        }
+                    }
 #pragma unroll
-                                for (int a = 0; a < D; ++a) gv[a] = gv[a] * s;
-                            } else if (dp < 0 && Wi[v] + dp < lo[v]) {
-                                const G s = lo[v] < Wi[v] ? (lo[v] - Wi[v]) / dp : G(0);
+                    for (int b = 0; b < kClipBatch; ++b) {
+                        if (k0 + b >= count) break;
+                        if (word[b] & kTinyBit) continue;
 #pragma unroll
-                                for (int a = 0; a < D; ++a) gv[a] = gv[a] * s;
-                            }
-                        } else {
-                            if (dp > 0 && dp > hi[v]) {
-                                const G s = hi[v] > 0 ? hi[v] / dp : G(0);
+                        for (int v = 0; v < V; ++v) {
+                            G* gv = g + D * v;
+                            const G dp = dot<D>(gv, rg[b]);
+                            if constexpr (exact) {
+                                if (dp > 0 && Wi[v] + dp > hi[v]) {
+                                    const G s = hi[v] > Wi[v] ? (hi[v] - Wi[v]) / dp : G(0);
 #pragma unroll
-                                for (int a = 0; a < D; ++a) gv[a] = gv[a] * s;
-                            } else if (dp < 0 && dp < lo[v]) {
-                                const G s = lo[v] < 0 ? lo[v] / dp : G(0);
+                                    for (int a = 0; a < D; ++a) gv[a] = gv[a] * s;
+                                } else if (dp < 0 && Wi[v] + dp < lo[v]) {
+                                    const G s = lo[v] < Wi[v] ? (lo[v] - Wi[v]) / dp : G(0);
 #pragma unroll
-                                for (int a = 0; a < D; ++a) gv[a] = gv[a] * s;
+                                    for (int a = 0; a < D; ++a) gv[a] = gv[a] * s;
+                                }
+                            } else {
+                                if (dp > 0 && dp > hi[v]) {
+                                    const G s = hi[v] > 0 ? hi[v] / dp : G(0);
+#pragma unroll
+                                    for (int a = 0; a < D; ++a) gv[a] = gv[a] * s;
+                                } else if (dp < 0 && dp < lo[v]) {
+                                    const G s = lo[v] < 0 ? lo[v] / dp : G(0);
+#pragma unroll
+                                    for (int a = 0; a < D; ++a) gv[a] = gv[a] * s;
+                                }
                             }
                         }
                     }
@@ -381,10 +415,12 @@ __global__ void __launch_bounds__(128) k_flux_rows(MeshDev<D> m, GeometryDev<D, 
     int count = 0;
     if (f < m.f) {
         FaceRow<G> r;
-        {  // the 32-B aligned row in vector loads
+        {  // the 32-B aligned row in vector loads, streamed once per step
             double* words = reinterpret_cast<double*>(&r);
+            const unsigned long long once = l2_evict_first();
 #pragma unroll
-            for (int c = 0; c < static_cast<int>(sizeof(FaceRow<G>) / 8); c += 4) ldg256(reinterpret_cast<const double*>(geo.faces + f) + c, words + c);
+            for (int c = 0; c < static_cast<int>(sizeof(FaceRow<G>) / 8); c += 4)
+                ldg256_hint(reinterpret_cast<const double*>(geo.faces + f) + c, words + c, once);
         }
         double F[V];
         if (r.mag == 0) {

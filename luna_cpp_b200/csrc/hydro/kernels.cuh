@@ -74,6 +74,52 @@ __device__ __forceinline__ void ldg256(const float* p, float* out) {
         : "l"(p));
 }
 
+// L2 eviction priority for rows streamed once per step (the rows gathered by every neighbour keep the default).
+__device__ __forceinline__ unsigned long long l2_evict_first() {
+    unsigned long long p;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+// Read-only loads with an L2 policy.
+__device__ __forceinline__ unsigned int ldg_hint(const unsigned int* p, unsigned long long pol) {
+    unsigned int v;
+    asm("ld.global.nc.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ double ldg_hint(const double* p, unsigned long long pol) {
+    double v;
+    asm("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ float ldg_hint(const float* p, unsigned long long pol) {
+    float v;
+    asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ double2 ldg_hint(const double2* p, unsigned long long pol) {
+    double2 v;
+    asm("ld.global.nc.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ float2 ldg_hint(const float2* p, unsigned long long pol) {
+    float2 v;
+    asm("ld.global.nc.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;" : "=f"(v.x), "=f"(v.y) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ void ldg256_hint(const double* p, double* out, unsigned long long pol) {
+    asm("ld.global.nc.L2::cache_hint.v4.f64 {%0, %1, %2, %3}, [%4], %5;"
+        : "=d"(out[0]), "=d"(out[1]), "=d"(out[2]), "=d"(out[3])
+        : "l"(p), "l"(pol));
+}
+__device__ __forceinline__ void ldg256_hint(const float* p, float* out, unsigned long long pol) {
+    asm("ld.global.nc.L2::cache_hint.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8], %9;"
+        : "=f"(out[0]), "=f"(out[1]), "=f"(out[2]), "=f"(out[3]), "=f"(out[4]), "=f"(out[5]), "=f"(out[6]), "=f"(out[7])
+        : "l"(p), "l"(pol));
+}
+__device__ __forceinline__ void prefetch_l2_hint(const void* p, unsigned int bytes, unsigned long long pol) {
+    asm volatile("cp.async.bulk.prefetch.L2.global.L2::cache_hint [%0], %1, %2;" ::"l"(p), "r"(bytes), "l"(pol) : "memory");
+}
+
 // A TMA bulk prefetch of [p, p + bytes) into L2 (p 16-B aligned, bytes a multiple of 16): one instruction per range,
 // no registers or shared memory held while the data is in flight.
 __device__ __forceinline__ void prefetch_l2(const void* p, unsigned int bytes) {
@@ -85,11 +131,7 @@ template <int D>
 __device__ __forceinline__ void load_prim_row(const double* prims, int i, double* row) {
     const double* p = prims + 8 * static_cast<int64_t>(i);
     ldg256(p, row);
-    if constexpr (D == 3) {
-        ldg256(p + 4, row + 4);
-    } else {
-        ldg256(p + 4, row + 4);
-    }
+    ldg256(p + 4, row + 4);
 }
 
 // Counters a step's kernels write; read back with dt (one copy).
