@@ -135,6 +135,30 @@ typedef struct {
 LUNA_API luna_status luna_fv_set_timing(luna_fv* fv, int on);
 LUNA_API luna_status luna_fv_timings(luna_fv* fv, luna_timings* out, int reset);
 
+/* The learned slope limiter (no counterpart in the reference; the plain face-centroid limiter, Sweep's walk 2,
+ * finite_volume.hpp:538-565, is its fallback and its judge). In the sweep each variable's admissible factor alpha (the
+ * largest scaling of the unlimited gradient that keeps every face-centroid value within the neighbours' range, capped
+ * at 2) and 32 features are computed; a 3-layer MLP (width 64, BF16 tensor-core MMA, FP32 accumulation) maps the
+ * features to logits o; the gradient is scaled by alpha * sigmoid(o) in [0, alpha]: monotone by construction.
+ * mode 0: the plain limiter; mode 1: the network with parameters `params` (device, luna_mlp_param_count() floats, kept
+ * by the caller); mode 2: the factors min(alpha, 1), the plain limiter in min-factor form through the same path.
+ * Order 1, the FP64 policy, the face-centroid limiter. */
+LUNA_API luna_status luna_fv_set_limiter_mlp(luna_fv* fv, const float* params, int mode);
+/* The limiter's inputs for the current state (device buffers): features [N][32] BF16, alpha [N][D + 2] (double, in rows
+ * of 5), and the unlimited gradients [N][D + 2][D] (double). For building training data. */
+LUNA_API luna_status luna_fv_limiter_inputs(luna_fv* fv, void* features, double* alpha, double* gradients);
+/* The network's kernels on caller buffers (device): parameters FP32 [luna_mlp_param_count()]; features BF16 [n][32];
+ * logits FP32 [n][16] (the first D + 2 used). train_step: the gradient of scale * sum w (sigmoid(o) - t)^2 over rows
+ * (targets t and weights w FP32 [n][5]) into grad, the loss into *loss (device); workspace of
+ * luna_mlp_train_workspace_floats(n) floats; deterministic. adam: one Adam update (step counts from 1). */
+LUNA_API int64_t luna_mlp_param_count(void);
+LUNA_API int64_t luna_mlp_train_workspace_floats(int64_t n);
+LUNA_API luna_status luna_mlp_forward(const float* params, const void* features, int64_t n, float* logits, void* stream);
+LUNA_API luna_status luna_mlp_train_step(const float* params, const void* features, const float* target, const float* weight, int64_t n,
+                                         float scale, float* grad, float* loss, float* workspace, int64_t workspace_floats, void* stream);
+LUNA_API luna_status luna_mlp_adam(float* params, const float* grad, float* m, float* v, float lr, float beta1, float beta2, float eps,
+                                   int step, void* stream);
+
 /* The flux-and-update pass of one static step (apply(), per-face loop) that allocates nothing, for callers that cannot
  * allocate device memory themselves: code that must run with a fixed device footprint, or under a runtime or memory
  * pool that owns every device allocation and hands the caller only finished buffers. It has no counterpart in the

@@ -16,6 +16,8 @@
 // Cells are swept in an order grouping lists of one length (see kOrderWindow).
 #pragma once
 
+#include <cuda_bf16.h>
+
 #include <type_traits>
 
 #include "kernels.cuh"
@@ -207,10 +209,29 @@ __global__ void __launch_bounds__(128) k_geometry(MeshDev<D> m, GeometryDev<D, G
 // gradient g_v = sum_k c_k (W_jv - W_iv) in list order, the neighbours' range (tiny faces left out) and the owned faces'
 // CFL terms; walk 2 clips at each face offset in list order. Per entry: streamed coalesced rows and one gathered
 // primitive row (two 256-bit loads).
-template <int D, bool Moving, bool Grad, class G, bool Limit>
+// The learned limiter's 32 features of a cell (FP64 policy: lo/hi are the neighbours' values): per variable v,
+//   alpha_v / 2                        the admissible factor (how far the slope may steepen or must flatten),
+//   (W_v - lo_v) / (hi_v - lo_v) - 1/2 where the cell sits in its neighbours' range,
+//   tanh(|g_v| r / (hi_v - lo_v))      the unlimited slope across the cell relative to the range (smoothness),
+//   tanh((hi_v - lo_v) / scale_v)      the size of the range relative to the values (a jump or a smooth region);
+// then tanh(log(hi_P / lo_P)) (a pressure jump), tanh(|v| / c), min_v min(alpha_v, 1) (the plain limiter's strongest
+// clip), 1, and zeros.
+template <int D, class G>
+__device__ __forceinline__ void write_learned_inputs(const struct LearnedInputs& out, int i, const double* Wi, double c, double r, const G* g,
+                                                     const G* lo, const G* hi, const double* alpha);
+
+// The learned limiter's inputs, written by the sweep in its learned mode (see write_learned_inputs).
+struct LearnedInputs {
+    __nv_bfloat16* features;  // [N][32]
+    double* alpha;            // [N][5]: the admissible slope factor per variable
+};
+constexpr double kAlphaCap = 2.0;  // the largest steepening the learned limiter may choose
+
+// Limit: 0 none, 1 the plain face-centroid limiter, 2 the learned limiter's inputs (the gradient left unlimited).
+template <int D, bool Moving, bool Grad, class G, int Limit>
 __global__ void __launch_bounds__(128) k_sweep_rows(MeshDev<D> m, GeometryDev<D, G> geo, const double* __restrict__ prims,
                                                     G* __restrict__ grad_out, double* __restrict__ w_out, double courant,
-                                                    Counters* __restrict__ ctr) {
+                                                    Counters* __restrict__ ctr, LearnedInputs learned) {
     constexpr int V = D + 2, GS = grad_stride<D>();
     constexpr bool exact = sizeof(G) == sizeof(double);
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -246,7 +267,7 @@ __global__ void __launch_bounds__(128) k_sweep_rows(MeshDev<D> m, GeometryDev<D,
             if constexpr (Grad) {
                 prefetch_l2_hint(geo.c01 + r, 32 * sizeof(Pair<G>), once);
                 if constexpr (D == 3) prefetch_l2_hint(geo.c2 + r, 32 * sizeof(G), once);
-                if constexpr (Limit) {
+                if constexpr (Limit != 0) {
                     prefetch_l2_hint(geo.off01 + r, 32 * sizeof(Pair<G>), once);
                     if constexpr (D == 3) prefetch_l2_hint(geo.off2 + r, 32 * sizeof(G), once);
                 }
@@ -347,7 +368,35 @@ __global__ void __launch_bounds__(128) k_sweep_rows(MeshDev<D> m, GeometryDev<D,
             smallest_dt = fmin(smallest_dt, courant * (ri / (ci + sqrt(dot<D>(rel, rel)))));
         }
         if constexpr (Grad) {
-            if constexpr (Limit) {
+            if constexpr (Limit == 2) {
+                // The admissible factor per variable: the smallest over the faces (tiny ones left out) of the factor that
+                // puts the face value on its bound, the min-factor form of the limiter (finite_volume.hpp:1008-1034),
+                // here not capped at 1.
+                double alpha[V];
+#pragma unroll
+                for (int v = 0; v < V; ++v) alpha[v] = kAlphaCap;
+                for (int k = 0; k < count; ++k) {
+                    const int64_t slot = slot0 + 32 * static_cast<int64_t>(k);
+                    if (ldg_hint(geo.nbr + slot, once) & kTinyBit) continue;
+                    const Pair<G> o01 = ldg_hint(geo.off01 + slot, once);
+                    G rg[D];
+                    rg[0] = o01.x;
+                    rg[1] = o01.y;
+                    if constexpr (D == 3) rg[2] = ldg_hint(geo.off2 + slot, once);
+#pragma unroll
+                    for (int v = 0; v < V; ++v) {
+                        const double dp = static_cast<double>(dot<D>(g + D * v, rg));
+                        double factor = kAlphaCap;
+                        if (dp > 0)
+                            factor = hi[v] > Wi[v] ? (hi[v] - Wi[v]) / dp : 0.0;
+                        else if (dp < 0)
+                            factor = lo[v] < Wi[v] ? (lo[v] - Wi[v]) / dp : 0.0;
+                        alpha[v] = fmin(alpha[v], factor);
+                    }
+                }
+                write_learned_inputs<D>(learned, i, Wi, pi[V], pi[V + 1], g, lo, hi, alpha);
+            }
+            if constexpr (Limit == 1) {
                 constexpr int kClipBatch = 4;
                 for (int k0 = 0; k0 < count; k0 += kClipBatch) {
                     unsigned int word[kClipBatch];
@@ -403,6 +452,68 @@ __global__ void __launch_bounds__(128) k_sweep_rows(MeshDev<D> m, GeometryDev<D,
     }
     block_min_to(smallest_dt, &ctr->dt_bits);
     if (t < m.n && !(smallest_dt == smallest_dt)) atomicOr(&ctr->error, 1ull);
+}
+
+template <int D, class G>
+__device__ __forceinline__ void write_learned_inputs(const LearnedInputs& out, int i, const double* Wi, double c, double r, const G* g,
+                                                     const G* lo, const G* hi, const double* alpha) {
+    constexpr int V = D + 2;
+    float f[32];
+#pragma unroll
+    for (int k = 0; k < 32; ++k) f[k] = 0.0f;
+    double plain = 1.0;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        if (v >= V) break;
+        const double range = static_cast<double>(hi[v]) - static_cast<double>(lo[v]);
+        const double scale = fabs(Wi[v]) + fabs(static_cast<double>(hi[v])) + fabs(static_cast<double>(lo[v])) + 1e-300;
+        const double safe = range > 1e-12 * scale ? range : 1e-12 * scale;
+        double gn = 0;
+#pragma unroll
+        for (int a = 0; a < D; ++a) gn += static_cast<double>(g[D * v + a]) * static_cast<double>(g[D * v + a]);
+        gn = sqrt(gn);
+        const double pos = fmin(fmax((Wi[v] - static_cast<double>(lo[v])) / safe, -1.0), 2.0);
+        f[4 * v + 0] = static_cast<float>(alpha[v] / kAlphaCap);
+        f[4 * v + 1] = static_cast<float>(pos - 0.5);
+        f[4 * v + 2] = static_cast<float>(tanh(gn * r / safe));
+        f[4 * v + 3] = static_cast<float>(tanh(range / scale * 3.0));
+        plain = fmin(plain, fmin(alpha[v], 1.0));
+        out.alpha[5 * static_cast<int64_t>(i) + v] = alpha[v];
+    }
+    const double plo = fmax(static_cast<double>(lo[D + 1]), 1e-300), phi = fmax(static_cast<double>(hi[D + 1]), plo);
+    double speed = 0;
+#pragma unroll
+    for (int a = 0; a < D; ++a) speed += Wi[1 + a] * Wi[1 + a];
+    f[20] = static_cast<float>(tanh(log(phi / plo)));
+    f[21] = static_cast<float>(tanh(sqrt(speed) / fmax(c, 1e-300)));
+    f[22] = static_cast<float>(plain);
+    f[23] = 1.0f;
+    __nv_bfloat16* row = out.features + 32 * static_cast<int64_t>(i);
+#pragma unroll
+    for (int k = 0; k < 32; k += 2) *reinterpret_cast<__nv_bfloat162*>(row + k) = __floats2bfloat162_rn(f[k], f[k + 1]);
+}
+
+// The learned slope factors applied: g_v *= alpha_v sigmoid(logit_v) (use_net), or min(alpha_v, 1), the plain limiter's
+// factor in min-factor form (a check of alpha against the plain sweep).
+template <int D>
+__global__ void k_apply_factors(int n, double* __restrict__ grad, const double* __restrict__ alpha, const float* __restrict__ logits,
+                                bool use_net) {
+    constexpr int V = D + 2, GS = grad_stride<D>();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        const double a = alpha[5 * static_cast<int64_t>(i) + v];
+        double phi;
+        if (use_net) {
+            const double o = logits[16 * static_cast<int64_t>(i) + v];
+            phi = a / (1.0 + exp(-o));
+        } else {
+            phi = fmin(a, 1.0);
+        }
+#pragma unroll
+        for (int d = 0; d < D; ++d) grad[static_cast<int64_t>(GS) * i + D * v + d] *= phi;
+    }
 }
 
 // The static flux pass over the face rows (FaceFlux::operator(), finite_volume.hpp:1415-1434): one streamed row per

@@ -19,6 +19,7 @@
 #include "adjoint.cuh"
 #include "geometry.cuh"
 #include "kernels.cuh"
+#include "mlp.cuh"
 #include "luna_b200.h"
 
 namespace {
@@ -106,6 +107,12 @@ struct luna_fv {
     DevArray<unsigned int> geo_nbr, geo_face;
     DevArray<int32_t> geo_slice_base, geo_order;
     DevArray<double> geo_angle;
+    // the learned limiter: inputs written by the sweep, the network's logits; mlp_params is the caller's device vector
+    DevArray<unsigned char> lim_features;
+    DevArray<double> lim_alpha;
+    DevArray<float> lim_logits;
+    const float* mlp_params = nullptr;
+    bool learned_inputs = false, apply_learned = false;
     // adjoint (allocated by the first luna_fv_step_adjoint)
     DevArray<double> adj_fit, adj_face_bar, adj_wbar, adj_bbar, adj_boundbar, adj_qbar;
     DevArray<int32_t> adj_flags, adj_bound_face;
@@ -320,17 +327,38 @@ template <int D, bool Moving, bool Grad, class G>
 luna_status launch_sweep(luna_fv* fv, G* grad, double courant) {
     const auto m = fv->mesh_dev<D>();
     const auto geo = fv->geometry_dev<D, G>();
+    luna::LearnedInputs learned{reinterpret_cast<__nv_bfloat16*>(fv->lim_features.ptr), fv->lim_alpha.ptr};
+    const bool learned_mode = Grad && fv->learned_inputs && fv->limiter == LUNA_LIMITER_FACE_CENTROID;
     {
         const long timed_ = fv->open_timed(1);
         if (fv->limiter == LUNA_LIMITER_NONE)
-            luna::k_sweep_rows<D, Moving, Grad, G, false><<<blocks(fv->n, kBlockCells), kBlockCells, 0, fv->stream>>>(m, geo, fv->prims.ptr, grad,
-                                                                                                                fv->w.ptr, courant, fv->counters.ptr);
-        else
-            luna::k_sweep_rows<D, Moving, Grad, G, true><<<blocks(fv->n, kBlockCells), kBlockCells, 0, fv->stream>>>(m, geo, fv->prims.ptr, grad,
-                                                                                                               fv->w.ptr, courant, fv->counters.ptr);
+            luna::k_sweep_rows<D, Moving, Grad, G, 0><<<blocks(fv->n, kBlockCells), kBlockCells, 0, fv->stream>>>(m, geo, fv->prims.ptr, grad,
+                                                                                                             fv->w.ptr, courant, fv->counters.ptr, learned);
+        else if (learned_mode) {
+            if constexpr (sizeof(G) == sizeof(double))
+                luna::k_sweep_rows<D, Moving, Grad, G, 2><<<blocks(fv->n, kBlockCells), kBlockCells, 0, fv->stream>>>(m, geo, fv->prims.ptr, grad,
+                                                                                                                 fv->w.ptr, courant, fv->counters.ptr, learned);
+        } else
+            luna::k_sweep_rows<D, Moving, Grad, G, 1><<<blocks(fv->n, kBlockCells), kBlockCells, 0, fv->stream>>>(m, geo, fv->prims.ptr, grad,
+                                                                                                             fv->w.ptr, courant, fv->counters.ptr, learned);
         fv->close_timed(timed_);
     }
     LUNA_CUDA(cudaGetLastError());
+    if constexpr (sizeof(G) == sizeof(double)) {
+        if (learned_mode && fv->apply_learned) {  // the network's factors, then the gradients scaled
+            const long timed_ = fv->open_timed(1);
+            if (fv->mlp_params) {
+                const int64_t warps = (fv->n + 15) / 16;
+                const int nb = static_cast<int>(std::min<int64_t>((warps + 3) / 4, 148 * 8));
+                luna::mlp::k_mlp_forward<<<nb, 128, 0, fv->stream>>>(fv->mlp_params, reinterpret_cast<const __nv_bfloat16*>(fv->lim_features.ptr),
+                                                                     static_cast<int>(fv->n), fv->lim_logits.ptr);
+            }
+            luna::k_apply_factors<D><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(static_cast<int>(fv->n), grad, fv->lim_alpha.ptr, fv->lim_logits.ptr,
+                                                                                 fv->mlp_params != nullptr);
+            fv->close_timed(timed_);
+            LUNA_CUDA(cudaGetLastError());
+        }
+    }
     return LUNA_OK;
 }
 
@@ -863,6 +891,58 @@ LUNA_API luna_status luna_fv_step_adjoint(luna_fv* fv, double dt, double* qbar, 
     return LUNA_OK;
 }
 
+// The learned limiter's buffers (64 B of features, 40 B of admissible factors, 64 B of logits a cell).
+static luna_status alloc_learned(luna_fv* fv) {
+    const size_t N = static_cast<size_t>(fv->n);
+    LUNA_TRY(fv->lim_features.alloc(N * 32 * sizeof(__nv_bfloat16), "limiter features"));
+    LUNA_TRY(fv->lim_alpha.alloc(N * 5, "limiter admissible factors"));
+    LUNA_TRY(fv->lim_logits.alloc(N * 16, "limiter logits"));
+    return LUNA_OK;
+}
+
+LUNA_API luna_status luna_fv_set_limiter_mlp(luna_fv* fv, const float* params, int mode) {
+    if (!fv) return set_error(LUNA_EINVAL, "fv is null");
+    if (mode == 0) {
+        fv->learned_inputs = fv->apply_learned = false;
+        fv->mlp_params = nullptr;
+        return LUNA_OK;
+    }
+    if (fv->order != 1 || fv->precision != LUNA_FP64 || fv->limiter != LUNA_LIMITER_FACE_CENTROID)
+        return set_error(LUNA_EINVAL, "the learned limiter needs order 1, the FP64 policy and the face-centroid limiter");
+    if (mode == 1 && !params) return set_error(LUNA_EINVAL, "mode 1 needs the network's parameters");
+    LUNA_TRY(alloc_learned(fv));
+    fv->learned_inputs = fv->apply_learned = true;
+    fv->mlp_params = mode == 1 ? params : nullptr;  // mode 2: the plain factor min(alpha, 1) through the same path
+    fv->swept = false;
+    return LUNA_OK;
+}
+
+LUNA_API luna_status luna_fv_limiter_inputs(luna_fv* fv, void* features, double* alpha, double* gradients) {
+    if (!fv || !features || !alpha || !gradients) return set_error(LUNA_EINVAL, "null argument");
+    if (fv->order != 1 || fv->precision != LUNA_FP64 || fv->limiter != LUNA_LIMITER_FACE_CENTROID)
+        return set_error(LUNA_EINVAL, "the learned limiter needs order 1, the FP64 policy and the face-centroid limiter");
+    if (fv->moving_pending) return set_error(LUNA_ESTATE, "inside a moving step");
+    LUNA_TRY(alloc_learned(fv));
+    const bool inputs = fv->learned_inputs, apply = fv->apply_learned;
+    fv->learned_inputs = true;
+    fv->apply_learned = false;
+    fv->prims_ready = false;
+    luna_status s = fv->dim == 3 ? prepare_sweep<3>(fv, 1.0) : prepare_sweep<2>(fv, 1.0);
+    fv->learned_inputs = inputs;
+    fv->apply_learned = apply;
+    fv->swept = false;
+    if (s != LUNA_OK) return s;
+    const size_t N = static_cast<size_t>(fv->n);
+    const int D = fv->dim, width = (D + 2) * D;
+    const size_t GS = D == 3 ? luna::grad_stride<3>() : luna::grad_stride<2>();
+    LUNA_CUDA(cudaMemcpyAsync(features, fv->lim_features.ptr, N * 32 * sizeof(__nv_bfloat16), cudaMemcpyDeviceToDevice, fv->stream));
+    LUNA_CUDA(cudaMemcpyAsync(alpha, fv->lim_alpha.ptr, N * 5 * sizeof(double), cudaMemcpyDeviceToDevice, fv->stream));
+    LUNA_CUDA(cudaMemcpy2DAsync(gradients, width * sizeof(double), fv->grad64.ptr, GS * sizeof(double), width * sizeof(double), N,
+                                cudaMemcpyDeviceToDevice, fv->stream));
+    LUNA_CUDA(cudaStreamSynchronize(fv->stream));
+    return LUNA_OK;
+}
+
 LUNA_API luna_status luna_fv_set_timing(luna_fv* fv, int on) {
     if (!fv) return set_error(LUNA_EINVAL, "fv is null");
     fv->timing = on != 0;
@@ -901,7 +981,7 @@ LUNA_API luna_status luna_fv_device_bytes(luna_fv* fv, int64_t* out) {
     b += fv->adj_qbar.bytes() + fv->adj_flags.bytes() + fv->adj_bound_face.bytes();
     b += fv->geo_c01.bytes() + fv->geo_c2.bytes() + fv->geo_off01.bytes() + fv->geo_off2.bytes() + fv->geo_nbr.bytes();
     b += fv->geo_face.bytes() + fv->geo_slice_base.bytes() + fv->geo_order.bytes() + fv->geo_dt.bytes() + fv->geo_faces.bytes();
-    b += fv->geo_angle.bytes();
+    b += fv->geo_angle.bytes() + fv->lim_features.bytes() + fv->lim_alpha.bytes() + fv->lim_logits.bytes();
     *out = static_cast<int64_t>(b);
     return LUNA_OK;
 }

@@ -81,6 +81,13 @@ SIGNATURES = {
     "luna_fv_set_timing": ([P, I], I),
     "luna_fv_step_adjoint": ([P, D64, P, I], I),
     "luna_apply_static_noalloc": ([P, P, I, I, P, P, P, D64, P, P], I),
+    "luna_fv_set_limiter_mlp": ([P, P, I], I),
+    "luna_fv_limiter_inputs": ([P, P, P, P], I),
+    "luna_mlp_param_count": ([], I64),
+    "luna_mlp_train_workspace_floats": ([I64], I64),
+    "luna_mlp_forward": ([P, P, I64, P, P], I),
+    "luna_mlp_train_step": ([P, P, P, P, I64, ctypes.c_float, P, P, P, I64, P], I),
+    "luna_mlp_adam": ([P, P, P, P, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, I, P], I),
     "luna_fv_timings": ([P, P, I], I),
 }
 
@@ -258,6 +265,25 @@ class FiniteVolume:
         a = np.ascontiguousarray(qbar, dtype=np.float64).copy()
         check(lib().luna_fv_step_adjoint(self._h, dt, a.ctypes.data, 0))
         return a
+
+    def set_limiter(self, mode: str = "plain", params=None) -> None:
+        """The slope limiter of the sweep: "plain" (the reference's), "learned" (the MLP with ``params``, a CUDA float32
+        tensor the caller keeps alive), or "factors" (the plain limiter in min-factor form through the learned path)."""
+        code = {"plain": 0, "learned": 1, "factors": 2}[mode]
+        self._limiter_params = params
+        ptr = ctypes.c_void_p(params.data_ptr()) if params is not None else None
+        check(lib().luna_fv_set_limiter_mlp(self._h, ptr, code))
+
+    def limiter_inputs(self):
+        """(features [N, 32] bf16, alpha [N, 5] float64, unlimited gradients [N, V*D] float64) as CUDA tensors."""
+        import torch
+
+        f = torch.empty((self.n, 32), dtype=torch.bfloat16, device="cuda")
+        a = torch.empty((self.n, 5), dtype=torch.float64, device="cuda")
+        g = torch.empty((self.n, self.V * self.dim), dtype=torch.float64, device="cuda")
+        check(lib().luna_fv_limiter_inputs(self._h, ctypes.c_void_p(f.data_ptr()), ctypes.c_void_p(a.data_ptr()),
+                                           ctypes.c_void_p(g.data_ptr())))
+        return f, a, g
 
     def set_stream(self, stream_ptr: int) -> None:
         check(lib().luna_fv_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
