@@ -84,3 +84,11 @@ def init_params(seed: int = 0) -> np.ndarray:
     p.append(rng.standard_normal((OUT, HID)) * np.sqrt(1.0 / HID) * 0.1)
     p.append(np.full(OUT, 2.0))
     return np.concatenate([a.ravel() for a in p]).astype(np.float32)
+
+
+def trained_params() -> np.ndarray:
+    """The network trained by ``python -m luna_cpp_b200.limiter_training`` (48 Riemann problems, 15 epochs), shipped so
+    the learned limiter runs without retraining."""
+    import os
+
+    return np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "limiter_mlp_params.npy"))
