@@ -175,6 +175,18 @@ LUNA_API luna_status luna_mlp_adam(float* params, const float* grad, float* m, f
 LUNA_API luna_status luna_apply_static_noalloc(const luna_mesh_desc* mesh, const luna_gas* gas, int order, int riemann, const double* prims,
                                                const double* gradients, double* q, double dt, void* stream, int64_t* fallbacks_out);
 
+/* The sweep's tiles for a mesh given in host memory: the layout luna_fv_create builds, computed on the host only (no
+ * device work; no counterpart in the reference, a diagnostic of this library). Cells in Morton order of their
+ * generators are cut into tiles of at most 128 cells; a tile's staged rows are its cells (in thread order) and then
+ * the cells their lists reach, at most 416 of them (a cell needing more gets a tile of its own).
+ * counts[6]: tiles, tiles within the 416-row budget, staged rows, entry slots, the most rows of a budget tile, the
+ * most rows of a single-cell tile. The arrays may be null (sizes from a first call); else order [tiles * 128] (the
+ * cell of each thread, -1 idle), slice_base [tiles * 4 + 1] (each warp's first entry slot / 32), stage_start
+ * [tiles + 1], stage_cells [staged rows], local [entry slots] (each list entry's neighbour as a row of its tile's
+ * staged cells, at slot (slice_base[t / 32] + k) * 32 + t % 32 for entry k of thread t). */
+LUNA_API luna_status luna_mesh_tiles(const luna_mesh_desc* mesh, int64_t counts[6], int32_t* order, int32_t* slice_base, int32_t* stage_start,
+                                     int32_t* stage_cells, uint32_t* local);
+
 LUNA_API const char* luna_status_string(luna_status s);
 LUNA_API const char* luna_last_error(void);
 /* Device bytes held by fv (all its buffers). */

@@ -4,16 +4,17 @@
 // costs three dependent loads (list -> face -> neighbour -> rows) plus the separation, the fit row X = [1, d + c_j - c_i]
 // and the face offset. Everything there except the neighbours' primitive rows depends on the mesh only, so this pass
 // computes it once, in the reference's arithmetic, into rows that the step streams in list order:
-//   entries          per list entry: w X_p (the fit's weighted row, p = 0..D), the face offset x_f - c_i, the neighbour,
-//                    whether the cell owns the face, the face, and whether the face is below 1e-6 of the cell's surface;
-//                    sliced by 32 cells (a warp): entry k of the slice's lane l sits at (slice_base + k) * 32 + l, each
-//                    field in an array of its own, so a warp's load of entry k of its 32 cells is one contiguous run;
-//                    the entry's row of the cell's gradient operator c_k (see k_geometry) instead of the fit's sums;
-//   dt rows [F]      the separation d of the face's generators and |d| (the CFL face terms, finite_volume.hpp:1074-1090);
+//   entries          per list entry: the entry's row of the cell's gradient operator c_k (see k_geometry) instead of
+//                    the fit's sums, the face offset x_f - c_i, the neighbour as a row of the tile's staged cells
+//                    (tiles.h), whether the cell owns the face and whether the face is below 1e-6 of the cell's
+//                    surface; sliced by 32 cells (a warp): entry k of the slice's lane l sits at
+//                    (slice_base + k) * 32 + l, each field in an array of its own, so a warp's load of entry k of its
+//                    32 cells is one contiguous run;
 //   face rows [F]    the unit normal A / |A|, |A|, both cells' face offsets and the two cells (FaceFlux, :1415-1434);
 //   cell angle [N]   the largest AREPO face angle of the cell (the moving mesh's regularisation, :509, :526-537).
-// The step then reads one streamed row per entry and gathers only the neighbour's primitive row: one dependent level.
-// Cells are swept in an order grouping lists of one length (see kOrderWindow).
+// The sweep runs one block per tile: it stages the primitive rows and generators of the tile's cells and of their
+// neighbours into shared memory, then each thread walks its cell's streamed entries and reads the neighbours' rows
+// there, so no list entry waits on a gather from HBM.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -21,6 +22,7 @@
 #include <type_traits>
 
 #include "kernels.cuh"
+#include "tiles.h"
 
 namespace luna {
 
@@ -49,28 +51,25 @@ struct alignas(32) FaceRow32 {
 template <class G>
 using FaceRow = typename std::conditional<sizeof(G) == sizeof(double), FaceRow64, FaceRow32>::type;
 
-struct DtRow {
-    double d[3];
-    double dist;
-};
-
-// Cells are swept in `order`: by list length within windows of kOrderWindow cells, so the 32 cells of a warp have lists
-// of nearly one length (lanes of a warp idle while the longest list runs) and stay close in the mesh.
-constexpr int kOrderWindow = 512;
+// A staged row in shared memory (12 doubles, 96 B): the cell's primitive row (W, c, r, pad: as in HBM), then its
+// generator (D doubles).
+constexpr int kStagedDoubles = 12;
+constexpr int kStagedPos = 8;
 
 template <int D, class G>
 struct GeometryDev {
-    const int32_t* __restrict__ order;       // [N]: thread t sweeps cell order[t]
-    const int32_t* __restrict__ slice_base;  // [ceil(N / 32) + 1], in slots of 32 entries
-    unsigned int* __restrict__ nbr;          // neighbour | tiny << 30 | owned << 31
-    unsigned int* __restrict__ face;         // the face (owned entries: their dt row)
-    Pair<G>* __restrict__ c01;               // gradient operator row c_k, x and y
-    G* __restrict__ c2;                      // z (3D)
-    Pair<G>* __restrict__ off01;             // face offset x, y
-    G* __restrict__ off2;                    // z (3D)
-    DtRow* __restrict__ dt_rows;             // [F]
-    FaceRow<G>* __restrict__ faces;          // [F]
-    double* __restrict__ max_angle;          // [N]
+    const int32_t* __restrict__ order;        // [tiles * kTileCells]: thread t sweeps cell order[t] (-1: idle)
+    const int32_t* __restrict__ slice_base;   // [tiles * kTileCells / 32 + 1], in slots of 32 entries
+    const int32_t* __restrict__ stage_start;  // [tiles + 1]
+    const int32_t* __restrict__ stage_cells;  // each tile's staged cells: its own in thread order, then the halo
+    unsigned int* __restrict__ nbr;           // staged row of the neighbour | tiny << 30 | owned << 31
+    Pair<G>* __restrict__ c01;                // gradient operator row c_k, x and y
+    G* __restrict__ c2;                       // z (3D)
+    Pair<G>* __restrict__ off01;              // face offset x, y
+    G* __restrict__ off2;                     // z (3D)
+    FaceRow<G>* __restrict__ faces;           // [F]
+    double* __restrict__ max_angle;           // [N]
+    int64_t threads;                          // tiles * kTileCells
 };
 
 // One thread a cell (in sweep order): the cell's geometry in list order. The least-squares fit of Sweep (an area-
@@ -78,13 +77,15 @@ struct GeometryDev {
 // neighbours' differences: x_v = M^-1 sum_k w_k X_k (W_kv - W_iv) with M = sum_k w_k X_k X_k^T, so the gradient is
 // g_v = sum_k c_k (W_kv - W_iv) with c_k = rows 1..D of M^-1 w_k X_k. M, its Cholesky factor and each c_k are formed
 // here in double, in the reference's order; the sweep then only sums c_k times the differences. Also the face rows of
-// the faces the cell owns, the dt rows and the largest face angle.
+// the faces the cell owns and the largest face angle. g.nbr holds each entry's staged row on entry (from the host's
+// tiles); the kernel adds the owned and tiny bits.
 template <int D, class G>
 __global__ void __launch_bounds__(128) k_geometry(MeshDev<D> m, GeometryDev<D, G> g) {
     constexpr int U = D + 1;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= m.n) return;
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= g.threads) return;
     const int i = g.order[t];
+    if (i < 0) return;
     double centroid[D];
 #pragma unroll
     for (int a = 0; a < D; ++a) centroid[a] = m.cen[D * i + a];
@@ -115,13 +116,6 @@ __global__ void __launch_bounds__(128) k_geometry(MeshDev<D> m, GeometryDev<D, G
         for (int p = 0; p < U; ++p)
 #pragma unroll
             for (int s = p; s < U; ++s) M[p][s] += magnitude * X[p] * X[s];
-        if (e >= 0) {
-            DtRow r;
-#pragma unroll
-            for (int a = 0; a < 3; ++a) r.d[a] = a < D ? d[a] : 0.0;
-            r.dist = sqrt(d2);
-            g.dt_rows[f] = r;
-        }
     }
     double L[U][U];
 #pragma unroll
@@ -173,8 +167,7 @@ __global__ void __launch_bounds__(128) k_geometry(MeshDev<D> m, GeometryDev<D, G
         g.off01[slot] = Pair<G>{static_cast<G>(off[0]), static_cast<G>(off[1])};
         if constexpr (D == 3) g.off2[slot] = static_cast<G>(off[2]);
         const bool tiny_face = any_tiny && magnitude < tiny;
-        g.nbr[slot] = static_cast<unsigned int>(j) | (owned ? kOwnedBit : 0u) | (tiny_face ? kTinyBit : 0u);
-        g.face[slot] = static_cast<unsigned int>(f);
+        g.nbr[slot] = (g.nbr[slot] & kIndexMask) | (owned ? kOwnedBit : 0u) | (tiny_face ? kTinyBit : 0u);
         if (owned) {  // the face row, written once by the owner
             double a[D];
 #pragma unroll
@@ -205,10 +198,12 @@ __global__ void __launch_bounds__(128) k_geometry(MeshDev<D> m, GeometryDev<D, G
     g.max_angle[i] = max_angle;
 }
 
-// The sweep over the reordered rows (Sweep<Moving, Grad>::operator(), finite_volume.hpp:463-569): walk 1 sums the
-// gradient g_v = sum_k c_k (W_jv - W_iv) in list order, the neighbours' range (tiny faces left out) and the owned faces'
-// CFL terms; walk 2 clips at each face offset in list order. Per entry: streamed coalesced rows and one gathered
-// primitive row (two 256-bit loads).
+// The sweep over the reordered rows (Sweep<Moving, Grad>::operator(), finite_volume.hpp:463-569), one block per tile:
+// the block stages the primitive rows and generators of the tile's cells and their neighbours into shared memory (the
+// rows are independent: all copies are in flight at once); then walk 1 sums the gradient g_v = sum_k c_k (W_jv - W_iv)
+// in list order, the neighbours' range (tiny faces left out) and the owned faces' CFL terms (FaceStep, :1074-1090,
+// the separation formed from the staged generators); walk 2 clips at each face offset in list order. Per entry: the
+// streamed coalesced entry rows and one shared-memory row.
 // The learned limiter's 32 features of a cell (FP64 policy: lo/hi are the neighbours' values): per variable v,
 //   alpha_v / 2                        the admissible factor (how far the slope may steepen or must flatten),
 //   (W_v - lo_v) / (hi_v - lo_v) - 1/2 where the cell sits in its neighbours' range,
@@ -227,23 +222,66 @@ struct LearnedInputs {
 };
 constexpr double kAlphaCap = 2.0;  // the largest steepening the learned limiter may choose
 
+// Resident blocks per SM the register budget is cut for, and the entries whose streamed rows are requested together;
+// measured at 128^3 FP64 (sweep ms): 3 blocks / 4 entries 1.74, 4 / 2 1.31 (a few spilled registers), 5 / 1 1.65.
+#ifndef LUNA_SWEEP_MIN_BLOCKS
+#define LUNA_SWEEP_MIN_BLOCKS 4
+#endif
+#ifndef LUNA_SWEEP_BATCH
+#define LUNA_SWEEP_BATCH 2
+#endif
 // Limit: 0 none, 1 the plain face-centroid limiter, 2 the learned limiter's inputs (the gradient left unlimited).
-template <int D, bool Moving, bool Grad, class G, int Limit>
-__global__ void __launch_bounds__(128) k_sweep_rows(MeshDev<D> m, GeometryDev<D, G> geo, const double* __restrict__ prims,
-                                                    G* __restrict__ grad_out, double* __restrict__ w_out, double courant,
-                                                    Counters* __restrict__ ctr, LearnedInputs learned) {
-    constexpr int V = D + 2, GS = grad_stride<D>();
+// KB: entries whose streamed rows are requested together. Launched with blocks of kTileCells threads over tiles [tile0, tile0 + gridDim.x) and the shared memory of the most
+// rows one of them stages (kStagedDoubles doubles a row).
+template <int D, bool Moving, bool Grad, class G, int Limit, int KB = LUNA_SWEEP_BATCH, int MINB = LUNA_SWEEP_MIN_BLOCKS>
+__global__ void __launch_bounds__(kTileCells, MINB) k_sweep_tiles(MeshDev<D> m, GeometryDev<D, G> geo, int tile0, const double* __restrict__ prims,
+                                                               G* __restrict__ grad_out, double* __restrict__ w_out, double courant,
+                                                               Counters* __restrict__ ctr, LearnedInputs learned) {
+    extern __shared__ double2 staged_rows[];
+    double* rows = reinterpret_cast<double*>(staged_rows);
+    constexpr int V = D + 2, GS = grad_stride<D>(), R = kStagedDoubles;
     constexpr bool exact = sizeof(G) == sizeof(double);
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    double smallest_dt = 1.0e300;
-    if (t < m.n) {
-        const int i = geo.order[t];
-        double pi[8];
-        load_prim_row<D>(prims, i, pi);
-        double Wi[V];
+    const int tile = tile0 + static_cast<int>(blockIdx.x);
+    const int64_t t = static_cast<int64_t>(tile) * kTileCells + threadIdx.x;
+    const int i = geo.order[t];
+    const int count = i >= 0 ? m.start[i + 1] - m.start[i] : 0;
+    const int64_t row0 = static_cast<int64_t>(geo.slice_base[t >> 5]) * 32;  // the warp's first slot
+    const int64_t slot0 = row0 + (t & 31);
+    const unsigned long long once = l2_evict_first();  // entry rows are read once per step
+    {
+        const int s0 = geo.stage_start[tile], staged = geo.stage_start[tile + 1] - s0;
+        constexpr int kRowsInFlight = 4;
+        for (int r0 = 0; r0 < staged; r0 += kRowsInFlight * kTileCells) {
+            int cell[kRowsInFlight];
 #pragma unroll
-        for (int v = 0; v < V; ++v) Wi[v] = pi[v];
-        const double ci = pi[V], ri = pi[V + 1];
+            for (int b = 0; b < kRowsInFlight; ++b) {
+                const int r = r0 + b * kTileCells + static_cast<int>(threadIdx.x);
+                cell[b] = r < staged ? geo.stage_cells[s0 + r] : -1;
+            }
+#pragma unroll
+            for (int b = 0; b < kRowsInFlight; ++b) {
+                if (cell[b] < 0) continue;
+                double* dst = rows + R * (r0 + b * kTileCells + static_cast<int>(threadIdx.x));
+                const double* src = prims + PS * static_cast<int64_t>(cell[b]);
+#pragma unroll
+                for (int q = 0; q < PS; q += 2) cp_async16(dst + q, src + q);
+#pragma unroll
+                for (int a = 0; a < D; ++a) cp_async8(dst + kStagedPos + a, m.pos + D * static_cast<int64_t>(cell[b]) + a);
+            }
+        }
+        cp_async_wait_all();
+        __syncthreads();
+    }
+    double smallest_dt = 1.0e300;
+    if (i >= 0) {
+        // the cell's own row: tile cells are staged first, in thread order
+        const double* own = rows + R * threadIdx.x;
+        double Wi[V], xi[D];
+#pragma unroll
+        for (int v = 0; v < V; ++v) Wi[v] = own[v];
+        const double ci = own[V], ri = own[V + 1];
+#pragma unroll
+        for (int a = 0; a < D; ++a) xi[a] = own[kStagedPos + a];
         G lo[V], hi[V], g[V * D];
 #pragma unroll
         for (int v = 0; v < V; ++v) {
@@ -252,53 +290,21 @@ __global__ void __launch_bounds__(128) k_sweep_rows(MeshDev<D> m, GeometryDev<D,
 #pragma unroll
             for (int a = 0; a < D; ++a) g[D * v + a] = G(0);
         }
-        const int count = m.start[i + 1] - m.start[i];
-        const int64_t row0 = static_cast<int64_t>(geo.slice_base[t >> 5]) * 32;  // the warp's first slot
-        const int64_t slot0 = row0 + (t & 31);
-        // Lane 0 holds the warp's longest list (cells are ordered by list length within windows): it streams the warp's
-        // entry rows into L2 kPrefetch entries ahead with bulk prefetches, one per array and entry.
-        constexpr int kPrefetch = 4;
-        const bool leader = (threadIdx.x & 31) == 0;
-        const unsigned long long once = l2_evict_first();
-        auto prefetch_rows = [&](int k) {
-            const int64_t r = row0 + 32 * static_cast<int64_t>(k);
-            prefetch_l2_hint(geo.nbr + r, 32 * sizeof(unsigned int), once);
-            prefetch_l2_hint(geo.face + r, 32 * sizeof(unsigned int), once);
-            if constexpr (Grad) {
-                prefetch_l2_hint(geo.c01 + r, 32 * sizeof(Pair<G>), once);
-                if constexpr (D == 3) prefetch_l2_hint(geo.c2 + r, 32 * sizeof(G), once);
-                if constexpr (Limit != 0) {
-                    prefetch_l2_hint(geo.off01 + r, 32 * sizeof(Pair<G>), once);
-                    if constexpr (D == 3) prefetch_l2_hint(geo.off2 + r, 32 * sizeof(G), once);
-                }
-            }
-        };
-        if (leader)
-            for (int k = 0; k < kPrefetch && k < count; ++k) prefetch_rows(k);
-        // kBatch entries at a time: all their loads are issued before any is used, so each thread keeps several
-        // gathers in flight (the entries of a list are independent; only the sums carry over, in list order).
-        constexpr int kBatch = 2;
+        // kBatch entries at a time: their streamed rows are all requested before any is used; the staged rows they
+        // name are shared-memory reads.
+        constexpr int kBatch = KB;
+        // The smallest face term courant (dist + r) / vsig, vsig = c_i + c_j - dv.d / dist (FaceStep), held as the
+        // fraction num / den = (dist + r) dist / ((c_i + c_j) dist - dv.d) and compared by cross products: one division
+        // a cell instead of two a face (the same minimum, rounded once).
+        double best_num = 1.0e300, best_den = 1.0;
         for (int k0 = 0; k0 < count; k0 += kBatch) {
-            if (leader)
-#pragma unroll
-                for (int b = 0; b < kBatch; ++b)
-                    if (k0 + b + kPrefetch < count) prefetch_rows(k0 + b + kPrefetch);
-            unsigned int word[kBatch], fword[kBatch];
-#pragma unroll
-            for (int b = 0; b < kBatch; ++b) {
-                const int64_t slot = slot0 + 32 * static_cast<int64_t>(k0 + b);
-                const bool valid = k0 + b < count;
-                word[b] = valid ? ldg_hint(geo.nbr + slot, once) : 0u;
-                fword[b] = valid && (word[b] & kOwnedBit) ? ldg_hint(geo.face + slot, once) : 0u;
-            }
-            double pj[kBatch][8], dtr[kBatch][4];
+            unsigned int word[kBatch];
             G c[kBatch][D];
 #pragma unroll
             for (int b = 0; b < kBatch; ++b) {
                 const int64_t slot = slot0 + 32 * static_cast<int64_t>(k0 + b);
                 if (k0 + b < count) {
-                    load_prim_row<D>(prims, static_cast<int>(word[b] & kIndexMask), pj[b]);
-                    if (word[b] & kOwnedBit) ldg256_hint(reinterpret_cast<const double*>(geo.dt_rows + fword[b]), dtr[b], once);
+                    word[b] = ldg_hint(geo.nbr + slot, once);
                     if constexpr (Grad) {
                         const Pair<G> c01 = ldg_hint(geo.c01 + slot, once);
                         c[b][0] = c01.x;
@@ -311,29 +317,41 @@ __global__ void __launch_bounds__(128) k_sweep_rows(MeshDev<D> m, GeometryDev<D,
             for (int b = 0; b < kBatch; ++b) {
                 if (k0 + b >= count) break;
                 const bool owned = (word[b] & kOwnedBit) != 0, tiny_face = (word[b] & kTinyBit) != 0;
+                const double* rj = rows + R * static_cast<int>(word[b] & kIndexMask);
+                double pj[8];
+#pragma unroll
+                for (int q = 0; q < 6; q += 2) {
+                    const double2 w2 = *reinterpret_cast<const double2*>(rj + q);
+                    pj[q] = w2.x;
+                    pj[q + 1] = w2.y;
+                }
                 if (owned) {  // FaceStep (finite_volume.hpp:1074-1090)
+                    const double2 w2 = *reinterpret_cast<const double2*>(rj + 6);
+                    pj[6] = w2.x;
+                    pj[7] = w2.y;
                     double dv[D], d[D];
 #pragma unroll
                     for (int a = 0; a < D; ++a) {
-                        dv[a] = pj[b][1 + a] - Wi[1 + a];
-                        d[a] = dtr[b][a];
+                        dv[a] = pj[1 + a] - Wi[1 + a];
+                        d[a] = m.wrap(rj[kStagedPos + a] - xi[a], a);  // Geometry::separation of owner and neighbour
                     }
-                    const double dist = dtr[b][3];
-                    const double vsig = ci + pj[b][V] - dot<D>(dv, d) / dist;
-                    if (vsig > 0) {
-                        // Both cells' terms (dist + r) / vsig: the smaller radius gives the smaller one, the same rounding.
-                        smallest_dt = fmin(smallest_dt, courant * ((dist + fmin(ri, pj[b][V + 1])) / vsig));
+                    const double dist = sqrt(dot<D>(d, d));
+                    // Both cells' terms: the smaller radius gives the smaller one. den > 0 is vsig > 0.
+                    const double num = (dist + fmin(ri, pj[V + 1])) * dist, den = (ci + pj[V]) * dist - dot<D>(dv, d);
+                    if (den > 0 && num * best_den < best_num * den) {
+                        best_num = num;
+                        best_den = den;
                     }
                 }
                 if constexpr (Grad) {
 #pragma unroll
                     for (int v = 0; v < V; ++v) {
-                        const double dW = pj[b][v] - Wi[v];
+                        const double dW = pj[v] - Wi[v];
                         const G dWg = static_cast<G>(dW);
 #pragma unroll
                         for (int a = 0; a < D; ++a) g[D * v + a] += c[b][a] * dWg;
                         if (!tiny_face) {
-                            const G value = exact ? static_cast<G>(pj[b][v]) : dWg;
+                            const G value = exact ? static_cast<G>(pj[v]) : dWg;
                             lo[v] = fmin(lo[v], value);
                             hi[v] = fmax(hi[v], value);
                         }
@@ -341,6 +359,7 @@ __global__ void __launch_bounds__(128) k_sweep_rows(MeshDev<D> m, GeometryDev<D,
                 }
             }
         }
+        if (best_num < 1.0e300) smallest_dt = courant * (best_num / best_den);
         double wi[D];
 #pragma unroll
         for (int a = 0; a < D; ++a) wi[a] = Wi[1 + a];
@@ -394,7 +413,7 @@ __global__ void __launch_bounds__(128) k_sweep_rows(MeshDev<D> m, GeometryDev<D,
                         alpha[v] = fmin(alpha[v], factor);
                     }
                 }
-                write_learned_inputs<D>(learned, i, Wi, pi[V], pi[V + 1], g, lo, hi, alpha);
+                write_learned_inputs<D>(learned, i, Wi, ci, ri, g, lo, hi, alpha);
             }
             if constexpr (Limit == 1) {
                 constexpr int kClipBatch = 4;
@@ -450,8 +469,8 @@ __global__ void __launch_bounds__(128) k_sweep_rows(MeshDev<D> m, GeometryDev<D,
             for (int c = 0; c < V * D; ++c) out[c] = g[c];
         }
     }
-    block_min_to(smallest_dt, &ctr->dt_bits);
-    if (t < m.n && !(smallest_dt == smallest_dt)) atomicOr(&ctr->error, 1ull);
+    warp_min_to(smallest_dt, &ctr->dt_bits);  // no block barrier: a warp done with its lists leaves
+    if (i >= 0 && !(smallest_dt == smallest_dt)) atomicOr(&ctr->error, 1ull);
 }
 
 template <int D, class G>
@@ -518,8 +537,13 @@ __global__ void k_apply_factors(int n, double* __restrict__ grad, const double* 
 
 // The static flux pass over the face rows (FaceFlux::operator(), finite_volume.hpp:1415-1434): one streamed row per
 // face, then the two cells' primitive and gradient rows.
+// Resident blocks per SM the flux pass's registers are cut for; measured at 128^3 FP64 (fluxes ms): unbounded (96
+// registers, 5 blocks) 0.80-0.84, 6 blocks 0.77, 8 blocks 1.03 (spills).
+#ifndef LUNA_FLUX_MIN_BLOCKS
+#define LUNA_FLUX_MIN_BLOCKS 6
+#endif
 template <int D, int Order, class G, bool RF, int Riemann>
-__global__ void __launch_bounds__(128) k_flux_rows(MeshDev<D> m, GeometryDev<D, G> geo, FluxArgs<D, G> x, double* __restrict__ flux,
+__global__ void __launch_bounds__(128, LUNA_FLUX_MIN_BLOCKS) k_flux_rows(MeshDev<D> m, GeometryDev<D, G> geo, FluxArgs<D, G> x, double* __restrict__ flux,
                                                    unsigned long long* __restrict__ fallbacks) {
     constexpr int V = D + 2;
     const int f = blockIdx.x * blockDim.x + threadIdx.x;

@@ -126,6 +126,18 @@ __device__ __forceinline__ void prefetch_l2(const void* p, unsigned int bytes) {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
+// Asynchronous copies global -> shared (no registers held while in flight); cp_async_wait_all waits for this
+// thread's copies, a barrier after it makes them visible to the block. 16 B: both addresses 16-B aligned; 8 B: 8-B.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned int s = static_cast<unsigned int>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned int s = static_cast<unsigned int>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // A cell's primitive row (W, c, r, pad: 64 B, 64-B aligned) in two vector loads (3D), one (2D: W only).
 template <int D>
 __device__ __forceinline__ void load_prim_row(const double* prims, int i, double* row) {
@@ -156,6 +168,13 @@ __device__ __forceinline__ void block_min_to(double value, unsigned long long* t
         // Positive doubles order as their bit patterns; NaN (skipped by fmin) and +inf never win.
         if (lane == 0 && value > 0.0 && value < 1.0e300) atomicMin(target, static_cast<unsigned long long>(__double_as_longlong(value)));
     }
+}
+
+// The warp's minimum (positive, finite values) into *target, without a block barrier.
+__device__ __forceinline__ void warp_min_to(double value, unsigned long long* target) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) value = fmin(value, __shfl_xor_sync(0xffffffffu, value, o));
+    if ((threadIdx.x & 31) == 0 && value > 0.0 && value < 1.0e300) atomicMin(target, static_cast<unsigned long long>(__double_as_longlong(value)));
 }
 
 __device__ __forceinline__ void block_sum_to(unsigned long long value, unsigned long long* target) {
@@ -473,13 +492,29 @@ __global__ void __launch_bounds__(256) k_update(MeshDev<D> m, double* __restrict
 #pragma unroll
     for (int v = 0; v < V; ++v) sum[v] = 0;
     const int first = m.start[i], end = m.start[i + 1];
-    for (int k = first; k < end; ++k) {
-        const int32_t e = m.list[k];
-        const int f = list_face(e);
-        const double sign = e >= 0 ? 1.0 : -1.0;
-        const double* row = flux + V * static_cast<int64_t>(f);
+    // kBatch entries at a time: their list words, then their flux rows, are all requested before any is used (the
+    // gathers of a list are independent); the sums stay in list order.
+    constexpr int kBatch = 4;
+    for (int k0 = first; k0 < end; k0 += kBatch) {
+        int32_t e[kBatch];
 #pragma unroll
-        for (int v = 0; v < V; ++v) sum[v] += sign * row[v];
+        for (int b = 0; b < kBatch; ++b) e[b] = k0 + b < end ? m.list[k0 + b] : 0;
+        double row[kBatch][V];
+#pragma unroll
+        for (int b = 0; b < kBatch; ++b) {
+            if (k0 + b < end) {
+                const double* r = flux + V * static_cast<int64_t>(list_face(e[b]));
+#pragma unroll
+                for (int v = 0; v < V; ++v) row[b][v] = __ldg(r + v);
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < kBatch; ++b) {
+            if (k0 + b >= end) break;
+            const double sign = e[b] >= 0 ? 1.0 : -1.0;
+#pragma unroll
+            for (int v = 0; v < V; ++v) sum[v] += sign * row[b][v];
+        }
     }
     double next[V];
     bool finite = true;

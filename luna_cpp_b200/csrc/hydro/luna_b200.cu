@@ -103,10 +103,12 @@ struct luna_fv {
     DevArray<int32_t> steps;
     DevArray<luna::Counters> counters;
     // the mesh reordered for the step (geometry.cuh), rebuilt by every load_mesh
-    DevArray<unsigned char> geo_c01, geo_c2, geo_off01, geo_off2, geo_dt, geo_faces;
-    DevArray<unsigned int> geo_nbr, geo_face;
-    DevArray<int32_t> geo_slice_base, geo_order;
+    DevArray<unsigned char> geo_c01, geo_c2, geo_off01, geo_off2, geo_faces;
+    DevArray<unsigned int> geo_nbr;
+    DevArray<int32_t> geo_slice_base, geo_order, geo_stage_start, geo_stage_cells;
     DevArray<double> geo_angle;
+    int64_t tiles = 0, normal_tiles = 0;  // the sweep's tiles (tiles.h)
+    int normal_rows = 0, big_rows = 0;
     // the learned limiter: inputs written by the sweep, the network's logits; mlp_params is the caller's device vector
     DevArray<unsigned char> lim_features;
     DevArray<double> lim_alpha;
@@ -164,15 +166,16 @@ struct luna_fv {
         luna::GeometryDev<D, G> g;
         g.order = geo_order.ptr;
         g.slice_base = geo_slice_base.ptr;
+        g.stage_start = geo_stage_start.ptr;
+        g.stage_cells = geo_stage_cells.ptr;
         g.nbr = geo_nbr.ptr;
-        g.face = geo_face.ptr;
         g.c01 = reinterpret_cast<luna::Pair<G>*>(geo_c01.ptr);
         g.c2 = reinterpret_cast<G*>(geo_c2.ptr);
         g.off01 = reinterpret_cast<luna::Pair<G>*>(geo_off01.ptr);
         g.off2 = reinterpret_cast<G*>(geo_off2.ptr);
-        g.dt_rows = reinterpret_cast<luna::DtRow*>(geo_dt.ptr);
         g.faces = reinterpret_cast<luna::FaceRow<G>*>(geo_faces.ptr);
         g.max_angle = geo_angle.ptr;
+        g.threads = tiles * luna::kTileCells;
         return g;
     }
 
@@ -239,40 +242,32 @@ luna_status validate_mesh(const luna_mesh_desc* m, int dim, int64_t n) {
 
 // The reordered rows of the current mesh (geometry.cuh::k_geometry), in the policy's gradient type.
 template <int D, class G>
-luna_status build_geometry(luna_fv* fv, const std::vector<int32_t>& start) {
+luna_status build_geometry(luna_fv* fv, const luna::SweepTiles& tiles) {
     const size_t N = static_cast<size_t>(fv->n), F = static_cast<size_t>(fv->f);
-    // The sweep order: cells by list length (longest first) within windows of kOrderWindow cells; then the slices of
-    // 32 threads, each as many slots as its longest list.
-    std::vector<int32_t> order(N);
-    for (size_t i = 0; i < N; ++i) order[i] = static_cast<int32_t>(i);
-    for (size_t w0 = 0; w0 < N; w0 += luna::kOrderWindow) {
-        const size_t w1 = std::min(N, w0 + static_cast<size_t>(luna::kOrderWindow));
-        std::stable_sort(order.begin() + w0, order.begin() + w1, [&](int32_t a, int32_t b) {
-            return start[a + 1] - start[a] > start[b + 1] - start[b];
-        });
-    }
-    const size_t S = (N + 31) / 32;
-    std::vector<int32_t> base(S + 1, 0);
-    for (size_t s = 0; s < S; ++s) {
-        int longest = 0;
-        for (size_t t = 32 * s; t < 32 * s + 32 && t < N; ++t) longest = std::max(longest, start[order[t] + 1] - start[order[t]]);
-        base[s + 1] = base[s] + longest;
-    }
-    const size_t slots = static_cast<size_t>(base[S]) * 32 > 0 ? static_cast<size_t>(base[S]) * 32 : 1;
-    LUNA_TRY(upload(fv->geo_order, order.data(), N, false, fv->stream, "sweep order"));
-    LUNA_TRY(upload(fv->geo_slice_base, base.data(), S + 1, false, fv->stream, "slice bases"));
-    LUNA_TRY(fv->geo_nbr.alloc(slots, "entry neighbours"));
-    LUNA_TRY(fv->geo_face.alloc(slots, "entry faces"));
+    const size_t slots = tiles.local.size();
+    fv->tiles = tiles.tiles;
+    fv->normal_tiles = tiles.normal_tiles;
+    fv->normal_rows = tiles.normal_rows;
+    fv->big_rows = tiles.big_rows;
+    LUNA_TRY(upload(fv->geo_order, tiles.order.data(), tiles.order.size(), false, fv->stream, "sweep order"));
+    LUNA_TRY(upload(fv->geo_slice_base, tiles.slice_base.data(), tiles.slice_base.size(), false, fv->stream, "slice bases"));
+    LUNA_TRY(upload(fv->geo_stage_start, tiles.stage_start.data(), tiles.stage_start.size(), false, fv->stream, "tile row starts"));
+    LUNA_TRY(upload(fv->geo_stage_cells, tiles.stage_cells.data(), tiles.stage_cells.size() > 0 ? tiles.stage_cells.size() : 0, false, fv->stream,
+                    "tile rows"));
+    // the entries' staged rows; k_geometry adds the owned and tiny bits in place
+    LUNA_TRY(upload(fv->geo_nbr, tiles.local.data(), slots, false, fv->stream, "entry neighbours"));
     LUNA_TRY(fv->geo_c01.alloc(sizeof(luna::Pair<G>) * slots, "entry gradient rows"));
     LUNA_TRY(fv->geo_c2.alloc(sizeof(G) * slots, "entry gradient rows"));
     LUNA_TRY(fv->geo_off01.alloc(sizeof(luna::Pair<G>) * slots, "entry offsets"));
     LUNA_TRY(fv->geo_off2.alloc(sizeof(G) * slots, "entry offsets"));
-    LUNA_TRY(fv->geo_dt.alloc(sizeof(luna::DtRow) * (F > 0 ? F : 1), "dt rows"));
     LUNA_TRY(fv->geo_faces.alloc(sizeof(luna::FaceRow<G>) * (F > 0 ? F : 1), "face rows"));
     LUNA_TRY(fv->geo_angle.alloc(N, "face angles"));
-    luna::k_geometry<D, G><<<blocks(N, 128), 128, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->geometry_dev<D, G>());
-    LUNA_CUDA(cudaGetLastError());
-    // The slice bases' host copy must outlive the asynchronous upload.
+    const int64_t threads = tiles.tiles * luna::kTileCells;
+    if (threads > 0) {
+        luna::k_geometry<D, G><<<blocks(threads, 128), 128, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->geometry_dev<D, G>());
+        LUNA_CUDA(cudaGetLastError());
+    }
+    // The host vectors' contents must outlive the asynchronous uploads.
     LUNA_CUDA(cudaStreamSynchronize(fv->stream));
     return LUNA_OK;
 }
@@ -302,14 +297,37 @@ luna_status load_mesh(luna_fv* fv, const luna_mesh_desc* m) {
         LUNA_CUDA(cudaGetLastError());
     }
     if (fv->update == LUNA_UPDATE_PER_FACE) LUNA_TRY(fv->flux.alloc(F * (D + 2) > 0 ? F * (D + 2) : 1, "flux rows"));
-    // Lists in device memory are trusted as voronoi-cpp's; the sweep does not re-check them.
-    std::vector<int32_t> start(N + 1);
-    if (dev)
-        LUNA_CUDA(cudaMemcpy(start.data(), m->cell_face_start, (N + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost));
-    else
-        std::copy(m->cell_face_start, m->cell_face_start + N + 1, start.begin());
-    return fv->precision == LUNA_FP64 ? (D == 3 ? build_geometry<3, double>(fv, start) : build_geometry<2, double>(fv, start))
-                                      : (D == 3 ? build_geometry<3, float>(fv, start) : build_geometry<2, float>(fv, start));
+    // The sweep's tiles are cut on the host from the lists and the generators (copied back once per mesh when the
+    // caller's arrays are on the device). Lists in device memory are trusted as voronoi-cpp's; the sweep does not
+    // re-check them.
+    std::vector<int32_t> h_start, h_list, h_owner, h_neighbour;
+    std::vector<double> h_pos;
+    const int32_t *start = m->cell_face_start, *list = m->cell_face, *own = m->owner, *nbr = m->neighbour;
+    const double* pos = m->positions;
+    if (dev) {
+        h_start.resize(N + 1);
+        h_list.resize(2 * F);
+        h_owner.resize(F);
+        h_neighbour.resize(F);
+        h_pos.resize(N * D);
+        LUNA_CUDA(cudaMemcpy(h_start.data(), start, (N + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost));
+        if (F > 0) {
+            LUNA_CUDA(cudaMemcpy(h_list.data(), list, 2 * F * sizeof(int32_t), cudaMemcpyDeviceToHost));
+            LUNA_CUDA(cudaMemcpy(h_owner.data(), own, F * sizeof(int32_t), cudaMemcpyDeviceToHost));
+            LUNA_CUDA(cudaMemcpy(h_neighbour.data(), nbr, F * sizeof(int32_t), cudaMemcpyDeviceToHost));
+        }
+        LUNA_CUDA(cudaMemcpy(h_pos.data(), pos, N * D * sizeof(double), cudaMemcpyDeviceToHost));
+        start = h_start.data();
+        list = h_list.data();
+        own = h_owner.data();
+        nbr = h_neighbour.data();
+        pos = h_pos.data();
+    }
+    luna::SweepTiles tiles;
+    const std::string why = luna::build_sweep_tiles(D, static_cast<int64_t>(N), pos, m->box, start, list, own, nbr, tiles);
+    if (!why.empty()) return set_error(LUNA_EINVAL, "mesh: " + why);
+    return fv->precision == LUNA_FP64 ? (D == 3 ? build_geometry<3, double>(fv, tiles) : build_geometry<2, double>(fv, tiles))
+                                      : (D == 3 ? build_geometry<3, float>(fv, tiles) : build_geometry<2, float>(fv, tiles));
 }
 
 template <int D>
@@ -323,25 +341,41 @@ luna_status run_primitives(luna_fv* fv) {
     return LUNA_OK;
 }
 
-template <int D, bool Moving, bool Grad, class G>
-luna_status launch_sweep(luna_fv* fv, G* grad, double courant) {
+// The sweep's launches: the tiles within the row budget, then (rare) the single-cell tiles that stage more rows.
+template <int D, bool Moving, bool Grad, class G, int Limit>
+luna_status launch_sweep_tiles(luna_fv* fv, G* grad, double courant) {
     const auto m = fv->mesh_dev<D>();
     const auto geo = fv->geometry_dev<D, G>();
-    luna::LearnedInputs learned{reinterpret_cast<__nv_bfloat16*>(fv->lim_features.ptr), fv->lim_alpha.ptr};
+    const luna::LearnedInputs learned{reinterpret_cast<__nv_bfloat16*>(fv->lim_features.ptr), fv->lim_alpha.ptr};
+    auto kernel = luna::k_sweep_tiles<D, Moving, Grad, G, Limit>;
+    const int64_t groups[2][2] = {{0, fv->normal_tiles}, {fv->normal_tiles, fv->tiles}};
+    const int most_rows[2] = {fv->normal_rows, fv->big_rows};
+    for (int k = 0; k < 2; ++k) {
+        const int64_t first = groups[k][0], count = groups[k][1] - groups[k][0];
+        if (count <= 0) continue;
+        const size_t smem = sizeof(double) * luna::kStagedDoubles * static_cast<size_t>(most_rows[k]);
+        if (smem > 48 * 1024) LUNA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        kernel<<<static_cast<unsigned int>(count), luna::kTileCells, smem, fv->stream>>>(m, geo, static_cast<int>(first), fv->prims.ptr, grad, fv->w.ptr,
+                                                                                        courant, fv->counters.ptr, learned);
+        LUNA_CUDA(cudaGetLastError());
+    }
+    return LUNA_OK;
+}
+
+template <int D, bool Moving, bool Grad, class G>
+luna_status launch_sweep(luna_fv* fv, G* grad, double courant) {
     const bool learned_mode = Grad && fv->learned_inputs && fv->limiter == LUNA_LIMITER_FACE_CENTROID;
     {
         const long timed_ = fv->open_timed(1);
+        luna_status st = LUNA_OK;
         if (fv->limiter == LUNA_LIMITER_NONE)
-            luna::k_sweep_rows<D, Moving, Grad, G, 0><<<blocks(fv->n, kBlockCells), kBlockCells, 0, fv->stream>>>(m, geo, fv->prims.ptr, grad,
-                                                                                                             fv->w.ptr, courant, fv->counters.ptr, learned);
+            st = launch_sweep_tiles<D, Moving, Grad, G, 0>(fv, grad, courant);
         else if (learned_mode) {
-            if constexpr (sizeof(G) == sizeof(double))
-                luna::k_sweep_rows<D, Moving, Grad, G, 2><<<blocks(fv->n, kBlockCells), kBlockCells, 0, fv->stream>>>(m, geo, fv->prims.ptr, grad,
-                                                                                                                 fv->w.ptr, courant, fv->counters.ptr, learned);
+            if constexpr (sizeof(G) == sizeof(double)) st = launch_sweep_tiles<D, Moving, Grad, G, 2>(fv, grad, courant);
         } else
-            luna::k_sweep_rows<D, Moving, Grad, G, 1><<<blocks(fv->n, kBlockCells), kBlockCells, 0, fv->stream>>>(m, geo, fv->prims.ptr, grad,
-                                                                                                             fv->w.ptr, courant, fv->counters.ptr, learned);
+            st = launch_sweep_tiles<D, Moving, Grad, G, 1>(fv, grad, courant);
         fv->close_timed(timed_);
+        if (st != LUNA_OK) return st;
     }
     LUNA_CUDA(cudaGetLastError());
     if constexpr (sizeof(G) == sizeof(double)) {
@@ -980,7 +1014,7 @@ LUNA_API luna_status luna_fv_device_bytes(luna_fv* fv, int64_t* out) {
     b += fv->adj_fit.bytes() + fv->adj_face_bar.bytes() + fv->adj_wbar.bytes() + fv->adj_bbar.bytes() + fv->adj_boundbar.bytes();
     b += fv->adj_qbar.bytes() + fv->adj_flags.bytes() + fv->adj_bound_face.bytes();
     b += fv->geo_c01.bytes() + fv->geo_c2.bytes() + fv->geo_off01.bytes() + fv->geo_off2.bytes() + fv->geo_nbr.bytes();
-    b += fv->geo_face.bytes() + fv->geo_slice_base.bytes() + fv->geo_order.bytes() + fv->geo_dt.bytes() + fv->geo_faces.bytes();
+    b += fv->geo_slice_base.bytes() + fv->geo_order.bytes() + fv->geo_stage_start.bytes() + fv->geo_stage_cells.bytes() + fv->geo_faces.bytes();
     b += fv->geo_angle.bytes() + fv->lim_features.bytes() + fv->lim_alpha.bytes() + fv->lim_logits.bytes();
     *out = static_cast<int64_t>(b);
     return LUNA_OK;

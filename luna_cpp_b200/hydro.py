@@ -89,6 +89,7 @@ SIGNATURES = {
     "luna_mlp_train_step": ([P, P, P, P, I64, ctypes.c_float, P, P, P, I64, P], I),
     "luna_mlp_adam": ([P, P, P, P, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, I, P], I),
     "luna_fv_timings": ([P, P, I], I),
+    "luna_mesh_tiles": ([P, P, P, P, P, P, P], I),
 }
 
 PHASES = ("primitives", "sweep", "fluxes", "update", "drift")
@@ -134,6 +135,22 @@ def mesh_desc(mesh, keep: list) -> MeshDesc:
         d.box[a] = mesh.box[a] if a < len(mesh.box) else 0.0
     d.on_device = 0
     return d
+
+
+def mesh_tiles(mesh) -> dict:
+    """The sweep's tiles of a host mesh (luna_mesh_tiles; host work only): counts and arrays."""
+    keep = []
+    desc = mesh_desc(mesh, keep)
+    counts = np.zeros(6, np.int64)
+    check(lib().luna_mesh_tiles(ctypes.byref(desc), counts.ctypes.data, None, None, None, None, None))
+    tiles, normal, staged, slots, most, most_single = (int(c) for c in counts)
+    out = {"tiles": tiles, "normal_tiles": normal, "most_rows": most, "most_rows_single": most_single,
+           "order": np.empty(tiles * 128, np.int32), "slice_base": np.empty(tiles * 4 + 1, np.int32),
+           "stage_start": np.empty(tiles + 1, np.int32), "stage_cells": np.empty(staged, np.int32),
+           "local": np.empty(slots, np.uint32)}
+    check(lib().luna_mesh_tiles(ctypes.byref(desc), counts.ctypes.data, out["order"].ctypes.data, out["slice_base"].ctypes.data,
+                                out["stage_start"].ctypes.data, out["stage_cells"].ctypes.data, out["local"].ctypes.data))
+    return out
 
 
 class FiniteVolume:

@@ -64,6 +64,34 @@ def test_limiter_none_and_uniform_random_mesh(cuda):
     assert relative(gpu.get_state(), ora.get_state()) < 1e-12
 
 
+def ring_mesh():
+    """A cell with 600 faces (a centre point inside a ring of 600 points, in a lattice background): more neighbours
+    than one tile of the sweep stages, so it takes the single-cell tiles' launch with more shared memory."""
+    from luna_cpp_b200.mesh import build_mesh
+
+    th = np.linspace(0, 2 * np.pi, 600, endpoint=False)
+    ring = np.stack([0.5 + 0.2 * np.cos(th), 0.5 + 0.2 * np.sin(th)], 1)
+    g = (np.arange(24) + 0.5) / 24
+    background = np.stack(np.meshgrid(g, g, indexing="ij"), -1).reshape(-1, 2)
+    background = background[np.hypot(background[:, 0] - 0.5, background[:, 1] - 0.5) > 0.3]
+    return build_mesh(np.concatenate([[[0.5, 0.5]], ring, background]), (1.0, 1.0))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "grad32"])
+def test_cell_with_more_faces_than_a_tile(cuda, precision):
+    mesh = ring_mesh()
+    assert mesh.cell_face_start[1] - mesh.cell_face_start[0] == 600
+    q0 = rough_state(mesh.n_cells, dim=2) * mesh.volume[:, None]
+    gpu, ora = pair(mesh, q0, precision=precision)
+    tol = 1e-12 if precision == "fp64" else 1e-6  # grad32: the float gradients' rounding differs from the oracle's
+    for _ in range(3):
+        dt = ora.time_step(0.3)
+        assert abs(gpu.time_step(0.3) - dt) <= tol * dt
+        gpu.step(dt)
+        ora.step(dt)
+    assert relative(gpu.get_state(), ora.get_state()) < tol
+
+
 def test_blast_32_fp64_50_steps(cuda):
     """The plain-method configuration: 32^3 jittered (0.1) mesh, point blast, MUSCL-Hancock + HLLC, CFL 0.3, 50 steps,
     FP64, against the oracle: relative L1 <= 1e-12 for every conserved field (each side takes its own dt)."""
