@@ -1,0 +1,174 @@
+"""Measurement drivers for the benchmark configurations beside the headline step (the GPU path only; the oracle
+comparisons of the same configurations are GPU tests).
+
+- ``precision``: 3D static Voronoi mesh from nx^3 jittered generators; (a) the point blast, (b) the plane acoustic wave
+  (amplitude 1e-6, background rho 1, p 3/5); 100 steps of the FP64 step and of the reduced policies (FP32 face
+  arithmetic; FP32 gradients) on the FP64 run's dt schedule: relative L1 and Linf of every conserved field against the
+  FP64 run, the wave's error relative to its perturbation, conservation, and device time per step.
+- ``adjoint``: 2D Voronoi mesh from nx^2 jittered generators, the shear layer with a_k ~ N(0, 1) from the seed, 200
+  steps; d/da_k of int rho vy^2 dA at the final time by the hand-written adjoint with checkpoints every 20 steps,
+  against central differences (h = 1e-6) on the same dt schedule; device time of the forward and of the backward.
+
+    python -m luna_cpp_b200.studies precision --nx 128 --steps 100 --out precision.json
+    python -m luna_cpp_b200.studies adjoint --nx 512 --steps 200 --out adjoint.json
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import hydro
+from .mesh import build_mesh, jittered_points
+from .problems import acoustic_wave, cell_centres, conserved, point_blast
+
+GAMMA = 5.0 / 3.0
+
+
+def _phases_ms(fv) -> float:
+    return float(sum(ms for ms, _ in fv.timings().values()))
+
+
+def _field_errors(q, ref, base=None) -> dict:
+    """Per conserved field: sum |q - ref| / sum |ref| (relative L1), max |q - ref| / max |ref| (relative Linf); with
+    ``base``, also relative to the deviation from it (sum |q - ref| / sum |ref - base|)."""
+    d = np.abs(q - ref)
+    out = {"rel_l1": (d.sum(0) / np.abs(ref).sum(0)).tolist(), "rel_linf": (d.max(0) / np.abs(ref).max(0)).tolist(),
+           "max_abs": d.max(0).tolist()}
+    if base is not None:
+        dev = np.abs(ref - base).sum(0)
+        out["rel_l1_of_perturbation"] = [float(a / b) if b > 0 else None for a, b in zip(d.sum(0), dev)]
+    return out
+
+
+def precision(nx=128, steps=100, courant=0.3, seed=1, threads=0, log=print) -> dict:
+    t0 = time.time()
+    mesh = build_mesh(jittered_points((nx, nx, nx), jitter=0.1, seed=seed), threads=threads)
+    log(f"mesh {nx}^3: {mesh.n_cells} cells, {mesh.n_faces} faces, {time.time() - t0:.1f} s")
+    wave_background = conserved(np.array([1.0, 0.0, 0.0, 0.0, 0.6]), GAMMA)[None, :] * mesh.volume[:, None]
+    out = {"config": {"cells": mesh.n_cells, "faces": mesh.n_faces, "steps": steps, "courant": courant, "jitter": 0.1,
+                      "seed": seed, "schedule": "every policy replays the FP64 run's dt schedule"}}
+    for name, q0 in (("blast", point_blast(mesh, GAMMA)), ("wave", acoustic_wave(mesh, GAMMA))):
+        result = {}
+        ref = hydro.FiniteVolume(mesh, precision="fp64")
+        ref.set_state(q0)
+        ref.set_timing(True)
+        dts = []
+        for _ in range(steps):
+            dt = ref.time_step(courant)
+            ref.step(dt)
+            dts.append(dt)
+        q64 = ref.get_state()
+        result["fp64"] = {"device_ms_per_step": _phases_ms(ref) / steps, "fallbacks": int(ref.fallbacks()),
+                          "mass_drift": float(abs(q64[:, 0].sum() - q0[:, 0].sum()) / q0[:, 0].sum()),
+                          "energy_drift": float(abs(q64[:, 4].sum() - q0[:, 4].sum()) / q0[:, 4].sum()),
+                          "t_end": float(sum(dts))}
+        ref.close()
+        for policy in ("fp32", "grad32"):
+            fv = hydro.FiniteVolume(mesh, precision=policy)
+            fv.set_state(q0)
+            fv.set_timing(True)
+            for dt in dts:
+                fv.time_step(courant)
+                fv.step(dt)
+            q = fv.get_state()
+            r = {"device_ms_per_step": _phases_ms(fv) / steps}
+            r.update(_field_errors(q, q64, wave_background if name == "wave" else None))
+            r["mass_drift"] = float(abs(q[:, 0].sum() - q0[:, 0].sum()) / q0[:, 0].sum())
+            r["energy_drift"] = float(abs(q[:, 4].sum() - q0[:, 4].sum()) / q0[:, 4].sum())
+            fv.close()
+            r["speedup_vs_fp64"] = result["fp64"]["device_ms_per_step"] / r["device_ms_per_step"]
+            result[policy] = r
+            log(f"{name} {policy}: {r['device_ms_per_step']:.3f} ms/step ({r['speedup_vs_fp64']:.2f}x), "
+                f"max rel L1 {max(r['rel_l1']):.2e}")
+        out[name] = result
+    return out
+
+
+def adjoint(nx=512, steps=200, every=20, h=1e-6, seed=3, courant=0.3, threads=0, log=print) -> dict:
+    import torch
+
+    from .autograd import kinetic_y, last_dts, rollout, shear_layer_torch
+
+    t0 = time.time()
+    mesh = build_mesh(jittered_points((nx, nx), jitter=0.1, seed=1), threads=threads)
+    log(f"mesh {nx}^2: {mesh.n_cells} cells, {mesh.n_faces} faces, {time.time() - t0:.1f} s")
+    dev = torch.device("cuda")
+    centres = torch.tensor(cell_centres(mesh), device=dev)
+    volume = torch.tensor(mesh.volume, device=dev)
+    coefficients = np.random.default_rng(seed).standard_normal(8)
+    a = torch.tensor(coefficients, device=dev, requires_grad=True)
+    fv = hydro.FiniteVolume(mesh)
+
+    # the plain forward (no checkpoints), for the cost ratio
+    with torch.no_grad():
+        fv.set_state(shear_layer_torch(centres, volume, a))
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for _ in range(steps):
+        fv.step(fv.time_step(courant))
+    torch.cuda.synchronize()
+    plain = time.perf_counter() - t
+
+    t = time.perf_counter()
+    out = rollout(shear_layer_torch(centres, volume, a), fv, steps, courant=courant, every=every)
+    J = kinetic_y(out)
+    torch.cuda.synchronize()
+    forward = time.perf_counter() - t
+    dts = last_dts(out)
+    t = time.perf_counter()
+    J.backward()
+    torch.cuda.synchronize()
+    backward = time.perf_counter() - t
+    grad = a.grad.detach().cpu().numpy()
+
+    fd = np.zeros(8)
+    t = time.perf_counter()
+    with torch.no_grad():
+        for k in range(8):
+            e = torch.zeros(8, dtype=torch.float64, device=dev)
+            e[k] = h
+            jp = kinetic_y(rollout(shear_layer_torch(centres, volume, a + e), fv, steps, courant=courant, every=every, dts=dts))
+            jm = kinetic_y(rollout(shear_layer_torch(centres, volume, a - e), fv, steps, courant=courant, every=every, dts=dts))
+            fd[k] = (jp - jm).item() / (2 * h)
+    fd_time = time.perf_counter() - t
+    err = np.abs(grad - fd)
+    res = {"config": {"cells": mesh.n_cells, "faces": mesh.n_faces, "steps": steps, "checkpoint_every": every, "h": h,
+                      "seed": seed, "coefficients": coefficients.tolist(), "t_end": float(sum(dts))},
+           "objective": float(J.item()), "gradient_adjoint": grad.tolist(), "gradient_fd": fd.tolist(),
+           "max_abs_error_over_max_fd": float(err.max() / np.abs(fd).max()),
+           "rel_error_per_coefficient": (err / np.abs(fd)).tolist(),
+           "seconds": {"plain_forward": plain, "checkpointed_forward": forward, "backward": backward,
+                       "finite_differences_16_rollouts": fd_time},
+           "backward_over_plain_forward": backward / plain}
+    log(json.dumps(res["seconds"]))
+    log(f"adjoint vs central differences: max |error| / max |fd| = {res['max_abs_error_over_max_fd']:.2e}")
+    fv.close()
+    return res
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("study", choices=["precision", "adjoint"])
+    ap.add_argument("--nx", type=int)
+    ap.add_argument("--steps", type=int)
+    ap.add_argument("--threads", type=int, default=0)
+    ap.add_argument("--out")
+    args = ap.parse_args()
+    kw = {"threads": args.threads}
+    if args.nx:
+        kw["nx"] = args.nx
+    if args.steps:
+        kw["steps"] = args.steps
+    res = precision(**kw) if args.study == "precision" else adjoint(**kw)
+    text = json.dumps(res, indent=1)
+    if args.out:
+        with open(args.out, "w") as f:
+            f.write(text)
+    print(text)
+
+
+if __name__ == "__main__":
+    main()

@@ -119,6 +119,31 @@ def test_reduced_policy_matches_oracle_policy(cuda, precision):
     assert relative(gpu.get_state(), ora.get_state()) < 1e-6
 
 
+@pytest.mark.parametrize("problem", ["blast", "wave"])
+def test_precision_config_128_fp64_against_oracle(cuda, problem):
+    """The precision configuration's FP64 reference run: 128^3 jittered (0.1) mesh, the point blast or the 1e-6 plane
+    acoustic wave, 100 steps on the oracle's dt schedule (each dt also checked). Blast: relative L1 <= 1e-12 for every
+    conserved field. Wave: the fields are O(1) backgrounds plus a 1e-6 perturbation (and rounding-level transverse
+    momenta), so the difference is measured against the perturbation: sum |gpu - oracle| / sum |oracle - background|
+    (x-momentum: against itself) <= 1e-8 for density, x-momentum and energy, i.e. ~1e-14 of the fields. (The reduced
+    policies are measured against this run by luna_cpp_b200.studies.precision.)"""
+    mesh = jittered_mesh(128)
+    q0 = point_blast(mesh) if problem == "blast" else acoustic_wave(mesh, amplitude=1e-6)
+    gpu, ora = pair(mesh, q0)
+    for _ in range(100):
+        dt = ora.time_step(0.3)
+        assert abs(gpu.time_step(0.3) - dt) <= 1e-13 * dt
+        gpu.step(dt)
+        ora.step(dt)
+    got, want = gpu.get_state(), ora.get_state()
+    if problem == "blast":
+        assert np.all(rel_l1(got, want) < 1e-12)
+    else:
+        perturbation = np.abs(want - acoustic_wave(mesh, amplitude=0.0)).sum(0)
+        err = np.abs(got - want).sum(0)
+        assert np.all(err[[0, 1, 4]] / perturbation[[0, 1, 4]] < 1e-8), err / perturbation
+
+
 @pytest.mark.parametrize("problem", ["wave", "blast"])
 def test_reduced_policies_against_fp64(cuda, problem):
     """The reduced policies against FP64 (20 steps, each run its own dt): relative L1 of Q within 1e-5 for both. On the
