@@ -5,12 +5,18 @@ comparisons of the same configurations are GPU tests).
   (amplitude 1e-6, background rho 1, p 3/5); 100 steps of the FP64 step and of the reduced policies (FP32 face
   arithmetic; FP32 gradients) on the FP64 run's dt schedule: relative L1 and Linf of every conserved field against the
   FP64 run, the wave's error relative to its perturbation, conservation, and device time per step.
+- ``moving``: the moving-mesh point blast (generators on the 2^-30 snapping grid, moved with the gas plus the
+  roundness velocity, fluxes on the old and the new faces) on nx^3 jittered generators to t_end, FP32 face
+  arithmetic with FP64 state by default (``riemann32``): steps taken, the hydro part's device time and cell-updates/s
+  (the remesh, voronoi-cpp's job, is timed apart, as the reference's hydro part is), the radial density profile; and
+  ``timed_steps`` moving steps at ``timed_nx``^3 for the hydro part's throughput at that size.
 - ``adjoint``: 2D Voronoi mesh from nx^2 jittered generators, the shear layer with a_k ~ N(0, 1) from the seed, 200
   steps; d/da_k of int rho vy^2 dA at the final time by the hand-written adjoint with checkpoints every 20 steps,
   against central differences (h = 1e-6) on the same dt schedule; device time of the forward and of the backward.
 
     python -m luna_cpp_b200.studies precision --nx 128 --steps 100 --out precision.json
     python -m luna_cpp_b200.studies adjoint --nx 512 --steps 200 --out adjoint.json
+    python -m luna_cpp_b200.studies moving --nx 32 --out moving.json
 """
 from __future__ import annotations
 
@@ -87,6 +93,76 @@ def precision(nx=128, steps=100, courant=0.3, seed=1, threads=0, log=print) -> d
     return out
 
 
+def radial_profile(mesh, q, bins=32) -> np.ndarray:
+    """Volume-weighted mean density in ``bins`` equal shells of radius from the box centre, out to half the box."""
+    c = cell_centres(mesh) - 0.5 * np.asarray(mesh.box)
+    r = np.sqrt((c * c).sum(1)) / (0.5 * min(mesh.box))
+    b = np.minimum((r * bins).astype(int), bins)
+    mass = np.bincount(b, weights=q[:, 0], minlength=bins + 1)[:bins]
+    vol = np.bincount(b, weights=mesh.volume, minlength=bins + 1)[:bins]
+    return np.where(vol > 0, mass / np.where(vol > 0, vol, 1.0), 0.0)
+
+
+def snapped_jittered_mesh(nx, dim=3, seed=1, threads=0):
+    """A jittered mesh whose generators sit on the moving step's 2^-30 snapping grid."""
+    step = 2.0 ** -30
+    pts = np.round(jittered_points((nx,) * dim, jitter=0.1, seed=seed) / step) * step
+    return build_mesh(pts, threads=threads)
+
+
+def run_moving(fv, t_end, courant=0.3, threads=0, max_steps=100000, log=print):
+    """Moving steps to t_end (the last step shortened); returns (steps, t, hydro ms, remesh s)."""
+    t, steps, remesh_s = 0.0, 0, 0.0
+
+    def remesh(pos):
+        nonlocal remesh_s
+        t0 = time.perf_counter()
+        m = build_mesh(pos, threads=threads)
+        remesh_s += time.perf_counter() - t0
+        return m
+
+    fv.set_timing(True)
+    fv.timings()
+    while t < t_end and steps < max_steps:
+        dt = min(fv.time_step(courant), t_end - t)
+        fv.step_moving(dt, remesh)
+        t += dt
+        steps += 1
+    return steps, t, _phases_ms(fv), remesh_s
+
+
+def moving(nx=32, t_end=0.05, precision_policy="fp32", timed_nx=128, timed_steps=5, courant=0.3, threads=0, log=print) -> dict:
+    t0 = time.time()
+    mesh = snapped_jittered_mesh(nx, threads=threads)
+    log(f"mesh {nx}^3: {mesh.n_cells} cells, {time.time() - t0:.1f} s")
+    q0 = point_blast(mesh, GAMMA)
+    out = {"config": {"cells": mesh.n_cells, "t_end": t_end, "precision": precision_policy, "courant": courant,
+                      "problem": "point blast, E = 1 within 2 cell widths, moving mesh"}}
+    fv = hydro.FiniteVolume(mesh, precision=precision_policy, motion="moving")
+    fv.set_state(q0)
+    steps, t, hydro_ms, remesh_s = run_moving(fv, t_end, courant, threads, log=log)
+    q = fv.get_state()
+    out["run"] = {"steps": steps, "t": t, "hydro_device_ms": hydro_ms, "remesh_host_s": remesh_s,
+                  "hydro_cell_updates_per_s": mesh.n_cells * steps / (hydro_ms * 1e-3),
+                  "mass_drift": float(abs(q[:, 0].sum() - q0[:, 0].sum()) / q0[:, 0].sum()),
+                  "energy_drift": float(abs(q[:, 4].sum() - q0[:, 4].sum()) / q0[:, 4].sum()),
+                  "radial_density_profile": radial_profile(fv.mesh, q).tolist()}
+    log(f"moving {nx}^3 to t = {t:.4f}: {steps} steps, hydro {hydro_ms:.1f} ms, remesh {remesh_s:.1f} s")
+    fv.close()
+    if timed_steps > 0:
+        t0 = time.time()
+        big = snapped_jittered_mesh(timed_nx, threads=threads)
+        log(f"mesh {timed_nx}^3: {time.time() - t0:.1f} s")
+        fv = hydro.FiniteVolume(big, precision=precision_policy, motion="moving")
+        fv.set_state(point_blast(big, GAMMA))
+        steps, t, hydro_ms, remesh_s = run_moving(fv, 1.0, courant, threads, max_steps=timed_steps, log=log)
+        out["timed"] = {"cells": big.n_cells, "steps": steps, "hydro_device_ms_per_step": hydro_ms / steps,
+                        "hydro_cell_updates_per_s": big.n_cells * steps / (hydro_ms * 1e-3), "remesh_host_s_per_step": remesh_s / steps}
+        log(f"moving {timed_nx}^3: {hydro_ms / steps:.3f} ms/step hydro, remesh {remesh_s / steps:.1f} s/step")
+        fv.close()
+    return out
+
+
 def adjoint(nx=512, steps=200, every=20, h=1e-6, seed=3, courant=0.3, threads=0, log=print) -> dict:
     import torch
 
@@ -151,7 +227,7 @@ def adjoint(nx=512, steps=200, every=20, h=1e-6, seed=3, courant=0.3, threads=0,
 
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("study", choices=["precision", "adjoint"])
+    ap.add_argument("study", choices=["precision", "adjoint", "moving"])
     ap.add_argument("--nx", type=int)
     ap.add_argument("--steps", type=int)
     ap.add_argument("--threads", type=int, default=0)
@@ -162,7 +238,9 @@ def main():
         kw["nx"] = args.nx
     if args.steps:
         kw["steps"] = args.steps
-    res = precision(**kw) if args.study == "precision" else adjoint(**kw)
+    if args.study == "moving":
+        kw.pop("steps", None)
+    res = {"precision": precision, "adjoint": adjoint, "moving": moving}[args.study](**kw)
     text = json.dumps(res, indent=1)
     if args.out:
         with open(args.out, "w") as f:
