@@ -69,6 +69,7 @@ struct GeometryDev {
     G* __restrict__ off2;                     // z (3D)
     FaceRow<G>* __restrict__ faces;           // [F]
     double* __restrict__ max_angle;           // [N]
+    double* __restrict__ reach2;              // [N]: the largest |x_f - c_i|^2 over the cell's faces
     int64_t threads;                          // tiles * kTileCells
 };
 
@@ -133,6 +134,7 @@ __global__ void __launch_bounds__(128) k_geometry(MeshDev<D> m, GeometryDev<D, G
         }
     const double tiny = 1e-6 * surface;
     const bool any_tiny = smallest < tiny;
+    double reach2 = 0;
     for (int k = first; k < end; ++k) {
         const int32_t e = m.list[k];
         const int f = list_face(e);
@@ -166,6 +168,15 @@ __global__ void __launch_bounds__(128) k_geometry(MeshDev<D> m, GeometryDev<D, G
         m.face_offset(f, i, off);
         g.off01[slot] = Pair<G>{static_cast<G>(off[0]), static_cast<G>(off[1])};
         if constexpr (D == 3) g.off2[slot] = static_cast<G>(off[2]);
+        {
+            double r2 = 0;
+#pragma unroll
+            for (int a = 0; a < D; ++a) {
+                const double o = static_cast<double>(static_cast<G>(off[a]));
+                r2 += o * o;
+            }
+            reach2 = fmax(reach2, r2);
+        }
         const bool tiny_face = any_tiny && magnitude < tiny;
         g.nbr[slot] = (g.nbr[slot] & kIndexMask) | (owned ? kOwnedBit : 0u) | (tiny_face ? kTinyBit : 0u);
         if (owned) {  // the face row, written once by the owner
@@ -196,6 +207,7 @@ __global__ void __launch_bounds__(128) k_geometry(MeshDev<D> m, GeometryDev<D, G
         }
     }
     g.max_angle[i] = max_angle;
+    g.reach2[i] = reach2;
 }
 
 // The sweep over the reordered rows (Sweep<Moving, Grad>::operator(), finite_volume.hpp:463-569), one block per tile:
@@ -239,7 +251,7 @@ constexpr double kAlphaCap = 2.0;  // the largest steepening the learned limiter
 template <int D, bool Moving, bool Grad, class G, int Limit, int KB = LUNA_SWEEP_BATCH, int MINB = LUNA_SWEEP_MIN_BLOCKS>
 __global__ void __launch_bounds__(kTileCells, MINB) k_sweep_tiles(MeshDev<D> m, GeometryDev<D, G> geo, int tile0, const double* __restrict__ prims,
                                                                G* __restrict__ grad_out, double* __restrict__ w_out, double courant,
-                                                               Counters* __restrict__ ctr, LearnedInputs learned) {
+                                                               double round_off2, Counters* __restrict__ ctr, LearnedInputs learned) {
     extern __shared__ double2 staged_rows[];
     double* rows = reinterpret_cast<double*>(staged_rows);
     constexpr int V = D + 2, GS = grad_stride<D>(), R = kStagedDoubles;
@@ -427,7 +439,31 @@ __global__ void __launch_bounds__(kTileCells, MINB) k_sweep_tiles(MeshDev<D> m, 
                 for (int v = 0; v < V; ++v) alpha[v] = num[v] / den[v];
                 write_learned_inputs<D>(learned, i, Wi, ci, ri, g, lo, hi, alpha);
             }
-            if constexpr (Limit == 1 && exact) {
+            // A slope that moves every face value of its variable by at most the policy's round-off of the variable's
+            // scale (|g_v| max_k |r_k| <= e s_v; s = |rho|, |v| + c for the velocity components, |P|; e = 2^-50 when
+            // the face states are solved in double, 2^-24 when the Riemann solve rounds them to float) is round-off of
+            // a uniform region, where a clip could change face states only at that level; when every variable's slope
+            // is such, walk 2 is left out. The step then differs from the reference's arithmetic only at that level
+            // in those cells' face states. round_off2 = e^2.
+            bool round_off_only = false;
+            if constexpr (Limit == 1) {
+                const double reach2 = geo.reach2[i];
+                const double kNoise2 = round_off2;
+                double speed2 = 0;
+#pragma unroll
+                for (int a = 0; a < D; ++a) speed2 += Wi[1 + a] * Wi[1 + a];
+                const double signal = sqrt(speed2) + ci;
+                round_off_only = true;
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    double gg = 0;
+#pragma unroll
+                    for (int a = 0; a < D; ++a) gg += static_cast<double>(g[D * v + a]) * static_cast<double>(g[D * v + a]);
+                    const double scale = (v >= 1 && v <= D) ? signal : fabs(Wi[v]);
+                    round_off_only = round_off_only && gg * reach2 <= kNoise2 * (scale * scale);
+                }
+            }
+            if constexpr (Limit == 1 && exact) if (!round_off_only) {
                 // The clip (Sweep walk 2, finite_volume.hpp:538-565): each face in list order (tiny ones left out)
                 // scales a variable's gradient so that its face value stays in [lo, hi].
                 constexpr int kClipBatch = LUNA_CLIP_BATCH;
@@ -466,7 +502,7 @@ __global__ void __launch_bounds__(kTileCells, MINB) k_sweep_tiles(MeshDev<D> m, 
                     }
                 }
             }
-            if constexpr (Limit == 1 && !exact) {
+            if constexpr (Limit == 1 && !exact) if (!round_off_only) {
                 // The float policies' clip (the range is of differences, lo <= 0 <= hi) in its min-factor form
                 // (finite_volume.hpp:1008-1034): scaling g by each face's factor in list order ends at g times the
                 // smallest factor, since after a clip the face sits on its bound and a later face clips again only

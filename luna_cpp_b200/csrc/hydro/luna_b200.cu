@@ -106,7 +106,7 @@ struct luna_fv {
     DevArray<unsigned char> geo_c01, geo_c2, geo_off01, geo_off2, geo_faces;
     DevArray<unsigned int> geo_nbr;
     DevArray<int32_t> geo_slice_base, geo_order, geo_stage_start, geo_stage_cells;
-    DevArray<double> geo_angle;
+    DevArray<double> geo_angle, geo_reach2;
     int64_t tiles = 0, normal_tiles = 0;  // the sweep's tiles (tiles.h)
     int normal_rows = 0, big_rows = 0;
     // the learned limiter: inputs written by the sweep, the network's logits; mlp_params is the caller's device vector
@@ -175,6 +175,7 @@ struct luna_fv {
         g.off2 = reinterpret_cast<G*>(geo_off2.ptr);
         g.faces = reinterpret_cast<luna::FaceRow<G>*>(geo_faces.ptr);
         g.max_angle = geo_angle.ptr;
+        g.reach2 = geo_reach2.ptr;
         g.threads = tiles * luna::kTileCells;
         return g;
     }
@@ -262,6 +263,7 @@ luna_status build_geometry(luna_fv* fv, const luna::SweepTiles& tiles) {
     LUNA_TRY(fv->geo_off2.alloc(sizeof(G) * slots, "entry offsets"));
     LUNA_TRY(fv->geo_faces.alloc(sizeof(luna::FaceRow<G>) * (F > 0 ? F : 1), "face rows"));
     LUNA_TRY(fv->geo_angle.alloc(N, "face angles"));
+    LUNA_TRY(fv->geo_reach2.alloc(N, "cell reach"));
     const int64_t threads = tiles.tiles * luna::kTileCells;
     if (threads > 0) {
         luna::k_geometry<D, G><<<blocks(threads, 128), 128, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->geometry_dev<D, G>());
@@ -350,13 +352,15 @@ luna_status launch_sweep_tiles(luna_fv* fv, G* grad, double courant) {
     auto kernel = luna::k_sweep_tiles<D, Moving, Grad, G, Limit>;
     const int64_t groups[2][2] = {{0, fv->normal_tiles}, {fv->normal_tiles, fv->tiles}};
     const int most_rows[2] = {fv->normal_rows, fv->big_rows};
+    // the round-off of the face states, squared: double face states (FP64, grad32), float ones (riemann32)
+    const double round_off2 = fv->precision == LUNA_FP32 ? 0x1p-48 : 0x1p-100;
     for (int k = 0; k < 2; ++k) {
         const int64_t first = groups[k][0], count = groups[k][1] - groups[k][0];
         if (count <= 0) continue;
         const size_t smem = sizeof(double) * luna::kStagedDoubles * static_cast<size_t>(most_rows[k]);
         if (smem > 48 * 1024) LUNA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
         kernel<<<static_cast<unsigned int>(count), luna::kTileCells, smem, fv->stream>>>(m, geo, static_cast<int>(first), fv->prims.ptr, grad, fv->w.ptr,
-                                                                                        courant, fv->counters.ptr, learned);
+                                                                                        courant, round_off2, fv->counters.ptr, learned);
         LUNA_CUDA(cudaGetLastError());
     }
     return LUNA_OK;
@@ -1015,7 +1019,7 @@ LUNA_API luna_status luna_fv_device_bytes(luna_fv* fv, int64_t* out) {
     b += fv->adj_qbar.bytes() + fv->adj_flags.bytes() + fv->adj_bound_face.bytes();
     b += fv->geo_c01.bytes() + fv->geo_c2.bytes() + fv->geo_off01.bytes() + fv->geo_off2.bytes() + fv->geo_nbr.bytes();
     b += fv->geo_slice_base.bytes() + fv->geo_order.bytes() + fv->geo_stage_start.bytes() + fv->geo_stage_cells.bytes() + fv->geo_faces.bytes();
-    b += fv->geo_angle.bytes() + fv->lim_features.bytes() + fv->lim_alpha.bytes() + fv->lim_logits.bytes();
+    b += fv->geo_angle.bytes() + fv->geo_reach2.bytes() + fv->lim_features.bytes() + fv->lim_alpha.bytes() + fv->lim_logits.bytes();
     *out = static_cast<int64_t>(b);
     return LUNA_OK;
 }
