@@ -195,6 +195,17 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def max_over_ranks(x: float, dist=None, device="cuda") -> float:
+    """The largest value of x over the ranks (every rank gets it): the job's time is its slowest replica's."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def timed_steps(fv, steps, torch):
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
@@ -235,13 +246,6 @@ def main():
         if dist is not None:
             dist.barrier()
 
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     results = {}
     for prec in ("fp32", "fp64") if args.precision == "both" else (args.precision,):
         fv = hydro.FiniteVolume(mesh, precision=prec)
@@ -258,7 +262,7 @@ def main():
         barrier()
         phases = fv.timings(reset=True)
         fv.set_timing(False)
-        ms = max_over_ranks(ms)
+        ms = max_over_ranks(ms, dist)
         results[prec] = {"ms": ms, "phases": phases, "clocks": clocks.summary(), "fallbacks": fv.fallbacks(), "fv": fv}
 
     if args.precision != "both":
@@ -285,7 +289,7 @@ def main():
         fv.step(fv.time_step(0.3))
         hydro.check(hydro.lib().luna_fv_get_state(fv.handle, host_out.data_ptr(), 0))
     torch.cuda.synchronize()
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
     barrier()
 
     if rank == 0:
