@@ -98,7 +98,8 @@ LUNA_API luna_status luna_fv_step(luna_fv* fv, double dt);
 /* fallbacks() (finite_volume.hpp:230-238): face sides of the last step that fell back to the cell's state. */
 LUNA_API luna_status luna_fv_fallbacks(luna_fv* fv, int64_t* out);
 /* The error word of the kernels since the last call (bit 0: non-finite dt term, bit 1: non-finite state after an update,
- * bit 2: a list entry out of range); cleared by the read. */
+ * bit 2: a list entry out of range, bit 4: the learned limiter's tensor-core completion wait gave up); cleared by the
+ * read. */
 LUNA_API luna_status luna_fv_error_word(luna_fv* fv, uint32_t* out);
 
 /* The moving step (step_moving, finite_volume.hpp:1497-1519), split around the caller's remesh because the mesh update
@@ -148,7 +149,9 @@ LUNA_API luna_status luna_fv_set_limiter_mlp(luna_fv* fv, const float* params, i
  * of 5), and the unlimited gradients [N][D + 2][D] (double). For building training data. */
 LUNA_API luna_status luna_fv_limiter_inputs(luna_fv* fv, void* features, double* alpha, double* gradients);
 /* The network's kernels on caller buffers (device): parameters FP32 [luna_mlp_param_count()]; features BF16 [n][32];
- * logits FP32 [n][16] (the first D + 2 used). train_step: the gradient of scale * sum w (sigmoid(o) - t)^2 over rows
+ * logits FP32 [n][16] (the first D + 2 used); features and logits 16-byte aligned. forward: on the 5th-generation tensor
+ * cores (tcgen05, accumulators in tensor memory); it synchronises the stream to read its completion status
+ * (LUNA_ETIMEOUT if a bounded wait gave up). train_step: the gradient of scale * sum w (sigmoid(o) - t)^2 over rows
  * (targets t and weights w FP32 [n][5]) into grad, the loss into *loss (device); workspace of
  * luna_mlp_train_workspace_floats(n) floats; deterministic. adam: one Adam update (step counts from 1). */
 LUNA_API int64_t luna_mlp_param_count(void);

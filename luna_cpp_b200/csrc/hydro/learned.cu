@@ -6,6 +6,7 @@
 
 #include "luna_b200.h"
 #include "mlp.cuh"
+#include "mlp_tc.cuh"
 
 namespace luna {
 luna_status report_error(luna_status s, const std::string& what);
@@ -21,7 +22,32 @@ luna_status check_launch(const char* what) {
     return LUNA_OK;
 }
 
+// The standalone forward's error word (luna_mlp_forward).
+__device__ unsigned long long g_forward_error;
+
 }  // namespace
+
+namespace luna {
+namespace mlp {
+
+luna_status forward_tc(const float* params, const __nv_bfloat16* x, int n, float* logits, unsigned long long* error, cudaStream_t stream) {
+    if (n <= 0) return LUNA_OK;
+    const int smem = static_cast<int>(sizeof(SmemTc));
+    static bool configured = false;
+    if (!configured) {
+        const cudaError_t e = cudaFuncSetAttribute(k_mlp_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return fail(LUNA_ECUDA, std::string("k_mlp_forward_tc shared memory: ") + cudaGetErrorString(e));
+        configured = true;
+    }
+    // a grid-stride loop over tiles of 128 rows; at most two CTAs an SM hold TMEM (128 of its 512 columns each)
+    const int64_t tiles = (static_cast<int64_t>(n) + kTcRows - 1) / kTcRows;
+    const int blocks = static_cast<int>(tiles < 148 * 2 ? tiles : 148 * 2);
+    k_mlp_forward_tc<<<blocks, 128, smem, stream>>>(params, x, n, logits, error);
+    return check_launch("k_mlp_forward_tc");
+}
+
+}  // namespace mlp
+}  // namespace luna
 
 extern "C" {
 
@@ -35,12 +61,20 @@ LUNA_API int64_t luna_mlp_train_workspace_floats(int64_t n) {
 LUNA_API luna_status luna_mlp_forward(const float* params, const void* features, int64_t n, float* logits, void* stream) {
     if (!params || !features || !logits || n < 0 || n >= (int64_t(1) << 31)) return fail(LUNA_EINVAL, "luna_mlp_forward: bad argument");
     if (n == 0) return LUNA_OK;
-    const int64_t warps = (n + luna::mlp::kRowsPerWarp - 1) / luna::mlp::kRowsPerWarp;
-    int blocks = static_cast<int>((warps + luna::mlp::kWarps - 1) / luna::mlp::kWarps);
-    blocks = blocks < 148 * 8 ? blocks : 148 * 8;
-    luna::mlp::k_mlp_forward<<<blocks, 128, 0, static_cast<cudaStream_t>(stream)>>>(params, static_cast<const __nv_bfloat16*>(features),
-                                                                                     static_cast<int>(n), logits);
-    return check_launch("k_mlp_forward");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    void* word = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&word, g_forward_error);
+    if (e == cudaSuccess) e = cudaMemsetAsync(word, 0, sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return fail(LUNA_ECUDA, std::string("luna_mlp_forward error word: ") + cudaGetErrorString(e));
+    const luna_status st = luna::mlp::forward_tc(params, static_cast<const __nv_bfloat16*>(features), static_cast<int>(n), logits,
+                                                 static_cast<unsigned long long*>(word), s);
+    if (st != LUNA_OK) return st;
+    unsigned long long bits = 0;
+    e = cudaMemcpyAsync(&bits, word, sizeof(bits), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(LUNA_ECUDA, std::string("luna_mlp_forward: ") + cudaGetErrorString(e));
+    if (bits & luna::mlp::kTcTimeoutBit) return fail(LUNA_ETIMEOUT, "luna_mlp_forward: a tensor-core completion wait gave up");
+    return LUNA_OK;
 }
 
 LUNA_API luna_status luna_mlp_train_step(const float* params, const void* features, const float* target, const float* weight, int64_t n,

@@ -386,10 +386,12 @@ luna_status launch_sweep(luna_fv* fv, G* grad, double courant) {
         if (learned_mode && fv->apply_learned) {  // the network's factors, then the gradients scaled
             const long timed_ = fv->open_timed(1);
             if (fv->mlp_params) {
-                const int64_t warps = (fv->n + 15) / 16;
-                const int nb = static_cast<int>(std::min<int64_t>((warps + 3) / 4, 148 * 8));
-                luna::mlp::k_mlp_forward<<<nb, 128, 0, fv->stream>>>(fv->mlp_params, reinterpret_cast<const __nv_bfloat16*>(fv->lim_features.ptr),
-                                                                     static_cast<int>(fv->n), fv->lim_logits.ptr);
+                const luna_status st = luna::mlp::forward_tc(fv->mlp_params, reinterpret_cast<const __nv_bfloat16*>(fv->lim_features.ptr),
+                                                             static_cast<int>(fv->n), fv->lim_logits.ptr, &fv->counters.ptr->error, fv->stream);
+                if (st != LUNA_OK) {
+                    fv->close_timed(timed_);
+                    return st;
+                }
             }
             luna::k_apply_factors<D><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(static_cast<int>(fv->n), grad, fv->lim_alpha.ptr, fv->lim_logits.ptr,
                                                                                  fv->mlp_params != nullptr);
@@ -811,6 +813,7 @@ LUNA_API luna_status luna_fv_time_step(luna_fv* fv, double courant, double* dt_o
     std::memcpy(&dt, &fv->host_counters->dt_bits, sizeof(dt));
     *dt_out = dt;
     if (fv->host_counters->error & 1ull) return set_error(LUNA_ENONFINITE, "a time-step term is not finite");
+    if (fv->host_counters->error & 16ull) return set_error(LUNA_ETIMEOUT, "the learned limiter's tensor-core completion wait gave up");
     return LUNA_OK;
 }
 

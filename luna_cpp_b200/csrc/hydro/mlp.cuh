@@ -7,7 +7,7 @@
 //
 // Kernels (one warp = 16 rows, m16n8k16 BF16 MMA with FP32 accumulation; the activations of a warp stay in registers
 // from layer to layer: the accumulator fragment of one layer is the A fragment of the next):
-//   k_mlp_forward   logits [n][16] of feature rows [n][32] (BF16)
+//   k_mlp_forward   logits [n][16] of feature rows [n][32] (BF16); inference runs forward_tc (tcgen05) instead
 //   k_mlp_train     forward + backward of the loss sum_r sum_c w_rc (sigmoid(o_rc) - t_rc)^2 over 64 rows a block,
 //                   the block's gradient written to its own slot (deterministic: no atomics)
 //   k_mlp_reduce    the slots summed in order, scaled by 1 / sum(w)
@@ -15,10 +15,17 @@
 #pragma once
 
 #include <cuda_bf16.h>
+#include <cuda_runtime.h>
 #include <cstdint>
+
+#include "luna_b200.h"
 
 namespace luna {
 namespace mlp {
+
+// The forward pass on the 5th-generation tensor cores (mlp_tc.cuh; defined in learned.cu): logits [n][16] of feature
+// rows [n][32] on `stream`; a wait that gives up sets bit 16 of *error.
+luna_status forward_tc(const float* params, const __nv_bfloat16* x, int n, float* logits, unsigned long long* error, cudaStream_t stream);
 
 constexpr int kIn = 32, kHidden = 64, kOut = 16, kUsed = 5;
 constexpr int kW1 = 0, kB1 = kW1 + kHidden * kIn, kW2 = kB1 + kHidden, kB2 = kW2 + kHidden * kHidden, kW3 = kB2 + kHidden,

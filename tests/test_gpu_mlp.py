@@ -119,3 +119,20 @@ def test_learned_limiter_keeps_face_values_in_range(cuda):
     want = g0.reshape(-1, 5, 3) * phi[:, :, None]
     assert np.max(np.abs(g.reshape(-1, 5, 3) - want)) <= 1e-6 * np.max(np.abs(want)) + 1e-300
     assert np.all(phi >= 0) and np.all(phi <= alpha + 1e-7)
+
+
+@pytest.mark.parametrize("n", [1, 127, 128, 129, 300_000])
+def test_tensor_core_forward_tiles(cuda, n):
+    """The tcgen05 forward (tiles of 128 rows, a grid-stride loop once the rows outnumber 296 tiles) against the numpy
+    oracle at row counts around a tile and at many tiles a CTA."""
+    import torch
+
+    from luna_cpp_b200.learned import LimiterMLP, init_params
+
+    x, _, _ = data(n, seed=n % 97)
+    p = init_params(7)
+    net = LimiterMLP(p)
+    logits = net.forward(torch.tensor(x, device="cuda").to(torch.bfloat16)).cpu().numpy()
+    want, _ = M.forward(p, x)
+    assert logits.shape == (n, M.OUT)
+    assert rel(logits, want) < 2e-3
