@@ -39,6 +39,7 @@ def parse():
     ap.add_argument("--impl", default="luna", choices=["luna", "reference"])
     ap.add_argument("--cpu-sample-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="leave out the learned limiter's section")
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "fp32"],
                     help="which policies to time (the JSON line needs both; one is for profiling runs)")
     return ap.parse_args()
@@ -206,6 +207,39 @@ def max_over_ranks(x: float, dist=None, device="cuda") -> float:
     return float(t.item())
 
 
+def learned_section(mesh, q0, steps, warmup, stream, torch) -> dict:
+    """The learned limiter beside the plain one (the metric's second half, L1 error per GPU time): (1) the FP64 step on
+    this mesh with the shipped trained network against the plain step, CUDA events, the same steps; (2) four held-out
+    seeded Riemann problems (quasi-1D strips of 1024 x 4 cells, the training's distribution) run to the same time by
+    plain and learned at the base resolution and by plain at 1.5x, each judged by the density profile's L1 against the
+    method's own 4x run, with the device time of each run (strips this small are bound by launches)."""
+    from luna_cpp_b200 import hydro
+    from luna_cpp_b200 import limiter_training as T
+    from luna_cpp_b200.learned import LimiterMLP, trained_params
+
+    net = LimiterMLP(trained_params())
+    step_ms = {}
+    for mode in ("plain", "learned"):
+        fv = hydro.FiniteVolume(mesh)
+        fv.set_stream(stream)
+        if mode == "learned":
+            fv.set_limiter("learned", net.params)
+        fv.set_state(q0)
+        for _ in range(warmup):
+            fv.step(fv.time_step(0.3))
+        step_ms[mode] = timed_steps(fv, steps, torch) / steps
+        fv.close()
+    rows = T.evaluate(net, [5000, 5001, 5002, 5003], nx=1024, ny=4, resolutions=(1.0, 1.5), log=lambda s: None)
+    summary = T.summarize(rows, resolutions=(1.0, 1.5))
+    gm, ms = summary["geomean_l1"], summary["mean_device_ms"]
+    return {"step_ms_at_this_mesh": step_ms, "learned_step_cost": step_ms["learned"] / step_ms["plain"],
+            "riemann_strips": {"problems": 4, "cells": 4096,
+                               "plain": {"l1": gm["plain@1.0"], "device_ms": ms["plain@1.0"]},
+                               "learned": {"l1": gm["learned@1.0"], "device_ms": ms["learned@1.0"]},
+                               "plain_1.5x": {"l1": gm["plain@1.5"], "device_ms": ms["plain@1.5"]},
+                               "plain_resolution_of_equal_error": summary["plain_resolution_of_equal_error"]}}
+
+
 def timed_steps(fv, steps, torch):
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
@@ -344,6 +378,8 @@ def main():
             "gpu_launches": int(launches),
             "fallbacks_last_step": r64["fallbacks"],
         }
+        if world == 1 and not args.no_learned:
+            line["learned_limiter"] = learned_section(mesh, q0, args.steps, args.warmup, stream, torch)
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(mesh, q0, args.cpu_sample_steps, os.cpu_count() or 1)
         print(json.dumps(line), flush=True)
