@@ -404,6 +404,31 @@ __global__ void __launch_bounds__(kTileCells, MINB) k_sweep_tiles(MeshDev<D> m, 
             smallest_dt = fmin(smallest_dt, courant * (ri / (ci + sqrt(dot<D>(rel, rel)))));
         }
         if constexpr (Grad) {
+            // A slope that moves every face value of its variable by at most the policy's round-off of the variable's
+            // scale (|g_v| max_k |r_k| <= e s_v; s = |rho|, |v| + c for the velocity components, |P|; e = 2^-50 when
+            // the face states are solved in double, 2^-24 when the Riemann solve rounds them to float) is round-off of
+            // a uniform region, where a clip could change face states only at that level; when every variable's slope
+            // is such, walk 2 is left out (the learned limiter's inputs then take the admissible factor 1, the plain
+            // limiter's choice there). The step then differs from the reference's arithmetic only at that level in
+            // those cells' face states. round_off2 = e^2.
+            bool round_off_only = false;
+            if constexpr (Limit != 0) {
+                const double reach2 = geo.reach2[i];
+                const double kNoise2 = round_off2;
+                double speed2 = 0;
+#pragma unroll
+                for (int a = 0; a < D; ++a) speed2 += Wi[1 + a] * Wi[1 + a];
+                const double signal = sqrt(speed2) + ci;
+                round_off_only = true;
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    double gg = 0;
+#pragma unroll
+                    for (int a = 0; a < D; ++a) gg += static_cast<double>(g[D * v + a]) * static_cast<double>(g[D * v + a]);
+                    const double scale = (v >= 1 && v <= D) ? signal : fabs(Wi[v]);
+                    round_off_only = round_off_only && gg * reach2 <= kNoise2 * (scale * scale);
+                }
+            }
             if constexpr (Limit == 2) {
                 // The admissible factor per variable: the smallest over the faces (tiny ones left out) of the factor that
                 // puts the face value on its bound, max(room, 0) / |dp|, the min-factor form of the limiter
@@ -412,10 +437,10 @@ __global__ void __launch_bounds__(kTileCells, MINB) k_sweep_tiles(MeshDev<D> m, 
                 double alpha[V], num[V], den[V];
 #pragma unroll
                 for (int v = 0; v < V; ++v) {
-                    num[v] = kAlphaCap;
+                    num[v] = round_off_only ? 1.0 : kAlphaCap;
                     den[v] = 1.0;
                 }
-                for (int k = 0; k < count; ++k) {
+                for (int k = 0; k < (round_off_only ? 0 : count); ++k) {
                     const int64_t slot = slot0 + 32 * static_cast<int64_t>(k);
                     if (any_tiny && (ldg_hint(geo.nbr + slot, once) & kTinyBit)) continue;
                     const Pair<G> o01 = ldg_hint(geo.off01 + slot, once);
@@ -438,30 +463,6 @@ __global__ void __launch_bounds__(kTileCells, MINB) k_sweep_tiles(MeshDev<D> m, 
 #pragma unroll
                 for (int v = 0; v < V; ++v) alpha[v] = num[v] / den[v];
                 write_learned_inputs<D>(learned, i, Wi, ci, ri, g, lo, hi, alpha);
-            }
-            // A slope that moves every face value of its variable by at most the policy's round-off of the variable's
-            // scale (|g_v| max_k |r_k| <= e s_v; s = |rho|, |v| + c for the velocity components, |P|; e = 2^-50 when
-            // the face states are solved in double, 2^-24 when the Riemann solve rounds them to float) is round-off of
-            // a uniform region, where a clip could change face states only at that level; when every variable's slope
-            // is such, walk 2 is left out. The step then differs from the reference's arithmetic only at that level
-            // in those cells' face states. round_off2 = e^2.
-            bool round_off_only = false;
-            if constexpr (Limit == 1) {
-                const double reach2 = geo.reach2[i];
-                const double kNoise2 = round_off2;
-                double speed2 = 0;
-#pragma unroll
-                for (int a = 0; a < D; ++a) speed2 += Wi[1 + a] * Wi[1 + a];
-                const double signal = sqrt(speed2) + ci;
-                round_off_only = true;
-#pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    double gg = 0;
-#pragma unroll
-                    for (int a = 0; a < D; ++a) gg += static_cast<double>(g[D * v + a]) * static_cast<double>(g[D * v + a]);
-                    const double scale = (v >= 1 && v <= D) ? signal : fabs(Wi[v]);
-                    round_off_only = round_off_only && gg * reach2 <= kNoise2 * (scale * scale);
-                }
             }
             if constexpr (Limit == 1 && exact) if (!round_off_only) {
                 // The clip (Sweep walk 2, finite_volume.hpp:538-565): each face in list order (tiny ones left out)
@@ -588,8 +589,8 @@ __device__ __forceinline__ void write_learned_inputs(const LearnedInputs& out, i
         const double pos = fmin(fmax((Wi[v] - static_cast<double>(lo[v])) / safe, -1.0), 2.0);
         f[4 * v + 0] = static_cast<float>(alpha[v] / kAlphaCap);
         f[4 * v + 1] = static_cast<float>(pos - 0.5);
-        f[4 * v + 2] = static_cast<float>(tanh(gn * r / safe));
-        f[4 * v + 3] = static_cast<float>(tanh(range / scale * 3.0));
+        f[4 * v + 2] = tanhf(static_cast<float>(gn * r / safe));  // the features are BF16: float is ample
+        f[4 * v + 3] = tanhf(static_cast<float>(range / scale * 3.0));
         plain = fmin(plain, fmin(alpha[v], 1.0));
         out.alpha[5 * static_cast<int64_t>(i) + v] = alpha[v];
     }
@@ -597,8 +598,8 @@ __device__ __forceinline__ void write_learned_inputs(const LearnedInputs& out, i
     double speed = 0;
 #pragma unroll
     for (int a = 0; a < D; ++a) speed += Wi[1 + a] * Wi[1 + a];
-    f[20] = static_cast<float>(tanh(log(phi / plo)));
-    f[21] = static_cast<float>(tanh(sqrt(speed) / fmax(c, 1e-300)));
+    f[20] = tanhf(logf(static_cast<float>(phi / plo)));
+    f[21] = tanhf(static_cast<float>(sqrt(speed) / fmax(c, 1e-300)));
     f[22] = static_cast<float>(plain);
     f[23] = 1.0f;
     __nv_bfloat16* row = out.features + 32 * static_cast<int64_t>(i);
