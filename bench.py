@@ -40,6 +40,8 @@ def parse():
     ap.add_argument("--cpu-sample-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="leave out the learned limiter's section")
+    ap.add_argument("--curve", default="row", choices=["row", "morton", "hilbert"],
+                    help="the cells' numbering along a space-filling curve (voronoi-cpp's Layout::curve)")
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "fp32"],
                     help="which policies to time (the JSON line needs both; one is for profiling runs)")
     return ap.parse_args()
@@ -139,11 +141,12 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def build_workload(nx: int, threads: int):
-    from luna_cpp_b200.mesh import build_mesh, jittered_points
+def build_workload(nx: int, threads: int, curve: str = "row"):
+    from luna_cpp_b200.mesh import build_mesh, curve_order, jittered_points
     from luna_cpp_b200.problems import point_blast
 
-    mesh = build_mesh(jittered_points((nx, nx, nx), jitter=0.1, seed=1), threads=threads)
+    points = jittered_points((nx, nx, nx), jitter=0.1, seed=1)
+    mesh = build_mesh(points[curve_order(points, curve=curve)], threads=threads)
     return mesh, point_blast(mesh)
 
 
@@ -171,7 +174,7 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    mesh, q0 = build_workload(args.nx, threads)
+    mesh, q0 = build_workload(args.nx, threads, args.curve)
     from oracle import oracle as O
 
     used = O.threads(threads)
@@ -272,7 +275,7 @@ def main():
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
     threads = max(1, (os.cpu_count() or 1) // world)
-    mesh, q0 = build_workload(args.nx, threads)
+    mesh, q0 = build_workload(args.nx, threads, args.curve)
     N, F = mesh.n_cells, mesh.n_faces
     stream = torch.cuda.current_stream().cuda_stream
 

@@ -227,10 +227,15 @@ template <int D, class G>
 __device__ __forceinline__ void write_learned_inputs(const struct LearnedInputs& out, int i, const double* Wi, double c, double r, const G* g,
                                                      const G* lo, const G* hi, const double* alpha);
 
-// The learned limiter's inputs, written by the sweep in its learned mode (see write_learned_inputs).
+// The learned limiter's inputs, written by the sweep in its learned mode (see write_learned_inputs). Dense (cells null):
+// row i is cell i. Compact: only cells whose slopes are not round-off get a row (their factor is the network's; the
+// others keep the factor 1, the plain limiter's there), taken in arrival order; cells[row] names the row's cell and
+// *count ends as the number of rows.
 struct LearnedInputs {
-    __nv_bfloat16* features;  // [N][32]
-    double* alpha;            // [N][5]: the admissible slope factor per variable
+    __nv_bfloat16* features;  // [rows][32]
+    double* alpha;            // [rows][5]: the admissible slope factor per variable
+    int* cells;               // [N] or null (dense)
+    unsigned int* count;      // the compact rows taken (reset to 0 before the sweep)
 };
 constexpr double kAlphaCap = 2.0;  // the largest steepening the learned limiter may choose
 
@@ -429,7 +434,7 @@ __global__ void __launch_bounds__(kTileCells, MINB) k_sweep_tiles(MeshDev<D> m, 
                     round_off_only = round_off_only && gg * reach2 <= kNoise2 * (scale * scale);
                 }
             }
-            if constexpr (Limit == 2) {
+            if constexpr (Limit == 2) if (!(learned.cells && round_off_only)) {
                 // The admissible factor per variable: the smallest over the faces (tiny ones left out) of the factor that
                 // puts the face value on its bound, max(room, 0) / |dp|, the min-factor form of the limiter
                 // (finite_volume.hpp:1008-1034), here capped at kAlphaCap instead of 1; held as a fraction and compared
@@ -462,7 +467,17 @@ __global__ void __launch_bounds__(kTileCells, MINB) k_sweep_tiles(MeshDev<D> m, 
                 }
 #pragma unroll
                 for (int v = 0; v < V; ++v) alpha[v] = num[v] / den[v];
-                write_learned_inputs<D>(learned, i, Wi, ci, ri, g, lo, hi, alpha);
+                int row = i;
+                if (learned.cells) {  // one atomic a warp: the lanes here take consecutive rows
+                    const unsigned int here = __activemask();
+                    const int lane = static_cast<int>(threadIdx.x & 31), leader = __ffs(here) - 1;
+                    unsigned int base = 0;
+                    if (lane == leader) base = atomicAdd(learned.count, static_cast<unsigned int>(__popc(here)));
+                    base = __shfl_sync(here, base, leader);
+                    row = static_cast<int>(base) + __popc(here & ((1u << lane) - 1u));
+                    learned.cells[row] = i;
+                }
+                write_learned_inputs<D>(learned, row, Wi, ci, ri, g, lo, hi, alpha);
             }
             if constexpr (Limit == 1 && exact) if (!round_off_only) {
                 // The clip (Sweep walk 2, finite_volume.hpp:538-565): each face in list order (tiny ones left out)
@@ -607,26 +622,28 @@ __device__ __forceinline__ void write_learned_inputs(const LearnedInputs& out, i
     for (int k = 0; k < 32; k += 2) *reinterpret_cast<__nv_bfloat162*>(row + k) = __floats2bfloat162_rn(f[k], f[k + 1]);
 }
 
-// The learned slope factors applied: g_v *= alpha_v sigmoid(logit_v) (use_net), or min(alpha_v, 1), the plain limiter's
-// factor in min-factor form (a check of alpha against the plain sweep).
+// The learned slope factors applied to the rows of LearnedInputs (dense: row s is cell s; compact: cells[s], the first
+// *count rows): g_v *= alpha_v sigmoid(logit_v) (use_net), or min(alpha_v, 1), the plain limiter's factor in min-factor
+// form (a check of alpha against the plain sweep).
 template <int D>
-__global__ void k_apply_factors(int n, double* __restrict__ grad, const double* __restrict__ alpha, const float* __restrict__ logits,
-                                bool use_net) {
+__global__ void k_apply_factors(int rows, const int* __restrict__ cells, const unsigned int* __restrict__ count, double* __restrict__ grad,
+                                const double* __restrict__ alpha, const float* __restrict__ logits, bool use_net) {
     constexpr int V = D + 2, GS = grad_stride<D>();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= rows || (count && s >= static_cast<int>(*count))) return;
+    const int64_t i = cells ? cells[s] : s;
 #pragma unroll
     for (int v = 0; v < V; ++v) {
-        const double a = alpha[5 * static_cast<int64_t>(i) + v];
+        const double a = alpha[5 * static_cast<int64_t>(s) + v];
         double phi;
         if (use_net) {
-            const double o = logits[16 * static_cast<int64_t>(i) + v];
+            const double o = logits[16 * static_cast<int64_t>(s) + v];
             phi = a / (1.0 + exp(-o));
         } else {
             phi = fmin(a, 1.0);
         }
 #pragma unroll
-        for (int d = 0; d < D; ++d) grad[static_cast<int64_t>(GS) * i + D * v + d] *= phi;
+        for (int d = 0; d < D; ++d) grad[GS * i + D * v + d] *= phi;
     }
 }
 

@@ -34,7 +34,8 @@ __device__ unsigned long long g_forward_error;
 namespace luna {
 namespace mlp {
 
-luna_status forward_tc(const float* params, const __nv_bfloat16* x, int n, float* logits, unsigned long long* error, cudaStream_t stream) {
+luna_status forward_tc(const float* params, const __nv_bfloat16* x, int n, const unsigned int* rows, float* logits, unsigned long long* error,
+                       cudaStream_t stream) {
     if (n <= 0) return LUNA_OK;
     const int smem = static_cast<int>(sizeof(SmemTc));
     static bool configured = false;
@@ -47,7 +48,7 @@ luna_status forward_tc(const float* params, const __nv_bfloat16* x, int n, float
     // each; 4 fill it)
     const int64_t tiles = (static_cast<int64_t>(n) + kTcRows - 1) / kTcRows;
     const int blocks = static_cast<int>(tiles < 148 * LUNA_MLP_CTAS_PER_SM ? tiles : 148 * LUNA_MLP_CTAS_PER_SM);
-    k_mlp_forward_tc<<<blocks, 128, smem, stream>>>(params, x, n, logits, error);
+    k_mlp_forward_tc<<<blocks, 128, smem, stream>>>(params, x, n, rows, logits, error);
     return check_launch("k_mlp_forward_tc");
 }
 
@@ -71,7 +72,7 @@ LUNA_API luna_status luna_mlp_forward(const float* params, const void* features,
     cudaError_t e = cudaGetSymbolAddress(&word, g_forward_error);
     if (e == cudaSuccess) e = cudaMemsetAsync(word, 0, sizeof(unsigned long long), s);
     if (e != cudaSuccess) return fail(LUNA_ECUDA, std::string("luna_mlp_forward error word: ") + cudaGetErrorString(e));
-    const luna_status st = luna::mlp::forward_tc(params, static_cast<const __nv_bfloat16*>(features), static_cast<int>(n), logits,
+    const luna_status st = luna::mlp::forward_tc(params, static_cast<const __nv_bfloat16*>(features), static_cast<int>(n), nullptr, logits,
                                                  static_cast<unsigned long long*>(word), s);
     if (st != LUNA_OK) return st;
     unsigned long long bits = 0;

@@ -113,6 +113,8 @@ struct luna_fv {
     DevArray<unsigned char> lim_features;
     DevArray<double> lim_alpha;
     DevArray<float> lim_logits;
+    DevArray<int32_t> lim_cells;       // the compact rows' cells (a step that applies the limiter)
+    DevArray<unsigned int> lim_count;  // the compact rows taken
     const float* mlp_params = nullptr;
     bool learned_inputs = false, apply_learned = false;
     // adjoint (allocated by the first luna_fv_step_adjoint)
@@ -348,7 +350,11 @@ template <int D, bool Moving, bool Grad, class G, int Limit>
 luna_status launch_sweep_tiles(luna_fv* fv, G* grad, double courant) {
     const auto m = fv->mesh_dev<D>();
     const auto geo = fv->geometry_dev<D, G>();
-    const luna::LearnedInputs learned{reinterpret_cast<__nv_bfloat16*>(fv->lim_features.ptr), fv->lim_alpha.ptr};
+    // compact rows when the factors are applied (a step); every cell's row when the inputs are read (training data)
+    const bool compact = fv->apply_learned;
+    const luna::LearnedInputs learned{reinterpret_cast<__nv_bfloat16*>(fv->lim_features.ptr), fv->lim_alpha.ptr,
+                                      compact ? fv->lim_cells.ptr : nullptr, compact ? fv->lim_count.ptr : nullptr};
+    if (Limit == 2 && compact) LUNA_CUDA(cudaMemsetAsync(fv->lim_count.ptr, 0, sizeof(unsigned int), fv->stream));
     auto kernel = luna::k_sweep_tiles<D, Moving, Grad, G, Limit>;
     const int64_t groups[2][2] = {{0, fv->normal_tiles}, {fv->normal_tiles, fv->tiles}};
     const int most_rows[2] = {fv->normal_rows, fv->big_rows};
@@ -387,14 +393,15 @@ luna_status launch_sweep(luna_fv* fv, G* grad, double courant) {
             const long timed_ = fv->open_timed(1);
             if (fv->mlp_params) {
                 const luna_status st = luna::mlp::forward_tc(fv->mlp_params, reinterpret_cast<const __nv_bfloat16*>(fv->lim_features.ptr),
-                                                             static_cast<int>(fv->n), fv->lim_logits.ptr, &fv->counters.ptr->error, fv->stream);
+                                                             static_cast<int>(fv->n), fv->lim_count.ptr, fv->lim_logits.ptr,
+                                                             &fv->counters.ptr->error, fv->stream);
                 if (st != LUNA_OK) {
                     fv->close_timed(timed_);
                     return st;
                 }
             }
-            luna::k_apply_factors<D><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(static_cast<int>(fv->n), grad, fv->lim_alpha.ptr, fv->lim_logits.ptr,
-                                                                                 fv->mlp_params != nullptr);
+            luna::k_apply_factors<D><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(static_cast<int>(fv->n), fv->lim_cells.ptr, fv->lim_count.ptr, grad,
+                                                                                 fv->lim_alpha.ptr, fv->lim_logits.ptr, fv->mlp_params != nullptr);
             fv->close_timed(timed_);
             LUNA_CUDA(cudaGetLastError());
         }
@@ -932,12 +939,15 @@ LUNA_API luna_status luna_fv_step_adjoint(luna_fv* fv, double dt, double* qbar, 
     return LUNA_OK;
 }
 
-// The learned limiter's buffers (64 B of features, 40 B of admissible factors, 64 B of logits a cell).
+// The learned limiter's buffers (64 B of features, 40 B of admissible factors, 64 B of logits and a compact row's cell a
+// cell, and the row count).
 static luna_status alloc_learned(luna_fv* fv) {
     const size_t N = static_cast<size_t>(fv->n);
     LUNA_TRY(fv->lim_features.alloc(N * 32 * sizeof(__nv_bfloat16), "limiter features"));
     LUNA_TRY(fv->lim_alpha.alloc(N * 5, "limiter admissible factors"));
     LUNA_TRY(fv->lim_logits.alloc(N * 16, "limiter logits"));
+    LUNA_TRY(fv->lim_cells.alloc(N, "limiter rows' cells"));
+    LUNA_TRY(fv->lim_count.alloc(1, "limiter row count"));
     return LUNA_OK;
 }
 
@@ -1023,6 +1033,7 @@ LUNA_API luna_status luna_fv_device_bytes(luna_fv* fv, int64_t* out) {
     b += fv->geo_c01.bytes() + fv->geo_c2.bytes() + fv->geo_off01.bytes() + fv->geo_off2.bytes() + fv->geo_nbr.bytes();
     b += fv->geo_slice_base.bytes() + fv->geo_order.bytes() + fv->geo_stage_start.bytes() + fv->geo_stage_cells.bytes() + fv->geo_faces.bytes();
     b += fv->geo_angle.bytes() + fv->geo_reach2.bytes() + fv->lim_features.bytes() + fv->lim_alpha.bytes() + fv->lim_logits.bytes();
+    b += fv->lim_cells.bytes() + fv->lim_count.bytes();
     *out = static_cast<int64_t>(b);
     return LUNA_OK;
 }

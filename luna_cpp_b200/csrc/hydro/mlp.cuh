@@ -24,8 +24,10 @@ namespace luna {
 namespace mlp {
 
 // The forward pass on the 5th-generation tensor cores (mlp_tc.cuh; defined in learned.cu): logits [n][16] of feature
-// rows [n][32] on `stream`; a wait that gives up sets bit 16 of *error.
-luna_status forward_tc(const float* params, const __nv_bfloat16* x, int n, float* logits, unsigned long long* error, cudaStream_t stream);
+// rows [n][32] on `stream`; rows (device, may be null): only the first min(n, *rows) rows, a count written earlier on the
+// stream; a wait that gives up sets bit 16 of *error.
+luna_status forward_tc(const float* params, const __nv_bfloat16* x, int n, const unsigned int* rows, float* logits, unsigned long long* error,
+                       cudaStream_t stream);
 
 constexpr int kIn = 32, kHidden = 64, kOut = 16, kUsed = 5;
 constexpr int kW1 = 0, kB1 = kW1 + kHidden * kIn, kW2 = kB1 + kHidden, kB2 = kW2 + kHidden * kHidden, kW3 = kB2 + kHidden,

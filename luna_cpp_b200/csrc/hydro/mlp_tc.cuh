@@ -131,12 +131,17 @@ __device__ __forceinline__ void tc_hidden_epilogue(uint32_t tbase, int col0, con
 }
 
 // logits [n][16] of feature rows [n][32] (BF16). A grid-stride loop over tiles of 128 rows; 128 threads; dynamic shared
-// memory sizeof(SmemTc). error: bit kTcTimeoutBit when a wait gave up (the CTA then stops and frees its TMEM).
+// memory sizeof(SmemTc). rows (device, may be null): the rows are the first min(n, *rows), a count the previous launch on
+// the stream wrote; a CTA with no tile returns before it stages weights or allocates TMEM. error: bit kTcTimeoutBit
+// when a wait gave up (the CTA then stops and frees its TMEM).
 static __global__ void __launch_bounds__(128, 1) k_mlp_forward_tc(const float* __restrict__ params, const __nv_bfloat16* __restrict__ x, int n,
-                                                                  float* __restrict__ logits, unsigned long long* __restrict__ error) {
+                                                                  const unsigned int* __restrict__ rows, float* __restrict__ logits,
+                                                                  unsigned long long* __restrict__ error) {
     extern __shared__ __align__(128) unsigned char tc_smem[];
     SmemTc& s = *reinterpret_cast<SmemTc*>(tc_smem);
     const int tid = static_cast<int>(threadIdx.x), warp = tid >> 5;
+    if (rows) n = min(n, static_cast<int>(*rows));
+    if (static_cast<int>(blockIdx.x) * kTcRows >= n) return;  // the same for every thread of the CTA
     // weights as BF16 operands, biases as FP32
     for (int i = tid; i < kHidden * kIn; i += blockDim.x)
         *reinterpret_cast<__nv_bfloat16*>(reinterpret_cast<char*>(s.w1) + core_offset(i / kIn, i % kIn, kIn)) = __float2bfloat16_rn(params[kW1 + i]);

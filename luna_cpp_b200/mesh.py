@@ -123,6 +123,57 @@ def build_mesh(points: np.ndarray, box=(1.0, 1.0, 1.0), threads: int = 0) -> Mes
         lib.luna_mesh_free(handle)
 
 
+def _hilbert_transpose(X: np.ndarray, bits: int) -> np.ndarray:
+    """Skilling's axes-to-transpose map (J. Skilling, "Programming the Hilbert curve", AIP Conf. Proc. 707, 381 (2004)),
+    vectorised over rows: X [n, dim] unsigned integer coordinates of ``bits`` bits, returned in transposed form (the
+    curve index's bits read across the axes, most significant level first)."""
+    X = X.copy()
+    dim = X.shape[1]
+    q = np.uint64(1) << np.uint64(bits - 1)
+    while q > 1:
+        p = q - np.uint64(1)
+        for i in range(dim):
+            hit = (X[:, i] & q) != 0
+            X[hit, 0] ^= p
+            t = (X[:, 0] ^ X[:, i]) & p
+            t[hit] = 0
+            X[:, 0] ^= t
+            X[:, i] ^= t
+        q >>= np.uint64(1)
+    for i in range(1, dim):
+        X[:, i] ^= X[:, i - 1]
+    t = np.zeros(X.shape[0], dtype=np.uint64)
+    q = np.uint64(1) << np.uint64(bits - 1)
+    while q > 1:
+        t[(X[:, dim - 1] & q) != 0] ^= q - np.uint64(1)
+        q >>= np.uint64(1)
+    X ^= t[:, None]
+    return X
+
+
+def curve_order(points: np.ndarray, box=None, curve: str = "hilbert", bits: int = 16) -> np.ndarray:
+    """The permutation that numbers ``points`` along a space-filling curve through the box: voronoi-cpp's cell
+    ordering (``voronoi::Layout::curve``: hilbert, morton, ...; luna-cpp's ``--curve``, README.md:75, :94), which keeps
+    a cell's neighbours close to it in memory. ``points[curve_order(points)]`` is the reordered set; "row" keeps the
+    given order."""
+    pts = np.asarray(points, dtype=np.float64)
+    n, dim = pts.shape
+    if curve == "row" or n == 0:
+        return np.arange(n)
+    side = np.ones(dim) if box is None else np.asarray(box, dtype=np.float64)[:dim]
+    scale = float(1 << bits)
+    X = np.clip(np.floor(pts / side * scale), 0, scale - 1).astype(np.uint64)
+    if curve == "hilbert":
+        X = _hilbert_transpose(X, bits)
+    elif curve != "morton":
+        raise ValueError(f"unknown curve {curve!r}")
+    code = np.zeros(n, dtype=np.uint64)
+    for level in range(bits - 1, -1, -1):
+        for i in range(dim):
+            code = (code << np.uint64(1)) | ((X[:, i] >> np.uint64(level)) & np.uint64(1))
+    return np.argsort(code, kind="stable")
+
+
 def jittered_points(cells, side=None, jitter: float = 0.1, seed: int = 1) -> np.ndarray:
     """problems_3d.hpp's ``jittered_points`` (src/hydro/problems_3d.hpp:37-53): the lattice point (i + 1/2) h moved by
     uniform(-jitter, jitter) spacings per axis from ``std::mt19937_64(seed)``, wrapped into [0, side); the last axis runs

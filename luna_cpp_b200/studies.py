@@ -10,6 +10,9 @@ comparisons of the same configurations are GPU tests).
   arithmetic with FP64 state by default (``riemann32``): steps taken, the hydro part's device time and cell-updates/s
   (the remesh, voronoi-cpp's job, is timed apart, as the reference's hydro part is), the radial density profile; and
   ``timed_steps`` moving steps at ``timed_nx``^3 for the hydro part's throughput at that size.
+- ``learned``: the learned limiter on the static 3D point blast: its density L1 against the method's own run at 4x the
+  resolution per axis, beside the plain limiter at the same and at finer resolutions, with device times; the GPU time
+  the plain limiter needs for the learned limiter's error, over the learned run's.
 - ``adjoint``: 2D Voronoi mesh from nx^2 jittered generators, the shear layer with a_k ~ N(0, 1) from the seed, 200
   steps; d/da_k of int rho vy^2 dA at the final time by the hand-written adjoint with checkpoints every 20 steps,
   against central differences (h = 1e-6) on the same dt schedule; device time of the forward and of the backward.
@@ -17,6 +20,7 @@ comparisons of the same configurations are GPU tests).
     python -m luna_cpp_b200.studies precision --nx 128 --steps 100 --out precision.json
     python -m luna_cpp_b200.studies adjoint --nx 512 --steps 200 --out adjoint.json
     python -m luna_cpp_b200.studies moving --nx 32 --out moving.json
+    python -m luna_cpp_b200.studies learned --nx 48 --out learned.json
 """
 from __future__ import annotations
 
@@ -163,6 +167,100 @@ def moving(nx=32, t_end=0.05, precision_policy="fp32", timed_nx=128, timed_steps
     return out
 
 
+def _run_to(fv, t_end, courant):
+    """Static steps to t_end (the last one shortened); returns (steps, device ms)."""
+    fv.set_timing(True)
+    fv.timings()
+    t, steps = 0.0, 0
+    while t < t_end:
+        dt = min(fv.time_step(courant), t_end - t)
+        fv.step(dt)
+        t += dt
+        steps += 1
+    return steps, _phases_ms(fv)
+
+
+def _radial_reference(mesh, q, bins=1024):
+    """The density of a (fine) run as a function of radius from the box centre: mass over volume in thin shells out to
+    the box's corner, for linear interpolation at other meshes' cell radii."""
+    c = cell_centres(mesh) - 0.5 * np.asarray(mesh.box)
+    r = np.sqrt((c * c).sum(1))
+    edge = float(np.sqrt((0.25 * np.asarray(mesh.box) ** 2).sum()))
+    b = np.minimum((r / edge * bins).astype(int), bins - 1)
+    mass = np.bincount(b, weights=q[:, 0], minlength=bins)
+    vol = np.bincount(b, weights=mesh.volume, minlength=bins)
+    centres = (np.arange(bins) + 0.5) * edge / bins
+    keep = vol > 0
+    return centres[keep], mass[keep] / vol[keep]
+
+
+def _profile_l1(mesh, q, reference) -> float:
+    """Volume-weighted L1 of the cell densities against the reference profile at the cells' radii."""
+    c = cell_centres(mesh) - 0.5 * np.asarray(mesh.box)
+    r = np.sqrt((c * c).sum(1))
+    rho = q[:, 0] / mesh.volume
+    want = np.interp(r, reference[0], reference[1])
+    return float((mesh.volume * np.abs(rho - want)).sum() / mesh.volume.sum())
+
+
+def learned_blast(nx=48, factor=4, plain_nx=(48, 56, 64, 72, 80), t_end=0.05, courant=0.3, threads=0, log=print) -> dict:
+    """The learned limiter in 3D: the static point blast (E = 1 within 2 cell widths, FP64) on nx^3 jittered generators
+    to t_end with the shipped network, and with the plain limiter at nx and at the finer ``plain_nx``, each judged by the
+    volume-weighted L1 of its density against the radial profile of the method's own run at factor x nx per axis; with
+    the device time of every run. The plain method's error and time are interpolated in log-log at the learned run's
+    error: the GPU time the plain limiter needs for the learned limiter's accuracy, over the learned run's."""
+    import torch
+
+    from .learned import LimiterMLP, trained_params
+
+    def mesh_of(n):
+        t0 = time.time()
+        m = build_mesh(jittered_points((n, n, n), jitter=0.1, seed=1), threads=threads)
+        log(f"mesh {n}^3: {m.n_cells} cells, {time.time() - t0:.1f} s")
+        return m
+
+    fine = mesh_of(factor * nx)
+    fv = hydro.FiniteVolume(fine)
+    fv.set_state(point_blast(fine, GAMMA))
+    steps, ms = _run_to(fv, t_end, courant)
+    reference = _radial_reference(fine, fv.get_state())
+    fv.close()
+    out = {"config": {"problem": "static point blast, E = 1 within 2 cell widths, gamma 5/3, FP64", "t_end": t_end,
+                      "courant": courant, "reference": {"cells": fine.n_cells, "steps": steps, "device_ms": ms}},
+           "plain": [], "learned": []}
+    del fine
+    net = LimiterMLP(trained_params())
+    for n in sorted(set(plain_nx) | {nx}):
+        mesh = mesh_of(n)
+        q0 = point_blast(mesh, GAMMA)
+        for mode in ("plain", "learned") if n == nx else ("plain",):
+            fv = hydro.FiniteVolume(mesh)
+            if mode == "learned":
+                fv.set_limiter("learned", net.params)
+            fv.set_state(q0)
+            steps, ms = _run_to(fv, t_end, courant)
+            row = {"nx": n, "cells": mesh.n_cells, "steps": steps, "device_ms": ms, "l1": _profile_l1(mesh, fv.get_state(), reference)}
+            fv.close()
+            out[mode].append(row)
+            log(f"{mode} {n}^3: {steps} steps, {ms:.1f} ms, L1 {row['l1']:.4e}")
+    torch.cuda.synchronize()
+    plain = sorted(out["plain"], key=lambda r: r["nx"])
+    learned = out["learned"][0]
+    le = np.log([r["l1"] for r in plain])
+    if np.all(np.diff(le) < 0) and le[-1] <= np.log(learned["l1"]) <= le[0]:
+        # error falls with resolution: interpolate log nx and log time at the learned error
+        x = np.interp(np.log(learned["l1"]), le[::-1], np.log([r["nx"] for r in plain])[::-1])
+        t = np.interp(x, np.log([r["nx"] for r in plain]), np.log([r["device_ms"] for r in plain]))
+        out["plain_nx_of_equal_error"] = float(np.exp(x))
+        out["plain_device_ms_at_equal_error"] = float(np.exp(t))
+        out["gpu_time_ratio_at_equal_error"] = float(np.exp(t) / learned["device_ms"])
+    else:
+        out["plain_nx_of_equal_error"] = None
+        out["gpu_time_ratio_at_equal_error"] = None
+    out["learned_l1_over_plain_l1"] = learned["l1"] / next(r["l1"] for r in plain if r["nx"] == nx)
+    return out
+
+
 def adjoint(nx=512, steps=200, every=20, h=1e-6, seed=3, courant=0.3, threads=0, log=print) -> dict:
     import torch
 
@@ -227,7 +325,7 @@ def adjoint(nx=512, steps=200, every=20, h=1e-6, seed=3, courant=0.3, threads=0,
 
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("study", choices=["precision", "adjoint", "moving"])
+    ap.add_argument("study", choices=["precision", "adjoint", "moving", "learned"])
     ap.add_argument("--nx", type=int)
     ap.add_argument("--steps", type=int)
     ap.add_argument("--threads", type=int, default=0)
@@ -238,9 +336,9 @@ def main():
         kw["nx"] = args.nx
     if args.steps:
         kw["steps"] = args.steps
-    if args.study == "moving":
+    if args.study in ("moving", "learned"):
         kw.pop("steps", None)
-    res = {"precision": precision, "adjoint": adjoint, "moving": moving}[args.study](**kw)
+    res = {"precision": precision, "adjoint": adjoint, "moving": moving, "learned": learned_blast}[args.study](**kw)
     text = json.dumps(res, indent=1)
     if args.out:
         with open(args.out, "w") as f:

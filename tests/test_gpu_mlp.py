@@ -121,6 +121,34 @@ def test_learned_limiter_keeps_face_values_in_range(cuda):
     assert np.all(phi >= 0) and np.all(phi <= alpha + 1e-7)
 
 
+def test_learned_limiter_leaves_round_off_cells_at_factor_one(cuda):
+    """In a step the network runs only on the cells whose slopes are not round-off (compact rows); the others keep the
+    factor 1, as the plain limiter does there. On the point blast most cells are round-off (alpha = 1 for every
+    variable in the dense inputs); the step's gradients are g0 there and g0 alpha sigmoid(logits) elsewhere."""
+    from conftest import jittered_mesh
+    from luna_cpp_b200 import hydro
+    from luna_cpp_b200.learned import LimiterMLP
+    from luna_cpp_b200.problems import point_blast
+
+    mesh = jittered_mesh(16)
+    q0 = point_blast(mesh)
+    fv = hydro.FiniteVolume(mesh)
+    fv.set_state(q0)
+    feats, alpha, g0 = fv.limiter_inputs()
+    net = LimiterMLP(seed=3)
+    fv.set_limiter("learned", net.params)
+    fv.set_state(q0)
+    fv.time_step(0.3)
+    g = fv.gradients().reshape(-1, 5, 3)
+    alpha = alpha.cpu().numpy()
+    round_off = np.all(alpha == 1.0, axis=1)
+    assert round_off.sum() > mesh.n_cells // 2 and (~round_off).sum() > 0
+    logits = net.forward(feats).cpu().numpy()
+    phi = np.where(round_off[:, None], 1.0, alpha * (1 / (1 + np.exp(-logits[:, :5]))))
+    want = g0.cpu().numpy().reshape(-1, 5, 3) * phi[:, :, None]
+    assert np.max(np.abs(g - want)) <= 1e-6 * np.max(np.abs(want)) + 1e-300
+
+
 @pytest.mark.parametrize("n", [1, 127, 128, 129, 300_000])
 def test_tensor_core_forward_tiles(cuda, n):
     """The tcgen05 forward (tiles of 128 rows, a grid-stride loop once the rows outnumber 296 tiles) against the numpy
