@@ -245,8 +245,12 @@ constexpr double kAlphaCap = 2.0;  // the largest steepening the learned limiter
 #define LUNA_SWEEP_MIN_BLOCKS 4
 #endif
 #ifndef LUNA_SWEEP_BATCH
-#define LUNA_SWEEP_BATCH 2
+#define LUNA_SWEEP_BATCH 0  // 0: 2 entries in FP64, 3 in the float policies (128^3 sweep ms: FP64 2: 0.748, 1: 0.760,
+                            // 3: 0.794; riemann32 3: 0.536, 2: 0.545)
 #endif
+#ifndef LUNA_SWEEP_L2_PREFETCH
+#define LUNA_SWEEP_L2_PREFETCH 2  // TMA bulk prefetches into L2: 1 the walk-1 entry rows at block start, 2 also walk 2's
+#endif                            // (measured at 128^3 FP64, sweep ms: none 0.800, 1: 0.775, 2: 0.772)
 #ifndef LUNA_CLIP_BATCH
 #define LUNA_CLIP_BATCH 4  // entries of the clip walk whose offset rows are requested together
 #endif
@@ -268,6 +272,18 @@ __global__ void __launch_bounds__(kTileCells, MINB) k_sweep_tiles(MeshDev<D> m, 
     const int64_t row0 = static_cast<int64_t>(geo.slice_base[t >> 5]) * 32;  // the warp's first slot
     const int64_t slot0 = row0 + (t & 31);
     const unsigned long long once = l2_evict_first();  // entry rows are read once per step
+#if LUNA_SWEEP_L2_PREFETCH
+    if ((threadIdx.x & 31) == 0) {  // the warp's walk-1 entry rows, on their way to L2 while the block stages
+        const int64_t rows = geo.slice_base[(t >> 5) + 1] - geo.slice_base[t >> 5];
+        if (rows > 0) {
+            prefetch_l2(geo.nbr + row0, static_cast<unsigned int>(rows * 32 * sizeof(unsigned int)));
+            if constexpr (Grad) {
+                prefetch_l2(geo.c01 + row0, static_cast<unsigned int>(rows * 32 * sizeof(Pair<G>)));
+                if constexpr (D == 3) prefetch_l2(geo.c2 + row0, static_cast<unsigned int>(rows * 32 * sizeof(G)));
+            }
+        }
+    }
+#endif
     {
         const int s0 = geo.stage_start[tile], staged = geo.stage_start[tile + 1] - s0;
         constexpr int kRowsInFlight = 4;
@@ -296,12 +312,23 @@ __global__ void __launch_bounds__(kTileCells, MINB) k_sweep_tiles(MeshDev<D> m, 
     if (i >= 0) {
         // the cell's own row: tile cells are staged first, in thread order
         const double* own = rows + R * threadIdx.x;
-        double Wi[V], xi[D];
+        double Wi[V];
 #pragma unroll
         for (int v = 0; v < V; ++v) Wi[v] = own[v];
-        const double ci = own[V], ri = own[V + 1];
+        // The own row's sound speed, radius and generator are read from shared memory where they are used. FP64:
+        // volatile loads, not held in registers through walk 1, whose double sums need them all (measured at 128^3:
+        // the sweep 0.772 -> 0.747 ms); the float policies have registers to spare and keep them (0.546 against 0.601).
+        double held[3 + D];  // the float policies: c, r, the generator, read once
+        if constexpr (!exact) {
+            held[0] = own[V];
+            held[1] = own[V + 1];
 #pragma unroll
-        for (int a = 0; a < D; ++a) xi[a] = own[kStagedPos + a];
+            for (int a = 0; a < D; ++a) held[2 + a] = own[kStagedPos + a];
+        }
+        const auto own_at = [own, &held](int k) -> double {
+            if constexpr (exact) return lds_volatile(own + k);
+            else return k == V ? held[0] : k == V + 1 ? held[1] : held[2 + k - kStagedPos];
+        };
         G lo[V], hi[V], g[V * D];
 #pragma unroll
         for (int v = 0; v < V; ++v) {
@@ -312,7 +339,7 @@ __global__ void __launch_bounds__(kTileCells, MINB) k_sweep_tiles(MeshDev<D> m, 
         }
         // kBatch entries at a time: their streamed rows are all requested before any is used; the staged rows they
         // name are shared-memory reads.
-        constexpr int kBatch = KB;
+        constexpr int kBatch = KB > 0 ? KB : (exact ? 2 : 3);
         // The smallest face term courant (dist + r) / vsig, vsig = c_i + c_j - dv.d / dist (FaceStep), held as the
         // fraction num / den = (dist + r) dist / ((c_i + c_j) dist - dv.d) and compared by cross products: one division
         // a cell instead of two a face (the same minimum, rounded once).
@@ -355,11 +382,11 @@ __global__ void __launch_bounds__(kTileCells, MINB) k_sweep_tiles(MeshDev<D> m, 
 #pragma unroll
                     for (int a = 0; a < D; ++a) {
                         dv[a] = pj[1 + a] - Wi[1 + a];
-                        d[a] = m.wrap(rj[kStagedPos + a] - xi[a], a);  // Geometry::separation of owner and neighbour
+                        d[a] = m.wrap(rj[kStagedPos + a] - own_at(kStagedPos + a), a);  // Geometry::separation of owner and neighbour
                     }
                     const double dist = sqrt(dot<D>(d, d));
                     // Both cells' terms: the smaller radius gives the smaller one. den > 0 is vsig > 0.
-                    const double num = (dist + fmin(ri, pj[V + 1])) * dist, den = (ci + pj[V]) * dist - dot<D>(dv, d);
+                    const double num = (dist + fmin(own_at(V + 1), pj[V + 1])) * dist, den = (own_at(V) + pj[V]) * dist - dot<D>(dv, d);
                     if (den > 0 && num * best_den < best_num * den) {
                         best_num = num;
                         best_den = den;
@@ -382,6 +409,7 @@ __global__ void __launch_bounds__(kTileCells, MINB) k_sweep_tiles(MeshDev<D> m, 
             }
         }
         if (best_num < 1.0e300) smallest_dt = courant * (best_num / best_den);
+        const double ci = own_at(V), ri = own_at(V + 1);
         double wi[D];
 #pragma unroll
         for (int a = 0; a < D; ++a) wi[a] = Wi[1 + a];
@@ -434,6 +462,17 @@ __global__ void __launch_bounds__(kTileCells, MINB) k_sweep_tiles(MeshDev<D> m, 
                     round_off_only = round_off_only && gg * reach2 <= kNoise2 * (scale * scale);
                 }
             }
+#if LUNA_SWEEP_L2_PREFETCH >= 2
+            if constexpr (Limit != 0) {  // the warp's walk-2 offset rows, when a lane of it clips
+                const unsigned int here = __activemask();
+                const unsigned int need = __ballot_sync(here, !round_off_only);
+                if (need && static_cast<int>(threadIdx.x & 31) == __ffs(here) - 1) {
+                    const int64_t rows = geo.slice_base[(t >> 5) + 1] - geo.slice_base[t >> 5];
+                    prefetch_l2(geo.off01 + row0, static_cast<unsigned int>(rows * 32 * sizeof(Pair<G>)));
+                    if constexpr (D == 3) prefetch_l2(geo.off2 + row0, static_cast<unsigned int>(rows * 32 * sizeof(G)));
+                }
+            }
+#endif
             if constexpr (Limit == 2) if (!(learned.cells && round_off_only)) {
                 // The admissible factor per variable: the smallest over the faces (tiny ones left out) of the factor that
                 // puts the face value on its bound, max(room, 0) / |dp|, the min-factor form of the limiter

@@ -126,6 +126,13 @@ __device__ __forceinline__ void prefetch_l2(const void* p, unsigned int bytes) {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
+// A shared-memory load the compiler keeps where it is written (not hoisted, not merged with another).
+__device__ __forceinline__ double lds_volatile(const double* p) {
+    double v;
+    asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(static_cast<unsigned int>(__cvta_generic_to_shared(p))));
+    return v;
+}
+
 // Asynchronous copies global -> shared (no registers held while in flight); cp_async_wait_all waits for this
 // thread's copies, a barrier after it makes them visible to the block. 16 B: both addresses 16-B aligned; 8 B: 8-B.
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
