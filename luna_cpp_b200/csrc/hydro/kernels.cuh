@@ -487,9 +487,37 @@ __global__ void __launch_bounds__(128) k_flux(MeshDev<D> m, FluxArgs<D, G> x, do
     block_sum_to(static_cast<unsigned long long>(count), fallbacks);
 }
 
+// A flux row of V doubles at p (8-B aligned) through the 32-B aligned 64-B window that holds it (V <= 5: a row starts at
+// most 24 B into its window): two 256-bit loads instead of V scalar ones, the row picked out of the window by its offset
+// (V = 4: rows are 32 B, aligned, one load). The buffer must be 32-B aligned and extend at least 24 B past its last row.
+template <int V>
+__device__ __forceinline__ void load_row_windowed(const double* p, double* row) {
+    static_assert(V == 4 || V == 5, "2D or 3D flux rows");
+    if constexpr (V == 4) {  // 32-B rows of a 32-B aligned buffer: one load
+        double w[4];
+        ldg256(p, w);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) row[v] = w[v];
+    } else {
+        const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+        const double* w = reinterpret_cast<const double*>(a & ~static_cast<uintptr_t>(31));
+        const int off = static_cast<int>((a >> 3) & 3);
+        double win[8];
+        ldg256(w, win);
+        ldg256(w + 4, win + 4);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            const double lo = (off & 1) ? win[v + 1] : win[v];
+            const double hi = (off & 1) ? win[v + 3] : win[v + 2];
+            row[v] = (off & 2) ? hi : lo;
+        }
+    }
+}
+
 // apply()'s update (finite_volume.hpp:1603-1615): Q_i -= dt sum_k sign_k F_k in list order; NextPrims: the next
 // primitive rows (a moving step's second pass; here every per-face step, which makes the next primitives() pass free).
-template <int D, bool NextPrims>
+// Windowed: flux rows through load_row_windowed (the library's own flux buffer, padded for it).
+template <int D, bool NextPrims, bool Windowed = false>
 __global__ void __launch_bounds__(256) k_update(MeshDev<D> m, double* __restrict__ q, const double* __restrict__ flux, double dt,
                                                 double* __restrict__ prims, GasDev gas, Counters* __restrict__ ctr) {
     constexpr int V = D + 2;
@@ -511,8 +539,12 @@ __global__ void __launch_bounds__(256) k_update(MeshDev<D> m, double* __restrict
         for (int b = 0; b < kBatch; ++b) {
             if (k0 + b < end) {
                 const double* r = flux + V * static_cast<int64_t>(list_face(e[b]));
+                if constexpr (Windowed) {
+                    load_row_windowed<V>(r, row[b]);
+                } else {
 #pragma unroll
-                for (int v = 0; v < V; ++v) row[b][v] = __ldg(r + v);
+                    for (int v = 0; v < V; ++v) row[b][v] = __ldg(r + v);
+                }
             }
         }
 #pragma unroll

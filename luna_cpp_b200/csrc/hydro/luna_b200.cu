@@ -300,7 +300,8 @@ luna_status load_mesh(luna_fv* fv, const luna_mesh_desc* m) {
             luna::k_magnitudes<2><<<blocks(F, 256), 256, 0, s>>>(fv->area.ptr, fv->mag.ptr, static_cast<int>(F));
         LUNA_CUDA(cudaGetLastError());
     }
-    if (fv->update == LUNA_UPDATE_PER_FACE) LUNA_TRY(fv->flux.alloc(F * (D + 2) > 0 ? F * (D + 2) : 1, "flux rows"));
+    // 4 doubles past the last row: the update reads each row through its 32-B aligned 64-B window (load_row_windowed)
+    if (fv->update == LUNA_UPDATE_PER_FACE) LUNA_TRY(fv->flux.alloc(F * (D + 2) + 4, "flux rows"));
     // The sweep's tiles are cut on the host from the lists and the generators (copied back once per mesh when the
     // caller's arrays are on the device). Lists in device memory are trusted as voronoi-cpp's; the sweep does not
     // re-check them.
@@ -522,7 +523,7 @@ luna_status run_apply(luna_fv* fv, const G* grad, double dt) {
         LUNA_TRY((dispatch_flux_rows<D, 1, G>(fv, x)));
     {
         const long timed_ = fv->open_timed(3);
-        luna::k_update<D, true><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->q.ptr, fv->flux.ptr, dt, fv->prims.ptr, fv->gas,
+        luna::k_update<D, true, true><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->q.ptr, fv->flux.ptr, dt, fv->prims.ptr, fv->gas,
                                                                             fv->counters.ptr);
         fv->close_timed(timed_);
     }
@@ -571,7 +572,7 @@ luna_status moving_begin(luna_fv* fv, double dt) {
     }
     {
         const long timed_ = fv->open_timed(3);
-        luna::k_update<D, false><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->q.ptr, fv->flux.ptr, 0.5 * dt, fv->prims.ptr, fv->gas,
+        luna::k_update<D, false, true><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->q.ptr, fv->flux.ptr, 0.5 * dt, fv->prims.ptr, fv->gas,
                                                                              fv->counters.ptr);
         fv->close_timed(timed_);
     }
@@ -607,7 +608,7 @@ luna_status moving_end(luna_fv* fv) {
     }
     {
         const long timed_ = fv->open_timed(3);
-        luna::k_update<D, true><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->q.ptr, fv->flux.ptr, 0.5 * dt, fv->prims.ptr, fv->gas,
+        luna::k_update<D, true, true><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->q.ptr, fv->flux.ptr, 0.5 * dt, fv->prims.ptr, fv->gas,
                                                                             fv->counters.ptr);
         fv->close_timed(timed_);
     }
