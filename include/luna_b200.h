@@ -37,6 +37,8 @@ typedef enum {
 
 enum { LUNA_UPDATE_PER_CELL = 0, LUNA_UPDATE_PER_FACE = 1 };            /* hydro::Update (finite_volume.hpp:25) */
 enum { LUNA_LIMITER_FACE_CENTROID = 0, LUNA_LIMITER_NONE = 1 };         /* hydro::Limiter (finite_volume.hpp:29) */
+enum { LUNA_LIMITER_MINMOD = 2, LUNA_LIMITER_VAN_LEER = 3 };            /* the 1D slopes (finite_volume_1d.hpp:187-192) */
+enum { LUNA_WALL_REFLECTIVE = 0, LUNA_WALL_OUTFLOW = 1, LUNA_WALL_INFLOW = 2 }; /* hydro::Wall (finite_volume_1d.hpp:9) */
 enum { LUNA_STATIC_MESH = 0, LUNA_MOVING = 1 };                         /* hydro::Motion (finite_volume.hpp:31) */
 enum { LUNA_HLLC = 0, LUNA_HLL = 1 };                                   /* Riemann parameter (euler.hpp:444, :546) */
 /* Precision policies (precision.hpp:26-54): LUNA_FP64 is Precision<> (double throughout); LUNA_FP32 is the reference's
@@ -194,6 +196,29 @@ LUNA_API const char* luna_status_string(luna_status s);
 LUNA_API const char* luna_last_error(void);
 /* Device bytes held by fv (all its buffers). */
 LUNA_API luna_status luna_fv_device_bytes(luna_fv* fv, int64_t* out);
+
+/* ---- The 1D solver: hydro::FiniteVolume<1, Exec, Riemann, Precision<>> on a static line (src/hydro/finite_volume_1d.hpp).
+ * A batch of `lines` independent lines sharing one geometry: n_cells generators at `positions` (any order) on [0, length],
+ * snapped to voronoi-cpp's grid (step = length 2^-30), closed by two walls (LUNA_WALL_*, inflow: the primitives
+ * rho, v, P of each inflow wall, [2][3]) or periodic. Q is [lines][n_cells][3] (rho, rho v, E, extensive) in the caller's
+ * cell order. limiter: LUNA_LIMITER_FACE_CENTROID (LUNA's MC on a uniform line), NONE, MINMOD, VAN_LEER; riemann:
+ * LUNA_HLLC or LUNA_HLL. The moving line (cells supplied by inflow walls) and the derivatives are not covered. */
+typedef struct luna_line luna_line;
+/* FiniteVolume(exec, mesh, gas, order, limiter, static_mesh, walls) (finite_volume_1d.hpp:41-56). */
+LUNA_API luna_status luna_line_create(int64_t n_cells, int lines, const double* positions, double length, int periodic, const int* walls,
+                                      const double* inflow, const luna_gas* gas, int order, int limiter, int riemann, luna_line** out);
+LUNA_API luna_status luna_line_destroy(luna_line* ln);
+LUNA_API luna_status luna_line_set_stream(luna_line* ln, void* stream);
+/* Each cell's length and its centroid's offset from its generator (Line::volume, Line::centroid), caller order, host. */
+LUNA_API luna_status luna_line_geometry(luna_line* ln, double* volume, double* centroid);
+LUNA_API luna_status luna_line_set_state(luna_line* ln, const double* q, int on_device);
+LUNA_API luna_status luna_line_get_state(luna_line* ln, double* q, int on_device);
+/* time_step(courant, rule) (:332-384) of every line into dt_out [lines] (host); rule 0: AREPO's, 1: LUNA's. Synchronises. */
+LUNA_API luna_status luna_line_time_step(luna_line* ln, double courant, int rule, double* dt_out);
+/* step(dt) (:389-410): line k by dt[k] (host array [lines]). Asynchronous. */
+LUNA_API luna_status luna_line_step(luna_line* ln, const double* dt);
+/* step_and_time_step(dt, courant) (:412-418): the step and each line's next dt by LUNA's rule, one launch. Synchronises. */
+LUNA_API luna_status luna_line_step_and_time_step(luna_line* ln, const double* dt, double courant, double* dt_next);
 
 #ifdef __cplusplus
 }

@@ -90,6 +90,15 @@ SIGNATURES = {
     "luna_mlp_adam": ([P, P, P, P, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, I, P], I),
     "luna_fv_timings": ([P, P, I], I),
     "luna_mesh_tiles": ([P, P, P, P, P, P, P], I),
+    "luna_line_create": ([I64, I, P, D64, I, P, P, P, I, I, I, P], I),
+    "luna_line_destroy": ([P], I),
+    "luna_line_set_stream": ([P, P], I),
+    "luna_line_geometry": ([P, P, P], I),
+    "luna_line_set_state": ([P, P, I], I),
+    "luna_line_get_state": ([P, P, I], I),
+    "luna_line_time_step": ([P, D64, I, P], I),
+    "luna_line_step": ([P, P], I),
+    "luna_line_step_and_time_step": ([P, P, D64, P], I),
 }
 
 PHASES = ("primitives", "sweep", "fluxes", "update", "drift")

@@ -85,3 +85,97 @@ def rough_state(n, dim=3, gamma=5.0 / 3.0, seed=11) -> np.ndarray:
         W[:, 1 + a] = 0.5 * rng.uniform(-1, 1, n)
     W[:, dim + 1] = np.where(np.arange(n) < 8, 100.0, 1.0) * (1 + 0.3 * rng.uniform(-1, 1, n))
     return conserved(W, gamma)
+
+
+# ---- 1D lines (luna-cpp's src/hydro/problems_1d.hpp): cell averages of LUNA's setups on [a, b] -----------------------
+
+def _conserved_1d(W, gamma):
+    """problems_1d.hpp's conserved (:31-33), in its operation order."""
+    return np.stack([W[0], W[0] * W[1], W[2] / (gamma - 1) + 0.5 * W[0] * W[1] * W[1]], axis=-1)
+
+
+def _fraction_below(x, a, b):
+    return np.clip((x - a) / (b - a), 0.0, 1.0)
+
+
+def _tube(left, right, x0, gamma):
+    """A jump at x0: exact cell averages by volume fraction (problems_1d.hpp:37-43)."""
+    l = _conserved_1d(np.asarray(left, dtype=np.float64), gamma)
+    r = _conserved_1d(np.asarray(right, dtype=np.float64), gamma)
+
+    def average(a, b):
+        f = _fraction_below(x0, a, b)[:, None]
+        return f * l + (1 - f) * r
+
+    return average
+
+
+def _shock_into_wave(left, x0, amp, k, gamma):
+    """A shock at x0 into 1 + amp sin(k x): exact cell averages (problems_1d.hpp:46-51)."""
+
+    def average(a, b):
+        h = b - a
+        f = _fraction_below(x0, a, b)
+        lo = np.maximum(a, x0)
+        rho = f * left[0] + (1 - f)
+        rho = np.where(b > lo, rho + amp * (np.cos(k * lo) - np.cos(k * b)) / k / h, rho)
+        return np.stack([rho, f * left[0] * left[1],
+                         f * (left[2] / (gamma - 1) + 0.5 * left[0] * left[1] * left[1]) + (1 - f) / (gamma - 1)], axis=-1)
+
+    return average
+
+
+def _woodward_colella(a, b):
+    """Woodward-Colella's cell averages (problems_1d.hpp:55-60)."""
+    f1, f2 = _fraction_below(0.1, a, b), _fraction_below(0.9, a, b)
+    p = f1 * 1000 + (f2 - f1) * 0.01 + (1 - f2) * 100
+    return np.stack([np.ones_like(p), np.zeros_like(p), p / (1.4 - 1)], axis=-1)
+
+
+def line_problem(name: str) -> dict:
+    """A 1D problem of problems_1d.hpp's table (:207-243): the line [origin, origin + L], its walls, t_end, gamma and
+    ``average(a, b)``, the extensive-per-length conserved state of cells [a, b] (absolute coordinates, arrays)."""
+    outflow, closed = ("outflow", "outflow"), ("reflective", "reflective")
+    toro = {"sod": ((1.0, 0.0, 1.0), (0.125, 0.0, 0.1), 0.25), "toro-1": ((1.0, 0.0, 1.0), (0.125, 0.0, 0.1), 0.25),
+            "toro-2": ((1.0, -2.0, 0.4), (1.0, 2.0, 0.4), 0.15), "toro-3": ((1.0, 0.0, 1000.0), (1.0, 0.0, 0.01), 0.012),
+            "toro-4": ((1.0, 0.0, 0.01), (1.0, 0.0, 100.0), 0.035),
+            "toro-5": ((5.99924, 19.5975, 460.894), (5.99242, -6.19633, 46.0950), 0.035)}
+    if name in toro:
+        left, right, t_end = toro[name]
+        return {"L": 1.0, "origin": 0.0, "t_end": t_end, "gamma": 1.4, "walls": outflow,
+                "average": _tube(left, right, 0.5, 1.4)}
+    if name == "shu-osher":
+        return {"L": 10.0, "origin": -5.0, "t_end": 1.8, "gamma": 1.4, "walls": outflow,
+                "average": _shock_into_wave((3.857143, 2.629369, 10.33333), -4.0, 0.2, 5.0, 1.4)}
+    if name == "woodward-colella":
+        return {"L": 1.0, "origin": 0.0, "t_end": 0.038, "gamma": 1.4, "walls": closed, "average": _woodward_colella}
+    raise ValueError(f"unknown 1D problem {name!r}")
+
+
+def line_tube(left, right, t_end: float, x0: float = 0.5, gamma: float = 1.4, walls=("outflow", "outflow"), L: float = 1.0) -> dict:
+    """A Riemann problem on [0, L] (problems_1d.hpp's tube, :37-43): primitives left of x0 and right of it."""
+    return {"L": L, "origin": 0.0, "t_end": t_end, "gamma": gamma, "walls": tuple(walls), "average": _tube(left, right, x0, gamma)}
+
+
+def line_keys(positions, L: float):
+    """The generators of a line of length L on voronoi-cpp's snapping grid (step = L 2^-30, period 2^30 steps): sorted
+    keys, the slot -> position order, the step and the period."""
+    x = np.asarray(positions, dtype=np.float64)
+    step = np.ldexp(L, -30)
+    keys = np.rint(x / step).astype(np.int64)
+    order = np.argsort(keys, kind="stable")
+    return keys[order], order, float(step), 1 << 30
+
+
+def line_state(problem: dict, keys, step: float) -> np.ndarray:
+    """Q [n, 3] in slot order: each cell's average of the problem over its extent (midway to its neighbours, to a wall at
+    the ends), as hydro1d_test.cpp's set() fills it (:40-55)."""
+    k = np.asarray(keys, dtype=np.float64)
+    gaps = np.concatenate([[2 * k[0]], np.diff(k), [2 * ((1 << 30) - k[-1])]])
+    volume = (gaps[:-1] + gaps[1:]) * (0.5 * step)
+    centroid = (gaps[1:] - gaps[:-1]) * (0.25 * step)
+    x = k * step
+    a = x + centroid - 0.5 * volume
+    b = x + centroid + 0.5 * volume
+    U = problem["average"](a + problem["origin"], b + problem["origin"])
+    return U * (b - a)[:, None]

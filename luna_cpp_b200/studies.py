@@ -13,6 +13,8 @@ comparisons of the same configurations are GPU tests).
 - ``learned``: the learned limiter on the static 3D point blast: its density L1 against the method's own run at 4x the
   resolution per axis, beside the plain limiter at the same and at finer resolutions, with device times; the GPU time
   the plain limiter needs for the learned limiter's error, over the learned run's.
+- ``lines``: the 1D solver as the learned limiter's data factory: a batch of seeded Riemann problems on lines of nx
+  cells, one launch a step; cell-updates/s beside the oracle's on one line.
 - ``adjoint``: 2D Voronoi mesh from nx^2 jittered generators, the shear layer with a_k ~ N(0, 1) from the seed, 200
   steps; d/da_k of int rho vy^2 dA at the final time by the hand-written adjoint with checkpoints every 20 steps,
   against central differences (h = 1e-6) on the same dt schedule; device time of the forward and of the backward.
@@ -21,6 +23,7 @@ comparisons of the same configurations are GPU tests).
     python -m luna_cpp_b200.studies adjoint --nx 512 --steps 200 --out adjoint.json
     python -m luna_cpp_b200.studies moving --nx 32 --out moving.json
     python -m luna_cpp_b200.studies learned --nx 48 --out learned.json
+    python -m luna_cpp_b200.studies lines --nx 4096 --out lines.json
 """
 from __future__ import annotations
 
@@ -261,6 +264,54 @@ def learned_blast(nx=48, factor=4, plain_nx=(48, 56, 64, 72, 80), t_end=0.05, co
     return out
 
 
+def lines(nx=4096, batch=1024, steps=200, courant=0.8, seed=9000, log=print) -> dict:
+    """The 1D solver as the learned limiter's data factory: ``batch`` seeded Riemann problems (the training
+    distribution) on lines of nx uniform cells between outflow walls, all in one launch a step: ``steps`` fused steps
+    (step_and_time_step, LUNA's rule), device time by CUDA events, cell-updates/s; and the oracle on one of the lines for
+    the CPU's rate."""
+    import torch
+
+    from oracle import oracle as O
+
+    from .limiter_training import riemann_problem
+    from .line import Line
+    from .problems import line_keys, line_state, line_tube
+
+    x = (np.arange(nx) + 0.5) / nx
+    keys, order, step, period = line_keys(x, 1.0)
+    q0 = np.stack([line_state(line_tube(*((r.rho[k], r.u[k], r.p[k]) for k in (0, 1)), t_end=1.0), keys, step)
+                   for r in (riemann_problem(seed + b) for b in range(batch))])
+    ln = Line(x, 1.0, lines=batch)
+    ln.set_state(q0)
+    dt = ln.time_step(courant, "luna")
+    for _ in range(5):
+        dt = ln.step_and_time_step(dt, courant)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record()
+    for _ in range(steps):
+        dt = ln.step_and_time_step(dt, courant)
+    end.record()
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(end)
+    q = ln.get_state()
+    ln.close()
+    ref = O.OracleLine(keys, step, period, gamma=1.4)
+    ref.set_state(q0[0])
+    t0 = time.perf_counter()
+    cpu_steps = 20
+    for _ in range(cpu_steps):
+        ref.step(ref.time_step(courant, "luna"))
+    cpu_s = time.perf_counter() - t0
+    out = {"config": {"cells": nx, "lines": batch, "steps": steps, "courant": courant, "rule": "luna", "fused": True},
+           "device_ms_per_step": ms / steps, "cell_updates_per_s": nx * batch * steps / (ms * 1e-3),
+           "finite": bool(np.all(np.isfinite(q))),
+           "oracle_cell_updates_per_s": nx * cpu_steps / cpu_s, "oracle_threads": O.threads(0)}
+    log(f"{batch} lines x {nx} cells: {ms / steps:.3f} ms/step, {out['cell_updates_per_s'] / 1e9:.2f} G cell-updates/s "
+        f"(oracle, one line: {out['oracle_cell_updates_per_s'] / 1e6:.1f} M/s)")
+    return out
+
+
 def adjoint(nx=512, steps=200, every=20, h=1e-6, seed=3, courant=0.3, threads=0, log=print) -> dict:
     import torch
 
@@ -325,7 +376,7 @@ def adjoint(nx=512, steps=200, every=20, h=1e-6, seed=3, courant=0.3, threads=0,
 
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("study", choices=["precision", "adjoint", "moving", "learned"])
+    ap.add_argument("study", choices=["precision", "adjoint", "moving", "learned", "lines"])
     ap.add_argument("--nx", type=int)
     ap.add_argument("--steps", type=int)
     ap.add_argument("--threads", type=int, default=0)
@@ -338,7 +389,10 @@ def main():
         kw["steps"] = args.steps
     if args.study in ("moving", "learned"):
         kw.pop("steps", None)
-    res = {"precision": precision, "adjoint": adjoint, "moving": moving, "learned": learned_blast}[args.study](**kw)
+    if args.study == "lines":
+        kw.pop("threads", None)
+    res = {"precision": precision, "adjoint": adjoint, "moving": moving, "learned": learned_blast,
+           "lines": lines}[args.study](**kw)
     text = json.dumps(res, indent=1)
     if args.out:
         with open(args.out, "w") as f:

@@ -74,6 +74,21 @@ void lo_fv_step_adjoint(lo_fv* fv, double dt, double* qbar);
 /* The snapping grid of a box (voronoi-cpp's exact_predicates): step = 2^-30 of the longest side. */
 double lo_grid_step(int D, const double* box);
 
+/* FiniteVolume<1> on a static line (oracle_line.c; src/hydro/finite_volume_1d.hpp). keys: the generators' sorted grid
+ * keys in [0, period]; walls: LO_WALL_* left, right (ignored when periodic); inflow: [2][3] primitives of inflow walls;
+ * limiter: LO_LIMITER_*; riemann: 0 HLLC, 1 HLL. The state is Q [n][3] in slot (key) order. */
+enum { LO_WALL_REFLECTIVE = 0, LO_WALL_OUTFLOW = 1, LO_WALL_INFLOW = 2 };
+enum { LO_LIMITER_FACE_CENTROID = 0, LO_LIMITER_NONE = 1, LO_LIMITER_MINMOD = 2, LO_LIMITER_VAN_LEER = 3 };
+typedef struct lo_line lo_line;
+lo_line* lo_line_create(int n, const int64_t* keys, int64_t period, double step, int periodic, const int* walls, const double* inflow,
+                        const lo_gas* gas, int order, int limiter, int riemann);
+void lo_line_destroy(lo_line* ln);
+double* lo_line_state(lo_line* ln);
+const double* lo_line_volumes(const lo_line* ln);
+const double* lo_line_centroids(const lo_line* ln);
+double lo_line_time_step(const lo_line* ln, double courant, int rule /* 0 AREPO's, 1 LUNA's */);
+void lo_line_step(lo_line* ln, double dt);
+
 #ifdef __cplusplus
 }
 #endif

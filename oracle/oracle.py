@@ -66,6 +66,19 @@ def lib():
         fn = getattr(L, name)
         fn.argtypes = args
         fn.restype = res
+    line_sig = {
+        "lo_line_create": ([ctypes.c_int, P, ctypes.c_int64, D, I, P, P, P, I, I, I], P),
+        "lo_line_destroy": ([P], V),
+        "lo_line_state": ([P], P),
+        "lo_line_volumes": ([P], P),
+        "lo_line_centroids": ([P], P),
+        "lo_line_time_step": ([P, D, I], D),
+        "lo_line_step": ([P, D], V),
+    }
+    for name, (args, res) in line_sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
     if hasattr(L, "lo_fv_step_adjoint"):
         L.lo_fv_step_adjoint.argtypes = [P, D, P]
         L.lo_fv_step_adjoint.restype = None
@@ -206,3 +219,50 @@ class OracleFV:
 
 def threads(n: int = 0) -> int:
     return int(lib().lo_fv_threads(n))
+
+
+WALLS = {"reflective": 0, "outflow": 1, "inflow": 2}
+LIMITERS = {"face_centroid": 0, "none": 1, "minmod": 2, "van_leer": 3}
+RULES = {"arepo": 0, "luna": 1}
+
+
+class OracleLine:
+    """FiniteVolume<1> on a static line (oracle_line.c): sorted grid keys, walls or periodic; Q [n, 3] in slot order."""
+
+    def __init__(self, keys, step, period=1 << 30, gamma=1.4, walls=("outflow", "outflow"), periodic=False, inflow=None,
+                 order=1, limiter="face_centroid", riemann="hllc"):
+        self.keys = np.ascontiguousarray(keys, dtype=np.int64)
+        self.n = len(self.keys)
+        self._gas = gas(gamma)
+        w = np.array([WALLS[walls[0]], WALLS[walls[1]]], dtype=np.int32)
+        inflow = np.zeros((2, 3)) if inflow is None else np.ascontiguousarray(inflow, dtype=np.float64)
+        self._keep = (w, inflow)
+        self._h = lib().lo_line_create(self.n, _ptr(self.keys), int(period), float(step), int(periodic), _ptr(w), _ptr(inflow),
+                                       ctypes.byref(self._gas), order, LIMITERS[limiter], 0 if riemann == "hllc" else 1)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().lo_line_destroy(self._h)
+            self._h = None
+
+    def _view(self, ptr, shape):
+        buf = (ctypes.c_double * int(np.prod(shape))).from_address(ptr)
+        return np.frombuffer(buf, dtype=np.float64).reshape(shape)
+
+    def set_state(self, q):
+        self._view(lib().lo_line_state(self._h), (self.n, 3))[:] = q
+
+    def get_state(self):
+        return self._view(lib().lo_line_state(self._h), (self.n, 3)).copy()
+
+    def volumes(self):
+        return self._view(lib().lo_line_volumes(self._h), (self.n,)).copy()
+
+    def centroids(self):
+        return self._view(lib().lo_line_centroids(self._h), (self.n,)).copy()
+
+    def time_step(self, courant, rule="arepo"):
+        return float(lib().lo_line_time_step(self._h, courant, RULES[rule]))
+
+    def step(self, dt):
+        lib().lo_line_step(self._h, dt)
