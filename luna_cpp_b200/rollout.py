@@ -1,0 +1,169 @@
+"""The rollout server of luna-cpp (src/examples/rollout.cpp) on libluna_b200: a fixed-dt rollout of the 2D or 3D step
+on the Voronoi mesh of the regular n^D lattice of the periodic unit box, and its reverse-mode derivative, served one
+command a line on stdin for Python optimisers (the reference's scripts/examples/rollout_client.py drives it unchanged:
+``Rollout("luna_cpp_b200/bin/rollout", dim, n, steps, dt, workdir)``).
+
+    python -m luna_cpp_b200.rollout --dim=2 --n=64 --steps=100 --dt=1e-3 [--gamma=5/3] [--courant=0.3]
+
+Commands (paths are raw float64 files, C order; cells in lattice C order, the last axis fastest):
+    forward <U0 in> <final out>       U0: N x V intensive; runs the steps keeping the tape (on the device); final: N x
+                                      (V + D + 1) rows of (Q extensive, x, volume). Answers "ok <ms> <cfl violations>".
+    adjoint <bars in> <U0bar out>     bars: N x (V + D + 1) at the end of the last forward; U0bar = dL/dU0 (intensive).
+                                      On the static mesh x and the volumes do not depend on U0: their bars drop out.
+    cfl <U0 in>                       "ok <time_step(courant) at U0>".
+    geometry <out>                    N x (D + 1) rows of (x, volume). Answers "ok".
+    memory                            "ok <peak device bytes> <bytes now>" (the step's buffers and the tape).
+    quit
+The fixed dt is checked against time_step(courant) of every step; the steps where it is larger are counted.
+``tangent`` and ``--moving`` answer an error: the step's tangent and the moving mesh's derivatives are not in the
+library.
+"""
+from __future__ import annotations
+
+import sys
+import time
+
+import numpy as np
+
+
+def flag(argv, name, fallback):
+    for a in argv:
+        if a.startswith(name + "="):
+            return a[len(name) + 1:]
+    return fallback
+
+
+def lattice(side: int, dim: int) -> np.ndarray:
+    """Rollout::lattice (rollout.cpp:119-133): the cell centres on the 2^-30 grid, C order (the last axis fastest)."""
+    step = 2.0 ** -30
+    idx = np.stack(np.meshgrid(*[np.arange(side)] * dim, indexing="ij"), -1).reshape(-1, dim)
+    return np.floor((idx + 0.5) / side / step) * step
+
+
+class Server:
+    def __init__(self, dim: int, side: int, steps: int, dt: float, gamma: float, courant: float):
+        import torch
+
+        from .hydro import FiniteVolume, Gas
+        from .mesh import build_mesh
+
+        self.torch = torch
+        self.dim, self.steps, self.dt, self.courant = dim, steps, dt, courant
+        self.V = dim + 2
+        self.x0 = lattice(side, dim)
+        self.mesh = build_mesh(self.x0, box=(1.0,) * dim)
+        self.n = self.mesh.n_cells
+        self.V0 = self.mesh.volume.copy()
+        self.fv = FiniteVolume(self.mesh, Gas(gamma), order=1, update="per_face", limiter="face_centroid")
+        self.tape = torch.empty((steps, self.n, self.V), dtype=torch.float64, device="cuda")
+        self.volume_dev = torch.tensor(self.V0, device="cuda")[:, None]
+        self.peak = self.now()
+
+    def now(self) -> int:
+        return int(self.fv.device_bytes() + self.tape.numel() * 8)
+
+    def load(self, U0: np.ndarray) -> None:
+        self.fv.set_state(np.ascontiguousarray(U0.reshape(self.n, self.V) * self.V0[:, None]))
+
+    def forward(self, U0: np.ndarray) -> int:
+        self.load(U0)
+        violations = 0
+        for s in range(self.steps):
+            self.fv.get_state(out=self.tape[s])
+            violations += self.fv.time_step(self.courant) < self.dt
+            self.fv.step(self.dt)
+        return violations
+
+    def final_rows(self) -> np.ndarray:
+        w = self.V + self.dim + 1
+        rows = np.empty((self.n, w))
+        rows[:, :self.V] = self.fv.get_state()
+        rows[:, self.V:self.V + self.dim] = self.x0
+        rows[:, -1] = self.V0
+        return rows
+
+    def adjoint(self, bars: np.ndarray) -> np.ndarray:
+        w = self.V + self.dim + 1
+        qbar = self.torch.tensor(np.ascontiguousarray(bars.reshape(self.n, w)[:, :self.V]), device="cuda")
+        for s in range(self.steps - 1, -1, -1):
+            self.fv.set_state(self.tape[s])
+            self.fv.step_adjoint(self.dt, qbar)
+        return (qbar * self.volume_dev).cpu().numpy()
+
+    def cfl(self, U0: np.ndarray) -> float:
+        self.load(U0)
+        return self.fv.time_step(self.courant)
+
+    def geometry(self) -> np.ndarray:
+        return np.concatenate([self.x0, self.V0[:, None]], axis=1)
+
+
+def now_ms(torch) -> float:
+    torch.cuda.synchronize()
+    return time.perf_counter() * 1e3
+
+
+def serve(argv, stdin=sys.stdin, stdout=sys.stdout) -> int:
+    if any(a == "--moving" for a in argv):
+        stdout.write("error the moving mesh's rollout needs its derivatives, which libluna_b200 does not have\n")
+        stdout.flush()
+        return 1
+    dim = int(flag(argv, "--dim", "2"))
+    srv = Server(dim, int(flag(argv, "--n", "64")), int(flag(argv, "--steps", "100")), float(flag(argv, "--dt", "1e-3")),
+                 float(flag(argv, "--gamma", "1.6666666666666667")), float(flag(argv, "--courant", "0.3")))
+    torch = srv.torch
+    N, V, w = srv.n, srv.V, srv.V + dim + 1
+
+    def answer(text):
+        stdout.write(text + "\n")
+        stdout.flush()
+
+    for line in stdin:
+        parts = line.split()
+        if not parts:
+            continue
+        cmd, args = parts[0], parts[1:]
+        try:
+            if cmd == "quit":
+                break
+            if cmd == "forward":
+                U0 = np.fromfile(args[0], dtype=np.float64, count=N * V)
+                t0 = now_ms(torch)
+                violations = srv.forward(U0)
+                ms = now_ms(torch) - t0
+                srv.final_rows().tofile(args[1])
+                srv.peak = max(srv.peak, srv.now())
+                answer(f"ok {ms:.17g} {violations}")
+            elif cmd == "adjoint":
+                bars = np.fromfile(args[0], dtype=np.float64, count=N * w)
+                t0 = now_ms(torch)
+                out = srv.adjoint(bars)
+                ms = now_ms(torch) - t0
+                out.tofile(args[1])
+                answer(f"ok {ms:.17g}")
+            elif cmd == "cfl":
+                answer(f"ok {srv.cfl(np.fromfile(args[0], dtype=np.float64, count=N * V)):.17g}")
+            elif cmd == "geometry":
+                srv.geometry().tofile(args[0])
+                answer("ok")
+            elif cmd == "memory":
+                answer(f"ok {srv.peak} {srv.now()}")
+            elif cmd == "tangent":
+                answer("error tangent: the step's tangent is not in libluna_b200")
+            else:
+                answer("error unknown command")
+        except Exception as e:  # one answer a line, as the reference's server: the client raises on anything but ok
+            answer(f"error {type(e).__name__}: {e}".replace("\n", " "))
+    return 0
+
+
+def main():
+    argv = sys.argv[1:]
+    if "--help" in argv:
+        print(__doc__)
+        return 0
+    return serve(argv)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

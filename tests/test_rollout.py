@@ -1,0 +1,101 @@
+"""The rollout server (luna_cpp_b200/rollout.py, the protocol of the reference's src/examples/rollout.cpp): the host side on
+the CPU, the served forward and adjoint on the GPU (checked against central differences through the protocol itself)."""
+import io
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from luna_cpp_b200 import rollout
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BIN = os.path.join(ROOT, "luna_cpp_b200", "bin", "rollout")
+
+
+def test_lattice_is_c_order_on_the_grid():
+    x = rollout.lattice(4, 3)
+    assert x.shape == (64, 3)
+    assert np.allclose(x[1], [0.125, 0.125, 0.375]) and np.allclose(x[4], [0.125, 0.375, 0.125])
+    assert np.all(np.round(x * 2 ** 30) == x * 2 ** 30)
+
+
+def test_moving_is_refused_with_an_error_line():
+    out = io.StringIO()
+    assert rollout.serve(["--dim=2", "--moving"], io.StringIO("quit\n"), out) == 1
+    assert out.getvalue().startswith("error ")
+
+
+class Client:
+    """A minimal client of the protocol (one command a line, raw float64 files)."""
+
+    def __init__(self, tmp, dim, n, steps, dt):
+        self.dim, self.N, self.V, self.tmp = dim, n ** dim, dim + 2, tmp
+        self.p = subprocess.Popen([BIN, f"--dim={dim}", f"--n={n}", f"--steps={steps}", f"--dt={dt!r}"], stdin=subprocess.PIPE,
+                                  stdout=subprocess.PIPE, text=True, bufsize=1)
+
+    def ask(self, line):
+        self.p.stdin.write(line + "\n")
+        self.p.stdin.flush()
+        return self.p.stdout.readline().split()
+
+    def forward(self, U0):
+        U0.astype(np.float64).tofile(self.tmp / "u0.bin")
+        out = self.ask(f"forward {self.tmp / 'u0.bin'} {self.tmp / 'fin.bin'}")
+        assert out[0] == "ok", out
+        return np.fromfile(self.tmp / "fin.bin").reshape(self.N, self.V + self.dim + 1), int(out[2])
+
+    def close(self):
+        self.p.stdin.write("quit\n")
+        self.p.stdin.flush()
+        assert self.p.wait(timeout=60) == 0
+
+
+@pytest.mark.gpu
+def test_served_adjoint_matches_central_differences(cuda, tmp_path):
+    """A 2D shear layer on the 32^2 lattice, 12 steps at a fixed dt: dL/dU0 from `adjoint` against central differences of
+    `forward` along a smooth direction (L = <bars, final rows>); `cfl`, `geometry`, `memory` and `tangent` answer."""
+    c = Client(tmp_path, 2, 32, 12, 2e-3)
+    try:
+        xc = (np.arange(32) + 0.5) / 32
+        X, Y = np.meshgrid(xc, xc, indexing="ij")
+        # the shear layer with smooth sides and a little seeded noise: on the lattice an exactly symmetric state puts
+        # the limiter's comparisons on ties, kinks at the very point the differences are taken
+        noise = np.random.default_rng(8).uniform(-1e-3, 1e-3, (4,) + X.shape)
+        layer = np.tanh((0.25 - np.abs(Y - 0.5)) / 0.05)
+        rho = 1.5 + 0.5 * layer + noise[0]
+        vx = 0.5 * layer + noise[1]
+        vy = 0.01 * np.sin(2 * np.pi * X) + noise[2]
+        P = 2.5 + noise[3]
+        U0 = np.stack([rho, rho * vx, rho * vy, P / (2 / 3) + 0.5 * rho * (vx * vx + vy * vy)], -1).reshape(-1, 4)
+        ok = c.ask(f"geometry {tmp_path / 'g.bin'}")
+        assert ok == ["ok"]
+        g = np.fromfile(tmp_path / "g.bin").reshape(-1, 3)
+        assert np.allclose(g[:, 2], 1 / 1024) and np.allclose(g[33, :2], [1.5 / 32, 1.5 / 32])
+        U0.tofile(tmp_path / "u0.bin")
+        out = c.ask(f"cfl {tmp_path / 'u0.bin'}")
+        assert out[0] == "ok" and float(out[1]) > 2e-3
+        fin, violations = c.forward(U0)
+        assert violations == 0 and np.all(np.isfinite(fin))
+        rng = np.random.default_rng(4)
+        bars = np.zeros_like(fin)
+        bars[:, :4] = rng.standard_normal((fin.shape[0], 4))
+        bars.tofile(tmp_path / "bars.bin")
+        out = c.ask(f"adjoint {tmp_path / 'bars.bin'} {tmp_path / 'ubar.bin'}")
+        assert out[0] == "ok", out
+        ubar = np.fromfile(tmp_path / "ubar.bin").reshape(-1, 4)
+        # along a smooth direction (a mode of the layer's vy), as the library's adjoint tests: a random field would
+        # move the limiter's clips within h, where the adjoint (one branch) and the differences part
+        d = np.zeros_like(U0)
+        d[:, 2] = (rho * np.sin(4 * np.pi * X)).reshape(-1)
+        d[:, 3] = (rho * vy * np.sin(4 * np.pi * X)).reshape(-1)
+        h = 1e-7  # the limiter's branches: at 1e-6 some clips switch within +-h over 12 steps (differences off by 8e-4)
+        Lp = float((c.forward(U0 + h * d)[0] * bars).sum())
+        Lm = float((c.forward(U0 - h * d)[0] * bars).sum())
+        fd = (Lp - Lm) / (2 * h)
+        assert abs(float((ubar * d).sum()) - fd) <= 1e-6 * abs(fd)
+        out = c.ask("memory")
+        assert out[0] == "ok" and int(out[1]) >= int(out[2]) > 0
+        assert c.ask(f"tangent {tmp_path / 'u0.bin'} {tmp_path / 'u0.bin'} {tmp_path / 'x.bin'}")[0] == "error"
+    finally:
+        c.close()
