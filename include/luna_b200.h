@@ -126,6 +126,10 @@ LUNA_API luna_status luna_fv_gradients(luna_fv* fv, double* out, int on_device);
  * per-face loop and the FP64 policy (else LUNA_EINVAL, as the reference's logic_error, :1674-1679). No atomics: the
  * same bits every run. */
 LUNA_API luna_status luna_fv_step_adjoint(luna_fv* fv, double dt, double* qbar, int on_device);
+/* step_tangent(dt, dq) (finite_volume.hpp:2023-2062): the step of step(dt) and, beside it, dq [N][D + 2] <- J dq (the
+ * tangent of Q, extensive) at fixed dt, linearised at the same point as luna_fv_step_adjoint (so the two are transposes:
+ * <J dq, qbar> = <dq, J^T qbar>). Q advances as luna_fv_step(fv, dt) advances it. The same restrictions as the adjoint. */
+LUNA_API luna_status luna_fv_step_tangent(luna_fv* fv, double dt, double* dq, int on_device);
 
 /* Per-phase device time (hydro::Timings, finite_volume.hpp:36-39, without its fences): with timing on, CUDA events on
  * fv's stream bracket every kernel; luna_fv_timings synchronises, adds the elapsed times since the last reset and counts

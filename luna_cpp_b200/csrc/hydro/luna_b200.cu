@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "adjoint.cuh"
+#include "tangent.cuh"
 #include "geometry.cuh"
 #include "kernels.cuh"
 #include "mlp.cuh"
@@ -119,6 +120,8 @@ struct luna_fv {
     bool learned_inputs = false, apply_learned = false;
     // adjoint (allocated by the first luna_fv_step_adjoint)
     DevArray<double> adj_fit, adj_face_bar, adj_wbar, adj_bbar, adj_boundbar, adj_qbar;
+    // tangent (allocated by the first luna_fv_step_tangent): dW, dg per cell, dF per face, a device copy of dq
+    DevArray<double> tan_dprims, tan_dgrad, tan_dflux, tan_dq;
     DevArray<int32_t> adj_flags, adj_bound_face;
     luna::Counters* host_counters = nullptr;  // pinned
 
@@ -671,6 +674,56 @@ luna_status run_adjoint(luna_fv* fv, double dt, double* qbar) {
     return LUNA_OK;
 }
 
+// step_tangent (finite_volume.hpp:2023-2062) before the step: dq <- J dq at fixed dt, linearised where step_adjoint is
+// (the reference's fit and clip pattern, k_sweep_fit), then the production step advances Q.
+template <int D>
+luna_status run_tangent(luna_fv* fv, double dt, double* dq) {
+    constexpr int V = D + 2;
+    using FL = luna::FitLayout<D>;
+    const size_t N = static_cast<size_t>(fv->n), F = static_cast<size_t>(fv->f);
+    LUNA_TRY(fv->adj_fit.alloc(N * FL::width, "adjoint fit rows"));
+    LUNA_TRY(fv->adj_flags.alloc(N * 2 * V, "adjoint flags"));
+    LUNA_TRY(fv->tan_dprims.alloc(N * V, "tangent dW"));
+    LUNA_TRY(fv->tan_dgrad.alloc(N * V * D, "tangent dg"));
+    LUNA_TRY(fv->tan_dflux.alloc(F > 0 ? F * V : 1, "tangent dF"));
+    const auto m = fv->mesh_dev<D>();
+    LUNA_TRY(run_primitives<D>(fv));
+    {
+        const long timed_ = fv->open_timed(1);
+        if (fv->limiter == LUNA_LIMITER_NONE)
+            luna::k_sweep_fit<D, false><<<blocks(N, kBlockCells), kBlockCells, 0, fv->stream>>>(m, fv->prims.ptr, fv->grad64.ptr, fv->adj_fit.ptr,
+                                                                                              fv->adj_flags.ptr);
+        else
+            luna::k_sweep_fit<D, true><<<blocks(N, kBlockCells), kBlockCells, 0, fv->stream>>>(m, fv->prims.ptr, fv->grad64.ptr, fv->adj_fit.ptr,
+                                                                                             fv->adj_flags.ptr);
+        luna::k_tangent_prims<D><<<blocks(N, 256), 256, 0, fv->stream>>>(static_cast<int>(N), fv->q.ptr, dq, fv->vol.ptr, fv->gas, fv->tan_dprims.ptr);
+        luna::k_tangent_sweep<D><<<blocks(N, kBlockCells), kBlockCells, 0, fv->stream>>>(m, fv->prims.ptr, fv->tan_dprims.ptr, fv->adj_fit.ptr,
+                                                                                        fv->adj_flags.ptr, fv->tan_dgrad.ptr);
+        fv->close_timed(timed_);
+    }
+    LUNA_CUDA(cudaGetLastError());
+    if (F > 0) {
+        const long timed_ = fv->open_timed(2);
+        if (fv->riemann == LUNA_HLL)
+            luna::k_tangent_fluxes<D, 1><<<blocks(F, kBlockFaces), kBlockFaces, 0, fv->stream>>>(m, fv->prims.ptr, fv->grad64.ptr, fv->tan_dprims.ptr,
+                                                                                               fv->tan_dgrad.ptr, dt, fv->gas, fv->tan_dflux.ptr);
+        else
+            luna::k_tangent_fluxes<D, 0><<<blocks(F, kBlockFaces), kBlockFaces, 0, fv->stream>>>(m, fv->prims.ptr, fv->grad64.ptr, fv->tan_dprims.ptr,
+                                                                                               fv->tan_dgrad.ptr, dt, fv->gas, fv->tan_dflux.ptr);
+        fv->close_timed(timed_);
+        LUNA_CUDA(cudaGetLastError());
+    }
+    {
+        const long timed_ = fv->open_timed(3);
+        luna::k_tangent_update<D><<<blocks(N, 256), 256, 0, fv->stream>>>(m, dq, fv->tan_dflux.ptr, dt);
+        fv->close_timed(timed_);
+    }
+    LUNA_CUDA(cudaGetLastError());
+    fv->prims_ready = true;  // Q is unchanged
+    fv->swept = false;       // grad64 holds the fit's gradients: the step sweeps again
+    return LUNA_OK;
+}
+
 luna_status copy_out(const double* src, double* dst, size_t count, int on_device, cudaStream_t s) {
     if (!dst) return set_error(LUNA_EINVAL, "output is null");
     LUNA_CUDA(cudaMemcpyAsync(dst, src, count * sizeof(double), on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
@@ -940,6 +993,25 @@ LUNA_API luna_status luna_fv_step_adjoint(luna_fv* fv, double dt, double* qbar, 
     return LUNA_OK;
 }
 
+LUNA_API luna_status luna_fv_step_tangent(luna_fv* fv, double dt, double* dq, int on_device) {
+    if (!fv || !dq) return set_error(LUNA_EINVAL, "null argument");
+    if (fv->motion != LUNA_STATIC_MESH || fv->order != 1 || fv->update != LUNA_UPDATE_PER_FACE || fv->precision != LUNA_FP64)
+        return set_error(LUNA_EINVAL, "hydro::FiniteVolume::step_tangent: a static mesh, order 1, the per-face loop, the FP64 policy");
+    if (fv->moving_pending) return set_error(LUNA_ESTATE, "inside a moving step");
+    if (!(dt >= 0)) return set_error(LUNA_EINVAL, "dt must be >= 0");
+    const size_t count = static_cast<size_t>(fv->n) * (fv->dim + 2);
+    double* dev = dq;
+    if (!on_device) {
+        LUNA_TRY(fv->tan_dq.alloc(count, "tangent dq"));
+        LUNA_CUDA(cudaMemcpyAsync(fv->tan_dq.ptr, dq, count * sizeof(double), cudaMemcpyHostToDevice, fv->stream));
+        dev = fv->tan_dq.ptr;
+    }
+    LUNA_TRY(fv->dim == 3 ? run_tangent<3>(fv, dt, dev) : run_tangent<2>(fv, dt, dev));
+    LUNA_TRY(fv->dim == 3 ? step_static<3>(fv, dt) : step_static<2>(fv, dt));
+    if (!on_device) LUNA_TRY(copy_out(dev, dq, count, 0, fv->stream));
+    return LUNA_OK;
+}
+
 // The learned limiter's buffers (64 B of features, 40 B of admissible factors, 64 B of logits and a compact row's cell a
 // cell, and the row count).
 static luna_status alloc_learned(luna_fv* fv) {
@@ -1031,6 +1103,7 @@ LUNA_API luna_status luna_fv_device_bytes(luna_fv* fv, int64_t* out) {
     b += fv->w.bytes() + fv->x.bytes() + fv->old_cen.bytes() + fv->steps.bytes() + fv->counters.bytes();
     b += fv->adj_fit.bytes() + fv->adj_face_bar.bytes() + fv->adj_wbar.bytes() + fv->adj_bbar.bytes() + fv->adj_boundbar.bytes();
     b += fv->adj_qbar.bytes() + fv->adj_flags.bytes() + fv->adj_bound_face.bytes();
+    b += fv->tan_dprims.bytes() + fv->tan_dgrad.bytes() + fv->tan_dflux.bytes() + fv->tan_dq.bytes();
     b += fv->geo_c01.bytes() + fv->geo_c2.bytes() + fv->geo_off01.bytes() + fv->geo_off2.bytes() + fv->geo_nbr.bytes();
     b += fv->geo_slice_base.bytes() + fv->geo_order.bytes() + fv->geo_stage_start.bytes() + fv->geo_stage_cells.bytes() + fv->geo_faces.bytes();
     b += fv->geo_angle.bytes() + fv->geo_reach2.bytes() + fv->lim_features.bytes() + fv->lim_alpha.bytes() + fv->lim_logits.bytes();

@@ -80,6 +80,7 @@ SIGNATURES = {
     "luna_fv_device_bytes": ([P, P], I),
     "luna_fv_set_timing": ([P, I], I),
     "luna_fv_step_adjoint": ([P, D64, P, I], I),
+    "luna_fv_step_tangent": ([P, D64, P, I], I),
     "luna_apply_static_noalloc": ([P, P, I, I, P, P, P, D64, P, P], I),
     "luna_fv_set_limiter_mlp": ([P, P, I], I),
     "luna_fv_limiter_inputs": ([P, P, P, P], I),
@@ -290,6 +291,16 @@ class FiniteVolume:
             return qbar
         a = np.ascontiguousarray(qbar, dtype=np.float64).copy()
         check(lib().luna_fv_step_adjoint(self._h, dt, a.ctypes.data, 0))
+        return a
+
+    def step_tangent(self, dt: float, dq):
+        """step(dt) with the tangent dq -> J dq beside it (fixed dt); numpy in, numpy out, or a CUDA float64 tensor
+        updated in place."""
+        if hasattr(dq, "is_cuda") and dq.is_cuda:
+            check(lib().luna_fv_step_tangent(self._h, dt, ctypes.c_void_p(dq.data_ptr()), 1))
+            return dq
+        a = np.ascontiguousarray(dq, dtype=np.float64).copy()
+        check(lib().luna_fv_step_tangent(self._h, dt, a.ctypes.data, 0))
         return a
 
     def set_limiter(self, mode: str = "plain", params=None) -> None:

@@ -10,13 +10,14 @@ Commands (paths are raw float64 files, C order; cells in lattice C order, the la
                                       (V + D + 1) rows of (Q extensive, x, volume). Answers "ok <ms> <cfl violations>".
     adjoint <bars in> <U0bar out>     bars: N x (V + D + 1) at the end of the last forward; U0bar = dL/dU0 (intensive).
                                       On the static mesh x and the volumes do not depend on U0: their bars drop out.
+    tangent <U0 in> <dU0 in> <dQ out> the forward with the tangent dU0 (intensive) beside it; dQ: N x V (extensive) at
+                                      the end. Answers "ok <ms>".
     cfl <U0 in>                       "ok <time_step(courant) at U0>".
     geometry <out>                    N x (D + 1) rows of (x, volume). Answers "ok".
     memory                            "ok <peak device bytes> <bytes now>" (the step's buffers and the tape).
     quit
 The fixed dt is checked against time_step(courant) of every step; the steps where it is larger are counted.
-``tangent`` and ``--moving`` answer an error: the step's tangent and the moving mesh's derivatives are not in the
-library.
+``--moving`` answers an error: the moving mesh's derivatives are not in the library.
 """
 from __future__ import annotations
 
@@ -90,6 +91,15 @@ class Server:
             self.fv.step_adjoint(self.dt, qbar)
         return (qbar * self.volume_dev).cpu().numpy()
 
+    def tangent(self, U0: np.ndarray, dU0: np.ndarray) -> np.ndarray:
+        """Rollout::tangent (rollout.cpp:170-196), static: time_step then step_tangent every step."""
+        self.load(U0)
+        dq = self.torch.tensor(np.ascontiguousarray(dU0.reshape(self.n, self.V) * self.V0[:, None]), device="cuda")
+        for _ in range(self.steps):
+            self.fv.time_step(self.courant)
+            self.fv.step_tangent(self.dt, dq)
+        return dq.cpu().numpy()
+
     def cfl(self, U0: np.ndarray) -> float:
         self.load(U0)
         return self.fv.time_step(self.courant)
@@ -149,7 +159,13 @@ def serve(argv, stdin=sys.stdin, stdout=sys.stdout) -> int:
             elif cmd == "memory":
                 answer(f"ok {srv.peak} {srv.now()}")
             elif cmd == "tangent":
-                answer("error tangent: the step's tangent is not in libluna_b200")
+                U0 = np.fromfile(args[0], dtype=np.float64, count=N * V)
+                dU0 = np.fromfile(args[1], dtype=np.float64, count=N * V)
+                t0 = now_ms(torch)
+                out = srv.tangent(U0, dU0)
+                ms = now_ms(torch) - t0
+                out.tofile(args[2])
+                answer(f"ok {ms:.17g}")
             else:
                 answer("error unknown command")
         except Exception as e:  # one answer a line, as the reference's server: the client raises on anything but ok

@@ -54,7 +54,8 @@ class Client:
 @pytest.mark.gpu
 def test_served_adjoint_matches_central_differences(cuda, tmp_path):
     """A 2D shear layer on the 32^2 lattice, 12 steps at a fixed dt: dL/dU0 from `adjoint` against central differences of
-    `forward` along a smooth direction (L = <bars, final rows>); `cfl`, `geometry`, `memory` and `tangent` answer."""
+    `forward` along a smooth direction (L = <bars, final rows>); the served tangent is its transpose (the dot test);
+    `cfl`, `geometry` and `memory` answer."""
     c = Client(tmp_path, 2, 32, 12, 2e-3)
     try:
         xc = (np.arange(32) + 0.5) / 32
@@ -96,6 +97,13 @@ def test_served_adjoint_matches_central_differences(cuda, tmp_path):
         assert abs(float((ubar * d).sum()) - fd) <= 1e-6 * abs(fd)
         out = c.ask("memory")
         assert out[0] == "ok" and int(out[1]) >= int(out[2]) > 0
-        assert c.ask(f"tangent {tmp_path / 'u0.bin'} {tmp_path / 'u0.bin'} {tmp_path / 'x.bin'}")[0] == "error"
+        # the served tangent is the served adjoint's transpose: <dQ(dU0), Qbar> = <dU0, U0bar>
+        U0.tofile(tmp_path / "u0.bin")
+        d.tofile(tmp_path / "du0.bin")
+        out = c.ask(f"tangent {tmp_path / 'u0.bin'} {tmp_path / 'du0.bin'} {tmp_path / 'dq.bin'}")
+        assert out[0] == "ok", out
+        dQ = np.fromfile(tmp_path / "dq.bin").reshape(-1, 4)
+        lhs, rhs = float((dQ * bars[:, :4]).sum()), float((ubar * d).sum())
+        assert abs(lhs - rhs) <= 1e-12 * abs(rhs)
     finally:
         c.close()
