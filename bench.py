@@ -42,7 +42,7 @@ def parse():
     ap.add_argument("--no-learned", action="store_true", help="leave out the learned limiter's section")
     ap.add_argument("--curve", default="row", choices=["row", "morton", "hilbert"],
                     help="the cells' numbering along a space-filling curve (voronoi-cpp's Layout::curve)")
-    ap.add_argument("--precision", default="both", choices=["both", "fp64", "fp32"],
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "fp32", "grad16"],
                     help="which policies to time (the JSON line needs both; one is for profiling runs)")
     return ap.parse_args()
 
@@ -284,7 +284,7 @@ def main():
             dist.barrier()
 
     results = {}
-    for prec in ("fp32", "fp64") if args.precision == "both" else (args.precision,):
+    for prec in ("fp32", "grad16", "fp64") if args.precision == "both" else (args.precision,):
         fv = hydro.FiniteVolume(mesh, precision=prec)
         fv.set_stream(stream)
         fv.set_state(q0)
@@ -367,6 +367,11 @@ def main():
             "fp32": {"value": fp32_value, "ms_per_step": results["fp32"]["ms"] / args.steps,
                      "speedup_vs_fp64": fp32_value / value,
                      "phases_ms_per_step": {k: v[0] / args.steps for k, v in results["fp32"]["phases"].items()}},
+            "grad16": {"policy": "the reference's 3D default (Grad16: binary16 gradient rows, float limiter, double Riemann)",
+                       "value": world * N * args.steps / (results["grad16"]["ms"] / 1e3),
+                       "ms_per_step": results["grad16"]["ms"] / args.steps,
+                       "speedup_vs_fp64": r64["ms"] / results["grad16"]["ms"],
+                       "phases_ms_per_step": {k: v[0] / args.steps for k, v in results["grad16"]["phases"].items()}},
             "phases_ms_per_step": {k: v[0] / args.steps for k, v in phases.items()},
             "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",

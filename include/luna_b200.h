@@ -47,7 +47,9 @@ enum { LUNA_HLLC = 0, LUNA_HLL = 1 };                                   /* Riema
  * per-cell accumulation in double. LUNA_GRAD32 is the reference's Grad32 (precision.hpp:43): float gradients, limiter and
  * face-state change, a double Riemann solve (it keeps perturbations far below float's resolution of the state, which
  * a float Riemann solve cannot). The reduced policies take HLLC only, as the reference's presets. */
-enum { LUNA_FP64 = 0, LUNA_FP32 = 1, LUNA_GRAD32 = 2 };
+enum { LUNA_FP64 = 0, LUNA_FP32 = 1, LUNA_GRAD32 = 2, LUNA_GRAD16 = 3 };
+/* LUNA_GRAD16 is the reference's Grad16 (precision.hpp:47, its 3D default): Grad32 with the gradient rows stored as
+ * binary16 (32 B a row) and one power-of-two exponent per group rho, v, P (4 B a cell). */
 
 /* hydro::Gas (euler.hpp:82-101): gamma and the RAMSES floors. */
 typedef struct {

@@ -239,6 +239,43 @@ struct LearnedInputs {
 };
 constexpr double kAlphaCap = 2.0;  // the largest steepening the learned limiter may choose
 
+// The Grad16 policy's gradient storage (Sweep::store with P::half, finite_volume.hpp:616-641): rows of 16 binary16
+// values (32 B) and a word of three int8 group exponents per cell; null rows: the gradients are stored as G.
+struct HalfRows {
+    uint16_t* rows;
+    uint32_t* exponents;
+};
+
+// Each group (rho, the velocity, P) scaled by 2^k that puts its largest magnitude in [2^14, 2^15) (k = 0 for an all-zero
+// group, within [-114, 126]; precision.hpp half::group_exponent), rounded to binary16 (nearest, ties to even).
+template <int D>
+__device__ __forceinline__ void store_half_row(const HalfRows& out, int i, const float* g) {
+    constexpr int V = D + 2;
+    float largest[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int c = 0; c < V * D; ++c) largest[half_group<D>(c)] = fmaxf(largest[half_group<D>(c)], fabsf(g[c]));
+    int k[3];
+    float scale[3];
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+        const int e = static_cast<int>((__float_as_uint(largest[s]) >> 23) & 0xffu) - 127;
+        k[s] = largest[s] > 0.0f ? min(max(14 - e, -114), 126) : 0;
+        scale[s] = two_to(k[s]);
+    }
+    uint32_t packed[8];
+#pragma unroll
+    for (int w = 0; w < 8; ++w) packed[w] = 0;
+#pragma unroll
+    for (int c = 0; c < V * D; ++c)
+        packed[c >> 1] |= static_cast<uint32_t>(__half_as_ushort(__float2half_rn(g[c] * scale[half_group<D>(c)]))) << (16 * (c & 1));
+    uint4* dst = reinterpret_cast<uint4*>(out.rows + 16 * static_cast<int64_t>(i));
+    dst[0] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+    dst[1] = make_uint4(packed[4], packed[5], packed[6], packed[7]);
+    out.exponents[i] = static_cast<uint32_t>(static_cast<uint8_t>(static_cast<int8_t>(k[0]))) |
+                       static_cast<uint32_t>(static_cast<uint8_t>(static_cast<int8_t>(k[1]))) << 8 |
+                       static_cast<uint32_t>(static_cast<uint8_t>(static_cast<int8_t>(k[2]))) << 16;
+}
+
 // Resident blocks per SM the register budget is cut for, and the entries whose streamed rows are requested together;
 // measured at 128^3 FP64 (sweep ms): 3 blocks / 4 entries 1.74, 4 / 2 1.31 (a few spilled registers), 5 / 1 1.65.
 #ifndef LUNA_SWEEP_MIN_BLOCKS
@@ -260,7 +297,8 @@ constexpr double kAlphaCap = 2.0;  // the largest steepening the learned limiter
 template <int D, bool Moving, bool Grad, class G, int Limit, int KB = LUNA_SWEEP_BATCH, int MINB = LUNA_SWEEP_MIN_BLOCKS>
 __global__ void __launch_bounds__(kTileCells, MINB) k_sweep_tiles(MeshDev<D> m, GeometryDev<D, G> geo, int tile0, const double* __restrict__ prims,
                                                                G* __restrict__ grad_out, double* __restrict__ w_out, double courant,
-                                                               double round_off2, Counters* __restrict__ ctr, LearnedInputs learned) {
+                                                               double round_off2, Counters* __restrict__ ctr, LearnedInputs learned,
+                                                               HalfRows half) {
     extern __shared__ double2 staged_rows[];
     double* rows = reinterpret_cast<double*>(staged_rows);
     constexpr int V = D + 2, GS = grad_stride<D>(), R = kStagedDoubles;
@@ -613,9 +651,17 @@ __global__ void __launch_bounds__(kTileCells, MINB) k_sweep_tiles(MeshDev<D> m, 
                     }
                 }
             }
-            G* out = grad_out + static_cast<int64_t>(GS) * i;
+            bool stored = false;
+            if constexpr (!exact)
+                if (half.rows) {
+                    store_half_row<D>(half, i, g);
+                    stored = true;
+                }
+            if (!stored) {
+                G* out = grad_out + static_cast<int64_t>(GS) * i;
 #pragma unroll
-            for (int c = 0; c < V * D; ++c) out[c] = g[c];
+                for (int c = 0; c < V * D; ++c) out[c] = g[c];
+            }
         }
     }
     warp_min_to(smallest_dt, &ctr->dt_bits);  // no block barrier: a warp done with its lists leaves
@@ -693,7 +739,7 @@ __global__ void k_apply_factors(int rows, const int* __restrict__ cells, const u
 #ifndef LUNA_FLUX_MIN_BLOCKS
 #define LUNA_FLUX_MIN_BLOCKS 6
 #endif
-template <int D, int Order, class G, bool RF, int Riemann>
+template <int D, int Order, class G, bool RF, int Riemann, bool H = false>
 __global__ void __launch_bounds__(128, LUNA_FLUX_MIN_BLOCKS) k_flux_rows(MeshDev<D> m, GeometryDev<D, G> geo, FluxArgs<D, G> x, double* __restrict__ flux,
                                                    unsigned long long* __restrict__ fallbacks) {
     constexpr int V = D + 2;
@@ -735,8 +781,8 @@ __global__ void __launch_bounds__(128, LUNA_FLUX_MIN_BLOCKS) k_flux_rows(MeshDev
                     ro[k] = static_cast<double>(r.offo[k]);
                     rj[k] = static_cast<double>(r.offj[k]);
                 }
-                face_side<D, G>(x, r.o, ro, x.dt, L, count);
-                face_side<D, G>(x, r.j, rj, x.dt, R, count);
+                face_side<D, G, H>(x, r.o, ro, x.dt, L, count);
+                face_side<D, G, H>(x, r.j, rj, x.dt, R, count);
             }
             riemann_solve<D, RF, Riemann>(L, R, n, wf, x.gas, F, false);
 #pragma unroll

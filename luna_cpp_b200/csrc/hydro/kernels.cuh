@@ -11,6 +11,8 @@
 
 #include <cstdint>
 
+#include <cuda_fp16.h>
+
 #include "physics.cuh"
 
 namespace luna {
@@ -281,7 +283,17 @@ struct FluxArgs {
     double dt;                              // the flux's dt (FaceFlux::dt)
     double unit;                            // moving: grid step / dt
     GasDev gas;
+    const uint16_t* __restrict__ grad16 = nullptr;    // Grad16: binary16 rows [N][16] instead of grad (G = float)
+    const uint32_t* __restrict__ exponents = nullptr;  // Grad16: the three int8 group exponents of each row
 };
+
+// The group (0 rho, 1 the velocity, 2 P) of gradient component c = D v + a: each has its own exponent in a Grad16 row.
+template <int D>
+__host__ __device__ constexpr int half_group(int c) {
+    return c < D ? 0 : c < D + D * D ? 1 : 2;
+}
+// 2^k as a float, k in [-126, 127] (exact).
+__device__ __forceinline__ float two_to(int k) { return __uint_as_float(static_cast<uint32_t>(k + 127) << 23); }
 
 // FaceFlux::side at order 1 (finite_volume.hpp:1306-1329): W + g . r - dt/2 A(W) g, or W if rho or P fall to <= 0.
 // A cell's gradient row (GS values of G, 32-B aligned) in vector loads.
@@ -293,7 +305,30 @@ __device__ __forceinline__ void load_grad_row(const G* grad, int i, G* row) {
     for (int c = 0; c < GS; c += per) ldg256(p + c, row + c);
 }
 
-template <int D, class G>
+// FaceFlux::gradient (finite_volume.hpp:1289-1302): a cell's gradient row; H (Grad16): one 32-B load of 16 binary16
+// values, each decoded to float times 2^-k of its group.
+template <int D, class G, bool H = false>
+__device__ __forceinline__ void load_side_grad(const FluxArgs<D, G>& x, int i, G* g) {
+    if constexpr (H && sizeof(G) == sizeof(float)) {
+        constexpr int GS = grad_stride<D>();
+        float raw[8];
+        ldg256(reinterpret_cast<const float*>(x.grad16 + 16 * static_cast<int64_t>(i)), raw);
+        const uint32_t k = __ldg(x.exponents + i);
+        float scale[3];
+#pragma unroll
+        for (int s = 0; s < 3; ++s) scale[s] = two_to(-static_cast<int>(static_cast<int8_t>((k >> (8 * s)) & 0xffu)));
+#pragma unroll
+        for (int c = 0; c < GS; ++c) {
+            const uint32_t pair = __float_as_uint(raw[c >> 1]);
+            const unsigned short h = static_cast<unsigned short>(c & 1 ? pair >> 16 : pair & 0xffffu);
+            g[c] = __half2float(__ushort_as_half(h)) * scale[half_group<D>(c)];
+        }
+    } else {
+        load_grad_row<D, G>(x.grad, i, g);
+    }
+}
+
+template <int D, class G, bool H = false>
 __device__ __forceinline__ void face_side(const FluxArgs<D, G>& x, int i, const double* r, double dt, double* Wf, int& fallbacks) {
     constexpr int V = D + 2, GS = grad_stride<D>();
     double prow[8];
@@ -302,7 +337,7 @@ __device__ __forceinline__ void face_side(const FluxArgs<D, G>& x, int i, const 
 #pragma unroll
     for (int v = 0; v < V; ++v) W[v] = prow[v];
     G g[GS];
-    load_grad_row<D, G>(x.grad, i, g);
+    load_side_grad<D, G, H>(x, i, g);
     if constexpr (sizeof(G) == sizeof(double)) {
         double A[V];
         half_step_rate<D, double>(W, g, x.gas.gamma, A);
@@ -328,7 +363,7 @@ __device__ __forceinline__ void face_side(const FluxArgs<D, G>& x, int i, const 
 }
 
 // MovingFlux<false>::pass_side (finite_volume.hpp:1457-1467): W + g . r on the mesh of t^n, no half step.
-template <int D, class G>
+template <int D, class G, bool H = false>
 __device__ __forceinline__ void pass1_side(const FluxArgs<D, G>& x, int i, const double* r, double* Wf, int& fallbacks) {
     constexpr int V = D + 2, GS = grad_stride<D>();
     double prow[8];
@@ -337,7 +372,7 @@ __device__ __forceinline__ void pass1_side(const FluxArgs<D, G>& x, int i, const
 #pragma unroll
     for (int v = 0; v < V; ++v) W[v] = prow[v];
     G g[GS];
-    load_grad_row<D, G>(x.grad, i, g);
+    load_side_grad<D, G, H>(x, i, g);
     if constexpr (sizeof(G) == sizeof(double)) {
 #pragma unroll
         for (int v = 0; v < V; ++v) Wf[v] = W[v] + dot<D>(g + D * v, r);
@@ -405,7 +440,7 @@ __device__ __forceinline__ void face_velocity(const MeshDev<D>& m, int f, int o,
 
 // The flux through face f times |A| (FaceFlux::operator(), finite_volume.hpp:1415-1434; MovingFlux::operator(),
 // :1469-1490). Pass: -1 static, 0 moving on the mesh of t^n, 1 moving on the mesh of t^n+1.
-template <int D, int Order, int Pass, class G, bool RF, int Riemann>
+template <int D, int Order, int Pass, class G, bool RF, int Riemann, bool H = false>
 __device__ __forceinline__ void face_flux(const MeshDev<D>& m, const FluxArgs<D, G>& x, int f, double* F, int& fb_o, int& fb_j) {
     constexpr int V = D + 2;
     const int o = m.owner[f], j = m.neighbour[f];
@@ -439,8 +474,8 @@ __device__ __forceinline__ void face_flux(const MeshDev<D>& m, const FluxArgs<D,
             double ro[D], rj[D];
             m.face_offset(f, o, ro);
             m.face_offset(f, j, rj);
-            face_side<D, G>(x, o, ro, x.dt, L, fb_o);
-            face_side<D, G>(x, j, rj, x.dt, R, fb_j);
+            face_side<D, G, H>(x, o, ro, x.dt, L, fb_o);
+            face_side<D, G, H>(x, j, rj, x.dt, R, fb_j);
         }
     } else {
         double wo[D], wj[D];
@@ -454,16 +489,16 @@ __device__ __forceinline__ void face_flux(const MeshDev<D>& m, const FluxArgs<D,
         m.face_offset(f, o, ro);
         m.face_offset(f, j, rj);
         if constexpr (Pass == 0) {
-            pass1_side<D, G>(x, o, ro, L, fb_o);
-            pass1_side<D, G>(x, j, rj, R, fb_j);
+            pass1_side<D, G, H>(x, o, ro, L, fb_o);
+            pass1_side<D, G, H>(x, j, rj, R, fb_j);
         } else {
             double r2[D];
 #pragma unroll
             for (int k = 0; k < D; ++k) r2[k] = ro[k] + m.cen[D * o + k] - x.old_cen[D * o + k] + wo[k] * (0.5 * x.dt);
-            face_side<D, G>(x, o, r2, x.dt, L, fb_o);
+            face_side<D, G, H>(x, o, r2, x.dt, L, fb_o);
 #pragma unroll
             for (int k = 0; k < D; ++k) r2[k] = rj[k] + m.cen[D * j + k] - x.old_cen[D * j + k] + wj[k] * (0.5 * x.dt);
-            face_side<D, G>(x, j, r2, x.dt, R, fb_j);
+            face_side<D, G, H>(x, j, r2, x.dt, R, fb_j);
         }
     }
     riemann_solve<D, RF, Riemann>(L, R, n, wf, x.gas, F, Pass >= 0);
@@ -472,7 +507,7 @@ __device__ __forceinline__ void face_flux(const MeshDev<D>& m, const FluxArgs<D,
 }
 
 // apply()'s flux pass (finite_volume.hpp:1591-1602): one flux row per face.
-template <int D, int Order, int Pass, class G, bool RF, int Riemann>
+template <int D, int Order, int Pass, class G, bool RF, int Riemann, bool H = false>
 __global__ void __launch_bounds__(128) k_flux(MeshDev<D> m, FluxArgs<D, G> x, double* __restrict__ flux,
                                               unsigned long long* __restrict__ fallbacks) {
     constexpr int V = D + 2;
@@ -480,7 +515,7 @@ __global__ void __launch_bounds__(128) k_flux(MeshDev<D> m, FluxArgs<D, G> x, do
     int count = 0;
     if (f < m.f) {
         double F[V];
-        face_flux<D, Order, Pass, G, RF, Riemann>(m, x, f, F, count, count);
+        face_flux<D, Order, Pass, G, RF, Riemann, H>(m, x, f, F, count, count);
 #pragma unroll
         for (int v = 0; v < V; ++v) flux[V * static_cast<int64_t>(f) + v] = F[v];
     }
@@ -579,7 +614,7 @@ __global__ void __launch_bounds__(256) k_update(MeshDev<D> m, double* __restrict
 }
 
 // apply()'s per-cell loop (finite_volume.hpp:1543-1562): each cell computes the fluxes of its faces itself, in list order.
-template <int D, int Order, class G, bool RF, int Riemann>
+template <int D, int Order, class G, bool RF, int Riemann, bool H = false>
 __global__ void __launch_bounds__(128) k_fluxes_and_update(MeshDev<D> m, FluxArgs<D, G> x, double* __restrict__ next, double dt,
                                                            Counters* __restrict__ ctr) {
     constexpr int V = D + 2;
@@ -594,7 +629,7 @@ __global__ void __launch_bounds__(128) k_fluxes_and_update(MeshDev<D> m, FluxArg
             const int f = list_face(e);
             int fo = 0, fj = 0;
             double F[V];
-            face_flux<D, Order, -1, G, RF, Riemann>(m, x, f, F, fo, fj);
+            face_flux<D, Order, -1, G, RF, Riemann, H>(m, x, f, F, fo, fj);
             const bool owned = e >= 0;
             count += owned ? fo : fj;
             const double sign = owned ? 1.0 : -1.0;

@@ -101,6 +101,8 @@ struct luna_fv {
     // state and rows
     DevArray<double> q, next, prims, grad64, flux, w, x, old_cen;
     DevArray<float> grad32;
+    DevArray<uint16_t> grad16;     // Grad16: binary16 gradient rows [N][16]
+    DevArray<uint32_t> grad16_exp;  // Grad16: the rows' group exponents [N]
     DevArray<int32_t> steps;
     DevArray<luna::Counters> counters;
     // the mesh reordered for the step (geometry.cuh), rebuilt by every load_mesh
@@ -360,6 +362,7 @@ luna_status launch_sweep_tiles(luna_fv* fv, G* grad, double courant) {
                                       compact ? fv->lim_cells.ptr : nullptr, compact ? fv->lim_count.ptr : nullptr};
     if (Limit == 2 && compact) LUNA_CUDA(cudaMemsetAsync(fv->lim_count.ptr, 0, sizeof(unsigned int), fv->stream));
     auto kernel = luna::k_sweep_tiles<D, Moving, Grad, G, Limit>;
+    const luna::HalfRows half{fv->precision == LUNA_GRAD16 ? fv->grad16.ptr : nullptr, fv->grad16_exp.ptr};
     const int64_t groups[2][2] = {{0, fv->normal_tiles}, {fv->normal_tiles, fv->tiles}};
     const int most_rows[2] = {fv->normal_rows, fv->big_rows};
     // the round-off of the face states, squared: double face states (FP64, grad32), float ones (riemann32)
@@ -370,7 +373,7 @@ luna_status launch_sweep_tiles(luna_fv* fv, G* grad, double courant) {
         const size_t smem = sizeof(double) * luna::kStagedDoubles * static_cast<size_t>(most_rows[k]);
         if (smem > 48 * 1024) LUNA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
         kernel<<<static_cast<unsigned int>(count), luna::kTileCells, smem, fv->stream>>>(m, geo, static_cast<int>(first), fv->prims.ptr, grad, fv->w.ptr,
-                                                                                        courant, round_off2, fv->counters.ptr, learned);
+                                                                                        courant, round_off2, fv->counters.ptr, learned, half);
         LUNA_CUDA(cudaGetLastError());
     }
     return LUNA_OK;
@@ -440,12 +443,12 @@ luna_status prepare_sweep(luna_fv* fv, double courant) {
     return run_sweep<D>(fv, courant);
 }
 
-template <int D, int Order, int Pass, class G, bool RF, int Riemann>
+template <int D, int Order, int Pass, class G, bool RF, int Riemann, bool H = false>
 luna_status launch_flux(luna_fv* fv, const luna::FluxArgs<D, G>& x) {
     if (fv->f == 0) return LUNA_OK;
     {
         const long timed_ = fv->open_timed(2);
-        luna::k_flux<D, Order, Pass, G, RF, Riemann><<<blocks(fv->f, kBlockFaces), kBlockFaces, 0, fv->stream>>>(
+        luna::k_flux<D, Order, Pass, G, RF, Riemann, H><<<blocks(fv->f, kBlockFaces), kBlockFaces, 0, fv->stream>>>(
             fv->mesh_dev<D>(), x, fv->flux.ptr, &fv->counters.ptr->fallbacks[Pass == 1 ? 1 : 0]);
         fv->close_timed(timed_);
     }
@@ -453,12 +456,12 @@ luna_status launch_flux(luna_fv* fv, const luna::FluxArgs<D, G>& x) {
     return LUNA_OK;
 }
 
-template <int D, int Order, class G, bool RF, int Riemann>
+template <int D, int Order, class G, bool RF, int Riemann, bool H = false>
 luna_status launch_flux_rows(luna_fv* fv, const luna::FluxArgs<D, G>& x) {
     if (fv->f == 0) return LUNA_OK;
     {
         const long timed_ = fv->open_timed(2);
-        luna::k_flux_rows<D, Order, G, RF, Riemann><<<blocks(fv->f, kBlockFaces), kBlockFaces, 0, fv->stream>>>(
+        luna::k_flux_rows<D, Order, G, RF, Riemann, H><<<blocks(fv->f, kBlockFaces), kBlockFaces, 0, fv->stream>>>(
             fv->mesh_dev<D>(), fv->geometry_dev<D, G>(), x, fv->flux.ptr, &fv->counters.ptr->fallbacks[0]);
         fv->close_timed(timed_);
     }
@@ -468,6 +471,7 @@ luna_status launch_flux_rows(luna_fv* fv, const luna::FluxArgs<D, G>& x) {
 
 template <int D, int Order, class G>
 luna_status dispatch_flux_rows(luna_fv* fv, const luna::FluxArgs<D, G>& x) {
+    if (fv->precision == LUNA_GRAD16) return launch_flux_rows<D, Order, G, false, 0, true>(fv, x);
     if (fv->precision == LUNA_FP32) return launch_flux_rows<D, Order, G, true, 0>(fv, x);
     if (fv->riemann == LUNA_HLL) return launch_flux_rows<D, Order, G, false, 1>(fv, x);
     return launch_flux_rows<D, Order, G, false, 0>(fv, x);
@@ -475,17 +479,18 @@ luna_status dispatch_flux_rows(luna_fv* fv, const luna::FluxArgs<D, G>& x) {
 
 template <int D, int Order, int Pass, class G>
 luna_status dispatch_flux(luna_fv* fv, const luna::FluxArgs<D, G>& x) {
+    if (fv->precision == LUNA_GRAD16) return launch_flux<D, Order, Pass, G, false, 0, true>(fv, x);
     if (fv->precision == LUNA_FP32) return launch_flux<D, Order, Pass, G, true, 0>(fv, x);
     if (fv->riemann == LUNA_HLL) return launch_flux<D, Order, Pass, G, false, 1>(fv, x);
     return launch_flux<D, Order, Pass, G, false, 0>(fv, x);
 }
 
-template <int D, int Order, class G, bool RF, int Riemann>
+template <int D, int Order, class G, bool RF, int Riemann, bool H = false>
 luna_status launch_per_cell(luna_fv* fv, const luna::FluxArgs<D, G>& x, double dt) {
     double* out = Order == 0 ? fv->next.ptr : fv->q.ptr;
     {
         const long timed_ = fv->open_timed(2);
-        luna::k_fluxes_and_update<D, Order, G, RF, Riemann><<<blocks(fv->n, kBlockCells), kBlockCells, 0, fv->stream>>>(fv->mesh_dev<D>(), x, out, dt,
+        luna::k_fluxes_and_update<D, Order, G, RF, Riemann, H><<<blocks(fv->n, kBlockCells), kBlockCells, 0, fv->stream>>>(fv->mesh_dev<D>(), x, out, dt,
                                                                                                                      fv->counters.ptr);
         fv->close_timed(timed_);
     }
@@ -505,6 +510,10 @@ luna::FluxArgs<D, G> flux_args(luna_fv* fv, const G* grad, double dt) {
     x.dt = dt;
     x.unit = 0;
     x.gas = fv->gas;
+    if (fv->precision == LUNA_GRAD16) {
+        x.grad16 = fv->grad16.ptr;
+        x.exponents = fv->grad16_exp.ptr;
+    }
     return x;
 }
 
@@ -515,9 +524,11 @@ luna_status run_apply(luna_fv* fv, const G* grad, double dt) {
     if (fv->update == LUNA_UPDATE_PER_CELL) {
         if (fv->order == 0) {
             if (fv->precision == LUNA_FP32) return launch_per_cell<D, 0, G, true, 0>(fv, x, dt);
+            if (fv->precision == LUNA_GRAD16) return launch_per_cell<D, 0, G, false, 0, true>(fv, x, dt);
             return fv->riemann == LUNA_HLL ? launch_per_cell<D, 0, G, false, 1>(fv, x, dt) : launch_per_cell<D, 0, G, false, 0>(fv, x, dt);
         }
         if (fv->precision == LUNA_FP32) return launch_per_cell<D, 1, G, true, 0>(fv, x, dt);
+        if (fv->precision == LUNA_GRAD16) return launch_per_cell<D, 1, G, false, 0, true>(fv, x, dt);
         return fv->riemann == LUNA_HLL ? launch_per_cell<D, 1, G, false, 1>(fv, x, dt) : launch_per_cell<D, 1, G, false, 0>(fv, x, dt);
     }
     if (fv->order == 0)
@@ -563,6 +574,8 @@ luna_status moving_begin(luna_fv* fv, double dt) {
         x.unit = fv->grid_step / dt;
         if (fv->precision == LUNA_FP32)
             LUNA_TRY((launch_flux<D, 1, 0, float, true, 0>(fv, x)));
+        else if (fv->precision == LUNA_GRAD16)
+            LUNA_TRY((launch_flux<D, 1, 0, float, false, 0, true>(fv, x)));
         else
             LUNA_TRY((launch_flux<D, 1, 0, float, false, 0>(fv, x)));
     } else {
@@ -599,6 +612,8 @@ luna_status moving_end(luna_fv* fv) {
         x.unit = fv->grid_step / dt;
         if (fv->precision == LUNA_FP32)
             LUNA_TRY((launch_flux<D, 1, 1, float, true, 0>(fv, x)));
+        else if (fv->precision == LUNA_GRAD16)
+            LUNA_TRY((launch_flux<D, 1, 1, float, false, 0, true>(fv, x)));
         else
             LUNA_TRY((launch_flux<D, 1, 1, float, false, 0>(fv, x)));
     } else {
@@ -724,6 +739,15 @@ luna_status run_tangent(luna_fv* fv, double dt, double* dq) {
     return LUNA_OK;
 }
 
+// IEEE binary16 -> float on the host (exact), for the Grad16 rows copied out.
+float half_to_float(uint16_t h) {
+    const int field = (h >> 10) & 0x1f, mant = h & 0x3ff;
+    const float sign = (h & 0x8000) ? -1.0f : 1.0f;
+    if (field == 0x1f) return mant ? std::nanf("") : sign * INFINITY;
+    if (field == 0) return sign * std::ldexp(static_cast<float>(mant), -24);
+    return sign * std::ldexp(static_cast<float>(mant | 0x400), field - 25);
+}
+
 luna_status copy_out(const double* src, double* dst, size_t count, int on_device, cudaStream_t s) {
     if (!dst) return set_error(LUNA_EINVAL, "output is null");
     LUNA_CUDA(cudaMemcpyAsync(dst, src, count * sizeof(double), on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
@@ -760,7 +784,8 @@ LUNA_API luna_status luna_fv_create(const luna_mesh_desc* mesh, const luna_gas* 
     if (limiter != LUNA_LIMITER_FACE_CENTROID && limiter != LUNA_LIMITER_NONE) return set_error(LUNA_EINVAL, "limiter: face_centroid or none");
     if (motion != LUNA_STATIC_MESH && motion != LUNA_MOVING) return set_error(LUNA_EINVAL, "motion: static_mesh or moving");
     if (riemann != LUNA_HLLC && riemann != LUNA_HLL) return set_error(LUNA_EINVAL, "riemann: HLLC or HLL");
-    if (precision != LUNA_FP64 && precision != LUNA_FP32 && precision != LUNA_GRAD32) return set_error(LUNA_EINVAL, "precision: FP64, FP32 or GRAD32");
+    if (precision != LUNA_FP64 && precision != LUNA_FP32 && precision != LUNA_GRAD32 && precision != LUNA_GRAD16)
+        return set_error(LUNA_EINVAL, "precision: FP64, FP32, GRAD32 or GRAD16");
     if (precision != LUNA_FP64 && riemann == LUNA_HLL)
         return set_error(LUNA_EINVAL, "the FP32 policy takes HLLC (the reference's reduced presets are HLLC only)");
     if (motion == LUNA_MOVING && (order != 1 || update != LUNA_UPDATE_PER_FACE))
@@ -801,7 +826,11 @@ LUNA_API luna_status luna_fv_create(const luna_mesh_desc* mesh, const luna_gas* 
     if ((s = fv->prims.alloc(N * luna::PS, "primitive rows")) != LUNA_OK) return fail(s);
     const size_t GS = D == 3 ? luna::grad_stride<3>() : luna::grad_stride<2>();
     if (order == 1) {
-        if (precision != LUNA_FP64) {
+        if (precision == LUNA_GRAD16) {
+            if ((s = fv->grad16.alloc(N * 16, "binary16 gradient rows")) != LUNA_OK) return fail(s);
+            if ((s = fv->grad16_exp.alloc(N, "gradient exponents")) != LUNA_OK) return fail(s);
+            if ((s = fv->grad32.alloc(1, "gradient rows (unused)")) != LUNA_OK) return fail(s);
+        } else if (precision != LUNA_FP64) {
             if ((s = fv->grad32.alloc(N * GS, "gradient rows")) != LUNA_OK) return fail(s);
         } else if ((s = fv->grad64.alloc(N * GS, "gradient rows")) != LUNA_OK) {
             return fail(s);
@@ -964,6 +993,20 @@ LUNA_API luna_status luna_fv_gradients(luna_fv* fv, double* out, int on_device) 
         return LUNA_OK;
     }
     if (on_device) return set_error(LUNA_EINVAL, "FP32 gradients are copied to host memory only");
+    if (fv->precision == LUNA_GRAD16) {  // decoded as the flux reads them: binary16 times 2^-k of the group
+        std::vector<uint16_t> rows(N * 16);
+        std::vector<uint32_t> k(N);
+        LUNA_CUDA(cudaMemcpyAsync(rows.data(), fv->grad16.ptr, N * 16 * sizeof(uint16_t), cudaMemcpyDeviceToHost, fv->stream));
+        LUNA_CUDA(cudaMemcpyAsync(k.data(), fv->grad16_exp.ptr, N * sizeof(uint32_t), cudaMemcpyDeviceToHost, fv->stream));
+        LUNA_CUDA(cudaStreamSynchronize(fv->stream));
+        for (size_t i = 0; i < N; ++i)
+            for (int c = 0; c < width; ++c) {
+                const int group = c < D ? 0 : c < D + D * D ? 1 : 2;
+                const int e = static_cast<int8_t>((k[i] >> (8 * group)) & 0xffu);
+                out[i * width + c] = std::ldexp(static_cast<double>(half_to_float(rows[i * 16 + c])), -e);
+            }
+        return LUNA_OK;
+    }
     float* tmp = nullptr;
     LUNA_CUDA(cudaMallocHost(&tmp, N * GS * sizeof(float)));
     cudaError_t e = cudaMemcpyAsync(tmp, fv->grad32.ptr, N * GS * sizeof(float), cudaMemcpyDeviceToHost, fv->stream);
@@ -1100,6 +1143,7 @@ LUNA_API luna_status luna_fv_device_bytes(luna_fv* fv, int64_t* out) {
     b += fv->owner.bytes() + fv->neighbour.bytes() + fv->start.bytes() + fv->list.bytes();
     b += fv->area.bytes() + fv->mag.bytes() + fv->fcen.bytes() + fv->cen.bytes() + fv->vol.bytes() + fv->pos.bytes();
     b += fv->q.bytes() + fv->next.bytes() + fv->prims.bytes() + fv->grad64.bytes() + fv->grad32.bytes() + fv->flux.bytes();
+    b += fv->grad16.bytes() + fv->grad16_exp.bytes();
     b += fv->w.bytes() + fv->x.bytes() + fv->old_cen.bytes() + fv->steps.bytes() + fv->counters.bytes();
     b += fv->adj_fit.bytes() + fv->adj_face_bar.bytes() + fv->adj_wbar.bytes() + fv->adj_bbar.bytes() + fv->adj_boundbar.bytes();
     b += fv->adj_qbar.bytes() + fv->adj_flags.bytes() + fv->adj_bound_face.bytes();

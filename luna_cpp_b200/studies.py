@@ -3,8 +3,9 @@ comparisons of the same configurations are GPU tests).
 
 - ``precision``: 3D static Voronoi mesh from nx^3 jittered generators; (a) the point blast, (b) the plane acoustic wave
   (amplitude 1e-6, background rho 1, p 3/5); 100 steps of the FP64 step and of the reduced policies (FP32 face
-  arithmetic; FP32 gradients) on the FP64 run's dt schedule: relative L1 and Linf of every conserved field against the
-  FP64 run, the wave's error relative to its perturbation, conservation, and device time per step.
+  arithmetic; FP32 gradients; FP16 gradient rows) on the FP64 run's dt schedule: relative L1 and Linf of every
+  conserved field against the FP64 run, the wave's error relative to its perturbation, conservation, and device time
+  per step.
 - ``moving``: the moving-mesh point blast (generators on the 2^-30 snapping grid, moved with the gas plus the
   roundness velocity, fluxes on the old and the new faces) on nx^3 jittered generators to t_end, FP32 face
   arithmetic with FP64 state by default (``riemann32``): steps taken, the hydro part's device time and cell-updates/s
@@ -79,7 +80,7 @@ def precision(nx=128, steps=100, courant=0.3, seed=1, threads=0, log=print) -> d
                           "energy_drift": float(abs(q64[:, 4].sum() - q0[:, 4].sum()) / q0[:, 4].sum()),
                           "t_end": float(sum(dts))}
         ref.close()
-        for policy in ("fp32", "grad32"):
+        for policy in ("fp32", "grad32", "grad16"):
             fv = hydro.FiniteVolume(mesh, precision=policy)
             fv.set_state(q0)
             fv.set_timing(True)

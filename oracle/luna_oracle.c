@@ -273,7 +273,7 @@ void lo_hllc_flux_float(int D, const float* L, const float* R, const float* n, c
 struct lo_fv {
     lo_mesh mesh;
     lo_gas gas;
-    int D, V, U, order, per_face, limiter_none, riemann, moving, grad_float, riemann_float;
+    int D, V, U, order, per_face, limiter_none, riemann, moving, grad_float, riemann_float, grad_half;
     int64_t n, f;
     double box_inverse[3], step, per_step;
     int64_t period[3];
@@ -580,6 +580,75 @@ static void sweep_cell_d(lo_fv* fv, int64_t i, int grad_on) {
 }
 
 /* The same sweep with the float gradient policy (Grad32: G = float; finite_volume.hpp:463-569 with exact = false). */
+/* IEEE binary16 <-> binary32 with round to nearest, ties to even (the conversions of the Grad16 policy's rows). */
+static uint16_t half_of(float f) {
+    uint32_t x;
+    memcpy(&x, &f, 4);
+    const uint32_t sign = (x >> 16) & 0x8000u, field = (x >> 23) & 0xffu, mant = x & 0x7fffffu;
+    if (field == 0xffu) return (uint16_t)(sign | 0x7c00u | (mant ? 0x200u : 0u));
+    const int e = (int)field - 127 + 15;
+    if (e >= 31) return (uint16_t)(sign | 0x7c00u);
+    if (e <= 0) {                                  /* a subnormal half (or zero): units of 2^-24 */
+        const int shift = 14 - e;
+        if (shift > 24) return (uint16_t)sign;     /* below half of the smallest subnormal */
+        const uint32_t full = mant | 0x800000u;
+        uint32_t h = full >> shift;
+        const uint32_t rest = full & ((1u << shift) - 1u), halfway = 1u << (shift - 1);
+        if (rest > halfway || (rest == halfway && (h & 1u))) ++h;
+        return (uint16_t)(sign | h);
+    }
+    uint32_t h = ((uint32_t)e << 10) | (mant >> 13);
+    const uint32_t rest = mant & 0x1fffu;
+    if (rest > 0x1000u || (rest == 0x1000u && (h & 1u))) ++h;  /* a carry moves into the exponent, to infinity at most */
+    return (uint16_t)(sign | h);
+}
+static float float_of_half(uint16_t h) {
+    const uint32_t sign = (uint32_t)(h & 0x8000u) << 16, field = (h >> 10) & 0x1fu, mant = h & 0x3ffu;
+    uint32_t x;
+    if (field == 0x1fu) {
+        x = sign | 0x7f800000u | (mant << 13);
+    } else if (field == 0) {
+        const float m = ldexpf((float)mant, -24);  /* exact */
+        return sign ? -m : m;
+    } else {
+        x = sign | ((field - 15u + 127u) << 23) | (mant << 13);
+    }
+    float f;
+    memcpy(&f, &x, 4);
+    return f;
+}
+static float two_to(int k) { /* 2^k, k in [-126, 127] */
+    const uint32_t x = (uint32_t)(k + 127) << 23;
+    float f;
+    memcpy(&f, &x, 4);
+    return f;
+}
+/* Sweep::store and FaceFlux::gradient with P::half (finite_volume.hpp:616-641, :1289-1302; precision.hpp's half::): each
+ * group (rho, the velocity, P) scaled by 2^k that puts its largest magnitude in [2^14, 2^15) (k = 0 for an all-zero
+ * group, k within [-114, 126]), rounded to binary16, and read back times 2^-k. */
+static void half_round_trip(int D, int V, float* g) {
+    float largest[3] = {0, 0, 0};
+    for (int c = 0; c < V * D; ++c) {
+        const int group = c < D ? 0 : c < D + D * D ? 1 : 2;
+        largest[group] = fmaxf(largest[group], fabsf(g[c]));
+    }
+    int k[3];
+    for (int s = 0; s < 3; ++s) {
+        if (!(largest[s] > 0)) {
+            k[s] = 0;
+            continue;
+        }
+        uint32_t bits;
+        memcpy(&bits, &largest[s], 4);
+        const int e = (int)((bits >> 23) & 0xffu) - 127;
+        k[s] = 14 - e < -114 ? -114 : 14 - e > 126 ? 126 : 14 - e;
+    }
+    for (int c = 0; c < V * D; ++c) {
+        const int group = c < D ? 0 : c < D + D * D ? 1 : 2;
+        g[c] = float_of_half(half_of(g[c] * two_to(k[group]))) * two_to(-k[group]);
+    }
+}
+
 static void sweep_cell_f(lo_fv* fv, int64_t i, int grad_on) {
     const int D = fv->D, V = fv->V, U = fv->U;
     const double* Wi = fv->prims + (V + 2) * i;
@@ -679,8 +748,11 @@ static void sweep_cell_f(lo_fv* fv, int64_t i, int grad_on) {
                 }
             }
         }
+    if (fv->grad_half) half_round_trip(D, V, grad);
     for (int c = 0; c < V * D; ++c) fv->grad[V * D * i + c] = (double)grad[c];
 }
+
+void lo_fv_set_half_gradients(lo_fv* fv, int on) { fv->grad_half = on != 0; }
 
 /* sweep() (finite_volume.hpp:1107-1149): Sweep, then the time-step reduction (TimeStep = FaceStep + CellStep,
  * finite_volume.hpp:1040-1104). */
