@@ -298,7 +298,7 @@ template <int D, bool Moving, bool Grad, class G, int Limit, int KB = LUNA_SWEEP
 __global__ void __launch_bounds__(kTileCells, MINB) k_sweep_tiles(MeshDev<D> m, GeometryDev<D, G> geo, int tile0, const double* __restrict__ prims,
                                                                G* __restrict__ grad_out, double* __restrict__ w_out, double courant,
                                                                double round_off2, Counters* __restrict__ ctr, LearnedInputs learned,
-                                                               HalfRows half) {
+                                                               HalfRows half, double* __restrict__ wg_out) {
     extern __shared__ double2 staged_rows[];
     double* rows = reinterpret_cast<double*>(staged_rows);
     constexpr int V = D + 2, GS = grad_stride<D>(), R = kStagedDoubles;
@@ -657,6 +657,21 @@ __global__ void __launch_bounds__(kTileCells, MINB) k_sweep_tiles(MeshDev<D> m, 
                     store_half_row<D>(half, i, g);
                     stored = true;
                 }
+            if constexpr (exact)
+                if (wg_out) {  // the merged row of the static per-face step: W (as staged) then g
+                    constexpr int S = wg_stride<D>();
+                    double row[S];
+#pragma unroll
+                    for (int v = 0; v < V; ++v) row[v] = Wi[v];
+#pragma unroll
+                    for (int c = 0; c < V * D; ++c) row[V + c] = g[c];
+#pragma unroll
+                    for (int c = V + V * D; c < S; ++c) row[c] = 0.0;
+                    double2* dst = reinterpret_cast<double2*>(wg_out + static_cast<int64_t>(S) * i);
+#pragma unroll
+                    for (int c = 0; c < S; c += 2) dst[c / 2] = make_double2(row[c], row[c + 1]);
+                    stored = true;
+                }
             if (!stored) {
                 G* out = grad_out + static_cast<int64_t>(GS) * i;
 #pragma unroll
@@ -739,7 +754,7 @@ __global__ void k_apply_factors(int rows, const int* __restrict__ cells, const u
 #ifndef LUNA_FLUX_MIN_BLOCKS
 #define LUNA_FLUX_MIN_BLOCKS 6
 #endif
-template <int D, int Order, class G, bool RF, int Riemann, bool H = false>
+template <int D, int Order, class G, bool RF, int Riemann, bool H = false, bool WG = false>
 __global__ void __launch_bounds__(128, LUNA_FLUX_MIN_BLOCKS) k_flux_rows(MeshDev<D> m, GeometryDev<D, G> geo, FluxArgs<D, G> x, double* __restrict__ flux,
                                                    unsigned long long* __restrict__ fallbacks) {
     constexpr int V = D + 2;
@@ -781,8 +796,8 @@ __global__ void __launch_bounds__(128, LUNA_FLUX_MIN_BLOCKS) k_flux_rows(MeshDev
                     ro[k] = static_cast<double>(r.offo[k]);
                     rj[k] = static_cast<double>(r.offj[k]);
                 }
-                face_side<D, G, H>(x, r.o, ro, x.dt, L, count);
-                face_side<D, G, H>(x, r.j, rj, x.dt, R, count);
+                face_side<D, G, H, WG>(x, r.o, ro, x.dt, L, count);
+                face_side<D, G, H, WG>(x, r.j, rj, x.dt, R, count);
             }
             riemann_solve<D, RF, Riemann>(L, R, n, wf, x.gas, F, false);
 #pragma unroll

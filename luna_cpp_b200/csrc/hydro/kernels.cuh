@@ -148,6 +148,13 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // A cell's primitive row (W, c, r, pad: 64 B, 64-B aligned) in two vector loads (3D), one (2D: W only).
+// A merged row of the FP64 static per-face step: the cell's W (V doubles) then its gradient (V D), padded to whole
+// 32-B sectors: 20 doubles (160 B, 5 sectors) in 3D against the 2 + 4 sectors of a primitive row and a gradient row.
+template <int D>
+constexpr int wg_stride() {
+    return ((D + 2) * (D + 1) + 3) / 4 * 4;
+}
+
 template <int D>
 __device__ __forceinline__ void load_prim_row(const double* prims, int i, double* row) {
     const double* p = prims + 8 * static_cast<int64_t>(i);
@@ -283,6 +290,7 @@ struct FluxArgs {
     double dt;                              // the flux's dt (FaceFlux::dt)
     double unit;                            // moving: grid step / dt
     GasDev gas;
+    const double* __restrict__ wg = nullptr;           // FP64 static per-face step: merged rows [N][wg_stride] (W, g)
     const uint16_t* __restrict__ grad16 = nullptr;    // Grad16: binary16 rows [N][16] instead of grad (G = float)
     const uint32_t* __restrict__ exponents = nullptr;  // Grad16: the three int8 group exponents of each row
 };
@@ -328,16 +336,28 @@ __device__ __forceinline__ void load_side_grad(const FluxArgs<D, G>& x, int i, G
     }
 }
 
-template <int D, class G, bool H = false>
+template <int D, class G, bool H = false, bool WG = false>
 __device__ __forceinline__ void face_side(const FluxArgs<D, G>& x, int i, const double* r, double dt, double* Wf, int& fallbacks) {
     constexpr int V = D + 2, GS = grad_stride<D>();
-    double prow[8];
-    load_prim_row<D>(x.prims, i, prow);
     double W[V];
-#pragma unroll
-    for (int v = 0; v < V; ++v) W[v] = prow[v];
     G g[GS];
-    load_side_grad<D, G, H>(x, i, g);
+    if constexpr (WG && sizeof(G) == sizeof(double)) {  // one merged row: W then g
+        constexpr int S = wg_stride<D>();
+        double row[S];
+        const double* p = x.wg + static_cast<int64_t>(S) * i;
+#pragma unroll
+        for (int c = 0; c < S; c += 4) ldg256(p + c, row + c);
+#pragma unroll
+        for (int v = 0; v < V; ++v) W[v] = row[v];
+#pragma unroll
+        for (int c = 0; c < V * D; ++c) g[c] = row[V + c];
+    } else {
+        double prow[8];
+        load_prim_row<D>(x.prims, i, prow);
+#pragma unroll
+        for (int v = 0; v < V; ++v) W[v] = prow[v];
+        load_side_grad<D, G, H>(x, i, g);
+    }
     if constexpr (sizeof(G) == sizeof(double)) {
         double A[V];
         half_step_rate<D, double>(W, g, x.gas.gamma, A);
@@ -552,8 +572,17 @@ __device__ __forceinline__ void load_row_windowed(const double* p, double* row) 
 // apply()'s update (finite_volume.hpp:1603-1615): Q_i -= dt sum_k sign_k F_k in list order; NextPrims: the next
 // primitive rows (a moving step's second pass; here every per-face step, which makes the next primitives() pass free).
 // Windowed: flux rows through load_row_windowed (the library's own flux buffer, padded for it).
+// The library's update (windowed rows): resident blocks of 256 its registers are cut for, and the entries whose rows are
+// requested together; measured at 128^3 (update ms, every policy alike): 1 / 4 0.395, 4 / 2 0.391, 4 / 3 0.410,
+// 4 / 4 0.444 (spills), 3 / 6 0.477. The no-allocation path's instantiation keeps 1 / 4.
+#ifndef LUNA_UPDATE_MIN_BLOCKS
+#define LUNA_UPDATE_MIN_BLOCKS 4
+#endif
+#ifndef LUNA_UPDATE_BATCH
+#define LUNA_UPDATE_BATCH 2
+#endif
 template <int D, bool NextPrims, bool Windowed = false>
-__global__ void __launch_bounds__(256) k_update(MeshDev<D> m, double* __restrict__ q, const double* __restrict__ flux, double dt,
+__global__ void __launch_bounds__(256, Windowed ? LUNA_UPDATE_MIN_BLOCKS : 1) k_update(MeshDev<D> m, double* __restrict__ q, const double* __restrict__ flux, double dt,
                                                 double* __restrict__ prims, GasDev gas, Counters* __restrict__ ctr) {
     constexpr int V = D + 2;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -564,7 +593,7 @@ __global__ void __launch_bounds__(256) k_update(MeshDev<D> m, double* __restrict
     const int first = m.start[i], end = m.start[i + 1];
     // kBatch entries at a time: their list words, then their flux rows, are all requested before any is used (the
     // gathers of a list are independent); the sums stay in list order.
-    constexpr int kBatch = 4;
+    constexpr int kBatch = Windowed ? LUNA_UPDATE_BATCH : 4;
     for (int k0 = first; k0 < end; k0 += kBatch) {
         int32_t e[kBatch];
 #pragma unroll

@@ -101,6 +101,8 @@ struct luna_fv {
     // state and rows
     DevArray<double> q, next, prims, grad64, flux, w, x, old_cen;
     DevArray<float> grad32;
+    DevArray<double> wg64;          // FP64 static per-face step: merged rows (W, g) [N][wg_stride] the flux reads
+    bool grads_in_wg = false;       // the last sweep wrote wg64 (not grad64)
     DevArray<uint16_t> grad16;     // Grad16: binary16 gradient rows [N][16]
     DevArray<uint32_t> grad16_exp;  // Grad16: the rows' group exponents [N]
     DevArray<int32_t> steps;
@@ -363,6 +365,9 @@ luna_status launch_sweep_tiles(luna_fv* fv, G* grad, double courant) {
     if (Limit == 2 && compact) LUNA_CUDA(cudaMemsetAsync(fv->lim_count.ptr, 0, sizeof(unsigned int), fv->stream));
     auto kernel = luna::k_sweep_tiles<D, Moving, Grad, G, Limit>;
     const luna::HalfRows half{fv->precision == LUNA_GRAD16 ? fv->grad16.ptr : nullptr, fv->grad16_exp.ptr};
+    // merged rows for the static per-face FP64 step (the learned limiter's mode scales plain gradient rows)
+    double* const wg_out = (Grad && Limit != 2 && sizeof(G) == sizeof(double)) ? fv->wg64.ptr : nullptr;
+    fv->grads_in_wg = wg_out != nullptr;
     const int64_t groups[2][2] = {{0, fv->normal_tiles}, {fv->normal_tiles, fv->tiles}};
     const int most_rows[2] = {fv->normal_rows, fv->big_rows};
     // the round-off of the face states, squared: double face states (FP64, grad32), float ones (riemann32)
@@ -373,7 +378,7 @@ luna_status launch_sweep_tiles(luna_fv* fv, G* grad, double courant) {
         const size_t smem = sizeof(double) * luna::kStagedDoubles * static_cast<size_t>(most_rows[k]);
         if (smem > 48 * 1024) LUNA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
         kernel<<<static_cast<unsigned int>(count), luna::kTileCells, smem, fv->stream>>>(m, geo, static_cast<int>(first), fv->prims.ptr, grad, fv->w.ptr,
-                                                                                        courant, round_off2, fv->counters.ptr, learned, half);
+                                                                                        courant, round_off2, fv->counters.ptr, learned, half, wg_out);
         LUNA_CUDA(cudaGetLastError());
     }
     return LUNA_OK;
@@ -456,12 +461,12 @@ luna_status launch_flux(luna_fv* fv, const luna::FluxArgs<D, G>& x) {
     return LUNA_OK;
 }
 
-template <int D, int Order, class G, bool RF, int Riemann, bool H = false>
+template <int D, int Order, class G, bool RF, int Riemann, bool H = false, bool WG = false>
 luna_status launch_flux_rows(luna_fv* fv, const luna::FluxArgs<D, G>& x) {
     if (fv->f == 0) return LUNA_OK;
     {
         const long timed_ = fv->open_timed(2);
-        luna::k_flux_rows<D, Order, G, RF, Riemann, H><<<blocks(fv->f, kBlockFaces), kBlockFaces, 0, fv->stream>>>(
+        luna::k_flux_rows<D, Order, G, RF, Riemann, H, WG><<<blocks(fv->f, kBlockFaces), kBlockFaces, 0, fv->stream>>>(
             fv->mesh_dev<D>(), fv->geometry_dev<D, G>(), x, fv->flux.ptr, &fv->counters.ptr->fallbacks[0]);
         fv->close_timed(timed_);
     }
@@ -471,6 +476,13 @@ luna_status launch_flux_rows(luna_fv* fv, const luna::FluxArgs<D, G>& x) {
 
 template <int D, int Order, class G>
 luna_status dispatch_flux_rows(luna_fv* fv, const luna::FluxArgs<D, G>& x) {
+    if constexpr (sizeof(G) == sizeof(double) && Order == 1)
+        if (fv->grads_in_wg) {
+            auto y = x;
+            y.wg = fv->wg64.ptr;
+            return fv->riemann == LUNA_HLL ? launch_flux_rows<D, Order, G, false, 1, false, true>(fv, y)
+                                           : launch_flux_rows<D, Order, G, false, 0, false, true>(fv, y);
+        }
     if (fv->precision == LUNA_GRAD16) return launch_flux_rows<D, Order, G, false, 0, true>(fv, x);
     if (fv->precision == LUNA_FP32) return launch_flux_rows<D, Order, G, true, 0>(fv, x);
     if (fv->riemann == LUNA_HLL) return launch_flux_rows<D, Order, G, false, 1>(fv, x);
@@ -640,6 +652,7 @@ luna_status moving_end(luna_fv* fv) {
 // faces' Riemann adjoints, the cells' adjoints and the gather into Qbar.
 template <int D>
 luna_status run_adjoint(luna_fv* fv, double dt, double* qbar) {
+    fv->grads_in_wg = false;  // k_sweep_fit writes grad64
     constexpr int V = D + 2, U = D + 1;
     using FL = luna::FitLayout<D>;
     const size_t N = static_cast<size_t>(fv->n), F = static_cast<size_t>(fv->f);
@@ -693,6 +706,7 @@ luna_status run_adjoint(luna_fv* fv, double dt, double* qbar) {
 // (the reference's fit and clip pattern, k_sweep_fit), then the production step advances Q.
 template <int D>
 luna_status run_tangent(luna_fv* fv, double dt, double* dq) {
+    fv->grads_in_wg = false;  // k_sweep_fit writes grad64
     constexpr int V = D + 2;
     using FL = luna::FitLayout<D>;
     const size_t N = static_cast<size_t>(fv->n), F = static_cast<size_t>(fv->f);
@@ -834,6 +848,10 @@ LUNA_API luna_status luna_fv_create(const luna_mesh_desc* mesh, const luna_gas* 
             if ((s = fv->grad32.alloc(N * GS, "gradient rows")) != LUNA_OK) return fail(s);
         } else if ((s = fv->grad64.alloc(N * GS, "gradient rows")) != LUNA_OK) {
             return fail(s);
+        }
+        if (precision == LUNA_FP64 && motion == LUNA_STATIC_MESH && update == LUNA_UPDATE_PER_FACE) {
+            const size_t S = D == 3 ? luna::wg_stride<3>() : luna::wg_stride<2>();
+            if ((s = fv->wg64.alloc(N * S, "merged W and gradient rows")) != LUNA_OK) return fail(s);
         }
     }
     if ((s = fv->w.alloc(N * D, "point velocities")) != LUNA_OK) return fail(s);
@@ -987,7 +1005,13 @@ LUNA_API luna_status luna_fv_gradients(luna_fv* fv, double* out, int on_device) 
     const size_t GS = D == 3 ? luna::grad_stride<3>() : luna::grad_stride<2>();
     const size_t N = static_cast<size_t>(fv->n);
     if (fv->precision == LUNA_FP64) {
-        LUNA_CUDA(cudaMemcpy2DAsync(out, width * sizeof(double), fv->grad64.ptr, GS * sizeof(double), width * sizeof(double), N,
+        const double* src = fv->grad64.ptr;
+        size_t pitch = GS;
+        if (fv->grads_in_wg) {  // the merged rows: g after the row's V values of W
+            src = fv->wg64.ptr + (D + 2);
+            pitch = D == 3 ? luna::wg_stride<3>() : luna::wg_stride<2>();
+        }
+        LUNA_CUDA(cudaMemcpy2DAsync(out, width * sizeof(double), src, pitch * sizeof(double), width * sizeof(double), N,
                                     on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, fv->stream));
         LUNA_CUDA(cudaStreamSynchronize(fv->stream));
         return LUNA_OK;
@@ -1143,7 +1167,7 @@ LUNA_API luna_status luna_fv_device_bytes(luna_fv* fv, int64_t* out) {
     b += fv->owner.bytes() + fv->neighbour.bytes() + fv->start.bytes() + fv->list.bytes();
     b += fv->area.bytes() + fv->mag.bytes() + fv->fcen.bytes() + fv->cen.bytes() + fv->vol.bytes() + fv->pos.bytes();
     b += fv->q.bytes() + fv->next.bytes() + fv->prims.bytes() + fv->grad64.bytes() + fv->grad32.bytes() + fv->flux.bytes();
-    b += fv->grad16.bytes() + fv->grad16_exp.bytes();
+    b += fv->grad16.bytes() + fv->grad16_exp.bytes() + fv->wg64.bytes();
     b += fv->w.bytes() + fv->x.bytes() + fv->old_cen.bytes() + fv->steps.bytes() + fv->counters.bytes();
     b += fv->adj_fit.bytes() + fv->adj_face_bar.bytes() + fv->adj_wbar.bytes() + fv->adj_bbar.bytes() + fv->adj_boundbar.bytes();
     b += fv->adj_qbar.bytes() + fv->adj_flags.bytes() + fv->adj_bound_face.bytes();
