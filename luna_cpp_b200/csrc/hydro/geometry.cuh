@@ -672,10 +672,20 @@ __global__ void __launch_bounds__(kTileCells, MINB) k_sweep_tiles(MeshDev<D> m, 
                     for (int c = 0; c < S; c += 2) dst[c / 2] = make_double2(row[c], row[c + 1]);
                     stored = true;
                 }
-            if (!stored) {
-                G* out = grad_out + static_cast<int64_t>(GS) * i;
+            if (!stored) {  // the row in 16-B vector stores (pad zeroed)
+                G row[GS];
 #pragma unroll
-                for (int c = 0; c < V * D; ++c) out[c] = g[c];
+                for (int c = 0; c < GS; ++c) row[c] = c < V * D ? g[c] : G(0);
+                using Vec16 = typename std::conditional<sizeof(G) == sizeof(double), double2, float4>::type;
+                constexpr int per = 16 / static_cast<int>(sizeof(G));
+                Vec16* out = reinterpret_cast<Vec16*>(grad_out + static_cast<int64_t>(GS) * i);
+#pragma unroll
+                for (int c = 0; c < GS; c += per) {
+                    if constexpr (sizeof(G) == sizeof(double))
+                        out[c / per] = make_double2(row[c], row[c + 1]);
+                    else
+                        out[c / per] = make_float4(row[c], row[c + 1], row[c + 2], row[c + 3]);
+                }
             }
         }
     }

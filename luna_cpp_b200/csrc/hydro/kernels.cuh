@@ -147,7 +147,6 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// A cell's primitive row (W, c, r, pad: 64 B, 64-B aligned) in two vector loads (3D), one (2D: W only).
 // A merged row of the FP64 static per-face step: the cell's W (V doubles) then its gradient (V D), padded to whole
 // 32-B sectors: 20 doubles (160 B, 5 sectors) in 3D against the 2 + 4 sectors of a primitive row and a gradient row.
 template <int D>
@@ -155,6 +154,7 @@ constexpr int wg_stride() {
     return ((D + 2) * (D + 1) + 3) / 4 * 4;
 }
 
+// A cell's primitive row (W, c, r, pad: 64 B, 64-B aligned) in two vector loads (3D), one (2D: W only).
 template <int D>
 __device__ __forceinline__ void load_prim_row(const double* prims, int i, double* row) {
     const double* p = prims + 8 * static_cast<int64_t>(i);
@@ -634,11 +634,22 @@ __global__ void __launch_bounds__(256, Windowed ? LUNA_UPDATE_MIN_BLOCKS : 1) k_
 #pragma unroll
         for (int v = 0; v < V; ++v) U[v] = next[v] * inv;
         primitive<D>(U, gas, W);
-        double* p = prims + PS * i;
+        double row[PS];
 #pragma unroll
-        for (int v = 0; v < V; ++v) p[v] = W[v];
-        p[V] = sqrt(gas.gamma * W[D + 1] / W[0]);
-        p[V + 1] = radius<D>(m.vol[i]);
+        for (int v = 0; v < V; ++v) row[v] = W[v];
+        row[V] = sqrt(gas.gamma * W[D + 1] / W[0]);
+        row[V + 1] = radius<D>(m.vol[i]);
+#pragma unroll
+        for (int c = V + 2; c < PS; ++c) row[c] = 0.0;
+        if constexpr (Windowed) {  // the library's rows: 16-B vector stores
+            double2* p = reinterpret_cast<double2*>(prims + PS * static_cast<int64_t>(i));
+#pragma unroll
+            for (int c = 0; c < PS; c += 2) p[c / 2] = make_double2(row[c], row[c + 1]);
+        } else {
+            double* p = prims + PS * i;
+#pragma unroll
+            for (int c = 0; c < V + 2; ++c) p[c] = row[c];
+        }
     }
 }
 
