@@ -1,7 +1,7 @@
 """In-tree build of the native libraries: ``python -m luna_cpp_b200.build [hydro|mesh|oracle|all]``.
 
 - ``libluna_b200.so``: the hydro step, CUDA for sm_100a only (nvcc -gencode arch=compute_100a,code=sm_100a), C ABI in
-  include/luna_b200.h;
+  include/luna_b200.h, and the device remesher of the moving mesh (include/luna_remesh.h);
 - ``libluna_mesh.so``: the periodic Voronoi mesh builder (host C++, OpenMP);
 - ``oracle/liboracle.so``: the CPU oracle the tests check against (plain C, no multiply-add contraction).
 The libraries are built next to their sources so they travel with the tree.
@@ -53,8 +53,10 @@ def _sources(directory, exts):
 def build_mesh(force=False):
     target = os.path.join(PKG, "libluna_mesh.so")
     srcs = [os.path.join(CSRC, "mesh", "voronoi_build.cpp")]
-    if force or _stale(target, srcs + [os.path.join(CSRC, "mesh", "luna_mesh.h")]):
-        _run(["g++", "-O3", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-Wall", "-o", target] + srcs)
+    headers = [os.path.join(CSRC, "mesh", h) for h in ("luna_mesh.h", "voronoi_cell.h", "voronoi_grid.h")]
+    if force or _stale(target, srcs + headers):
+        # no contraction: the device remesher compiles the same cell code with -fmad=false and must match it bit for bit
+        _run(["g++", "-O3", "-std=c++17", "-ffp-contract=off", "-fopenmp", "-fPIC", "-shared", "-Wall", "-o", target] + srcs)
     return target
 
 
@@ -70,14 +72,25 @@ def build_oracle(force=False):
 def build_hydro(force=False, extra=()):
     target = os.path.join(PKG, "libluna_b200.so")
     hydro = os.path.join(CSRC, "hydro")
+    mesh = os.path.join(CSRC, "mesh")
     cu = [s for s in _sources(hydro, {".cu"})]
-    deps = _sources(hydro, {".cu", ".cuh", ".h", ".hpp"}) + _sources(INCLUDE, {".h"})
+    remesh = os.path.join(mesh, "remesh.cu")
+    remesh_deps = [remesh] + [os.path.join(mesh, h) for h in ("voronoi_cell.h", "voronoi_grid.h")]
+    deps = _sources(hydro, {".cu", ".cuh", ".h", ".hpp"}) + _sources(INCLUDE, {".h"}) + remesh_deps
     if not cu:
         return None
     if force or _stale(target, deps):
+        # The device remesher runs the host mesh builder's cell code and must give its bits: no multiply-add
+        # contraction in that object (the hydro kernels keep it).
+        obj_dir = os.path.join(PKG, "_build")
+        os.makedirs(obj_dir, exist_ok=True)
+        remesh_obj = os.path.join(obj_dir, "remesh.o")
+        _run([_nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler",
+              "-ffp-contract=off", "-Xcompiler", "-fvisibility=hidden", "-c", "-I", INCLUDE, "-I", mesh, "-o", remesh_obj,
+              remesh])
         _run([_nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-fvisibility=hidden", "-shared", "-I", INCLUDE, "-I", hydro, "-o", target, *extra, *cu,
-              "-lcudart"])
+              remesh_obj, "-lcudart"])
     return target
 
 

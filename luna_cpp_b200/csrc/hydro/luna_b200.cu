@@ -44,11 +44,12 @@ luna_status set_error(luna_status s, const std::string& what) {
         if (st_ != LUNA_OK) return st_;     \
     } while (0)
 
-// A device allocation that frees itself.
+// A device allocation that frees itself. It only grows: a smaller request (the next mesh of a moving run, whose face
+// count changes every step) reuses the allocation instead of freeing it (cudaFree synchronises the device).
 template <class T>
 struct DevArray {
     T* ptr = nullptr;
-    size_t count = 0;
+    size_t count = 0, capacity = 0;
     DevArray() = default;
     DevArray(const DevArray&) = delete;
     DevArray& operator=(const DevArray&) = delete;
@@ -56,10 +57,13 @@ struct DevArray {
     void release() {
         if (ptr) cudaFree(ptr);
         ptr = nullptr;
-        count = 0;
+        count = capacity = 0;
     }
     luna_status alloc(size_t n, const char* what) {
-        if (n == count && ptr) return LUNA_OK;
+        if (ptr && n <= capacity) {
+            count = n;
+            return LUNA_OK;
+        }
         release();
         if (n == 0) return LUNA_OK;
         cudaError_t e = cudaMalloc(&ptr, n * sizeof(T));
@@ -69,10 +73,10 @@ struct DevArray {
             return set_error(e == cudaErrorMemoryAllocation ? LUNA_ENOMEM : LUNA_ECUDA,
                              std::string("cudaMalloc(") + what + "): " + cudaGetErrorString(e));
         }
-        count = n;
+        count = capacity = n;
         return LUNA_OK;
     }
-    size_t bytes() const { return count * sizeof(T); }
+    size_t bytes() const { return capacity * sizeof(T); }
 };
 
 constexpr int kBlockCells = 128;
@@ -141,7 +145,11 @@ struct luna_fv {
     double grid_step = 0, per_step = 0;
     long long period[3] = {1, 1, 1};
 
+    luna::DeviceTiler* tiler = nullptr;  // the sweep's tiles cut on the device, for meshes given in device memory
+    DevArray<unsigned int> list_check;   // bad entries found in a device mesh's lists
+
     ~luna_fv() {
+        if (tiler) luna::device_tiler_destroy(tiler);
         if (host_counters) cudaFreeHost(host_counters);
         for (auto& e : event_pool) {
             cudaEventDestroy(e.first);
@@ -250,10 +258,36 @@ luna_status validate_mesh(const luna_mesh_desc* m, int dim, int64_t n) {
     return LUNA_OK;
 }
 
-// The reordered rows of the current mesh (geometry.cuh::k_geometry), in the policy's gradient type.
+// The reordered rows of the current mesh (geometry.cuh::k_geometry), in the policy's gradient type, once the tiles are
+// in place (geo_order, geo_slice_base, geo_stage_start, geo_stage_cells, geo_nbr holding each entry's staged row).
 template <int D, class G>
-luna_status build_geometry(luna_fv* fv, const luna::SweepTiles& tiles) {
+luna_status finish_geometry(luna_fv* fv, size_t slots) {
     const size_t N = static_cast<size_t>(fv->n), F = static_cast<size_t>(fv->f);
+    LUNA_TRY(fv->geo_c01.alloc(sizeof(luna::Pair<G>) * slots, "entry gradient rows"));
+    LUNA_TRY(fv->geo_c2.alloc(sizeof(G) * slots, "entry gradient rows"));
+    LUNA_TRY(fv->geo_off01.alloc(sizeof(luna::Pair<G>) * slots, "entry offsets"));
+    LUNA_TRY(fv->geo_off2.alloc(sizeof(G) * slots, "entry offsets"));
+    LUNA_TRY(fv->geo_faces.alloc(sizeof(luna::FaceRow<G>) * (F > 0 ? F : 1), "face rows"));
+    LUNA_TRY(fv->geo_angle.alloc(N, "face angles"));
+    LUNA_TRY(fv->geo_reach2.alloc(N, "cell reach"));
+    const int64_t threads = fv->tiles * luna::kTileCells;
+    if (threads > 0) {
+        luna::k_geometry<D, G><<<blocks(threads, 128), 128, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->geometry_dev<D, G>());
+        LUNA_CUDA(cudaGetLastError());
+    }
+    // The host vectors' contents (host tiles) must outlive the asynchronous uploads.
+    LUNA_CUDA(cudaStreamSynchronize(fv->stream));
+    return LUNA_OK;
+}
+
+luna_status finish_geometry_any(luna_fv* fv, size_t slots) {
+    const int D = fv->dim;
+    return fv->precision == LUNA_FP64 ? (D == 3 ? finish_geometry<3, double>(fv, slots) : finish_geometry<2, double>(fv, slots))
+                                      : (D == 3 ? finish_geometry<3, float>(fv, slots) : finish_geometry<2, float>(fv, slots));
+}
+
+// Geometry from tiles cut on the host.
+luna_status build_geometry(luna_fv* fv, const luna::SweepTiles& tiles) {
     const size_t slots = tiles.local.size();
     fv->tiles = tiles.tiles;
     fv->normal_tiles = tiles.normal_tiles;
@@ -266,20 +300,65 @@ luna_status build_geometry(luna_fv* fv, const luna::SweepTiles& tiles) {
                     "tile rows"));
     // the entries' staged rows; k_geometry adds the owned and tiny bits in place
     LUNA_TRY(upload(fv->geo_nbr, tiles.local.data(), slots, false, fv->stream, "entry neighbours"));
-    LUNA_TRY(fv->geo_c01.alloc(sizeof(luna::Pair<G>) * slots, "entry gradient rows"));
-    LUNA_TRY(fv->geo_c2.alloc(sizeof(G) * slots, "entry gradient rows"));
-    LUNA_TRY(fv->geo_off01.alloc(sizeof(luna::Pair<G>) * slots, "entry offsets"));
-    LUNA_TRY(fv->geo_off2.alloc(sizeof(G) * slots, "entry offsets"));
-    LUNA_TRY(fv->geo_faces.alloc(sizeof(luna::FaceRow<G>) * (F > 0 ? F : 1), "face rows"));
-    LUNA_TRY(fv->geo_angle.alloc(N, "face angles"));
-    LUNA_TRY(fv->geo_reach2.alloc(N, "cell reach"));
-    const int64_t threads = tiles.tiles * luna::kTileCells;
-    if (threads > 0) {
-        luna::k_geometry<D, G><<<blocks(threads, 128), 128, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->geometry_dev<D, G>());
-        LUNA_CUDA(cudaGetLastError());
+    return finish_geometry_any(fv, slots);
+}
+
+// Geometry from tiles cut on the device (tiles_device.cu), for a mesh the caller holds in device memory; false in
+// *done when a tile does not fit the device cut (the caller cuts on the host instead).
+luna_status build_geometry_device(luna_fv* fv, bool* done) {
+    *done = false;
+    if (!fv->tiler) fv->tiler = luna::device_tiler_create();
+    luna::DeviceTilePlan plan;
+    LUNA_TRY(luna::device_tiles_plan(fv->tiler, fv->dim, fv->n, fv->pos.ptr, fv->box, fv->start.ptr, fv->list.ptr, fv->owner.ptr,
+                                     fv->neighbour.ptr, fv->stream, &plan));
+    if (!plan.fits) return LUNA_OK;
+    const size_t slots = static_cast<size_t>(plan.slots > 0 ? plan.slots : 1);
+    fv->tiles = plan.tiles;
+    fv->normal_tiles = plan.normal_tiles;
+    fv->normal_rows = plan.normal_rows;
+    fv->big_rows = plan.big_rows;
+    LUNA_TRY(fv->geo_order.alloc(static_cast<size_t>(plan.tiles) * luna::kTileCells, "sweep order"));
+    LUNA_TRY(fv->geo_slice_base.alloc(static_cast<size_t>(plan.tiles) * (luna::kTileCells / 32) + 1, "slice bases"));
+    LUNA_TRY(fv->geo_stage_start.alloc(static_cast<size_t>(plan.tiles) + 1, "tile row starts"));
+    LUNA_TRY(fv->geo_stage_cells.alloc(static_cast<size_t>(plan.staged > 0 ? plan.staged : 1), "tile rows"));
+    LUNA_TRY(fv->geo_nbr.alloc(slots, "entry neighbours"));
+    LUNA_TRY(luna::device_tiles_fill(fv->tiler, fv->geo_order.ptr, fv->geo_slice_base.ptr, fv->geo_stage_start.ptr, fv->geo_stage_cells.ptr,
+                                     fv->geo_nbr.ptr, fv->stream));
+    LUNA_TRY(finish_geometry_any(fv, slots));
+    *done = true;
+    return LUNA_OK;
+}
+
+// A device mesh's lists checked in place before any kernel follows them (the host's are checked by validate_mesh): the
+// list starts run from 0 to 2F and do not fall, list entries name faces below F, owners and neighbours name cells below
+// N. Counts the bad entries.
+__global__ void k_check_lists(int64_t N, int64_t F, const int32_t* __restrict__ start, const int32_t* __restrict__ list,
+                              const int32_t* __restrict__ owner, const int32_t* __restrict__ neighbour, unsigned int* __restrict__ bad) {
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    unsigned int wrong = 0;
+    if (i < N) {
+        const int64_t s0 = start[i], s1 = start[i + 1];
+        wrong += s0 < 0 || s1 < s0 || s1 > 2 * F || (i == 0 && s0 != 0) || (i == N - 1 && s1 != 2 * F);
     }
-    // The host vectors' contents must outlive the asynchronous uploads.
+    if (i < 2 * F) {
+        const int32_t e = list[i];
+        wrong += (e >= 0 ? e : ~e) >= F;
+    }
+    if (i < F) wrong += owner[i] < 0 || owner[i] >= N || neighbour[i] < 0 || neighbour[i] >= N;
+    if (wrong) atomicAdd(bad, wrong);
+}
+
+luna_status check_device_lists(luna_fv* fv, int64_t N, int64_t F) {
+    LUNA_TRY(fv->list_check.alloc(1, "list check"));
+    LUNA_CUDA(cudaMemsetAsync(fv->list_check.ptr, 0, sizeof(unsigned int), fv->stream));
+    const int64_t threads = N > 2 * F ? N : 2 * F;
+    k_check_lists<<<blocks(threads, 256), 256, 0, fv->stream>>>(N, F, fv->start.ptr, fv->list.ptr, fv->owner.ptr, fv->neighbour.ptr,
+                                                                 fv->list_check.ptr);
+    LUNA_CUDA(cudaGetLastError());
+    unsigned int bad = 0;
+    LUNA_CUDA(cudaMemcpyAsync(&bad, fv->list_check.ptr, sizeof(bad), cudaMemcpyDeviceToHost, fv->stream));
     LUNA_CUDA(cudaStreamSynchronize(fv->stream));
+    if (bad) return set_error(LUNA_EINVAL, "mesh: " + std::to_string(bad) + " bad entries in the device lists");
     return LUNA_OK;
 }
 
@@ -309,9 +388,15 @@ luna_status load_mesh(luna_fv* fv, const luna_mesh_desc* m) {
     }
     // 4 doubles past the last row: the update reads each row through its 32-B aligned 64-B window (load_row_windowed)
     if (fv->update == LUNA_UPDATE_PER_FACE) LUNA_TRY(fv->flux.alloc(F * (D + 2) + 4, "flux rows"));
-    // The sweep's tiles are cut on the host from the lists and the generators (copied back once per mesh when the
-    // caller's arrays are on the device). Lists in device memory are trusted as voronoi-cpp's; the sweep does not
-    // re-check them.
+    // The sweep's tiles: cut on the device when the caller's arrays are there (a mesh rebuilt every step stays on the
+    // device), else on the host from the lists and the generators (also the fallback for a tile the device cut cannot
+    // hold). Lists in device memory are checked for indices out of range first.
+    if (dev) {
+        LUNA_TRY(check_device_lists(fv, static_cast<int64_t>(N), static_cast<int64_t>(F)));
+        bool done = false;
+        LUNA_TRY(build_geometry_device(fv, &done));
+        if (done) return LUNA_OK;
+    }
     std::vector<int32_t> h_start, h_list, h_owner, h_neighbour;
     std::vector<double> h_pos;
     const int32_t *start = m->cell_face_start, *list = m->cell_face, *own = m->owner, *nbr = m->neighbour;
@@ -338,8 +423,7 @@ luna_status load_mesh(luna_fv* fv, const luna_mesh_desc* m) {
     luna::SweepTiles tiles;
     const std::string why = luna::build_sweep_tiles(D, static_cast<int64_t>(N), pos, m->box, start, list, own, nbr, tiles);
     if (!why.empty()) return set_error(LUNA_EINVAL, "mesh: " + why);
-    return fv->precision == LUNA_FP64 ? (D == 3 ? build_geometry<3, double>(fv, tiles) : build_geometry<2, double>(fv, tiles))
-                                      : (D == 3 ? build_geometry<3, float>(fv, tiles) : build_geometry<2, float>(fv, tiles));
+    return build_geometry(fv, tiles);
 }
 
 template <int D>

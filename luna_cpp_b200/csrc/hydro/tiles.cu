@@ -8,27 +8,6 @@
 
 namespace luna {
 
-namespace {
-
-// The Morton key of a generator: its cell on a 2^b grid of the box per axis (b = 21 in 3D, 32 in 2D), bits
-// interleaved with axis 0 lowest.
-uint64_t morton_key(int dim, const double* x, const double* box) {
-    const int bits = dim == 3 ? 21 : 32;
-    const double cells = std::ldexp(1.0, bits);
-    uint64_t key = 0;
-    for (int a = 0; a < dim; ++a) {
-        double u = x[a] / box[a];
-        u -= std::floor(u);  // generators may sit anywhere in their periodic image
-        uint64_t q = static_cast<uint64_t>(u * cells);
-        const uint64_t top = (uint64_t(1) << bits) - 1;
-        if (q > top) q = top;
-        for (int b = 0; b < bits; ++b) key |= ((q >> b) & 1u) << (dim * b + a);
-    }
-    return key;
-}
-
-}  // namespace
-
 std::string build_sweep_tiles(int dim, int64_t n_cells, const double* positions, const double* box, const int32_t* start,
                               const int32_t* list, const int32_t* owner, const int32_t* neighbour, SweepTiles& out) {
     const int64_t N = n_cells;

@@ -1,4 +1,4 @@
-// Periodic Voronoi mesh builder: cells by half-space clipping, faces in voronoi-cpp's layout (see luna_mesh.h).
+// Periodic Voronoi mesh builder: cells by half-space clipping (voronoi_cell.h), faces in voronoi-cpp's layout (see luna_mesh.h).
 //
 // Each cell starts as the periodic box centred on its generator (its own images bound it there) and is clipped by the
 // bisector plane (2D: line) of every generator image that can still cut it. Candidates come from a bucket grid visited in
@@ -7,15 +7,17 @@
 // cells; faces are numbered by owner, then by neighbour, and every cell's list is ordered by neighbour.
 
 #include "luna_mesh.h"
+#include "voronoi_cell.h"
+#include "voronoi_grid.h"
 
 #include <algorithm>
 #include <array>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <memory>
 #include <random>
 #include <string>
-#include <type_traits>
 #include <vector>
 
 #ifdef _OPENMP
@@ -31,14 +33,6 @@ int fail(const std::string& what) {
     return 1;
 }
 
-using V3 = std::array<double, 3>;
-
-inline double dot3(const V3& a, const V3& b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
-inline V3 cross3(const V3& a, const V3& b) {
-    return {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
-}
-inline V3 sub3(const V3& a, const V3& b) { return {a[0] - b[0], a[1] - b[1], a[2] - b[2]}; }
-
 // One emitted face of a cell: the neighbour, area vector out of the cell, face centroid relative to the cell's generator.
 struct CellFace {
     int32_t j;
@@ -46,230 +40,44 @@ struct CellFace {
     double c[3];
 };
 
-// A convex polyhedron around the origin: vertices, and faces as CCW (seen from outside) vertex loops with a tag each.
-struct Poly3 {
-    std::vector<V3> v, nv;
-    std::vector<int> idx, nidx;           // face loops, concatenated
-    std::vector<int> fo, nfo;             // face offsets into idx (size faces + 1)
-    std::vector<int64_t> tag, ntag;       // neighbour per face (-1: box)
-    std::vector<double> s;                // signed distances of the vertices to the cutting plane
-    std::vector<int> remap;               // old vertex -> new vertex (-1: removed)
-    std::vector<std::pair<uint64_t, int>> edge_memo;  // intersection vertex per cut edge
-    std::vector<int> cut;                 // vertices of the new face
-    double eps = 0;
+// The grid's buckets filled on the host: items in index order within each bucket.
+struct HostGrid {
+    luna_voronoi::GridShape shape;
+    std::vector<int64_t> start;
+    std::vector<int32_t> items;
 
-    void box(const double* half) {
-        v.clear();
-        for (int k = 0; k < 8; ++k)
-            v.push_back({(k & 1) ? half[0] : -half[0], (k & 2) ? half[1] : -half[1], (k & 4) ? half[2] : -half[2]});
-        // Faces CCW seen from outside (-x, +x, -y, +y, -z, +z).
-        const int loops[6][4] = {{0, 4, 6, 2}, {1, 3, 7, 5}, {0, 1, 5, 4}, {2, 6, 7, 3}, {0, 2, 3, 1}, {4, 5, 7, 6}};
-        idx.clear();
-        fo.assign(1, 0);
-        tag.clear();
-        for (auto& l : loops) {
-            for (int k = 0; k < 4; ++k) idx.push_back(l[k]);
-            fo.push_back(static_cast<int>(idx.size()));
-            tag.push_back(-1);
-        }
-    }
-    double max_radius2() const {
-        double r = 0;
-        for (const V3& p : v) r = std::max(r, dot3(p, p));
-        return r;
-    }
-    int memo(int a, int b) {
-        const uint64_t key = a < b ? (uint64_t(a) << 32 | uint32_t(b)) : (uint64_t(b) << 32 | uint32_t(a));
-        for (const auto& e : edge_memo)
-            if (e.first == key) return e.second;
-        const double t = s[a] / (s[a] - s[b]);
-        const V3& p = v[a];
-        const V3& q = v[b];
-        nv.push_back({p[0] + t * (q[0] - p[0]), p[1] + t * (q[1] - p[1]), p[2] + t * (q[2] - p[2])});
-        const int id = static_cast<int>(nv.size()) - 1;
-        edge_memo.push_back({key, id});
-        cut.push_back(id);
-        return id;
-    }
-    // Keeps {y : n.y <= c}; the new face gets tag t. Returns whether anything was cut.
-    bool clip(const V3& n, double c, int64_t t) {
-        const int nvert = static_cast<int>(v.size());
-        s.resize(nvert);
-        double smax = -1e300;
-        for (int k = 0; k < nvert; ++k) {
-            s[k] = dot3(n, v[k]) - c;
-            smax = std::max(smax, s[k]);
-        }
-        if (smax <= eps) return false;
-        remap.assign(nvert, -1);
-        nv.clear();
-        cut.clear();
-        edge_memo.clear();
-        for (int k = 0; k < nvert; ++k)
-            if (s[k] <= eps) {
-                remap[k] = static_cast<int>(nv.size());
-                nv.push_back(v[k]);
-                if (s[k] >= -eps) cut.push_back(remap[k]);
-            }
-        nidx.clear();
-        nfo.assign(1, 0);
-        ntag.clear();
-        const int nf = static_cast<int>(tag.size());
-        for (int f = 0; f < nf; ++f) {
-            const int a0 = fo[f], m = fo[f + 1] - fo[f];
-            const size_t begin = nidx.size();
-            for (int k = 0; k < m; ++k) {
-                const int a = idx[a0 + k], b = idx[a0 + (k + 1) % m];
-                if (s[a] <= eps) nidx.push_back(remap[a]);
-                if ((s[a] < -eps && s[b] > eps) || (s[a] > eps && s[b] < -eps)) nidx.push_back(memo(a, b));
-            }
-            if (nidx.size() - begin >= 3) {
-                nfo.push_back(static_cast<int>(nidx.size()));
-                ntag.push_back(tag[f]);
-            } else {
-                nidx.resize(begin);
-            }
-        }
-        // The new face: the cut vertices sorted by angle around their mean, CCW about n (outward).
-        std::sort(cut.begin(), cut.end());
-        cut.erase(std::unique(cut.begin(), cut.end()), cut.end());
-        if (cut.size() >= 3) {
-            V3 mean{0, 0, 0};
-            for (int id : cut)
-                for (int a = 0; a < 3; ++a) mean[a] += nv[id][a];
-            for (int a = 0; a < 3; ++a) mean[a] /= static_cast<double>(cut.size());
-            V3 u = std::fabs(n[0]) < 0.6 ? V3{1, 0, 0} : V3{0, 1, 0};
-            const double un = dot3(u, n);
-            u = {u[0] - un * n[0], u[1] - un * n[1], u[2] - un * n[2]};
-            const double ul = std::sqrt(dot3(u, u));
-            u = {u[0] / ul, u[1] / ul, u[2] / ul};
-            const V3 w = cross3(n, u);
-            std::vector<std::pair<double, int>> order;
-            order.reserve(cut.size());
-            for (int id : cut) {
-                const V3 d = sub3(nv[id], mean);
-                order.push_back({std::atan2(dot3(d, w), dot3(d, u)), id});
-            }
-            std::sort(order.begin(), order.end());
-            for (const auto& o : order) nidx.push_back(o.second);
-            nfo.push_back(static_cast<int>(nidx.size()));
-            ntag.push_back(t);
-        }
-        v.swap(nv);
-        idx.swap(nidx);
-        fo.swap(nfo);
-        tag.swap(ntag);
-        return true;
-    }
-};
-
-// A convex polygon around the origin, CCW, with the tag of the edge leaving each vertex.
-struct Poly2 {
-    std::vector<std::array<double, 2>> v, nv;
-    std::vector<int64_t> tag, ntag;
-    double eps = 0;
-    void box(const double* half) {
-        v = {{-half[0], -half[1]}, {half[0], -half[1]}, {half[0], half[1]}, {-half[0], half[1]}};
-        tag = {-1, -1, -1, -1};
-    }
-    double max_radius2() const {
-        double r = 0;
-        for (const auto& p : v) r = std::max(r, p[0] * p[0] + p[1] * p[1]);
-        return r;
-    }
-    bool clip(const double* n, double c, int64_t t) {
-        const int m = static_cast<int>(v.size());
-        std::vector<double> s(m);
-        double smax = -1e300;
-        for (int k = 0; k < m; ++k) {
-            s[k] = n[0] * v[k][0] + n[1] * v[k][1] - c;
-            smax = std::max(smax, s[k]);
-        }
-        if (smax <= eps) return false;
-        nv.clear();
-        ntag.clear();
-        for (int k = 0; k < m; ++k) {
-            const int b = (k + 1) % m;
-            const bool ain = s[k] <= eps, bin = s[b] <= eps;
-            if (ain) {
-                nv.push_back(v[k]);
-                // The edge k -> b stays (tag[k]) if b is inside; if b is outside, the edge is cut and continues to the
-                // exit point with tag[k].
-                ntag.push_back(tag[k]);
-                if (!bin && s[k] < -eps) {
-                    const double u = s[k] / (s[k] - s[b]);
-                    nv.push_back({v[k][0] + u * (v[b][0] - v[k][0]), v[k][1] + u * (v[b][1] - v[k][1])});
-                    ntag.push_back(t);  // from the exit point along the cut
-                } else if (!bin) {
-                    ntag.back() = t;  // k sits on the line: the cut starts here
-                }
-            } else if (bin && s[b] < -eps) {
-                const double u = s[k] / (s[k] - s[b]);
-                nv.push_back({v[k][0] + u * (v[b][0] - v[k][0]), v[k][1] + u * (v[b][1] - v[k][1])});
-                ntag.push_back(tag[k]);  // entry point, then along edge k to b
-            }
-        }
-        v.swap(nv);
-        tag.swap(ntag);
-        return true;
-    }
-};
-
-struct Grid {
-    int dim;
-    int nb[3];
-    double w[3];
-    std::vector<int64_t> start;   // bucket -> first item
-    std::vector<int32_t> items;   // point ids by bucket
-    std::vector<std::array<int, 3>> offsets;  // sorted by the lower bound of their distance
-    std::vector<double> bound2;
-
-    int bucket_of(const double* x, int a) const {
-        int b = static_cast<int>(std::floor(x[a] / w[a]));
-        return std::min(std::max(b, 0), nb[a] - 1);
-    }
     void build(int d, int64_t n, const double* pts, const double* side) {
-        dim = d;
-        double vol = 1;
-        for (int a = 0; a < d; ++a) vol *= side[a];
-        const double spacing = std::pow(vol / static_cast<double>(n), 1.0 / d);
-        int64_t total = 1;
-        for (int a = 0; a < 3; ++a) {
-            nb[a] = a < d ? std::max(1, static_cast<int>(std::floor(side[a] / spacing))) : 1;
-            w[a] = a < d ? side[a] / nb[a] : 1.0;
-            total *= nb[a];
-        }
-        std::vector<int64_t> count(total + 1, 0);
+        shape.build(d, n, side);
+        const luna_voronoi::Grid g = view();
+        std::vector<int64_t> count(shape.buckets + 1, 0);
         std::vector<int64_t> of(n);
         for (int64_t i = 0; i < n; ++i) {
             int64_t b = 0;
-            for (int a = 0; a < d; ++a) b = b * nb[a] + bucket_of(pts + d * i, a);
+            for (int a = 0; a < d; ++a) b = b * shape.nb[a] + luna_voronoi::bucket_of(g, pts + d * i, a);
             of[i] = b;
             ++count[b + 1];
         }
-        for (int64_t b = 0; b < total; ++b) count[b + 1] += count[b];
+        for (int64_t b = 0; b < shape.buckets; ++b) count[b + 1] += count[b];
         start = count;
         items.resize(n);
         std::vector<int64_t> fill(count.begin(), count.end() - 1);
         for (int64_t i = 0; i < n; ++i) items[fill[of[i]]++] = static_cast<int32_t>(i);
-        const int K = 8;
-        offsets.clear();
-        for (int x = -K; x <= K; ++x)
-            for (int y = (d >= 2 ? -K : 0); y <= (d >= 2 ? K : 0); ++y)
-                for (int z = (d >= 3 ? -K : 0); z <= (d >= 3 ? K : 0); ++z) offsets.push_back({x, y, z});
-        auto lower = [&](const std::array<int, 3>& o) {
-            double s = 0;
-            for (int a = 0; a < d; ++a) {
-                const double g = std::max(0, std::abs(o[a]) - 1) * w[a];
-                s += g * g;
-            }
-            return s;
-        };
-        std::stable_sort(offsets.begin(), offsets.end(), [&](const auto& p, const auto& q) { return lower(p) < lower(q); });
-        bound2.resize(offsets.size());
-        for (size_t k = 0; k < offsets.size(); ++k) bound2[k] = lower(offsets[k]);
+    }
+    luna_voronoi::Grid view() const {
+        return shape.view(start.data(), items.data(), shape.offsets.data(), shape.bound2.data());
     }
 };
+
+const char* cell_error(int code) {
+    switch (code) {
+        case luna_voronoi::kOutOfOffsets: return "voronoi: the bucket search ran out of offsets (points too sparse for the grid)";
+        case luna_voronoi::kReachesBox: return "voronoi: a cell reaches the box (box too small for the points)";
+        case luna_voronoi::kTouchesSelf: return "voronoi: a cell touches its own periodic image (box too small for the points)";
+        case luna_voronoi::kDuplicatePair: return "voronoi: two faces between the same pair of cells (box too small for unique nearest images)";
+        case luna_voronoi::kCapacity: return "voronoi: a cell has more vertices or faces than the builder holds";
+        default: return "voronoi: unknown cell error";
+    }
+}
 
 }  // namespace
 
@@ -283,144 +91,28 @@ struct luna_mesh_build {
 
 namespace {
 
-// Cell i: clipped, then its faces (sorted by neighbour), volume and centroid. Returns false with a message on error.
-template <class Poly>
-bool cell(int dim, int64_t i, const double* pos, const double* side, const Grid& grid, Poly& poly, std::vector<CellFace>& faces,
-          double& volume, double* centroid, std::string& err) {
-    const double* xi = pos + dim * i;
-    double half[3];
-    double scale = 0;
-    for (int a = 0; a < dim; ++a) {
-        half[a] = 0.5 * side[a];
-        scale = std::max(scale, side[a]);
-    }
-    poly.box(half);
-    poly.eps = 1e-13 * scale;
-    int bi[3] = {0, 0, 0};
-    for (int a = 0; a < dim; ++a) bi[a] = grid.bucket_of(xi, a);
-    double rmax2 = poly.max_radius2();
-    bool done = false;
-    for (size_t k = 0; k < grid.offsets.size(); ++k) {
-        if (grid.bound2[k] > 4.0 * rmax2) {
-            done = true;
-            break;
-        }
-        const auto& o = grid.offsets[k];
-        int64_t b = 0;
-        double shift[3] = {0, 0, 0};
-        for (int a = 0; a < dim; ++a) {
-            const int t = bi[a] + o[a];
-            const int tw = ((t % grid.nb[a]) + grid.nb[a]) % grid.nb[a];
-            shift[a] = static_cast<double>((t - tw) / grid.nb[a]) * side[a];
-            b = b * grid.nb[a] + tw;
-        }
-        for (int64_t q = grid.start[b]; q < grid.start[b + 1]; ++q) {
-            const int32_t j = grid.items[q];
-            double d[3] = {0, 0, 0};
-            double d2 = 0;
-            for (int a = 0; a < dim; ++a) {
-                d[a] = pos[dim * j + a] + shift[a] - xi[a];
-                d2 += d[a] * d[a];
-            }
-            if (d2 == 0) continue;  // the generator itself
-            if (d2 > 4.0 * rmax2) continue;
-            const double inv = 1.0 / std::sqrt(d2);
-            if constexpr (std::is_same_v<Poly, Poly3>) {
-                const V3 n{d[0] * inv, d[1] * inv, d[2] * inv};
-                if (poly.clip(n, 0.5 * d2 * inv, j)) rmax2 = poly.max_radius2();
-            } else {
-                const double n[2] = {d[0] * inv, d[1] * inv};
-                if (poly.clip(n, 0.5 * d2 * inv, j)) rmax2 = poly.max_radius2();
-            }
+// Cell i: clipped (voronoi_cell.h), then its faces by neighbour, volume and centroid. Returns 0 or a cell error.
+struct CellWork {
+    luna_voronoi::HostPoly3 p3;
+    luna_voronoi::HostPoly2 p2;
+    luna_voronoi::HostCellFaces faces;
+};
+
+int cell(int dim, int64_t i, const double* pos, const double* side, const luna_voronoi::Grid& grid, CellWork& work,
+         std::vector<CellFace>& faces, double& volume, double* centroid) {
+    const int code = dim == 3 ? luna_voronoi::build_cell<3>(i, pos, side, grid, work.p3, work.faces, volume, centroid)
+                              : luna_voronoi::build_cell<2>(i, pos, side, grid, work.p2, work.faces, volume, centroid);
+    if (code != luna_voronoi::kCellOk) return code;
+    faces.resize(work.faces.n);
+    for (int k = 0; k < work.faces.n; ++k) {
+        const int e = work.faces.order[k];
+        faces[k].j = work.faces.j[e];
+        for (int a = 0; a < 3; ++a) {
+            faces[k].a[a] = work.faces.a[e][a];
+            faces[k].c[a] = work.faces.c[e][a];
         }
     }
-    if (!done) {
-        err = "voronoi: the bucket search ran out of offsets (points too sparse for the grid)";
-        return false;
-    }
-    faces.clear();
-    volume = 0;
-    double cm[3] = {0, 0, 0};
-    if constexpr (std::is_same_v<Poly, Poly3>) {
-        const int nf = static_cast<int>(poly.tag.size());
-        for (int f = 0; f < nf; ++f) {
-            const int a0 = poly.fo[f], m = poly.fo[f + 1] - a0;
-            const V3& p0 = poly.v[poly.idx[a0]];
-            V3 A{0, 0, 0};
-            V3 C{0, 0, 0};
-            double wsum = 0;
-            std::vector<std::pair<V3, V3>> tris;
-            for (int k = 1; k + 1 < m; ++k) {
-                const V3& p1 = poly.v[poly.idx[a0 + k]];
-                const V3& p2 = poly.v[poly.idx[a0 + k + 1]];
-                const V3 t = cross3(sub3(p1, p0), sub3(p2, p0));
-                for (int a = 0; a < 3; ++a) A[a] += 0.5 * t[a];
-                // Tetrahedron (origin, p0, p1, p2): 6 V = p0 . (p1 x p2).
-                const double v6 = dot3(p0, cross3(p1, p2));
-                volume += v6 / 6.0;
-                for (int a = 0; a < 3; ++a) cm[a] += v6 / 6.0 * (p0[a] + p1[a] + p2[a]) / 4.0;
-                tris.push_back({t, {(p0[0] + p1[0] + p2[0]) / 3.0, (p0[1] + p1[1] + p2[1]) / 3.0, (p0[2] + p1[2] + p2[2]) / 3.0}});
-            }
-            const double amag = std::sqrt(dot3(A, A));
-            if (poly.tag[f] < 0) {
-                err = "voronoi: a cell reaches the box (box too small for the points)";
-                return false;
-            }
-            if (poly.tag[f] == i) {
-                err = "voronoi: a cell touches its own periodic image (box too small for the points)";
-                return false;
-            }
-            for (const auto& tr : tris) {
-                const double wgt = amag > 0 ? dot3(tr.first, A) / amag : 0.0;
-                for (int a = 0; a < 3; ++a) C[a] += wgt * tr.second[a];
-                wsum += wgt;
-            }
-            if (wsum > 0)
-                for (int a = 0; a < 3; ++a) C[a] /= wsum;
-            else
-                C = p0;
-            CellFace cf;
-            cf.j = static_cast<int32_t>(poly.tag[f]);
-            for (int a = 0; a < 3; ++a) {
-                cf.a[a] = A[a];
-                cf.c[a] = C[a];
-            }
-            faces.push_back(cf);
-        }
-    } else {
-        const int m = static_cast<int>(poly.v.size());
-        for (int k = 0; k < m; ++k) {
-            const auto& p = poly.v[k];
-            const auto& q = poly.v[(k + 1) % m];
-            const double cr = p[0] * q[1] - p[1] * q[0];
-            volume += 0.5 * cr;
-            cm[0] += cr * (p[0] + q[0]) / 6.0;
-            cm[1] += cr * (p[1] + q[1]) / 6.0;
-            if (poly.tag[k] < 0) {
-                err = "voronoi: a cell reaches the box (box too small for the points)";
-                return false;
-            }
-            if (poly.tag[k] == i) {
-                err = "voronoi: a cell touches its own periodic image (box too small for the points)";
-                return false;
-            }
-            CellFace cf{};
-            cf.j = static_cast<int32_t>(poly.tag[k]);
-            cf.a[0] = q[1] - p[1];
-            cf.a[1] = -(q[0] - p[0]);
-            cf.c[0] = 0.5 * (p[0] + q[0]);
-            cf.c[1] = 0.5 * (p[1] + q[1]);
-            faces.push_back(cf);
-        }
-    }
-    for (int a = 0; a < dim; ++a) centroid[a] = cm[a] / volume;
-    std::sort(faces.begin(), faces.end(), [](const CellFace& p, const CellFace& q) { return p.j < q.j; });
-    for (size_t k = 1; k < faces.size(); ++k)
-        if (faces[k].j == faces[k - 1].j) {
-            err = "voronoi: two faces between the same pair of cells (box too small for unique nearest images)";
-            return false;
-        }
-    return true;
+    return 0;
 }
 
 }  // namespace
@@ -449,15 +141,13 @@ int luna_mesh_create(int dim, int64_t n, const double* points, const double* box
                 delete m;
                 return fail("luna_mesh_create: non-finite point");
             }
-            x -= box[a] * std::floor(x / box[a]);
-            if (x >= box[a]) x -= box[a];
-            m->positions[dim * i + a] = x;
+            m->positions[dim * i + a] = luna_voronoi::wrap_coordinate(x, box[a]);
         }
-    Grid grid;
+    HostGrid grid;
     grid.build(dim, n, m->positions.data(), box);
+    const luna_voronoi::Grid view = grid.view();
     m->volume.resize(n);
     m->centroid.resize(static_cast<size_t>(n) * dim);
-    std::vector<int64_t> count(n + 1, 0);
     // Per cell faces, kept per thread chunk and gathered after.
     std::vector<std::vector<CellFace>> per_cell(n);
     std::string first_error;
@@ -467,20 +157,17 @@ int luna_mesh_create(int dim, int64_t n, const double* points, const double* box
 #endif
 #pragma omp parallel
     {
-        Poly3 p3;
-        Poly2 p2;
+        std::unique_ptr<CellWork> work(new CellWork());
         std::vector<CellFace> faces;
-        std::string err;
 #pragma omp for schedule(dynamic, 256)
         for (int64_t i = 0; i < n; ++i) {
             if (!ok) continue;
             double vol = 0;
-            bool good = dim == 3 ? cell(dim, i, m->positions.data(), box, grid, p3, faces, vol, &m->centroid[dim * i], err)
-                                 : cell(dim, i, m->positions.data(), box, grid, p2, faces, vol, &m->centroid[dim * i], err);
-            if (!good) {
+            const int code = cell(dim, i, m->positions.data(), box, view, *work, faces, vol, &m->centroid[dim * i]);
+            if (code != 0) {
 #pragma omp critical
                 {
-                    if (ok) first_error = err;
+                    if (ok) first_error = cell_error(code);
                     ok = false;
                 }
                 continue;

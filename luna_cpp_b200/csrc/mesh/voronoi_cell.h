@@ -1,0 +1,488 @@
+// One periodic Voronoi cell by half-space clipping, in fixed-capacity storage, for the host builder
+// (voronoi_build.cpp) and the device remesher (remesh.cu) alike. Both compile this one source without floating-point
+// contraction (-ffp-contract=off on the host, -fmad=false on the device) and use only correctly rounded operations
+// (+ - * /, sqrt, floor, nearbyint), so a mesh built on the device has the host builder's bits.
+//
+// A cell starts as the periodic box centred on its generator (its own images bound it there) and is clipped by the
+// bisector plane (2D: line) of every generator image that can still cut it. Candidates come from a bucket grid visited
+// in order of a lower bound on their distance; the walk stops once that bound exceeds twice the largest vertex radius of
+// the cell (no farther generator can cut it).
+#pragma once
+
+#include <cmath>
+#include <cstdint>
+
+#if defined(__CUDACC__)
+#define LUNA_VC_HD __host__ __device__ __forceinline__
+#else
+#define LUNA_VC_HD inline
+#endif
+
+namespace luna_voronoi {
+
+// The storage of a cell is fixed at compile time (the template arguments below): the device remesher's is sized for the
+// cells of gas meshes (a thread's local memory), the host builder's for cells of up to a thousand faces; a cell that
+// outgrows its storage is an error, never a different result.
+
+// Why a cell could not be built (0: it was).
+enum : int {
+    kCellOk = 0,
+    kOutOfOffsets = 1,   // the bucket search ran out of offsets (points too sparse for the grid)
+    kReachesBox = 2,     // a face of the starting box survived: the box is too small for the points
+    kTouchesSelf = 3,    // a face towards the cell's own image
+    kDuplicatePair = 4,  // two faces towards the same cell (no unique nearest images)
+    kCapacity = 5,       // more vertices, faces or loop entries than the storage holds
+};
+
+// The bucket grid: nb buckets of width w per axis, items by bucket (CSR), and the bucket offsets to visit, sorted by a
+// lower bound bound2 on the squared distance of any point in the offset bucket.
+struct Grid {
+    int dim;
+    int nb[3];
+    double w[3];
+    const int64_t* start;
+    const int32_t* items;
+    const int32_t* offsets;  // [n_offsets][3]
+    const double* bound2;    // [n_offsets]
+    int n_offsets;
+};
+
+LUNA_VC_HD int bucket_of(const Grid& g, const double* x, int a) {
+    const int b = static_cast<int>(floor(x[a] / g.w[a]));
+    return b < 0 ? 0 : (b > g.nb[a] - 1 ? g.nb[a] - 1 : b);
+}
+
+LUNA_VC_HD double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+LUNA_VC_HD void cross3(const double* a, const double* b, double* out) {
+    out[0] = a[1] * b[2] - a[2] * b[1];
+    out[1] = a[2] * b[0] - a[0] * b[2];
+    out[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+// A monotone stand-in for the polar angle of (x, y) in [0, 4): the position along the unit diamond |x| + |y| = 1,
+// counter-clockwise from +x. One division, so the host and the device order a face's vertices alike.
+LUNA_VC_HD double diamond_angle(double x, double y) {
+    if (x == 0 && y == 0) return 0;
+    if (y >= 0) return x >= 0 ? y / (x + y) : 1 - x / (y - x);
+    return x < 0 ? 2 + y / (x + y) : 3 + x / (x - y);
+}
+
+// A convex polyhedron around the origin: vertices, and faces as counter-clockwise (seen from outside) vertex loops, each
+// with the neighbour across it (-1: the starting box). Two copies, the current one and the one a clip builds. Room for
+// kMaxVerts vertices, kMaxFaces faces, kMaxLoop loop entries and kMaxCut vertices of one new face.
+template <int kMaxVerts, int kMaxFaces, int kMaxLoop, int kMaxCut>
+struct Poly3T {
+    double v[2][kMaxVerts][3];
+    int idx[2][kMaxLoop];
+    int fo[2][kMaxFaces + 1];  // face offsets into idx
+    int32_t tag[2][kMaxFaces];
+    int nv[2], nf[2];
+    int cur;
+    double s[kMaxVerts];  // signed distances of the vertices to the cutting plane
+    int remap[kMaxVerts];  // old vertex -> new vertex (-1: removed)
+    uint64_t memo_key[kMaxCut];  // the intersection vertex of each cut edge
+    int memo_id[kMaxCut];
+    int nmemo;
+    int cut[kMaxCut];  // vertices of the new face
+    double angle[kMaxCut];
+    int ncut;
+    double eps;
+    bool full;  // a capacity ran out
+
+    LUNA_VC_HD void box(const double* half) {
+        cur = 0;
+        full = false;
+        nv[0] = 8;
+        for (int k = 0; k < 8; ++k) {
+            v[0][k][0] = (k & 1) ? half[0] : -half[0];
+            v[0][k][1] = (k & 2) ? half[1] : -half[1];
+            v[0][k][2] = (k & 4) ? half[2] : -half[2];
+        }
+        // faces counter-clockwise seen from outside: -x, +x, -y, +y, -z, +z
+        const int loops[6][4] = {{0, 4, 6, 2}, {1, 3, 7, 5}, {0, 1, 5, 4}, {2, 6, 7, 3}, {0, 2, 3, 1}, {4, 5, 7, 6}};
+        nf[0] = 6;
+        fo[0][0] = 0;
+        for (int f = 0; f < 6; ++f) {
+            for (int k = 0; k < 4; ++k) idx[0][4 * f + k] = loops[f][k];
+            fo[0][f + 1] = 4 * f + 4;
+            tag[0][f] = -1;
+        }
+    }
+    LUNA_VC_HD double max_radius2() const {
+        double r = 0;
+        for (int k = 0; k < nv[cur]; ++k) {
+            const double d = dot3(v[cur][k], v[cur][k]);
+            r = d > r ? d : r;
+        }
+        return r;
+    }
+    // The new vertex on the edge a-b (each cut edge once).
+    LUNA_VC_HD int memo(int a, int b) {
+        const uint64_t key = a < b ? (uint64_t(a) << 32 | uint32_t(b)) : (uint64_t(b) << 32 | uint32_t(a));
+        for (int k = 0; k < nmemo; ++k)
+            if (memo_key[k] == key) return memo_id[k];
+        const int o = cur, n = cur ^ 1;
+        if (nv[n] >= kMaxVerts || nmemo >= kMaxCut || ncut >= kMaxCut) {
+            full = true;
+            return 0;
+        }
+        const double t = s[a] / (s[a] - s[b]);
+        const double* p = v[o][a];
+        const double* q = v[o][b];
+        const int id = nv[n]++;
+        v[n][id][0] = p[0] + t * (q[0] - p[0]);
+        v[n][id][1] = p[1] + t * (q[1] - p[1]);
+        v[n][id][2] = p[2] + t * (q[2] - p[2]);
+        memo_key[nmemo] = key;
+        memo_id[nmemo++] = id;
+        cut[ncut++] = id;
+        return id;
+    }
+    // Keeps {y : n.y <= c}; the new face gets tag t. Returns whether anything was cut.
+    LUNA_VC_HD bool clip(const double* nrm, double c, int32_t t) {
+        const int o = cur, n = cur ^ 1;
+        const int nvert = nv[o];
+        double smax = -1e300;
+        for (int k = 0; k < nvert; ++k) {
+            s[k] = dot3(nrm, v[o][k]) - c;
+            smax = s[k] > smax ? s[k] : smax;
+        }
+        if (smax <= eps) return false;
+        nv[n] = 0;
+        nmemo = 0;
+        ncut = 0;
+        for (int k = 0; k < nvert; ++k) {
+            remap[k] = -1;
+            if (s[k] <= eps) {
+                remap[k] = nv[n];
+                v[n][nv[n]][0] = v[o][k][0];
+                v[n][nv[n]][1] = v[o][k][1];
+                v[n][nv[n]][2] = v[o][k][2];
+                if (s[k] >= -eps) {
+                    if (ncut >= kMaxCut) {
+                        full = true;
+                        return false;
+                    }
+                    cut[ncut++] = nv[n];
+                }
+                ++nv[n];
+            }
+        }
+        int li = 0, fi = 0;
+        fo[n][0] = 0;
+        for (int f = 0; f < nf[o]; ++f) {
+            const int a0 = fo[o][f], m = fo[o][f + 1] - fo[o][f];
+            const int begin = li;
+            for (int k = 0; k < m; ++k) {
+                const int a = idx[o][a0 + k], b = idx[o][a0 + (k + 1) % m];
+                if (li + 2 > kMaxLoop) {
+                    full = true;
+                    return false;
+                }
+                if (s[a] <= eps) idx[n][li++] = remap[a];
+                if ((s[a] < -eps && s[b] > eps) || (s[a] > eps && s[b] < -eps)) {
+                    const int id = memo(a, b);
+                    if (full) return false;
+                    idx[n][li++] = id;
+                }
+            }
+            if (li - begin >= 3) {
+                if (fi >= kMaxFaces) {
+                    full = true;
+                    return false;
+                }
+                tag[n][fi] = tag[o][f];
+                fo[n][++fi] = li;
+            } else {
+                li = begin;
+            }
+        }
+        // The new face: the cut vertices (sorted, once each) ordered counter-clockwise about nrm (outward) around their
+        // mean, by diamond angle, then by vertex.
+        for (int k = 1; k < ncut; ++k) {
+            const int x = cut[k];
+            int j = k - 1;
+            while (j >= 0 && cut[j] > x) {
+                cut[j + 1] = cut[j];
+                --j;
+            }
+            cut[j + 1] = x;
+        }
+        int unique = 0;
+        for (int k = 0; k < ncut; ++k)
+            if (unique == 0 || cut[unique - 1] != cut[k]) cut[unique++] = cut[k];
+        ncut = unique;
+        if (ncut >= 3) {
+            double mean[3] = {0, 0, 0};
+            for (int k = 0; k < ncut; ++k)
+                for (int a = 0; a < 3; ++a) mean[a] += v[n][cut[k]][a];
+            for (int a = 0; a < 3; ++a) mean[a] /= static_cast<double>(ncut);
+            double u[3] = {0, 0, 0};
+            u[fabs(nrm[0]) < 0.6 ? 0 : 1] = 1;
+            const double un = dot3(u, nrm);
+            for (int a = 0; a < 3; ++a) u[a] = u[a] - un * nrm[a];
+            const double ul = sqrt(dot3(u, u));
+            for (int a = 0; a < 3; ++a) u[a] = u[a] / ul;
+            double w[3];
+            cross3(nrm, u, w);
+            for (int k = 0; k < ncut; ++k) {
+                const double* p = v[n][cut[k]];
+                const double d[3] = {p[0] - mean[0], p[1] - mean[1], p[2] - mean[2]};
+                angle[k] = diamond_angle(dot3(d, u), dot3(d, w));
+            }
+            for (int k = 1; k < ncut; ++k) {  // by angle, then by vertex (cut is sorted by vertex: a stable sort)
+                const int x = cut[k];
+                const double ax = angle[k];
+                int j = k - 1;
+                while (j >= 0 && angle[j] > ax) {
+                    cut[j + 1] = cut[j];
+                    angle[j + 1] = angle[j];
+                    --j;
+                }
+                cut[j + 1] = x;
+                angle[j + 1] = ax;
+            }
+            if (fi >= kMaxFaces || li + ncut > kMaxLoop) {
+                full = true;
+                return false;
+            }
+            for (int k = 0; k < ncut; ++k) idx[n][li++] = cut[k];
+            tag[n][fi] = t;
+            fo[n][++fi] = li;
+        }
+        nf[n] = fi;
+        cur = n;
+        return true;
+    }
+};
+
+// A convex polygon around the origin, counter-clockwise, with the neighbour across the edge leaving each vertex; room
+// for kMaxFaces vertices.
+template <int kMaxFaces>
+struct Poly2T {
+    double v[2][kMaxFaces][2];
+    int32_t tag[2][kMaxFaces];
+    int nv[2];
+    int cur;
+    double s[kMaxFaces];
+    double eps;
+    bool full;
+
+    LUNA_VC_HD void box(const double* half) {
+        cur = 0;
+        full = false;
+        nv[0] = 4;
+        const double x[4] = {-half[0], half[0], half[0], -half[0]}, y[4] = {-half[1], -half[1], half[1], half[1]};
+        for (int k = 0; k < 4; ++k) {
+            v[0][k][0] = x[k];
+            v[0][k][1] = y[k];
+            tag[0][k] = -1;
+        }
+    }
+    LUNA_VC_HD double max_radius2() const {
+        double r = 0;
+        for (int k = 0; k < nv[cur]; ++k) {
+            const double d = v[cur][k][0] * v[cur][k][0] + v[cur][k][1] * v[cur][k][1];
+            r = d > r ? d : r;
+        }
+        return r;
+    }
+    LUNA_VC_HD bool clip(const double* nrm, double c, int32_t t) {
+        const int o = cur, n = cur ^ 1;
+        const int m = nv[o];
+        double smax = -1e300;
+        for (int k = 0; k < m; ++k) {
+            s[k] = nrm[0] * v[o][k][0] + nrm[1] * v[o][k][1] - c;
+            smax = s[k] > smax ? s[k] : smax;
+        }
+        if (smax <= eps) return false;
+        int q = 0;
+        for (int k = 0; k < m; ++k) {
+            const int b = (k + 1) % m;
+            const bool ain = s[k] <= eps, bin = s[b] <= eps;
+            if (q + 2 > kMaxFaces) {
+                full = true;
+                return false;
+            }
+            if (ain) {
+                v[n][q][0] = v[o][k][0];
+                v[n][q][1] = v[o][k][1];
+                // The edge k -> b stays (tag k) if b is inside; if b is outside the edge is cut, and continues to the
+                // exit point with tag k.
+                tag[n][q++] = tag[o][k];
+                if (!bin && s[k] < -eps) {
+                    const double u = s[k] / (s[k] - s[b]);
+                    v[n][q][0] = v[o][k][0] + u * (v[o][b][0] - v[o][k][0]);
+                    v[n][q][1] = v[o][k][1] + u * (v[o][b][1] - v[o][k][1]);
+                    tag[n][q++] = t;  // from the exit point along the cut
+                } else if (!bin) {
+                    tag[n][q - 1] = t;  // k sits on the line: the cut starts here
+                }
+            } else if (bin && s[b] < -eps) {
+                const double u = s[k] / (s[k] - s[b]);
+                v[n][q][0] = v[o][k][0] + u * (v[o][b][0] - v[o][k][0]);
+                v[n][q][1] = v[o][k][1] + u * (v[o][b][1] - v[o][k][1]);
+                tag[n][q++] = tag[o][k];  // entry point, then along edge k to b
+            }
+        }
+        nv[n] = q;
+        cur = n;
+        return true;
+    }
+};
+
+// The faces of one built cell, by neighbour: area vector out of the cell, centroid relative to the cell's generator.
+template <int kMaxFaces>
+struct CellFacesT {
+    int32_t j[kMaxFaces];
+    double a[kMaxFaces][3];
+    double c[kMaxFaces][3];
+    int order[kMaxFaces];  // faces by neighbour
+    int n;
+};
+
+// Cell i of the points pos [n][dim] (wrapped into [0, side)): clipped, then its faces (out.order by neighbour), volume
+// and centroid relative to the generator. Returns kCellOk or why the cell could not be built.
+template <int D, class Poly, class Faces>
+LUNA_VC_HD int build_cell(int64_t i, const double* pos, const double* side, const Grid& grid, Poly& poly, Faces& out,
+                          double& volume, double* centroid) {
+    const double* xi = pos + D * i;
+    double half[3] = {0, 0, 0};
+    double scale = 0;
+    for (int a = 0; a < D; ++a) {
+        half[a] = 0.5 * side[a];
+        scale = side[a] > scale ? side[a] : scale;
+    }
+    poly.box(half);
+    poly.eps = 1e-13 * scale;
+    int bi[3] = {0, 0, 0};
+    for (int a = 0; a < D; ++a) bi[a] = bucket_of(grid, xi, a);
+    double rmax2 = poly.max_radius2();
+    bool done = false;
+    for (int k = 0; k < grid.n_offsets; ++k) {
+        if (grid.bound2[k] > 4.0 * rmax2) {
+            done = true;
+            break;
+        }
+        const int32_t* o = grid.offsets + 3 * k;
+        int64_t b = 0;
+        double shift[3] = {0, 0, 0};
+        for (int a = 0; a < D; ++a) {
+            const int t = bi[a] + o[a];
+            const int tw = ((t % grid.nb[a]) + grid.nb[a]) % grid.nb[a];
+            shift[a] = static_cast<double>((t - tw) / grid.nb[a]) * side[a];
+            b = b * grid.nb[a] + tw;
+        }
+        for (int64_t q = grid.start[b]; q < grid.start[b + 1]; ++q) {
+            const int32_t j = grid.items[q];
+            double d[3] = {0, 0, 0};
+            double d2 = 0;
+            for (int a = 0; a < D; ++a) {
+                d[a] = pos[D * j + a] + shift[a] - xi[a];
+                d2 += d[a] * d[a];
+            }
+            if (d2 == 0) continue;  // the generator itself
+            if (d2 > 4.0 * rmax2) continue;
+            const double inv = 1.0 / sqrt(d2);
+            const double nrm[3] = {d[0] * inv, d[1] * inv, d[2] * inv};
+            if (poly.clip(nrm, 0.5 * d2 * inv, j)) rmax2 = poly.max_radius2();
+            if (poly.full) return kCapacity;
+        }
+    }
+    if (!done) return kOutOfOffsets;
+    out.n = 0;
+    volume = 0;
+    double cm[3] = {0, 0, 0};
+    if constexpr (D == 3) {
+        const int c = poly.cur;
+        for (int f = 0; f < poly.nf[c]; ++f) {
+            const int a0 = poly.fo[c][f], m = poly.fo[c][f + 1] - a0;
+            if (poly.tag[c][f] < 0) return kReachesBox;
+            if (poly.tag[c][f] == i) return kTouchesSelf;
+            const double* p0 = poly.v[c][poly.idx[c][a0]];
+            double A[3] = {0, 0, 0};
+            for (int k = 1; k + 1 < m; ++k) {
+                const double* p1 = poly.v[c][poly.idx[c][a0 + k]];
+                const double* p2 = poly.v[c][poly.idx[c][a0 + k + 1]];
+                const double e1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+                const double e2[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
+                double t[3], x12[3];
+                cross3(e1, e2, t);
+                for (int a = 0; a < 3; ++a) A[a] += 0.5 * t[a];
+                // tetrahedron (origin, p0, p1, p2): 6 V = p0 . (p1 x p2)
+                cross3(p1, p2, x12);
+                const double v6 = dot3(p0, x12);
+                volume += v6 / 6.0;
+                for (int a = 0; a < 3; ++a) cm[a] += v6 / 6.0 * (p0[a] + p1[a] + p2[a]) / 4.0;
+            }
+            // the face centroid: its triangles' centroids weighted by their areas along the face normal
+            const double amag = sqrt(dot3(A, A));
+            double C[3] = {0, 0, 0};
+            double wsum = 0;
+            for (int k = 1; k + 1 < m; ++k) {
+                const double* p1 = poly.v[c][poly.idx[c][a0 + k]];
+                const double* p2 = poly.v[c][poly.idx[c][a0 + k + 1]];
+                const double e1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+                const double e2[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
+                double t[3];
+                cross3(e1, e2, t);
+                const double wgt = amag > 0 ? dot3(t, A) / amag : 0.0;
+                for (int a = 0; a < 3; ++a) C[a] += wgt * ((p0[a] + p1[a] + p2[a]) / 3.0);
+                wsum += wgt;
+            }
+            if (wsum > 0)
+                for (int a = 0; a < 3; ++a) C[a] /= wsum;
+            else
+                for (int a = 0; a < 3; ++a) C[a] = p0[a];
+            const int e = out.n++;
+            out.j[e] = poly.tag[c][f];
+            for (int a = 0; a < 3; ++a) {
+                out.a[e][a] = A[a];
+                out.c[e][a] = C[a];
+            }
+        }
+    } else {
+        const int c = poly.cur, m = poly.nv[c];
+        for (int k = 0; k < m; ++k) {
+            const double* p = poly.v[c][k];
+            const double* q = poly.v[c][(k + 1) % m];
+            const double cr = p[0] * q[1] - p[1] * q[0];
+            volume += 0.5 * cr;
+            cm[0] += cr * (p[0] + q[0]) / 6.0;
+            cm[1] += cr * (p[1] + q[1]) / 6.0;
+            if (poly.tag[c][k] < 0) return kReachesBox;
+            if (poly.tag[c][k] == i) return kTouchesSelf;
+            const int e = out.n++;
+            out.j[e] = poly.tag[c][k];
+            out.a[e][0] = q[1] - p[1];
+            out.a[e][1] = -(q[0] - p[0]);
+            out.a[e][2] = 0;
+            out.c[e][0] = 0.5 * (p[0] + q[0]);
+            out.c[e][1] = 0.5 * (p[1] + q[1]);
+            out.c[e][2] = 0;
+        }
+    }
+    for (int a = 0; a < D; ++a) centroid[a] = cm[a] / volume;
+    for (int k = 0; k < out.n; ++k) {
+        const int x = k;
+        int j = k - 1;
+        while (j >= 0 && out.j[out.order[j]] > out.j[x]) {
+            out.order[j + 1] = out.order[j];
+            --j;
+        }
+        out.order[j + 1] = x;
+    }
+    for (int k = 1; k < out.n; ++k)
+        if (out.j[out.order[k]] == out.j[out.order[k - 1]]) return kDuplicatePair;
+    return kCellOk;
+}
+
+// The device remesher's storage (about 18 KB a thread in 3D) and the host builder's.
+using Poly3 = Poly3T<128, 64, 512, 64>;
+using Poly2 = Poly2T<64>;
+using CellFaces = CellFacesT<64>;
+using HostPoly3 = Poly3T<2048, 1024, 8192, 1024>;
+using HostPoly2 = Poly2T<4096>;
+using HostCellFaces = CellFacesT<4096>;
+
+}  // namespace luna_voronoi

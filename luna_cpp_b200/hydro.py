@@ -100,6 +100,12 @@ SIGNATURES = {
     "luna_line_time_step": ([P, D64, I, P], I),
     "luna_line_step": ([P, P], I),
     "luna_line_step_and_time_step": ([P, P, D64, P], I),
+    "luna_remesh_create": ([I, P, P], I),
+    "luna_remesh_destroy": ([P], I),
+    "luna_remesh_set_stream": ([P, P], I),
+    "luna_remesh_points": ([P, I64, P], I),
+    "luna_remesh_build": ([P, I64, P, I, P, P], I),
+    "luna_remesh_device_bytes": ([P, P], I),
 }
 
 PHASES = ("primitives", "sweep", "fluxes", "update", "drift")
@@ -127,7 +133,10 @@ def check(status: int):
 
 
 def mesh_desc(mesh, keep: list) -> MeshDesc:
-    """A luna_mesh_desc over the host arrays of a luna_cpp_b200.mesh.Mesh (kept alive through ``keep``)."""
+    """A luna_mesh_desc over the host arrays of a luna_cpp_b200.mesh.Mesh (kept alive through ``keep``), or the device
+    descriptor of a luna_cpp_b200.remesh.DeviceMesh."""
+    if isinstance(getattr(mesh, "desc", None), MeshDesc):
+        return mesh.desc
     arrays = [np.ascontiguousarray(mesh.owner, dtype=np.int32), np.ascontiguousarray(mesh.neighbour, dtype=np.int32),
               np.ascontiguousarray(mesh.cell_face_start, dtype=np.int32),
               np.ascontiguousarray(mesh.cell_face, dtype=np.int32), np.ascontiguousarray(mesh.area, dtype=np.float64),
@@ -243,6 +252,17 @@ class FiniteVolume:
         keep: list = []
         desc = mesh_desc(new_mesh, keep)
         check(lib().luna_fv_step_moving_end(self._h, ctypes.byref(desc)))
+        self.mesh = new_mesh
+        return new_mesh
+
+    def step_moving_device(self, dt: float, remesher) -> object:
+        """One moving step with the generators and the mesh on the device: the t^n fluxes, the drift into the
+        remesher's buffer, ``remesher``'s device remesh (luna_cpp_b200.remesh.Remesher), the t^n+1 fluxes. Returns the
+        new DeviceMesh."""
+        ptr = remesher.points_buffer(self.n)
+        check(lib().luna_fv_step_moving_begin(self._h, dt, ptr, 1))
+        new_mesh = remesher.build_device(ptr, self.n)
+        check(lib().luna_fv_step_moving_end(self._h, ctypes.byref(new_mesh.desc)))
         self.mesh = new_mesh
         return new_mesh
 

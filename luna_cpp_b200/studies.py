@@ -29,6 +29,7 @@ comparisons of the same configurations are GPU tests).
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import time
 
@@ -36,6 +37,7 @@ import numpy as np
 
 from . import hydro
 from .mesh import build_mesh, jittered_points
+from .remesh import Remesher
 from .problems import acoustic_wave, cell_centres, conserved, point_blast
 
 GAMMA = 5.0 / 3.0
@@ -118,56 +120,92 @@ def snapped_jittered_mesh(nx, dim=3, seed=1, threads=0):
     return build_mesh(pts, threads=threads)
 
 
-def run_moving(fv, t_end, courant=0.3, threads=0, max_steps=100000, log=print):
-    """Moving steps to t_end (the last step shortened); returns (steps, t, hydro ms, remesh s)."""
-    t, steps, remesh_s = 0.0, 0, 0.0
-
-    def remesh(pos):
-        nonlocal remesh_s
-        t0 = time.perf_counter()
-        m = build_mesh(pos, threads=threads)
-        remesh_s += time.perf_counter() - t0
-        return m
-
+def run_moving(fv, t_end, courant=0.3, threads=0, max_steps=100000, remesher=None, log=print) -> dict:
+    """Moving steps to t_end (the last step shortened). With ``remesher`` (luna_cpp_b200.remesh.Remesher) the
+    generators and the mesh stay on the device; otherwise the host builder remeshes. Returns the steps, t, the hydro
+    kernels' device ms, and the wall seconds of the remesh, of taking the new mesh (tiles and geometry rows) and of the
+    whole steps."""
+    t, steps, remesh_s, load_s = 0.0, 0, 0.0, 0.0
     fv.set_timing(True)
     fv.timings()
+    lib = hydro.lib()
+    wall0 = time.perf_counter()
     while t < t_end and steps < max_steps:
         dt = min(fv.time_step(courant), t_end - t)
-        fv.step_moving(dt, remesh)
+        if remesher is None:
+            pos = np.empty((fv.n, fv.dim), dtype=np.float64)
+            hydro.check(lib.luna_fv_step_moving_begin(fv.handle, dt, pos.ctypes.data, 0))
+            t0 = time.perf_counter()
+            mesh = build_mesh(pos, box=fv.mesh.box, threads=threads)
+            t1 = time.perf_counter()
+            keep: list = []
+            hydro.check(lib.luna_fv_step_moving_end(fv.handle, ctypes.byref(hydro.mesh_desc(mesh, keep))))
+        else:
+            ptr = remesher.points_buffer(fv.n)
+            hydro.check(lib.luna_fv_step_moving_begin(fv.handle, dt, ptr, 1))
+            t0 = time.perf_counter()
+            mesh = remesher.build_device(ptr, fv.n)
+            t1 = time.perf_counter()
+            hydro.check(lib.luna_fv_step_moving_end(fv.handle, ctypes.byref(mesh.desc)))
+        load_s += time.perf_counter() - t1
+        remesh_s += t1 - t0
+        fv.mesh = mesh
         t += dt
         steps += 1
-    return steps, t, _phases_ms(fv), remesh_s
+    hydro_ms = _phases_ms(fv)  # synchronises
+    wall = time.perf_counter() - wall0
+    return {"steps": steps, "t": t, "hydro_device_ms": hydro_ms, "remesh_s": remesh_s, "mesh_load_s": load_s, "wall_s": wall}
 
 
-def moving(nx=32, t_end=0.05, precision_policy="fp32", timed_nx=128, timed_steps=5, courant=0.3, threads=0, log=print) -> dict:
+def _moving_run(nx, t_end, precision_policy, courant, threads, remesh, max_steps, log):
+    """The moving point blast on nx^3 snapped jittered generators; the initial mesh built where the remesh runs."""
+    step = 2.0 ** -30
+    pts = np.round(jittered_points((nx, nx, nx), jitter=0.1, seed=1) / step) * step
+    remesher = Remesher(3, (1.0, 1.0, 1.0)) if remesh == "device" else None
     t0 = time.time()
-    mesh = snapped_jittered_mesh(nx, threads=threads)
-    log(f"mesh {nx}^3: {mesh.n_cells} cells, {time.time() - t0:.1f} s")
-    q0 = point_blast(mesh, GAMMA)
-    out = {"config": {"cells": mesh.n_cells, "t_end": t_end, "precision": precision_policy, "courant": courant,
-                      "problem": "point blast, E = 1 within 2 cell widths, moving mesh"}}
+    if remesher is not None:
+        mesh = remesher.build(pts)
+        cells = mesh.cells()
+    else:
+        mesh = cells = build_mesh(pts, threads=threads)
+    log(f"mesh {nx}^3 ({remesh}): {time.time() - t0:.1f} s")
+    q0 = point_blast(cells, GAMMA)
     fv = hydro.FiniteVolume(mesh, precision=precision_policy, motion="moving")
     fv.set_state(q0)
-    steps, t, hydro_ms, remesh_s = run_moving(fv, t_end, courant, threads, log=log)
+    run = run_moving(fv, t_end, courant, threads, max_steps=max_steps, remesher=remesher, log=log)
     q = fv.get_state()
-    out["run"] = {"steps": steps, "t": t, "hydro_device_ms": hydro_ms, "remesh_host_s": remesh_s,
-                  "hydro_cell_updates_per_s": mesh.n_cells * steps / (hydro_ms * 1e-3),
-                  "mass_drift": float(abs(q[:, 0].sum() - q0[:, 0].sum()) / q0[:, 0].sum()),
-                  "energy_drift": float(abs(q[:, 4].sum() - q0[:, 4].sum()) / q0[:, 4].sum()),
-                  "radial_density_profile": radial_profile(fv.mesh, q).tolist()}
-    log(f"moving {nx}^3 to t = {t:.4f}: {steps} steps, hydro {hydro_ms:.1f} ms, remesh {remesh_s:.1f} s")
+    final = fv.mesh.cells() if remesher is not None else fv.mesh
+    N, n = cells.n_cells, run["steps"]
+    out = {"cells": N, "remesh": remesh, **run,
+           "hydro_ms_per_step": run["hydro_device_ms"] / n, "remesh_ms_per_step": 1e3 * run["remesh_s"] / n,
+           "mesh_load_ms_per_step": 1e3 * run["mesh_load_s"] / n, "step_wall_ms": 1e3 * run["wall_s"] / n,
+           "hydro_cell_updates_per_s": N * n / (run["hydro_device_ms"] * 1e-3),
+           "cell_updates_per_s": N * n / run["wall_s"],
+           "mass_drift": float(abs(q[:, 0].sum() - q0[:, 0].sum()) / q0[:, 0].sum()),
+           "energy_drift": float(abs(q[:, 4].sum() - q0[:, 4].sum()) / q0[:, 4].sum()),
+           "radial_density_profile": radial_profile(final, q).tolist()}
+    log(f"moving {nx}^3 to t = {run['t']:.4f}: {n} steps; a step: hydro {out['hydro_ms_per_step']:.2f} ms (device), remesh "
+        f"{out['remesh_ms_per_step']:.1f} ms, mesh load {out['mesh_load_ms_per_step']:.1f} ms, whole {out['step_wall_ms']:.1f} ms")
     fv.close()
-    if timed_steps > 0:
-        t0 = time.time()
-        big = snapped_jittered_mesh(timed_nx, threads=threads)
-        log(f"mesh {timed_nx}^3: {time.time() - t0:.1f} s")
-        fv = hydro.FiniteVolume(big, precision=precision_policy, motion="moving")
-        fv.set_state(point_blast(big, GAMMA))
-        steps, t, hydro_ms, remesh_s = run_moving(fv, 1.0, courant, threads, max_steps=timed_steps, log=log)
-        out["timed"] = {"cells": big.n_cells, "steps": steps, "hydro_device_ms_per_step": hydro_ms / steps,
-                        "hydro_cell_updates_per_s": big.n_cells * steps / (hydro_ms * 1e-3), "remesh_host_s_per_step": remesh_s / steps}
-        log(f"moving {timed_nx}^3: {hydro_ms / steps:.3f} ms/step hydro, remesh {remesh_s / steps:.1f} s/step")
-        fv.close()
+    if remesher is not None:
+        remesher.close()
+    return out
+
+
+def moving(nx=32, t_end=0.05, precision_policy="fp32", scale_nx=(128, 256), scale_steps=(0, 10), courant=0.3, threads=0,
+           remesh="device", log=print) -> dict:
+    """The moving-mesh configuration: the point blast on snapped jittered generators, generators moved with the gas plus
+    AREPO's roundness velocity, fluxes on the old and the new faces, FP64 state with FP32 face arithmetic
+    (riemann32). nx^3 runs to t_end; each of ``scale_nx`` runs to t_end (steps 0) or for that many steps. With remesh
+    "device" the generators and the meshes stay on the GPU (luna_cpp_b200.remesh); "host" remeshes with the host
+    builder."""
+    out = {"config": {"t_end": t_end, "precision": precision_policy, "courant": courant, "remesh": remesh,
+                      "problem": "point blast, E = 1 within 2 cell widths, moving mesh"}}
+    out["run"] = _moving_run(nx, t_end, precision_policy, courant, threads, remesh, 100000, log)
+    out["scale"] = []
+    for big, steps in zip(scale_nx, scale_steps):
+        out["scale"].append(_moving_run(big, t_end if steps == 0 else 1.0, precision_policy, courant, threads, remesh,
+                                        100000 if steps == 0 else steps, log))
     return out
 
 
@@ -381,9 +419,15 @@ def main():
     ap.add_argument("--nx", type=int)
     ap.add_argument("--steps", type=int)
     ap.add_argument("--threads", type=int, default=0)
+    ap.add_argument("--remesh", choices=["device", "host"], help="moving: where the mesh is rebuilt (default device)")
+    ap.add_argument("--scale-steps", help="moving: steps at 128^3,256^3 (0: to t_end), e.g. 0,10")
     ap.add_argument("--out")
     args = ap.parse_args()
     kw = {"threads": args.threads}
+    if args.study == "moving" and args.remesh:
+        kw["remesh"] = args.remesh
+    if args.study == "moving" and args.scale_steps:
+        kw["scale_steps"] = tuple(int(x) for x in args.scale_steps.split(","))
     if args.nx:
         kw["nx"] = args.nx
     if args.steps:
