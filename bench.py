@@ -40,6 +40,8 @@ def parse():
     ap.add_argument("--cpu-sample-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="leave out the learned limiter's section")
+    ap.add_argument("--no-moving", action="store_true", help="leave out the moving-mesh section")
+    ap.add_argument("--moving-steps", type=int, default=5)
     ap.add_argument("--curve", default="row", choices=["row", "morton", "hilbert"],
                     help="the cells' numbering along a space-filling curve (voronoi-cpp's Layout::curve)")
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "fp32", "grad16"],
@@ -243,6 +245,37 @@ def learned_section(mesh, q0, steps, warmup, stream, torch) -> dict:
                                "plain_resolution_of_equal_error": summary["plain_resolution_of_equal_error"]}}
 
 
+def moving_section(nx, steps, warmup) -> dict:
+    """The moving-mesh configuration's step at nx^3 (the point blast on snapped jittered generators, generators moved with
+    the gas plus the roundness velocity, fluxes on the old and the new faces, FP32 face arithmetic with FP64 state:
+    riemann32), with the mesh rebuilt on the GPU every step: the hydro part's device time (CUDA events around the
+    hydro kernels, the geometry rows of the new mesh included; the remesh outside, as the reference's hydro part) and
+    the whole step's wall time (remesh and taking the new mesh included), after ``warmup`` steps."""
+    from luna_cpp_b200 import hydro
+    from luna_cpp_b200.mesh import jittered_points
+    from luna_cpp_b200.problems import point_blast
+    from luna_cpp_b200.remesh import Remesher
+    from luna_cpp_b200.studies import run_moving
+
+    grid = 2.0 ** -30
+    pts = np.round(jittered_points((nx, nx, nx), jitter=0.1, seed=1) / grid) * grid
+    remesher = Remesher(3, (1.0, 1.0, 1.0))
+    mesh = remesher.build(pts)
+    fv = hydro.FiniteVolume(mesh, precision="fp32", motion="moving")
+    fv.set_state(point_blast(mesh.cells()))
+    run_moving(fv, 1.0, max_steps=warmup, remesher=remesher)
+    r = run_moving(fv, 1.0, max_steps=steps, remesher=remesher)
+    N, n = mesh.n_cells, r["steps"]
+    out = {"workload": f"3D moving point blast {nx}^3 jittered (0.1), riemann32, CFL 0.3, remesh on the GPU every step",
+           "steps": n, "warmup": warmup, "hydro_ms_per_step": r["hydro_device_ms"] / n,
+           "hydro_cell_updates_per_s": N * n / (r["hydro_device_ms"] * 1e-3),
+           "remesh_ms_per_step": 1e3 * r["remesh_s"] / n, "mesh_load_ms_per_step": 1e3 * r["mesh_load_s"] / n,
+           "step_ms": 1e3 * r["wall_s"] / n, "cell_updates_per_s": N * n / r["wall_s"]}
+    fv.close()
+    remesher.close()
+    return out
+
+
 def timed_steps(fv, steps, torch):
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
@@ -388,6 +421,8 @@ def main():
         }
         if world == 1 and not args.no_learned:
             line["learned_limiter"] = learned_section(mesh, q0, args.steps, args.warmup, stream, torch)
+        if world == 1 and not args.no_moving:
+            line["moving"] = moving_section(args.nx, args.moving_steps, 2)
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(mesh, q0, args.cpu_sample_steps, os.cpu_count() or 1)
         print(json.dumps(line), flush=True)

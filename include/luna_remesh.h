@@ -35,7 +35,7 @@ LUNA_API luna_status luna_remesh_points(luna_remesh* r, int64_t n, double** poin
  * *mesh holds device pointers owned by r (valid until the next build or luna_remesh_destroy) and *inconsistent the
  * faces seen from one side only (kept from the side that saw them, as luna_mesh_create keeps them). Synchronises on
  * r's stream (the face count is read back). Errors: LUNA_EINVAL for n out of [2, 2^30), a non-finite point or a cell
- * that cannot be built (box too small for the points, points too sparse for the bucket search, more than 64 faces).
+ * that cannot be built (box too small for the points, points too sparse for the bucket search, a cell of more than 48 faces).
  */
 LUNA_API luna_status luna_remesh_build(luna_remesh* r, int64_t n, const double* points, int on_device, luna_mesh_desc* mesh,
                                        int64_t* inconsistent);

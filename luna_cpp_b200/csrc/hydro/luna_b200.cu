@@ -272,7 +272,11 @@ luna_status finish_geometry(luna_fv* fv, size_t slots) {
     LUNA_TRY(fv->geo_reach2.alloc(N, "cell reach"));
     const int64_t threads = fv->tiles * luna::kTileCells;
     if (threads > 0) {
+        // timed with the sweep: the fit's operator rows, which the reference's sweep forms every step (a moving mesh
+        // forms them every step here too)
+        const long timed_ = fv->open_timed(1);
         luna::k_geometry<D, G><<<blocks(threads, 128), 128, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->geometry_dev<D, G>());
+        fv->close_timed(timed_);
         LUNA_CUDA(cudaGetLastError());
     }
     // The host vectors' contents (host tiles) must outlive the asynchronous uploads.

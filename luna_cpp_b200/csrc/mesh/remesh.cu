@@ -78,6 +78,7 @@ struct Counters {
     int error;                        // the first cell error (voronoi_cell.h), 0: none
     int error_cell;
     int nonfinite;                    // a generator coordinate was not finite
+    unsigned int retry;               // cells the fast path handed to the far search
 };
 
 struct Box {
@@ -144,20 +145,28 @@ struct CellOut {
     unsigned long long capacity;
 };
 
-template <int D>
-__global__ void __launch_bounds__(128) k_cells(int64_t n, const double* __restrict__ pos, Box box, Grid g, CellOut out,
-                                               Counters* c) {
-    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-    if (i >= n) return;
+// The cells (all of them, or those of the list), each built by one thread. Without Far, a cell whose search would
+// pass the grid's sorted offsets or fill the candidate store is put on the retry list for the Far pass (the same cell
+// either way, voronoi_cell.h), which keeps the common cell's code small.
+template <int D, bool Far>
+__global__ void __launch_bounds__(128) k_cells(int64_t n, const int32_t* __restrict__ list, const double* __restrict__ pos, Box box, Grid g,
+                                               CellOut out, Counters* c, int32_t* __restrict__ retry) {
+    const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (k >= n) return;
+    const int64_t i = list ? list[k] : k;
     using Poly = std::conditional_t<D == 3, Poly3, Poly2>;
     Poly poly;
     CellFaces faces;
+    Candidates cand;
     double volume = 0, centroid[3] = {0, 0, 0};
-    const int code = build_cell<D>(i, pos, box.s, g, poly, faces, volume, centroid);
+    const int code = build_cell<D, Far>(i, pos, box.s, g, poly, faces, cand, volume, centroid);
     if (code != kCellOk) {
-        if (atomicCAS(&c->error, 0, code) == 0) c->error_cell = static_cast<int>(i);
         out.first[i] = 0;
         out.count[i] = 0;
+        if (!Far && (code == kOutOfOffsets || code == kCandidates))
+            retry[atomicAdd(&c->retry, 1u)] = static_cast<int32_t>(i);
+        else if (atomicCAS(&c->error, 0, code) == 0)
+            c->error_cell = static_cast<int>(i);
         return;
     }
     out.volume[i] = volume;
@@ -166,13 +175,13 @@ __global__ void __launch_bounds__(128) k_cells(int64_t n, const double* __restri
     out.first[i] = static_cast<int64_t>(base);
     out.count[i] = faces.n;
     if (base + faces.n > out.capacity) return;  // the host grows the buffer and runs the cells again
-    for (int k = 0; k < faces.n; ++k) {
-        const int e = faces.order[k];
-        const int64_t r = static_cast<int64_t>(base) + k;
-        out.fj[r] = faces.j[e];
+    for (int e = 0; e < faces.n; ++e) {
+        const int f = faces.order[e];
+        const int64_t r = static_cast<int64_t>(base) + e;
+        out.fj[r] = faces.j[f];
         for (int a = 0; a < D; ++a) {
-            out.fa[D * r + a] = faces.a[e][a];
-            out.fc[D * r + a] = faces.c[e][a];
+            out.fa[D * r + a] = faces.a[f][a];
+            out.fc[D * r + a] = faces.c[f][a];
         }
     }
 }
@@ -337,11 +346,12 @@ __global__ void k_list_sort(int64_t n, const int32_t* __restrict__ start, int32_
 
 const char* cell_error(int code) {
     switch (code) {
-        case kOutOfOffsets: return "the bucket search ran out of offsets (points too sparse for the grid)";
+        case kOutOfOffsets: return "a cell reaches farther than a box side from its generator (too few points for the box)";
         case kReachesBox: return "a cell reaches the box (box too small for the points)";
         case kTouchesSelf: return "a cell touches its own periodic image (box too small for the points)";
         case kDuplicatePair: return "two faces between the same pair of cells (box too small for unique nearest images)";
         case kCapacity: return "a cell has more vertices or faces than the remesher holds";
+        case kCandidates: return "more generators at one distance from a cell than the remesher holds";
         default: return "unknown cell error";
     }
 }
@@ -363,6 +373,8 @@ struct luna_remesh {
     Buf<int32_t> items;
     Buf<double> volume, centroid;
     Buf<int64_t> first;
+    Buf<int32_t> retry;
+    int64_t far_cells = 0;  // cells of the last build that took the far search
     Buf<int32_t> count, fj;
     Buf<double> fa, fc;
     Buf<int32_t> fwd, flips;
@@ -408,6 +420,7 @@ luna_status luna_remesh::build(int64_t n, const double* points, bool on_device, 
     RM_TRY(volume.reserve(n, "volumes"));
     RM_TRY(centroid.reserve(n * D, "centroids"));
     RM_TRY(first.reserve(n, "cell records"));
+    RM_TRY(retry.reserve(n, "far cells"));
     RM_TRY(count.reserve(n, "cell records"));
     RM_TRY(fwd.reserve(n, "owned faces"));
     RM_TRY(flips.reserve(n, "flipped faces"));
@@ -446,10 +459,17 @@ luna_status luna_remesh::build(int64_t n, const double* points, bool on_device, 
         RM_TRY(fc.reserve(capacity * D, "face records"));
         if (attempt > 0) RM_CUDA(cudaMemsetAsync(counters.ptr, 0, sizeof(Counters), stream));
         const CellOut out{volume.ptr, centroid.ptr, first.ptr, count.ptr, fj.ptr, fa.ptr, fc.ptr, capacity};
-        k_cells<D><<<grid_blocks(n, 128), 128, 0, stream>>>(n, pos.ptr, box, g, out, counters.ptr);
+        k_cells<D, false><<<grid_blocks(n, 128), 128, 0, stream>>>(n, nullptr, pos.ptr, box, g, out, counters.ptr, retry.ptr);
         RM_CUDA(cudaGetLastError());
         RM_CUDA(cudaMemcpyAsync(&h, counters.ptr, sizeof(Counters), cudaMemcpyDeviceToHost, stream));
         RM_CUDA(cudaStreamSynchronize(stream));
+        if (h.retry > 0 && !h.error && !h.nonfinite) {  // the far search for the cells the fast path handed on
+            k_cells<D, true><<<grid_blocks(h.retry, 128), 128, 0, stream>>>(h.retry, retry.ptr, pos.ptr, box, g, out, counters.ptr, nullptr);
+            RM_CUDA(cudaGetLastError());
+            RM_CUDA(cudaMemcpyAsync(&h, counters.ptr, sizeof(Counters), cudaMemcpyDeviceToHost, stream));
+            RM_CUDA(cudaStreamSynchronize(stream));
+        }
+        far_cells = h.retry;
         if (h.nonfinite) return fail(LUNA_EINVAL, "luna_remesh_build: non-finite point");
         if (h.error) return fail(LUNA_EINVAL, std::string("luna_remesh_build: cell ") + std::to_string(h.error_cell) + ": " + cell_error(h.error));
         if (h.faces <= capacity) break;
@@ -555,7 +575,7 @@ LUNA_API luna_status luna_remesh_device_bytes(const luna_remesh* r, int64_t* out
     if (!r || !out) return fail(LUNA_EINVAL, "luna_remesh_device_bytes: null argument");
     const size_t b = r->offsets.bytes() + r->bound2.bytes() + r->input.bytes() + r->pos.bytes() + r->bucket.bytes() +
                      r->bucket_start.bytes() + r->bucket_count.bytes() + r->cursor.bytes() + r->items.bytes() + r->volume.bytes() +
-                     r->centroid.bytes() + r->first.bytes() + r->count.bytes() + r->fj.bytes() + r->fa.bytes() + r->fc.bytes() +
+                     r->centroid.bytes() + r->first.bytes() + r->retry.bytes() + r->count.bytes() + r->fj.bytes() + r->fa.bytes() + r->fc.bytes() +
                      r->fwd.bytes() + r->flips.bytes() + r->seg_length.bytes() + r->face_start.bytes() + r->owner.bytes() +
                      r->neighbour.bytes() + r->degree.bytes() + r->start.bytes() + r->list.bytes() + r->key.bytes() + r->area.bytes() +
                      r->fcen.bytes() + r->counters.bytes() + r->scan_temp.bytes();

@@ -70,11 +70,12 @@ struct HostGrid {
 
 const char* cell_error(int code) {
     switch (code) {
-        case luna_voronoi::kOutOfOffsets: return "voronoi: the bucket search ran out of offsets (points too sparse for the grid)";
+        case luna_voronoi::kOutOfOffsets: return "voronoi: a cell reaches farther than a box side from its generator (too few points for the box)";
         case luna_voronoi::kReachesBox: return "voronoi: a cell reaches the box (box too small for the points)";
         case luna_voronoi::kTouchesSelf: return "voronoi: a cell touches its own periodic image (box too small for the points)";
         case luna_voronoi::kDuplicatePair: return "voronoi: two faces between the same pair of cells (box too small for unique nearest images)";
         case luna_voronoi::kCapacity: return "voronoi: a cell has more vertices or faces than the builder holds";
+        case luna_voronoi::kCandidates: return "voronoi: more generators at one distance from a cell than the builder holds";
         default: return "voronoi: unknown cell error";
     }
 }
@@ -96,12 +97,13 @@ struct CellWork {
     luna_voronoi::HostPoly3 p3;
     luna_voronoi::HostPoly2 p2;
     luna_voronoi::HostCellFaces faces;
+    luna_voronoi::HostCandidates cand;
 };
 
 int cell(int dim, int64_t i, const double* pos, const double* side, const luna_voronoi::Grid& grid, CellWork& work,
          std::vector<CellFace>& faces, double& volume, double* centroid) {
-    const int code = dim == 3 ? luna_voronoi::build_cell<3>(i, pos, side, grid, work.p3, work.faces, volume, centroid)
-                              : luna_voronoi::build_cell<2>(i, pos, side, grid, work.p2, work.faces, volume, centroid);
+    const int code = dim == 3 ? luna_voronoi::build_cell<3>(i, pos, side, grid, work.p3, work.faces, work.cand, volume, centroid)
+                              : luna_voronoi::build_cell<2>(i, pos, side, grid, work.p2, work.faces, work.cand, volume, centroid);
     if (code != luna_voronoi::kCellOk) return code;
     faces.resize(work.faces.n);
     for (int k = 0; k < work.faces.n; ++k) {

@@ -27,11 +27,12 @@ namespace luna_voronoi {
 // Why a cell could not be built (0: it was).
 enum : int {
     kCellOk = 0,
-    kOutOfOffsets = 1,   // the bucket search ran out of offsets (points too sparse for the grid)
+    kOutOfOffsets = 1,   // the search reached its limit (the grid's offsets; with Far, a box side)
     kReachesBox = 2,     // a face of the starting box survived: the box is too small for the points
     kTouchesSelf = 3,    // a face towards the cell's own image
     kDuplicatePair = 4,  // two faces towards the same cell (no unique nearest images)
     kCapacity = 5,       // more vertices, faces or loop entries than the storage holds
+    kCandidates = 6,     // more generator images at one distance than the candidate storage holds
 };
 
 // The bucket grid: nb buckets of width w per axis, items by bucket (CSR), and the bucket offsets to visit, sorted by a
@@ -45,6 +46,7 @@ struct Grid {
     const int32_t* offsets;  // [n_offsets][3]
     const double* bound2;    // [n_offsets]
     int n_offsets;
+    int reach;               // the offsets cover -reach .. reach buckets per axis
 };
 
 LUNA_VC_HD int bucket_of(const Grid& g, const double* x, int a) {
@@ -341,55 +343,160 @@ struct CellFacesT {
     int n;
 };
 
+// The generator images a cell is clipped by, one batch at a time: offset from the cell's generator, squared distance,
+// index; in clipping order.
+template <int kMax>
+struct CandidatesT {
+    double d[kMax][3];
+    double d2[kMax];
+    int32_t j[kMax];
+    int order[kMax];
+    int n;
+};
+
+// Appends to the batch the images in the bucket at offset o from the cell's bucket bi with lo2 < d2 <= hi2 from its
+// generator xi. Returns false when the batch outgrows the storage.
+template <int D, class Cand>
+LUNA_VC_HD bool gather_bucket(const double* xi, const int* bi, const int32_t* o, const double* pos, const double* side, const Grid& grid,
+                              double lo2, double hi2, Cand& cand) {
+    constexpr int kMax = sizeof(cand.j) / sizeof(cand.j[0]);
+    int64_t b = 0;
+    double shift[3] = {0, 0, 0};
+    for (int a = 0; a < D; ++a) {
+        const int t = bi[a] + o[a];
+        const int tw = ((t % grid.nb[a]) + grid.nb[a]) % grid.nb[a];
+        shift[a] = static_cast<double>((t - tw) / grid.nb[a]) * side[a];
+        b = b * grid.nb[a] + tw;
+    }
+    for (int64_t q = grid.start[b]; q < grid.start[b + 1]; ++q) {
+        const int32_t j = grid.items[q];
+        double d[3] = {0, 0, 0};
+        double d2 = 0;
+        for (int a = 0; a < D; ++a) {
+            d[a] = pos[D * j + a] + shift[a] - xi[a];
+            d2 += d[a] * d[a];
+        }
+        if (!(d2 > lo2 && d2 <= hi2)) continue;
+        if (cand.n >= kMax) return false;
+        const int e = cand.n++;
+        for (int a = 0; a < 3; ++a) cand.d[e][a] = d[a];
+        cand.d2[e] = d2;
+        cand.j[e] = j;
+    }
+    return true;
+}
+
+// The far search of a cell much larger than the mean spacing (the evacuated middle of a blast on a moving mesh): every
+// offset of the cube that can hold an image within hi2, by the grid's lower bound of its distance.
+template <int D, class Cand>
+LUNA_VC_HD bool gather_cube(const double* xi, const int* bi, const double* pos, const double* side, const Grid& grid, double lo2,
+                            double hi2, Cand& cand) {
+    int R[3] = {0, 0, 0};
+    for (int a = 0; a < D; ++a) R[a] = static_cast<int>(floor(sqrt(hi2) / grid.w[a])) + 1;
+    int32_t o[3] = {0, 0, 0};
+    for (o[0] = -R[0]; o[0] <= R[0]; ++o[0])
+        for (o[1] = -R[1]; o[1] <= R[1]; ++o[1])
+            for (o[2] = -R[2]; o[2] <= R[2]; ++o[2]) {
+                double lower = 0;
+                for (int a = 0; a < D; ++a) {
+                    const int gap = (o[a] < 0 ? -o[a] : o[a]) - 1;
+                    const double g = (gap > 0 ? gap : 0) * grid.w[a];
+                    lower += g * g;
+                }
+                if (lower > hi2) continue;
+                if (!gather_bucket<D>(xi, bi, o, pos, side, grid, lo2, hi2, cand)) return false;
+            }
+    return true;
+}
+
+// Gathers the images of generators with lo2 < d2 <= hi2 from the cell's generator xi (every bucket whose lower bound is
+// at most hi2: through the grid's sorted offsets while they reach, table2, else over the cube of offsets), then orders
+// the batch by (d2, index). Returns false when the batch outgrows the storage.
+template <int D, bool Far, class Cand>
+LUNA_VC_HD bool gather(const double* xi, const int* bi, const double* pos, const double* side, const Grid& grid, double lo2, double hi2,
+                       double table2, Cand& cand) {
+    cand.n = 0;
+    if (!Far || hi2 <= table2) {
+        for (int k = 0; k < grid.n_offsets && grid.bound2[k] <= hi2; ++k)
+            if (!gather_bucket<D>(xi, bi, grid.offsets + 3 * k, pos, side, grid, lo2, hi2, cand)) return false;
+    } else if (!gather_cube<D>(xi, bi, pos, side, grid, lo2, hi2, cand)) {
+        return false;
+    }
+    for (int k = 0; k < cand.n; ++k) {  // insertion sort by (d2, j), stable
+        int x = k, m = k - 1;
+        while (m >= 0 && (cand.d2[cand.order[m]] > cand.d2[x] || (cand.d2[cand.order[m]] == cand.d2[x] && cand.j[cand.order[m]] > cand.j[x]))) {
+            cand.order[m + 1] = cand.order[m];
+            --m;
+        }
+        cand.order[m + 1] = x;
+    }
+    return true;
+}
+
 // Cell i of the points pos [n][dim] (wrapped into [0, side)): clipped, then its faces (out.order by neighbour), volume
 // and centroid relative to the generator. Returns kCellOk or why the cell could not be built.
-template <int D, class Poly, class Faces>
-LUNA_VC_HD int build_cell(int64_t i, const double* pos, const double* side, const Grid& grid, Poly& poly, Faces& out,
+//
+// The cell is clipped by the generator images nearest first, in (distance, index) order, and is complete at the first
+// image farther than twice its largest vertex radius: the images are gathered in batches, all of those within a radius
+// at a time (first 2.1 bucket widths; then, while the cell still reaches past a batch, out to twice its reach, 1.5
+// times the batch's radius or the search's limit, whichever is nearest; with Far, a batch too large for the candidate
+// storage is gathered again as a thinner shell). The order, and so the cell, does not depend on where the batches
+// end. Nearest first, a cell is cut about as often as it has faces. Without Far the search ends at the grid's sorted
+// offsets (kOutOfOffsets) and at a full candidate store (kCandidates): the common cell's fast path, the cells it
+// refuses built again with Far, which searches out to a box side and thins its batches.
+template <int D, bool Far = true, class Poly, class Faces, class Cand>
+LUNA_VC_HD int build_cell(int64_t i, const double* pos, const double* side, const Grid& grid, Poly& poly, Faces& out, Cand& cand,
                           double& volume, double* centroid) {
     const double* xi = pos + D * i;
     double half[3] = {0, 0, 0};
-    double scale = 0;
+    double scale = 0, wmax = 0, wmin = 1e300;
     for (int a = 0; a < D; ++a) {
         half[a] = 0.5 * side[a];
         scale = side[a] > scale ? side[a] : scale;
+        wmax = grid.w[a] > wmax ? grid.w[a] : wmax;
+        wmin = grid.w[a] < wmin ? grid.w[a] : wmin;
     }
     poly.box(half);
     poly.eps = 1e-13 * scale;
     int bi[3] = {0, 0, 0};
     for (int a = 0; a < D; ++a) bi[a] = bucket_of(grid, xi, a);
     double rmax2 = poly.max_radius2();
-    bool done = false;
-    for (int k = 0; k < grid.n_offsets; ++k) {
-        if (grid.bound2[k] > 4.0 * rmax2) {
-            done = true;
-            break;
+    // the grid's offsets reach every bucket whose lower bound is below (K - 1)^2 w_min^2 (K: their reach per axis); the
+    // far search stops at a box side from the generator
+    const double reach = static_cast<double>(grid.reach - 1) * wmin;
+    const double table2 = reach * reach;
+    double far2 = 0;
+    for (int a = 0; a < D; ++a) far2 = side[a] * side[a] > far2 ? side[a] * side[a] : far2;
+    const double limit2 = Far ? far2 : table2;
+    double lo2 = 0, hi2 = 4.41 * wmax * wmax;  // (d2 = 0: the generator itself)
+    hi2 = hi2 < limit2 ? hi2 : limit2;
+    for (;;) {
+        if (!gather<D, Far>(xi, bi, pos, side, grid, lo2, hi2, table2, cand)) {  // too many for the storage
+            if (!Far) return kCandidates;
+            const double thinner = lo2 + 0.25 * (hi2 - lo2);
+            if (!(thinner > lo2 && thinner < hi2)) return kCandidates;
+            hi2 = thinner;
+            continue;
         }
-        const int32_t* o = grid.offsets + 3 * k;
-        int64_t b = 0;
-        double shift[3] = {0, 0, 0};
-        for (int a = 0; a < D; ++a) {
-            const int t = bi[a] + o[a];
-            const int tw = ((t % grid.nb[a]) + grid.nb[a]) % grid.nb[a];
-            shift[a] = static_cast<double>((t - tw) / grid.nb[a]) * side[a];
-            b = b * grid.nb[a] + tw;
-        }
-        for (int64_t q = grid.start[b]; q < grid.start[b + 1]; ++q) {
-            const int32_t j = grid.items[q];
-            double d[3] = {0, 0, 0};
-            double d2 = 0;
-            for (int a = 0; a < D; ++a) {
-                d[a] = pos[D * j + a] + shift[a] - xi[a];
-                d2 += d[a] * d[a];
+        bool done = false;
+        for (int k = 0; k < cand.n; ++k) {
+            const int e = cand.order[k];
+            const double d2 = cand.d2[e];
+            if (d2 > 4.0 * rmax2) {
+                done = true;
+                break;
             }
-            if (d2 == 0) continue;  // the generator itself
-            if (d2 > 4.0 * rmax2) continue;
             const double inv = 1.0 / sqrt(d2);
-            const double nrm[3] = {d[0] * inv, d[1] * inv, d[2] * inv};
-            if (poly.clip(nrm, 0.5 * d2 * inv, j)) rmax2 = poly.max_radius2();
+            const double nrm[3] = {cand.d[e][0] * inv, cand.d[e][1] * inv, cand.d[e][2] * inv};
+            if (poly.clip(nrm, 0.5 * d2 * inv, cand.j[e])) rmax2 = poly.max_radius2();
             if (poly.full) return kCapacity;
         }
+        if (done || 4.0 * rmax2 <= hi2) break;  // every image within twice the reach has been clipped by
+        if (hi2 >= limit2) return kOutOfOffsets;
+        lo2 = hi2;
+        hi2 = 4.0 * rmax2 < 2.25 * hi2 ? 4.0 * rmax2 : 2.25 * hi2;
+        hi2 = hi2 < limit2 ? hi2 : limit2;
     }
-    if (!done) return kOutOfOffsets;
     out.n = 0;
     volume = 0;
     double cm[3] = {0, 0, 0};
@@ -477,12 +584,15 @@ LUNA_VC_HD int build_cell(int64_t i, const double* pos, const double* side, cons
     return kCellOk;
 }
 
-// The device remesher's storage (about 18 KB a thread in 3D) and the host builder's.
-using Poly3 = Poly3T<128, 64, 512, 64>;
+// The device remesher's storage (about 17 KB a thread in 3D, of which a gas cell touches a third) and the host
+// builder's.
+using Poly3 = Poly3T<96, 48, 384, 48>;
 using Poly2 = Poly2T<64>;
-using CellFaces = CellFacesT<64>;
+using CellFaces = CellFacesT<48>;
 using HostPoly3 = Poly3T<2048, 1024, 8192, 1024>;
 using HostPoly2 = Poly2T<4096>;
 using HostCellFaces = CellFacesT<4096>;
+using Candidates = CandidatesT<160>;
+using HostCandidates = CandidatesT<16384>;
 
 }  // namespace luna_voronoi

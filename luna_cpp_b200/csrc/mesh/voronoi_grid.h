@@ -14,6 +14,7 @@
 namespace luna_voronoi {
 
 struct GridShape {
+    static constexpr int kReach = 8;  // buckets per axis the offsets reach
     int dim = 3;
     int nb[3] = {1, 1, 1};
     double w[3] = {1, 1, 1};
@@ -34,7 +35,7 @@ struct GridShape {
             w[a] = a < d ? side[a] / nb[a] : 1.0;
             buckets *= nb[a];
         }
-        const int K = 8;
+        const int K = kReach;
         std::vector<std::array<int, 3>> all;
         for (int x = -K; x <= K; ++x)
             for (int y = (d >= 2 ? -K : 0); y <= (d >= 2 ? K : 0); ++y)
@@ -67,6 +68,7 @@ struct GridShape {
         g.offsets = offsets_at;
         g.bound2 = bound2_at;
         g.n_offsets = static_cast<int>(bound2.size());
+        g.reach = kReach;
         return g;
     }
 };

@@ -157,7 +157,7 @@ def run_moving(fv, t_end, courant=0.3, threads=0, max_steps=100000, remesher=Non
     return {"steps": steps, "t": t, "hydro_device_ms": hydro_ms, "remesh_s": remesh_s, "mesh_load_s": load_s, "wall_s": wall}
 
 
-def _moving_run(nx, t_end, precision_policy, courant, threads, remesh, max_steps, log):
+def _moving_run(nx, t_end, precision_policy, courant, threads, remesh, max_steps, log, check_final_mesh=False):
     """The moving point blast on nx^3 snapped jittered generators; the initial mesh built where the remesh runs."""
     step = 2.0 ** -30
     pts = np.round(jittered_points((nx, nx, nx), jitter=0.1, seed=1) / step) * step
@@ -176,7 +176,13 @@ def _moving_run(nx, t_end, precision_policy, courant, threads, remesh, max_steps
     q = fv.get_state()
     final = fv.mesh.cells() if remesher is not None else fv.mesh
     N, n = cells.n_cells, run["steps"]
-    out = {"cells": N, "remesh": remesh, **run,
+    same = None
+    if remesher is not None and check_final_mesh:  # the last device mesh against the host builder on its generators
+        dev = fv.mesh.to_host()
+        host = build_mesh(dev.positions, threads=threads)
+        same = all(np.ascontiguousarray(getattr(dev, f)).tobytes() == np.ascontiguousarray(getattr(host, f)).tobytes()
+                   for f in ("owner", "neighbour", "cell_face_start", "cell_face", "area", "face_centroid", "centroid", "volume"))
+    out = {"cells": N, "remesh": remesh, **run, "final_mesh_equals_host_builder": same,
            "hydro_ms_per_step": run["hydro_device_ms"] / n, "remesh_ms_per_step": 1e3 * run["remesh_s"] / n,
            "mesh_load_ms_per_step": 1e3 * run["mesh_load_s"] / n, "step_wall_ms": 1e3 * run["wall_s"] / n,
            "hydro_cell_updates_per_s": N * n / (run["hydro_device_ms"] * 1e-3),
@@ -185,7 +191,8 @@ def _moving_run(nx, t_end, precision_policy, courant, threads, remesh, max_steps
            "energy_drift": float(abs(q[:, 4].sum() - q0[:, 4].sum()) / q0[:, 4].sum()),
            "radial_density_profile": radial_profile(final, q).tolist()}
     log(f"moving {nx}^3 to t = {run['t']:.4f}: {n} steps; a step: hydro {out['hydro_ms_per_step']:.2f} ms (device), remesh "
-        f"{out['remesh_ms_per_step']:.1f} ms, mesh load {out['mesh_load_ms_per_step']:.1f} ms, whole {out['step_wall_ms']:.1f} ms")
+        f"{out['remesh_ms_per_step']:.1f} ms, mesh load {out['mesh_load_ms_per_step']:.1f} ms, whole {out['step_wall_ms']:.1f} ms; "
+        f"final mesh equals the host builder's: {same}")
     fv.close()
     if remesher is not None:
         remesher.close()
@@ -201,11 +208,11 @@ def moving(nx=32, t_end=0.05, precision_policy="fp32", scale_nx=(128, 256), scal
     builder."""
     out = {"config": {"t_end": t_end, "precision": precision_policy, "courant": courant, "remesh": remesh,
                       "problem": "point blast, E = 1 within 2 cell widths, moving mesh"}}
-    out["run"] = _moving_run(nx, t_end, precision_policy, courant, threads, remesh, 100000, log)
+    out["run"] = _moving_run(nx, t_end, precision_policy, courant, threads, remesh, 100000, log, check_final_mesh=True)
     out["scale"] = []
     for big, steps in zip(scale_nx, scale_steps):
         out["scale"].append(_moving_run(big, t_end if steps == 0 else 1.0, precision_policy, courant, threads, remesh,
-                                        100000 if steps == 0 else steps, log))
+                                        100000 if steps == 0 else steps, log, check_final_mesh=big <= 128))
     return out
 
 

@@ -49,3 +49,25 @@ def test_jittered_points_law():
 def test_too_small_box_is_an_error():
     with pytest.raises(ValueError):
         build_mesh(np.array([[0.5, 0.5, 0.5], [0.1, 0.1, 0.1]]))
+
+
+def hollow_points(nx=20, hole=0.36):
+    """A jittered lattice with a hole of radius ``hole`` around the box centre and one generator at the centre: the
+    centre cell reaches several times farther than the grid's sorted offsets."""
+    p = jittered_points((nx, nx, nx), jitter=0.1, seed=4)
+    keep = np.linalg.norm(p - 0.5, axis=1) > hole
+    return np.concatenate([[[0.5, 0.5, 0.5]], p[keep]])
+
+
+def test_cell_far_larger_than_the_spacing():
+    """The search continues past the grid's offsets over the cube of buckets that can hold a cutting image: the centre
+    cell of a hollow lattice is a closed polyhedron of the hole's size; volumes tile the box."""
+    m = build_mesh(hollow_points())
+    assert np.isclose(m.volume.sum(), 1.0, rtol=0, atol=1e-12)
+    S = np.zeros((m.n_cells, 3))
+    np.add.at(S, m.owner, m.area)
+    np.add.at(S, m.neighbour, -m.area)
+    assert np.abs(S).max() < 1e-14
+    r = 0.36 / 2  # the centre cell holds at least the ball of half the hole's radius
+    assert m.volume[0] > 4.0 / 3.0 * np.pi * r ** 3
+    assert m.cell_face_start[1] - m.cell_face_start[0] > 30
