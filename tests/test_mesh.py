@@ -71,3 +71,11 @@ def test_cell_far_larger_than_the_spacing():
     r = 0.36 / 2  # the centre cell holds at least the ball of half the hole's radius
     assert m.volume[0] > 4.0 / 3.0 * np.pi * r ** 3
     assert m.cell_face_start[1] - m.cell_face_start[0] > 30
+
+
+def test_threads_do_not_change_the_mesh():
+    """Cells are built independently and assembled in a fixed order: one thread and all threads give the same bytes."""
+    p = jittered_points((14, 14, 14), jitter=0.1, seed=9)
+    a, b = build_mesh(p, threads=1), build_mesh(p, threads=0)
+    for f in ("owner", "neighbour", "cell_face_start", "cell_face", "area", "face_centroid", "centroid", "volume"):
+        assert np.ascontiguousarray(getattr(a, f)).tobytes() == np.ascontiguousarray(getattr(b, f)).tobytes(), f
