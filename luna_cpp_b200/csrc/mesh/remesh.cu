@@ -373,8 +373,7 @@ struct luna_remesh {
     Buf<int32_t> items;
     Buf<double> volume, centroid;
     Buf<int64_t> first;
-    Buf<int32_t> retry;
-    int64_t far_cells = 0;  // cells of the last build that took the far search
+    Buf<int32_t> retry;  // cells the fast path handed to the far search
     Buf<int32_t> count, fj;
     Buf<double> fa, fc;
     Buf<int32_t> fwd, flips;
@@ -469,7 +468,6 @@ luna_status luna_remesh::build(int64_t n, const double* points, bool on_device, 
             RM_CUDA(cudaMemcpyAsync(&h, counters.ptr, sizeof(Counters), cudaMemcpyDeviceToHost, stream));
             RM_CUDA(cudaStreamSynchronize(stream));
         }
-        far_cells = h.retry;
         if (h.nonfinite) return fail(LUNA_EINVAL, "luna_remesh_build: non-finite point");
         if (h.error) return fail(LUNA_EINVAL, std::string("luna_remesh_build: cell ") + std::to_string(h.error_cell) + ": " + cell_error(h.error));
         if (h.faces <= capacity) break;

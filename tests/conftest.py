@@ -57,3 +57,32 @@ def cuda():
 
     hydro.lib()
     return True
+
+
+def voronoi_invariants(m, tol=1e-11):
+    """Geometric properties every periodic Voronoi mesh has, independent of how it was built: the volumes tile the box;
+    each cell's outward area vectors close; each face lies on the bisector plane of its two generators (its centroid
+    equidistant from both, its area vector along their separation); each cell's volume is a third of the flux of the
+    position through its faces (divergence theorem, 3D; half in 2D)."""
+    N, F, D = m.n_cells, m.n_faces, m.dim
+    box = np.asarray(m.box, dtype=np.float64)[:D]
+    assert np.isclose(m.volume.sum(), np.prod(box), rtol=0, atol=1e-12)
+    S = np.zeros((N, D))
+    np.add.at(S, m.owner, m.area)
+    np.add.at(S, m.neighbour, -m.area)
+    assert np.abs(S).max() < 1e-14
+    d = m.positions[m.neighbour] - m.positions[m.owner]
+    d -= box * np.round(d / box)
+    c = m.face_centroid  # relative to the owner's generator
+    r_o = np.linalg.norm(c, axis=1)
+    r_j = np.linalg.norm(c - d, axis=1)
+    assert np.max(np.abs(r_o - r_j) / np.linalg.norm(d, axis=1)) < tol
+    a = np.linalg.norm(m.area, axis=1)
+    keep = a > 1e-12 * a.max()
+    cos = np.einsum("fk,fk->f", m.area[keep], d[keep]) / (a[keep] * np.linalg.norm(d[keep], axis=1))
+    assert np.max(np.abs(cos - 1)) < 1e-9
+    flux = np.einsum("fk,fk->f", m.area, c)  # A . x_f from the owner's generator
+    V = np.zeros(N)
+    np.add.at(V, m.owner, flux)
+    np.add.at(V, m.neighbour, -np.einsum("fk,fk->f", m.area, c - d))
+    assert np.max(np.abs(V / D - m.volume) / m.volume) < tol

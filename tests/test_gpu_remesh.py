@@ -10,7 +10,7 @@ import ctypes
 
 import numpy as np
 import pytest
-from conftest import jittered_mesh
+from conftest import jittered_mesh, voronoi_invariants
 
 from luna_cpp_b200 import hydro
 from luna_cpp_b200.mesh import build_mesh, jittered_points
@@ -47,6 +47,7 @@ def test_device_mesh_equals_host_builder(cuda, name, points, box):
     r = Remesher(len(box), box)
     dev = r.build(points).to_host()
     assert_same_mesh(host, dev)
+    voronoi_invariants(dev)
     r.close()
 
 

@@ -2,7 +2,7 @@
 import numpy as np
 import pytest
 
-from conftest import jittered_mesh, random_mesh
+from conftest import jittered_mesh, random_mesh, voronoi_invariants
 from luna_cpp_b200.mesh import build_mesh, jittered_points
 
 
@@ -79,3 +79,9 @@ def test_threads_do_not_change_the_mesh():
     a, b = build_mesh(p, threads=1), build_mesh(p, threads=0)
     for f in ("owner", "neighbour", "cell_face_start", "cell_face", "area", "face_centroid", "centroid", "volume"):
         assert np.ascontiguousarray(getattr(a, f)).tobytes() == np.ascontiguousarray(getattr(b, f)).tobytes(), f
+
+
+@pytest.mark.parametrize("mesh_fn", [lambda: jittered_mesh(16), lambda: random_mesh(4096), lambda: jittered_mesh(32, 2),
+                                     lambda: build_mesh(hollow_points())])
+def test_voronoi_invariants(mesh_fn):
+    voronoi_invariants(mesh_fn())
