@@ -1,0 +1,73 @@
+"""The mesh builder against an independent Voronoi implementation: qhull (through scipy.spatial), run on the 27
+periodic images of the generators. The device remesher equals the host builder bit for bit (tests/test_gpu_remesh.py),
+so this pins both to a third-party construction: the same face pairs, area vectors, face centroids and cell volumes to
+round-off. CPU only."""
+import itertools
+
+import numpy as np
+import pytest
+
+from luna_cpp_b200.mesh import build_mesh, jittered_points
+
+scipy_spatial = pytest.importorskip("scipy.spatial")
+
+
+def periodic_qhull(pts, box):
+    """Faces {(i, j): (area vector out of i, centroid relative to i's generator)} and volumes of the periodic Voronoi
+    mesh of pts, from qhull's Voronoi diagram of the 3^D images (the central image's cells)."""
+    n, D = pts.shape
+    shifts = np.array(list(itertools.product((-1, 0, 1), repeat=D)), dtype=float)
+    zero = int(np.where((shifts == 0).all(1))[0][0])
+    allp = np.concatenate([pts + s * box for s in shifts])
+    vor = scipy_spatial.Voronoi(allp)
+    base = zero * n
+    faces = {}
+    for (p, q), rv in zip(vor.ridge_points, vor.ridge_vertices):
+        for a, b in ((p, q), (q, p)):
+            if not base <= a < base + n:
+                continue
+            assert -1 not in rv
+            i, j = a - base, b % n
+            V = vor.vertices[rv]
+            nrm = (allp[b] - allp[a]) / np.linalg.norm(allp[b] - allp[a])
+            if D == 3:  # the ridge's polygon ordered around its mean, fanned from its first vertex
+                c0 = V.mean(0)
+                u = np.cross(nrm, [1.0, 0, 0] if abs(nrm[0]) < 0.6 else [0, 1.0, 0])
+                u /= np.linalg.norm(u)
+                w = np.cross(nrm, u)
+                V = V[np.argsort(np.arctan2((V - c0) @ w, (V - c0) @ u))]
+                A, C, tot = np.zeros(3), np.zeros(3), 0.0
+                for k in range(1, len(V) - 1):
+                    t = 0.5 * np.cross(V[k] - V[0], V[k + 1] - V[0])
+                    A += t
+                    C += (t @ nrm) * (V[0] + V[k] + V[k + 1]) / 3
+                    tot += t @ nrm
+                faces[(i, j)] = (A, C / tot - pts[i])
+            else:
+                A = np.array([V[1, 1] - V[0, 1], -(V[1, 0] - V[0, 0])])
+                faces[(i, j)] = (A if A @ nrm > 0 else -A, V.mean(0) - pts[i])
+    vol = np.array([scipy_spatial.ConvexHull(vor.vertices[vor.regions[vor.point_region[base + i]]]).volume for i in range(n)])
+    return faces, vol
+
+
+CASES = [("jittered 8^3", lambda: jittered_points((8, 8, 8), jitter=0.1, seed=1), 3),
+         ("uniform random 400", lambda: np.random.default_rng(2).random((400, 3)), 3),
+         ("2D jittered 16^2", lambda: jittered_points((16, 16), jitter=0.1, seed=1), 2)]
+
+
+@pytest.mark.parametrize("name,points,dim", CASES, ids=[c[0] for c in CASES])
+def test_builder_matches_qhull(name, points, dim):
+    pts = points()
+    box = np.ones(dim)
+    ref, vol = periodic_qhull(pts, box)
+    m = build_mesh(pts, box=tuple(box))
+    ours = {(int(m.owner[f]), int(m.neighbour[f])): (m.area[f], m.face_centroid[f]) for f in range(m.n_faces)}
+    amax = max(np.linalg.norm(a) for a, _ in ours.values())
+    # faces of zero area (four or more generators on a sphere) are qhull's to keep or merge: compared above 1e-9
+    want = {k for k, (a, _) in ref.items() if k[0] < k[1] and np.linalg.norm(a) > 1e-9 * amax}
+    got = {k for k, (a, _) in ours.items() if np.linalg.norm(a) > 1e-9 * amax}
+    assert want == got
+    for k in got:
+        assert np.abs(ref[k][0] - ours[k][0]).max() < 1e-13 * amax
+        assert np.abs(ref[k][1] - ours[k][1]).max() < 1e-13
+    assert np.max(np.abs(vol - m.volume) / m.volume) < 1e-13
