@@ -275,7 +275,7 @@ def main():
     ap.add_argument("--nx", type=int, default=1024)
     ap.add_argument("--ny", type=int, default=4)
     ap.add_argument("--epochs", type=int, default=20)
-    ap.add_argument("--out", default="gpurun_out/limiter")
+    ap.add_argument("--out", default="limiter_out")
     args = ap.parse_args()
     os.makedirs(os.path.dirname(args.out) or ".", exist_ok=True)
     lines = []
