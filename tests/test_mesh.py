@@ -85,3 +85,12 @@ def test_threads_do_not_change_the_mesh():
                                      lambda: build_mesh(hollow_points())])
 def test_voronoi_invariants(mesh_fn):
     voronoi_invariants(mesh_fn())
+
+
+def test_cell_far_larger_than_the_spacing_2d():
+    """The far search in 2D: a jittered 40^2 lattice with a hole of radius 0.3 and one generator in its middle."""
+    p = jittered_points((40, 40), jitter=0.1, seed=4)
+    p = np.concatenate([[[0.5, 0.5]], p[np.linalg.norm(p - 0.5, axis=1) > 0.3]])
+    m = build_mesh(p, box=(1.0, 1.0))
+    voronoi_invariants(m)
+    assert m.volume[0] > np.pi * 0.15 ** 2
