@@ -433,6 +433,78 @@ LUNA_VC_HD bool gather(const double* xi, const int* bi, const double* pos, const
     return true;
 }
 
+// The faces of a built 3D cell (vertex loops idx with offsets fo and neighbours tag): area vector, centroid relative to
+// the generator, into out; the cell's volume and first moment summed into volume and cm (tetrahedra from the
+// generator, face by face, each fanned from its first vertex). Returns kCellOk, or why the cell is not a gas cell.
+template <class Faces>
+LUNA_VC_HD int cell_faces3(int64_t i, const double (*v)[3], const int* idx, const int* fo, const int32_t* tag, int nf, Faces& out,
+                           double& volume, double* cm) {
+    for (int f = 0; f < nf; ++f) {
+        const int a0 = fo[f], m = fo[f + 1] - a0;
+        if (tag[f] < 0) return kReachesBox;
+        if (tag[f] == i) return kTouchesSelf;
+        const double* p0 = v[idx[a0]];
+        double A[3] = {0, 0, 0};
+        for (int k = 1; k + 1 < m; ++k) {
+            const double* p1 = v[idx[a0 + k]];
+            const double* p2 = v[idx[a0 + k + 1]];
+            const double e1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+            const double e2[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
+            double t[3], x12[3];
+            cross3(e1, e2, t);
+            for (int a = 0; a < 3; ++a) A[a] += 0.5 * t[a];
+            // tetrahedron (origin, p0, p1, p2): 6 V = p0 . (p1 x p2)
+            cross3(p1, p2, x12);
+            const double v6 = dot3(p0, x12);
+            volume += v6 / 6.0;
+            for (int a = 0; a < 3; ++a) cm[a] += v6 / 6.0 * (p0[a] + p1[a] + p2[a]) / 4.0;
+        }
+        // the face centroid: its triangles' centroids weighted by their areas along the face normal
+        const double amag = sqrt(dot3(A, A));
+        double C[3] = {0, 0, 0};
+        double wsum = 0;
+        for (int k = 1; k + 1 < m; ++k) {
+            const double* p1 = v[idx[a0 + k]];
+            const double* p2 = v[idx[a0 + k + 1]];
+            const double e1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+            const double e2[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
+            double t[3];
+            cross3(e1, e2, t);
+            const double wgt = amag > 0 ? dot3(t, A) / amag : 0.0;
+            for (int a = 0; a < 3; ++a) C[a] += wgt * ((p0[a] + p1[a] + p2[a]) / 3.0);
+            wsum += wgt;
+        }
+        if (wsum > 0)
+            for (int a = 0; a < 3; ++a) C[a] /= wsum;
+        else
+            for (int a = 0; a < 3; ++a) C[a] = p0[a];
+        const int e = out.n++;
+        out.j[e] = tag[f];
+        for (int a = 0; a < 3; ++a) {
+            out.a[e][a] = A[a];
+            out.c[e][a] = C[a];
+        }
+    }
+    return kCellOk;
+}
+
+// out.order: the faces by neighbour (insertion sort). Returns kDuplicatePair if two faces share a neighbour.
+template <class Faces>
+LUNA_VC_HD int order_faces(Faces& out) {
+    for (int k = 0; k < out.n; ++k) {
+        const int x = k;
+        int j = k - 1;
+        while (j >= 0 && out.j[out.order[j]] > out.j[x]) {
+            out.order[j + 1] = out.order[j];
+            --j;
+        }
+        out.order[j + 1] = x;
+    }
+    for (int k = 1; k < out.n; ++k)
+        if (out.j[out.order[k]] == out.j[out.order[k - 1]]) return kDuplicatePair;
+    return kCellOk;
+}
+
 // Cell i of the points pos [n][dim] (wrapped into [0, side)): clipped, then its faces (out.order by neighbour), volume
 // and centroid relative to the generator. Returns kCellOk or why the cell could not be built.
 //
@@ -502,52 +574,8 @@ LUNA_VC_HD int build_cell(int64_t i, const double* pos, const double* side, cons
     double cm[3] = {0, 0, 0};
     if constexpr (D == 3) {
         const int c = poly.cur;
-        for (int f = 0; f < poly.nf[c]; ++f) {
-            const int a0 = poly.fo[c][f], m = poly.fo[c][f + 1] - a0;
-            if (poly.tag[c][f] < 0) return kReachesBox;
-            if (poly.tag[c][f] == i) return kTouchesSelf;
-            const double* p0 = poly.v[c][poly.idx[c][a0]];
-            double A[3] = {0, 0, 0};
-            for (int k = 1; k + 1 < m; ++k) {
-                const double* p1 = poly.v[c][poly.idx[c][a0 + k]];
-                const double* p2 = poly.v[c][poly.idx[c][a0 + k + 1]];
-                const double e1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
-                const double e2[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
-                double t[3], x12[3];
-                cross3(e1, e2, t);
-                for (int a = 0; a < 3; ++a) A[a] += 0.5 * t[a];
-                // tetrahedron (origin, p0, p1, p2): 6 V = p0 . (p1 x p2)
-                cross3(p1, p2, x12);
-                const double v6 = dot3(p0, x12);
-                volume += v6 / 6.0;
-                for (int a = 0; a < 3; ++a) cm[a] += v6 / 6.0 * (p0[a] + p1[a] + p2[a]) / 4.0;
-            }
-            // the face centroid: its triangles' centroids weighted by their areas along the face normal
-            const double amag = sqrt(dot3(A, A));
-            double C[3] = {0, 0, 0};
-            double wsum = 0;
-            for (int k = 1; k + 1 < m; ++k) {
-                const double* p1 = poly.v[c][poly.idx[c][a0 + k]];
-                const double* p2 = poly.v[c][poly.idx[c][a0 + k + 1]];
-                const double e1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
-                const double e2[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
-                double t[3];
-                cross3(e1, e2, t);
-                const double wgt = amag > 0 ? dot3(t, A) / amag : 0.0;
-                for (int a = 0; a < 3; ++a) C[a] += wgt * ((p0[a] + p1[a] + p2[a]) / 3.0);
-                wsum += wgt;
-            }
-            if (wsum > 0)
-                for (int a = 0; a < 3; ++a) C[a] /= wsum;
-            else
-                for (int a = 0; a < 3; ++a) C[a] = p0[a];
-            const int e = out.n++;
-            out.j[e] = poly.tag[c][f];
-            for (int a = 0; a < 3; ++a) {
-                out.a[e][a] = A[a];
-                out.c[e][a] = C[a];
-            }
-        }
+        const int code = cell_faces3(i, poly.v[c], poly.idx[c], poly.fo[c], poly.tag[c], poly.nf[c], out, volume, cm);
+        if (code != kCellOk) return code;
     } else {
         const int c = poly.cur, m = poly.nv[c];
         for (int k = 0; k < m; ++k) {
@@ -570,18 +598,7 @@ LUNA_VC_HD int build_cell(int64_t i, const double* pos, const double* side, cons
         }
     }
     for (int a = 0; a < D; ++a) centroid[a] = cm[a] / volume;
-    for (int k = 0; k < out.n; ++k) {
-        const int x = k;
-        int j = k - 1;
-        while (j >= 0 && out.j[out.order[j]] > out.j[x]) {
-            out.order[j + 1] = out.order[j];
-            --j;
-        }
-        out.order[j + 1] = x;
-    }
-    for (int k = 1; k < out.n; ++k)
-        if (out.j[out.order[k]] == out.j[out.order[k - 1]]) return kDuplicatePair;
-    return kCellOk;
+    return order_faces(out);
 }
 
 // The device remesher's storage (about 17 KB a thread in 3D, of which a gas cell touches a third) and the host
