@@ -50,3 +50,17 @@ def test_create_rejects_bad_order_without_touching_the_gpu():
     with pytest.raises(hydro.LunaError) as e:
         hydro.FiniteVolume(m, order=2)
     assert e.value.status == 1
+
+
+def test_remesher_rejects_bad_arguments_without_touching_the_gpu():
+    """luna_remesh_create checks its arguments before any CUDA call: EINVAL (1) with a message."""
+    lib = hydro.lib()
+    h = ctypes.c_void_p()
+    box = (ctypes.c_double * 3)(1.0, 1.0, 1.0)
+    assert lib.luna_remesh_create(4, box, ctypes.byref(h)) == 1
+    assert b"dim" in lib.luna_last_error()
+    bad = (ctypes.c_double * 3)(1.0, -1.0, 1.0)
+    assert lib.luna_remesh_create(3, bad, ctypes.byref(h)) == 1
+    assert lib.luna_remesh_create(3, None, ctypes.byref(h)) == 1
+    assert lib.luna_remesh_build(None, 10, None, 0, None, None) == 1
+    assert lib.luna_remesh_destroy(None) == 0
