@@ -50,7 +50,14 @@ def periodic_qhull(pts, box):
     return faces, vol
 
 
+def hollow():
+    """A 10^3 lattice with a hole of radius 0.33 and one generator in it: a cell of 64 faces."""
+    p = jittered_points((10, 10, 10), jitter=0.1, seed=4)
+    return np.concatenate([[[0.5, 0.5, 0.5]], p[np.linalg.norm(p - 0.5, axis=1) > 0.33]])
+
+
 CASES = [("jittered 8^3", lambda: jittered_points((8, 8, 8), jitter=0.1, seed=1), 3),
+         ("hollow 10^3", hollow, 3),
          ("uniform random 400", lambda: np.random.default_rng(2).random((400, 3)), 3),
          ("2D jittered 16^2", lambda: jittered_points((16, 16), jitter=0.1, seed=1), 2)]
 
