@@ -25,6 +25,9 @@
 #ifndef LUNA_REMESH_WARP
 #define LUNA_REMESH_WARP 0  // 1: the fast path builds a 3D cell with a warp (remesh_warp.cuh); 0: with one thread
 #endif
+#ifndef LUNA_REMESH_DUAL
+#define LUNA_REMESH_DUAL 0  // 1: 3D cells kept as triangles of plane triples (DualT), as the host builder's LUNA_MESH_DUAL=1
+#endif
 
 namespace luna {
 luna_status report_error(luna_status s, const std::string& what);
@@ -159,12 +162,24 @@ __global__ void __launch_bounds__(128) k_cells(int64_t n, const int32_t* __restr
     const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (k >= n) return;
     const int64_t i = list ? list[k] : k;
+#if LUNA_REMESH_DUAL
+    using Poly = std::conditional_t<D == 3, Dual, Poly2>;
+#else
     using Poly = std::conditional_t<D == 3, Poly3, Poly2>;
+#endif
     Poly poly;
     CellFaces faces;
     Candidates cand;
     double volume = 0, centroid[3] = {0, 0, 0};
+#if LUNA_REMESH_DUAL
+    int code;
+    if constexpr (D == 3)
+        code = build_cell_dual<Far>(i, pos, box.s, g, poly, faces, cand, volume, centroid);
+    else
+        code = build_cell<D, Far>(i, pos, box.s, g, poly, faces, cand, volume, centroid);
+#else
     const int code = build_cell<D, Far>(i, pos, box.s, g, poly, faces, cand, volume, centroid);
+#endif
     if (code != kCellOk) {
         out.first[i] = 0;
         out.count[i] = 0;

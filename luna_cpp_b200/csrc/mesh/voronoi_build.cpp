@@ -14,6 +14,7 @@
 #include <array>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <random>
@@ -92,17 +93,28 @@ struct luna_mesh_build {
 
 namespace {
 
+// LUNA_MESH_DUAL=1 in the environment builds 3D cells as DualT (voronoi_cell.h) instead of face loops.
+bool dual_cells() {
+    static const bool on = [] {
+        const char* v = std::getenv("LUNA_MESH_DUAL");
+        return v && v[0] == '1';
+    }();
+    return on;
+}
+
 // Cell i: clipped (voronoi_cell.h), then its faces by neighbour, volume and centroid. Returns 0 or a cell error.
 struct CellWork {
     luna_voronoi::HostPoly3 p3;
     luna_voronoi::HostPoly2 p2;
     luna_voronoi::HostCellFaces faces;
     luna_voronoi::HostCandidates cand;
+    luna_voronoi::HostDual dual;
 };
 
 int cell(int dim, int64_t i, const double* pos, const double* side, const luna_voronoi::Grid& grid, CellWork& work,
          std::vector<CellFace>& faces, double& volume, double* centroid) {
-    const int code = dim == 3 ? luna_voronoi::build_cell<3>(i, pos, side, grid, work.p3, work.faces, work.cand, volume, centroid)
+    const int code = dim == 3 ? (dual_cells() ? luna_voronoi::build_cell_dual<true>(i, pos, side, grid, work.dual, work.faces, work.cand, volume, centroid)
+                                              : luna_voronoi::build_cell<3>(i, pos, side, grid, work.p3, work.faces, work.cand, volume, centroid))
                               : luna_voronoi::build_cell<2>(i, pos, side, grid, work.p2, work.faces, work.cand, volume, centroid);
     if (code != luna_voronoi::kCellOk) return code;
     faces.resize(work.faces.n);

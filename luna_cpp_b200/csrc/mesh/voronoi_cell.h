@@ -601,6 +601,252 @@ LUNA_VC_HD int build_cell(int64_t i, const double* pos, const double* side, cons
     return order_faces(out);
 }
 
+// A 3D cell kept as triangles of plane triples, the dual of its vertices (each vertex is where three planes meet; a
+// triangle's cyclic order gives the vertex's orientation): a cut drops the triangles beyond the plane and fans the new
+// plane over the boundary edges of the dropped region (edges whose reverse is not also dropped), instead of rebuilding
+// every face loop. Room for kMaxPlanes planes (the starting box's six first) and kMaxTris vertices; vertex positions
+// are kept beside their triangles. Its vertices are plane intersections, so its meshes agree with the face-loop
+// cell's to round-off, not bit for bit; the host builder and the device remesher run the same code when they use it.
+template <int kMaxPlanes, int kMaxTris>
+struct DualT {
+    double pn[kMaxPlanes][3], pc[kMaxPlanes];  // planes n.x <= c
+    int32_t ptag[kMaxPlanes];
+    int np;
+    uint8_t tri[kMaxTris][3];
+    double tv[kMaxTris][3];
+    bool out[kMaxTris];
+    uint8_t eu[3 * kMaxTris], ev[3 * kMaxTris];
+    bool boundary[3 * kMaxTris];
+    int nt;
+    double eps;
+    bool full;
+
+    LUNA_VC_HD void vertex(int t) {  // the meeting point of the triangle's three planes (Cramer's rule)
+        const double* a = pn[tri[t][0]];
+        const double* b = pn[tri[t][1]];
+        const double* c = pn[tri[t][2]];
+        double bc[3], ca[3], ab[3];
+        cross3(b, c, bc);
+        cross3(c, a, ca);
+        cross3(a, b, ab);
+        const double det = dot3(a, bc);
+        for (int k = 0; k < 3; ++k) tv[t][k] = (pc[tri[t][0]] * bc[k] + pc[tri[t][1]] * ca[k] + pc[tri[t][2]] * ab[k]) / det;
+    }
+    LUNA_VC_HD void box(const double* half) {
+        full = false;
+        np = 6;
+        nt = 0;
+        for (int k = 0; k < 6; ++k) {
+            for (int a = 0; a < 3; ++a) pn[k][a] = a == k / 2 ? ((k & 1) ? 1.0 : -1.0) : 0.0;
+            pc[k] = half[k / 2];
+            ptag[k] = -1;
+        }
+        for (int x = 0; x < 2; ++x)
+            for (int y = 0; y < 2; ++y)
+                for (int z = 0; z < 2; ++z) {
+                    int p0 = x, p1 = 2 + y, p2 = 4 + z;
+                    double c01[3];
+                    cross3(pn[p0], pn[p1], c01);
+                    if (dot3(c01, pn[p2]) < 0) {  // oriented: (n0 x n1) . n2 > 0
+                        const int sw = p1;
+                        p1 = p2;
+                        p2 = sw;
+                    }
+                    tri[nt][0] = static_cast<uint8_t>(p0);
+                    tri[nt][1] = static_cast<uint8_t>(p1);
+                    tri[nt][2] = static_cast<uint8_t>(p2);
+                    vertex(nt);
+                    ++nt;
+                }
+    }
+    LUNA_VC_HD double max_radius2() const {
+        double r = 0;
+        for (int t = 0; t < nt; ++t) {
+            const double d = dot3(tv[t], tv[t]);
+            r = d > r ? d : r;
+        }
+        return r;
+    }
+    LUNA_VC_HD bool clip(const double* nrm, double c, int32_t tag) {
+        bool any = false;
+        for (int t = 0; t < nt; ++t) {
+            out[t] = dot3(nrm, tv[t]) - c > eps;
+            any = any || out[t];
+        }
+        if (!any) return false;
+        if (np >= kMaxPlanes) {
+            full = true;
+            return false;
+        }
+        const int q = np++;
+        for (int a = 0; a < 3; ++a) pn[q][a] = nrm[a];
+        pc[q] = c;
+        ptag[q] = tag;
+        int ne = 0;
+        for (int t = 0; t < nt; ++t)
+            if (out[t])
+                for (int k = 0; k < 3; ++k) {
+                    eu[ne] = tri[t][k];
+                    ev[ne] = tri[t][(k + 1) % 3];
+                    ++ne;
+                }
+        for (int e = 0; e < ne; ++e) {  // the boundary edges: those whose reverse is not a dropped triangle's edge
+            bool paired = false;
+            for (int f = 0; f < ne && !paired; ++f) paired = eu[f] == ev[e] && ev[f] == eu[e];
+            boundary[e] = !paired;
+        }
+        int nb = 0;  // compacted in place, after every pairing is known
+        for (int e = 0; e < ne; ++e)
+            if (boundary[e]) {
+                eu[nb] = eu[e];
+                ev[nb] = ev[e];
+                ++nb;
+            }
+        int w = 0;
+        for (int t = 0; t < nt; ++t)
+            if (!out[t]) {
+                if (w != t) {
+                    for (int k = 0; k < 3; ++k) tri[w][k] = tri[t][k];
+                    for (int k = 0; k < 3; ++k) tv[w][k] = tv[t][k];
+                }
+                ++w;
+            }
+        nt = w;
+        if (nt + nb > kMaxTris) {
+            full = true;
+            return false;
+        }
+        for (int e = 0; e < nb; ++e) {
+            tri[nt][0] = eu[e];
+            tri[nt][1] = ev[e];
+            tri[nt][2] = static_cast<uint8_t>(q);
+            vertex(nt);
+            ++nt;
+        }
+        return true;
+    }
+    // The faces (one per plane still holding vertices), volume and first moment, as cell_faces3: each face's vertices
+    // in order around it (from its lowest triangle, each next triangle the one sharing the plane and the last vertex's
+    // other plane), turned to run counter-clockwise seen from outside, fanned from the first.
+    template <class Faces>
+    LUNA_VC_HD int finish(int64_t i, Faces& faces, double& volume, double* cm) {
+        int loop[kMaxTris];
+        for (int p = 0; p < np; ++p) {
+            int t0 = -1, m = 0;
+            for (int t = 0; t < nt && t0 < 0; ++t)
+                if (tri[t][0] == p || tri[t][1] == p || tri[t][2] == p) t0 = t;
+            if (t0 < 0) continue;
+            if (ptag[p] < 0) return kReachesBox;
+            if (ptag[p] == i) return kTouchesSelf;
+            int cur = t0;
+            int r = tri[cur][0] == p ? 0 : tri[cur][1] == p ? 1 : 2;
+            int b = tri[cur][(r + 2) % 3];
+            do {
+                if (m >= kMaxTris) return kCapacity;
+                loop[m++] = cur;
+                int next = -1;  // the triangle with p followed by b
+                for (int t = 0; t < nt && next < 0; ++t)
+                    for (int k = 0; k < 3; ++k)
+                        if (tri[t][k] == p && tri[t][(k + 1) % 3] == b) {
+                            next = t;
+                            b = tri[t][(k + 2) % 3];
+                            break;
+                        }
+                if (next < 0) return kCapacity;
+                cur = next;
+            } while (cur != t0);
+            if (m < 3) continue;
+            double A[3] = {0, 0, 0};
+            for (int k = 1; k + 1 < m; ++k) {
+                const double* p0 = tv[loop[0]];
+                const double* p1 = tv[loop[k]];
+                const double* p2 = tv[loop[k + 1]];
+                const double e1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+                const double e2[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
+                double tt[3];
+                cross3(e1, e2, tt);
+                for (int a = 0; a < 3; ++a) A[a] += 0.5 * tt[a];
+            }
+            if (dot3(A, pn[p]) < 0)  // the other way round
+                for (int k = 1, l = m - 1; k < l; ++k, --l) {
+                    const int sw = loop[k];
+                    loop[k] = loop[l];
+                    loop[l] = sw;
+                }
+            if (faces.n >= static_cast<int>(sizeof(faces.j) / sizeof(faces.j[0]))) return kCapacity;
+            int idx[kMaxTris + 1];
+            for (int k = 0; k < m; ++k) idx[k] = loop[k];
+            const int fo[2] = {0, m};
+            const int32_t tag = ptag[p];
+            const int code = cell_faces3(i, tv, idx, fo, &tag, 1, faces, volume, cm);
+            if (code != kCellOk) return code;
+        }
+        return kCellOk;
+    }
+};
+
+// Cell i as build_cell<3, Far> builds it, with the dual cell.
+template <bool Far, class Dual, class Faces, class Cand>
+LUNA_VC_HD int build_cell_dual(int64_t i, const double* pos, const double* side, const Grid& grid, Dual& poly, Faces& out, Cand& cand,
+                               double& volume, double* centroid) {
+    constexpr int D = 3;
+    const double* xi = pos + D * i;
+    double half[3] = {0, 0, 0};
+    double scale = 0, wmax = 0, wmin = 1e300;
+    for (int a = 0; a < D; ++a) {
+        half[a] = 0.5 * side[a];
+        scale = side[a] > scale ? side[a] : scale;
+        wmax = grid.w[a] > wmax ? grid.w[a] : wmax;
+        wmin = grid.w[a] < wmin ? grid.w[a] : wmin;
+    }
+    poly.box(half);
+    poly.eps = 1e-13 * scale;
+    int bi[3] = {0, 0, 0};
+    for (int a = 0; a < D; ++a) bi[a] = bucket_of(grid, xi, a);
+    double rmax2 = poly.max_radius2();
+    const double reach = static_cast<double>(grid.reach - 1) * wmin;
+    const double table2 = reach * reach;
+    double far2 = 0;
+    for (int a = 0; a < D; ++a) far2 = side[a] * side[a] > far2 ? side[a] * side[a] : far2;
+    const double limit2 = Far ? far2 : table2;
+    double lo2 = 0, hi2 = 4.41 * wmax * wmax;
+    hi2 = hi2 < limit2 ? hi2 : limit2;
+    for (;;) {
+        if (!gather<D, Far>(xi, bi, pos, side, grid, lo2, hi2, table2, cand)) {
+            if (!Far) return kCandidates;
+            const double thinner = lo2 + 0.25 * (hi2 - lo2);
+            if (!(thinner > lo2 && thinner < hi2)) return kCandidates;
+            hi2 = thinner;
+            continue;
+        }
+        bool done = false;
+        for (int k = 0; k < cand.n; ++k) {
+            const int e = cand.order[k];
+            const double d2 = cand.d2[e];
+            if (d2 > 4.0 * rmax2) {
+                done = true;
+                break;
+            }
+            const double inv = 1.0 / sqrt(d2);
+            const double nrm[3] = {cand.d[e][0] * inv, cand.d[e][1] * inv, cand.d[e][2] * inv};
+            if (poly.clip(nrm, 0.5 * d2 * inv, cand.j[e])) rmax2 = poly.max_radius2();
+            if (poly.full) return kCapacity;
+        }
+        if (done || 4.0 * rmax2 <= hi2) break;
+        if (hi2 >= limit2) return kOutOfOffsets;
+        lo2 = hi2;
+        hi2 = 4.0 * rmax2 < 2.25 * hi2 ? 4.0 * rmax2 : 2.25 * hi2;
+        hi2 = hi2 < limit2 ? hi2 : limit2;
+    }
+    out.n = 0;
+    volume = 0;
+    double cm[3] = {0, 0, 0};
+    const int code = poly.finish(i, out, volume, cm);
+    if (code != kCellOk) return code;
+    for (int a = 0; a < D; ++a) centroid[a] = cm[a] / volume;
+    return order_faces(out);
+}
+
 // The device remesher's storage (about 17 KB a thread in 3D, of which a gas cell touches a third) and the host
 // builder's.
 using Poly3 = Poly3T<96, 48, 384, 48>;
@@ -611,5 +857,7 @@ using HostPoly2 = Poly2T<4096>;
 using HostCellFaces = CellFacesT<4096>;
 using Candidates = CandidatesT<160>;
 using HostCandidates = CandidatesT<16384>;
+using Dual = DualT<64, 128>;
+using HostDual = DualT<256, 510>;
 
 }  // namespace luna_voronoi

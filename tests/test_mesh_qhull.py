@@ -78,3 +78,27 @@ def test_builder_matches_qhull(name, points, dim):
         assert np.abs(ref[k][0] - ours[k][0]).max() < 1e-13 * amax
         assert np.abs(ref[k][1] - ours[k][1]).max() < 1e-13
     assert np.max(np.abs(vol - m.volume) / m.volume) < 1e-13
+
+
+def test_dual_cells_match_qhull():
+    """The builder with its cells kept as triangles of plane triples (LUNA_MESH_DUAL=1, read once per process: a
+    subprocess) against qhull and the Voronoi invariants."""
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = (
+        "import sys; sys.path.insert(0, 'tests')\n"
+        "import numpy as np\n"
+        "from conftest import voronoi_invariants\n"
+        "from test_mesh_qhull import CASES, test_builder_matches_qhull\n"
+        "from luna_cpp_b200.mesh import build_mesh\n"
+        "for name, points, dim in CASES:\n"
+        "    test_builder_matches_qhull(name, points, dim)\n"
+        "    voronoi_invariants(build_mesh(points(), box=(1.0,) * dim))\n"
+        "print('ok')\n"
+    )
+    r = subprocess.run([sys.executable, "-c", code], cwd=root, env=dict(os.environ, LUNA_MESH_DUAL="1"), capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stderr[-2000:]
