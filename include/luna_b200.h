@@ -182,7 +182,11 @@ LUNA_API luna_status luna_mlp_adam(float* params, const float* grad, float* m, f
  * holds that array until the process exits. Every call shares it and it keeps the last call's contents; calls that
  * overlap on the GPU (other streams, other threads) race. The first call on a device looks up the array's device
  * address (once per device, with that device current); make that first call before any stream capture.
- * fallbacks_out (optional): the face sides that fell back to the cell's state; reading it synchronises the stream. */
+ * fallbacks_out (optional): the face sides that fell back to the cell's state. Giving it synchronises the stream and
+ * also reads the pass's error word: a state that is not finite after the update returns LUNA_ENONFINITE (Q is then
+ * already written). Without it the call does not synchronise and cannot report that.
+ * The device mesh arrays are trusted: unlike luna_fv_create, this call does not check the lists, so an owner,
+ * neighbour or cell_face entry out of range makes the kernels read out of bounds. */
 LUNA_API luna_status luna_apply_static_noalloc(const luna_mesh_desc* mesh, const luna_gas* gas, int order, int riemann, const double* prims,
                                                const double* gradients, double* q, double dt, void* stream, int64_t* fallbacks_out);
 

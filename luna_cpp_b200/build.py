@@ -80,17 +80,27 @@ def build_hydro(force=False, extra=()):
     if not cu:
         return None
     if force or _stale(target, deps):
-        # The device remesher runs the host mesh builder's cell code and must give its bits: no multiply-add
-        # contraction in that object (the hydro kernels keep it).
+        # One object per source, compiled in parallel, then one link. The device remesher runs the host mesh builder's
+        # cell code and must give its bits: no multiply-add contraction in that object (the hydro kernels keep it).
+        from concurrent.futures import ThreadPoolExecutor
+
         obj_dir = os.path.join(PKG, "_build")
         os.makedirs(obj_dir, exist_ok=True)
         remesh_obj = os.path.join(obj_dir, "remesh.o")
-        _run([_nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler",
-              "-ffp-contract=off", "-Xcompiler", "-fvisibility=hidden", "-c", "-I", INCLUDE, "-I", mesh, "-o", remesh_obj,
-              remesh])
-        _run([_nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
-              "-Xcompiler", "-fvisibility=hidden", "-shared", "-I", INCLUDE, "-I", hydro, "-o", target, *extra, *cu,
-              remesh_obj, "-lcudart"])
+        jobs = [[_nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler",
+                 "-ffp-contract=off", "-Xcompiler", "-fvisibility=hidden", "-c", "-I", INCLUDE, "-I", mesh, "-o",
+                 remesh_obj, remesh]]
+        objs = [remesh_obj]
+        for src in cu:
+            obj = os.path.join(obj_dir, os.path.splitext(os.path.basename(src))[0] + ".o")
+            objs.append(obj)
+            jobs.append([_nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler",
+                         "-fPIC", "-Xcompiler", "-fvisibility=hidden", "-c", "-I", INCLUDE, "-I", hydro, *extra, "-o",
+                         obj, src])
+        with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 1)) as pool:
+            for _ in pool.map(_run, jobs):
+                pass
+        _run([_nvcc(), *ARCH, "-shared", "-o", target, *objs, "-lcudart"])
     return target
 
 

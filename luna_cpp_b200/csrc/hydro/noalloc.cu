@@ -154,12 +154,17 @@ LUNA_API luna_status luna_apply_static_noalloc(const luna_mesh_desc* mesh, const
     }
     if (s != LUNA_OK) return s;
     if (fallbacks_out) {
-        unsigned long long count = 0;
+        // The pass's counters in one copy: the fallback count and the error word the update writes (bit 1: a state
+        // that is not finite, bit 2: an index out of range), reported as every other entry point reports them.
+        luna::Counters host{};
         const auto* counters = reinterpret_cast<const luna::Counters*>(scratch);
-        cudaError_t e = cudaMemcpyAsync(&count, &counters->fallbacks[0], sizeof(count), cudaMemcpyDeviceToHost, st);
+        cudaError_t e = cudaMemcpyAsync(&host, counters, sizeof(host), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) return fail(LUNA_ECUDA, std::string("reading the fallback count: ") + cudaGetErrorString(e));
-        *fallbacks_out = static_cast<int64_t>(count);
+        if (e != cudaSuccess) return fail(LUNA_ECUDA, std::string("reading the pass's counters: ") + cudaGetErrorString(e));
+        *fallbacks_out = static_cast<int64_t>(host.fallbacks[0]);
+        if (host.error & 7ull)
+            return fail(LUNA_ENONFINITE, "luna_apply_static_noalloc: the update produced a state that is not finite (error word " +
+                                             std::to_string(host.error) + ")");
     }
     return LUNA_OK;
 }

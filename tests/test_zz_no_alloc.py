@@ -86,3 +86,27 @@ def test_noalloc_rejects_meshes_beyond_its_scratch(cuda):
                                                    ctypes.c_void_p(8), 1e-3, None, None)
     assert status == 1
     assert b"838854" in hydro.lib().luna_last_error()
+
+
+def test_noalloc_reports_a_state_that_is_not_finite(cuda):
+    """A NaN planted in Q on the host: the update's error word comes back as LUNA_ENONFINITE when the call reads its
+    counters (fallbacks_out given), as every other entry point reports it; the next clean call returns LUNA_OK."""
+    import torch
+
+    mesh = jittered_mesh(8)
+    q0 = point_blast(mesh, radius_cells=2.0)
+    keep = []
+    desc = device_desc(mesh, torch, keep)
+    gas = hydro._Gas(5.0 / 3.0, 1e-10, 1e-10)
+    stream = torch.cuda.current_stream().cuda_stream
+    bad = q0.copy()
+    bad[5, 0] = np.nan
+    for q_host, want in ((bad, 4), (q0, 0)):
+        q = torch.tensor(q_host, device="cuda")
+        fallbacks = ctypes.c_int64(-1)
+        status = hydro.lib().luna_apply_static_noalloc(
+            ctypes.byref(desc), ctypes.byref(gas), 0, 0, None, None, ctypes.c_void_p(q.data_ptr()), 1e-4,
+            ctypes.c_void_p(stream), ctypes.byref(fallbacks))
+        assert status == want, (status, hydro.lib().luna_last_error())
+        if want == 4:
+            assert b"not finite" in hydro.lib().luna_last_error()
