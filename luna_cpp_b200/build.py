@@ -3,7 +3,9 @@
 - ``libluna_b200.so``: the hydro step, CUDA for sm_100a only (nvcc -gencode arch=compute_100a,code=sm_100a), C ABI in
   include/luna_b200.h, and the device remesher of the moving mesh (include/luna_remesh.h);
 - ``libluna_mesh.so``: the periodic Voronoi mesh builder (host C++, OpenMP);
-- ``oracle/liboracle.so``: the CPU oracle the tests check against (plain C, no multiply-add contraction).
+- ``oracle/liboracle.so``: the CPU oracle the tests check against (plain C, no multiply-add contraction);
+- ``oracle/_ref/libluna_ref.so``: the reference's own solver compiled on the CPU (``oracle/Makefile``), which pins the
+  oracle; built only where the reference's source tree is present (the Makefile names it), kept otherwise.
 The libraries are built next to their sources so they travel with the tree.
 """
 from __future__ import annotations
@@ -104,13 +106,28 @@ def build_hydro(force=False, extra=()):
     return target
 
 
+def build_reference(force=False):
+    """The reference's solver on the CPU (test infrastructure): make -C oracle. Without the reference's source tree a
+    library built earlier is kept; without either, the tests that need it skip."""
+    target = os.path.join(ORACLE, "_ref", "libluna_ref.so")
+    cmd = ["make", "-s", "-C", ORACLE, "-j3"] + (["-B"] if force else [])
+    try:
+        _run(cmd)
+    except subprocess.CalledProcessError:
+        print("the reference's solver was not built (its source tree is not here)"
+              + ("; keeping the library built earlier" if os.path.exists(target) else ""), flush=True)
+    return target
+
+
 def build_all(force=False):
     build_mesh(force)
     build_oracle(force)
+    build_reference(force)
     build_hydro(force)
 
 
 if __name__ == "__main__":
     what = sys.argv[1] if len(sys.argv) > 1 else "all"
     force = "--force" in sys.argv
-    {"all": build_all, "hydro": build_hydro, "mesh": build_mesh, "oracle": build_oracle}[what](force)
+    {"all": build_all, "hydro": build_hydro, "mesh": build_mesh, "oracle": build_oracle,
+     "reference": build_reference}[what](force)
