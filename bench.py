@@ -38,10 +38,12 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--nx", type=int, default=128)
     ap.add_argument("--impl", default="luna", choices=["luna", "reference"])
-    ap.add_argument("--cpu-sample-steps", type=int, default=3)
+    ap.add_argument("--cpu-sample-steps", type=int, default=5)
+    ap.add_argument("--cpu-warmup", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="leave out the learned limiter's section")
     ap.add_argument("--no-moving", action="store_true", help="leave out the moving-mesh section")
+    ap.add_argument("--no-adjoint", action="store_true", help="leave out the adjoint's cost")
     ap.add_argument("--moving-steps", type=int, default=5)
     ap.add_argument("--curve", default="row", choices=["row", "morton", "hilbert"],
                     help="the cells' numbering along a space-filling curve (voronoi-cpp's Layout::curve)")
@@ -153,51 +155,75 @@ def build_workload(nx: int, threads: int, curve: str = "row"):
     return mesh, point_blast(mesh)
 
 
-def cpu_baseline(mesh, q0, steps: int, threads: int):
-    """The CPU oracle (a restatement of the reference's step; the reference itself needs Kokkos and voronoi-cpp, absent
-    here) on the same mesh and state, all its steps timed after one warm-up step."""
+def workload_name(nx: int) -> str:
+    """The configuration both arms run (the same string in both JSON lines)."""
+    return (f"3D static Voronoi {nx}^3 jittered (0.1) point blast, MUSCL-Hancock + HLLC, face-centroid limiter, CFL 0.3, "
+            "FP64, one step = time_step + step")
+
+
+def cpu_solver(mesh, threads: int):
+    """The reference's CPU path of the step on this mesh: its own FiniteVolume<3> built on the CPU (oracle/_ref, OpenMP)
+    where that library exists, else the C restatement of it (the oracle port, OpenMP). OMP_PROC_BIND=close is set before
+    either OpenMP runtime starts."""
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    from oracle import ref as R
+
+    if R.available():
+        used = R.threads(threads)
+        return R.ReferenceFV(mesh), "reference", used
     from oracle import oracle as O
 
     used = O.threads(threads)
-    fv = O.OracleFV(mesh)
-    fv.set_state(q0)
-    fv.step(fv.time_step(0.3))
-    t0 = time.perf_counter()
-    for _ in range(steps):
+    return O.OracleFV(mesh), "port", used
+
+
+def cpu_steps(fv, steps: int, warmup: int) -> list:
+    """Wall time of each of `steps` whole steps (time_step + step) after `warmup` untimed ones."""
+    for _ in range(warmup):
         fv.step(fv.time_step(0.3))
-    t = time.perf_counter() - t0
-    return {"value": mesh.n_cells * steps / t, "unit": UNIT, "cores": used, "kind": "port",
-            "sample": f"{steps} oracle steps (after 1 warm-up) of the same {mesh.n_cells}-cell mesh and state",
-            "ms_per_step": 1e3 * t / steps}
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        fv.step(fv.time_step(0.3))
+        times.append(time.perf_counter() - t0)
+    return times
+
+
+def cpu_baseline(mesh, q0, steps: int, warmup: int, threads: int):
+    """The reference's CPU path on the same mesh and state: the median of `steps` step times after `warmup` steps."""
+    fv, kind, used = cpu_solver(mesh, threads)
+    fv.set_state(q0)
+    times = cpu_steps(fv, steps, warmup)
+    med = float(np.median(times))
+    what = "the reference's FiniteVolume<3> built on the CPU" if kind == "reference" else "the oracle port"
+    return {"value": mesh.n_cells / med, "unit": UNIT, "cores": used, "kind": kind,
+            "sample": f"median of {steps} steps of {what} after {warmup} warm-up steps, the same {mesh.n_cells}-cell "
+                      f"mesh and state, OMP_PROC_BIND={os.environ.get('OMP_PROC_BIND')}",
+            "ms_per_step": 1e3 * med}
 
 
 def run_reference(args, rank, world):
-    """--impl reference: the CPU implementation of the path (the oracle port: the reference's own build needs Kokkos and
-    voronoi-cpp), all host threads, on the same workload; rank 0 only."""
+    """--impl reference: the reference's CPU path of the step (its own FiniteVolume<3> built on the CPU with OpenMP, or
+    the oracle port where that library is absent), all host threads, on the same workload; rank 0 only. Each step is
+    timed on its own; the value is the cells over the median step time."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
     mesh, q0 = build_workload(args.nx, threads, args.curve)
-    from oracle import oracle as O
-
-    used = O.threads(threads)
-    fv = O.OracleFV(mesh)
+    fv, kind, used = cpu_solver(mesh, threads)
     fv.set_state(q0)
-    for _ in range(args.warmup):
-        fv.step(fv.time_step(0.3))
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        fv.step(fv.time_step(0.3))
-    t = time.perf_counter() - t0
-    value = mesh.n_cells * args.steps / t
+    times = cpu_steps(fv, args.steps, args.warmup)
+    med = float(np.median(times))
+    value = mesh.n_cells / med
+    what = "the reference's FiniteVolume<3> built on the CPU" if kind == "reference" else "the oracle port"
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": 1e3 * med, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": f"3D static Voronoi {args.nx}^3 jittered (0.1) point blast, MUSCL-Hancock + HLLC, "
-                                   "face-centroid limiter, CFL 0.3, FP64", "n_cells": mesh.n_cells,
-                       "n_faces": mesh.n_faces, "parallelism": "replicas"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": "port",
-                             "sample": f"{args.steps} full oracle steps after {args.warmup} warm-up steps"},
+            "config": {"workload": workload_name(args.nx), "n_cells": mesh.n_cells, "n_faces": mesh.n_faces,
+                       "parallelism": "replicas"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": kind,
+                             "sample": f"median of {args.steps} steps of {what} after {args.warmup} warm-up steps, "
+                                       f"OMP_PROC_BIND={os.environ.get('OMP_PROC_BIND')}"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -275,6 +301,36 @@ def moving_section(nx, steps, warmup) -> dict:
     fv.close()
     remesher.close()
     return out
+
+
+def adjoint_section(mesh, q0, steps, warmup, stream, torch) -> dict:
+    """The adjoint's cost on the bench mesh, FP64: device time of step_adjoint (primitives and the sweep recomputed with
+    the fit kept, the faces' Riemann adjoints, the cells' adjoints, the gather) against the forward step (time_step +
+    step), both over `steps` calls after `warmup`, CUDA events on the library's stream. The reference measures 2.46x
+    (its step_adjoint against its step at 128^3 in double, A100)."""
+    from luna_cpp_b200 import hydro
+
+    fv = hydro.FiniteVolume(mesh)
+    fv.set_stream(stream)
+    fv.set_state(q0)
+    for _ in range(warmup):
+        fv.step(fv.time_step(0.3))
+    fwd_ms = timed_steps(fv, steps, torch) / steps
+    dt = fv.time_step(0.3)
+    qbar = torch.randn(mesh.n_cells, 5, dtype=torch.float64, device="cuda") * 1e-3
+    for _ in range(2):
+        fv.step_adjoint(dt, qbar)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record()
+    for _ in range(steps):
+        fv.step_adjoint(dt, qbar)
+    end.record()
+    torch.cuda.synchronize()
+    adj_ms = start.elapsed_time(end) / steps
+    fv.close()
+    return {"step_ms": fwd_ms, "step_adjoint_ms": adj_ms, "ratio": adj_ms / fwd_ms, "reference_ratio": 2.46,
+            "finite": bool(torch.isfinite(qbar).all().item())}
 
 
 def timed_steps(fv, steps, torch):
@@ -392,8 +448,7 @@ def main():
             "dtype": "f64",
             "data": "synthetic",
             "config": {
-                "workload": f"3D static Voronoi {args.nx}^3 jittered (0.1) point blast, MUSCL-Hancock + HLLC, "
-                            "face-centroid limiter, CFL 0.3, FP64 (time_step + step)",
+                "workload": workload_name(args.nx),
                 "n_cells": N, "n_faces": F, "faces_per_cell": F / N, "parallelism": f"replicas x{world}",
                 "l2": "inputs larger than L2 (working set ~3 GB > 126 MB), no flush",
             },
@@ -422,10 +477,12 @@ def main():
         }
         if world == 1 and not args.no_learned:
             line["learned_limiter"] = learned_section(mesh, q0, args.steps, args.warmup, stream, torch)
+        if world == 1 and not args.no_adjoint:
+            line["adjoint_cost"] = adjoint_section(mesh, q0, args.steps, args.warmup, stream, torch)
         if world == 1 and not args.no_moving:
             line["moving"] = moving_section(args.nx, args.moving_steps, 2)
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(mesh, q0, args.cpu_sample_steps, os.cpu_count() or 1)
+            line["cpu_baseline"] = cpu_baseline(mesh, q0, args.cpu_sample_steps, args.cpu_warmup, os.cpu_count() or 1)
         print(json.dumps(line), flush=True)
     for r in results.values():
         r["fv"].close()

@@ -1,5 +1,5 @@
-"""bench.py's contract on the CPU: the reference arm's JSON line (the oracle port on the host cores, run by rank 0
-alone under torchrun) and the cross-rank maximum the GPU arm takes of its timings (world size 2 over gloo)."""
+"""bench.py's contract on the CPU: the reference arm's JSON line (the reference's own solver built on the CPU, or the
+oracle port where that library is absent, on the host cores, run by rank 0 alone under torchrun) and the cross-rank maximum the GPU arm takes of its timings (world size 2 over gloo)."""
 import json
 import os
 import subprocess
@@ -21,7 +21,11 @@ def test_reference_arm_line():
     line = json.loads(r.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["unit"] == "cell-updates/s" and line["value"] > 0
     assert line["steps"] == 2 and line["warmup"] == 1 and line["higher_is_better"] is True
-    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["value"] == line["value"]
+    from oracle import ref as R
+
+    assert line["cpu_baseline"]["kind"] == ("reference" if R.available() else "port")
+    assert line["cpu_baseline"]["value"] == line["value"]
+    assert line["config"]["workload"].startswith("3D static Voronoi 8^3")
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
 
 
