@@ -163,6 +163,11 @@ LUNA_API luna_status luna_fv_limiter_inputs(luna_fv* fv, void* features, double*
  * (targets t and weights w FP32 [n][5]) into grad, the loss into *loss (device); workspace of
  * luna_mlp_train_workspace_floats(n) floats; deterministic. adam: one Adam update (step counts from 1). */
 LUNA_API int64_t luna_mlp_param_count(void);
+/* The polls a tensor-core completion wait of the learned limiter's forward makes before it gives up (LUNA_ETIMEOUT from
+ * luna_mlp_forward and from the learned step's luna_fv_time_step), for every later launch in this process; < 0 restores
+ * the default (2^22). After giving up, a CTA still waits for its MMA in flight with the default bound before it frees
+ * tensor memory. Returns the previous limit. No counterpart in the reference (it has no learned limiter). */
+LUNA_API int luna_mlp_set_wait_limit(int polls);
 LUNA_API int64_t luna_mlp_train_workspace_floats(int64_t n);
 LUNA_API luna_status luna_mlp_forward(const float* params, const void* features, int64_t n, float* logits, void* stream);
 LUNA_API luna_status luna_mlp_train_step(const float* params, const void* features, const float* target, const float* weight, int64_t n,

@@ -29,6 +29,9 @@ luna_status check_launch(const char* what) {
 // The standalone forward's error word (luna_mlp_forward).
 __device__ unsigned long long g_forward_error;
 
+// Polls of an MMA-completion wait before it gives up (luna_mlp_set_wait_limit).
+int g_wait_limit = luna::mlp::kTcWaitLimit;
+
 }  // namespace
 
 namespace luna {
@@ -48,7 +51,7 @@ luna_status forward_tc(const float* params, const __nv_bfloat16* x, int n, const
     // each; 4 fill it)
     const int64_t tiles = (static_cast<int64_t>(n) + kTcRows - 1) / kTcRows;
     const int blocks = static_cast<int>(tiles < 148 * LUNA_MLP_CTAS_PER_SM ? tiles : 148 * LUNA_MLP_CTAS_PER_SM);
-    k_mlp_forward_tc<<<blocks, 128, smem, stream>>>(params, x, n, rows, logits, error);
+    k_mlp_forward_tc<<<blocks, 128, smem, stream>>>(params, x, n, rows, logits, error, g_wait_limit);
     return check_launch("k_mlp_forward_tc");
 }
 
@@ -58,6 +61,12 @@ luna_status forward_tc(const float* params, const __nv_bfloat16* x, int n, const
 extern "C" {
 
 LUNA_API int64_t luna_mlp_param_count(void) { return luna::mlp::kParams; }
+
+LUNA_API int luna_mlp_set_wait_limit(int polls) {
+    const int previous = g_wait_limit;
+    g_wait_limit = polls < 0 ? luna::mlp::kTcWaitLimit : polls;
+    return previous;
+}
 
 LUNA_API int64_t luna_mlp_train_workspace_floats(int64_t n) {
     const int64_t blocks = (n + luna::mlp::kRowsPerBlock - 1) / luna::mlp::kRowsPerBlock;

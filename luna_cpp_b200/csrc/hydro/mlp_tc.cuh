@@ -20,7 +20,9 @@ namespace mlp {
 
 constexpr int kTcRows = 128;       // rows of a tile: the MMA's M
 constexpr int kTcCols = 128;       // TMEM columns a CTA holds: D1 (and D3) at 0, D2 at 64
-constexpr int kTcWaitLimit = 1 << 22;  // mbarrier polls before a wait gives up (an error bit, not a hang)
+constexpr int kTcWaitLimit = 1 << 22;  // mbarrier polls before a wait gives up (an error bit, not a hang); the
+                                       // default of the per-launch limit of the first waits (set_wait_limit), and
+                                       // always the bound of the last wait before TMEM is freed
 constexpr unsigned long long kTcTimeoutBit = 16ull;
 
 struct __align__(128) SmemTc {
@@ -98,11 +100,11 @@ __device__ __forceinline__ void tc_load16(uint32_t taddr, float* v) {
     for (int c = 0; c < 16; ++c) v[c] = __uint_as_float(r[c]);
 }
 
-// Waits for the MMA completion of this phase, polling a bounded number of times; every thread sees the same outcome.
-__device__ __forceinline__ bool tc_wait(SmemTc& s, uint32_t parity) {
+// Waits for the MMA completion of this phase, polling at most `limit` times; every thread sees the same outcome.
+__device__ __forceinline__ bool tc_wait(SmemTc& s, uint32_t parity, int limit) {
     const uint32_t mbar = smem_addr(&s.mbar);
     bool ok = false;
-    for (int it = 0; it < kTcWaitLimit && !ok; ++it) ok = mbar_try_wait(mbar, parity);
+    for (int it = 0; it < limit && !ok; ++it) ok = mbar_try_wait(mbar, parity);
     if (!ok) s.failed = 1;
     __syncthreads();
     return s.failed == 0;
@@ -133,10 +135,11 @@ __device__ __forceinline__ void tc_hidden_epilogue(uint32_t tbase, int col0, con
 // logits [n][16] of feature rows [n][32] (BF16). A grid-stride loop over tiles of 128 rows; 128 threads; dynamic shared
 // memory sizeof(SmemTc). rows (device, may be null): the rows are the first min(n, *rows), a count the previous launch on
 // the stream wrote; a CTA with no tile returns before it stages weights or allocates TMEM. error: bit kTcTimeoutBit
-// when a wait gave up (the CTA then stops and frees its TMEM).
+// when a wait gave up after wait_limit polls (the CTA then stops, waits for the MMA it issued with the full bound
+// kTcWaitLimit, and frees its TMEM: TMEM is never freed under an MMA in flight).
 static __global__ void __launch_bounds__(128, 1) k_mlp_forward_tc(const float* __restrict__ params, const __nv_bfloat16* __restrict__ x, int n,
                                                                   const unsigned int* __restrict__ rows, float* __restrict__ logits,
-                                                                  unsigned long long* __restrict__ error) {
+                                                                  unsigned long long* __restrict__ error, int wait_limit) {
     extern __shared__ __align__(128) unsigned char tc_smem[];
     SmemTc& s = *reinterpret_cast<SmemTc*>(tc_smem);
     const int tid = static_cast<int>(threadIdx.x), warp = tid >> 5;
@@ -193,7 +196,7 @@ static __global__ void __launch_bounds__(128, 1) k_mlp_forward_tc(const float* _
             for (int k = 0; k < kIn / 16; ++k) tc_mma(tbase, tc_operand(ax, k, kIn), tc_operand(aw1, k, kIn), tc_idesc(kTcRows, kHidden), k > 0);
             tc_commit(smem_addr(&s.mbar));
         }
-        if (!tc_wait(s, parity)) {
+        if (!tc_wait(s, parity, wait_limit)) {
             ok = false;
             break;
         }
@@ -210,7 +213,7 @@ static __global__ void __launch_bounds__(128, 1) k_mlp_forward_tc(const float* _
                 tc_mma(tbase + 64u, tc_operand(ah1, k, kHidden), tc_operand(aw2, k, kHidden), tc_idesc(kTcRows, kHidden), k > 0);
             tc_commit(smem_addr(&s.mbar));
         }
-        if (!tc_wait(s, parity)) {
+        if (!tc_wait(s, parity, wait_limit)) {
             ok = false;
             break;
         }
@@ -227,7 +230,7 @@ static __global__ void __launch_bounds__(128, 1) k_mlp_forward_tc(const float* _
                 tc_mma(tbase, tc_operand(ah2, k, kHidden), tc_operand(aw3, k, kHidden), tc_idesc(kTcRows, kOut), k > 0);
             tc_commit(smem_addr(&s.mbar));
         }
-        if (!tc_wait(s, parity)) {
+        if (!tc_wait(s, parity, wait_limit)) {
             ok = false;
             break;
         }

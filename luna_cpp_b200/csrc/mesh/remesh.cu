@@ -18,13 +18,9 @@
 
 #include "luna_b200.h"
 #include "luna_remesh.h"
-#include "remesh_warp.cuh"
 #include "voronoi_cell.h"
 #include "voronoi_grid.h"
 
-#ifndef LUNA_REMESH_WARP
-#define LUNA_REMESH_WARP 0  // 1: the fast path builds a 3D cell with a warp (remesh_warp.cuh); 0: with one thread
-#endif
 #ifndef LUNA_REMESH_DUAL
 #define LUNA_REMESH_DUAL 0  // 1: 3D cells kept as triangles of plane triples (DualT), as the host builder's LUNA_MESH_DUAL=1
 #endif
@@ -203,52 +199,6 @@ __global__ void __launch_bounds__(128) k_cells(int64_t n, const int32_t* __restr
             out.fa[D * r + a] = faces.a[f][a];
             out.fc[D * r + a] = faces.c[f][a];
         }
-    }
-}
-
-constexpr int kWarpsPerBlock = 4;
-
-// The fast path of 3D cells, one warp a cell, the warps striding over the cells (WarpCell in shared memory); the
-// cells it hands on go to the retry list for k_cells<3, true>.
-__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_cells_warp(int64_t n, const double* __restrict__ pos, Box box, Grid g, CellOut out,
-                                                                   Counters* c, int32_t* __restrict__ retry) {
-    extern __shared__ double2 warp_cells[];
-    WarpCell& w = reinterpret_cast<WarpCell*>(warp_cells)[threadIdx.x >> 5];
-    const int lane = threadIdx.x & 31;
-    const int64_t warps = static_cast<int64_t>(gridDim.x) * kWarpsPerBlock;
-    for (int64_t i = static_cast<int64_t>(blockIdx.x) * kWarpsPerBlock + (threadIdx.x >> 5); i < n; i += warps) {
-        double volume = 0, centroid[3] = {0, 0, 0};
-        const int code = warp_build_cell(i, pos, box.s, g, w, volume, centroid, lane);
-        unsigned long long base = 0;
-        if (lane == 0) {
-            if (code != kCellOk) {
-                out.first[i] = 0;
-                out.count[i] = 0;
-                if (code == kOutOfOffsets || code == kCandidates)
-                    retry[atomicAdd(&c->retry, 1u)] = static_cast<int32_t>(i);
-                else if (atomicCAS(&c->error, 0, code) == 0)
-                    c->error_cell = static_cast<int>(i);
-            } else {
-                out.volume[i] = volume;
-                for (int a = 0; a < 3; ++a) out.centroid[3 * i + a] = centroid[a];
-                base = atomicAdd(&c->faces, static_cast<unsigned long long>(w.faces.n));
-                out.first[i] = static_cast<int64_t>(base);
-                out.count[i] = w.faces.n;
-            }
-        }
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (code == kCellOk && base + w.faces.n <= out.capacity) {
-            for (int e = lane; e < w.faces.n; e += 32) {
-                const int f = w.faces.order[e];
-                const int64_t r = static_cast<int64_t>(base) + e;
-                out.fj[r] = w.faces.j[f];
-                for (int a = 0; a < 3; ++a) {
-                    out.fa[3 * r + a] = w.faces.a[f][a];
-                    out.fc[3 * r + a] = w.faces.c[f][a];
-                }
-            }
-        }
-        __syncwarp();
     }
 }
 
@@ -524,19 +474,7 @@ luna_status luna_remesh::build(int64_t n, const double* points, bool on_device, 
         RM_TRY(fc.reserve(capacity * D, "face records"));
         if (attempt > 0) RM_CUDA(cudaMemsetAsync(counters.ptr, 0, sizeof(Counters), stream));
         const CellOut out{volume.ptr, centroid.ptr, first.ptr, count.ptr, fj.ptr, fa.ptr, fc.ptr, capacity};
-        if (LUNA_REMESH_WARP && D == 3) {
-            const size_t smem = sizeof(WarpCell) * kWarpsPerBlock;
-            RM_CUDA(cudaFuncSetAttribute(k_cells_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-            int device = 0, sms = 0, per_sm = 0;
-            RM_CUDA(cudaGetDevice(&device));
-            RM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-            RM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cells_warp, 32 * kWarpsPerBlock, smem));
-            const int64_t wanted = (n + kWarpsPerBlock - 1) / kWarpsPerBlock, most = static_cast<int64_t>(sms) * (per_sm > 0 ? per_sm : 1);
-            k_cells_warp<<<static_cast<unsigned int>(wanted < most ? wanted : most), 32 * kWarpsPerBlock, smem, stream>>>(n, pos.ptr, box, g, out,
-                                                                                                                    counters.ptr, retry.ptr);
-        } else {
-            k_cells<D, false><<<grid_blocks(n, 128), 128, 0, stream>>>(n, nullptr, pos.ptr, box, g, out, counters.ptr, retry.ptr);
-        }
+        k_cells<D, false><<<grid_blocks(n, 128), 128, 0, stream>>>(n, nullptr, pos.ptr, box, g, out, counters.ptr, retry.ptr);
         RM_CUDA(cudaGetLastError());
         RM_CUDA(cudaMemcpyAsync(&h, counters.ptr, sizeof(Counters), cudaMemcpyDeviceToHost, stream));
         RM_CUDA(cudaStreamSynchronize(stream));

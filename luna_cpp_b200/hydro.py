@@ -85,6 +85,7 @@ SIGNATURES = {
     "luna_fv_set_limiter_mlp": ([P, P, I], I),
     "luna_fv_limiter_inputs": ([P, P, P, P], I),
     "luna_mlp_param_count": ([], I64),
+    "luna_mlp_set_wait_limit": ([I], I),
     "luna_mlp_train_workspace_floats": ([I64], I64),
     "luna_mlp_forward": ([P, P, I64, P, P], I),
     "luna_mlp_train_step": ([P, P, P, P, I64, ctypes.c_float, P, P, P, I64, P], I),

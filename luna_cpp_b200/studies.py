@@ -15,7 +15,7 @@ comparisons of the same configurations are GPU tests).
   resolution per axis, beside the plain limiter at the same and at finer resolutions, with device times; the GPU time
   the plain limiter needs for the learned limiter's error, over the learned run's.
 - ``lines``: the 1D solver as the learned limiter's data factory: a batch of seeded Riemann problems on lines of nx
-  cells, one launch a step; cell-updates/s beside the oracle's on one line.
+  cells, one launch a step; cell-updates/s.
 - ``adjoint``: 2D Voronoi mesh from nx^2 jittered generators, the shear layer with a_k ~ N(0, 1) from the seed, 200
   steps; d/da_k of int rho vy^2 dA at the final time by the hand-written adjoint with checkpoints every 20 steps,
   against central differences (h = 1e-6) on the same dt schedule; device time of the forward and of the backward.
@@ -313,11 +313,8 @@ def learned_blast(nx=48, factor=4, plain_nx=(48, 56, 64, 72, 80), t_end=0.05, co
 def lines(nx=4096, batch=1024, steps=200, courant=0.8, seed=9000, log=print) -> dict:
     """The 1D solver as the learned limiter's data factory: ``batch`` seeded Riemann problems (the training
     distribution) on lines of nx uniform cells between outflow walls, all in one launch a step: ``steps`` fused steps
-    (step_and_time_step, LUNA's rule), device time by CUDA events, cell-updates/s; and the oracle on one of the lines for
-    the CPU's rate."""
+    (step_and_time_step, LUNA's rule), device time by CUDA events, cell-updates/s."""
     import torch
-
-    from oracle import oracle as O
 
     from .limiter_training import riemann_problem
     from .line import Line
@@ -342,19 +339,10 @@ def lines(nx=4096, batch=1024, steps=200, courant=0.8, seed=9000, log=print) -> 
     ms = start.elapsed_time(end)
     q = ln.get_state()
     ln.close()
-    ref = O.OracleLine(keys, step, period, gamma=1.4)
-    ref.set_state(q0[0])
-    t0 = time.perf_counter()
-    cpu_steps = 20
-    for _ in range(cpu_steps):
-        ref.step(ref.time_step(courant, "luna"))
-    cpu_s = time.perf_counter() - t0
     out = {"config": {"cells": nx, "lines": batch, "steps": steps, "courant": courant, "rule": "luna", "fused": True},
            "device_ms_per_step": ms / steps, "cell_updates_per_s": nx * batch * steps / (ms * 1e-3),
-           "finite": bool(np.all(np.isfinite(q))),
-           "oracle_cell_updates_per_s": nx * cpu_steps / cpu_s, "oracle_threads": O.threads(0)}
-    log(f"{batch} lines x {nx} cells: {ms / steps:.3f} ms/step, {out['cell_updates_per_s'] / 1e9:.2f} G cell-updates/s "
-        f"(oracle, one line: {out['oracle_cell_updates_per_s'] / 1e6:.1f} M/s)")
+           "finite": bool(np.all(np.isfinite(q)))}
+    log(f"{batch} lines x {nx} cells: {ms / steps:.3f} ms/step, {out['cell_updates_per_s'] / 1e9:.2f} G cell-updates/s")
     return out
 
 

@@ -28,7 +28,9 @@ def parse(text, name):
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2:
+        sys.exit("usage: python tests/golden/make_golden.py <luna-cpp source tree>")
+    root = sys.argv[1]
     with open(os.path.join(root, "src/test/hydro_test.cpp")) as f:
         text = f.read()
     out = {

@@ -164,3 +164,34 @@ def test_tensor_core_forward_tiles(cuda, n):
     want, _ = M.forward(p, x)
     assert logits.shape == (n, M.OUT)
     assert rel(logits, want) < 2e-3
+
+
+def test_tensor_core_wait_that_runs_out_reports_a_timeout(cuda):
+    """The bounded MMA-completion wait made to run out (no polls allowed): luna_mlp_forward returns LUNA_ETIMEOUT, the
+    CTAs still wait for their MMAs in flight (full bound) and free tensor memory, and the context stays usable: the next
+    forward with the default limit matches the oracle. Nothing faults or hangs: the MMAs complete; only the first wait
+    is told to give up."""
+    import ctypes
+
+    import torch
+
+    from luna_cpp_b200 import hydro
+    from luna_cpp_b200.learned import LimiterMLP, init_params
+
+    lib = hydro.lib()
+    x, _, _ = data(1000, seed=5)
+    p = init_params(3)
+    net = LimiterMLP(p)
+    feats = torch.tensor(x, device="cuda").to(torch.bfloat16)
+    logits = torch.empty((1000, M.OUT), dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    previous = lib.luna_mlp_set_wait_limit(0)
+    try:
+        status = lib.luna_mlp_forward(ctypes.c_void_p(net.params.data_ptr()), ctypes.c_void_p(feats.data_ptr()), 1000,
+                                      ctypes.c_void_p(logits.data_ptr()), ctypes.c_void_p(stream))
+    finally:
+        lib.luna_mlp_set_wait_limit(previous)
+    assert status == 5, (status, lib.luna_last_error())  # LUNA_ETIMEOUT
+    assert b"gave up" in lib.luna_last_error()
+    want, _ = M.forward(p, x)
+    assert rel(net.forward(feats).cpu().numpy(), want) < 2e-3
