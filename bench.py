@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--moving-steps", type=int, default=5)
     ap.add_argument("--curve", default="row", choices=["row", "morton", "hilbert"],
                     help="the cells' numbering along a space-filling curve (voronoi-cpp's Layout::curve)")
-    ap.add_argument("--precision", default="both", choices=["both", "fp64", "fp32", "grad16"],
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "fp32", "single", "grad16"],
                     help="which policies to time (the JSON line needs both; one is for profiling runs)")
     return ap.parse_args()
 
@@ -374,7 +374,7 @@ def main():
             dist.barrier()
 
     results = {}
-    for prec in ("fp32", "grad16", "fp64") if args.precision == "both" else (args.precision,):
+    for prec in ("single", "fp32", "grad16", "fp64") if args.precision == "both" else (args.precision,):
         fv = hydro.FiniteVolume(mesh, precision=prec)
         fv.set_stream(stream)
         fv.set_state(q0)
@@ -433,7 +433,8 @@ def main():
         step_s = r64["ms"] / args.steps / 1e3
         launches = sum(v[1] for v in phases.values())
         value = world * N * args.steps / (r64["ms"] / 1e3)
-        fp32_value = world * N * args.steps / (results["fp32"]["ms"] / 1e3)
+        fp32_value = world * N * args.steps / (results["single"]["ms"] / 1e3)
+        r32_value = world * N * args.steps / (results["fp32"]["ms"] / 1e3)
         line = {
             "metric": METRIC,
             "value": value,
@@ -453,9 +454,16 @@ def main():
                 "l2": "inputs larger than L2 (working set ~3 GB > 126 MB), no flush",
             },
             "face_fluxes_per_s": world * F * args.steps / (r64["ms"] / 1e3),
-            "fp32": {"value": fp32_value, "ms_per_step": results["fp32"]["ms"] / args.steps,
+            "fp32": {"policy": "single: the reference's Precision<double, float, float, float> (gradients, limiter, face "
+                               "states and the Riemann solve in float, flux rows stored in float, geometry, primitives and "
+                               "the per-cell sums in double)",
+                     "value": fp32_value, "ms_per_step": results["single"]["ms"] / args.steps,
                      "speedup_vs_fp64": fp32_value / value,
-                     "phases_ms_per_step": {k: v[0] / args.steps for k, v in results["fp32"]["phases"].items()}},
+                     "phases_ms_per_step": {k: v[0] / args.steps for k, v in results["single"]["phases"].items()}},
+            "riemann32": {"policy": "riemann32: Precision<double, float, double, float> (as single, flux rows in double)",
+                          "value": r32_value, "ms_per_step": results["fp32"]["ms"] / args.steps,
+                          "speedup_vs_fp64": r32_value / value,
+                          "phases_ms_per_step": {k: v[0] / args.steps for k, v in results["fp32"]["phases"].items()}},
             "grad16": {"policy": "the reference's 3D default (Grad16: binary16 gradient rows, float limiter, double Riemann)",
                        "value": world * N * args.steps / (results["grad16"]["ms"] / 1e3),
                        "ms_per_step": results["grad16"]["ms"] / args.steps,

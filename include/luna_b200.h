@@ -47,7 +47,10 @@ enum { LUNA_HLLC = 0, LUNA_HLL = 1 };                                   /* Riema
  * per-cell accumulation in double. LUNA_GRAD32 is the reference's Grad32 (precision.hpp:43): float gradients, limiter and
  * face-state change, a double Riemann solve (it keeps perturbations far below float's resolution of the state, which
  * a float Riemann solve cannot). The reduced policies take HLLC only, as the reference's presets. */
-enum { LUNA_FP64 = 0, LUNA_FP32 = 1, LUNA_GRAD32 = 2, LUNA_GRAD16 = 3 };
+enum { LUNA_FP64 = 0, LUNA_FP32 = 1, LUNA_GRAD32 = 2, LUNA_GRAD16 = 3, LUNA_SINGLE = 4 };
+/* LUNA_SINGLE is the reference's `single` preset Precision<double, float, float, float> (hydro_sedov.cpp:423): LUNA_FP32
+ * with the per-face flux rows stored in float (each flux rounded once, summed per cell in double), 32 B a row in 3D
+ * instead of 40; the per-cell loop stores no rows, so there it is LUNA_FP32. */
 /* LUNA_GRAD16 is the reference's Grad16 (precision.hpp:47, its 3D default): Grad32 with the gradient rows stored as
  * binary16 (32 B a row) and one power-of-two exponent per group rho, v, P (4 B a cell). */
 

@@ -764,8 +764,8 @@ __global__ void k_apply_factors(int rows, const int* __restrict__ cells, const u
 #ifndef LUNA_FLUX_MIN_BLOCKS
 #define LUNA_FLUX_MIN_BLOCKS 6
 #endif
-template <int D, int Order, class G, bool RF, int Riemann, bool H = false, bool WG = false>
-__global__ void __launch_bounds__(128, LUNA_FLUX_MIN_BLOCKS) k_flux_rows(MeshDev<D> m, GeometryDev<D, G> geo, FluxArgs<D, G> x, double* __restrict__ flux,
+template <int D, int Order, class G, bool RF, int Riemann, bool H = false, bool WG = false, class FS = double>
+__global__ void __launch_bounds__(128, LUNA_FLUX_MIN_BLOCKS) k_flux_rows(MeshDev<D> m, GeometryDev<D, G> geo, FluxArgs<D, G> x, FS* __restrict__ flux,
                                                    unsigned long long* __restrict__ fallbacks) {
     constexpr int V = D + 2;
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
@@ -813,8 +813,7 @@ __global__ void __launch_bounds__(128, LUNA_FLUX_MIN_BLOCKS) k_flux_rows(MeshDev
 #pragma unroll
             for (int v = 0; v < V; ++v) F[v] *= r.mag;
         }
-#pragma unroll
-        for (int v = 0; v < V; ++v) flux[V * static_cast<int64_t>(f) + v] = F[v];
+        store_flux_row<D, FS>(flux, f, F);
     }
     block_sum_to(static_cast<unsigned long long>(count), fallbacks);
 }

@@ -526,9 +526,33 @@ __device__ __forceinline__ void face_flux(const MeshDev<D>& m, const FluxArgs<D,
     for (int v = 0; v < V; ++v) F[v] *= magnitude;
 }
 
+// Flux rows in the precision policy's flux storage (Precision::flux, precision.hpp:26-39; FaceFluxes, finite_volume.hpp:65):
+// double rows of V values, or float rows rounded once as the reference's static_cast<FluxStore> does, padded to 8 floats
+// (3D, one 32-B sector) or 4 (2D, 16 B) so that a row is one aligned vector store and one aligned vector load.
+template <int D, class FS>
+__host__ __device__ constexpr int flux_stride() {
+    return sizeof(FS) == sizeof(double) ? D + 2 : (D == 3 ? 8 : 4);
+}
+template <int D, class FS>
+__device__ __forceinline__ void store_flux_row(FS* flux, int64_t f, const double* F) {
+    constexpr int V = D + 2;
+    if constexpr (sizeof(FS) == sizeof(double)) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) flux[V * f + v] = F[v];
+    } else {
+        constexpr int S = flux_stride<D, FS>();
+        float r[S];
+#pragma unroll
+        for (int c = 0; c < S; ++c) r[c] = c < V ? static_cast<float>(F[c]) : 0.0f;
+        float4* p = reinterpret_cast<float4*>(flux + S * f);
+#pragma unroll
+        for (int c = 0; c < S; c += 4) p[c / 4] = make_float4(r[c], r[c + 1], r[c + 2], r[c + 3]);
+    }
+}
+
 // apply()'s flux pass (finite_volume.hpp:1591-1602): one flux row per face.
-template <int D, int Order, int Pass, class G, bool RF, int Riemann, bool H = false>
-__global__ void __launch_bounds__(128) k_flux(MeshDev<D> m, FluxArgs<D, G> x, double* __restrict__ flux,
+template <int D, int Order, int Pass, class G, bool RF, int Riemann, bool H = false, class FS = double>
+__global__ void __launch_bounds__(128) k_flux(MeshDev<D> m, FluxArgs<D, G> x, FS* __restrict__ flux,
                                               unsigned long long* __restrict__ fallbacks) {
     constexpr int V = D + 2;
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
@@ -536,8 +560,7 @@ __global__ void __launch_bounds__(128) k_flux(MeshDev<D> m, FluxArgs<D, G> x, do
     if (f < m.f) {
         double F[V];
         face_flux<D, Order, Pass, G, RF, Riemann, H>(m, x, f, F, count, count);
-#pragma unroll
-        for (int v = 0; v < V; ++v) flux[V * static_cast<int64_t>(f) + v] = F[v];
+        store_flux_row<D, FS>(flux, f, F);
     }
     block_sum_to(static_cast<unsigned long long>(count), fallbacks);
 }
@@ -581,8 +604,10 @@ __device__ __forceinline__ void load_row_windowed(const double* p, double* row) 
 #ifndef LUNA_UPDATE_BATCH
 #define LUNA_UPDATE_BATCH 2
 #endif
-template <int D, bool NextPrims, bool Windowed = false>
-__global__ void __launch_bounds__(256, Windowed ? LUNA_UPDATE_MIN_BLOCKS : 1) k_update(MeshDev<D> m, double* __restrict__ q, const double* __restrict__ flux, double dt,
+// FS = float: the rows of store_flux_row, one aligned vector load each, widened to double before the sum (the
+// reference's static_cast<double>(F(f, v)), finite_volume.hpp:1607).
+template <int D, bool NextPrims, bool Windowed = false, class FS = double>
+__global__ void __launch_bounds__(256, Windowed ? LUNA_UPDATE_MIN_BLOCKS : 1) k_update(MeshDev<D> m, double* __restrict__ q, const FS* __restrict__ flux, double dt,
                                                 double* __restrict__ prims, GasDev gas, Counters* __restrict__ ctr) {
     constexpr int V = D + 2;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -602,12 +627,26 @@ __global__ void __launch_bounds__(256, Windowed ? LUNA_UPDATE_MIN_BLOCKS : 1) k_
 #pragma unroll
         for (int b = 0; b < kBatch; ++b) {
             if (k0 + b < end) {
-                const double* r = flux + V * static_cast<int64_t>(list_face(e[b]));
-                if constexpr (Windowed) {
-                    load_row_windowed<V>(r, row[b]);
-                } else {
+                if constexpr (sizeof(FS) == sizeof(float)) {
+                    constexpr int S = flux_stride<D, FS>();
+                    const float* r = reinterpret_cast<const float*>(flux) + S * static_cast<int64_t>(list_face(e[b]));
+                    float w[8];
+                    if constexpr (S == 8) {
+                        ldg256(r, w);
+                    } else {
+                        const float4 t = __ldg(reinterpret_cast<const float4*>(r));
+                        w[0] = t.x, w[1] = t.y, w[2] = t.z, w[3] = t.w;
+                    }
 #pragma unroll
-                    for (int v = 0; v < V; ++v) row[b][v] = __ldg(r + v);
+                    for (int v = 0; v < V; ++v) row[b][v] = static_cast<double>(w[v]);
+                } else {
+                    const double* r = reinterpret_cast<const double*>(flux) + V * static_cast<int64_t>(list_face(e[b]));
+                    if constexpr (Windowed) {
+                        load_row_windowed<V>(r, row[b]);
+                    } else {
+#pragma unroll
+                        for (int v = 0; v < V; ++v) row[b][v] = __ldg(r + v);
+                    }
                 }
             }
         }

@@ -220,6 +220,11 @@ struct luna_fv {
     }
 };
 
+// The Riemann solve in float in the face's frame (riemann32 and single), and float flux rows (single).
+inline bool float_riemann(const luna_fv* fv) { return fv->precision == LUNA_FP32 || fv->precision == LUNA_SINGLE; }
+inline bool float_flux(const luna_fv* fv) { return fv->precision == LUNA_SINGLE; }
+
+
 namespace {
 
 template <class T>
@@ -459,7 +464,7 @@ luna_status launch_sweep_tiles(luna_fv* fv, G* grad, double courant) {
     const int64_t groups[2][2] = {{0, fv->normal_tiles}, {fv->normal_tiles, fv->tiles}};
     const int most_rows[2] = {fv->normal_rows, fv->big_rows};
     // the round-off of the face states, squared: double face states (FP64, grad32), float ones (riemann32)
-    const double round_off2 = fv->precision == LUNA_FP32 ? 0x1p-48 : 0x1p-100;
+    const double round_off2 = float_riemann(fv) ? 0x1p-48 : 0x1p-100;
     for (int k = 0; k < 2; ++k) {
         const int64_t first = groups[k][0], count = groups[k][1] - groups[k][0];
         if (count <= 0) continue;
@@ -541,21 +546,29 @@ luna_status launch_flux(luna_fv* fv, const luna::FluxArgs<D, G>& x) {
     if (fv->f == 0) return LUNA_OK;
     {
         const long timed_ = fv->open_timed(2);
-        luna::k_flux<D, Order, Pass, G, RF, Riemann, H><<<blocks(fv->f, kBlockFaces), kBlockFaces, 0, fv->stream>>>(
-            fv->mesh_dev<D>(), x, fv->flux.ptr, &fv->counters.ptr->fallbacks[Pass == 1 ? 1 : 0]);
+        bool single = false;
+        if constexpr (sizeof(G) == sizeof(float) && RF) {
+            single = float_flux(fv);
+            if (single)
+                luna::k_flux<D, Order, Pass, G, RF, Riemann, H, float><<<blocks(fv->f, kBlockFaces), kBlockFaces, 0, fv->stream>>>(
+                    fv->mesh_dev<D>(), x, reinterpret_cast<float*>(fv->flux.ptr), &fv->counters.ptr->fallbacks[Pass == 1 ? 1 : 0]);
+        }
+        if (!single)
+            luna::k_flux<D, Order, Pass, G, RF, Riemann, H><<<blocks(fv->f, kBlockFaces), kBlockFaces, 0, fv->stream>>>(
+                fv->mesh_dev<D>(), x, fv->flux.ptr, &fv->counters.ptr->fallbacks[Pass == 1 ? 1 : 0]);
         fv->close_timed(timed_);
     }
     LUNA_CUDA(cudaGetLastError());
     return LUNA_OK;
 }
 
-template <int D, int Order, class G, bool RF, int Riemann, bool H = false, bool WG = false>
+template <int D, int Order, class G, bool RF, int Riemann, bool H = false, bool WG = false, class FS = double>
 luna_status launch_flux_rows(luna_fv* fv, const luna::FluxArgs<D, G>& x) {
     if (fv->f == 0) return LUNA_OK;
     {
         const long timed_ = fv->open_timed(2);
-        luna::k_flux_rows<D, Order, G, RF, Riemann, H, WG><<<blocks(fv->f, kBlockFaces), kBlockFaces, 0, fv->stream>>>(
-            fv->mesh_dev<D>(), fv->geometry_dev<D, G>(), x, fv->flux.ptr, &fv->counters.ptr->fallbacks[0]);
+        luna::k_flux_rows<D, Order, G, RF, Riemann, H, WG, FS><<<blocks(fv->f, kBlockFaces), kBlockFaces, 0, fv->stream>>>(
+            fv->mesh_dev<D>(), fv->geometry_dev<D, G>(), x, reinterpret_cast<FS*>(fv->flux.ptr), &fv->counters.ptr->fallbacks[0]);
         fv->close_timed(timed_);
     }
     LUNA_CUDA(cudaGetLastError());
@@ -572,7 +585,8 @@ luna_status dispatch_flux_rows(luna_fv* fv, const luna::FluxArgs<D, G>& x) {
                                            : launch_flux_rows<D, Order, G, false, 0, false, true>(fv, y);
         }
     if (fv->precision == LUNA_GRAD16) return launch_flux_rows<D, Order, G, false, 0, true>(fv, x);
-    if (fv->precision == LUNA_FP32) return launch_flux_rows<D, Order, G, true, 0>(fv, x);
+    if (float_flux(fv)) return launch_flux_rows<D, Order, G, true, 0, false, false, float>(fv, x);
+    if (float_riemann(fv)) return launch_flux_rows<D, Order, G, true, 0>(fv, x);
     if (fv->riemann == LUNA_HLL) return launch_flux_rows<D, Order, G, false, 1>(fv, x);
     return launch_flux_rows<D, Order, G, false, 0>(fv, x);
 }
@@ -580,7 +594,7 @@ luna_status dispatch_flux_rows(luna_fv* fv, const luna::FluxArgs<D, G>& x) {
 template <int D, int Order, int Pass, class G>
 luna_status dispatch_flux(luna_fv* fv, const luna::FluxArgs<D, G>& x) {
     if (fv->precision == LUNA_GRAD16) return launch_flux<D, Order, Pass, G, false, 0, true>(fv, x);
-    if (fv->precision == LUNA_FP32) return launch_flux<D, Order, Pass, G, true, 0>(fv, x);
+    if (float_riemann(fv)) return launch_flux<D, Order, Pass, G, true, 0>(fv, x);
     if (fv->riemann == LUNA_HLL) return launch_flux<D, Order, Pass, G, false, 1>(fv, x);
     return launch_flux<D, Order, Pass, G, false, 0>(fv, x);
 }
@@ -617,17 +631,28 @@ luna::FluxArgs<D, G> flux_args(luna_fv* fv, const G* grad, double dt) {
     return x;
 }
 
+// apply()'s update of the library's flux rows (windowed double rows, or single's float rows).
+template <int D, bool NextPrims>
+void launch_update(luna_fv* fv, double dt) {
+    if (float_flux(fv))
+        luna::k_update<D, NextPrims, true, float><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(
+            fv->mesh_dev<D>(), fv->q.ptr, reinterpret_cast<const float*>(fv->flux.ptr), dt, fv->prims.ptr, fv->gas, fv->counters.ptr);
+    else
+        luna::k_update<D, NextPrims, true><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->q.ptr, fv->flux.ptr, dt, fv->prims.ptr,
+                                                                                      fv->gas, fv->counters.ptr);
+}
+
 // apply() for a static mesh (finite_volume.hpp:1538-1631).
 template <int D, class G>
 luna_status run_apply(luna_fv* fv, const G* grad, double dt) {
     const auto x = flux_args<D, G>(fv, grad, dt);
     if (fv->update == LUNA_UPDATE_PER_CELL) {
         if (fv->order == 0) {
-            if (fv->precision == LUNA_FP32) return launch_per_cell<D, 0, G, true, 0>(fv, x, dt);
+            if (float_riemann(fv)) return launch_per_cell<D, 0, G, true, 0>(fv, x, dt);
             if (fv->precision == LUNA_GRAD16) return launch_per_cell<D, 0, G, false, 0, true>(fv, x, dt);
             return fv->riemann == LUNA_HLL ? launch_per_cell<D, 0, G, false, 1>(fv, x, dt) : launch_per_cell<D, 0, G, false, 0>(fv, x, dt);
         }
-        if (fv->precision == LUNA_FP32) return launch_per_cell<D, 1, G, true, 0>(fv, x, dt);
+        if (float_riemann(fv)) return launch_per_cell<D, 1, G, true, 0>(fv, x, dt);
         if (fv->precision == LUNA_GRAD16) return launch_per_cell<D, 1, G, false, 0, true>(fv, x, dt);
         return fv->riemann == LUNA_HLL ? launch_per_cell<D, 1, G, false, 1>(fv, x, dt) : launch_per_cell<D, 1, G, false, 0>(fv, x, dt);
     }
@@ -637,8 +662,7 @@ luna_status run_apply(luna_fv* fv, const G* grad, double dt) {
         LUNA_TRY((dispatch_flux_rows<D, 1, G>(fv, x)));
     {
         const long timed_ = fv->open_timed(3);
-        luna::k_update<D, true, true><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->q.ptr, fv->flux.ptr, dt, fv->prims.ptr, fv->gas,
-                                                                            fv->counters.ptr);
+        launch_update<D, true>(fv, dt);
         fv->close_timed(timed_);
     }
     LUNA_CUDA(cudaGetLastError());
@@ -672,7 +696,7 @@ luna_status moving_begin(luna_fv* fv, double dt) {
     if (fv->precision != LUNA_FP64) {
         auto x = flux_args<D, float>(fv, fv->grad32.ptr, 0.0);
         x.unit = fv->grid_step / dt;
-        if (fv->precision == LUNA_FP32)
+        if (float_riemann(fv))
             LUNA_TRY((launch_flux<D, 1, 0, float, true, 0>(fv, x)));
         else if (fv->precision == LUNA_GRAD16)
             LUNA_TRY((launch_flux<D, 1, 0, float, false, 0, true>(fv, x)));
@@ -688,8 +712,7 @@ luna_status moving_begin(luna_fv* fv, double dt) {
     }
     {
         const long timed_ = fv->open_timed(3);
-        luna::k_update<D, false, true><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->q.ptr, fv->flux.ptr, 0.5 * dt, fv->prims.ptr, fv->gas,
-                                                                             fv->counters.ptr);
+        launch_update<D, false>(fv, 0.5 * dt);
         fv->close_timed(timed_);
     }
     LUNA_CUDA(cudaGetLastError());
@@ -710,7 +733,7 @@ luna_status moving_end(luna_fv* fv) {
     if (fv->precision != LUNA_FP64) {
         auto x = flux_args<D, float>(fv, fv->grad32.ptr, 2 * dt);
         x.unit = fv->grid_step / dt;
-        if (fv->precision == LUNA_FP32)
+        if (float_riemann(fv))
             LUNA_TRY((launch_flux<D, 1, 1, float, true, 0>(fv, x)));
         else if (fv->precision == LUNA_GRAD16)
             LUNA_TRY((launch_flux<D, 1, 1, float, false, 0, true>(fv, x)));
@@ -726,8 +749,7 @@ luna_status moving_end(luna_fv* fv) {
     }
     {
         const long timed_ = fv->open_timed(3);
-        luna::k_update<D, true, true><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->q.ptr, fv->flux.ptr, 0.5 * dt, fv->prims.ptr, fv->gas,
-                                                                            fv->counters.ptr);
+        launch_update<D, true>(fv, 0.5 * dt);
         fv->close_timed(timed_);
     }
     LUNA_CUDA(cudaGetLastError());
@@ -886,8 +908,8 @@ LUNA_API luna_status luna_fv_create(const luna_mesh_desc* mesh, const luna_gas* 
     if (limiter != LUNA_LIMITER_FACE_CENTROID && limiter != LUNA_LIMITER_NONE) return set_error(LUNA_EINVAL, "limiter: face_centroid or none");
     if (motion != LUNA_STATIC_MESH && motion != LUNA_MOVING) return set_error(LUNA_EINVAL, "motion: static_mesh or moving");
     if (riemann != LUNA_HLLC && riemann != LUNA_HLL) return set_error(LUNA_EINVAL, "riemann: HLLC or HLL");
-    if (precision != LUNA_FP64 && precision != LUNA_FP32 && precision != LUNA_GRAD32 && precision != LUNA_GRAD16)
-        return set_error(LUNA_EINVAL, "precision: FP64, FP32, GRAD32 or GRAD16");
+    if (precision != LUNA_FP64 && precision != LUNA_FP32 && precision != LUNA_GRAD32 && precision != LUNA_GRAD16 && precision != LUNA_SINGLE)
+        return set_error(LUNA_EINVAL, "precision: FP64, FP32, GRAD32, GRAD16 or SINGLE");
     if (precision != LUNA_FP64 && riemann == LUNA_HLL)
         return set_error(LUNA_EINVAL, "the FP32 policy takes HLLC (the reference's reduced presets are HLLC only)");
     if (motion == LUNA_MOVING && (order != 1 || update != LUNA_UPDATE_PER_FACE))

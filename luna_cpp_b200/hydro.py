@@ -23,7 +23,7 @@ UPDATE = {"per_cell": 0, "per_face": 1}
 LIMITER = {"face_centroid": 0, "none": 1}
 MOTION = {"static_mesh": 0, "static": 0, "moving": 1}
 RIEMANN = {"hllc": 0, "hll": 1}
-PRECISION = {"fp64": 0, "double": 0, "fp32": 1, "riemann32": 1, "grad32": 2, "grad16": 3}
+PRECISION = {"fp64": 0, "double": 0, "fp32": 1, "riemann32": 1, "grad32": 2, "grad16": 3, "single": 4}
 
 
 class LunaError(RuntimeError):

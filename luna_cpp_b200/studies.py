@@ -82,7 +82,7 @@ def precision(nx=128, steps=100, courant=0.3, seed=1, threads=0, log=print) -> d
                           "energy_drift": float(abs(q64[:, 4].sum() - q0[:, 4].sum()) / q0[:, 4].sum()),
                           "t_end": float(sum(dts))}
         ref.close()
-        for policy in ("fp32", "grad32", "grad16"):
+        for policy in ("fp32", "single", "grad32", "grad16"):
             fv = hydro.FiniteVolume(mesh, precision=policy)
             fv.set_state(q0)
             fv.set_timing(True)

@@ -273,7 +273,7 @@ void lo_hllc_flux_float(int D, const float* L, const float* R, const float* n, c
 struct lo_fv {
     lo_mesh mesh;
     lo_gas gas;
-    int D, V, U, order, per_face, limiter_none, riemann, moving, grad_float, riemann_float, grad_half;
+    int D, V, U, order, per_face, limiter_none, riemann, moving, grad_float, riemann_float, grad_half, flux_float;
     int64_t n, f;
     double box_inverse[3], step, per_step;
     int64_t period[3];
@@ -753,6 +753,7 @@ static void sweep_cell_f(lo_fv* fv, int64_t i, int grad_on) {
 }
 
 void lo_fv_set_half_gradients(lo_fv* fv, int on) { fv->grad_half = on != 0; }
+void lo_fv_set_float_fluxes(lo_fv* fv, int on) { fv->flux_float = on != 0; }
 
 /* sweep() (finite_volume.hpp:1107-1149): Sweep, then the time-step reduction (TimeStep = FaceStep + CellStep,
  * finite_volume.hpp:1040-1104). */
@@ -977,6 +978,9 @@ static void apply(lo_fv* fv, double dt_flux, double dt_update, int pass) {
     for (int64_t f = 0; f < fv->f; ++f) {
         int fb = 0;
         face_flux(fv, f, dt_flux, pass, fv->flux + V * f, &fb, &fb);
+        /* Precision::flux = float: F(f, v) = static_cast<FluxStore>(value[v]) (finite_volume.hpp:1597), read back as double */
+        if (fv->flux_float)
+            for (int v = 0; v < V; ++v) fv->flux[V * f + v] = (double)(float)fv->flux[V * f + v];
         count += fb;
     }
     fv->fallbacks[pass < 0 ? 0 : pass] = count;

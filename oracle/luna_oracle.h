@@ -57,6 +57,8 @@ double lo_fv_time_step(lo_fv* fv, double courant);
 /* The Grad16 policy (grad_float and on): the float gradients stored as binary16 with one power-of-two exponent per group
  * rho, v, P (finite_volume.hpp:616-641), so the flux reads them rounded. */
 void lo_fv_set_half_gradients(lo_fv* fv, int on);
+/* The flux rows of the per-face loop stored in float (Precision::flux = float, the reference's `single` preset). */
+void lo_fv_set_float_fluxes(lo_fv* fv, int on);
 void lo_fv_step(lo_fv* fv, double dt);
 int64_t lo_fv_fallbacks(const lo_fv* fv);
 int lo_fv_threads(int threads); /* sets the OpenMP thread count (<= 0: all); returns the count in use */

@@ -62,6 +62,7 @@ def lib():
         "lo_fv_step_moving_end": ([P, P], V),
         "lo_grid_step": ([I, P], D),
         "lo_fv_set_half_gradients": ([P, I], V),
+        "lo_fv_set_float_fluxes": ([P, I], V),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -134,13 +135,15 @@ class OracleFV:
         self.V = mesh.dim + 2
         self._gas = gas(gamma)
         m = self._desc(mesh)
-        grad_float = 1 if precision in ("grad32", "riemann32", "grad16") else 0
-        riemann_float = 1 if precision == "riemann32" else 0
+        grad_float = 1 if precision in ("grad32", "riemann32", "grad16", "single") else 0
+        riemann_float = 1 if precision in ("riemann32", "single") else 0
         self._h = lib().lo_fv_create(ctypes.byref(m), ctypes.byref(self._gas), order, 1 if per_face else 0,
                                       1 if limiter == "none" else 0, 1 if riemann == "hll" else 0,
                                       1 if moving else 0, grad_float, riemann_float)
         if precision == "grad16":
             lib().lo_fv_set_half_gradients(self._h, 1)
+        if precision == "single":
+            lib().lo_fv_set_float_fluxes(self._h, 1)
 
     def _desc(self, mesh):
         arrays = [np.ascontiguousarray(x) for x in (mesh.owner, mesh.neighbour, mesh.cell_face_start, mesh.cell_face,

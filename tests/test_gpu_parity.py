@@ -28,7 +28,7 @@ def pair(mesh, q0, **kw):
     ora = O.OracleFV(mesh, order=kw.get("order", 1), per_face=kw.get("update", "per_face") == "per_face",
                      limiter=kw.get("limiter", "face_centroid"), riemann=kw.get("riemann", "hllc"),
                      moving=kw.get("motion", "static_mesh") == "moving",
-                     precision={"fp32": "riemann32", "grad32": "grad32", "grad16": "grad16"}.get(prec, "double"))
+                     precision={"fp32": "riemann32", "grad32": "grad32", "grad16": "grad16", "single": "single"}.get(prec, "double"))
     gpu.set_state(q0)
     ora.set_state(q0)
     return gpu, ora
@@ -107,7 +107,7 @@ def test_blast_32_fp64_50_steps(cuda):
     assert gpu.fallbacks() == ora.fallbacks()
 
 
-@pytest.mark.parametrize("precision", ["fp32", "grad32", "grad16"])
+@pytest.mark.parametrize("precision", ["fp32", "grad32", "grad16", "single"])
 def test_reduced_policy_matches_oracle_policy(cuda, precision):
     mesh = jittered_mesh(16)
     q0 = rough_state(mesh.n_cells) * mesh.volume[:, None]
@@ -162,24 +162,24 @@ def test_reduced_policies_against_fp64(cuda, problem):
     mesh = jittered_mesh(16)
     q0 = acoustic_wave(mesh, amplitude=1e-6) if problem == "wave" else point_blast(mesh, radius_cells=2.5)
     res = {}
-    for prec in ("fp64", "fp32", "grad32"):
+    for prec in ("fp64", "fp32", "grad32", "single"):
         fv = hydro.FiniteVolume(mesh, precision=prec)
         fv.set_state(q0)
         for _ in range(20):
             fv.step(fv.time_step(0.3))
         res[prec] = fv.get_state()
-    for prec in ("fp32", "grad32"):
+    for prec in ("fp32", "grad32", "single"):
         assert np.abs(res[prec] - res["fp64"]).sum() / np.abs(res["fp64"]).sum() < 1e-5
     if problem == "wave":
         background = acoustic_wave(mesh, amplitude=0.0)
         p64 = res["fp64"] - background
-        pert = {prec: np.abs(res[prec] - res["fp64"]).sum() / np.abs(p64).sum() for prec in ("fp32", "grad32")}
+        pert = {prec: np.abs(res[prec] - res["fp64"]).sum() / np.abs(p64).sum() for prec in ("fp32", "grad32", "single")}
         assert pert["grad32"] < 1e-5
-        assert pert["fp32"] < 0.2
+        assert pert["fp32"] < 0.2 and pert["single"] < 0.2
 
 
 @pytest.mark.parametrize("order", [0, 1])
-@pytest.mark.parametrize("precision", ["fp64", "fp32", "grad32", "grad16"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "grad32", "grad16", "single"])
 def test_uniform_state_stays_uniform(cuda, order, precision):
     mesh = jittered_mesh(16)
     W = np.array([1.3, 0.3, -0.2, 0.1, 0.7])
@@ -192,7 +192,7 @@ def test_uniform_state_stays_uniform(cuda, order, precision):
     assert relative(got, np.tile(U, (mesh.n_cells, 1))) < (1e-13 if precision == "fp64" else 1e-6)
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32", "grad32", "grad16"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "grad32", "grad16", "single"])
 def test_conservation_and_determinism(cuda, precision):
     mesh = jittered_mesh(16)
     q0 = rough_state(mesh.n_cells) * mesh.volume[:, None]

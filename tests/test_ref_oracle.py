@@ -76,7 +76,7 @@ def test_variants(reference, dim, kw):
 
 
 @pytest.mark.parametrize("dim", [3, 2])
-@pytest.mark.parametrize("precision", ["grad32", "riemann32", "grad16"])
+@pytest.mark.parametrize("precision", ["grad32", "riemann32", "grad16", "single"])
 def test_precision_policies(reference, dim, precision):
     """Grad32, riemann32 (Precision<double, float, double, float>) and Grad16 (binary16 gradient rows), 10 steps."""
     mesh = jittered_mesh(12 if dim == 3 else 32, dim=dim)
