@@ -408,9 +408,93 @@ def adjoint(nx=512, steps=200, every=20, h=1e-6, seed=3, courant=0.3, threads=0,
     return res
 
 
+def kernels(case="adjoint", nx=64, repeat=3, log=print) -> dict:
+    """Small profiling workloads of the kernels beside the static step, each run `repeat` times after one warm-up on the
+    nx^3 jittered point blast (FP64), for ncu captures of one kernel family at a time:
+      adjoint  step_adjoint (k_sweep_fit, k_faces_adjoint, k_cell_adjoint, k_gather_adjoint), Q bar on the device;
+      tangent  step_tangent (k_tangent_prims, k_tangent_sweep, k_tangent_fluxes, k_tangent_update);
+      mlp      the limiter network on nx^3 feature rows: the tensor-core forward (k_mlp_forward_tc) and a training step's
+               gradient (k_mlp_train, k_mlp_reduce);
+      line     256 Riemann-problem lines of 4096 cells, fused steps (k_line_step);
+      tiles    the sweep's tiles cut on the device and the geometry rows of a device mesh (k_morton, k_tiles, ...,
+               k_geometry), by taking a device remesh of the generators as the mesh;
+      moving   moving steps with the device remesh (k_geometry of each new mesh, the two flux passes)."""
+    import torch
+
+    from . import hydro
+    from .learned import LimiterMLP, init_params
+    from .problems import point_blast
+
+    out = {"case": case, "nx": nx, "repeat": repeat}
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if case in ("adjoint", "tangent"):
+        mesh = build_mesh(jittered_points((nx, nx, nx), jitter=0.1, seed=1))
+        fv = hydro.FiniteVolume(mesh)
+        fv.set_state(point_blast(mesh))
+        for _ in range(2):
+            fv.step(fv.time_step(0.3))
+        q = fv.get_state()
+        dt = fv.time_step(0.3)
+        bar = torch.randn(mesh.n_cells, 5, dtype=torch.float64, device="cuda") * 1e-3
+        call = (lambda: fv.step_adjoint(dt, bar)) if case == "adjoint" else (lambda: (fv.set_state(q), fv.time_step(0.3), fv.step_tangent(dt, bar)))
+        call()
+        torch.cuda.synchronize()
+        start.record()
+        for _ in range(repeat):
+            call()
+        end.record()
+        torch.cuda.synchronize()
+        out["ms_per_call"] = start.elapsed_time(end) / repeat
+        fv.close()
+    elif case == "mlp":
+        n = nx ** 3
+        net = LimiterMLP(init_params(1))
+        x = (torch.rand(n, 32, device="cuda") * 2 - 1).to(torch.bfloat16)
+        t = torch.rand(n, 5, device="cuda")
+        w = torch.ones(n, 5, device="cuda")
+        net.forward(x)
+        net.gradient(x, t, w)
+        torch.cuda.synchronize()
+        start.record()
+        for _ in range(repeat):
+            net.forward(x)
+        end.record()
+        torch.cuda.synchronize()
+        out["forward_ms"] = start.elapsed_time(end) / repeat
+        for _ in range(repeat):
+            net.gradient(x, t, w)
+        torch.cuda.synchronize()
+    elif case == "line":
+        out.update(lines(nx=4096, batch=256, steps=repeat, log=log))
+    elif case in ("tiles", "moving"):
+        from .remesh import Remesher
+
+        grid = 2.0 ** -30
+        pts = np.round(jittered_points((nx, nx, nx), jitter=0.1, seed=1) / grid) * grid
+        remesher = Remesher(3, (1.0, 1.0, 1.0))
+        mesh = remesher.build(pts)
+        if case == "tiles":
+            for _ in range(repeat + 1):
+                fv = hydro.FiniteVolume(mesh)
+                fv.close()
+        else:
+            fv = hydro.FiniteVolume(mesh, precision="fp32", motion="moving")
+            fv.set_state(point_blast(mesh.cells()))
+            r = run_moving(fv, 1.0, max_steps=repeat + 1, remesher=remesher, log=lambda s: None)
+            out["hydro_device_ms_per_step"] = r["hydro_device_ms"] / r["steps"]
+            fv.close()
+        remesher.close()
+    else:
+        raise ValueError(case)
+    torch.cuda.synchronize()
+    log(json.dumps(out))
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("study", choices=["precision", "adjoint", "moving", "learned", "lines"])
+    ap.add_argument("study", choices=["precision", "adjoint", "moving", "learned", "lines", "kernels"])
+    ap.add_argument("--case", default="adjoint", help="kernels: adjoint, tangent, mlp, line, tiles or moving")
     ap.add_argument("--nx", type=int)
     ap.add_argument("--steps", type=int)
     ap.add_argument("--threads", type=int, default=0)
@@ -431,8 +515,13 @@ def main():
         kw.pop("steps", None)
     if args.study == "lines":
         kw.pop("threads", None)
+    if args.study == "kernels":
+        kw.pop("threads", None)
+        kw["case"] = args.case
+        if args.steps:
+            kw["repeat"] = kw.pop("steps")
     res = {"precision": precision, "adjoint": adjoint, "moving": moving, "learned": learned_blast,
-           "lines": lines}[args.study](**kw)
+           "lines": lines, "kernels": kernels}[args.study](**kw)
     text = json.dumps(res, indent=1)
     if args.out:
         with open(args.out, "w") as f:
