@@ -80,16 +80,26 @@ struct GeometryDev {
 // here in double, in the reference's order; the sweep then only sums c_k times the differences. Also the face rows of
 // the faces the cell owns and the largest face angle. g.nbr holds each entry's staged row on entry (from the host's
 // tiles); the kernel adds the owned and tiny bits.
+// Both walks take the list in batches of LUNA_GEOMETRY_BATCH entries whose loads are all issued before any is used:
+// the entries' list words, then their faces' cells and |A| (and the face rows' area and centroid), then the neighbours'
+// generators and centroids: three dependent load levels a batch instead of three an entry (the kernel is bound by
+// these gathers; on a moving mesh it runs after every remesh). The arithmetic is the per-entry one, in list order.
+#ifndef LUNA_GEOMETRY_BATCH
+#define LUNA_GEOMETRY_BATCH 4
+#endif
 template <int D, class G>
 __global__ void __launch_bounds__(128) k_geometry(MeshDev<D> m, GeometryDev<D, G> g) {
-    constexpr int U = D + 1;
+    constexpr int U = D + 1, B = LUNA_GEOMETRY_BATCH;
     const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= g.threads) return;
     const int i = g.order[t];
     if (i < 0) return;
-    double centroid[D];
+    double centroid[D], pi[D];
 #pragma unroll
-    for (int a = 0; a < D; ++a) centroid[a] = m.cen[D * i + a];
+    for (int a = 0; a < D; ++a) {
+        centroid[a] = m.cen[D * i + a];
+        pi[a] = m.pos[D * i + a];
+    }
     const int first = m.start[i], end = m.start[i + 1];
     const int64_t slot0 = static_cast<int64_t>(g.slice_base[t >> 5]) * 32 + (t & 31);
     double surface = 0, smallest = __longlong_as_double(0x7ff0000000000000ll), max_angle = 0;
@@ -98,25 +108,45 @@ __global__ void __launch_bounds__(128) k_geometry(MeshDev<D> m, GeometryDev<D, G
     for (int p = 0; p < U; ++p)
 #pragma unroll
         for (int s = 0; s < U; ++s) M[p][s] = 0;
-    for (int k = first; k < end; ++k) {
-        const int32_t e = m.list[k];
-        const int f = list_face(e);
-        const int j = e >= 0 ? m.neighbour[f] : m.owner[f];
-        double d[D];
-        m.separation(i, j, d);
-        const double magnitude = m.mag[f];
-        surface += magnitude;
-        smallest = fmin(smallest, magnitude);
-        const double d2 = dot<D>(d, d);
-        max_angle = fmax(max_angle, face_angle<D>(magnitude) / (0.5 * sqrt(d2)));
-        double X[U];
-        X[0] = 1;
+    for (int k0 = first; k0 < end; k0 += B) {
+        int32_t e[B];
+        int j[B];
+        double mag[B], pj[B][D], cj[B][D];
 #pragma unroll
-        for (int p = 1; p < U; ++p) X[p] = d[p - 1] + m.cen[D * j + p - 1] - centroid[p - 1];
+        for (int b = 0; b < B; ++b) e[b] = k0 + b < end ? m.list[k0 + b] : 0;
 #pragma unroll
-        for (int p = 0; p < U; ++p)
+        for (int b = 0; b < B; ++b) {
+            const int f = list_face(e[b]);
+            j[b] = k0 + b < end ? (e[b] >= 0 ? m.neighbour[f] : m.owner[f]) : i;
+            mag[b] = k0 + b < end ? m.mag[f] : 0.0;
+        }
 #pragma unroll
-            for (int s = p; s < U; ++s) M[p][s] += magnitude * X[p] * X[s];
+        for (int b = 0; b < B; ++b)
+#pragma unroll
+            for (int a = 0; a < D; ++a) {
+                pj[b][a] = m.pos[D * j[b] + a];
+                cj[b][a] = m.cen[D * j[b] + a];
+            }
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+            if (k0 + b >= end) break;
+            double d[D];
+#pragma unroll
+            for (int a = 0; a < D; ++a) d[a] = m.wrap(pj[b][a] - pi[a], a);  // Geometry::separation(i, j)
+            const double magnitude = mag[b];
+            surface += magnitude;
+            smallest = fmin(smallest, magnitude);
+            const double d2 = dot<D>(d, d);
+            max_angle = fmax(max_angle, face_angle<D>(magnitude) / (0.5 * sqrt(d2)));
+            double X[U];
+            X[0] = 1;
+#pragma unroll
+            for (int p = 1; p < U; ++p) X[p] = d[p - 1] + cj[b][p - 1] - centroid[p - 1];
+#pragma unroll
+            for (int p = 0; p < U; ++p)
+#pragma unroll
+                for (int s = p; s < U; ++s) M[p][s] += magnitude * X[p] * X[s];
+        }
     }
     double L[U][U];
 #pragma unroll
@@ -135,75 +165,105 @@ __global__ void __launch_bounds__(128) k_geometry(MeshDev<D> m, GeometryDev<D, G
     const double tiny = 1e-6 * surface;
     const bool any_tiny = smallest < tiny;
     double reach2 = 0;
-    for (int k = first; k < end; ++k) {
-        const int32_t e = m.list[k];
-        const int f = list_face(e);
-        const bool owned = e >= 0;
-        const int j = owned ? m.neighbour[f] : m.owner[f];
-        const int64_t slot = slot0 + 32 * static_cast<int64_t>(k - first);
-        // c_k: M^-1 (w X_k) by the factor, rows 1..D
-        double d[D], z[U], x[U], wX[U];
-        m.separation(i, j, d);
-        const double magnitude = m.mag[f];
-        wX[0] = magnitude;
+    for (int k0 = first; k0 < end; k0 += B) {
+        int32_t e[B];
+        int j[B];
+        double mag[B], fc[B][D], pj[B][D], cj[B][D];
 #pragma unroll
-        for (int p = 1; p < U; ++p) wX[p] = magnitude * (d[p - 1] + m.cen[D * j + p - 1] - centroid[p - 1]);
+        for (int b = 0; b < B; ++b) e[b] = k0 + b < end ? m.list[k0 + b] : 0;
 #pragma unroll
-        for (int p = 0; p < U; ++p) {
-            double sum = wX[p];
+        for (int b = 0; b < B; ++b) {
+            const int f = list_face(e[b]);
+            const bool in = k0 + b < end;
+            j[b] = in ? (e[b] >= 0 ? m.neighbour[f] : m.owner[f]) : i;
+            mag[b] = in ? m.mag[f] : 0.0;
 #pragma unroll
-            for (int q = 0; q < p; ++q) sum -= L[p][q] * z[q];
-            z[p] = sum / L[p][p];
+            for (int a = 0; a < D; ++a) fc[b][a] = in ? m.fcen[D * f + a] : 0.0;
         }
 #pragma unroll
-        for (int p = U - 1; p >= 0; --p) {
-            double sum = z[p];
-#pragma unroll
-            for (int q = p + 1; q < U; ++q) sum -= L[q][p] * x[q];
-            x[p] = sum / L[p][p];
-        }
-        g.c01[slot] = Pair<G>{static_cast<G>(x[1]), static_cast<G>(x[2])};
-        if constexpr (D == 3) g.c2[slot] = static_cast<G>(x[3]);
-        double off[D];
-        m.face_offset(f, i, off);
-        g.off01[slot] = Pair<G>{static_cast<G>(off[0]), static_cast<G>(off[1])};
-        if constexpr (D == 3) g.off2[slot] = static_cast<G>(off[2]);
-        {
-            double r2 = 0;
+        for (int b = 0; b < B; ++b)
 #pragma unroll
             for (int a = 0; a < D; ++a) {
-                const double o = static_cast<double>(static_cast<G>(off[a]));
-                r2 += o * o;
+                pj[b][a] = m.pos[D * j[b] + a];
+                cj[b][a] = m.cen[D * j[b] + a];
             }
-            reach2 = fmax(reach2, r2);
-        }
-        const bool tiny_face = any_tiny && magnitude < tiny;
-        g.nbr[slot] = (g.nbr[slot] & kIndexMask) | (owned ? kOwnedBit : 0u) | (tiny_face ? kTinyBit : 0u);
-        if (owned) {  // the face row, written once by the owner
-            double a[D];
 #pragma unroll
-            for (int q = 0; q < D; ++q) a[q] = m.area[D * f + q];
-            const double amag = sqrt(dot<D>(a, a));
-            double offj[D];
-            m.face_offset(f, j, offj);
-            FaceRow<G> r;
-            const double inv = amag == 0 ? 0.0 : 1.0 / amag;
+        for (int b = 0; b < B; ++b) {
+            const int k = k0 + b;
+            if (k >= end) break;
+            const int f = list_face(e[b]);
+            const bool owned = e[b] >= 0;
+            const int64_t slot = slot0 + 32 * static_cast<int64_t>(k - first);
+            // c_k: M^-1 (w X_k) by the factor, rows 1..D
+            double d[D], z[U], x[U], wX[U];
 #pragma unroll
-            for (int q = 0; q < 3; ++q) {
-                r.n[q] = q < D ? a[q] * inv : 0.0;
-                if constexpr (sizeof(G) == sizeof(double)) {
-                    r.offo[q] = q < D ? off[q] : 0.0;
-                    r.offj[q] = q < D ? offj[q] : 0.0;
-                } else {
-                    r.offo[q] = q < D ? static_cast<float>(off[q]) : 0.0f;
-                    r.offj[q] = q < D ? static_cast<float>(offj[q]) : 0.0f;
+            for (int a = 0; a < D; ++a) d[a] = m.wrap(pj[b][a] - pi[a], a);
+            const double magnitude = mag[b];
+            wX[0] = magnitude;
+#pragma unroll
+            for (int p = 1; p < U; ++p) wX[p] = magnitude * (d[p - 1] + cj[b][p - 1] - centroid[p - 1]);
+#pragma unroll
+            for (int p = 0; p < U; ++p) {
+                double sum = wX[p];
+#pragma unroll
+                for (int q = 0; q < p; ++q) sum -= L[p][q] * z[q];
+                z[p] = sum / L[p][p];
+            }
+#pragma unroll
+            for (int p = U - 1; p >= 0; --p) {
+                double sum = z[p];
+#pragma unroll
+                for (int q = p + 1; q < U; ++q) sum -= L[q][p] * x[q];
+                x[p] = sum / L[p][p];
+            }
+            g.c01[slot] = Pair<G>{static_cast<G>(x[1]), static_cast<G>(x[2])};
+            if constexpr (D == 3) g.c2[slot] = static_cast<G>(x[3]);
+            // Geometry::face_offset(f, i): the face centroid (relative to the owner) moved to i's generator when the
+            // owner is the other cell, minus i's centroid
+            double off[D];
+#pragma unroll
+            for (int a = 0; a < D; ++a) off[a] = (owned ? fc[b][a] : fc[b][a] + d[a]) - centroid[a];
+            g.off01[slot] = Pair<G>{static_cast<G>(off[0]), static_cast<G>(off[1])};
+            if constexpr (D == 3) g.off2[slot] = static_cast<G>(off[2]);
+            {
+                double r2 = 0;
+#pragma unroll
+                for (int a = 0; a < D; ++a) {
+                    const double o = static_cast<double>(static_cast<G>(off[a]));
+                    r2 += o * o;
                 }
+                reach2 = fmax(reach2, r2);
             }
-            r.mag = amag;
-            r.o = i;
-            r.j = j;
-            if constexpr (sizeof(G) == sizeof(double)) r.pad = 0;
-            g.faces[f] = r;
+            const bool tiny_face = any_tiny && magnitude < tiny;
+            g.nbr[slot] = (g.nbr[slot] & kIndexMask) | (owned ? kOwnedBit : 0u) | (tiny_face ? kTinyBit : 0u);
+            if (owned) {  // the face row, written once by the owner
+                double a[D];
+#pragma unroll
+                for (int q = 0; q < D; ++q) a[q] = m.area[D * f + q];
+                const double amag = sqrt(dot<D>(a, a));
+                // face_offset(f, j): the owner i seen from j, minus j's centroid
+                double offj[D];
+#pragma unroll
+                for (int q = 0; q < D; ++q) offj[q] = (fc[b][q] + m.wrap(pi[q] - pj[b][q], q)) - cj[b][q];
+                FaceRow<G> r;
+                const double inv = amag == 0 ? 0.0 : 1.0 / amag;
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    r.n[q] = q < D ? a[q] * inv : 0.0;
+                    if constexpr (sizeof(G) == sizeof(double)) {
+                        r.offo[q] = q < D ? off[q] : 0.0;
+                        r.offj[q] = q < D ? offj[q] : 0.0;
+                    } else {
+                        r.offo[q] = q < D ? static_cast<float>(off[q]) : 0.0f;
+                        r.offj[q] = q < D ? static_cast<float>(offj[q]) : 0.0f;
+                    }
+                }
+                r.mag = amag;
+                r.o = i;
+                r.j = j[b];
+                if constexpr (sizeof(G) == sizeof(double)) r.pad = 0;
+                g.faces[f] = r;
+            }
         }
     }
     g.max_angle[i] = max_angle;
@@ -693,6 +753,13 @@ __global__ void __launch_bounds__(kTileCells, MINB) k_sweep_tiles(MeshDev<D> m, 
     if (i >= 0 && !(smallest_dt == smallest_dt)) atomicOr(&ctr->error, 1ull);
 }
 
+// The network's slot of variable v, by role in every dimension: density 0, velocity components 1 .. D, pressure 4 (in 2D
+// slot 3, the z velocity's, stays empty), so that one network serves 2D and 3D meshes.
+template <int D>
+__host__ __device__ constexpr int learned_slot(int v) {
+    return v == D + 1 ? 4 : v;
+}
+
 template <int D, class G>
 __device__ __forceinline__ void write_learned_inputs(const LearnedInputs& out, int i, const double* Wi, double c, double r, const G* g,
                                                      const G* lo, const G* hi, const double* alpha) {
@@ -712,10 +779,11 @@ __device__ __forceinline__ void write_learned_inputs(const LearnedInputs& out, i
         for (int a = 0; a < D; ++a) gn += static_cast<double>(g[D * v + a]) * static_cast<double>(g[D * v + a]);
         gn = sqrt(gn);
         const double pos = fmin(fmax((Wi[v] - static_cast<double>(lo[v])) / safe, -1.0), 2.0);
-        f[4 * v + 0] = static_cast<float>(alpha[v] / kAlphaCap);
-        f[4 * v + 1] = static_cast<float>(pos - 0.5);
-        f[4 * v + 2] = tanhf(static_cast<float>(gn * r / safe));  // the features are BF16: float is ample
-        f[4 * v + 3] = tanhf(static_cast<float>(range / scale * 3.0));
+        const int slot = learned_slot<D>(v);
+        f[4 * slot + 0] = static_cast<float>(alpha[v] / kAlphaCap);
+        f[4 * slot + 1] = static_cast<float>(pos - 0.5);
+        f[4 * slot + 2] = tanhf(static_cast<float>(gn * r / safe));  // the features are BF16: float is ample
+        f[4 * slot + 3] = tanhf(static_cast<float>(range / scale * 3.0));
         plain = fmin(plain, fmin(alpha[v], 1.0));
         out.alpha[5 * static_cast<int64_t>(i) + v] = alpha[v];
     }
@@ -747,7 +815,7 @@ __global__ void k_apply_factors(int rows, const int* __restrict__ cells, const u
         const double a = alpha[5 * static_cast<int64_t>(s) + v];
         double phi;
         if (use_net) {
-            const double o = logits[16 * static_cast<int64_t>(s) + v];
+            const double o = logits[16 * static_cast<int64_t>(s) + learned_slot<D>(v)];
             phi = a / (1.0 + exp(-o));
         } else {
             phi = fmin(a, 1.0);
@@ -764,12 +832,18 @@ __global__ void k_apply_factors(int rows, const int* __restrict__ cells, const u
 #ifndef LUNA_FLUX_MIN_BLOCKS
 #define LUNA_FLUX_MIN_BLOCKS 6
 #endif
-template <int D, int Order, class G, bool RF, int Riemann, bool H = false, bool WG = false, class FS = double>
+// OP: the owner-partial layout (kernels.cuh, OwnerPartials): the row goes to the neighbour's run and the owner's side
+// is summed per warp segment.
+template <int D, int Order, class G, bool RF, int Riemann, bool H = false, bool WG = false, class FS = double, bool OP = false>
 __global__ void __launch_bounds__(128, LUNA_FLUX_MIN_BLOCKS) k_flux_rows(MeshDev<D> m, GeometryDev<D, G> geo, FluxArgs<D, G> x, FS* __restrict__ flux,
-                                                   unsigned long long* __restrict__ fallbacks) {
+                                                   unsigned long long* __restrict__ fallbacks, OwnerPartials op = {}) {
     constexpr int V = D + 2;
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     int count = 0;
+    double F[V];
+    int owner = -1;
+#pragma unroll
+    for (int v = 0; v < V; ++v) F[v] = 0;
     if (f < m.f) {
         FaceRow<G> r;
         {  // the 32-B aligned row in vector loads, streamed once per step
@@ -779,7 +853,7 @@ __global__ void __launch_bounds__(128, LUNA_FLUX_MIN_BLOCKS) k_flux_rows(MeshDev
             for (int c = 0; c < static_cast<int>(sizeof(FaceRow<G>) / 8); c += 4)
                 ldg256_hint(reinterpret_cast<const double*>(geo.faces + f) + c, words + c, once);
         }
-        double F[V];
+        owner = r.o;
         if (r.mag == 0) {
 #pragma unroll
             for (int v = 0; v < V; ++v) F[v] = 0;
@@ -813,8 +887,9 @@ __global__ void __launch_bounds__(128, LUNA_FLUX_MIN_BLOCKS) k_flux_rows(MeshDev
 #pragma unroll
             for (int v = 0; v < V; ++v) F[v] *= r.mag;
         }
-        store_flux_row<D, FS>(flux, f, F);
+        if constexpr (!OP) store_flux_row<D, FS>(flux, f, F);
     }
+    if constexpr (OP) owner_partial_epilogue<D, FS>(op, flux, f, f < m.f, owner, F);
     block_sum_to(static_cast<unsigned long long>(count), fallbacks);
 }
 

@@ -53,6 +53,7 @@ def strip(nx: int, ny: int, seed: int = 1):
 
 
 def riemann_state(mesh, prob: Riemann, gamma=GAMMA) -> np.ndarray:
+    """The 1D problem across a strip: the left state in [0.25, 0.75), the right one elsewhere."""
     x = cell_centres(mesh)[:, 0]
     left = (x >= 0.25) & (x < 0.75)
     W = np.zeros((mesh.n_cells, 4))
@@ -66,8 +67,9 @@ def riemann_state(mesh, prob: Riemann, gamma=GAMMA) -> np.ndarray:
 def primitives(q, mesh, gamma=GAMMA):
     U = q / mesh.volume[:, None]
     rho = U[:, 0]
-    v = U[:, 1:3] / rho[:, None]
-    P = (gamma - 1) * (U[:, 3] - 0.5 * rho * np.sum(v * v, 1))
+    d = U.shape[1] - 2
+    v = U[:, 1 : 1 + d] / rho[:, None]
+    P = (gamma - 1) * (U[:, 1 + d] - 0.5 * rho * np.sum(v * v, 1))
     return np.column_stack([rho, v, P])
 
 
@@ -128,8 +130,14 @@ def subcell_slopes(fine_mesh, W_fine, groups, coarse_mesh):
     return np.linalg.solve(C, B).transpose(0, 2, 1)  # [n][var][dim]
 
 
+def slots(dim):
+    """The network's output slot of each variable (by role: density 0, velocity 1 .. D, pressure 4), as the library's
+    learned_slot."""
+    return list(range(dim + 1)) + [4]
+
+
 def targets(alpha, g, s):
-    """t = clip((s . g) / (g . g) / alpha, 0, 1) and weights (1 where alpha > 0 and g != 0)."""
+    """t = clip((s . g) / (g . g) / alpha, 0, 1) and weights (1 where alpha > 0 and g != 0), in the variables' slots."""
     g = g.reshape(s.shape)
     gg = np.sum(g * g, 2)
     proj = np.sum(s * g, 2) / np.where(gg > 0, gg, 1.0)
@@ -139,24 +147,51 @@ def targets(alpha, g, s):
     w = ok.astype(np.float32)
     T = np.zeros((s.shape[0], 5), np.float32)
     Wt = np.zeros((s.shape[0], 5), np.float32)
-    T[:, : s.shape[1]] = t
-    Wt[:, : s.shape[1]] = w
+    where = slots(s.shape[2])
+    T[:, where] = t
+    Wt[:, where] = w
     return T, Wt
 
 
-def build_dataset(problems, nx=1024, ny=4, factor=4, snapshots=(0.25, 0.5, 0.75, 1.0), travel=0.2, log=print):
-    """Features, targets and weights from the fine runs of `problems` (seeds)."""
-    coarse = strip(nx, ny, seed=11)
-    fine = strip(factor * nx, factor * ny, seed=12)
-    groups = group_index(factor * nx, factor * ny, factor)
+@dataclass
+class Quadrants:
+    """A 2D Riemann problem: four constant states (rho, u, v, P) in the quadrants of the periodic unit box."""
+    states: tuple
+
+    def max_speed(self, gamma=GAMMA) -> float:
+        return max(math.hypot(u, v) + math.sqrt(gamma * p / r) for r, u, v, p in self.states)
+
+
+def quadrant_problem(seed: int) -> Quadrants:
+    """Four states from the 1D problems' distribution: rho log-uniform in [0.1, 10], P log-uniform in [0.01, 10], each
+    velocity component uniform in [-1, 1]."""
+    rng = np.random.default_rng(seed)
+    return Quadrants(tuple((float(10 ** rng.uniform(-1, 1)), float(rng.uniform(-1, 1)), float(rng.uniform(-1, 1)),
+                            float(10 ** rng.uniform(-2, 1))) for _ in range(4)))
+
+
+def square(n: int, seed: int = 1):
+    """A periodic unit square of n x n jittered (0.1) cells."""
+    return build_mesh(jittered_points((n, n), jitter=0.1, seed=seed), box=(1.0, 1.0))
+
+
+def quadrant_state(mesh, prob: Quadrants, gamma=GAMMA) -> np.ndarray:
+    c = cell_centres(mesh)
+    k = (c[:, 0] >= 0.5).astype(int) + 2 * (c[:, 1] >= 0.5).astype(int)
+    W = np.array(prob.states)[k]
+    return conserved(W, gamma) * mesh.volume[:, None]
+
+
+def _dataset(coarse, fine, groups, problems, make_state, gamma, snapshots, travel, log, what):
+    """Features, targets and weights of the coarse mesh at `snapshots` of each problem's fine run (plain limiter),
+    coarse-grained onto the coarse cells."""
     feats, tars, wts = [], [], []
     t0 = time.time()
-    for seed in problems:
-        prob = riemann_problem(seed)
-        t_end = travel / prob.max_speed()
-        ffv = hydro.FiniteVolume(fine, gas=hydro.Gas(GAMMA))
-        ffv.set_state(riemann_state(fine, prob))
-        cfv = hydro.FiniteVolume(coarse, gas=hydro.Gas(GAMMA))
+    for prob in problems:
+        t_end = travel / prob.max_speed(gamma)
+        ffv = hydro.FiniteVolume(fine, gas=hydro.Gas(gamma))
+        ffv.set_state(make_state(fine, prob, gamma))
+        cfv = hydro.FiniteVolume(coarse, gas=hydro.Gas(gamma))
         t_prev = 0.0
         for frac in snapshots:
             run_to(ffv, t_end * frac - t_prev)
@@ -165,16 +200,34 @@ def build_dataset(problems, nx=1024, ny=4, factor=4, snapshots=(0.25, 0.5, 0.75,
             qc = coarse_grain(qf, groups, coarse.n_cells, coarse, fine)
             cfv.set_state(qc)
             f, alpha, g = cfv.limiter_inputs()
-            s = subcell_slopes(fine, primitives(qf, fine), groups, coarse)
+            s = subcell_slopes(fine, primitives(qf, fine, gamma), groups, coarse)
             T, Wt = targets(alpha.cpu().numpy(), g.cpu().numpy(), s)
             feats.append(f)
             tars.append(torch.tensor(T, device="cuda"))
             wts.append(torch.tensor(Wt, device="cuda"))
         ffv.close()
         cfv.close()
-    log(f"dataset: {len(problems)} problems x {len(snapshots)} snapshots, {sum(x.shape[0] for x in feats)} cells, "
+    log(f"dataset ({what}): {len(problems)} problems x {len(snapshots)} snapshots, {sum(x.shape[0] for x in feats)} cells, "
         f"{time.time() - t0:.1f} s")
     return torch.cat(feats), torch.cat(tars), torch.cat(wts)
+
+
+def build_dataset_2d(problems, n=256, factor=4, gamma=GAMMA, snapshots=(0.25, 0.5, 0.75, 1.0), travel=0.2, log=print):
+    """The 2D part of the training data: four-quadrant Riemann problems (seeds) on an n^2 jittered mesh, labelled from
+    the method's own run on (factor n)^2 cells, coarse-grained by lattice index (factor^2 fine cells a coarse cell)."""
+    coarse, fine = square(n, seed=11), square(factor * n, seed=12)
+    groups = group_index(factor * n, factor * n, factor)
+    return _dataset(coarse, fine, groups, [quadrant_problem(s) for s in problems], quadrant_state, gamma, snapshots, travel,
+                    log, f"2D {n}^2 quadrants, gamma {gamma:g}")
+
+
+def build_dataset(problems, nx=1024, ny=4, factor=4, gamma=GAMMA, snapshots=(0.25, 0.5, 0.75, 1.0), travel=0.2, log=print):
+    """The 1D part of the training data: 1D Riemann problems (seeds) across quasi-1D strips of nx x ny cells, labelled
+    from the method's own run on a strip of factor x the cells along each axis."""
+    coarse, fine = strip(nx, ny, seed=11), strip(factor * nx, factor * ny, seed=12)
+    groups = group_index(factor * nx, factor * ny, factor)
+    return _dataset(coarse, fine, groups, [riemann_problem(s) for s in problems], riemann_state, gamma, snapshots, travel,
+                    log, f"1D strips {nx}x{ny}, gamma {gamma:g}")
 
 
 def train(features, target, weight, epochs=20, batch=16384, lr=2e-3, seed=0, log=print) -> LimiterMLP:
@@ -242,6 +295,48 @@ def evaluate(net, problems, nx=1024, ny=4, factor=4, travel=0.2, resolutions=(1.
     return rows
 
 
+def binned_density(mesh, q, bins: int):
+    """Volume-weighted mean density in bins x bins equal squares of the unit box."""
+    c = cell_centres(mesh)
+    b = np.minimum((c[:, 0] * bins).astype(int), bins - 1) * bins + np.minimum((c[:, 1] * bins).astype(int), bins - 1)
+    m = np.bincount(b, weights=q[:, 0], minlength=bins * bins)
+    v = np.bincount(b, weights=mesh.volume, minlength=bins * bins)
+    return m / np.where(v > 0, v, 1.0)
+
+
+def evaluate_2d(net, problems, n=256, factor=4, gamma=GAMMA, travel=0.2, resolutions=(1.0, 1.25, 1.5), log=print):
+    """The 2D held-out set: each four-quadrant problem run by plain and learned at n^2 and by plain at the finer
+    resolutions, judged by the L1 of the density binned on the n x n lattice against the method's own (factor n)^2 run;
+    with the device time of each run."""
+    fine = square(factor * n, seed=12)
+    meshes = {r: square(int(round(r * n)), seed=11) for r in resolutions}
+    rows = []
+    for seed in problems:
+        prob = quadrant_problem(seed)
+        t_end = travel / prob.max_speed(gamma)
+        ffv = hydro.FiniteVolume(fine, gas=hydro.Gas(gamma))
+        ffv.set_state(quadrant_state(fine, prob, gamma))
+        run_to(ffv, t_end)
+        ref = binned_density(fine, ffv.get_state(), n)
+        ffv.close()
+        row = {"seed": seed}
+        for r, mesh in meshes.items():
+            for mode in (("plain", "learned") if r == 1.0 else ("plain",)):
+                fv = hydro.FiniteVolume(mesh, gas=hydro.Gas(gamma))
+                if mode == "learned":
+                    fv.set_limiter("learned", net.params)
+                fv.set_state(quadrant_state(mesh, prob, gamma))
+                fv.set_timing(True)
+                steps = run_to(fv, t_end)
+                ms = sum(v[0] for v in fv.timings().values())
+                err = float(np.mean(np.abs(binned_density(mesh, fv.get_state(), n) - ref)))
+                row[f"{mode}@{r}"] = {"l1": err, "steps": steps, "device_ms": ms}
+                fv.close()
+        rows.append(row)
+        log(f"2D problem {seed}: " + ", ".join(f"{k} {v['l1']:.3e}" for k, v in row.items() if k != "seed"))
+    return rows
+
+
 def summarize(rows, resolutions=(1.0, 1.5, 2.0)):
     """Geometric-mean L1 per configuration, and the plain resolution whose error the learned limiter reaches (log-log
     interpolation of plain's error against resolution) with the device time each needs."""
@@ -270,12 +365,17 @@ def main():
     import os
 
     ap = argparse.ArgumentParser(description="train and judge the learned slope limiter")
-    ap.add_argument("--train-problems", type=int, default=64)
-    ap.add_argument("--test-problems", type=int, default=16)
+    ap.add_argument("--train-problems", type=int, default=48, help="1D Riemann problems (strips)")
+    ap.add_argument("--train-problems-2d", type=int, default=16, help="2D four-quadrant problems (n2d^2 meshes)")
+    ap.add_argument("--test-problems", type=int, default=8)
+    ap.add_argument("--test-problems-2d", type=int, default=4)
     ap.add_argument("--nx", type=int, default=1024)
     ap.add_argument("--ny", type=int, default=4)
+    ap.add_argument("--n2d", type=int, default=256)
+    ap.add_argument("--gammas", default="1.4,1.6666666666666667", help="the data's adiabatic indices")
     ap.add_argument("--epochs", type=int, default=20)
-    ap.add_argument("--out", default="limiter_out")
+    ap.add_argument("--moving-nx", type=int, default=0, help="also judge on the 3D moving blast at this size (0: no)")
+    ap.add_argument("--out", default="limiter_out/limiter")
     args = ap.parse_args()
     os.makedirs(os.path.dirname(args.out) or ".", exist_ok=True)
     lines = []
@@ -285,15 +385,34 @@ def main():
         lines.append(s)
 
     t0 = time.time()
-    x, t, w = build_dataset(range(1000, 1000 + args.train_problems), nx=args.nx, ny=args.ny, log=log)
+    parts = []
+    for k, gamma in enumerate(float(g) for g in args.gammas.split(",")):
+        parts.append(build_dataset(range(1000 + 100 * k, 1000 + 100 * k + args.train_problems), nx=args.nx, ny=args.ny, gamma=gamma,
+                                   log=log))
+        if args.train_problems_2d > 0:
+            parts.append(build_dataset_2d(range(2000 + 100 * k, 2000 + 100 * k + args.train_problems_2d), n=args.n2d, gamma=gamma,
+                                          log=log))
+    x, t, w = (torch.cat([p[c] for p in parts]) for c in range(3))
     net = train(x, t, w, epochs=args.epochs, log=log)
     np.save(args.out + "_params.npy", net.state())
+    report = {"train_problems": args.train_problems, "train_problems_2d": args.train_problems_2d, "gammas": args.gammas,
+              "epochs": args.epochs, "nx": args.nx, "ny": args.ny, "n2d": args.n2d, "rows": len(x)}
     rows = evaluate(net, range(5000, 5000 + args.test_problems), nx=args.nx, ny=args.ny, log=log)
-    summary = summarize(rows)
-    log(json.dumps(summary))
+    report["strips"] = {"summary": summarize(rows), "rows": rows}
+    log(json.dumps(report["strips"]["summary"]))
+    if args.test_problems_2d > 0:
+        rows2 = evaluate_2d(net, range(6000, 6000 + args.test_problems_2d), n=args.n2d, log=log)
+        report["quadrants_2d"] = {"summary": summarize(rows2, resolutions=(1.0, 1.25, 1.5)), "rows": rows2}
+        log(json.dumps(report["quadrants_2d"]["summary"]))
+    if args.moving_nx > 0:
+        from .studies import learned_moving
+
+        n = args.moving_nx
+        report["moving_blast_3d"] = learned_moving(nx=n, plain_nx=(n, int(n * 1.125), int(n * 1.25), int(n * 1.375)),
+                                                   params=net.state(), log=log)
+    report["wall_s"] = time.time() - t0
     with open(args.out + "_eval.json", "w") as f:
-        json.dump({"summary": summary, "rows": rows, "train_problems": args.train_problems, "epochs": args.epochs,
-                   "nx": args.nx, "ny": args.ny, "wall_s": time.time() - t0}, f, indent=1)
+        json.dump(report, f, indent=1)
 
 
 if __name__ == "__main__":

@@ -252,6 +252,72 @@ def _profile_l1(mesh, q, reference) -> float:
     return float((mesh.volume * np.abs(rho - want)).sum() / mesh.volume.sum())
 
 
+def learned_moving(nx=64, plain_nx=(64, 72, 80, 88), cells_factor=4.0, t_end=0.05, courant=0.3, params=None, log=print) -> dict:
+    """The learned limiter on the moving point blast (the learned-limiter configuration's evaluation): nx^3 snapped jittered
+    generators, E = 1 within 2 cell widths, gamma 5/3, FP64, generators moved with the gas plus the roundness velocity,
+    the mesh rebuilt on the GPU every step, to t_end; the learned limiter (``params``, default the shipped network) at nx
+    and the plain one at nx and at the finer ``plain_nx``, each judged by the volume-weighted L1 of its density against
+    the radial profile of the plain method's own run on cells_factor x the cells (round(nx cells_factor^(1/3))^3). GPU
+    time: the hydro kernels' device time, and the whole steps' time (remesh included; it is GPU work). The plain method's
+    error and times are interpolated in log-log at the learned run's error."""
+    import torch
+
+    from .learned import LimiterMLP, trained_params
+    from .remesh import Remesher
+
+    grid = 2.0 ** -30
+
+    def run(n, mode, net=None):
+        pts = np.round(jittered_points((n, n, n), jitter=0.1, seed=1) / grid) * grid
+        remesher = Remesher(3, (1.0, 1.0, 1.0))
+        mesh = remesher.build(pts)
+        cells = mesh.cells()
+        fv = hydro.FiniteVolume(mesh, motion="moving")
+        if mode == "learned":
+            fv.set_limiter("learned", net.params)
+        fv.set_state(point_blast(cells, GAMMA))
+        torch.cuda.synchronize()
+        r = run_moving(fv, t_end, courant, remesher=remesher, log=lambda m: None)
+        q = fv.get_state()
+        final = fv.mesh.cells()
+        fv.close()
+        remesher.close()
+        return r, final, q
+
+    n_ref = int(round(nx * cells_factor ** (1.0 / 3.0)))
+    r, final, q = run(n_ref, "plain")
+    reference = _radial_reference(final, q)
+    out = {"config": {"problem": "moving point blast, E = 1 within 2 cell widths, gamma 5/3, FP64, device remesh",
+                      "t_end": t_end, "courant": courant,
+                      "reference": {"nx": n_ref, "cells": n_ref ** 3, "cells_over_base": n_ref ** 3 / nx ** 3, "steps": r["steps"],
+                                    "hydro_device_ms": r["hydro_device_ms"], "wall_s": r["wall_s"]}},
+           "plain": [], "learned": []}
+    log(f"reference {n_ref}^3: {r['steps']} steps, {r['wall_s']:.1f} s")
+    net = LimiterMLP(trained_params() if params is None else params)
+    for n in sorted(set(plain_nx) | {nx}):
+        for mode in ("plain", "learned") if n == nx else ("plain",):
+            r, final, q = run(n, mode, net)
+            row = {"nx": n, "cells": n ** 3, "steps": r["steps"], "hydro_device_ms": r["hydro_device_ms"],
+                   "whole_ms": 1e3 * r["wall_s"], "l1": _profile_l1(final, q, reference)}
+            out[mode].append(row)
+            log(f"{mode} {n}^3: {row['steps']} steps, hydro {row['hydro_device_ms']:.1f} ms, whole {row['whole_ms']:.0f} ms, "
+                f"L1 {row['l1']:.4e}")
+    plain = sorted(out["plain"], key=lambda r: r["nx"])
+    learned = out["learned"][0]
+    out["learned_l1_over_plain_l1"] = learned["l1"] / next(r["l1"] for r in plain if r["nx"] == nx)
+    le = np.log([r["l1"] for r in plain])
+    for key in ("hydro_device_ms", "whole_ms"):
+        if np.all(np.diff(le) < 0) and le[-1] <= np.log(learned["l1"]) <= le[0]:
+            x = np.interp(np.log(learned["l1"]), le[::-1], np.log([r["nx"] for r in plain])[::-1])
+            t = np.interp(x, np.log([r["nx"] for r in plain]), np.log([r[key] for r in plain]))
+            out["plain_nx_of_equal_error"] = float(np.exp(x))
+            out[f"gpu_time_ratio_at_equal_error_{key}"] = float(np.exp(t) / learned[key])
+        else:
+            out["plain_nx_of_equal_error"] = None
+            out[f"gpu_time_ratio_at_equal_error_{key}"] = None
+    return out
+
+
 def learned_blast(nx=48, factor=4, plain_nx=(48, 56, 64, 72, 80), t_end=0.05, courant=0.3, threads=0, log=print) -> dict:
     """The learned limiter in 3D: the static point blast (E = 1 within 2 cell widths, FP64) on nx^3 jittered generators
     to t_end with the shipped network, and with the plain limiter at nx and at the finer ``plain_nx``, each judged by the
@@ -493,7 +559,7 @@ def kernels(case="adjoint", nx=64, repeat=3, log=print) -> dict:
 
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("study", choices=["precision", "adjoint", "moving", "learned", "lines", "kernels"])
+    ap.add_argument("study", choices=["precision", "adjoint", "moving", "learned", "learned_moving", "lines", "kernels"])
     ap.add_argument("--case", default="adjoint", help="kernels: adjoint, tangent, mlp, line, tiles or moving")
     ap.add_argument("--nx", type=int)
     ap.add_argument("--steps", type=int)
@@ -511,8 +577,10 @@ def main():
         kw["nx"] = args.nx
     if args.steps:
         kw["steps"] = args.steps
-    if args.study in ("moving", "learned"):
+    if args.study in ("moving", "learned", "learned_moving"):
         kw.pop("steps", None)
+    if args.study == "learned_moving":
+        kw.pop("threads", None)
     if args.study == "lines":
         kw.pop("threads", None)
     if args.study == "kernels":
@@ -521,7 +589,7 @@ def main():
         if args.steps:
             kw["repeat"] = kw.pop("steps")
     res = {"precision": precision, "adjoint": adjoint, "moving": moving, "learned": learned_blast,
-           "lines": lines, "kernels": kernels}[args.study](**kw)
+           "learned_moving": learned_moving, "lines": lines, "kernels": kernels}[args.study](**kw)
     text = json.dumps(res, indent=1)
     if args.out:
         with open(args.out, "w") as f:
