@@ -1,10 +1,10 @@
 // The sweep's tiles cut on the device (tiles.h: DeviceTilePlan), for meshes rebuilt on the device every step.
 //
 // One block of kTileCells threads per tile of 128 consecutive cells in Morton order. The block orders its cells by list
-// length (longest first, then Morton position), gathers their lists' neighbours into shared memory, sorts them (bitonic)
-// and keeps each neighbour that is not a cell of the tile once: the halo, by cell index, as the host cut stages it. A
-// planning pass counts each tile's rows and its warps' longest lists; scans turn them into the row and slot offsets; a
-// filling pass repeats the block's work and writes the tiles.
+// length (longest first, then Morton position), puts their lists' neighbours into a shared-memory hash table and keeps
+// each neighbour that is not a cell of the tile once: the halo, by cell index (sorted in the fill), as the host cut
+// stages it. A planning pass counts each tile's rows and its warps' longest lists; scans turn them into the row and slot
+// offsets; a filling pass repeats the table and writes the tiles.
 #include <cuda_runtime.h>
 
 #include <climits>
@@ -21,7 +21,7 @@ luna_status report_error(luna_status s, const std::string& what);
 
 namespace {
 
-constexpr int kCandidates = 8192;  // list entries of one tile's cells a block sorts in shared memory (32 KB)
+constexpr int kCandidates = 8192;  // list entries of one tile's cells a block takes
 static_assert(luna::kTileCells == 128, "4 warps a tile");
 
 luna_status fail(luna_status s, const std::string& what) { return luna::report_error(s, what); }
@@ -110,14 +110,25 @@ struct FillOut {
     uint32_t* local;
 };
 
-// One tile: plan (Fill false) or fill (Fill true).
+// A tile's distinct list neighbours are kept in a shared-memory hash table (open addressing, linear probing): kHash
+// slots, at most kHashFill distinct neighbours (more send the mesh to the host cut, as a tile with too many entries does).
+constexpr int kHash = 4096;
+constexpr int kHashFill = 3072;
+__device__ __forceinline__ int hash_slot(int32_t x) { return static_cast<int>((static_cast<uint32_t>(x) * 2654435761u) >> 20); }
+
+// One tile: plan (Fill false) or fill (Fill true). Each cell's thread inserts its list's neighbours into the block's
+// table; a neighbour seen for the first time that is not a cell of the tile joins the halo. The plan counts the rows
+// (the tile's cells and the halo); the fill sorts the halo by cell index, stages the rows and gives each list entry its
+// neighbour's row (a binary search among the tile's cells, else a table lookup).
 template <bool Fill>
 __global__ void __launch_bounds__(luna::kTileCells) k_tiles(int64_t n, const int32_t* __restrict__ sorted_cells, MeshLists m, PlanOut plan,
                                                             FillOut fill) {
     constexpr int C = luna::kTileCells;
-    __shared__ int32_t cand[kCandidates];
-    __shared__ int32_t own_cell[C], own_len[C], ordered[C], own_sorted[C], own_row[C], chunk_prefix[C + 1];
-    __shared__ int n_cand;
+    __shared__ int32_t key[kHash];
+    __shared__ int16_t row_of[kHash];
+    __shared__ int32_t halo[kHash];
+    __shared__ int32_t own_cell[C], own_len[C], ordered[C], own_sorted[C], own_row[C];
+    __shared__ int n_halo, n_entries, table_full;
     const int64_t t = blockIdx.x;
     const int k = threadIdx.x;
     const int64_t idx = t * C + k;
@@ -125,7 +136,8 @@ __global__ void __launch_bounds__(luna::kTileCells) k_tiles(int64_t n, const int
     const int len = c >= 0 ? m.start[c + 1] - m.start[c] : -1;
     own_cell[k] = c;
     own_len[k] = len;
-    if (k == 0) n_cand = 0;
+    for (int q = k; q < kHash; q += C) key[q] = -1;
+    if (k == 0) n_halo = n_entries = table_full = 0;
     __syncthreads();
     // place in the tile: longest list first, then Morton position (idle threads last); rank among the cells by index
     int rank = 0, by_index = 0, n_own = 0;
@@ -139,36 +151,9 @@ __global__ void __launch_bounds__(luna::kTileCells) k_tiles(int64_t n, const int
     if (c >= 0) {
         own_sorted[by_index] = c;
         own_row[by_index] = rank;
-        const int base = atomicAdd(&n_cand, len);
-        for (int e = 0; e < len; ++e)
-            if (base + e < kCandidates) cand[base + e] = m.other(m.list[m.start[c] + e]);
     }
     __syncthreads();
-    const int total = n_cand;
-    if (total > kCandidates) {
-        if (!Fill && k == 0) atomicOr(&plan.ctr->overflow, 1);
-        return;
-    }
-    int P = 1;
-    while (P < total) P <<= 1;
-    for (int q = total + k; q < P; q += C) cand[q] = INT_MAX;
-    __syncthreads();
-    for (int size = 2; size <= P; size <<= 1)  // bitonic sort, ascending
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            for (int q = k; q < P; q += C) {
-                const int r = q ^ stride;
-                if (r > q) {
-                    const int32_t a = cand[q], b = cand[r];
-                    if ((a > b) == ((q & size) == 0)) {
-                        cand[q] = b;
-                        cand[r] = a;
-                    }
-                }
-            }
-            __syncthreads();
-        }
-    // the halo: first copies of the sorted neighbours that are not the tile's cells; each thread counts its chunk
-    auto is_own = [&](int32_t x) {
+    auto own_index = [&](int32_t x) {  // x's place among the tile's cells by index, or -1
         int lo = 0, hi = n_own;
         while (lo < hi) {
             const int mid = (lo + hi) >> 1;
@@ -177,21 +162,37 @@ __global__ void __launch_bounds__(luna::kTileCells) k_tiles(int64_t n, const int
             else
                 hi = mid;
         }
-        return lo < n_own && own_sorted[lo] == x;
+        return lo < n_own && own_sorted[lo] == x ? lo : -1;
     };
-    auto is_halo = [&](int q) { return (q == 0 || cand[q] != cand[q - 1]) && !is_own(cand[q]); };
-    const int chunk = (total + C - 1) / C;
-    const int q0 = k * chunk < total ? k * chunk : total, q1 = q0 + chunk < total ? q0 + chunk : total;
-    int mine = 0;
-    for (int q = q0; q < q1; ++q) mine += is_halo(q);
-    chunk_prefix[k + 1] = mine;
-    __syncthreads();
-    if (k == 0) {
-        chunk_prefix[0] = 0;
-        for (int q = 0; q < C; ++q) chunk_prefix[q + 1] += chunk_prefix[q];
+    if (c >= 0) {
+        atomicAdd(&n_entries, len);
+        const int first = m.start[c];
+        for (int e = 0; e < len; ++e) {
+            const int32_t x = m.other(m.list[first + e]);
+            int h = hash_slot(x);
+            int probe = 0;
+            for (; probe < kHash; ++probe) {
+                const int32_t prev = atomicCAS(&key[h], -1, x);
+                if (prev == -1) {
+                    if (own_index(x) < 0) {
+                        const int q = atomicAdd(&n_halo, 1);
+                        if (q < kHashFill) halo[q] = x;
+                    }
+                    break;
+                }
+                if (prev == x) break;
+                h = (h + 1) & (kHash - 1);
+            }
+            if (probe == kHash) table_full = 1;
+        }
     }
     __syncthreads();
-    const int rows = n_own + chunk_prefix[C];
+    const int halo_n = n_halo;
+    if (n_entries > kCandidates || halo_n > kHashFill || table_full) {
+        if (!Fill && k == 0) atomicOr(&plan.ctr->overflow, 1);
+        return;
+    }
+    const int rows = n_own + halo_n;
     if constexpr (!Fill) {
         if (k < C / 32) {
             const int32_t lead = ordered[32 * k];  // a warp's first cell has its longest list
@@ -205,44 +206,52 @@ __global__ void __launch_bounds__(luna::kTileCells) k_tiles(int64_t n, const int
                 atomicMax(rows > luna::kTileRows ? &plan.ctr->big_rows : &plan.ctr->normal_rows, rows);
         }
     } else {
+        // the halo by cell index (bitonic, ascending)
+        int P = 1;
+        while (P < halo_n) P <<= 1;
+        for (int q = halo_n + k; q < P; q += C) halo[q] = INT_MAX;
+        __syncthreads();
+        for (int size = 2; size <= P; size <<= 1)
+            for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                for (int q = k; q < P; q += C) {
+                    const int r = q ^ stride;
+                    if (r > q) {
+                        const int32_t a = halo[q], b = halo[r];
+                        if ((a > b) == ((q & size) == 0)) {
+                            halo[q] = b;
+                            halo[r] = a;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        for (int q = k; q < halo_n; q += C) {  // each halo cell's row, in the table (x was inserted: found within kHash)
+            const int32_t x = halo[q];
+            int h = hash_slot(x);
+            for (int probe = 0; probe < kHash && key[h] != x; ++probe) h = (h + 1) & (kHash - 1);
+            if (key[h] == x) row_of[h] = static_cast<int16_t>(n_own + q);
+        }
+        __syncthreads();
         const int64_t u = fill.tile_pos[t];
         const int64_t s0 = fill.stage_start[u];
         const int32_t mine_cell = ordered[k];
         fill.order[u * C + k] = mine_cell;
         if (k < n_own) fill.stage_cells[s0 + k] = mine_cell;
-        int h = chunk_prefix[k];
-        for (int q = q0; q < q1; ++q)
-            if (is_halo(q)) fill.stage_cells[s0 + n_own + h++] = cand[q];
+        for (int q = k; q < halo_n; q += C) fill.stage_cells[s0 + n_own + q] = halo[q];
         if (mine_cell >= 0) {  // each entry's neighbour as a staged row
             const int64_t tg = u * C + k;
             const int64_t slot0 = static_cast<int64_t>(fill.slice_base[tg >> 5]) * 32 + (tg & 31);
             const int first = m.start[mine_cell], count = m.start[mine_cell + 1] - first;
             for (int e = 0; e < count; ++e) {
                 const int32_t x = m.other(m.list[first + e]);
-                int lo = 0, hi = n_own;
-                while (lo < hi) {
-                    const int mid = (lo + hi) >> 1;
-                    if (own_sorted[mid] < x)
-                        lo = mid + 1;
-                    else
-                        hi = mid;
-                }
+                const int o = own_index(x);
                 int row;
-                if (lo < n_own && own_sorted[lo] == x) {
-                    row = own_row[lo];
-                } else {  // the halo row: halo entries before x's first copy
-                    int a = 0, b = total;
-                    while (a < b) {
-                        const int mid = (a + b) >> 1;
-                        if (cand[mid] < x)
-                            a = mid + 1;
-                        else
-                            b = mid;
-                    }
-                    const int owner_chunk = a / chunk;
-                    int before = chunk_prefix[owner_chunk];
-                    for (int q = owner_chunk * chunk; q < a; ++q) before += is_halo(q);
-                    row = n_own + before;
+                if (o >= 0) {
+                    row = own_row[o];
+                } else {  // a row the tile check rejects if x were missing (it was inserted: found within kHash)
+                    int h = hash_slot(x);
+                    for (int probe = 0; probe < kHash && key[h] != x; ++probe) h = (h + 1) & (kHash - 1);
+                    row = key[h] == x ? row_of[h] : rows;
                 }
                 fill.local[slot0 + 32 * static_cast<int64_t>(e)] = static_cast<uint32_t>(row);
             }

@@ -22,7 +22,8 @@
 #include "voronoi_grid.h"
 
 #ifndef LUNA_REMESH_DUAL
-#define LUNA_REMESH_DUAL 0  // 1: 3D cells kept as triangles of plane triples (DualT), as the host builder's LUNA_MESH_DUAL=1
+#define LUNA_REMESH_DUAL 1  // 3D cells kept as triangles of plane triples (DualT), as the host builder's default; 0: face
+                            // loops (Poly3T), as the host builder with LUNA_MESH_DUAL=0
 #endif
 
 namespace luna {

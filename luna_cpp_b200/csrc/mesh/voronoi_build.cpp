@@ -93,11 +93,12 @@ struct luna_mesh_build {
 
 namespace {
 
-// LUNA_MESH_DUAL=1 in the environment builds 3D cells as DualT (voronoi_cell.h) instead of face loops.
+// 3D cells are built as DualT (voronoi_cell.h: triangles of plane triples), as the device remesher builds them, unless
+// LUNA_MESH_DUAL=0 in the environment (read once per process) selects the face-loop cell (Poly3T).
 bool dual_cells() {
     static const bool on = [] {
         const char* v = std::getenv("LUNA_MESH_DUAL");
-        return v && v[0] == '1';
+        return !(v && v[0] == '0');
     }();
     return on;
 }

@@ -87,8 +87,9 @@ def init_params(seed: int = 0) -> np.ndarray:
 
 
 def trained_params() -> np.ndarray:
-    """The network trained by ``python -m luna_cpp_b200.limiter_training`` (48 Riemann problems, 15 epochs), shipped so
-    the learned limiter runs without retraining."""
+    """The network trained on the GPU by ``python -m luna_cpp_b200.limiter_training`` (its defaults: 48 1D Riemann strips
+    and 16 2D four-quadrant problems on 256^2, each at gamma 1.4 and 5/3, labelled from the method's own 4x runs; 20
+    epochs), shipped with its evaluation (data/limiter_mlp_eval.json) so the learned limiter runs without retraining."""
     import os
 
     return np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "limiter_mlp_params.npy"))

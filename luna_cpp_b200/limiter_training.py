@@ -92,13 +92,21 @@ def group_index(nx_f, ny_f, factor):
     return (i // factor) * ny_c + j // factor
 
 
+def _group_sum(groups, values, n):
+    """Per-group sums of the rows of values ([m] or [m, ...]) into n groups (column by column, bincount)."""
+    v = np.asarray(values, dtype=np.float64)
+    if v.ndim == 1:
+        return np.bincount(groups, weights=v, minlength=n)
+    flat = v.reshape(v.shape[0], -1)
+    out = np.stack([np.bincount(groups, weights=flat[:, c], minlength=n) for c in range(flat.shape[1])], 1)
+    return out.reshape((n,) + v.shape[1:])
+
+
 def coarse_grain(q_fine, groups, n_coarse, coarse_mesh, fine_mesh):
     """Fine Q summed per coarse cell, rescaled to the coarse cell's volume (densities kept, totals conserved up to the
     two meshes' volume difference)."""
-    q = np.zeros((n_coarse, q_fine.shape[1]))
-    vol = np.zeros(n_coarse)
-    np.add.at(q, groups, q_fine)
-    np.add.at(vol, groups, fine_mesh.volume)
+    q = _group_sum(groups, q_fine, n_coarse)
+    vol = _group_sum(groups, fine_mesh.volume, n_coarse)
     return q * (coarse_mesh.volume / vol)[:, None]
 
 
@@ -112,21 +120,13 @@ def subcell_slopes(fine_mesh, W_fine, groups, coarse_mesh):
     d -= box * np.round(d / box)
     V = fine_mesh.volume
     n = coarse_mesh.n_cells
-    # weighted means
-    sv = np.zeros(n)
-    np.add.at(sv, groups, V)
-    dm = np.zeros((n, 2))
-    np.add.at(dm, groups, V[:, None] * d)
-    dm /= sv[:, None]
-    wm = np.zeros((n, W_fine.shape[1]))
-    np.add.at(wm, groups, V[:, None] * W_fine)
-    wm /= sv[:, None]
+    sv = _group_sum(groups, V, n)
+    dm = _group_sum(groups, V[:, None] * d, n) / sv[:, None]
+    wm = _group_sum(groups, V[:, None] * W_fine, n) / sv[:, None]
     dd = d - dm[groups]
     dw = W_fine - wm[groups]
-    C = np.zeros((n, 2, 2))
-    np.add.at(C, groups, V[:, None, None] * dd[:, :, None] * dd[:, None, :])
-    B = np.zeros((n, 2, W_fine.shape[1]))
-    np.add.at(B, groups, V[:, None, None] * dd[:, :, None] * dw[:, None, :])
+    C = _group_sum(groups, V[:, None, None] * dd[:, :, None] * dd[:, None, :], n)
+    B = _group_sum(groups, V[:, None, None] * dd[:, :, None] * dw[:, None, :], n)
     return np.linalg.solve(C, B).transpose(0, 2, 1)  # [n][var][dim]
 
 
@@ -219,6 +219,62 @@ def build_dataset_2d(problems, n=256, factor=4, gamma=GAMMA, snapshots=(0.25, 0.
     groups = group_index(factor * n, factor * n, factor)
     return _dataset(coarse, fine, groups, [quadrant_problem(s) for s in problems], quadrant_state, gamma, snapshots, travel,
                     log, f"2D {n}^2 quadrants, gamma {gamma:g}")
+
+
+# Directions of the oblique 3D problems: integer normals, so that n . x mod 1 is periodic in the unit cube.
+DIRECTIONS = ((1, 1, 1), (1, 1, 0), (1, 0, 1), (0, 1, 1), (1, -1, 1), (2, 1, 0), (1, 2, 1), (1, 0, 0))
+
+
+@dataclass
+class Oblique:
+    """A 1D Riemann problem across planes of integer normal n in the periodic unit cube: the left state where
+    frac(n . x) lies in [0.25, 0.75), the right one elsewhere; the velocity along n."""
+    riemann: Riemann
+    normal: tuple
+
+    def max_speed(self, gamma=GAMMA) -> float:
+        return self.riemann.max_speed(gamma)
+
+
+def oblique_problem(seed: int) -> Oblique:
+    return Oblique(riemann_problem(seed), DIRECTIONS[seed % len(DIRECTIONS)])
+
+
+def cube(n: int, seed: int = 1):
+    """A periodic unit cube of n^3 jittered (0.1) cells."""
+    return build_mesh(jittered_points((n, n, n), jitter=0.1, seed=seed), box=(1.0, 1.0, 1.0))
+
+
+def oblique_state(mesh, prob: Oblique, gamma=GAMMA) -> np.ndarray:
+    n = np.asarray(prob.normal, dtype=np.float64)
+    s = cell_centres(mesh) @ n
+    left = (s - np.floor(s) >= 0.25) & (s - np.floor(s) < 0.75)
+    unit = n / np.linalg.norm(n)
+    W = np.zeros((mesh.n_cells, 5))
+    r = prob.riemann
+    for a, side in ((0, left), (1, ~left)):
+        W[side, 0] = r.rho[a]
+        W[side, 1:4] = r.u[a] * unit
+        W[side, 4] = r.p[a]
+    return conserved(W, gamma) * mesh.volume[:, None]
+
+
+def group_index_3d(n_f, factor):
+    """Coarse cell of each fine cell of two cubic lattices (jittered_points orders i, j, then k)."""
+    idx = np.arange(n_f ** 3)
+    i, j, k = idx // (n_f * n_f), (idx // n_f) % n_f, idx % n_f
+    n_c = n_f // factor
+    return ((i // factor) * n_c + j // factor) * n_c + k // factor
+
+
+def build_dataset_3d(problems, n=32, factor=4, gamma=GAMMA, snapshots=(0.25, 0.5, 0.75, 1.0), travel=0.2, log=print):
+    """3D rows from the 1D problems: each seeded Riemann problem across oblique planes (DIRECTIONS) of an n^3 jittered
+    cube, labelled from the method's own run on (factor n)^3 cells, coarse-grained by lattice index. These give the
+    network rows in which all three velocity slots are active, as on a 3D mesh."""
+    coarse, fine = cube(n, seed=11), cube(factor * n, seed=12)
+    groups = group_index_3d(factor * n, factor)
+    return _dataset(coarse, fine, groups, [oblique_problem(s) for s in problems], oblique_state, gamma, snapshots, travel,
+                    log, f"3D oblique {n}^3, gamma {gamma:g}")
 
 
 def build_dataset(problems, nx=1024, ny=4, factor=4, gamma=GAMMA, snapshots=(0.25, 0.5, 0.75, 1.0), travel=0.2, log=print):
@@ -374,6 +430,8 @@ def main():
     ap.add_argument("--n2d", type=int, default=256)
     ap.add_argument("--gammas", default="1.4,1.6666666666666667", help="the data's adiabatic indices")
     ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--train-problems-3d", type=int, default=12, help="1D problems across oblique planes of n3d^3 cubes")
+    ap.add_argument("--n3d", type=int, default=24)
     ap.add_argument("--moving-nx", type=int, default=0, help="also judge on the 3D moving blast at this size (0: no)")
     ap.add_argument("--out", default="limiter_out/limiter")
     args = ap.parse_args()
@@ -392,10 +450,14 @@ def main():
         if args.train_problems_2d > 0:
             parts.append(build_dataset_2d(range(2000 + 100 * k, 2000 + 100 * k + args.train_problems_2d), n=args.n2d, gamma=gamma,
                                           log=log))
+        if args.train_problems_3d > 0:
+            parts.append(build_dataset_3d(range(3000 + 100 * k, 3000 + 100 * k + args.train_problems_3d), n=args.n3d, gamma=gamma,
+                                          snapshots=(0.5, 1.0), log=log))
     x, t, w = (torch.cat([p[c] for p in parts]) for c in range(3))
     net = train(x, t, w, epochs=args.epochs, log=log)
     np.save(args.out + "_params.npy", net.state())
-    report = {"train_problems": args.train_problems, "train_problems_2d": args.train_problems_2d, "gammas": args.gammas,
+    report = {"train_problems": args.train_problems, "train_problems_2d": args.train_problems_2d,
+              "train_problems_3d": args.train_problems_3d, "n3d": args.n3d, "gammas": args.gammas,
               "epochs": args.epochs, "nx": args.nx, "ny": args.ny, "n2d": args.n2d, "rows": len(x)}
     rows = evaluate(net, range(5000, 5000 + args.test_problems), nx=args.nx, ny=args.ny, log=log)
     report["strips"] = {"summary": summarize(rows), "rows": rows}

@@ -80,9 +80,9 @@ def test_builder_matches_qhull(name, points, dim):
     assert np.max(np.abs(vol - m.volume) / m.volume) < 1e-13
 
 
-def test_dual_cells_match_qhull():
-    """The builder with its cells kept as triangles of plane triples (LUNA_MESH_DUAL=1, read once per process: a
-    subprocess) against qhull and the Voronoi invariants."""
+def test_face_loop_cells_match_qhull():
+    """The builder with its 3D cells kept as face loops (LUNA_MESH_DUAL=0, read once per process: a subprocess; the
+    default keeps them as triangles of plane triples) against qhull and the Voronoi invariants."""
     import os
     import subprocess
     import sys
@@ -99,6 +99,31 @@ def test_dual_cells_match_qhull():
         "    voronoi_invariants(build_mesh(points(), box=(1.0,) * dim))\n"
         "print('ok')\n"
     )
-    r = subprocess.run([sys.executable, "-c", code], cwd=root, env=dict(os.environ, LUNA_MESH_DUAL="1"), capture_output=True,
+    r = subprocess.run([sys.executable, "-c", code], cwd=root, env=dict(os.environ, LUNA_MESH_DUAL="0"), capture_output=True,
                        text=True, timeout=600)
     assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stderr[-2000:]
+
+
+def test_degenerate_lattices():
+    """The exact regular lattice of the rollout server (rollout.lattice: four or more bisector planes meet at every
+    vertex) gives the regular mesh: every cell a cube of the lattice's volume with 6 faces of area h^2, the invariants
+    hold. Moved by ~1e-9 the near-degenerate vertices are still resolved (the invariants hold). Moved by ~1e-12 the
+    builder either gives a mesh that satisfies the invariants or refuses the points with an error, never a broken mesh."""
+    from conftest import voronoi_invariants
+    from luna_cpp_b200.mesh import build_mesh
+    from luna_cpp_b200.rollout import lattice
+
+    for n in (5, 8):
+        m = build_mesh(lattice(n, 3))
+        voronoi_invariants(m)
+        assert m.n_faces == 3 * n ** 3
+        assert np.allclose(m.volume, 1.0 / n ** 3, rtol=1e-7)
+        assert np.allclose(np.linalg.norm(m.area, axis=1), 1.0 / n ** 2, rtol=1e-7)
+    m = build_mesh(lattice(6, 3) + np.random.default_rng(2).uniform(-1e-9, 1e-9, (216, 3)))
+    voronoi_invariants(m)
+    try:
+        m = build_mesh(lattice(8, 3) + np.random.default_rng(1).uniform(-1e-12, 1e-12, (512, 3)))
+    except ValueError as e:
+        assert "more vertices or faces" in str(e)
+    else:
+        voronoi_invariants(m)
