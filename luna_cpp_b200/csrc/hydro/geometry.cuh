@@ -81,11 +81,13 @@ struct GeometryDev {
 // the faces the cell owns and the largest face angle. g.nbr holds each entry's staged row on entry (from the host's
 // tiles); the kernel adds the owned and tiny bits.
 // Both walks take the list in batches of LUNA_GEOMETRY_BATCH entries whose loads are all issued before any is used:
-// the entries' list words, then their faces' cells and |A| (and the face rows' area and centroid), then the neighbours'
-// generators and centroids: three dependent load levels a batch instead of three an entry (the kernel is bound by
-// these gathers; on a moving mesh it runs after every remesh). The arithmetic is the per-entry one, in list order.
+// the entries' list words, then their faces' cells and |A| (and the face's centroid), then the neighbours' generators
+// and centroids. The cell's own generator is read once and each face offset is formed from the loaded rows. The
+// arithmetic is the per-entry one, in list order. Measured on the 128^3 moving blast's hydro part (the rows rebuilt
+// every step): batches of 1, 2, 4 entries 5.16, 5.44, 6.08 ms a step (the larger batches' registers cost occupancy),
+// against 5.8 ms before the own generator and the offsets were taken from registers.
 #ifndef LUNA_GEOMETRY_BATCH
-#define LUNA_GEOMETRY_BATCH 4
+#define LUNA_GEOMETRY_BATCH 1
 #endif
 template <int D, class G>
 __global__ void __launch_bounds__(128) k_geometry(MeshDev<D> m, GeometryDev<D, G> g) {
@@ -832,18 +834,12 @@ __global__ void k_apply_factors(int rows, const int* __restrict__ cells, const u
 #ifndef LUNA_FLUX_MIN_BLOCKS
 #define LUNA_FLUX_MIN_BLOCKS 6
 #endif
-// OP: the owner-partial layout (kernels.cuh, OwnerPartials): the row goes to the neighbour's run and the owner's side
-// is summed per warp segment.
-template <int D, int Order, class G, bool RF, int Riemann, bool H = false, bool WG = false, class FS = double, bool OP = false>
+template <int D, int Order, class G, bool RF, int Riemann, bool H = false, bool WG = false, class FS = double>
 __global__ void __launch_bounds__(128, LUNA_FLUX_MIN_BLOCKS) k_flux_rows(MeshDev<D> m, GeometryDev<D, G> geo, FluxArgs<D, G> x, FS* __restrict__ flux,
-                                                   unsigned long long* __restrict__ fallbacks, OwnerPartials op = {}) {
+                                                   unsigned long long* __restrict__ fallbacks) {
     constexpr int V = D + 2;
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     int count = 0;
-    double F[V];
-    int owner = -1;
-#pragma unroll
-    for (int v = 0; v < V; ++v) F[v] = 0;
     if (f < m.f) {
         FaceRow<G> r;
         {  // the 32-B aligned row in vector loads, streamed once per step
@@ -853,7 +849,7 @@ __global__ void __launch_bounds__(128, LUNA_FLUX_MIN_BLOCKS) k_flux_rows(MeshDev
             for (int c = 0; c < static_cast<int>(sizeof(FaceRow<G>) / 8); c += 4)
                 ldg256_hint(reinterpret_cast<const double*>(geo.faces + f) + c, words + c, once);
         }
-        owner = r.o;
+        double F[V];
         if (r.mag == 0) {
 #pragma unroll
             for (int v = 0; v < V; ++v) F[v] = 0;
@@ -887,9 +883,8 @@ __global__ void __launch_bounds__(128, LUNA_FLUX_MIN_BLOCKS) k_flux_rows(MeshDev
 #pragma unroll
             for (int v = 0; v < V; ++v) F[v] *= r.mag;
         }
-        if constexpr (!OP) store_flux_row<D, FS>(flux, f, F);
+        store_flux_row<D, FS>(flux, f, F);
     }
-    if constexpr (OP) owner_partial_epilogue<D, FS>(op, flux, f, f < m.f, owner, F);
     block_sum_to(static_cast<unsigned long long>(count), fallbacks);
 }
 

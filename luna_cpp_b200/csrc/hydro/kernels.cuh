@@ -692,123 +692,6 @@ __global__ void __launch_bounds__(256, Windowed ? LUNA_UPDATE_MIN_BLOCKS : 1) k_
     }
 }
 
-// apply()'s update without gathers, for a static mesh whose faces are numbered by owner (voronoi-cpp's owner_faces
-// layout, which FiniteVolume's fast_layout asks for on a static mesh, finite_volume.hpp:118-127). The flux pass writes
-// each face's row at its neighbour's side, in the order of the neighbours' lists (faces by neighbour: cell i's
-// non-owned entries are one contiguous run), and sums the owner's side itself: each warp adds its faces of one owner
-// (a fixed shuffle tree, the same bits run to run) into one partial row per (owner, warp) segment. The update then
-// streams its run and its one or two partials: Q_i -= dt (-sum of the run in list order + the owner's partials in face
-// order), no list walk and no gathered rows. The sums differ from the list-order sum only in rounding.
-struct OwnerPartials {
-    const int32_t* __restrict__ nslot;  // [F]: the face's row among the rows by neighbour
-    const int32_t* __restrict__ ns;     // [N + 1]: cell i's run of non-owned rows
-    const int32_t* __restrict__ fs;     // [N + 1]: cell i's owned faces (faces numbered by owner)
-    const int32_t* __restrict__ seg;    // [N + 1]: cell i's partial rows (one per warp its owned faces span)
-    double* __restrict__ partial;       // [segments][V]
-};
-
-// In the flux pass, after each lane has its face's flux F (zeros and a key of its own for a lane without a face): the
-// neighbour's row, and the segmented warp sum of the owner's side.
-template <int D, class FS>
-__device__ __forceinline__ void owner_partial_epilogue(const OwnerPartials& op, FS* flux, int f, bool active, int owner, double* F) {
-    constexpr int V = D + 2;
-    const int lane = threadIdx.x & 31;
-    if constexpr (sizeof(FS) == sizeof(float)) {  // the stored row's values (FluxStore = float) are the ones summed
-#pragma unroll
-        for (int v = 0; v < V; ++v) F[v] = static_cast<double>(static_cast<float>(F[v]));
-    }
-    if (active) store_flux_row<D, FS>(flux, op.nslot[f], F);
-    const int key = active ? owner : -1 - lane;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const int up_key = __shfl_up_sync(0xffffffffu, key, d);
-        double up[V];
-#pragma unroll
-        for (int v = 0; v < V; ++v) up[v] = __shfl_up_sync(0xffffffffu, F[v], d);
-        if (lane >= d && up_key == key) {
-#pragma unroll
-            for (int v = 0; v < V; ++v) F[v] += up[v];
-        }
-    }
-    const int next_key = __shfl_down_sync(0xffffffffu, key, 1);
-    if (active && (lane == 31 || next_key != key)) {
-        const int64_t s = op.seg[owner] + (f >> 5) - (op.fs[owner] >> 5);
-#pragma unroll
-        for (int v = 0; v < V; ++v) op.partial[V * s + v] = F[v];
-    }
-}
-
-// The update of the owner-partial layout (see OwnerPartials), writing the next primitive rows as k_update does.
-template <int D, class FS>
-__global__ void __launch_bounds__(256, 4) k_update_partials(MeshDev<D> m, OwnerPartials op, double* __restrict__ q, const FS* __restrict__ flux,
-                                                            double dt, double* __restrict__ prims, GasDev gas, Counters* __restrict__ ctr) {
-    constexpr int V = D + 2, S = flux_stride<D, FS>();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m.n) return;
-    double sum[V];
-#pragma unroll
-    for (int v = 0; v < V; ++v) sum[v] = 0;
-    const int first = op.ns[i], end = op.ns[i + 1];
-    constexpr int kBatch = 4;
-    for (int k0 = first; k0 < end; k0 += kBatch) {
-        double row[kBatch][V];
-#pragma unroll
-        for (int b = 0; b < kBatch; ++b) {
-            if (k0 + b < end) {
-                if constexpr (sizeof(FS) == sizeof(float)) {
-                    float w[8];
-                    if constexpr (S == 8) {
-                        ldg256(reinterpret_cast<const float*>(flux) + S * static_cast<int64_t>(k0 + b), w);
-                    } else {
-                        const float4 t = __ldg(reinterpret_cast<const float4*>(reinterpret_cast<const float*>(flux) + S * static_cast<int64_t>(k0 + b)));
-                        w[0] = t.x, w[1] = t.y, w[2] = t.z, w[3] = t.w;
-                    }
-#pragma unroll
-                    for (int v = 0; v < V; ++v) row[b][v] = static_cast<double>(w[v]);
-                } else {
-                    const double* r = reinterpret_cast<const double*>(flux) + V * static_cast<int64_t>(k0 + b);
-#pragma unroll
-                    for (int v = 0; v < V; ++v) row[b][v] = __ldg(r + v);
-                }
-            }
-        }
-#pragma unroll
-        for (int b = 0; b < kBatch; ++b) {
-            if (k0 + b >= end) break;
-#pragma unroll
-            for (int v = 0; v < V; ++v) sum[v] += -1.0 * row[b][v];
-        }
-    }
-    for (int s = op.seg[i]; s < op.seg[i + 1]; ++s) {
-#pragma unroll
-        for (int v = 0; v < V; ++v) sum[v] += op.partial[V * static_cast<int64_t>(s) + v];
-    }
-    double next[V];
-    bool finite = true;
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-        next[v] = q[V * i + v] - dt * sum[v];
-        q[V * i + v] = next[v];
-        finite = finite && isfinite(next[v]);
-    }
-    if (!finite) atomicOr(&ctr->error, 2ull);
-    const double inv = 1.0 / m.vol[i];
-    double U[V], W[V];
-#pragma unroll
-    for (int v = 0; v < V; ++v) U[v] = next[v] * inv;
-    primitive<D>(U, gas, W);
-    double prow[PS];
-#pragma unroll
-    for (int v = 0; v < V; ++v) prow[v] = W[v];
-    prow[V] = sqrt(gas.gamma * W[D + 1] / W[0]);
-    prow[V + 1] = radius<D>(m.vol[i]);
-#pragma unroll
-    for (int c = V + 2; c < PS; ++c) prow[c] = 0.0;
-    double2* p = reinterpret_cast<double2*>(prims + PS * static_cast<int64_t>(i));
-#pragma unroll
-    for (int c = 0; c < PS; c += 2) p[c / 2] = make_double2(prow[c], prow[c + 1]);
-}
-
 // apply()'s per-cell loop (finite_volume.hpp:1543-1562): each cell computes the fluxes of its faces itself, in list order.
 template <int D, int Order, class G, bool RF, int Riemann, bool H = false>
 __global__ void __launch_bounds__(128) k_fluxes_and_update(MeshDev<D> m, FluxArgs<D, G> x, double* __restrict__ next, double dt,

@@ -111,11 +111,6 @@ struct luna_fv {
     DevArray<uint32_t> grad16_exp;  // Grad16: the rows' group exponents [N]
     DevArray<int32_t> steps;
     DevArray<luna::Counters> counters;
-    // the owner-partial layout of a static per-face step (kernels.cuh, OwnerPartials), built with the host tiles when the
-    // faces are numbered by owner
-    DevArray<int32_t> op_nslot, op_ns, op_fs, op_seg;
-    DevArray<double> op_partial;
-    bool owner_partials = false;
     // the mesh reordered for the step (geometry.cuh), rebuilt by every load_mesh
     DevArray<unsigned char> geo_c01, geo_c2, geo_off01, geo_off2, geo_faces;
     DevArray<unsigned int> geo_nbr;
@@ -200,10 +195,6 @@ struct luna_fv {
         g.reach2 = geo_reach2.ptr;
         g.threads = tiles * luna::kTileCells;
         return g;
-    }
-
-    luna::OwnerPartials owner_partials_dev() const {
-        return luna::OwnerPartials{op_nslot.ptr, op_ns.ptr, op_fs.ptr, op_seg.ptr, op_partial.ptr};
     }
 
     template <int D>
@@ -380,42 +371,6 @@ luna_status check_device_lists(luna_fv* fv, int64_t N, int64_t F) {
     return LUNA_OK;
 }
 
-// The owner-partial layout (kernels.cuh, OwnerPartials) of a static per-face step, from host lists: used when the faces
-// are numbered by owner and every face has exactly one non-owned list entry; otherwise the step keeps the list-walking
-// update (k_update).
-luna_status build_owner_partials(luna_fv* fv, int64_t N, int64_t F, const int32_t* start, const int32_t* list, const int32_t* owner) {
-    fv->owner_partials = false;
-    if (fv->motion != LUNA_STATIC_MESH || fv->update != LUNA_UPDATE_PER_FACE || F == 0) return LUNA_OK;
-    for (int64_t f = 1; f < F; ++f)
-        if (owner[f] < owner[f - 1]) return LUNA_OK;
-    std::vector<int32_t> fs(N + 1, 0), seg(N + 1, 0), ns(N + 1, 0), nslot(F, -1);
-    for (int64_t f = 0; f < F; ++f) ++fs[owner[f] + 1];
-    for (int64_t i = 0; i < N; ++i) fs[i + 1] += fs[i];
-    for (int64_t i = 0; i < N; ++i) seg[i + 1] = seg[i] + (fs[i + 1] > fs[i] ? (fs[i + 1] - 1) / 32 - fs[i] / 32 + 1 : 0);
-    int64_t cursor = 0;
-    for (int64_t i = 0; i < N; ++i) {
-        ns[i] = static_cast<int32_t>(cursor);
-        for (int32_t k = start[i]; k < start[i + 1]; ++k) {
-            const int32_t e = list[k];
-            if (e >= 0) continue;
-            const int64_t f = ~e;
-            if (f >= F || nslot[f] >= 0) return LUNA_OK;  // a face seen twice from its neighbour side: keep k_update
-            nslot[f] = static_cast<int32_t>(cursor++);
-        }
-    }
-    ns[N] = static_cast<int32_t>(cursor);
-    if (cursor != F) return LUNA_OK;
-    cudaStream_t s = fv->stream;
-    LUNA_TRY(upload(fv->op_nslot, nslot.data(), F, false, s, "owner partials"));
-    LUNA_TRY(upload(fv->op_ns, ns.data(), N + 1, false, s, "owner partials"));
-    LUNA_TRY(upload(fv->op_fs, fs.data(), N + 1, false, s, "owner partials"));
-    LUNA_TRY(upload(fv->op_seg, seg.data(), N + 1, false, s, "owner partials"));
-    LUNA_TRY(fv->op_partial.alloc(static_cast<size_t>(seg[N]) * (fv->dim + 2) + 1, "owner partial rows"));
-    LUNA_CUDA(cudaStreamSynchronize(s));  // the host vectors go out of scope
-    fv->owner_partials = true;
-    return LUNA_OK;
-}
-
 luna_status load_mesh(luna_fv* fv, const luna_mesh_desc* m) {
     const int D = m->dim;
     const size_t N = static_cast<size_t>(m->n_cells), F = static_cast<size_t>(m->n_faces);
@@ -477,7 +432,6 @@ luna_status load_mesh(luna_fv* fv, const luna_mesh_desc* m) {
     luna::SweepTiles tiles;
     const std::string why = luna::build_sweep_tiles(D, static_cast<int64_t>(N), pos, m->box, start, list, own, nbr, tiles);
     if (!why.empty()) return set_error(LUNA_EINVAL, "mesh: " + why);
-    LUNA_TRY(build_owner_partials(fv, static_cast<int64_t>(N), static_cast<int64_t>(F), start, list, own));
     return build_geometry(fv, tiles);
 }
 
@@ -613,12 +567,7 @@ luna_status launch_flux_rows(luna_fv* fv, const luna::FluxArgs<D, G>& x) {
     if (fv->f == 0) return LUNA_OK;
     {
         const long timed_ = fv->open_timed(2);
-        if (fv->owner_partials)
-            luna::k_flux_rows<D, Order, G, RF, Riemann, H, WG, FS, true><<<blocks(fv->f, kBlockFaces), kBlockFaces, 0, fv->stream>>>(
-                fv->mesh_dev<D>(), fv->geometry_dev<D, G>(), x, reinterpret_cast<FS*>(fv->flux.ptr), &fv->counters.ptr->fallbacks[0],
-                fv->owner_partials_dev());
-        else
-            luna::k_flux_rows<D, Order, G, RF, Riemann, H, WG, FS><<<blocks(fv->f, kBlockFaces), kBlockFaces, 0, fv->stream>>>(
+        luna::k_flux_rows<D, Order, G, RF, Riemann, H, WG, FS><<<blocks(fv->f, kBlockFaces), kBlockFaces, 0, fv->stream>>>(
                 fv->mesh_dev<D>(), fv->geometry_dev<D, G>(), x, reinterpret_cast<FS*>(fv->flux.ptr), &fv->counters.ptr->fallbacks[0]);
         fv->close_timed(timed_);
     }
@@ -682,20 +631,9 @@ luna::FluxArgs<D, G> flux_args(luna_fv* fv, const G* grad, double dt) {
     return x;
 }
 
-// apply()'s update of the library's flux rows (windowed double rows, or single's float rows; the owner-partial layout's
-// rows and partials for a static step that has it).
+// apply()'s update of the library's flux rows (windowed double rows, or single's float rows).
 template <int D, bool NextPrims>
 void launch_update(luna_fv* fv, double dt) {
-    if (NextPrims && fv->owner_partials) {
-        if (float_flux(fv))
-            luna::k_update_partials<D, float><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(
-                fv->mesh_dev<D>(), fv->owner_partials_dev(), fv->q.ptr, reinterpret_cast<const float*>(fv->flux.ptr), dt, fv->prims.ptr, fv->gas,
-                fv->counters.ptr);
-        else
-            luna::k_update_partials<D, double><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(
-                fv->mesh_dev<D>(), fv->owner_partials_dev(), fv->q.ptr, fv->flux.ptr, dt, fv->prims.ptr, fv->gas, fv->counters.ptr);
-        return;
-    }
     if (float_flux(fv))
         luna::k_update<D, NextPrims, true, float><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(
             fv->mesh_dev<D>(), fv->q.ptr, reinterpret_cast<const float*>(fv->flux.ptr), dt, fv->prims.ptr, fv->gas, fv->counters.ptr);
