@@ -353,10 +353,19 @@ __device__ __forceinline__ bool side_value(const double* W, const double* g, con
     return fallback;
 }
 
+// Resident blocks an SM the adjoint's register-heavy kernels are cut for (1: no cap), and the list entries the gather
+// requests together.
+#ifndef LUNA_ADJ_MIN_BLOCKS
+#define LUNA_ADJ_MIN_BLOCKS 1
+#endif
+#ifndef LUNA_ADJ_GATHER_BATCH
+#define LUNA_ADJ_GATHER_BATCH 1
+#endif
+
 // The sweep again with the fit kept (Sweep<false, true, SweepFitHook<false>>): the same gradients as k_sweep's FP64
 // policy, plus fit rows [N][FitLayout::width] and flags [N][2V] (clipped | upper << 1 | zero << 2; the bound's face).
 template <int D, bool Limit>
-__global__ void __launch_bounds__(128) k_sweep_fit(MeshDev<D> m, const double* __restrict__ prims, double* __restrict__ grad_out,
+__global__ void __launch_bounds__(128, LUNA_ADJ_MIN_BLOCKS) k_sweep_fit(MeshDev<D> m, const double* __restrict__ prims, double* __restrict__ grad_out,
                                                    double* __restrict__ fit, int32_t* __restrict__ flags) {
     constexpr int V = D + 2, U = D + 1, GS = grad_stride<D>();
     using FL = FitLayout<D>;
@@ -512,7 +521,7 @@ __global__ void __launch_bounds__(128) k_sweep_fit(MeshDev<D> m, const double* _
 
 // AdjointFaces (finite_volume.hpp:2078-2102): per face, the bars of its two face states from Qbar's jump across it.
 template <int D, int Riemann>
-__global__ void __launch_bounds__(128) k_faces_adjoint(MeshDev<D> m, const double* __restrict__ prims, const double* __restrict__ grad,
+__global__ void __launch_bounds__(128, LUNA_ADJ_MIN_BLOCKS) k_faces_adjoint(MeshDev<D> m, const double* __restrict__ prims, const double* __restrict__ grad,
                                                        const double* __restrict__ qbar, double dt, GasDev gas, double* __restrict__ face_bar) {
     constexpr int V = D + 2, GS = grad_stride<D>();
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
@@ -561,7 +570,7 @@ __global__ void __launch_bounds__(128) k_faces_adjoint(MeshDev<D> m, const doubl
 
 // AdjointCell (finite_volume.hpp:2107-2169).
 template <int D>
-__global__ void __launch_bounds__(128) k_cell_adjoint(MeshDev<D> m, const double* __restrict__ prims, const double* __restrict__ grad,
+__global__ void __launch_bounds__(128, LUNA_ADJ_MIN_BLOCKS) k_cell_adjoint(MeshDev<D> m, const double* __restrict__ prims, const double* __restrict__ grad,
                                                       const double* __restrict__ face_bar, const double* __restrict__ fit,
                                                       const int32_t* __restrict__ flags, double dt, GasDev gas, double* __restrict__ wbar,
                                                       double* __restrict__ bbar, double* __restrict__ boundbar, int32_t* __restrict__ bound_face) {
@@ -677,22 +686,32 @@ __global__ void __launch_bounds__(128) k_gather_adjoint(MeshDev<D> m, const doub
     double cj[D];
 #pragma unroll
     for (int a = 0; a < D; ++a) cj[a] = m.cen[D * j + a];
-    for (int k = m.start[j]; k < m.start[j + 1]; ++k) {
-        const int32_t e = m.list[k];
-        const int f = list_face(e);
-        const int i = e >= 0 ? m.neighbour[f] : m.owner[f];
-        double sep[D], between[D];
-        m.separation(i, j, sep);
+    constexpr int B = LUNA_ADJ_GATHER_BATCH;
+    const int first = m.start[j], end = m.start[j + 1];
+    for (int k0 = first; k0 < end; k0 += B) {
+        int f[B], i[B];
 #pragma unroll
-        for (int a = 0; a < D; ++a) between[a] = sep[a] + cj[a] - m.cen[D * i + a];
-        const double w = m.mag[f];
+        for (int b = 0; b < B; ++b) {
+            const int32_t e = k0 + b < end ? m.list[k0 + b] : 0;
+            f[b] = list_face(e);
+            i[b] = k0 + b < end ? (e >= 0 ? m.neighbour[f[b]] : m.owner[f[b]]) : j;
+        }
 #pragma unroll
-        for (int v = 0; v < V; ++v) {
-            const double* bb = bbar + static_cast<int64_t>(U * V) * i + U * v;
-            double sum = bb[0];
+        for (int b = 0; b < B; ++b) {
+            if (k0 + b >= end) break;
+            double sep[D], between[D];
+            m.separation(i[b], j, sep);
 #pragma unroll
-            for (int p = 1; p < U; ++p) sum += between[p - 1] * bb[p];
-            W_bar[v] += w * sum + (bound_face[V * i + v] == f ? boundbar[V * i + v] : 0.0);
+            for (int a = 0; a < D; ++a) between[a] = sep[a] + cj[a] - m.cen[D * i[b] + a];
+            const double w = m.mag[f[b]];
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                const double* bb = bbar + static_cast<int64_t>(U * V) * i[b] + U * v;
+                double sum = bb[0];
+#pragma unroll
+                for (int p = 1; p < U; ++p) sum += between[p - 1] * bb[p];
+                W_bar[v] += w * sum + (bound_face[V * i[b] + v] == f[b] ? boundbar[V * i[b] + v] : 0.0);
+            }
         }
     }
     const double inv = 1.0 / m.vol[j];
