@@ -277,6 +277,54 @@ def build_dataset_3d(problems, n=32, factor=4, gamma=GAMMA, snapshots=(0.25, 0.5
                     log, f"3D oblique {n}^3, gamma {gamma:g}")
 
 
+@dataclass
+class Blast:
+    """A point blast in the periodic unit cube: energy E deposited evenly (by volume) as thermal energy in the cells whose
+    centroid lies within r0 of the centre c, in a uniform gas of density rho and pressure p; run to t_end, when a Sedov
+    blast wave has reached a radius of about 0.3 (R = 1.15 (E t^2 / rho)^(1/5))."""
+    energy: float
+    rho: float
+    p: float
+    r0: float
+    centre: tuple
+
+    @property
+    def t_end(self) -> float:
+        return 0.035 * math.sqrt(self.rho / self.energy)
+
+    def max_speed(self, gamma=GAMMA) -> float:  # as _dataset reads it: travel 0.2 over t_end
+        return 0.2 / self.t_end
+
+
+def blast_problem(seed: int, cell: float = 1.0 / 32) -> Blast:
+    """Energy log-uniform in [0.3, 3], density in [0.3, 3], pressure in [1e-6, 1e-3]; the deposit radius 1.5 to 3 coarse
+    cells; the centre uniform in [0.4, 0.6]^3."""
+    rng = np.random.default_rng(seed)
+    return Blast(float(10 ** rng.uniform(np.log10(0.3), np.log10(3))), float(10 ** rng.uniform(np.log10(0.3), np.log10(3))),
+                 float(10 ** rng.uniform(-6, -3)), float(rng.uniform(1.5, 3.0) * cell), tuple(float(x) for x in rng.uniform(0.4, 0.6, 3)))
+
+
+def blast_state(mesh, prob: Blast, gamma=GAMMA) -> np.ndarray:
+    d = cell_centres(mesh) - np.asarray(prob.centre)
+    d -= np.round(d)
+    inside = np.sqrt(np.sum(d * d, 1)) < prob.r0
+    W = np.zeros((mesh.n_cells, 5))
+    W[:, 0] = prob.rho
+    W[:, 4] = prob.p
+    Q = conserved(W, gamma) * mesh.volume[:, None]
+    Q[inside, 4] += prob.energy * mesh.volume[inside] / mesh.volume[inside].sum()
+    return Q
+
+
+def build_dataset_blast(problems, n=32, factor=4, gamma=5.0 / 3.0, snapshots=(0.2, 0.5, 1.0), log=print):
+    """3D rows from point blasts of random energy, density, pressure, deposit radius and centre (seeds) on an n^3 jittered
+    cube, labelled from the method's own run on (factor n)^3 cells (the deposit the same physical sphere)."""
+    coarse, fine = cube(n, seed=11), cube(factor * n, seed=12)
+    groups = group_index_3d(factor * n, factor)
+    return _dataset(coarse, fine, groups, [blast_problem(s, 1.0 / n) for s in problems], blast_state, gamma, snapshots, 0.2, log,
+                    f"3D point blasts {n}^3, gamma {gamma:g}")
+
+
 def build_dataset(problems, nx=1024, ny=4, factor=4, gamma=GAMMA, snapshots=(0.25, 0.5, 0.75, 1.0), travel=0.2, log=print):
     """The 1D part of the training data: 1D Riemann problems (seeds) across quasi-1D strips of nx x ny cells, labelled
     from the method's own run on a strip of factor x the cells along each axis."""
@@ -432,6 +480,7 @@ def main():
     ap.add_argument("--epochs", type=int, default=20)
     ap.add_argument("--train-problems-3d", type=int, default=12, help="1D problems across oblique planes of n3d^3 cubes")
     ap.add_argument("--n3d", type=int, default=24)
+    ap.add_argument("--train-blasts", type=int, default=0, help="3D point blasts of random parameters (gamma 5/3, n3d^3)")
     ap.add_argument("--moving-nx", type=int, default=0, help="also judge on the 3D moving blast at this size (0: no)")
     ap.add_argument("--out", default="limiter_out/limiter")
     args = ap.parse_args()
@@ -453,11 +502,13 @@ def main():
         if args.train_problems_3d > 0:
             parts.append(build_dataset_3d(range(3000 + 100 * k, 3000 + 100 * k + args.train_problems_3d), n=args.n3d, gamma=gamma,
                                           snapshots=(0.5, 1.0), log=log))
+    if args.train_blasts > 0:
+        parts.append(build_dataset_blast(range(4000, 4000 + args.train_blasts), n=args.n3d, log=log))
     x, t, w = (torch.cat([p[c] for p in parts]) for c in range(3))
     net = train(x, t, w, epochs=args.epochs, log=log)
     np.save(args.out + "_params.npy", net.state())
     report = {"train_problems": args.train_problems, "train_problems_2d": args.train_problems_2d,
-              "train_problems_3d": args.train_problems_3d, "n3d": args.n3d, "gammas": args.gammas,
+              "train_problems_3d": args.train_problems_3d, "n3d": args.n3d, "train_blasts": args.train_blasts, "gammas": args.gammas,
               "epochs": args.epochs, "nx": args.nx, "ny": args.ny, "n2d": args.n2d, "rows": len(x)}
     rows = evaluate(net, range(5000, 5000 + args.test_problems), nx=args.nx, ny=args.ny, log=log)
     report["strips"] = {"summary": summarize(rows), "rows": rows}
