@@ -85,7 +85,8 @@ struct GeometryDev {
 // and centroids. The cell's own generator is read once and each face offset is formed from the loaded rows. The
 // arithmetic is the per-entry one, in list order. Measured on the 128^3 moving blast's hydro part (the rows rebuilt
 // every step): batches of 1, 2, 4 entries 5.16, 5.44, 6.08 ms a step (the larger batches' registers cost occupancy),
-// against 5.8 ms before the own generator and the offsets were taken from registers.
+// against 5.8 ms before the own generator and the offsets were taken from registers; 16 lanes a cell (the fit's sums
+// by a shuffle tree) 6.55 ms.
 #ifndef LUNA_GEOMETRY_BATCH
 #define LUNA_GEOMETRY_BATCH 1
 #endif
@@ -270,172 +271,6 @@ __global__ void __launch_bounds__(128) k_geometry(MeshDev<D> m, GeometryDev<D, G
     }
     g.max_angle[i] = max_angle;
     g.reach2[i] = reach2;
-}
-
-// The same rows with 16 lanes a cell (two cells a warp): lane l takes the cell's list entries l, l + 16, ...; the fit's
-// sums, the surface, the smallest face and the largest face angle are combined by a fixed shuffle tree (the same bits
-// run to run; the fit's matrix rounded in another order than the one-thread walk's); every lane factors M, then forms
-// its entries' rows. The gathers of a cell's entries are in flight together instead of one entry after another.
-template <int D, class G>
-__global__ void __launch_bounds__(128) k_geometry_lanes(MeshDev<D> m, GeometryDev<D, G> g) {
-    constexpr int U = D + 1, L = 16, MU = U * (U + 1) / 2;
-    const int64_t gt = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const int64_t t = gt / L;  // the cell's place in sweep order
-    const int lane = static_cast<int>(threadIdx.x & (L - 1));
-    const unsigned mask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
-    const int i = t < g.threads ? g.order[t] : -1;
-    if (__all_sync(0xffffffffu, i < 0)) return;
-    double centroid[D], pi[D];
-    int first = 0, end = 0;
-    if (i >= 0) {
-#pragma unroll
-        for (int a = 0; a < D; ++a) {
-            centroid[a] = m.cen[D * i + a];
-            pi[a] = m.pos[D * i + a];
-        }
-        first = m.start[i];
-        end = m.start[i + 1];
-    }
-    double surface = 0, smallest = __longlong_as_double(0x7ff0000000000000ll), max_angle = 0, M[MU];
-#pragma unroll
-    for (int q = 0; q < MU; ++q) M[q] = 0;
-    for (int k = first + lane; k < end; k += L) {
-        const int32_t e = m.list[k];
-        const int f = list_face(e);
-        const int j = e >= 0 ? m.neighbour[f] : m.owner[f];
-        double d[D], X[U];
-#pragma unroll
-        for (int a = 0; a < D; ++a) d[a] = m.wrap(m.pos[D * j + a] - pi[a], a);
-        const double magnitude = m.mag[f];
-        surface += magnitude;
-        smallest = fmin(smallest, magnitude);
-        max_angle = fmax(max_angle, face_angle<D>(magnitude) / (0.5 * sqrt(dot<D>(d, d))));
-        X[0] = 1;
-#pragma unroll
-        for (int p = 1; p < U; ++p) X[p] = d[p - 1] + m.cen[D * j + p - 1] - centroid[p - 1];
-        int q = 0;
-#pragma unroll
-        for (int p = 0; p < U; ++p)
-#pragma unroll
-            for (int s2 = p; s2 < U; ++s2) M[q++] += magnitude * X[p] * X[s2];
-    }
-#pragma unroll
-    for (int o = L / 2; o > 0; o >>= 1) {
-        surface += __shfl_xor_sync(mask, surface, o, L);
-        smallest = fmin(smallest, __shfl_xor_sync(mask, smallest, o, L));
-        max_angle = fmax(max_angle, __shfl_xor_sync(mask, max_angle, o, L));
-#pragma unroll
-        for (int q = 0; q < MU; ++q) M[q] += __shfl_xor_sync(mask, M[q], o, L);
-    }
-    if (i < 0) return;
-    double Lc[U][U];
-    {
-        double Mf[U][U];
-        int q = 0;
-#pragma unroll
-        for (int p = 0; p < U; ++p)
-#pragma unroll
-            for (int s2 = p; s2 < U; ++s2) Mf[p][s2] = M[q++];
-#pragma unroll
-        for (int p = 0; p < U; ++p)
-#pragma unroll
-            for (int s2 = 0; s2 < U; ++s2) Lc[p][s2] = 0;
-#pragma unroll
-        for (int p = 0; p < U; ++p)
-#pragma unroll
-            for (int s2 = 0; s2 <= p; ++s2) {
-                double sum = Mf[s2][p];
-#pragma unroll
-                for (int r = 0; r < s2; ++r) sum -= Lc[p][r] * Lc[s2][r];
-                Lc[p][s2] = p == s2 ? sqrt(sum) : sum / Lc[s2][s2];
-            }
-    }
-    const double tiny = 1e-6 * surface;
-    const bool any_tiny = smallest < tiny;
-    const int64_t slot0 = static_cast<int64_t>(g.slice_base[t >> 5]) * 32 + (t & 31);
-    double reach2 = 0;
-    for (int k = first + lane; k < end; k += L) {
-        const int32_t e = m.list[k];
-        const int f = list_face(e);
-        const bool owned = e >= 0;
-        const int j = owned ? m.neighbour[f] : m.owner[f];
-        const int64_t slot = slot0 + 32 * static_cast<int64_t>(k - first);
-        double pj[D], cj[D], fc[D], d[D], z[U], x[U], wX[U];
-#pragma unroll
-        for (int a = 0; a < D; ++a) {
-            pj[a] = m.pos[D * j + a];
-            cj[a] = m.cen[D * j + a];
-            fc[a] = m.fcen[D * f + a];
-            d[a] = m.wrap(pj[a] - pi[a], a);
-        }
-        const double magnitude = m.mag[f];
-        wX[0] = magnitude;
-#pragma unroll
-        for (int p = 1; p < U; ++p) wX[p] = magnitude * (d[p - 1] + cj[p - 1] - centroid[p - 1]);
-#pragma unroll
-        for (int p = 0; p < U; ++p) {
-            double sum = wX[p];
-#pragma unroll
-            for (int q = 0; q < p; ++q) sum -= Lc[p][q] * z[q];
-            z[p] = sum / Lc[p][p];
-        }
-#pragma unroll
-        for (int p = U - 1; p >= 0; --p) {
-            double sum = z[p];
-#pragma unroll
-            for (int q = p + 1; q < U; ++q) sum -= Lc[q][p] * x[q];
-            x[p] = sum / Lc[p][p];
-        }
-        g.c01[slot] = Pair<G>{static_cast<G>(x[1]), static_cast<G>(x[2])};
-        if constexpr (D == 3) g.c2[slot] = static_cast<G>(x[3]);
-        double off[D];
-#pragma unroll
-        for (int a = 0; a < D; ++a) off[a] = (owned ? fc[a] : fc[a] + d[a]) - centroid[a];
-        g.off01[slot] = Pair<G>{static_cast<G>(off[0]), static_cast<G>(off[1])};
-        if constexpr (D == 3) g.off2[slot] = static_cast<G>(off[2]);
-        double r2 = 0;
-#pragma unroll
-        for (int a = 0; a < D; ++a) {
-            const double o = static_cast<double>(static_cast<G>(off[a]));
-            r2 += o * o;
-        }
-        reach2 = fmax(reach2, r2);
-        const bool tiny_face = any_tiny && magnitude < tiny;
-        g.nbr[slot] = (g.nbr[slot] & kIndexMask) | (owned ? kOwnedBit : 0u) | (tiny_face ? kTinyBit : 0u);
-        if (owned) {
-            double a[D];
-#pragma unroll
-            for (int q = 0; q < D; ++q) a[q] = m.area[D * f + q];
-            const double amag = sqrt(dot<D>(a, a));
-            double offj[D];
-#pragma unroll
-            for (int q = 0; q < D; ++q) offj[q] = (fc[q] + m.wrap(pi[q] - pj[q], q)) - cj[q];
-            FaceRow<G> r;
-            const double inv = amag == 0 ? 0.0 : 1.0 / amag;
-#pragma unroll
-            for (int q = 0; q < 3; ++q) {
-                r.n[q] = q < D ? a[q] * inv : 0.0;
-                if constexpr (sizeof(G) == sizeof(double)) {
-                    r.offo[q] = q < D ? off[q] : 0.0;
-                    r.offj[q] = q < D ? offj[q] : 0.0;
-                } else {
-                    r.offo[q] = q < D ? static_cast<float>(off[q]) : 0.0f;
-                    r.offj[q] = q < D ? static_cast<float>(offj[q]) : 0.0f;
-                }
-            }
-            r.mag = amag;
-            r.o = i;
-            r.j = j;
-            if constexpr (sizeof(G) == sizeof(double)) r.pad = 0;
-            g.faces[f] = r;
-        }
-    }
-#pragma unroll
-    for (int o = L / 2; o > 0; o >>= 1) reach2 = fmax(reach2, __shfl_xor_sync(mask, reach2, o, L));
-    if (lane == 0) {
-        g.max_angle[i] = max_angle;
-        g.reach2[i] = reach2;
-    }
 }
 
 // The sweep over the reordered rows (Sweep<Moving, Grad>::operator(), finite_volume.hpp:463-569), one block per tile:

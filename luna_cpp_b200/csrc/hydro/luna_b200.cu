@@ -220,10 +220,6 @@ struct luna_fv {
     }
 };
 
-#ifndef LUNA_GEOMETRY_LANES
-#define LUNA_GEOMETRY_LANES 0  // 1: the geometry rows with 16 lanes a cell (k_geometry_lanes), else one thread a cell
-#endif
-
 // The Riemann solve in float in the face's frame (riemann32 and single), and float flux rows (single).
 inline bool float_riemann(const luna_fv* fv) { return fv->precision == LUNA_FP32 || fv->precision == LUNA_SINGLE; }
 inline bool float_flux(const luna_fv* fv) { return fv->precision == LUNA_SINGLE; }
@@ -284,11 +280,7 @@ luna_status finish_geometry(luna_fv* fv, size_t slots) {
         // timed with the sweep: the fit's operator rows, which the reference's sweep forms every step (a moving mesh
         // forms them every step here too)
         const long timed_ = fv->open_timed(1);
-#if LUNA_GEOMETRY_LANES
-        luna::k_geometry_lanes<D, G><<<blocks(threads * 16, 128), 128, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->geometry_dev<D, G>());
-#else
         luna::k_geometry<D, G><<<blocks(threads, 128), 128, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->geometry_dev<D, G>());
-#endif
         fv->close_timed(timed_);
         LUNA_CUDA(cudaGetLastError());
     }
