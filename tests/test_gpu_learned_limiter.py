@@ -55,3 +55,15 @@ def test_2d_dataset_builds(cuda):
     assert x.shape[0] == 2 * 2 * 32 * 32
     wt = w.cpu().numpy()
     assert wt[:, 3].sum() == 0 and wt[:, [0, 1, 2, 4]].sum() > 0
+
+
+def test_3d_datasets_build(cuda):
+    """The 3D rows: a 1D problem across oblique planes and a point blast, each on 6^3 against 24^3 (all five slots
+    filled: the three velocity components are active)."""
+    from luna_cpp_b200 import limiter_training as T
+
+    for build in (T.build_dataset_3d, T.build_dataset_blast):
+        x, t, w = build([3000] if build is T.build_dataset_3d else [4000], n=6, snapshots=(1.0,), log=lambda s: None)
+        assert x.shape[0] == 6 ** 3
+        wt = w.cpu().numpy()
+        assert wt.sum() > 0 and np.all(np.isfinite(t.cpu().numpy()))

@@ -7,6 +7,7 @@ the same mesh given in host memory (tiles cut on the host). A moving step with t
 moving step with the host remesh, bit for bit.
 """
 import ctypes
+import os
 
 import numpy as np
 import pytest
@@ -22,12 +23,21 @@ pytestmark = pytest.mark.gpu
 FIELDS = ("owner", "neighbour", "cell_face_start", "cell_face", "area", "face_centroid", "centroid", "volume", "positions")
 
 
+# LUNA_MESH_DUAL=0 in the environment switches the host builder's 3D cells to face loops while the device keeps plane
+# triples: the two then agree to round-off (the same faces and lists; areas, centroids and volumes to 1e-12), not bit for
+# bit.
+HOST_FACE_LOOPS = os.environ.get("LUNA_MESH_DUAL") == "0"
+
+
 def assert_same_mesh(host, dev):
     assert (dev.n_cells, dev.n_faces, dev.inconsistent) == (host.n_cells, host.n_faces, host.inconsistent)
     for f in FIELDS:
         a, b = np.ascontiguousarray(getattr(host, f)), np.ascontiguousarray(getattr(dev, f))
         assert a.shape == b.shape, f
-        assert a.tobytes() == b.tobytes(), f
+        if HOST_FACE_LOOPS and host.dim == 3 and a.dtype.kind == "f":
+            assert np.max(np.abs(a - b)) <= 1e-12 * max(np.max(np.abs(a)), 1e-300), f
+        else:
+            assert a.tobytes() == b.tobytes(), f
 
 
 def cases():
