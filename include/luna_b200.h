@@ -220,7 +220,7 @@ LUNA_API luna_status luna_fv_device_bytes(luna_fv* fv, int64_t* out);
  * snapped to voronoi-cpp's grid (step = length 2^-30), closed by two walls (LUNA_WALL_*, inflow: the primitives
  * rho, v, P of each inflow wall, [2][3]) or periodic. Q is [lines][n_cells][3] (rho, rho v, E, extensive) in the caller's
  * cell order. limiter: LUNA_LIMITER_FACE_CENTROID (LUNA's MC on a uniform line), NONE, MINMOD, VAN_LEER; riemann:
- * LUNA_HLLC or LUNA_HLL. The moving line (cells supplied by inflow walls) and the derivatives are not covered. */
+ * LUNA_HLLC or LUNA_HLL. The moving line (cells supplied by inflow walls) is not covered. */
 typedef struct luna_line luna_line;
 /* FiniteVolume(exec, mesh, gas, order, limiter, static_mesh, walls) (finite_volume_1d.hpp:41-56). */
 LUNA_API luna_status luna_line_create(int64_t n_cells, int lines, const double* positions, double length, int periodic, const int* walls,
@@ -237,6 +237,13 @@ LUNA_API luna_status luna_line_time_step(luna_line* ln, double courant, int rule
 LUNA_API luna_status luna_line_step(luna_line* ln, const double* dt);
 /* step_and_time_step(dt, courant) (:412-418): the step and each line's next dt by LUNA's rule, one launch. Synchronises. */
 LUNA_API luna_status luna_line_step_and_time_step(luna_line* ln, const double* dt, double courant, double* dt_next);
+/* The step's derivatives at fixed dt (finite_volume_1d.hpp:852-898, FiniteVolume<1>::step_tangent / step_adjoint), each
+ * line by dt[k]; x is [lines][n_cells][3] in the caller's cell order, in device memory (on_device != 0) or host memory.
+ * step_tangent(dt, dq): dq <- J dq (J = d Q_after / d Q_before, extensive on both sides) and the state advances by the
+ * step, as luna_line_step. step_adjoint(dt, qbar): qbar <- J^T qbar, the state unchanged (the step's start). A periodic
+ * line needs 5 cells or more (the 5-cell stencil must not wrap onto itself). Synchronises when x is in host memory. */
+LUNA_API luna_status luna_line_step_tangent(luna_line* ln, const double* dt, double* dq, int on_device);
+LUNA_API luna_status luna_line_step_adjoint(luna_line* ln, const double* dt, double* qbar, int on_device);
 
 #ifdef __cplusplus
 }

@@ -19,6 +19,7 @@
 
 #include "kernels.cuh"
 #include "luna_b200.h"
+#include "tangent.cuh"
 
 namespace luna {
 luna_status report_error(luna_status s, const std::string& what);
@@ -283,6 +284,249 @@ __global__ void k_line_permute(int64_t n, int lines, const int64_t* __restrict__
     }
 }
 
+// ---- The step's derivatives at fixed dt (the reference's FiniteVolume<1>::step_tangent / step_adjoint,
+// finite_volume_1d.hpp:711-823, checked against LUNA's jax.jvp / jax.vjp). Cell s's update reads the cells s - 2 .. s + 2
+// (its two faces, each from the two cells' slopes). Both derivatives run the step's expressions on forward-mode dual
+// numbers (fwd::Dual; each branch the forward took): the tangent in one pass a slot seeded by dq; the adjoint forms each
+// row's 3 x 15 block of the band Jacobian (one pass per input) and gathers J^T w from it (no atomics: the same bits every
+// run).
+
+// primitive() (euler.hpp:104-113) on any arithmetic type: the step's operations, floors included.
+template <class T>
+__device__ __forceinline__ void primitive1(const T* U, const luna::GasDev& gas, T* W) {
+    const T rho = fmax(U[0], T(gas.smallr));
+    const T inv_rho = T(1.0) / rho;
+    const T v = U[1] * inv_rho;
+    const double smalle = gas.smallc * gas.smallc / gas.gamma / (gas.gamma - 1.0);
+    const T kinetic = T(0.5) * rho * (v * v);
+    const T e = fmax(U[2] - kinetic, T(smalle) * rho);
+    W[0] = rho;
+    W[1] = v;
+    W[2] = T(gas.gamma - 1.0) * e;
+}
+template <class T>
+__device__ __forceinline__ void ghost_t(const LineDev& L, const T* W, bool left, T* out) {
+    const int wall = L.wall[left ? 0 : 1];
+    if (wall == LUNA_WALL_REFLECTIVE) {
+        out[0] = W[0];
+        out[1] = -W[1];
+        out[2] = W[2];
+    } else if (wall == LUNA_WALL_INFLOW) {
+#pragma unroll
+        for (int v = 0; v < 3; ++v) out[v] = T(L.inflow[left ? 0 : 1][v]);
+    } else {
+#pragma unroll
+        for (int v = 0; v < 3; ++v) out[v] = W[v];
+    }
+}
+template <class T>
+__device__ __forceinline__ void ghost_face_t(const LineDev& L, const T* Wf, const T* W, bool left, T* out) {
+    if (L.wall[left ? 0 : 1] == LUNA_WALL_REFLECTIVE) {
+        out[0] = Wf[0];
+        out[1] = -Wf[1];
+        out[2] = Wf[2];
+    } else {
+        ghost_t(L, W, left, out);
+    }
+}
+struct CellT {
+    luna::fwd::Dual W[3];
+    double c;
+    bool real;
+};
+// gradient() on dual numbers (Stencil::gradient, finite_volume_1d.hpp:183-207).
+__device__ __forceinline__ luna::fwd::Dual gradient_t(const LineDev& L, const CellT* cell, double gapL, double gapR, int v) {
+    using T = luna::fwd::Dual;
+    const CellT& me = *cell;
+    const double dL = -gapL + cell[-1].c - me.c, dR = gapR + cell[1].c - me.c;
+    const T Wi = me.W[v], left = cell[-1].W[v], right = cell[1].W[v];
+    if (L.limiter == LUNA_LIMITER_MINMOD || L.limiter == LUNA_LIMITER_VAN_LEER) {
+        const T sL = (left - Wi) / T(dL), sR = (right - Wi) / T(dR);
+        if (!(sL * sR > T(0))) return T(0);
+        if (L.limiter == LUNA_LIMITER_VAN_LEER) return T(2) * sL * sR / (sL + sR);
+        return fabs(sL) < fabs(sR) ? sL : sR;
+    }
+    T g = ((right - Wi) - (left - Wi)) / T(dR - dL);
+    if (L.limiter == LUNA_LIMITER_NONE) return g;
+    const double r[2] = {-0.5 * gapL - me.c, 0.5 * gapR - me.c};
+    const T lo = fmin(left, right), hi = fmax(left, right);
+#pragma unroll
+    for (int f = 0; f < 2; ++f) {
+        const T dp = g * T(r[f]);
+        if (dp > T(0) && Wi + dp > hi)
+            g = g * (hi > Wi ? (hi - Wi) / dp : T(0));
+        else if (dp < T(0) && Wi + dp < lo)
+            g = g * (lo < Wi ? (lo - Wi) / dp : T(0));
+    }
+    return g;
+}
+
+// The tangent of slot s's update for the tangents dU of the stencil's U = Q / V (d[k][u], positions k = 0 .. 4; a ghost
+// position's ignored): d Q'_s = -dt (dF_right - dF_left), on dual numbers (the step's operations and branches).
+template <int Order>
+__device__ __forceinline__ void update_tangent(const LineDev& L, const double* q, const int (&slot)[5], const double (&gap)[4], double dt,
+                                               const double (&d)[5][3], double (&out)[3]) {
+    using T = luna::fwd::Dual;
+    CellT cell[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        cell[k].real = slot[k] >= 0;
+        cell[k].c = 0;
+#pragma unroll
+        for (int v = 0; v < 3; ++v) cell[k].W[v] = T(0);
+        if (slot[k] >= 0) {
+            const double inv = 1.0 / L.volume[slot[k]];
+            T U[3];
+#pragma unroll
+            for (int v = 0; v < 3; ++v) U[v] = T(q[3 * slot[k] + v] * inv, d[k][v]);
+            primitive1(U, L.gas, cell[k].W);
+            cell[k].c = L.centroid[slot[k]];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        if (slot[k] >= 0) continue;
+        const int end = k < 2 ? k + 1 : k - 1;
+        if (slot[end] < 0) continue;
+        ghost_t(L, cell[end].W, k < 2, cell[k].W);
+        cell[k].c = -cell[end].c;
+    }
+    T grad[5][3];
+#pragma unroll
+    for (int k = 1; k <= 3; ++k) {
+#pragma unroll
+        for (int v = 0; v < 3; ++v) grad[k][v] = T(0);
+        if constexpr (Order == 1)
+            if (cell[k].real)
+#pragma unroll
+                for (int v = 0; v < 3; ++v) grad[k][v] = gradient_t(L, cell + k, gap[k - 1], gap[k], v);
+    }
+    T F[2][3];
+#pragma unroll
+    for (int f = 0; f < 2; ++f) {
+        const int a = 1 + f, b = 2 + f;
+        T Wl[3] = {T(0), T(0), T(0)}, Wr[3] = {T(0), T(0), T(0)};
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            const int c = side == 0 ? a : b;
+            if (!cell[c].real) continue;
+            T* o = side == 0 ? Wl : Wr;
+            const double r = side == 0 ? 0.5 * gap[a] - cell[a].c : -0.5 * gap[a] - cell[b].c;
+            if constexpr (Order == 0) {
+#pragma unroll
+                for (int v = 0; v < 3; ++v) o[v] = cell[c].W[v];
+            } else {  // Kernel::face_state (:492-506)
+                T A[3];
+                luna::half_step_rate<1, T>(cell[c].W, grad[c], T(L.gas.gamma), A);
+#pragma unroll
+                for (int v = 0; v < 3; ++v) o[v] = cell[c].W[v] - T(0.5 * dt) * A[v];
+#pragma unroll
+                for (int v = 0; v < 3; ++v) o[v] += grad[c][v] * T(r);
+                if (!(o[0] > T(0) && o[2] > T(0)))
+#pragma unroll
+                    for (int v = 0; v < 3; ++v) o[v] = cell[c].W[v];
+            }
+        }
+        if (!cell[a].real) ghost_face_t(L, Wr, cell[b].W, true, Wl);
+        if (!cell[b].real) ghost_face_t(L, Wl, cell[a].W, false, Wr);
+        const T n[1] = {T(1.0)}, w[1] = {T(0.0)};
+        if (L.riemann == LUNA_HLL)
+            luna::fwd::hll_flux_t<1, T>(Wl, Wr, n, w, T(L.gas.gamma), T(L.gas.inverse_gm1), F[f]);
+        else
+            luna::hllc_flux<1, T>(Wl, Wr, n, w, T(L.gas.gamma), T(L.gas.inverse_gm1), F[f], false);
+    }
+#pragma unroll
+    for (int v = 0; v < 3; ++v) out[v] = -dt * (F[1][v].d - F[0][v].d);
+}
+
+__device__ __forceinline__ void stencil_of(const LineDev& L, int s, int (&slot)[5], double (&gap)[4]) {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) slot[k] = slot_at(L, s, k - 2);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int a = slot[k], b = slot[k + 1];
+        gap[k] = a >= 0 ? L.gap[a + 1] * L.step : b >= 0 ? L.gap[0] * L.step : 0.0;
+    }
+}
+
+// step_tangent's derivative (:852-883): dout = dq + d Q' for the tangent dq, one dual pass a slot (slot order).
+template <int Order>
+__global__ void __launch_bounds__(128) k_line_tangent(LineDev L, const double* __restrict__ q_all, const double* __restrict__ dt_of,
+                                                      const double* __restrict__ dq_all, double* __restrict__ dout_all) {
+    const int line = blockIdx.y, s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= L.n) return;
+    const int64_t base = static_cast<int64_t>(line) * L.n * V1;
+    const double *q = q_all + base, *dq = dq_all + base;
+    int slot[5];
+    double gap[4], d[5][3], out[3];
+    stencil_of(L, s, slot, gap);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const double inv = slot[k] >= 0 ? 1.0 / L.volume[slot[k]] : 0.0;
+#pragma unroll
+        for (int v = 0; v < 3; ++v) d[k][v] = slot[k] >= 0 ? dq[3 * slot[k] + v] * inv : 0.0;
+    }
+    update_tangent<Order>(L, q, slot, gap, dt_of[line], d, out);
+#pragma unroll
+    for (int v = 0; v < 3; ++v) dout_all[base + 3 * s + v] = dq[3 * s + v] + out[v];
+}
+
+// Row s's block of the step's Jacobian for step_adjoint: jac[line][s][v][3 k + u] = d Q'_s,v / d Q_{s + k - 2},u, one
+// dual pass per input (a ghost position's column 0: a ghost's dependence on its wall's end cell runs through that cell's
+// column).
+template <int Order>
+__global__ void __launch_bounds__(128) k_line_jacobian(LineDev L, const double* __restrict__ q_all, const double* __restrict__ dt_of,
+                                                       double* __restrict__ jac_all) {
+    const int line = blockIdx.y, s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= L.n) return;
+    const double* q = q_all + static_cast<int64_t>(line) * L.n * V1;
+    double* jac = jac_all + (static_cast<int64_t>(line) * L.n + s) * 45;
+    const double dt = dt_of[line];
+    int slot[5];
+    double gap[4];
+    stencil_of(L, s, slot, gap);
+    for (int seed = 0; seed < 15; ++seed) {
+        const int sk = seed / 3, sv = seed % 3;
+        double out[3] = {0, 0, 0};
+        if (slot[sk] >= 0) {
+            double d[5][3];
+#pragma unroll
+            for (int k = 0; k < 5; ++k)
+#pragma unroll
+                for (int v = 0; v < 3; ++v) d[k][v] = k == sk && v == sv ? 1.0 / L.volume[slot[sk]] : 0.0;
+            update_tangent<Order>(L, q, slot, gap, dt, d, out);
+        }
+#pragma unroll
+        for (int v = 0; v < 3; ++v) jac[15 * v + seed] = (sk == 2 && sv == v ? 1.0 : 0.0) + out[v];
+    }
+}
+
+// out = J^T w with the blocks of k_line_jacobian, slot order: column t gathers the rows s whose stencil position k is t
+// (s = t + 2 - k), no atomics (the same bits every run).
+__global__ void __launch_bounds__(128) k_line_band_adjoint(LineDev L, const double* __restrict__ jac_all, const double* __restrict__ w_all,
+                                                           double* __restrict__ out_all) {
+    const int line = blockIdx.y, t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= L.n) return;
+    const int64_t base = static_cast<int64_t>(line) * L.n;
+    const double* w = w_all + base * V1;
+    double out[3] = {0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const int s = slot_at(L, t, 2 - k);
+        if (s < 0) continue;
+        const double* J = jac_all + (base + s) * 45;
+#pragma unroll
+        for (int v = 0; v < 3; ++v) {
+            const double ws = w[3 * s + v];
+#pragma unroll
+            for (int u = 0; u < 3; ++u) out[u] += J[15 * v + 3 * k + u] * ws;
+        }
+    }
+    double* o = out_all + (base + t) * V1;
+#pragma unroll
+    for (int v = 0; v < 3; ++v) o[v] = out[v];
+}
+
 luna_status fail(luna_status s, const std::string& what) { return luna::report_error(s, what); }
 
 #define LINE_CUDA(call)                                                                                     \
@@ -330,6 +574,7 @@ struct luna_line {
     std::vector<int64_t> keys, order;  // sorted keys; slot -> caller cell
     std::vector<double> host_volume, host_centroid;
     Buffer<double> q, next, gap, volume, centroid, dt, staging;
+    Buffer<double> jac, dvec, dout;  // the derivatives (allocated by their first call): Jacobian blocks, vectors in slot order
     Buffer<int64_t> order_dev;
     Buffer<unsigned long long> bits, error;
     std::vector<unsigned long long> host_bits;
@@ -556,6 +801,57 @@ LUNA_API luna_status luna_line_step_and_time_step(luna_line* ln, const double* d
     LINE_CUDA(cudaGetLastError());
     ln->q.swap(ln->next);
     return ln->read_dt(dt_next);
+}
+
+// The step's derivatives at fixed dt (finite_volume_1d.hpp:711-823): x in the caller's cell order [lines][n][3] (device
+// or host memory). tangent: x <- J x in one dual pass, then the step itself (Q advances as luna_line_step); adjoint: the
+// Jacobian blocks at the current state and x <- J^T x, Q unchanged (the state must be the step's start).
+static luna_status line_derivative(luna_line* ln, const double* dt, double* x, int on_device, bool tangent) {
+    if (!ln || !dt || !x) return fail(LUNA_EINVAL, "null argument");
+    if (ln->dev.periodic && ln->n < 5) return fail(LUNA_EINVAL, "the derivatives of a periodic line need 5 cells or more");
+    const size_t cells = static_cast<size_t>(ln->n) * ln->lines;
+    if (!ln->dvec.ptr) {
+        luna_status st = ln->dvec.alloc(cells * V1, "line derivative vector");
+        if (st == LUNA_OK) st = ln->dout.alloc(cells * V1, "line derivative vector");
+        if (st != LUNA_OK) return st;
+    }
+    if (!tangent && !ln->jac.ptr) {
+        const luna_status st = ln->jac.alloc(cells * 45, "line Jacobian blocks");
+        if (st != LUNA_OK) return st;
+    }
+    luna_status st = ln->upload_dt(dt);
+    if (st != LUNA_OK) return st;
+    const size_t bytes = sizeof(double) * cells * V1;
+    const int64_t total = ln->n * ln->lines;
+    const unsigned int pblocks = static_cast<unsigned int>((total + 255) / 256);
+    LINE_CUDA(cudaMemcpyAsync(ln->staging.ptr, x, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ln->stream));
+    k_line_permute<true><<<pblocks, 256, 0, ln->stream>>>(ln->n, ln->lines, ln->order_dev.ptr, ln->staging.ptr, ln->dvec.ptr);
+    if (tangent) {
+        if (ln->dev.order == 1)
+            k_line_tangent<1><<<ln->grid(), 128, 0, ln->stream>>>(ln->dev, ln->q.ptr, ln->dt.ptr, ln->dvec.ptr, ln->dout.ptr);
+        else
+            k_line_tangent<0><<<ln->grid(), 128, 0, ln->stream>>>(ln->dev, ln->q.ptr, ln->dt.ptr, ln->dvec.ptr, ln->dout.ptr);
+    } else {
+        if (ln->dev.order == 1)
+            k_line_jacobian<1><<<ln->grid(), 128, 0, ln->stream>>>(ln->dev, ln->q.ptr, ln->dt.ptr, ln->jac.ptr);
+        else
+            k_line_jacobian<0><<<ln->grid(), 128, 0, ln->stream>>>(ln->dev, ln->q.ptr, ln->dt.ptr, ln->jac.ptr);
+        k_line_band_adjoint<<<ln->grid(), 128, 0, ln->stream>>>(ln->dev, ln->jac.ptr, ln->dvec.ptr, ln->dout.ptr);
+    }
+    k_line_permute<false><<<pblocks, 256, 0, ln->stream>>>(ln->n, ln->lines, ln->order_dev.ptr, ln->dout.ptr, ln->staging.ptr);
+    LINE_CUDA(cudaGetLastError());
+    LINE_CUDA(cudaMemcpyAsync(x, ln->staging.ptr, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ln->stream));
+    if (!on_device) LINE_CUDA(cudaStreamSynchronize(ln->stream));
+    if (tangent) return luna_line_step(ln, dt);
+    return LUNA_OK;
+}
+
+LUNA_API luna_status luna_line_step_tangent(luna_line* ln, const double* dt, double* dq, int on_device) {
+    return line_derivative(ln, dt, dq, on_device, true);
+}
+
+LUNA_API luna_status luna_line_step_adjoint(luna_line* ln, const double* dt, double* qbar, int on_device) {
+    return line_derivative(ln, dt, qbar, on_device, false);
 }
 
 }  // extern "C"

@@ -101,6 +101,8 @@ SIGNATURES = {
     "luna_line_time_step": ([P, D64, I, P], I),
     "luna_line_step": ([P, P], I),
     "luna_line_step_and_time_step": ([P, P, D64, P], I),
+    "luna_line_step_tangent": ([P, P, P, I], I),
+    "luna_line_step_adjoint": ([P, P, P, I], I),
     "luna_remesh_create": ([I, P, P], I),
     "luna_remesh_destroy": ([P], I),
     "luna_remesh_set_stream": ([P, P], I),

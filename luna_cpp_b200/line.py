@@ -7,7 +7,8 @@ launch.
     t = run_to(ln, t_end, courant=0.8, rule="luna")
     W = ln.primitives()
 
-Mirrors the reference's interface: time_step(courant, rule) -> dt (per line), step(dt), step_and_time_step(dt, courant).
+Mirrors the reference's interface: time_step(courant, rule) -> dt (per line), step(dt), step_and_time_step(dt, courant),
+step_tangent(dt, dq), step_adjoint(dt, qbar).
 No CPU fallback: the library must be built (``python -m luna_cpp_b200.build``) and a GPU present.
 """
 from __future__ import annotations
@@ -78,6 +79,21 @@ class Line:
         out = np.empty(self.lines)
         check(lib().luna_line_step_and_time_step(self._h, d.ctypes.data, float(courant), out.ctypes.data))
         return out
+
+    def step_tangent(self, dt, dq) -> np.ndarray:
+        """step_tangent(dt, dq) (finite_volume_1d.hpp:852-883): returns J dq (the step's Jacobian at fixed dt, extensive
+        on both sides) and advances the state by the step."""
+        d = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, dtype=np.float64), (self.lines,)))
+        x = np.ascontiguousarray(np.broadcast_to(np.asarray(dq, dtype=np.float64), (self.lines, self.n, 3))).copy()
+        check(lib().luna_line_step_tangent(self._h, d.ctypes.data, x.ctypes.data, 0))
+        return x
+
+    def step_adjoint(self, dt, qbar) -> np.ndarray:
+        """step_adjoint(dt, qbar) (finite_volume_1d.hpp:885-923): returns J^T qbar; the state stays the step's start."""
+        d = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, dtype=np.float64), (self.lines,)))
+        x = np.ascontiguousarray(np.broadcast_to(np.asarray(qbar, dtype=np.float64), (self.lines, self.n, 3))).copy()
+        check(lib().luna_line_step_adjoint(self._h, d.ctypes.data, x.ctypes.data, 0))
+        return x
 
 
 def run_to(ln: Line, t_end, courant: float = 0.8, rule: str = "luna", fused: bool = False, max_steps: int = 10 ** 7):

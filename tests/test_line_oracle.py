@@ -95,3 +95,25 @@ def test_oracle_conserves(periodic):
     assert abs(tot[2] - tot0[2]) < 1e-14 * abs(tot0[2])
     if periodic:
         assert abs(tot[1] - tot0[1]) < 1e-14 * abs(tot0[0])
+
+
+def test_oracle_forward_of_luna_derivative_cases():
+    """The forward of LUNA's derivative cases (src/test/luna_derivative_values.hpp, hydro_derivatives_test.cpp:1054):
+    K fixed-dt steps of U0 on N = 64 uniform cells within 1e-12 of LUNA's U, relative to its largest entry, for every
+    case (Sod between outflow walls, the periodic sound wave; minmod, MC, van Leer)."""
+    golden = json.load(open(os.path.join(os.path.dirname(GOLDEN), "luna_1d_derivatives.json")))
+    limiters = {0: "minmod", 1: "face_centroid", 2: "van_leer"}
+    for name, case in golden["cases"].items():
+        p = golden["problems"][case["problem"]]
+        n = case["n"]
+        keys, order, step, period = line_keys(p["L"] * (np.arange(n) + 0.5) / n, p["L"])
+        walls = tuple(p["walls"]) if p["walls"] else ("outflow", "outflow")
+        ln = O.OracleLine(keys, step, period, gamma=p["gamma"], walls=walls, periodic=p["periodic"],
+                          limiter=limiters[case["limiter"]])
+        V = ln.volumes()[:, None]
+        ln.set_state(np.array(case["U0"]) * V)
+        for _ in range(case["steps"]):
+            ln.step(case["dt"])
+        want = np.array(case["U"])
+        err = np.max(np.abs(ln.get_state() / V - want)) / np.max(np.abs(want))
+        assert err < golden["tolerance"]["forward"], (name, err)
