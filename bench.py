@@ -59,12 +59,13 @@ def algorithmic_bytes(faces_per_cell: float, gradient_bytes: int = 120) -> dict:
                           + face rows 56 F/N (owner+neighbour 8, area 24, centroid 24) + gradient row written
       F (fluxes+update):  face rows 56 F/N + Q read 40 + gradient row read + centroid 24 + position 24 + V 8 + Q 40
     With F/N = 7.95 and FP64 gradient rows (120 B): 728.8 + 701.2 = 1430 B. The kernel split: the sweep is phase G; the
-    flux kernel reads the face rows and the cell rows (phase F without the Q traffic); the update reads Q and writes Q."""
+    flux kernel reads the face rows and the cell rows (phase F without the Q traffic); the update reads Q and writes Q;
+    the fused pass (crossing faces, then the tiles' fluxes and update) is phase F."""
     fpc = faces_per_cell
     g = 40 + 8 + 24 + 24 + 4 + 4 * 2 * fpc + 56 * fpc + gradient_bytes
     f = 56 * fpc + 40 + gradient_bytes + 24 + 24 + 8 + 40
     return {"step": g + f, "sweep": g, "fluxes": 56 * fpc + gradient_bytes + 24 + 24 + 8 + 40, "update": 80.0 + 4 + 4 * 2 * fpc,
-            "primitives": 40 + 8 + 56}
+            "primitives": 40 + 8 + 56, "flux_and_update": f}
 
 
 def measured_peaks():
@@ -333,6 +334,39 @@ def adjoint_section(mesh, q0, steps, warmup, stream, torch) -> dict:
             "finite": bool(torch.isfinite(qbar).all().item())}
 
 
+def fused_section(mesh, q0, steps, warmup, stream, torch, two_kernel_ms, two_kernel_bytes) -> dict:
+    """The static FP64 step with the fused flux-and-update pass (LUNA_FUSED_STEP=1: a tile's interior faces solved into
+    shared memory, the faces between tiles by their own pass), the same workload: its time a step against the default
+    two-kernel pass and its device memory."""
+    from luna_cpp_b200 import hydro
+
+    old = os.environ.get("LUNA_FUSED_STEP")
+    os.environ["LUNA_FUSED_STEP"] = "1"
+    try:
+        fv = hydro.FiniteVolume(mesh)
+        fv.set_stream(stream)
+        fv.set_state(q0)
+        for _ in range(warmup):
+            fv.step(fv.time_step(0.3))
+    finally:
+        if old is None:
+            del os.environ["LUNA_FUSED_STEP"]
+        else:
+            os.environ["LUNA_FUSED_STEP"] = old
+    fv.set_timing(True)
+    fv.timings(reset=True)
+    ms = timed_steps(fv, steps, torch) / steps
+    phases = fv.timings(reset=True)
+    fused, crossing = fv.fused_pass()
+    out = {"fused": fused, "ms_per_step": ms, "vs_two_kernel": two_kernel_ms / ms,
+           "phases_ms_per_step": {"crossing_faces": phases["fluxes"][0] / steps, "tiles": phases["update"][0] / steps,
+                                  "sweep": phases["sweep"][0] / steps},
+           "crossing_fraction": crossing / mesh.n_faces, "device_bytes": fv.device_bytes(),
+           "two_kernel_device_bytes": two_kernel_bytes}
+    fv.close()
+    return out
+
+
 def timed_steps(fv, steps, torch):
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
@@ -390,7 +424,8 @@ def main():
         phases = fv.timings(reset=True)
         fv.set_timing(False)
         ms = max_over_ranks(ms, dist)
-        results[prec] = {"ms": ms, "phases": phases, "clocks": clocks.summary(), "fallbacks": fv.fallbacks(), "fv": fv}
+        results[prec] = {"ms": ms, "phases": phases, "clocks": clocks.summary(), "fallbacks": fv.fallbacks(), "fv": fv,
+                         "fused": fv.fused_pass()}
 
     if args.precision != "both":
         for r in results.values():
@@ -424,12 +459,21 @@ def main():
         peak, peak_kind = measured_peaks()
         r64 = results["fp64"]
         phases = r64["phases"]
-        dominant = max(("sweep", "fluxes", "update", "primitives"), key=lambda k: phases[k][0])
-        dom_ms, dom_launches = phases[dominant]
+        fused, crossing = r64["fused"]
+        tpc = traffic_per_cell()
+        if fused:
+            # the fused pass: the crossing faces' kernel (phase "fluxes") and the tiles' kernel (phase "update") together
+            # do phase F; against the sweep, the one kernel pair per step
+            pair_ms = phases["fluxes"][0] + phases["update"][0]
+            dominant = "flux_and_update" if pair_ms > phases["sweep"][0] else "sweep"
+            dom_ms, dom_launches = (pair_ms, phases["update"][1]) if dominant != "sweep" else phases["sweep"]
+            traffic = tpc.get(("fp64", "fused")) if dominant != "sweep" else tpc.get(("fp64", "sweep"))
+        else:
+            dominant = max(("sweep", "fluxes", "update", "primitives"), key=lambda k: phases[k][0])
+            dom_ms, dom_launches = phases[dominant]
+            traffic = tpc.get(("fp64", dominant))
         avg_s = dom_ms / max(dom_launches, 1) / 1e3
         achieved = ab[dominant] * N / avg_s / 1e9
-        tpc = traffic_per_cell()
-        traffic = tpc.get(("fp64", dominant))
         step_s = r64["ms"] / args.steps / 1e3
         launches = sum(v[1] for v in phases.values())
         value = world * N * args.steps / (r64["ms"] / 1e3)
@@ -470,6 +514,7 @@ def main():
                        "speedup_vs_fp64": r64["ms"] / results["grad16"]["ms"],
                        "phases_ms_per_step": {k: v[0] / args.steps for k, v in results["grad16"]["phases"].items()}},
             "phases_ms_per_step": {k: v[0] / args.steps for k, v in phases.items()},
+            "flux_pass": {"fused": fused, "crossing_faces": crossing, "crossing_fraction": crossing / F if fused else None},
             "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
                          "algorithmic_bytes_per_cell": ab[dominant],
@@ -487,6 +532,9 @@ def main():
             line["learned_limiter"] = learned_section(mesh, q0, args.steps, args.warmup, stream, torch)
         if world == 1 and not args.no_adjoint:
             line["adjoint_cost"] = adjoint_section(mesh, q0, args.steps, args.warmup, stream, torch)
+        if world == 1:
+            line["fused_flux_update"] = fused_section(mesh, q0, args.steps, args.warmup, stream, torch, r64["ms"] / args.steps,
+                                                      r64["fv"].device_bytes())
         if world == 1 and not args.no_moving:
             line["moving"] = moving_section(args.nx, args.moving_steps, 2)
         if world == 1 and not args.no_cpu_baseline:

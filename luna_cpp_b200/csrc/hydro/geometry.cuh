@@ -835,6 +835,55 @@ __global__ void k_apply_factors(int rows, const int* __restrict__ cells, const u
 #ifndef LUNA_FLUX_MIN_BLOCKS
 #define LUNA_FLUX_MIN_BLOCKS 6
 #endif
+// One face row, 32-B aligned, in vector loads (streamed once per step: evict-first in L2).
+template <class G>
+__device__ __forceinline__ void load_face_row(const FaceRow<G>* p, FaceRow<G>& r) {
+    double* words = reinterpret_cast<double*>(&r);
+    const unsigned long long once = l2_evict_first();
+#pragma unroll
+    for (int c = 0; c < static_cast<int>(sizeof(FaceRow<G>) / 8); c += 4) ldg256_hint(reinterpret_cast<const double*>(p) + c, words + c, once);
+}
+
+// The flux of one face row (FaceFlux::operator() :1415-1434): both sides' face states from the cells' rows, the Riemann
+// solve in the face's frame, times the area. count: the sides that fell back to the cell's state.
+template <int D, int Order, class G, bool RF, int Riemann, bool H, bool WG>
+__device__ __forceinline__ void row_flux(const MeshDev<D>& m, const FluxArgs<D, G>& x, const FaceRow<G>& r, double (&F)[D + 2], int& count) {
+    constexpr int V = D + 2;
+    if (r.mag == 0) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) F[v] = 0;
+        return;
+    }
+    double L[V], R[V], n[D], wf[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        n[k] = r.n[k];
+        wf[k] = 0;
+    }
+    if constexpr (Order == 0) {
+        double U[V];
+        const double io = 1.0 / m.vol[r.o], ij = 1.0 / m.vol[r.j];
+#pragma unroll
+        for (int v = 0; v < V; ++v) U[v] = x.q[V * r.o + v] * io;
+        primitive<D>(U, x.gas, L);
+#pragma unroll
+        for (int v = 0; v < V; ++v) U[v] = x.q[V * r.j + v] * ij;
+        primitive<D>(U, x.gas, R);
+    } else {
+        double ro[D], rj[D];
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            ro[k] = static_cast<double>(r.offo[k]);
+            rj[k] = static_cast<double>(r.offj[k]);
+        }
+        face_side<D, G, H, WG>(x, r.o, ro, x.dt, L, count);
+        face_side<D, G, H, WG>(x, r.j, rj, x.dt, R, count);
+    }
+    riemann_solve<D, RF, Riemann>(L, R, n, wf, x.gas, F, false);
+#pragma unroll
+    for (int v = 0; v < V; ++v) F[v] *= r.mag;
+}
+
 template <int D, int Order, class G, bool RF, int Riemann, bool H = false, bool WG = false, class FS = double>
 __global__ void __launch_bounds__(128, LUNA_FLUX_MIN_BLOCKS) k_flux_rows(MeshDev<D> m, GeometryDev<D, G> geo, FluxArgs<D, G> x, FS* __restrict__ flux,
                                                    unsigned long long* __restrict__ fallbacks) {
@@ -843,50 +892,87 @@ __global__ void __launch_bounds__(128, LUNA_FLUX_MIN_BLOCKS) k_flux_rows(MeshDev
     int count = 0;
     if (f < m.f) {
         FaceRow<G> r;
-        {  // the 32-B aligned row in vector loads, streamed once per step
-            double* words = reinterpret_cast<double*>(&r);
-            const unsigned long long once = l2_evict_first();
-#pragma unroll
-            for (int c = 0; c < static_cast<int>(sizeof(FaceRow<G>) / 8); c += 4)
-                ldg256_hint(reinterpret_cast<const double*>(geo.faces + f) + c, words + c, once);
-        }
+        load_face_row<G>(geo.faces + f, r);
         double F[V];
-        if (r.mag == 0) {
-#pragma unroll
-            for (int v = 0; v < V; ++v) F[v] = 0;
-        } else {
-            double L[V], R[V], n[D], wf[D];
-#pragma unroll
-            for (int k = 0; k < D; ++k) {
-                n[k] = r.n[k];
-                wf[k] = 0;
-            }
-            if constexpr (Order == 0) {
-                double U[V];
-                const double io = 1.0 / m.vol[r.o], ij = 1.0 / m.vol[r.j];
-#pragma unroll
-                for (int v = 0; v < V; ++v) U[v] = x.q[V * r.o + v] * io;
-                primitive<D>(U, x.gas, L);
-#pragma unroll
-                for (int v = 0; v < V; ++v) U[v] = x.q[V * r.j + v] * ij;
-                primitive<D>(U, x.gas, R);
-            } else {
-                double ro[D], rj[D];
-#pragma unroll
-                for (int k = 0; k < D; ++k) {
-                    ro[k] = static_cast<double>(r.offo[k]);
-                    rj[k] = static_cast<double>(r.offj[k]);
-                }
-                face_side<D, G, H, WG>(x, r.o, ro, x.dt, L, count);
-                face_side<D, G, H, WG>(x, r.j, rj, x.dt, R, count);
-            }
-            riemann_solve<D, RF, Riemann>(L, R, n, wf, x.gas, F, false);
-#pragma unroll
-            for (int v = 0; v < V; ++v) F[v] *= r.mag;
-        }
+        row_flux<D, Order, G, RF, Riemann, H, WG>(m, x, r, F, count);
         store_flux_row<D, FS>(flux, f, F);
     }
     block_sum_to(static_cast<unsigned long long>(count), fallbacks);
+}
+
+// The fused flux-and-update pass of a static FP64 mesh (apply(), :1538-1631), one block a sweep tile (tiles.h
+// TileFaces): the tile's interior face rows (contiguous, tile order) prefetched into L2 by one bulk copy and solved into
+// shared memory, then each cell of the tile sums its faces' fluxes in list order, from shared memory or, for a face
+// between tiles, from the crossing pass's flux row in HBM, and updates Q and its next primitive row. The same fluxes and
+// the same sums in the same order as k_flux_rows then k_update: the same bits.
+#ifndef LUNA_FUSED_MIN_BLOCKS
+#define LUNA_FUSED_MIN_BLOCKS 6
+#endif
+template <int D, int Riemann>
+__global__ void __launch_bounds__(kTileCells, LUNA_FUSED_MIN_BLOCKS) k_tile_flux_update(MeshDev<D> m, FluxArgs<D, double> x, const int32_t* __restrict__ order,
+                                                                                       const int32_t* __restrict__ tstart, const FaceRow64* __restrict__ trows,
+                                                                                       const int32_t* __restrict__ eslot, const double* __restrict__ xflux,
+                                                                                       double* q, double dt, double* __restrict__ prims,
+                                                                                       Counters* __restrict__ ctr) {
+    constexpr int V = D + 2;
+    extern __shared__ double tile_flux[];  // [interior faces][V]
+    const int tile = blockIdx.x;
+    const int s0 = tstart[tile], slots = tstart[tile + 1] - s0;
+    if (threadIdx.x == 0 && slots > 0) prefetch_l2(trows + s0, static_cast<unsigned int>(slots * sizeof(FaceRow64)));
+    int count = 0;
+    for (int j = threadIdx.x; j < slots; j += kTileCells) {
+        FaceRow64 r;
+        load_face_row<double>(trows + s0 + j, r);
+        double F[V];
+        row_flux<D, 1, double, false, Riemann, false, true>(m, x, r, F, count);
+#pragma unroll
+        for (int v = 0; v < V; ++v) tile_flux[V * j + v] = F[v];
+    }
+    __syncthreads();
+    const int i = order[static_cast<int64_t>(tile) * kTileCells + threadIdx.x];
+    if (i >= 0) {
+        double sum[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) sum[v] = 0;
+        const int first = m.start[i], end = m.start[i + 1];
+        constexpr int kBatch = 4;  // the entries' words, then their rows, requested before any is summed
+        for (int k0 = first; k0 < end; k0 += kBatch) {
+            int32_t e[kBatch];
+#pragma unroll
+            for (int b = 0; b < kBatch; ++b) e[b] = k0 + b < end ? eslot[k0 + b] : 0;
+            double row[kBatch][V];
+#pragma unroll
+            for (int b = 0; b < kBatch; ++b) {
+                const int32_t w = e[b] >= 0 ? e[b] : ~e[b];
+                if (k0 + b < end && (w & kCrossing)) load_row_windowed<V>(xflux + V * static_cast<int64_t>(w & ~kCrossing), row[b]);
+            }
+#pragma unroll
+            for (int b = 0; b < kBatch; ++b) {
+                if (k0 + b >= end) break;
+                const int32_t w = e[b] >= 0 ? e[b] : ~e[b];
+                if (!(w & kCrossing))
+#pragma unroll
+                    for (int v = 0; v < V; ++v) row[b][v] = tile_flux[V * w + v];
+                const double sign = e[b] >= 0 ? 1.0 : -1.0;
+#pragma unroll
+                for (int v = 0; v < V; ++v) sum[v] += sign * row[b][v];
+            }
+        }
+        update_cell<D, true, true>(m, q, i, sum, dt, prims, x.gas, ctr);
+    }
+    block_sum_to(static_cast<unsigned long long>(count), &ctr->fallbacks[0]);
+}
+
+// rows[k] = faces[index[k]] (Gather: the face rows of the fused pass, interior in tile order, crossing in face order),
+// or faces[index[k]] = rows[k] (the face-ordered rows back, for a step that leaves the fused pass).
+template <class G, bool Gather>
+__global__ void k_move_face_rows(FaceRow<G>* __restrict__ faces, const int32_t* __restrict__ index, int64_t count, FaceRow<G>* __restrict__ rows) {
+    const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (k >= count) return;
+    if (Gather)
+        rows[k] = faces[index[k]];
+    else
+        faces[index[k]] = rows[k];
 }
 
 }  // namespace luna

@@ -592,6 +592,46 @@ __device__ __forceinline__ void load_row_windowed(const double* p, double* row) 
     }
 }
 
+// The end of a cell's update (finite_volume.hpp:1603-1615): Q_i -= dt sum, the error word's bit 1 if not finite; NextPrims:
+// the next primitive rows (Windowed: the library's rows, 16-B vector stores).
+template <int D, bool NextPrims, bool Windowed>
+__device__ __forceinline__ void update_cell(const MeshDev<D>& m, double* __restrict__ q, int i, const double (&sum)[D + 2], double dt,
+                                            double* __restrict__ prims, const GasDev& gas, Counters* __restrict__ ctr) {
+    constexpr int V = D + 2;
+    double next[V];
+    bool finite = true;
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        next[v] = q[V * i + v] - dt * sum[v];
+        q[V * i + v] = next[v];
+        finite = finite && isfinite(next[v]);
+    }
+    if (!finite) atomicOr(&ctr->error, 2ull);
+    if constexpr (NextPrims) {
+        const double inv = 1.0 / m.vol[i];
+        double U[V], W[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) U[v] = next[v] * inv;
+        primitive<D>(U, gas, W);
+        double row[PS];
+#pragma unroll
+        for (int v = 0; v < V; ++v) row[v] = W[v];
+        row[V] = sqrt(gas.gamma * W[D + 1] / W[0]);
+        row[V + 1] = radius<D>(m.vol[i]);
+#pragma unroll
+        for (int c = V + 2; c < PS; ++c) row[c] = 0.0;
+        if constexpr (Windowed) {
+            double2* p = reinterpret_cast<double2*>(prims + PS * static_cast<int64_t>(i));
+#pragma unroll
+            for (int c = 0; c < PS; c += 2) p[c / 2] = make_double2(row[c], row[c + 1]);
+        } else {
+            double* p = prims + PS * i;
+#pragma unroll
+            for (int c = 0; c < V + 2; ++c) p[c] = row[c];
+        }
+    }
+}
+
 // apply()'s update (finite_volume.hpp:1603-1615): Q_i -= dt sum_k sign_k F_k in list order; NextPrims: the next
 // primitive rows (a moving step's second pass; here every per-face step, which makes the next primitives() pass free).
 // Windowed: flux rows through load_row_windowed (the library's own flux buffer, padded for it).
@@ -658,38 +698,7 @@ __global__ void __launch_bounds__(256, Windowed ? LUNA_UPDATE_MIN_BLOCKS : 1) k_
             for (int v = 0; v < V; ++v) sum[v] += sign * row[b][v];
         }
     }
-    double next[V];
-    bool finite = true;
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-        next[v] = q[V * i + v] - dt * sum[v];
-        q[V * i + v] = next[v];
-        finite = finite && isfinite(next[v]);
-    }
-    if (!finite) atomicOr(&ctr->error, 2ull);
-    if constexpr (NextPrims) {
-        const double inv = 1.0 / m.vol[i];
-        double U[V], W[V];
-#pragma unroll
-        for (int v = 0; v < V; ++v) U[v] = next[v] * inv;
-        primitive<D>(U, gas, W);
-        double row[PS];
-#pragma unroll
-        for (int v = 0; v < V; ++v) row[v] = W[v];
-        row[V] = sqrt(gas.gamma * W[D + 1] / W[0]);
-        row[V + 1] = radius<D>(m.vol[i]);
-#pragma unroll
-        for (int c = V + 2; c < PS; ++c) row[c] = 0.0;
-        if constexpr (Windowed) {  // the library's rows: 16-B vector stores
-            double2* p = reinterpret_cast<double2*>(prims + PS * static_cast<int64_t>(i));
-#pragma unroll
-            for (int c = 0; c < PS; c += 2) p[c / 2] = make_double2(row[c], row[c + 1]);
-        } else {
-            double* p = prims + PS * i;
-#pragma unroll
-            for (int c = 0; c < V + 2; ++c) p[c] = row[c];
-        }
-    }
+    update_cell<D, NextPrims, Windowed>(m, q, i, sum, dt, prims, gas, ctr);
 }
 
 // apply()'s per-cell loop (finite_volume.hpp:1543-1562): each cell computes the fluxes of its faces itself, in list order.

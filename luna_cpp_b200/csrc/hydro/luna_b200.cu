@@ -9,6 +9,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -144,6 +145,15 @@ struct luna_fv {
     double pending_dt = 0;
     double grid_step = 0, per_step = 0;
     long long period[3] = {1, 1, 1};
+
+    // The fused flux-and-update pass of the static FP64 step (tiles.h TileFaces), planned by the first step on a mesh
+    // when LUNA_FUSED_STEP=1: fused 0 not planned, 1 ready, -1 not used (not asked for, or the mesh does not fit it).
+    int fused = 0;
+    int fused_smem = 0;
+    int64_t fused_crossing = 0;
+    DevArray<int32_t> fz_tstart, fz_eslot, fz_tface, fz_xface;
+    DevArray<unsigned char> fz_trows, fz_xrows;
+    DevArray<double> fz_xflux;
 
     luna::DeviceTiler* tiler = nullptr;  // the sweep's tiles cut on the device, for meshes given in device memory
     DevArray<unsigned int> list_check;   // bad entries found in a device mesh's lists
@@ -373,6 +383,7 @@ luna_status check_device_lists(luna_fv* fv, int64_t N, int64_t F) {
 
 luna_status load_mesh(luna_fv* fv, const luna_mesh_desc* m) {
     const int D = m->dim;
+    fv->fused = 0;
     const size_t N = static_cast<size_t>(m->n_cells), F = static_cast<size_t>(m->n_faces);
     const bool dev = m->on_device != 0;
     cudaStream_t s = fv->stream;
@@ -541,9 +552,13 @@ luna_status prepare_sweep(luna_fv* fv, double courant) {
     return run_sweep<D>(fv, courant);
 }
 
+template <int D>
+luna_status ensure_step_rows(luna_fv* fv);
+
 template <int D, int Order, int Pass, class G, bool RF, int Riemann, bool H = false>
 luna_status launch_flux(luna_fv* fv, const luna::FluxArgs<D, G>& x) {
     if (fv->f == 0) return LUNA_OK;
+    LUNA_TRY(ensure_step_rows<D>(fv));
     {
         const long timed_ = fv->open_timed(2);
         bool single = false;
@@ -565,6 +580,7 @@ luna_status launch_flux(luna_fv* fv, const luna::FluxArgs<D, G>& x) {
 template <int D, int Order, class G, bool RF, int Riemann, bool H = false, bool WG = false, class FS = double>
 luna_status launch_flux_rows(luna_fv* fv, const luna::FluxArgs<D, G>& x) {
     if (fv->f == 0) return LUNA_OK;
+    LUNA_TRY(ensure_step_rows<D>(fv));
     {
         const long timed_ = fv->open_timed(2);
         luna::k_flux_rows<D, Order, G, RF, Riemann, H, WG, FS><<<blocks(fv->f, kBlockFaces), kBlockFaces, 0, fv->stream>>>(
@@ -642,6 +658,104 @@ void launch_update(luna_fv* fv, double dt) {
                                                                                       fv->gas, fv->counters.ptr);
 }
 
+// The fused pass's plan for the current mesh (tiles.h build_tile_faces on the host, from the device arrays), its face
+// rows gathered from the step's rows (k_geometry's) in tile order and in crossing order. Leaves fv->fused at 1, or -1
+// where the plan does not apply (the step then runs k_flux_rows and k_update).
+template <int D>
+luna_status plan_fused(luna_fv* fv) {
+    fv->fused = -1;
+    const char* env = std::getenv("LUNA_FUSED_STEP");
+    if (!(env && env[0] == '1') || fv->f == 0 || fv->tiles == 0) return LUNA_OK;
+    const size_t N = static_cast<size_t>(fv->n), F = static_cast<size_t>(fv->f), T = static_cast<size_t>(fv->tiles);
+    std::vector<int32_t> order(T * luna::kTileCells), start(N + 1), list(2 * F), owner(F), neighbour(F);
+    LUNA_CUDA(cudaMemcpyAsync(order.data(), fv->geo_order.ptr, order.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, fv->stream));
+    LUNA_CUDA(cudaMemcpyAsync(start.data(), fv->start.ptr, start.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, fv->stream));
+    LUNA_CUDA(cudaMemcpyAsync(list.data(), fv->list.ptr, list.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, fv->stream));
+    LUNA_CUDA(cudaMemcpyAsync(owner.data(), fv->owner.ptr, F * sizeof(int32_t), cudaMemcpyDeviceToHost, fv->stream));
+    LUNA_CUDA(cudaMemcpyAsync(neighbour.data(), fv->neighbour.ptr, F * sizeof(int32_t), cudaMemcpyDeviceToHost, fv->stream));
+    LUNA_CUDA(cudaStreamSynchronize(fv->stream));
+    luna::TileFaces plan;
+    const std::string why = luna::build_tile_faces(fv->n, fv->f, fv->tiles, order.data(), start.data(), list.data(), owner.data(),
+                                                   neighbour.data(), plan);
+    if (!why.empty()) return LUNA_OK;
+    const size_t smem = sizeof(double) * (D + 2) * static_cast<size_t>(plan.max_slots);
+    if (smem > 200 * 1024) return LUNA_OK;
+    using Row = luna::FaceRow<double>;
+    const size_t inner = plan.tface.size(), crossing = plan.xface.size();
+    LUNA_TRY(upload(fv->fz_tstart, plan.tstart.data(), plan.tstart.size(), false, fv->stream, "fused tile starts"));
+    LUNA_TRY(upload(fv->fz_eslot, plan.eslot.data(), plan.eslot.size(), false, fv->stream, "fused entry slots"));
+    LUNA_TRY(upload(fv->fz_tface, plan.tface.data(), inner, false, fv->stream, "fused interior faces"));
+    LUNA_TRY(upload(fv->fz_xface, plan.xface.data(), crossing, false, fv->stream, "fused crossing faces"));
+    LUNA_TRY(fv->fz_trows.alloc(sizeof(Row) * (inner > 0 ? inner : 1), "fused interior face rows"));
+    LUNA_TRY(fv->fz_xrows.alloc(sizeof(Row) * (crossing > 0 ? crossing : 1), "fused crossing face rows"));
+    // 4 doubles past the last row: the update reads each row through its 32-B aligned 64-B window
+    LUNA_TRY(fv->fz_xflux.alloc((D + 2) * crossing + 4, "fused crossing flux rows"));
+    auto* faces = reinterpret_cast<Row*>(fv->geo_faces.ptr);
+    if (inner > 0)
+        luna::k_move_face_rows<double, true><<<blocks(inner, 256), 256, 0, fv->stream>>>(faces, fv->fz_tface.ptr, static_cast<int64_t>(inner),
+                                                                                          reinterpret_cast<Row*>(fv->fz_trows.ptr));
+    if (crossing > 0)
+        luna::k_move_face_rows<double, true><<<blocks(crossing, 256), 256, 0, fv->stream>>>(faces, fv->fz_xface.ptr, static_cast<int64_t>(crossing),
+                                                                                             reinterpret_cast<Row*>(fv->fz_xrows.ptr));
+    LUNA_CUDA(cudaGetLastError());
+    LUNA_CUDA(cudaStreamSynchronize(fv->stream));  // the host plan must outlive the copies
+    // The fused pass keeps the face rows in its own two orders and needs no flux row of an interior face: the face-ordered
+    // rows and the flux rows are released (a step that leaves the fused pass takes them back, ensure_step_rows).
+    fv->geo_faces.release();
+    fv->flux.release();
+    fv->fused_smem = static_cast<int>(smem);
+    fv->fused_crossing = static_cast<int64_t>(crossing);
+    fv->fused = 1;
+    return LUNA_OK;
+}
+
+// The face-ordered rows and the flux rows of the two-kernel passes, after the fused pass released them.
+template <int D>
+luna_status ensure_step_rows(luna_fv* fv) {
+    if (fv->update == LUNA_UPDATE_PER_FACE) LUNA_TRY(fv->flux.alloc(static_cast<size_t>(fv->f) * (D + 2) + 4, "flux rows"));
+    if (fv->fused == 1 && !fv->geo_faces.ptr && fv->f > 0 && fv->precision == LUNA_FP64) {
+        using Row = luna::FaceRow<double>;
+        LUNA_TRY(fv->geo_faces.alloc(sizeof(Row) * static_cast<size_t>(fv->f), "face rows"));
+        auto* faces = reinterpret_cast<Row*>(fv->geo_faces.ptr);
+        const int64_t inner = static_cast<int64_t>(fv->fz_tface.count), crossing = fv->fused_crossing;
+        if (inner > 0)
+            luna::k_move_face_rows<double, false><<<blocks(inner, 256), 256, 0, fv->stream>>>(faces, fv->fz_tface.ptr, inner,
+                                                                                               reinterpret_cast<Row*>(fv->fz_trows.ptr));
+        if (crossing > 0)
+            luna::k_move_face_rows<double, false><<<blocks(crossing, 256), 256, 0, fv->stream>>>(faces, fv->fz_xface.ptr, crossing,
+                                                                                                  reinterpret_cast<Row*>(fv->fz_xrows.ptr));
+        LUNA_CUDA(cudaGetLastError());
+    }
+    return LUNA_OK;
+}
+
+// The fused static FP64 pass: the crossing faces' rows (k_flux_rows over the crossing rows), then one block a tile.
+template <int D, int Riemann>
+luna_status launch_fused(luna_fv* fv, const luna::FluxArgs<D, double>& x, double dt) {
+    auto m = fv->mesh_dev<D>();
+    auto geo = fv->geometry_dev<D, double>();
+    if (fv->fused_crossing > 0) {
+        auto mx = m;
+        mx.f = static_cast<int32_t>(fv->fused_crossing);
+        geo.faces = reinterpret_cast<luna::FaceRow<double>*>(fv->fz_xrows.ptr);
+        const long timed_ = fv->open_timed(2);
+        luna::k_flux_rows<D, 1, double, false, Riemann, false, true><<<blocks(fv->fused_crossing, kBlockFaces), kBlockFaces, 0, fv->stream>>>(
+            mx, geo, x, fv->fz_xflux.ptr, &fv->counters.ptr->fallbacks[0]);
+        fv->close_timed(timed_);
+    }
+    auto kernel = luna::k_tile_flux_update<D, Riemann>;
+    if (fv->fused_smem > 48 * 1024) LUNA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, fv->fused_smem));
+    {
+        const long timed_ = fv->open_timed(3);
+        kernel<<<static_cast<unsigned int>(fv->tiles), luna::kTileCells, fv->fused_smem, fv->stream>>>(
+            m, x, fv->geo_order.ptr, fv->fz_tstart.ptr, reinterpret_cast<const luna::FaceRow64*>(fv->fz_trows.ptr), fv->fz_eslot.ptr,
+            fv->fz_xflux.ptr, fv->q.ptr, dt, fv->prims.ptr, fv->counters.ptr);
+        fv->close_timed(timed_);
+    }
+    LUNA_CUDA(cudaGetLastError());
+    return LUNA_OK;
+}
+
 // apply() for a static mesh (finite_volume.hpp:1538-1631).
 template <int D, class G>
 luna_status run_apply(luna_fv* fv, const G* grad, double dt) {
@@ -655,6 +769,18 @@ luna_status run_apply(luna_fv* fv, const G* grad, double dt) {
         if (float_riemann(fv)) return launch_per_cell<D, 1, G, true, 0>(fv, x, dt);
         if (fv->precision == LUNA_GRAD16) return launch_per_cell<D, 1, G, false, 0, true>(fv, x, dt);
         return fv->riemann == LUNA_HLL ? launch_per_cell<D, 1, G, false, 1>(fv, x, dt) : launch_per_cell<D, 1, G, false, 0>(fv, x, dt);
+    }
+    if constexpr (sizeof(G) == sizeof(double)) {
+        if (fv->order == 1 && fv->grads_in_wg) {
+            if (fv->fused == 0) LUNA_TRY(plan_fused<D>(fv));
+            if (fv->fused == 1) {
+                auto y = x;
+                y.wg = fv->wg64.ptr;
+                LUNA_TRY(fv->riemann == LUNA_HLL ? (launch_fused<D, 1>(fv, y, dt)) : (launch_fused<D, 0>(fv, y, dt)));
+                fv->prims_ready = true;  // the update wrote the next primitive rows
+                return LUNA_OK;
+            }
+        }
     }
     if (fv->order == 0)
         LUNA_TRY((dispatch_flux_rows<D, 0, G>(fv, x)));
@@ -1271,6 +1397,13 @@ LUNA_API luna_status luna_fv_timings(luna_fv* fv, luna_timings* out, int reset) 
     return LUNA_OK;
 }
 
+LUNA_API luna_status luna_fv_fused_pass(luna_fv* fv, int* fused, int64_t* crossing_faces) {
+    if (!fv || !fused) return set_error(LUNA_EINVAL, "null argument");
+    *fused = fv->fused == 1 ? 1 : 0;
+    if (crossing_faces) *crossing_faces = fv->fused == 1 ? fv->fused_crossing : 0;
+    return LUNA_OK;
+}
+
 LUNA_API luna_status luna_fv_device_bytes(luna_fv* fv, int64_t* out) {
     if (!fv || !out) return set_error(LUNA_EINVAL, "null argument");
     size_t b = 0;
@@ -1286,6 +1419,8 @@ LUNA_API luna_status luna_fv_device_bytes(luna_fv* fv, int64_t* out) {
     b += fv->geo_slice_base.bytes() + fv->geo_order.bytes() + fv->geo_stage_start.bytes() + fv->geo_stage_cells.bytes() + fv->geo_faces.bytes();
     b += fv->geo_angle.bytes() + fv->geo_reach2.bytes() + fv->lim_features.bytes() + fv->lim_alpha.bytes() + fv->lim_logits.bytes();
     b += fv->lim_cells.bytes() + fv->lim_count.bytes();
+    b += fv->fz_tstart.bytes() + fv->fz_eslot.bytes() + fv->fz_tface.bytes() + fv->fz_xface.bytes() + fv->fz_trows.bytes() + fv->fz_xrows.bytes();
+    b += fv->fz_xflux.bytes();
     *out = static_cast<int64_t>(b);
     return LUNA_OK;
 }

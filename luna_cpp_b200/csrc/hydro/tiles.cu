@@ -124,6 +124,63 @@ std::string build_sweep_tiles(int dim, int64_t n_cells, const double* positions,
     return std::string();
 }
 
+std::string build_tile_faces(int64_t n_cells, int64_t n_faces, int64_t tiles, const int32_t* order, const int32_t* start, const int32_t* list,
+                             const int32_t* owner, const int32_t* neighbour, TileFaces& out) {
+    const int64_t N = n_cells, F = n_faces;
+    if (F >= kCrossing) return "too many faces for the fused pass";
+    std::vector<int32_t> tile_of(static_cast<size_t>(N), -1);
+    for (int64_t t = 0; t < tiles; ++t)
+        for (int k = 0; k < kTileCells; ++k) {
+            const int32_t c = order[t * kTileCells + k];
+            if (c < 0) continue;
+            if (c >= N || tile_of[c] >= 0) return "a cell out of range or in two tiles";
+            tile_of[c] = static_cast<int32_t>(t);
+        }
+    for (int64_t i = 0; i < N; ++i)
+        if (tile_of[i] < 0) return "a cell in no tile";
+    // every list entry must be its face's owner's (owned) or neighbour's (not owned) entry
+    for (int64_t i = 0; i < N; ++i)
+        for (int32_t k = start[i]; k < start[i + 1]; ++k) {
+            const int32_t e = list[k], f = e >= 0 ? e : ~e;
+            if ((e >= 0 ? owner[f] : neighbour[f]) != i) return "a list entry its face's owner or neighbour does not match";
+        }
+    std::vector<int32_t> xindex(static_cast<size_t>(F), -1), slot_of(static_cast<size_t>(F), -1);
+    out.xface.clear();
+    for (int64_t f = 0; f < F; ++f)
+        if (tile_of[owner[f]] != tile_of[neighbour[f]]) {
+            xindex[f] = static_cast<int32_t>(out.xface.size());
+            out.xface.push_back(static_cast<int32_t>(f));
+        }
+    out.tstart.assign(static_cast<size_t>(tiles) + 1, 0);
+    out.tface.clear();
+    out.max_slots = 0;
+    for (int64_t t = 0; t < tiles; ++t) {
+        const size_t base = out.tface.size();
+        for (int k = 0; k < kTileCells; ++k) {
+            const int32_t c = order[t * kTileCells + k];
+            if (c < 0) continue;
+            for (int32_t j = start[c]; j < start[c + 1]; ++j) {
+                const int32_t e = list[j];
+                if (e < 0 || xindex[e] >= 0) continue;
+                slot_of[e] = static_cast<int32_t>(out.tface.size() - base);
+                out.tface.push_back(e);
+            }
+        }
+        const size_t slots = out.tface.size() - base;
+        if (slots >= static_cast<size_t>(kCrossing)) return "too many faces in a tile";
+        out.max_slots = std::max(out.max_slots, static_cast<int>(slots));
+        out.tstart[t + 1] = static_cast<int32_t>(out.tface.size());
+    }
+    out.eslot.resize(static_cast<size_t>(2 * F));
+    for (int64_t k = 0; k < 2 * F; ++k) {
+        const int32_t e = list[k], f = e >= 0 ? e : ~e;
+        const int32_t v = xindex[f] >= 0 ? (kCrossing | xindex[f]) : slot_of[f];
+        if (v < 0) return "an interior face without its owner's entry";
+        out.eslot[k] = e >= 0 ? v : ~v;
+    }
+    return std::string();
+}
+
 }  // namespace luna
 
 namespace luna {

@@ -52,6 +52,25 @@ __host__ __device__ inline uint64_t morton_key(int dim, const double* x, const d
 std::string build_sweep_tiles(int dim, int64_t n_cells, const double* positions, const double* box, const int32_t* start,
                               const int32_t* list, const int32_t* owner, const int32_t* neighbour, SweepTiles& out);
 
+// The faces of the tiles for the fused flux-and-update pass of a static mesh (geometry.cuh::k_tile_flux_update): a face
+// whose two cells share a tile is an interior face of that tile, solved by the tile's block into shared memory; a face
+// between two tiles is a crossing face, solved once by its own pass into a flux row in HBM. Each list entry names its
+// face's flux: an interior slot s of its cell's tile, or kCrossing | the crossing index; ~ of that for a face the cell
+// does not own (the list's own encoding).
+constexpr int32_t kCrossing = 1 << 30;
+struct TileFaces {
+    std::vector<int32_t> tstart;  // [tiles + 1]: each tile's interior faces in tface
+    std::vector<int32_t> tface;   // the interior faces, tile by tile: the tile's cells in thread order, each cell's owned
+                                  // entries in list order
+    std::vector<int32_t> xface;   // the crossing faces, in face order
+    std::vector<int32_t> eslot;   // [2F]: each list entry's flux
+    int max_slots = 0;            // the most interior faces of a tile
+};
+// From the sweep's tiles (order [tiles * kTileCells]) and the mesh's lists; an empty string, or why the plan cannot be
+// made (a cell in no tile or in two, a list entry its face's owner or neighbour does not match).
+std::string build_tile_faces(int64_t n_cells, int64_t n_faces, int64_t tiles, const int32_t* order, const int32_t* start, const int32_t* list,
+                             const int32_t* owner, const int32_t* neighbour, TileFaces& out);
+
 // The same tiles cut on the device from a device mesh, for a mesh that is rebuilt every step (the moving mesh's
 // remesh): the cells of a tile are 128 consecutive cells of the Morton order (no greedy cut), within a tile by list
 // length, longest first; a tile staging more than kTileRows rows goes with the single-cell tiles of the host cut to the

@@ -78,6 +78,7 @@ SIGNATURES = {
     "luna_status_string": ([I], ctypes.c_char_p),
     "luna_last_error": ([], ctypes.c_char_p),
     "luna_fv_device_bytes": ([P, P], I),
+    "luna_fv_fused_pass": ([P, P, P], I),
     "luna_fv_set_timing": ([P, I], I),
     "luna_fv_step_adjoint": ([P, D64, P, I], I),
     "luna_fv_step_tangent": ([P, D64, P, I], I),
@@ -356,6 +357,12 @@ class FiniteVolume:
         t = _Timings()
         check(lib().luna_fv_timings(self._h, ctypes.byref(t), 1 if reset else 0))
         return {name: (t.ms[k], int(t.launches[k])) for k, name in enumerate(PHASES)}
+
+    def fused_pass(self) -> tuple:
+        """(whether the static steps run the fused flux-and-update pass, the faces between its tiles)."""
+        fused, crossing = ctypes.c_int(), ctypes.c_int64()
+        check(lib().luna_fv_fused_pass(self._h, ctypes.byref(fused), ctypes.byref(crossing)))
+        return bool(fused.value), int(crossing.value)
 
     def device_bytes(self) -> int:
         out = ctypes.c_int64()
