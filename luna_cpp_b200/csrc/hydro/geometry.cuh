@@ -90,10 +90,31 @@ struct GeometryDev {
 #ifndef LUNA_GEOMETRY_BATCH
 #define LUNA_GEOMETRY_BATCH 1
 #endif
-template <int D, class G>
-__global__ void __launch_bounds__(128) k_geometry(MeshDev<D> m, GeometryDev<D, G> g) {
+// FaceRows: also the static flux pass's face rows (a moving mesh's flux passes read the mesh arrays, not the rows).
+// One block a tile, tiles [tile0, tile0 + gridDim.x). Staged: the generators and centroids of the tile's staged cells
+// (its own and the halo, tiles.h) copied into shared memory first (2 D doubles a row), each entry's neighbour read there
+// through its staged row (the tiler's entry words) instead of through the face's owner / neighbour; the same values, so
+// the same rows.
+template <int D, class G, bool FaceRows = true, bool Staged = false>
+__global__ void __launch_bounds__(128) k_geometry(MeshDev<D> m, GeometryDev<D, G> g, int tile0) {
     constexpr int U = D + 1, B = LUNA_GEOMETRY_BATCH;
-    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    extern __shared__ double geo_rows[];  // Staged: [staged rows][2 D]: generator, centroid
+    const int tile = tile0 + static_cast<int>(blockIdx.x);
+    const int64_t t = static_cast<int64_t>(tile) * kTileCells + threadIdx.x;
+    int s0 = 0;
+    if constexpr (Staged) {
+        s0 = g.stage_start[tile];
+        const int staged = g.stage_start[tile + 1] - s0;
+        for (int r = threadIdx.x; r < staged; r += kTileCells) {
+            const int c = g.stage_cells[s0 + r];
+#pragma unroll
+            for (int a = 0; a < D; ++a) {
+                geo_rows[2 * D * r + a] = m.pos[D * static_cast<int64_t>(c) + a];
+                geo_rows[2 * D * r + D + a] = m.cen[D * static_cast<int64_t>(c) + a];
+            }
+        }
+        __syncthreads();
+    }
     if (t >= g.threads) return;
     const int i = g.order[t];
     if (i < 0) return;
@@ -120,15 +141,23 @@ __global__ void __launch_bounds__(128) k_geometry(MeshDev<D> m, GeometryDev<D, G
 #pragma unroll
         for (int b = 0; b < B; ++b) {
             const int f = list_face(e[b]);
-            j[b] = k0 + b < end ? (e[b] >= 0 ? m.neighbour[f] : m.owner[f]) : i;
+            if constexpr (Staged)
+                j[b] = k0 + b < end ? static_cast<int>(g.nbr[slot0 + 32 * static_cast<int64_t>(k0 + b - first)] & kIndexMask) : 0;
+            else
+                j[b] = k0 + b < end ? (e[b] >= 0 ? m.neighbour[f] : m.owner[f]) : i;
             mag[b] = k0 + b < end ? m.mag[f] : 0.0;
         }
 #pragma unroll
         for (int b = 0; b < B; ++b)
 #pragma unroll
             for (int a = 0; a < D; ++a) {
-                pj[b][a] = m.pos[D * j[b] + a];
-                cj[b][a] = m.cen[D * j[b] + a];
+                if constexpr (Staged) {  // j: the staged row
+                    pj[b][a] = geo_rows[2 * D * j[b] + a];
+                    cj[b][a] = geo_rows[2 * D * j[b] + D + a];
+                } else {
+                    pj[b][a] = m.pos[D * j[b] + a];
+                    cj[b][a] = m.cen[D * j[b] + a];
+                }
             }
 #pragma unroll
         for (int b = 0; b < B; ++b) {
@@ -178,7 +207,10 @@ __global__ void __launch_bounds__(128) k_geometry(MeshDev<D> m, GeometryDev<D, G
         for (int b = 0; b < B; ++b) {
             const int f = list_face(e[b]);
             const bool in = k0 + b < end;
-            j[b] = in ? (e[b] >= 0 ? m.neighbour[f] : m.owner[f]) : i;
+            if constexpr (Staged)
+                j[b] = in ? static_cast<int>(g.nbr[slot0 + 32 * static_cast<int64_t>(k0 + b - first)] & kIndexMask) : 0;
+            else
+                j[b] = in ? (e[b] >= 0 ? m.neighbour[f] : m.owner[f]) : i;
             mag[b] = in ? m.mag[f] : 0.0;
 #pragma unroll
             for (int a = 0; a < D; ++a) fc[b][a] = in ? m.fcen[D * f + a] : 0.0;
@@ -187,8 +219,13 @@ __global__ void __launch_bounds__(128) k_geometry(MeshDev<D> m, GeometryDev<D, G
         for (int b = 0; b < B; ++b)
 #pragma unroll
             for (int a = 0; a < D; ++a) {
-                pj[b][a] = m.pos[D * j[b] + a];
-                cj[b][a] = m.cen[D * j[b] + a];
+                if constexpr (Staged) {
+                    pj[b][a] = geo_rows[2 * D * j[b] + a];
+                    cj[b][a] = geo_rows[2 * D * j[b] + D + a];
+                } else {
+                    pj[b][a] = m.pos[D * j[b] + a];
+                    cj[b][a] = m.cen[D * j[b] + a];
+                }
             }
 #pragma unroll
         for (int b = 0; b < B; ++b) {
@@ -239,7 +276,7 @@ __global__ void __launch_bounds__(128) k_geometry(MeshDev<D> m, GeometryDev<D, G
             }
             const bool tiny_face = any_tiny && magnitude < tiny;
             g.nbr[slot] = (g.nbr[slot] & kIndexMask) | (owned ? kOwnedBit : 0u) | (tiny_face ? kTinyBit : 0u);
-            if (owned) {  // the face row, written once by the owner
+            if (FaceRows && owned) {  // the face row, written once by the owner
                 double a[D];
 #pragma unroll
                 for (int q = 0; q < D; ++q) a[q] = m.area[D * f + q];
@@ -263,7 +300,10 @@ __global__ void __launch_bounds__(128) k_geometry(MeshDev<D> m, GeometryDev<D, G
                 }
                 r.mag = amag;
                 r.o = i;
-                r.j = j[b];
+                if constexpr (Staged)
+                    r.j = g.stage_cells[s0 + j[b]];
+                else
+                    r.j = j[b];
                 if constexpr (sizeof(G) == sizeof(double)) r.pad = 0;
                 g.faces[f] = r;
             }
@@ -344,6 +384,9 @@ __device__ __forceinline__ void store_half_row(const HalfRows& out, int i, const
 #ifndef LUNA_SWEEP_MIN_BLOCKS
 #define LUNA_SWEEP_MIN_BLOCKS 4
 #endif
+#ifndef LUNA_SWEEP_MIN_BLOCKS_F
+#define LUNA_SWEEP_MIN_BLOCKS_F LUNA_SWEEP_MIN_BLOCKS  // the float policies' sweep
+#endif
 #ifndef LUNA_SWEEP_BATCH
 #define LUNA_SWEEP_BATCH 0  // 0: 2 entries in FP64, 3 in the float policies (128^3 sweep ms: FP64 2: 0.748, 1: 0.760,
                             // 3: 0.794; riemann32 3: 0.536, 2: 0.545)
@@ -357,7 +400,8 @@ __device__ __forceinline__ void store_half_row(const HalfRows& out, int i, const
 // Limit: 0 none, 1 the plain face-centroid limiter, 2 the learned limiter's inputs (the gradient left unlimited).
 // KB: entries whose streamed rows are requested together. Launched with blocks of kTileCells threads over tiles [tile0, tile0 + gridDim.x) and the shared memory of the most
 // rows one of them stages (kStagedDoubles doubles a row).
-template <int D, bool Moving, bool Grad, class G, int Limit, int KB = LUNA_SWEEP_BATCH, int MINB = LUNA_SWEEP_MIN_BLOCKS>
+template <int D, bool Moving, bool Grad, class G, int Limit, int KB = LUNA_SWEEP_BATCH,
+          int MINB = sizeof(G) == sizeof(double) ? LUNA_SWEEP_MIN_BLOCKS : LUNA_SWEEP_MIN_BLOCKS_F>
 __global__ void __launch_bounds__(kTileCells, MINB) k_sweep_tiles(MeshDev<D> m, GeometryDev<D, G> geo, int tile0, const double* __restrict__ prims,
                                                                G* __restrict__ grad_out, double* __restrict__ w_out, double courant,
                                                                double round_off2, Counters* __restrict__ ctr, LearnedInputs learned,
@@ -835,6 +879,9 @@ __global__ void k_apply_factors(int rows, const int* __restrict__ cells, const u
 #ifndef LUNA_FLUX_MIN_BLOCKS
 #define LUNA_FLUX_MIN_BLOCKS 6
 #endif
+#ifndef LUNA_FLUX_MIN_BLOCKS_F
+#define LUNA_FLUX_MIN_BLOCKS_F 8  // the float policies' flux pass (128^3 single, fluxes ms: 6 blocks 0.534, 7 0.492, 8 0.458)
+#endif
 // One face row, 32-B aligned, in vector loads (streamed once per step: evict-first in L2).
 template <class G>
 __device__ __forceinline__ void load_face_row(const FaceRow<G>* p, FaceRow<G>& r) {
@@ -885,7 +932,7 @@ __device__ __forceinline__ void row_flux(const MeshDev<D>& m, const FluxArgs<D, 
 }
 
 template <int D, int Order, class G, bool RF, int Riemann, bool H = false, bool WG = false, class FS = double>
-__global__ void __launch_bounds__(128, LUNA_FLUX_MIN_BLOCKS) k_flux_rows(MeshDev<D> m, GeometryDev<D, G> geo, FluxArgs<D, G> x, FS* __restrict__ flux,
+__global__ void __launch_bounds__(128, sizeof(G) == sizeof(double) ? LUNA_FLUX_MIN_BLOCKS : LUNA_FLUX_MIN_BLOCKS_F) k_flux_rows(MeshDev<D> m, GeometryDev<D, G> geo, FluxArgs<D, G> x, FS* __restrict__ flux,
                                                    unsigned long long* __restrict__ fallbacks) {
     constexpr int V = D + 2;
     const int f = blockIdx.x * blockDim.x + threadIdx.x;

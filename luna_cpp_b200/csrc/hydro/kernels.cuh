@@ -644,10 +644,13 @@ __device__ __forceinline__ void update_cell(const MeshDev<D>& m, double* __restr
 #ifndef LUNA_UPDATE_BATCH
 #define LUNA_UPDATE_BATCH 2
 #endif
+#ifndef LUNA_UPDATE_MIN_BLOCKS_F
+#define LUNA_UPDATE_MIN_BLOCKS_F LUNA_UPDATE_MIN_BLOCKS  // single's float flux rows
+#endif
 // FS = float: the rows of store_flux_row, one aligned vector load each, widened to double before the sum (the
 // reference's static_cast<double>(F(f, v)), finite_volume.hpp:1607).
 template <int D, bool NextPrims, bool Windowed = false, class FS = double>
-__global__ void __launch_bounds__(256, Windowed ? LUNA_UPDATE_MIN_BLOCKS : 1) k_update(MeshDev<D> m, double* __restrict__ q, const FS* __restrict__ flux, double dt,
+__global__ void __launch_bounds__(256, Windowed ? (sizeof(FS) == sizeof(float) ? LUNA_UPDATE_MIN_BLOCKS_F : LUNA_UPDATE_MIN_BLOCKS) : 1) k_update(MeshDev<D> m, double* __restrict__ q, const FS* __restrict__ flux, double dt,
                                                 double* __restrict__ prims, GasDev gas, Counters* __restrict__ ctr) {
     constexpr int V = D + 2;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -282,7 +282,12 @@ luna_status finish_geometry(luna_fv* fv, size_t slots) {
     LUNA_TRY(fv->geo_c2.alloc(sizeof(G) * slots, "entry gradient rows"));
     LUNA_TRY(fv->geo_off01.alloc(sizeof(luna::Pair<G>) * slots, "entry offsets"));
     LUNA_TRY(fv->geo_off2.alloc(sizeof(G) * slots, "entry offsets"));
-    LUNA_TRY(fv->geo_faces.alloc(sizeof(luna::FaceRow<G>) * (F > 0 ? F : 1), "face rows"));
+    // a moving mesh's flux passes read the mesh arrays: no face rows
+    const bool face_rows = fv->motion != LUNA_MOVING;
+    if (face_rows)
+        LUNA_TRY(fv->geo_faces.alloc(sizeof(luna::FaceRow<G>) * (F > 0 ? F : 1), "face rows"));
+    else
+        fv->geo_faces.release();
     LUNA_TRY(fv->geo_angle.alloc(N, "face angles"));
     LUNA_TRY(fv->geo_reach2.alloc(N, "cell reach"));
     const int64_t threads = fv->tiles * luna::kTileCells;
@@ -290,7 +295,19 @@ luna_status finish_geometry(luna_fv* fv, size_t slots) {
         // timed with the sweep: the fit's operator rows, which the reference's sweep forms every step (a moving mesh
         // forms them every step here too)
         const long timed_ = fv->open_timed(1);
-        luna::k_geometry<D, G><<<blocks(threads, 128), 128, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->geometry_dev<D, G>());
+        // the tiles within the staged-row budget read their neighbours from shared memory; the single-cell tiles past it
+        // through the face's cells
+        const auto m = fv->mesh_dev<D>();
+        const auto g = fv->geometry_dev<D, G>();
+        const unsigned int normal = static_cast<unsigned int>(fv->normal_tiles), big = static_cast<unsigned int>(fv->tiles - fv->normal_tiles);
+        const size_t smem = sizeof(double) * 2 * D * static_cast<size_t>(fv->normal_rows > 0 ? fv->normal_rows : 1);
+        if (face_rows) {
+            if (normal > 0) luna::k_geometry<D, G, true, true><<<normal, luna::kTileCells, smem, fv->stream>>>(m, g, 0);
+            if (big > 0) luna::k_geometry<D, G, true, false><<<big, luna::kTileCells, 0, fv->stream>>>(m, g, static_cast<int>(normal));
+        } else {
+            if (normal > 0) luna::k_geometry<D, G, false, true><<<normal, luna::kTileCells, smem, fv->stream>>>(m, g, 0);
+            if (big > 0) luna::k_geometry<D, G, false, false><<<big, luna::kTileCells, 0, fv->stream>>>(m, g, static_cast<int>(normal));
+        }
         fv->close_timed(timed_);
         LUNA_CUDA(cudaGetLastError());
     }

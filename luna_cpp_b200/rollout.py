@@ -17,7 +17,10 @@ Commands (paths are raw float64 files, C order; cells in lattice C order, the la
     memory                            "ok <peak device bytes> <bytes now>" (the step's buffers and the tape).
     quit
 The fixed dt is checked against time_step(courant) of every step; the steps where it is larger are counted.
-``--moving`` answers an error: the moving mesh's derivatives are not in the library.
+``--moving``: the moving mesh (Rollout with Motion::moving, rollout.cpp:138-163), remeshed on the device every step;
+the forward keeps the positions' tape beside the states' and its final rows carry the moved generators and the final
+mesh's volumes; ``cfl`` and ``geometry`` start from the lattice's mesh. ``adjoint`` and ``tangent`` answer an error
+line there: the moving step's derivatives (step_moving_adjoint, step_moving_tangent) are not in the library.
 """
 from __future__ import annotations
 
@@ -42,48 +45,72 @@ def lattice(side: int, dim: int) -> np.ndarray:
 
 
 class Server:
-    def __init__(self, dim: int, side: int, steps: int, dt: float, gamma: float, courant: float):
+    def __init__(self, dim: int, side: int, steps: int, dt: float, gamma: float, courant: float, moving: bool = False):
         import torch
 
         from .hydro import FiniteVolume, Gas
         from .mesh import build_mesh
 
         self.torch = torch
-        self.dim, self.steps, self.dt, self.courant = dim, steps, dt, courant
+        self.dim, self.steps, self.dt, self.courant, self.moving = dim, steps, dt, courant, moving
         self.V = dim + 2
         self.x0 = lattice(side, dim)
         self.mesh = build_mesh(self.x0, box=(1.0,) * dim)
         self.n = self.mesh.n_cells
         self.V0 = self.mesh.volume.copy()
-        self.fv = FiniteVolume(self.mesh, Gas(gamma), order=1, update="per_face", limiter="face_centroid")
+        self.fv = FiniteVolume(self.mesh, Gas(gamma), order=1, update="per_face", limiter="face_centroid",
+                               motion="moving" if moving else "static_mesh")
         self.tape = torch.empty((steps, self.n, self.V), dtype=torch.float64, device="cuda")
+        self.xtape = None
+        if moving:
+            from .remesh import Remesher
+
+            self.remesher = Remesher(dim, (1.0,) * dim)
+            self.xtape = torch.empty((steps, self.n, dim), dtype=torch.float64, device="cuda")
         self.volume_dev = torch.tensor(self.V0, device="cuda")[:, None]
         self.peak = self.now()
 
     def now(self) -> int:
-        return int(self.fv.device_bytes() + self.tape.numel() * 8)
+        tapes = self.tape.numel() + (self.xtape.numel() if self.xtape is not None else 0)
+        remesh = self.remesher.device_bytes() if self.moving else 0
+        return int(self.fv.device_bytes() + remesh + tapes * 8)
 
     def load(self, U0: np.ndarray) -> None:
+        if self.moving:  # load_positions(x0): back to the lattice's mesh
+            self.fv.set_mesh(self.mesh)
         self.fv.set_state(np.ascontiguousarray(U0.reshape(self.n, self.V) * self.V0[:, None]))
 
     def forward(self, U0: np.ndarray) -> int:
+        """Rollout::forward (rollout.cpp:153-168): the tape of states (and of positions, moving) before each step."""
         self.load(U0)
         violations = 0
         for s in range(self.steps):
             self.fv.get_state(out=self.tape[s])
+            if self.moving:
+                self.xtape[s].copy_(self.torch.from_numpy(self.fv.positions()))
             violations += self.fv.time_step(self.courant) < self.dt
-            self.fv.step(self.dt)
+            if self.moving:
+                self.fv.step_moving_device(self.dt, self.remesher)
+            else:
+                self.fv.step(self.dt)
         return violations
 
     def final_rows(self) -> np.ndarray:
+        """Rollout::final_rows (rollout.cpp:169-183): Q, x and the volumes of the final mesh."""
         w = self.V + self.dim + 1
         rows = np.empty((self.n, w))
         rows[:, :self.V] = self.fv.get_state()
-        rows[:, self.V:self.V + self.dim] = self.x0
-        rows[:, -1] = self.V0
+        if self.moving:
+            rows[:, self.V:self.V + self.dim] = self.fv.positions()
+            rows[:, -1] = self.fv.mesh.cells().volume if hasattr(self.fv.mesh, "cells") else self.fv.mesh.volume
+        else:
+            rows[:, self.V:self.V + self.dim] = self.x0
+            rows[:, -1] = self.V0
         return rows
 
     def adjoint(self, bars: np.ndarray) -> np.ndarray:
+        if self.moving:
+            raise NotImplementedError("the moving mesh's adjoint (step_moving_adjoint) is not in libluna_b200")
         w = self.V + self.dim + 1
         qbar = self.torch.tensor(np.ascontiguousarray(bars.reshape(self.n, w)[:, :self.V]), device="cuda")
         for s in range(self.steps - 1, -1, -1):
@@ -93,6 +120,8 @@ class Server:
 
     def tangent(self, U0: np.ndarray, dU0: np.ndarray) -> np.ndarray:
         """Rollout::tangent (rollout.cpp:170-196), static: time_step then step_tangent every step."""
+        if self.moving:
+            raise NotImplementedError("the moving mesh's tangent (step_moving_tangent) is not in libluna_b200")
         self.load(U0)
         dq = self.torch.tensor(np.ascontiguousarray(dU0.reshape(self.n, self.V) * self.V0[:, None]), device="cuda")
         for _ in range(self.steps):
@@ -114,13 +143,10 @@ def now_ms(torch) -> float:
 
 
 def serve(argv, stdin=sys.stdin, stdout=sys.stdout) -> int:
-    if any(a == "--moving" for a in argv):
-        stdout.write("error the moving mesh's rollout needs its derivatives, which libluna_b200 does not have\n")
-        stdout.flush()
-        return 1
     dim = int(flag(argv, "--dim", "2"))
     srv = Server(dim, int(flag(argv, "--n", "64")), int(flag(argv, "--steps", "100")), float(flag(argv, "--dt", "1e-3")),
-                 float(flag(argv, "--gamma", "1.6666666666666667")), float(flag(argv, "--courant", "0.3")))
+                 float(flag(argv, "--gamma", "1.6666666666666667")), float(flag(argv, "--courant", "0.3")),
+                 moving=any(a == "--moving" for a in argv))
     torch = srv.torch
     N, V, w = srv.n, srv.V, srv.V + dim + 1
 
