@@ -83,7 +83,7 @@ typedef struct luna_fv luna_fv;
 
 /* FiniteVolume(exec, mesh, gas, order, update, limiter, motion) (finite_volume.hpp:79-107) with the Riemann and
  * Precision template parameters as arguments. order 0 or 1 (else LUNA_EINVAL, as the reference's invalid_argument).
- * A moving mesh requires order 1 and the per-face update. */
+ * A moving mesh requires the per-face update. */
 LUNA_API luna_status luna_fv_create(const luna_mesh_desc* mesh, const luna_gas* gas, int order, int update, int limiter,
                                     int motion, int riemann, int precision, luna_fv** out);
 LUNA_API luna_status luna_fv_destroy(luna_fv* fv);
@@ -113,7 +113,9 @@ LUNA_API luna_status luna_fv_error_word(luna_fv* fv, uint32_t* out);
  * belongs to the mesh library: begin snaps the points to the mesh grid (2^-30 of the longest side), keeps the
  * centroids of t^n, applies the t^n fluxes at dt/2 and drifts the points; it writes the new generator positions
  * [N][D] (host or device memory) for the caller's remesh. end takes the t^n+1 mesh (same cells, same order) and
- * applies its fluxes at dt/2. */
+ * applies its fluxes at dt/2. Order 0 (step(): advance<0, true>() then move(), :205-226, :1212-1228): begin applies the
+ * fluxes of the current mesh at dt (each side the cell's W, the face velocities from the point velocities) and drifts
+ * the points off the grid (x + dt w, wrapped); end takes the new mesh. */
 LUNA_API luna_status luna_fv_step_moving_begin(luna_fv* fv, double dt, double* positions_out, int on_device);
 LUNA_API luna_status luna_fv_step_moving_end(luna_fv* fv, const luna_mesh_desc* new_mesh);
 /* A static mesh replaced by another of the same cells (checkpoint restore; FiniteVolume::mesh_moved). */
@@ -135,6 +137,22 @@ LUNA_API luna_status luna_fv_step_adjoint(luna_fv* fv, double dt, double* qbar, 
  * tangent of Q, extensive) at fixed dt, linearised at the same point as luna_fv_step_adjoint (so the two are transposes:
  * <J dq, qbar> = <dq, J^T qbar>). Q advances as luna_fv_step(fv, dt) advances it. The same restrictions as the adjoint. */
 LUNA_API luna_status luna_fv_step_tangent(luna_fv* fv, double dt, double* dq, int on_device);
+
+/* The order-0 moving step's derivatives at fixed topology (step_moving_tangent / step_moving_adjoint,
+ * finite_volume.hpp:2431-2604): the state is (Q, x); a moving mesh, order 0, the per-face loop, the FP64 policy, dt
+ * fixed, outside a moving step. The geometry's own derivative in the generators (V, c, A, x_f) belongs to the mesh
+ * library (GeometryDerivative, mesh_derivative.hpp:10-29): the tangent takes its tangents, the adjoint hands back its
+ * bars. All arrays host or all device memory (on_device); Q's rows [N][D + 2], x's [N][D], V's [N], c's [N][D], A's and
+ * x_f's [F][D].
+ * tangent: dq, dx (of Q, x at the step's start) become those after the step; dV, dc, dA, dxf are GeometryDerivative::
+ * tangent(dx) of the current mesh. Nothing steps: the caller then runs the step (begin, remesh, end).
+ * adjoint: qbar, xbar (of Q, x after the step) become those at its start, but for the geometry's part: Vbar, cbar, Abar,
+ * xfbar are written, and the caller adds GeometryDerivative::adjoint(Vbar, cbar, Abar, xfbar) to xbar. Q and the mesh
+ * must be the step's start; nothing steps. No atomics: the same bits every run. */
+LUNA_API luna_status luna_fv_step_moving_tangent(luna_fv* fv, double dt, double* dq, double* dx, const double* dV, const double* dc,
+                                                 const double* dA, const double* dxf, int on_device);
+LUNA_API luna_status luna_fv_step_moving_adjoint(luna_fv* fv, double dt, double* qbar, double* xbar, double* Vbar, double* cbar, double* Abar,
+                                                 double* xfbar, int on_device);
 
 /* Per-phase device time (hydro::Timings, finite_volume.hpp:36-39, without its fences): with timing on, CUDA events on
  * fv's stream bracket every kernel; luna_fv_timings synchronises, adds the elapsed times since the last reset and counts

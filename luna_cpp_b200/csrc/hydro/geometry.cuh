@@ -95,8 +95,11 @@ struct GeometryDev {
 // (its own and the halo, tiles.h) copied into shared memory first (2 D doubles a row), each entry's neighbour read there
 // through its staged row (the tiler's entry words) instead of through the face's owner / neighbour; the same values, so
 // the same rows.
+#ifndef LUNA_GEOMETRY_MIN_BLOCKS
+#define LUNA_GEOMETRY_MIN_BLOCKS 5  // measured at 128^3 (moving hydro ms): unbounded (114 registers) 4.70, 5 4.62, 6 4.69
+#endif
 template <int D, class G, bool FaceRows = true, bool Staged = false>
-__global__ void __launch_bounds__(128) k_geometry(MeshDev<D> m, GeometryDev<D, G> g, int tile0) {
+__global__ void __launch_bounds__(128, LUNA_GEOMETRY_MIN_BLOCKS) k_geometry(MeshDev<D> m, GeometryDev<D, G> g, int tile0) {
     constexpr int U = D + 1, B = LUNA_GEOMETRY_BATCH;
     extern __shared__ double geo_rows[];  // Staged: [staged rows][2 D]: generator, centroid
     const int tile = tile0 + static_cast<int>(blockIdx.x);

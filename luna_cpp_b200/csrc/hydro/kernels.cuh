@@ -291,6 +291,7 @@ struct FluxArgs {
     double unit;                            // moving: grid step / dt
     GasDev gas;
     const double* __restrict__ wg = nullptr;           // FP64 static per-face step: merged rows [N][wg_stride] (W, g)
+    const double* __restrict__ w = nullptr;            // order-0 moving step: the point velocities [N][D]
     const uint16_t* __restrict__ grad16 = nullptr;    // Grad16: binary16 rows [N][16] instead of grad (G = float)
     const uint32_t* __restrict__ exponents = nullptr;  // Grad16: the three int8 group exponents of each row
 };
@@ -459,7 +460,8 @@ __device__ __forceinline__ void face_velocity(const MeshDev<D>& m, int f, int o,
 }
 
 // The flux through face f times |A| (FaceFlux::operator(), finite_volume.hpp:1415-1434; MovingFlux::operator(),
-// :1469-1490). Pass: -1 static, 0 moving on the mesh of t^n, 1 moving on the mesh of t^n+1.
+// :1469-1490). Pass: -1 static, 0 moving on the mesh of t^n, 1 moving on the mesh of t^n+1, 2 the order-0 moving step
+// (FaceFlux<0, true>: each side the cell's W, the face velocity from the point velocities).
 template <int D, int Order, int Pass, class G, bool RF, int Riemann, bool H = false>
 __device__ __forceinline__ void face_flux(const MeshDev<D>& m, const FluxArgs<D, G>& x, int f, double* F, int& fb_o, int& fb_j) {
     constexpr int V = D + 2;
@@ -480,7 +482,18 @@ __device__ __forceinline__ void face_flux(const MeshDev<D>& m, const FluxArgs<D,
         n[k] = a[k] * inv;
         wf[k] = 0;
     }
-    if constexpr (Pass < 0) {
+    if constexpr (Pass == 2) {
+        static_assert(Order == 0, "the order-0 moving step");
+        face_velocity<D>(m, f, o, j, x.w + D * o, x.w + D * j, wf);
+        double U[V];
+        const double io = 1.0 / m.vol[o], ij = 1.0 / m.vol[j];
+#pragma unroll
+        for (int v = 0; v < V; ++v) U[v] = x.q[V * o + v] * io;
+        primitive<D>(U, x.gas, L);
+#pragma unroll
+        for (int v = 0; v < V; ++v) U[v] = x.q[V * j + v] * ij;
+        primitive<D>(U, x.gas, R);
+    } else if constexpr (Pass < 0) {
         if constexpr (Order == 0) {
             double U[V];
             const double io = 1.0 / m.vol[o], ij = 1.0 / m.vol[j];
@@ -551,8 +564,11 @@ __device__ __forceinline__ void store_flux_row(FS* flux, int64_t f, const double
 }
 
 // apply()'s flux pass (finite_volume.hpp:1591-1602): one flux row per face.
+#ifndef LUNA_KFLUX_MIN_BLOCKS_F
+#define LUNA_KFLUX_MIN_BLOCKS_F 8  // the float policies' flux passes over the mesh arrays (the moving step's); measured at
+#endif                             // 128^3 (moving hydro ms): unbounded (72-80 registers) 4.70, 7 blocks 4.20, 8 4.16
 template <int D, int Order, int Pass, class G, bool RF, int Riemann, bool H = false, class FS = double>
-__global__ void __launch_bounds__(128) k_flux(MeshDev<D> m, FluxArgs<D, G> x, FS* __restrict__ flux,
+__global__ void __launch_bounds__(128, sizeof(G) == sizeof(float) ? LUNA_KFLUX_MIN_BLOCKS_F : 1) k_flux(MeshDev<D> m, FluxArgs<D, G> x, FS* __restrict__ flux,
                                               unsigned long long* __restrict__ fallbacks) {
     constexpr int V = D + 2;
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
@@ -760,6 +776,19 @@ __global__ void k_keep_centroids(int n, const double* __restrict__ cen, double* 
         if (d > p / 2) d -= p;
         if (d < -(p / 2)) d += p;
         steps[D * i + a] = static_cast<int32_t>(d);
+    }
+}
+
+// move() of the order-0 moving step (finite_volume.hpp:1212-1228, off the grid): x + dt w, wrapped into the box.
+template <int D>
+__global__ void k_drift_free(int n, double* __restrict__ x, const double* __restrict__ w, double dt, double s0, double s1, double s2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double side[3] = {s0, s1, s2};
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        const double moved = x[D * i + a] + dt * w[D * i + a];
+        x[D * i + a] = moved - side[a] * floor(moved / side[a]);
     }
 }
 

@@ -22,6 +22,7 @@
 #include "geometry.cuh"
 #include "kernels.cuh"
 #include "mlp.cuh"
+#include "moving_derivative.cuh"
 #include "luna_b200.h"
 
 namespace {
@@ -132,6 +133,10 @@ struct luna_fv {
     // tangent (allocated by the first luna_fv_step_tangent): dW, dg per cell, dF per face, a device copy of dq
     DevArray<double> tan_dprims, tan_dgrad, tan_dflux, tan_dq;
     DevArray<int32_t> adj_flags, adj_bound_face;
+    // the order-0 moving step's derivatives (allocated by their first call): W and c_s rows and their tangents, w, dw, the
+    // faces' dG or bar rows, the angle faces' bars, and device copies of the caller's host arrays
+    DevArray<double> mv_W, mv_dW, mv_w, mv_dw, mv_face, mv_angle_Abar, mv_angle_dbar, mv_in[6];
+    DevArray<int32_t> mv_angle_f;
     luna::Counters* host_counters = nullptr;  // pinned
 
     // Per-phase timing: event pairs recorded around each launch, reduced on request.
@@ -549,10 +554,10 @@ luna_status run_sweep(luna_fv* fv, double courant) {
     LUNA_CUDA(cudaMemcpyAsync(&fv->counters.ptr->dt_bits, &init, sizeof(init), cudaMemcpyHostToDevice, fv->stream));
     const bool moving = fv->motion == LUNA_MOVING, grad = fv->order == 1;
     if (fv->precision != LUNA_FP64) {
-        if (moving) return launch_sweep<D, true, true, float>(fv, fv->grad32.ptr, courant);
+        if (moving) return grad ? launch_sweep<D, true, true, float>(fv, fv->grad32.ptr, courant) : launch_sweep<D, true, false, float>(fv, fv->grad32.ptr, courant);
         return grad ? launch_sweep<D, false, true, float>(fv, fv->grad32.ptr, courant) : launch_sweep<D, false, false, float>(fv, fv->grad32.ptr, courant);
     }
-    if (moving) return launch_sweep<D, true, true, double>(fv, fv->grad64.ptr, courant);
+    if (moving) return grad ? launch_sweep<D, true, true, double>(fv, fv->grad64.ptr, courant) : launch_sweep<D, true, false, double>(fv, fv->grad64.ptr, courant);
     return grad ? launch_sweep<D, false, true, double>(fv, fv->grad64.ptr, courant) : launch_sweep<D, false, false, double>(fv, fv->grad64.ptr, courant);
 }
 
@@ -827,6 +832,33 @@ luna_status moving_begin(luna_fv* fv, double dt) {
     if (!fv->swept) LUNA_TRY(prepare_sweep<D>(fv, 1.0));
     fv->swept = false;
     LUNA_CUDA(cudaMemsetAsync(&fv->counters.ptr->fallbacks[0], 0, 2 * sizeof(unsigned long long), fv->stream));
+    if (fv->order == 0) {  // step(): advance<0, true>() on this mesh, then move() (finite_volume.hpp:205-226, :1212-1228)
+        fv->pending_dt = dt;
+        if (fv->precision != LUNA_FP64) {
+            auto x = flux_args<D, float>(fv, fv->grad32.ptr, dt);
+            x.w = fv->w.ptr;
+            LUNA_TRY(float_riemann(fv) ? (launch_flux<D, 0, 2, float, true, 0>(fv, x)) : (launch_flux<D, 0, 2, float, false, 0>(fv, x)));
+        } else {
+            auto x = flux_args<D, double>(fv, fv->grad64.ptr, dt);
+            x.w = fv->w.ptr;
+            LUNA_TRY(fv->riemann == LUNA_HLL ? (launch_flux<D, 0, 2, double, false, 1>(fv, x)) : (launch_flux<D, 0, 2, double, false, 0>(fv, x)));
+        }
+        {
+            const long timed_ = fv->open_timed(3);
+            launch_update<D, false>(fv, dt);
+            fv->close_timed(timed_);
+        }
+        LUNA_CUDA(cudaGetLastError());
+        {
+            const long timed_ = fv->open_timed(4);
+            luna::k_drift_free<D><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(static_cast<int>(fv->n), fv->x.ptr, fv->w.ptr, dt, fv->box[0],
+                                                                              fv->box[1], fv->box[2]);
+            fv->close_timed(timed_);
+        }
+        LUNA_CUDA(cudaGetLastError());
+        fv->moving_pending = true;
+        return LUNA_OK;
+    }
     {
         const long timed_ = fv->open_timed(4);
         luna::k_keep_centroids<D><<<blocks(fv->n, 256), 256, 0, fv->stream>>>(static_cast<int>(fv->n), fv->cen.ptr, fv->old_cen.ptr, fv->x.ptr, fv->w.ptr,
@@ -873,6 +905,13 @@ luna_status moving_begin(luna_fv* fv, double dt) {
 template <int D>
 luna_status moving_end(luna_fv* fv) {
     const double dt = fv->pending_dt;
+    if (fv->order == 0) {  // the new mesh is taken; its volumes change W, so the next step recomputes the primitive rows
+        LUNA_CUDA(cudaMemcpyAsync(fv->x.ptr, fv->pos.ptr, static_cast<size_t>(fv->n) * fv->dim * sizeof(double), cudaMemcpyDeviceToDevice,
+                                  fv->stream));
+        fv->prims_ready = false;
+        fv->moving_pending = false;
+        return LUNA_OK;
+    }
     if (fv->precision != LUNA_FP64) {
         auto x = flux_args<D, float>(fv, fv->grad32.ptr, 2 * dt);
         x.unit = fv->grid_step / dt;
@@ -1022,6 +1061,89 @@ luna_status copy_out(const double* src, double* dst, size_t count, int on_device
     return LUNA_OK;
 }
 
+// The order-0 moving step's derivatives (finite_volume.hpp:2431-2604; kernels in moving_derivative.cuh).
+
+luna_status check_moving_derivative(luna_fv* fv, double dt, const char* what) {
+    if (fv->motion != LUNA_MOVING || fv->order != 0 || fv->update != LUNA_UPDATE_PER_FACE || fv->precision != LUNA_FP64)
+        return set_error(LUNA_EINVAL, std::string("hydro::FiniteVolume::") + what + ": a moving mesh, order 0, the per-face loop, the FP64 policy");
+    if (fv->moving_pending) return set_error(LUNA_ESTATE, "inside a moving step");
+    if (!(dt >= 0)) return set_error(LUNA_EINVAL, "dt must be >= 0");
+    return LUNA_OK;
+}
+
+// The caller's arrays on the device: the array itself (on_device) or a copy into the library's slot k.
+luna_status device_view(luna_fv* fv, int k, const double* src, size_t count, int on_device, const double** out) {
+    if (!src) return set_error(LUNA_EINVAL, "null argument");
+    if (on_device) {
+        *out = src;
+        return LUNA_OK;
+    }
+    LUNA_TRY(fv->mv_in[k].alloc(count > 0 ? count : 1, "moving derivative input"));
+    if (count) LUNA_CUDA(cudaMemcpyAsync(fv->mv_in[k].ptr, src, count * sizeof(double), cudaMemcpyHostToDevice, fv->stream));
+    *out = fv->mv_in[k].ptr;
+    return LUNA_OK;
+}
+
+template <int D>
+luna_status moving_work(luna_fv* fv) {
+    constexpr int V = D + 2;
+    const size_t N = static_cast<size_t>(fv->n), F = static_cast<size_t>(fv->f);
+    LUNA_TRY(fv->mv_W.alloc(N * (V + 1), "moving W rows"));
+    LUNA_TRY(fv->mv_dW.alloc(N * (V + 1), "moving W tangents"));
+    LUNA_TRY(fv->mv_w.alloc(N * D, "moving point velocities"));
+    LUNA_TRY(fv->mv_dw.alloc(N * D, "moving point velocity tangents"));
+    LUNA_TRY(fv->mv_face.alloc((F > 0 ? F : 1) * luna::mvd::bar_width<D>(), "moving face rows"));
+    LUNA_TRY(fv->mv_angle_Abar.alloc(N * D, "angle faces' area bars"));
+    LUNA_TRY(fv->mv_angle_dbar.alloc(N * D, "angle faces' separation bars"));
+    LUNA_TRY(fv->mv_angle_f.alloc(N, "angle faces"));
+    return LUNA_OK;
+}
+
+template <int D>
+luna_status run_moving_tangent(luna_fv* fv, double dt, double* dq, double* dx, const double* dV, const double* dc, const double* dA,
+                               const double* dxf) {
+    LUNA_TRY(moving_work<D>(fv));
+    const auto m = fv->mesh_dev<D>();
+    const unsigned int cb = blocks(fv->n, 128), fb = blocks(fv->f > 0 ? fv->f : 1, 128);
+    luna::mvd::k_mv_prims<D><<<cb, 128, 0, fv->stream>>>(m, fv->q.ptr, dq, dV, fv->gas, fv->mv_W.ptr, fv->mv_dW.ptr);
+    luna::mvd::k_mv_velocity<D><<<cb, 128, 0, fv->stream>>>(m, fv->mv_W.ptr, fv->mv_dW.ptr, dx, dc, dA, fv->mv_w.ptr, fv->mv_dw.ptr,
+                                                            fv->mv_angle_f.ptr);
+    if (fv->f > 0) {
+        if (fv->riemann == LUNA_HLL)
+            luna::mvd::k_mv_faces_tangent<D, 1><<<fb, 128, 0, fv->stream>>>(m, fv->mv_W.ptr, fv->mv_dW.ptr, fv->mv_w.ptr, fv->mv_dw.ptr, dx, dA, dxf,
+                                                                            fv->gas, fv->mv_face.ptr);
+        else
+            luna::mvd::k_mv_faces_tangent<D, 0><<<fb, 128, 0, fv->stream>>>(m, fv->mv_W.ptr, fv->mv_dW.ptr, fv->mv_w.ptr, fv->mv_dw.ptr, dx, dA, dxf,
+                                                                            fv->gas, fv->mv_face.ptr);
+    }
+    luna::mvd::k_mv_update_tangent<D><<<cb, 128, 0, fv->stream>>>(m, fv->mv_face.ptr, fv->mv_dw.ptr, dt, dq, dx);
+    LUNA_CUDA(cudaGetLastError());
+    return LUNA_OK;
+}
+
+template <int D>
+luna_status run_moving_adjoint(luna_fv* fv, double dt, double* qbar, double* xbar, double* Vbar, double* cbar, double* Abar, double* xfbar) {
+    LUNA_TRY(moving_work<D>(fv));
+    const auto m = fv->mesh_dev<D>();
+    const unsigned int cb = blocks(fv->n, 128), fb = blocks(fv->f > 0 ? fv->f : 1, 128);
+    luna::mvd::k_mv_prims<D><<<cb, 128, 0, fv->stream>>>(m, fv->q.ptr, nullptr, nullptr, fv->gas, fv->mv_W.ptr, nullptr);
+    luna::mvd::k_mv_velocity<D><<<cb, 128, 0, fv->stream>>>(m, fv->mv_W.ptr, nullptr, nullptr, nullptr, nullptr, fv->mv_w.ptr, nullptr,
+                                                            fv->mv_angle_f.ptr);
+    if (fv->f > 0) {
+        if (fv->riemann == LUNA_HLL)
+            luna::mvd::k_mv_faces_adjoint<D, 1><<<fb, 128, 0, fv->stream>>>(m, fv->mv_W.ptr, fv->mv_w.ptr, qbar, dt, fv->gas, fv->mv_face.ptr, xfbar);
+        else
+            luna::mvd::k_mv_faces_adjoint<D, 0><<<fb, 128, 0, fv->stream>>>(m, fv->mv_W.ptr, fv->mv_w.ptr, qbar, dt, fv->gas, fv->mv_face.ptr, xfbar);
+    }
+    luna::mvd::k_mv_cells_adjoint<D><<<cb, 128, 0, fv->stream>>>(m, fv->q.ptr, fv->mv_W.ptr, fv->mv_face.ptr, xbar, fv->mv_angle_f.ptr, dt, fv->gas,
+                                                                 qbar, Vbar, cbar, fv->mv_angle_Abar.ptr, fv->mv_angle_dbar.ptr);
+    if (fv->f > 0)
+        luna::mvd::k_mv_area_adjoint<D><<<fb, 128, 0, fv->stream>>>(m, fv->mv_face.ptr, fv->mv_angle_f.ptr, fv->mv_angle_Abar.ptr, Abar);
+    luna::mvd::k_mv_separation_adjoint<D><<<cb, 128, 0, fv->stream>>>(m, fv->mv_face.ptr, fv->mv_angle_f.ptr, fv->mv_angle_dbar.ptr, xbar);
+    LUNA_CUDA(cudaGetLastError());
+    return LUNA_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1055,8 +1177,7 @@ LUNA_API luna_status luna_fv_create(const luna_mesh_desc* mesh, const luna_gas* 
         return set_error(LUNA_EINVAL, "precision: FP64, FP32, GRAD32, GRAD16 or SINGLE");
     if (precision != LUNA_FP64 && riemann == LUNA_HLL)
         return set_error(LUNA_EINVAL, "the FP32 policy takes HLLC (the reference's reduced presets are HLLC only)");
-    if (motion == LUNA_MOVING && (order != 1 || update != LUNA_UPDATE_PER_FACE))
-        return set_error(LUNA_EINVAL, "a moving mesh runs order 1 with the per-face update");
+    if (motion == LUNA_MOVING && update != LUNA_UPDATE_PER_FACE) return set_error(LUNA_EINVAL, "a moving mesh runs the per-face update");
     LUNA_TRY(validate_mesh(mesh, 0, 0));
     luna_fv* fv = new (std::nothrow) luna_fv();
     if (!fv) return set_error(LUNA_ENOMEM, "luna_fv");
@@ -1332,6 +1453,64 @@ LUNA_API luna_status luna_fv_step_tangent(luna_fv* fv, double dt, double* dq, in
     return LUNA_OK;
 }
 
+LUNA_API luna_status luna_fv_step_moving_tangent(luna_fv* fv, double dt, double* dq, double* dx, const double* dV, const double* dc,
+                                                 const double* dA, const double* dxf, int on_device) {
+    if (!fv || !dq || !dx) return set_error(LUNA_EINVAL, "null argument");
+    LUNA_TRY(check_moving_derivative(fv, dt, "step_moving_tangent"));
+    const int D = fv->dim;
+    const size_t N = static_cast<size_t>(fv->n), F = static_cast<size_t>(fv->f), nq = N * (D + 2), nx = N * D;
+    const double *gV, *gc, *gA, *gxf, *gq, *gx;
+    LUNA_TRY(device_view(fv, 0, dq, nq, on_device, &gq));
+    LUNA_TRY(device_view(fv, 1, dx, nx, on_device, &gx));
+    LUNA_TRY(device_view(fv, 2, dV, N, on_device, &gV));
+    LUNA_TRY(device_view(fv, 3, dc, nx, on_device, &gc));
+    LUNA_TRY(device_view(fv, 4, dA, F * D, on_device, &gA));
+    LUNA_TRY(device_view(fv, 5, dxf, F * D, on_device, &gxf));
+    double* q_dev = const_cast<double*>(gq);
+    double* x_dev = const_cast<double*>(gx);
+    LUNA_TRY(D == 3 ? run_moving_tangent<3>(fv, dt, q_dev, x_dev, gV, gc, gA, gxf) : run_moving_tangent<2>(fv, dt, q_dev, x_dev, gV, gc, gA, gxf));
+    if (!on_device) {
+        LUNA_CUDA(cudaMemcpyAsync(dq, q_dev, nq * sizeof(double), cudaMemcpyDeviceToHost, fv->stream));
+        LUNA_CUDA(cudaMemcpyAsync(dx, x_dev, nx * sizeof(double), cudaMemcpyDeviceToHost, fv->stream));
+    }
+    LUNA_CUDA(cudaStreamSynchronize(fv->stream));
+    return LUNA_OK;
+}
+
+LUNA_API luna_status luna_fv_step_moving_adjoint(luna_fv* fv, double dt, double* qbar, double* xbar, double* Vbar, double* cbar, double* Abar,
+                                                 double* xfbar, int on_device) {
+    if (!fv || !qbar || !xbar || !Vbar || !cbar || !Abar || !xfbar) return set_error(LUNA_EINVAL, "null argument");
+    LUNA_TRY(check_moving_derivative(fv, dt, "step_moving_adjoint"));
+    const int D = fv->dim;
+    const size_t N = static_cast<size_t>(fv->n), F = static_cast<size_t>(fv->f), nq = N * (D + 2), nx = N * D;
+    const double *gq, *gx;
+    LUNA_TRY(device_view(fv, 0, qbar, nq, on_device, &gq));
+    LUNA_TRY(device_view(fv, 1, xbar, nx, on_device, &gx));
+    double* outs[4] = {Vbar, cbar, Abar, xfbar};
+    const size_t counts[4] = {N, nx, F * D, F * D};
+    double* dev_out[4];
+    for (int k = 0; k < 4; ++k) {
+        if (on_device) {
+            dev_out[k] = outs[k];
+        } else {
+            LUNA_TRY(fv->mv_in[2 + k].alloc(counts[k] > 0 ? counts[k] : 1, "moving derivative output"));
+            dev_out[k] = fv->mv_in[2 + k].ptr;
+        }
+    }
+    double* q_dev = const_cast<double*>(gq);
+    double* x_dev = const_cast<double*>(gx);
+    LUNA_TRY(D == 3 ? run_moving_adjoint<3>(fv, dt, q_dev, x_dev, dev_out[0], dev_out[1], dev_out[2], dev_out[3])
+                    : run_moving_adjoint<2>(fv, dt, q_dev, x_dev, dev_out[0], dev_out[1], dev_out[2], dev_out[3]));
+    if (!on_device) {
+        LUNA_CUDA(cudaMemcpyAsync(qbar, q_dev, nq * sizeof(double), cudaMemcpyDeviceToHost, fv->stream));
+        LUNA_CUDA(cudaMemcpyAsync(xbar, x_dev, nx * sizeof(double), cudaMemcpyDeviceToHost, fv->stream));
+        for (int k = 0; k < 4; ++k)
+            if (counts[k]) LUNA_CUDA(cudaMemcpyAsync(outs[k], dev_out[k], counts[k] * sizeof(double), cudaMemcpyDeviceToHost, fv->stream));
+    }
+    LUNA_CUDA(cudaStreamSynchronize(fv->stream));
+    return LUNA_OK;
+}
+
 // The learned limiter's buffers (64 B of features, 40 B of admissible factors, 64 B of logits and a compact row's cell a
 // cell, and the row count).
 static luna_status alloc_learned(luna_fv* fv) {
@@ -1438,6 +1617,9 @@ LUNA_API luna_status luna_fv_device_bytes(luna_fv* fv, int64_t* out) {
     b += fv->lim_cells.bytes() + fv->lim_count.bytes();
     b += fv->fz_tstart.bytes() + fv->fz_eslot.bytes() + fv->fz_tface.bytes() + fv->fz_xface.bytes() + fv->fz_trows.bytes() + fv->fz_xrows.bytes();
     b += fv->fz_xflux.bytes();
+    b += fv->mv_W.bytes() + fv->mv_dW.bytes() + fv->mv_w.bytes() + fv->mv_dw.bytes() + fv->mv_face.bytes() + fv->mv_angle_Abar.bytes();
+    b += fv->mv_angle_dbar.bytes() + fv->mv_angle_f.bytes();
+    for (const auto& a : fv->mv_in) b += a.bytes();
     *out = static_cast<int64_t>(b);
     return LUNA_OK;
 }

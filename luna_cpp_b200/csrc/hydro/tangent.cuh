@@ -63,7 +63,8 @@ __device__ __forceinline__ Dual fmax(const Dual& a, const Dual& b) { return b.v 
 
 // HLL (euler.hpp:444-461) for any arithmetic type T (the step's hll_flux is double only).
 template <int D, class T>
-__device__ __forceinline__ void hll_flux_t(const T* L, const T* R, const T* n, const T* w, T gamma, T inverse_gm1, T* F) {
+__device__ __forceinline__ void hll_flux_t(const T* L, const T* R, const T* n, const T* w, T gamma, T inverse_gm1, T* F,
+                                           bool moving_frame = false) {
     constexpr int P = D + 1;
     Side<D, T> l, r;
     T rel[D];
@@ -94,6 +95,7 @@ __device__ __forceinline__ void hll_flux_t(const T* L, const T* R, const T* n, c
 #pragma unroll
         for (int v = 0; v < D + 2; ++v) F[v] = (SR * l.F[v] - SL * r.F[v] + SL * SR * (r.U[v] - l.U[v])) * inv_dS;
     }
+    if (moving_frame) to_lab<D, T>(F, w);
 }
 
 }  // namespace fwd

@@ -79,6 +79,8 @@ SIGNATURES = {
     "luna_last_error": ([], ctypes.c_char_p),
     "luna_fv_device_bytes": ([P, P], I),
     "luna_fv_fused_pass": ([P, P, P], I),
+    "luna_fv_step_moving_tangent": ([P, D64, P, P, P, P, P, P, I], I),
+    "luna_fv_step_moving_adjoint": ([P, D64, P, P, P, P, P, P, I], I),
     "luna_fv_set_timing": ([P, I], I),
     "luna_fv_step_adjoint": ([P, D64, P, I], I),
     "luna_fv_step_tangent": ([P, D64, P, I], I),
@@ -326,6 +328,29 @@ class FiniteVolume:
         a = np.ascontiguousarray(dq, dtype=np.float64).copy()
         check(lib().luna_fv_step_tangent(self._h, dt, a.ctypes.data, 0))
         return a
+
+    def step_moving_tangent(self, dt: float, dq, dx, geometry):
+        """The order-0 moving step's tangent at fixed topology (luna_fv_step_moving_tangent): (dq, dx) of (Q, x) at the
+        step's start -> after it; ``geometry`` is the current mesh's GeometryDerivative (``tangent(dx) -> dV, dc, dA,
+        dxf``, e.g. luna_cpp_b200.geometry_derivative.Geometry2D). Nothing steps. Returns (dq, dx) as new arrays."""
+        q = np.ascontiguousarray(dq, dtype=np.float64).copy()
+        x = np.ascontiguousarray(dx, dtype=np.float64).copy()
+        dV, dc, dA, dxf = (np.ascontiguousarray(a, dtype=np.float64) for a in geometry.tangent(x))
+        check(lib().luna_fv_step_moving_tangent(self._h, dt, q.ctypes.data, x.ctypes.data, dV.ctypes.data, dc.ctypes.data,
+                                                dA.ctypes.data, dxf.ctypes.data, 0))
+        return q, x
+
+    def step_moving_adjoint(self, dt: float, qbar, xbar, geometry):
+        """The order-0 moving step's adjoint (luna_fv_step_moving_adjoint), the geometry's part through ``geometry``'s
+        ``adjoint(Vbar, cbar, Abar, xfbar) -> xbar``: (qbar, xbar) after the step -> at its start. The state and the mesh
+        must be the step's start. Returns (qbar, xbar) as new arrays."""
+        q = np.ascontiguousarray(qbar, dtype=np.float64).copy()
+        x = np.ascontiguousarray(xbar, dtype=np.float64).copy()
+        N, F, D = self.n, int(self.mesh.n_faces), self.dim
+        Vb, cb, Ab, xfb = np.empty(N), np.empty((N, D)), np.empty((F, D)), np.empty((F, D))
+        check(lib().luna_fv_step_moving_adjoint(self._h, dt, q.ctypes.data, x.ctypes.data, Vb.ctypes.data, cb.ctypes.data,
+                                                Ab.ctypes.data, xfb.ctypes.data, 0))
+        return q, x + geometry.adjoint(Vb, cb, Ab, xfb)
 
     def set_limiter(self, mode: str = "plain", params=None) -> None:
         """The slope limiter of the sweep: "plain" (the reference's), "learned" (the MLP with ``params``, a CUDA float32

@@ -108,3 +108,27 @@ def test_moving_steps(reference):
     assert np.array_equal(gpu.positions(), ref.positions())
     got, want = gpu.get_state(), ref.get_state()
     assert np.max(np.abs(got - want)) <= 1e-12 * np.max(np.abs(want))
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_moving_steps_order_0(reference, dim):
+    """The order-0 moving step (step(): FaceFlux<0, true> on the current mesh with the point velocities' face velocities,
+    then move() off the grid and the mesh update, finite_volume.hpp:205-226, :1212-1228): three steps against the
+    reference's own, each side remeshing with the host builder."""
+    from luna_cpp_b200.problems import rough_state
+
+    mesh = jittered_mesh(24 if dim == 2 else 12, dim=dim, jitter=0.3 if dim == 2 else 0.1)
+    q0 = rough_state(mesh.n_cells, dim=dim) * mesh.volume[:, None]
+    box = tuple(mesh.box[:dim])
+    gpu = hydro.FiniteVolume(mesh, order=0, motion="moving")
+    ref = R.ReferenceFV(mesh, order=0, moving=True, remesh=lambda x: build_mesh(x, box=box))
+    gpu.set_state(q0)
+    ref.set_state(q0)
+    for _ in range(3):
+        dg, dr = gpu.time_step(0.3), ref.time_step(0.3)
+        assert abs(dg - dr) <= 1e-13 * dr
+        gpu.step_moving(dr, lambda x: build_mesh(x, box=box))
+        ref.step(dr)
+    assert np.max(np.abs(gpu.positions() - ref.positions())) <= 1e-15
+    got, want = gpu.get_state(), ref.get_state()
+    assert np.max(np.abs(got - want)) <= 1e-12 * np.max(np.abs(want))
