@@ -29,6 +29,11 @@ class _Arrays(ctypes.Structure):
 
 
 _REMESH = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(_Arrays))
+# the caller's GeometryDerivative (mesh_derivative.hpp:10-29): tangent(dx -> dV, dc, dA, dxf), adjoint(bars -> adds to xbar)
+_GEO_TANGENT = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                ctypes.c_void_p)
+_GEO_ADJOINT = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                ctypes.c_void_p)
 _lib = None
 
 
@@ -67,6 +72,9 @@ def lib():
         "lr_fv_cells": ([P], I),
         "lr_fv_faces": ([P], I),
         "lr_fv_density_gradients": ([P, P], I),
+        "lr_fv_set_positions": ([P, P], I),
+        "lr_fv_step_moving_tangent": ([P, D, P, P, _GEO_TANGENT, _GEO_ADJOINT, P], I),
+        "lr_fv_step_moving_adjoint": ([P, D, P, P, _GEO_TANGENT, _GEO_ADJOINT, P], I),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -194,3 +202,47 @@ class ReferenceFV:
         out = np.zeros((self.n, self.dim))
         _check(lib().lr_fv_density_gradients(self._h, out.ctypes.data))
         return out
+
+    def set_positions(self, x):
+        """A moving mesh's positions and their mesh (Rollout::load_positions, rollout.cpp:146-152); Q is kept."""
+        a = np.ascontiguousarray(x, dtype=np.float64)
+        _check(lib().lr_fv_set_positions(self._h, a.ctypes.data))
+
+    def _geometry_callbacks(self, geometry):
+        """The caller's geometry derivative of the current mesh as the driver's two callbacks."""
+        N, D = self.n, self.dim
+
+        def view(ptr, shape):
+            return np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ctypes.c_double)), shape=shape)
+
+        def tangent(user, dx, dV, dc, dA, dxf):
+            F = self.mesh.n_faces
+            out = geometry.tangent(view(dx, (N, D)).copy())
+            for arr, ptr, shape in zip(out, (dV, dc, dA, dxf), ((N,), (N, D), (F, D), (F, D))):
+                view(ptr, shape)[...] = arr
+
+        def adjoint(user, Vbar, cbar, Abar, xfbar, xbar):
+            F = self.mesh.n_faces
+            add = geometry.adjoint(view(Vbar, (N,)).copy(), view(cbar, (N, D)).copy(), view(Abar, (F, D)).copy(),
+                                   view(xfbar, (F, D)).copy())
+            view(xbar, (N, D))[...] += add
+
+        return _GEO_TANGENT(tangent), _GEO_ADJOINT(adjoint)
+
+    def step_moving_tangent(self, dt, dq, dx, geometry):
+        """step_moving_tangent(dt, dq, dx, geometry) (finite_volume.hpp:2431-2486): (dq, dx) -> after the step, and the
+        step itself (the state advances, the mesh moves)."""
+        q = np.ascontiguousarray(dq, dtype=np.float64).copy()
+        x = np.ascontiguousarray(dx, dtype=np.float64).copy()
+        t, a = self._geometry_callbacks(geometry)
+        _check(lib().lr_fv_step_moving_tangent(self._h, dt, q.ctypes.data, x.ctypes.data, t, a, None))
+        return q, x
+
+    def step_moving_adjoint(self, dt, qbar, xbar, geometry):
+        """step_moving_adjoint(dt, qbar, xbar, geometry) (:2490-2604): the bars after the step -> at its start; the state
+        and the mesh must be the step's start."""
+        q = np.ascontiguousarray(qbar, dtype=np.float64).copy()
+        x = np.ascontiguousarray(xbar, dtype=np.float64).copy()
+        t, a = self._geometry_callbacks(geometry)
+        _check(lib().lr_fv_step_moving_adjoint(self._h, dt, q.ctypes.data, x.ctypes.data, t, a, None))
+        return q, x

@@ -17,6 +17,11 @@
 
 namespace lr {
 
+// A GeometryDerivative (mesh_derivative.hpp:10-29) whose tangent and adjoint are the caller's: the tests hand in their
+// own 2D geometry derivative (as the reference's tests hand in theirs, src/test/reference_geometry_2d.hpp).
+typedef void (*GeoTangent)(void* user, const double* dx, double* dV, double* dc, double* dA, double* dxf);
+typedef void (*GeoAdjoint)(void* user, const double* Vbar, const double* cbar, const double* Abar, const double* xfbar, double* xbar);
+
 struct Solver {
     virtual ~Solver() = default;
     virtual int cells() const = 0;
@@ -31,6 +36,25 @@ struct Solver {
     virtual const double* positions() = 0;
     virtual const double* point_velocities() = 0;
     virtual void density_gradients(double* out) = 0;
+    virtual void set_positions(const double* x) = 0;
+    virtual void step_moving_tangent(double dt, double* dq, double* dx, GeoTangent t, GeoAdjoint a, void* user) = 0;
+    virtual void step_moving_adjoint(double dt, double* qbar, double* xbar, GeoTangent t, GeoAdjoint a, void* user) = 0;
+};
+
+template <class Base>
+struct CallbackGeometry : Base {
+    using typename Base::Points;
+    using typename Base::Scalars;
+    GeoTangent t;
+    GeoAdjoint a;
+    void* user;
+    CallbackGeometry(GeoTangent t_, GeoAdjoint a_, void* u) : t(t_), a(a_), user(u) {}
+    void tangent(const Points& dx, const Scalars& dV, const Points& dc, const Points& dA, const Points& dxf) const override {
+        t(user, dx.data(), dV.data(), dc.data(), dA.data(), dxf.data());
+    }
+    void adjoint(const Scalars& Vbar, const Points& cbar, const Points& Abar, const Points& xfbar, const Points& xbar) const override {
+        a(user, Vbar.data(), cbar.data(), Abar.data(), xfbar.data(), xbar.data());
+    }
 };
 
 template <int D, class Riemann, class Precision>
@@ -81,6 +105,34 @@ struct SolverOf : Solver {
     void density_gradients(double* out) override {
         const auto rows = fv.density_gradients();
         std::memcpy(out, rows.data(), sizeof(double) * rows.size());
+    }
+    // Rollout::load_positions (rollout.cpp:146-152): the positions, the mesh of them, mesh_moved().
+    void set_positions(const double* x) override {
+        if (fv.motion() != hydro::Motion::moving) throw std::logic_error("set_positions: a moving mesh");
+        std::memcpy(fv.positions().data(), x, sizeof(double) * D * static_cast<std::size_t>(cells()));
+        mesh.update(fv.positions());
+        mesh.update_cells();
+        fv.mesh_moved();
+    }
+    void step_moving_tangent(double dt, double* dq, double* dx, GeoTangent t, GeoAdjoint a, void* user) override {
+        if constexpr (std::is_same_v<typename Precision::flux, double> && std::is_same_v<typename Precision::riemann, double>) {
+            typename FV::Cells q(dq, static_cast<std::size_t>(cells()));
+            typename FV::Points x(dx, static_cast<std::size_t>(cells()));
+            const CallbackGeometry<typename FV::Derivative> geometry(t, a, user);
+            fv.step_moving_tangent(dt, q, x, geometry);
+        } else {
+            throw std::logic_error("step_moving_tangent: double flux rows and Riemann solve only");
+        }
+    }
+    void step_moving_adjoint(double dt, double* qbar, double* xbar, GeoTangent t, GeoAdjoint a, void* user) override {
+        if constexpr (std::is_same_v<typename Precision::flux, double> && std::is_same_v<typename Precision::riemann, double>) {
+            typename FV::Cells q(qbar, static_cast<std::size_t>(cells()));
+            typename FV::Points x(xbar, static_cast<std::size_t>(cells()));
+            const CallbackGeometry<typename FV::Derivative> geometry(t, a, user);
+            fv.step_moving_adjoint(dt, q, x, geometry);
+        } else {
+            throw std::logic_error("step_moving_adjoint: double flux rows and Riemann solve only");
+        }
     }
 };
 
@@ -193,6 +245,17 @@ int lr_fv_cells(void* h) { return static_cast<Solver*>(h)->cells(); }
 int lr_fv_faces(void* h) { return static_cast<Solver*>(h)->faces(); }
 int lr_fv_density_gradients(void* h, double* out) {
     return guarded([&] { static_cast<Solver*>(h)->density_gradients(out); });
+}
+// A moving mesh's positions [N][D] and the mesh of them (the state is kept).
+int lr_fv_set_positions(void* h, const double* x) {
+    return guarded([&] { static_cast<Solver*>(h)->set_positions(x); });
+}
+// step_moving_tangent / step_moving_adjoint (finite_volume.hpp:2431-2604) with the caller's geometry derivative.
+int lr_fv_step_moving_tangent(void* h, double dt, double* dq, double* dx, lr::GeoTangent t, lr::GeoAdjoint a, void* user) {
+    return guarded([&] { static_cast<Solver*>(h)->step_moving_tangent(dt, dq, dx, t, a, user); });
+}
+int lr_fv_step_moving_adjoint(void* h, double dt, double* qbar, double* xbar, lr::GeoTangent t, lr::GeoAdjoint a, void* user) {
+    return guarded([&] { static_cast<Solver*>(h)->step_moving_adjoint(dt, qbar, xbar, t, a, user); });
 }
 
 }  // extern "C"

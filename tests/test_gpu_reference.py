@@ -132,3 +132,38 @@ def test_moving_steps_order_0(reference, dim):
     assert np.max(np.abs(gpu.positions() - ref.positions())) <= 1e-15
     got, want = gpu.get_state(), ref.get_state()
     assert np.max(np.abs(got - want)) <= 1e-12 * np.max(np.abs(want))
+
+
+@pytest.mark.parametrize("riemann", ["hllc", "hll"])
+def test_moving_derivatives_order_0(reference, riemann):
+    """The GPU's order-0 moving tangent and adjoint against the reference's own step_moving_tangent /
+    step_moving_adjoint (finite_volume.hpp:2431-2604) on a 2D shear layer, both with this repository's 2D geometry
+    derivative: J (dq, dx) and J^T (qbar, xbar) within 1e-10 of the largest entry."""
+    from luna_cpp_b200.geometry_derivative import Geometry2D
+
+    mesh = jittered_mesh(24, dim=2, jitter=0.3, seed=2)
+    x0 = mesh.positions.copy()
+    layer = np.tanh((0.25 - np.abs(x0[:, 1] - 0.5)) / 0.08)
+    rho, vx, vy = 1.5 + 0.5 * layer, 0.4 * layer, 0.05 * np.sin(2 * np.pi * x0[:, 0])
+    q0 = np.stack([rho, rho * vx, rho * vy, 2.5 / (2 / 3) + 0.5 * rho * (vx * vx + vy * vy)], -1) * mesh.volume[:, None]
+    remesh = lambda p: build_mesh(p, box=(1.0, 1.0))  # noqa: E731
+    gpu = hydro.FiniteVolume(mesh, hydro.Gas(5.0 / 3.0), order=0, motion="moving", riemann=riemann)
+    ref = R.ReferenceFV(mesh, gamma=5.0 / 3.0, order=0, moving=True, riemann=riemann, remesh=remesh)
+    gpu.set_state(q0)
+    ref.set_state(q0)
+    dt = 0.5 * ref.time_step(0.3)
+    gpu.time_step(0.3)
+    rng = np.random.default_rng(5)
+    dq, dx = rng.normal(size=q0.shape) * np.abs(q0), rng.normal(size=x0.shape) * 1e-3
+    got = gpu.step_moving_tangent(dt, dq, dx, Geometry2D(gpu.mesh))
+    want = ref.step_moving_tangent(dt, dq, dx, Geometry2D(ref.mesh))
+    for a, b in zip(got, want):
+        assert np.max(np.abs(a - b)) <= 1e-10 * np.max(np.abs(b))
+    ref.set_positions(x0)
+    ref.set_state(q0)
+    ref.time_step(0.3)
+    qb, xb = rng.normal(size=q0.shape), rng.normal(size=x0.shape)
+    got = gpu.step_moving_adjoint(dt, qb, xb, Geometry2D(gpu.mesh))
+    want = ref.step_moving_adjoint(dt, qb, xb, Geometry2D(ref.mesh))
+    for a, b in zip(got, want):
+        assert np.max(np.abs(a - b)) <= 1e-10 * np.max(np.abs(b))

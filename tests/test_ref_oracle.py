@@ -135,3 +135,37 @@ def test_step_adjoint(reference, dim, nx):
     ga, gb = a.step_adjoint(dt, qbar), b.step_adjoint(dt, qbar)
     assert np.max(np.abs(ga - gb)) <= 1e-11 * np.max(np.abs(gb))
     assert np.array_equal(ga, gb)
+
+
+def _shear(mesh, gamma=5.0 / 3.0):
+    x = mesh.positions
+    layer = np.tanh((0.25 - np.abs(x[:, 1] - 0.5)) / 0.08)
+    rho = 1.5 + 0.5 * layer + 1e-3 * np.random.default_rng(4).uniform(-1, 1, len(x))
+    vx, vy, P = 0.4 * layer, 0.05 * np.sin(2 * np.pi * x[:, 0]), 2.5 + 0.1 * np.cos(2 * np.pi * x[:, 1])
+    U = np.stack([rho, rho * vx, rho * vy, P / (gamma - 1) + 0.5 * rho * (vx * vx + vy * vy)], -1)
+    return U * mesh.volume[:, None]
+
+
+def test_reference_moving_derivatives_dot_test(reference):
+    """The reference's own step_moving_tangent / step_moving_adjoint (order 0, 2D) with this repository's 2D geometry
+    derivative as their GeometryDerivative: the dot test to 1e-12 (the reference's C1, hydro_derivatives_test.cpp:595),
+    which pins the geometry derivative's interface (tangent and adjoint, the adjoint adding to x's bar) to the reference's
+    use of it."""
+    from luna_cpp_b200.geometry_derivative import Geometry2D
+
+    mesh = jittered_mesh(16, dim=2, jitter=0.3, seed=2)
+    q0, x0 = _shear(mesh), mesh.positions.copy()
+    ref = R.ReferenceFV(mesh, gamma=5.0 / 3.0, order=0, moving=True, remesh=lambda p: build_mesh(p, box=(1.0, 1.0)))
+    ref.set_state(q0)
+    dt = 0.5 * ref.time_step(0.3)
+    rng = np.random.default_rng(1)
+    dq, dx = rng.normal(size=q0.shape) * np.abs(q0), rng.normal(size=x0.shape) * 1e-3
+    Jq, Jx = ref.step_moving_tangent(dt, dq, dx, Geometry2D(ref.mesh))
+    ref.set_positions(x0)
+    ref.set_state(q0)
+    ref.time_step(0.3)
+    qb, xb = rng.normal(size=q0.shape), rng.normal(size=x0.shape)
+    Tq, Tx = ref.step_moving_adjoint(dt, qb, xb, Geometry2D(ref.mesh))
+    lhs, rhs = np.sum(qb * Jq) + np.sum(xb * Jx), np.sum(Tq * dq) + np.sum(Tx * dx)
+    size = np.sum(np.abs(qb * Jq)) + np.sum(np.abs(xb * Jx)) + np.sum(np.abs(Tq * dq)) + np.sum(np.abs(Tx * dx))
+    assert abs(lhs - rhs) < 1e-12 * size
