@@ -11,7 +11,8 @@ to the owner). Each Voronoi vertex is the circumcentre of its Delaunay triangle,
 offsets of the triangle's other two generators; a face's two vertices v+ and v- give e = v+ - v-, A = (e_y, -e_x),
 x_f = (v+ + v-) / 2 - x_o; a cell's faces give p_f = A_f . d_f (d_f from the owner to the neighbour), V = sum p_f / 4,
 c = (2/3) sum p_f x_f,i / sum p_f with x_f,i the face centroid relative to the cell. Each vertex's triangle is found
-from the mesh: the third generator is the common neighbour of the face's two cells whose circumcentre is that vertex.
+from the mesh: the third generator is the common neighbour of the face's two cells whose circumcentre is that vertex
+(where four generators are cocircular, as on an exact lattice, a neighbour of either cell: one triangulation's).
 The Jacobian is assembled once per mesh as a sparse matrix (rows V, c, A, x_f; columns x), so the tangent and the
 adjoint are exact transposes. Host code (numpy, scipy): test and driver infrastructure beside the library, as in the
 reference.
@@ -81,17 +82,25 @@ class Geometry2D:
         scale = np.sqrt(np.prod(box) / self.n)
         for f in range(self.f):
             o, j = int(own[f]), int(nbr[f])
-            cands = list(neighbours[o] & neighbours[j])
-            if not cands:
-                raise ValueError(f"Geometry2D: face {f} has no common neighbour of its cells")
-            b = wrap(x[cands] - x[o])
-            cc = _circle(np.repeat(d[f:f + 1], len(cands), 0), b)
+            common = sorted(neighbours[o] & neighbours[j])
+            # A vertex where four or more generators are cocircular (an exact lattice) has no face between the diagonal
+            # pairs, so its third generator need not be a common neighbour: then any neighbour of either cell whose
+            # circumcentre with the face's two is the vertex (the derivative there is that of one triangulation).
+            either = sorted((neighbours[o] | neighbours[j]) - {o, j})
             for s in range(2):
-                err = np.sqrt(np.sum((cc - ends[s][f]) ** 2, -1))
-                k = int(np.argmin(err))
-                if err[k] > tolerance * scale:
-                    raise ValueError(f"Geometry2D: face {f}'s vertex {s} is no circumcentre of its cells' common neighbours "
-                                     f"({err[k]:.2e})")
+                for cands in (common, either):
+                    if not cands:
+                        continue
+                    b = wrap(x[cands] - x[o])
+                    with np.errstate(divide="ignore", invalid="ignore"):  # a candidate in line with the face's two
+                        cc = _circle(np.repeat(d[f:f + 1], len(cands), 0), b)
+                    err = np.sqrt(np.sum((cc - ends[s][f]) ** 2, -1))
+                    err = np.where(np.isfinite(err), err, np.inf)
+                    k = int(np.argmin(err))
+                    if err[k] <= tolerance * scale:
+                        break
+                else:
+                    raise ValueError(f"Geometry2D: face {f}'s vertex {s} is no circumcentre of its cells' neighbours")
                 third[s, f] = cands[k]
                 offset[s, f] = b[k]
         self.own, self.nbr, self.d = own.astype(np.int64), nbr.astype(np.int64), d

@@ -3,7 +3,7 @@ on the Voronoi mesh of the regular n^D lattice of the periodic unit box, and its
 command a line on stdin for Python optimisers (the reference's scripts/examples/rollout_client.py drives it unchanged:
 ``Rollout("luna_cpp_b200/bin/rollout", dim, n, steps, dt, workdir)``).
 
-    python -m luna_cpp_b200.rollout --dim=2 --n=64 --steps=100 --dt=1e-3 [--gamma=5/3] [--courant=0.3]
+    python -m luna_cpp_b200.rollout --dim=2 --n=64 --steps=100 --dt=1e-3 [--gamma=5/3] [--courant=0.3] [--moving] [--order=1]
 
 Commands (paths are raw float64 files, C order; cells in lattice C order, the last axis fastest):
     forward <U0 in> <final out>       U0: N x V intensive; runs the steps keeping the tape (on the device); final: N x
@@ -19,8 +19,11 @@ Commands (paths are raw float64 files, C order; cells in lattice C order, the la
 The fixed dt is checked against time_step(courant) of every step; the steps where it is larger are counted.
 ``--moving``: the moving mesh (Rollout with Motion::moving, rollout.cpp:138-163), remeshed on the device every step;
 the forward keeps the positions' tape beside the states' and its final rows carry the moved generators and the final
-mesh's volumes; ``cfl`` and ``geometry`` start from the lattice's mesh. ``adjoint`` and ``tangent`` answer an error
-line there: the moving step's derivatives (step_moving_adjoint, step_moving_tangent) are not in the library.
+mesh's volumes; ``cfl`` and ``geometry`` start from the lattice's mesh. ``--order=0|1`` (default 1, as the reference's
+server): the scheme's order. The moving derivatives (rollout.cpp:170-271: step_moving_tangent / step_moving_adjoint,
+the final volumes' bars onto the positions through the geometry derivative) are served for order 0 in 2D, with the 2D
+geometry derivative of luna_cpp_b200.geometry_derivative; for order 1, or in 3D, ``adjoint`` and ``tangent`` answer an
+error line (the order-1 moving derivatives and a 3D geometry derivative are not in the library).
 """
 from __future__ import annotations
 
@@ -45,7 +48,8 @@ def lattice(side: int, dim: int) -> np.ndarray:
 
 
 class Server:
-    def __init__(self, dim: int, side: int, steps: int, dt: float, gamma: float, courant: float, moving: bool = False):
+    def __init__(self, dim: int, side: int, steps: int, dt: float, gamma: float, courant: float, moving: bool = False,
+                 order: int = 1):
         import torch
 
         from .hydro import FiniteVolume, Gas
@@ -58,7 +62,8 @@ class Server:
         self.mesh = build_mesh(self.x0, box=(1.0,) * dim)
         self.n = self.mesh.n_cells
         self.V0 = self.mesh.volume.copy()
-        self.fv = FiniteVolume(self.mesh, Gas(gamma), order=1, update="per_face", limiter="face_centroid",
+        self.order = order
+        self.fv = FiniteVolume(self.mesh, Gas(gamma), order=order, update="per_face", limiter="face_centroid",
                                motion="moving" if moving else "static_mesh")
         self.tape = torch.empty((steps, self.n, self.V), dtype=torch.float64, device="cuda")
         self.xtape = None
@@ -93,6 +98,8 @@ class Server:
                 self.fv.step_moving_device(self.dt, self.remesher)
             else:
                 self.fv.step(self.dt)
+        if self.moving:
+            self.final_x = self.fv.positions()  # the final mesh's generators (the adjoint's volume bars)
         return violations
 
     def final_rows(self) -> np.ndarray:
@@ -108,9 +115,18 @@ class Server:
             rows[:, -1] = self.V0
         return rows
 
+    def _moving_derivatives(self, what):
+        if self.order != 0 or self.dim != 2:
+            raise NotImplementedError(f"the moving mesh's {what} is served for order 0 in 2D (the order-1 moving derivatives "
+                                      "and a 3D geometry derivative are not in libluna_b200)")
+        from .geometry_derivative import Geometry2D
+        from .mesh import build_mesh
+
+        return Geometry2D, (lambda x: build_mesh(x, box=(1.0,) * self.dim))
+
     def adjoint(self, bars: np.ndarray) -> np.ndarray:
         if self.moving:
-            raise NotImplementedError("the moving mesh's adjoint (step_moving_adjoint) is not in libluna_b200")
+            return self._moving_adjoint(bars)
         w = self.V + self.dim + 1
         qbar = self.torch.tensor(np.ascontiguousarray(bars.reshape(self.n, w)[:, :self.V]), device="cuda")
         for s in range(self.steps - 1, -1, -1):
@@ -118,10 +134,41 @@ class Server:
             self.fv.step_adjoint(self.dt, qbar)
         return (qbar * self.volume_dev).cpu().numpy()
 
+    def _moving_adjoint(self, bars: np.ndarray) -> np.ndarray:
+        """Rollout::adjoint, moving (rollout.cpp:228-262): the final mesh's volume bars onto the positions, then each step
+        backwards from its taped (Q, x) and the geometry derivative of that step's mesh."""
+        Geometry2D, remesh = self._moving_derivatives("adjoint")
+        w, D = self.V + self.dim + 1, self.dim
+        rows = bars.reshape(self.n, w)
+        qbar, xbar = rows[:, :self.V].copy(), rows[:, self.V:self.V + D].copy()
+        final = remesh(self.final_x)  # the last forward's final mesh (the host builder's is the device remesh's)
+        zero_c, zero_f = np.zeros((self.n, D)), np.zeros((final.n_faces, D))
+        xbar += Geometry2D(final).adjoint(rows[:, -1], zero_c, zero_f, zero_f)
+        for s in range(self.steps - 1, -1, -1):
+            x = self.xtape[s].cpu().numpy()
+            self.fv.set_mesh(remesh(x))
+            self.fv.set_state(self.tape[s])
+            self.fv.time_step(self.courant)  # the point velocities of this state
+            qbar, xbar = self.fv.step_moving_adjoint(self.dt, qbar, xbar, Geometry2D(self.fv.mesh))
+        return qbar * self.V0[:, None]
+
+    def _moving_tangent(self, U0: np.ndarray, dU0: np.ndarray) -> np.ndarray:
+        """Rollout::tangent, moving (rollout.cpp:170-196): the positions' tangent starts at 0; each step's tangent with
+        the geometry derivative of its mesh, then the step (host remesh: the same mesh as the device remesh's)."""
+        Geometry2D, remesh = self._moving_derivatives("tangent")
+        self.load(U0)
+        dq = np.ascontiguousarray(dU0.reshape(self.n, self.V) * self.V0[:, None])
+        dx = np.zeros((self.n, self.dim))
+        for _ in range(self.steps):
+            self.fv.time_step(self.courant)
+            dq, dx = self.fv.step_moving_tangent(self.dt, dq, dx, Geometry2D(self.fv.mesh))
+            self.fv.step_moving(self.dt, remesh)
+        return dq
+
     def tangent(self, U0: np.ndarray, dU0: np.ndarray) -> np.ndarray:
         """Rollout::tangent (rollout.cpp:170-196), static: time_step then step_tangent every step."""
         if self.moving:
-            raise NotImplementedError("the moving mesh's tangent (step_moving_tangent) is not in libluna_b200")
+            return self._moving_tangent(U0, dU0)
         self.load(U0)
         dq = self.torch.tensor(np.ascontiguousarray(dU0.reshape(self.n, self.V) * self.V0[:, None]), device="cuda")
         for _ in range(self.steps):
@@ -146,7 +193,7 @@ def serve(argv, stdin=sys.stdin, stdout=sys.stdout) -> int:
     dim = int(flag(argv, "--dim", "2"))
     srv = Server(dim, int(flag(argv, "--n", "64")), int(flag(argv, "--steps", "100")), float(flag(argv, "--dt", "1e-3")),
                  float(flag(argv, "--gamma", "1.6666666666666667")), float(flag(argv, "--courant", "0.3")),
-                 moving=any(a == "--moving" for a in argv))
+                 moving=any(a == "--moving" for a in argv), order=int(flag(argv, "--order", "1")))
     torch = srv.torch
     N, V, w = srv.n, srv.V, srv.V + dim + 1
 

@@ -22,9 +22,10 @@ def test_lattice_is_c_order_on_the_grid():
 class Client:
     """A minimal client of the protocol (one command a line, raw float64 files)."""
 
-    def __init__(self, tmp, dim, n, steps, dt, moving=False):
+    def __init__(self, tmp, dim, n, steps, dt, moving=False, order=1):
         self.dim, self.N, self.V, self.tmp = dim, n ** dim, dim + 2, tmp
-        self.p = subprocess.Popen([BIN, f"--dim={dim}", f"--n={n}", f"--steps={steps}", f"--dt={dt!r}"] + (["--moving"] if moving else []),
+        extra = (["--moving"] if moving else []) + [f"--order={order}"]
+        self.p = subprocess.Popen([BIN, f"--dim={dim}", f"--n={n}", f"--steps={steps}", f"--dt={dt!r}"] + extra,
                                   stdin=subprocess.PIPE, stdout=subprocess.PIPE, text=True, bufsize=1)
 
     def ask(self, line):
@@ -132,5 +133,55 @@ def test_served_moving_forward(cuda, tmp_path):
         assert c.ask(f"adjoint {tmp_path / 'bars.bin'} {tmp_path / 'ubar.bin'}")[0] == "error"
         out = c.ask("memory")
         assert out[0] == "ok" and int(out[1]) >= int(out[2]) > 0
+    finally:
+        c.close()
+
+
+@pytest.mark.gpu
+def test_served_moving_derivatives_order_0(cuda, tmp_path):
+    """--moving --order=0 in 2D: the served adjoint (the final volumes' bars onto the positions, then each step's
+    step_moving_adjoint with the 2D geometry derivative, rollout.cpp:228-262) against central differences of the served
+    forward of L = <bars, final rows>, and the served tangent against it by the dot test (1e-10). The lattice start puts
+    HLLC's contact speed at zero on the quiet faces (a kink within 1e-5 of U0 along d) and the moved mesh near four-way
+    cocircular vertices, so the differences are good to about 1e-6 with bars on Q alone (h = 1e-6; the reference's own
+    step_moving_tangent gives 8.5e-8 there) and to about 1e-5 with bars on x and V as well."""
+    c = Client(tmp_path, 2, 24, 6, 2e-3, moving=True, order=0)
+    try:
+        xc = (np.arange(24) + 0.5) / 24
+        X, Y = np.meshgrid(xc, xc, indexing="ij")
+        noise = np.random.default_rng(8).uniform(-1e-3, 1e-3, (4,) + X.shape)
+        layer = np.tanh((0.25 - np.abs(Y - 0.5)) / 0.08)
+        rho = 1.5 + 0.5 * layer + noise[0]
+        vx = 0.4 * layer + noise[1]
+        vy = 0.05 * np.sin(2 * np.pi * X) + noise[2]
+        P = 2.5 + noise[3]
+        U0 = np.stack([rho, rho * vx, rho * vy, P / (2 / 3) + 0.5 * rho * (vx * vx + vy * vy)], -1).reshape(-1, 4)
+        fin, violations = c.forward(U0)
+        assert violations == 0
+        rng = np.random.default_rng(4)
+        bars = rng.standard_normal(fin.shape)
+        bars[:, 4:6] *= 10.0  # the positions' and volumes' bars on the scale of Q's effect
+        d = rng.standard_normal(U0.shape) * np.abs(U0) * 1e-2
+        qbars = np.zeros_like(fin)
+        qbars[:, :4] = bars[:, :4]
+        h = 1e-6
+        plus, minus = c.forward(U0 + h * d)[0], c.forward(U0 - h * d)[0]
+        c.forward(U0)  # the adjoint's tape is the last forward's
+        for b, bound in ((qbars, 1e-6), (bars, 1e-4)):
+            b.tofile(tmp_path / "bars.bin")
+            out = c.ask(f"adjoint {tmp_path / 'bars.bin'} {tmp_path / 'ubar.bin'}")
+            assert out[0] == "ok", out
+            ubar = np.fromfile(tmp_path / "ubar.bin").reshape(-1, 4)
+            fd = float(((plus - minus) * b).sum()) / (2 * h)
+            assert abs(float((ubar * d).sum()) - fd) <= bound * abs(fd), (float((ubar * d).sum()), fd)
+            if b is qbars:
+                qbar_u = ubar
+        U0.tofile(tmp_path / "u0.bin")
+        d.tofile(tmp_path / "du0.bin")
+        out = c.ask(f"tangent {tmp_path / 'u0.bin'} {tmp_path / 'du0.bin'} {tmp_path / 'dq.bin'}")
+        assert out[0] == "ok", out
+        dQ = np.fromfile(tmp_path / "dq.bin").reshape(-1, 4)
+        lhs, rhs = float((dQ * bars[:, :4]).sum()), float((qbar_u * d).sum())
+        assert abs(lhs - rhs) <= 1e-10 * abs(rhs)
     finally:
         c.close()
