@@ -138,9 +138,8 @@ LUNA_API luna_status luna_fv_step_adjoint(luna_fv* fv, double dt, double* qbar, 
  * <J dq, qbar> = <dq, J^T qbar>). Q advances as luna_fv_step(fv, dt) advances it. The same restrictions as the adjoint. */
 LUNA_API luna_status luna_fv_step_tangent(luna_fv* fv, double dt, double* dq, int on_device);
 
-/* The order-0 moving step's derivatives at fixed topology (step_moving_tangent / step_moving_adjoint,
- * finite_volume.hpp:2431-2604): the state is (Q, x); a moving mesh, order 0, the per-face loop, the FP64 policy, dt
- * fixed, outside a moving step. The geometry's own derivative in the generators (V, c, A, x_f) belongs to the mesh
+/* The moving step's derivatives at fixed topology (step_moving_tangent / step_moving_adjoint, finite_volume.hpp:
+ * 2431-3155): the state is (Q, x); a moving mesh, the per-face loop, the FP64 policy, dt fixed, outside a moving step. The geometry's own derivative in the generators (V, c, A, x_f) belongs to the mesh
  * library (GeometryDerivative, mesh_derivative.hpp:10-29): the tangent takes its tangents, the adjoint hands back its
  * bars. All arrays host or all device memory (on_device); Q's rows [N][D + 2], x's [N][D], V's [N], c's [N][D], A's and
  * x_f's [F][D].
@@ -148,9 +147,28 @@ LUNA_API luna_status luna_fv_step_tangent(luna_fv* fv, double dt, double* dq, in
  * tangent(dx) of the current mesh. Nothing steps: the caller then runs the step (begin, remesh, end).
  * adjoint: qbar, xbar (of Q, x after the step) become those at its start, but for the geometry's part: Vbar, cbar, Abar,
  * xfbar are written, and the caller adds GeometryDerivative::adjoint(Vbar, cbar, Abar, xfbar) to xbar. Q and the mesh
- * must be the step's start; nothing steps. No atomics: the same bits every run. */
+ * must be the step's start; nothing steps. No atomics: the same bits every run.
+ * Order 1 (the two-pass MUSCL-Hancock step, step_moving_tangent_1 / step_moving_adjoint_1, :2767-3155; the grid steps'
+ * quantisation taken as the identity) needs the mesh of t^n+1 between its passes, so each runs in parts around the
+ * caller's step:
+ *   tangent: luna_fv_step_moving_tangent (the first pass's tangent; dx becomes x^n+1's tangent), the step (begin,
+ *   remesh, end), then luna_fv_step_moving_tangent_end with GeometryDerivative::tangent(dx) of the new mesh (the
+ *   second pass's tangent, into dq).
+ *   adjoint, at the step's start: luna_fv_step_moving_adjoint_begin; the step; luna_fv_step_moving_adjoint_new_mesh
+ *   (qbar, xbar of Q, x after the step: xbar gains the second pass's bars, Abar and xfbar are the new mesh's for the
+ *   caller's GeometryDerivative::adjoint, which the caller adds to xbar); the caller restores Q and the mesh of t^n;
+ *   then luna_fv_step_moving_adjoint as for order 0 (qbar, xbar become those at the step's start, but for the
+ *   geometry's part of t^n, handed back in Vbar, cbar, Abar, xfbar). */
 LUNA_API luna_status luna_fv_step_moving_tangent(luna_fv* fv, double dt, double* dq, double* dx, const double* dV, const double* dc,
                                                  const double* dA, const double* dxf, int on_device);
+/* The reference's steps_fixed argument of the order-1 derivatives: the grid steps of the moving points held (no
+ * derivative through w-hat), as central differences small enough to change no step see it. Off by default. */
+LUNA_API luna_status luna_fv_set_steps_fixed(luna_fv* fv, int held);
+LUNA_API luna_status luna_fv_step_moving_tangent_end(luna_fv* fv, double dt, double* dq, const double* dx, const double* dV, const double* dc,
+                                                     const double* dA, const double* dxf, int on_device);
+LUNA_API luna_status luna_fv_step_moving_adjoint_begin(luna_fv* fv, double dt);
+LUNA_API luna_status luna_fv_step_moving_adjoint_new_mesh(luna_fv* fv, double dt, const double* qbar, double* xbar, double* Abar,
+                                                          double* xfbar, int on_device);
 LUNA_API luna_status luna_fv_step_moving_adjoint(luna_fv* fv, double dt, double* qbar, double* xbar, double* Vbar, double* cbar, double* Abar,
                                                  double* xfbar, int on_device);
 

@@ -137,6 +137,11 @@ struct luna_fv {
     // faces' dG or bar rows, the angle faces' bars, and device copies of the caller's host arrays
     DevArray<double> mv_W, mv_dW, mv_w, mv_dw, mv_face, mv_angle_Abar, mv_angle_dbar, mv_in[6];
     DevArray<int32_t> mv_angle_f;
+    // order 1: the gradients and their tangents, w-hat, c^n and its tangent, the running bars, the fit's entry rows;
+    // stage: 1 a tangent's first pass done (its second pass due after the step), 2 an adjoint begun, 3 its second pass done
+    DevArray<double> mv_g, mv_dg, mv_wh, mv_c0, mv_dc0, mv_Wb, mv_gb, mv_whb, mv_cb, mv_xb, mv_entry;
+    int mv_stage = 0;
+    bool mv_steps_fixed = false;  // the reference's steps_fixed: the grid steps held, no derivative through w-hat
     luna::Counters* host_counters = nullptr;  // pinned
 
     // Per-phase timing: event pairs recorded around each launch, reduced on request.
@@ -1064,8 +1069,8 @@ luna_status copy_out(const double* src, double* dst, size_t count, int on_device
 // The order-0 moving step's derivatives (finite_volume.hpp:2431-2604; kernels in moving_derivative.cuh).
 
 luna_status check_moving_derivative(luna_fv* fv, double dt, const char* what) {
-    if (fv->motion != LUNA_MOVING || fv->order != 0 || fv->update != LUNA_UPDATE_PER_FACE || fv->precision != LUNA_FP64)
-        return set_error(LUNA_EINVAL, std::string("hydro::FiniteVolume::") + what + ": a moving mesh, order 0, the per-face loop, the FP64 policy");
+    if (fv->motion != LUNA_MOVING || fv->update != LUNA_UPDATE_PER_FACE || fv->precision != LUNA_FP64)
+        return set_error(LUNA_EINVAL, std::string("hydro::FiniteVolume::") + what + ": a moving mesh, the per-face loop, the FP64 policy");
     if (fv->moving_pending) return set_error(LUNA_ESTATE, "inside a moving step");
     if (!(dt >= 0)) return set_error(LUNA_EINVAL, "dt must be >= 0");
     return LUNA_OK;
@@ -1118,6 +1123,149 @@ luna_status run_moving_tangent(luna_fv* fv, double dt, double* dq, double* dx, c
     }
     luna::mvd::k_mv_update_tangent<D><<<cb, 128, 0, fv->stream>>>(m, fv->mv_face.ptr, fv->mv_dw.ptr, dt, dq, dx);
     LUNA_CUDA(cudaGetLastError());
+    return LUNA_OK;
+}
+
+template <int D>
+luna_status moving_work1(luna_fv* fv) {
+    constexpr int V = D + 2;
+    const size_t N = static_cast<size_t>(fv->n), F = static_cast<size_t>(fv->f > 0 ? fv->f : 1);
+    LUNA_TRY(fv->mv_g.alloc(N * V * D, "moving gradients"));
+    LUNA_TRY(fv->mv_dg.alloc(N * V * D, "moving gradient tangents"));
+    LUNA_TRY(fv->mv_wh.alloc(N * D, "grid-step velocities"));
+    LUNA_TRY(fv->mv_c0.alloc(N * D, "centroids of t^n"));
+    LUNA_TRY(fv->mv_dc0.alloc(N * D, "centroid tangents of t^n"));
+    LUNA_TRY(fv->mv_Wb.alloc(N * V, "W bars"));
+    LUNA_TRY(fv->mv_gb.alloc(N * V * D, "gradient bars"));
+    LUNA_TRY(fv->mv_whb.alloc(N * D, "grid-step velocity bars"));
+    LUNA_TRY(fv->mv_cb.alloc(N * D, "centroid bars"));
+    LUNA_TRY(fv->mv_xb.alloc(N * D, "position bars"));
+    LUNA_TRY(fv->mv_entry.alloc(2 * F * luna::mvd::entry_width<D>(), "fit entry bars"));
+    return LUNA_OK;
+}
+
+template <int D>
+void launch_mv1_cells(luna_fv* fv, double dt, const double* dW, const double* dx, const double* dc, const double* dA, const double* dxf) {
+    const unsigned int cb = blocks(fv->n, 128);
+    luna::mvd::k_mv1_cells<D><<<cb, 128, 0, fv->stream>>>(fv->mesh_dev<D>(), fv->mv_W.ptr, dW, dx, dc, dA, dxf, fv->x.ptr, fv->mv_w.ptr,
+                                                          fv->limiter == LUNA_LIMITER_FACE_CENTROID, dt, fv->grid_step, fv->per_step, fv->period[0],
+                                                          fv->period[1], fv->period[2], fv->mv_g.ptr, dW ? fv->mv_dg.ptr : nullptr, fv->mv_wh.ptr,
+                                                          fv->mv_c0.ptr, dW ? fv->mv_dc0.ptr : nullptr);
+}
+
+template <int D, bool Second>
+void launch_mv1_pass_tangent(luna_fv* fv, double dt, double* dq, const double* dx, const double* dc, const double* dA, const double* dxf) {
+    const auto m = fv->mesh_dev<D>();
+    const unsigned int cb = blocks(fv->n, 128), fb = blocks(fv->f > 0 ? fv->f : 1, 128);
+    if (fv->f > 0) {
+        if (fv->riemann == LUNA_HLL)
+            luna::mvd::k_mv1_pass_tangent<D, 1, Second><<<fb, 128, 0, fv->stream>>>(m, fv->mv_W.ptr, fv->mv_dW.ptr, fv->mv_g.ptr, fv->mv_dg.ptr,
+                                                                                    fv->mv_wh.ptr, fv->mv_dw.ptr, fv->mv_c0.ptr, fv->mv_dc0.ptr, dx, dc,
+                                                                                    dA, dxf, dt, fv->gas, fv->mv_face.ptr);
+        else
+            luna::mvd::k_mv1_pass_tangent<D, 0, Second><<<fb, 128, 0, fv->stream>>>(m, fv->mv_W.ptr, fv->mv_dW.ptr, fv->mv_g.ptr, fv->mv_dg.ptr,
+                                                                                    fv->mv_wh.ptr, fv->mv_dw.ptr, fv->mv_c0.ptr, fv->mv_dc0.ptr, dx, dc,
+                                                                                    dA, dxf, dt, fv->gas, fv->mv_face.ptr);
+    }
+    luna::mvd::k_mv1_pass_update_tangent<D><<<cb, 128, 0, fv->stream>>>(m, fv->mv_face.ptr, dt, dq);
+}
+
+// Order 1, the first part (step_moving_tangent_1, :2767-2815): the gradients, the point velocities and their tangents, the
+// first pass's tangent, then x^n+1's (dx += dt dw). The second pass's tangent follows the step (run_moving_tangent1_end).
+template <int D>
+luna_status run_moving_tangent1(luna_fv* fv, double dt, double* dq, double* dx, const double* dV, const double* dc, const double* dA,
+                                const double* dxf) {
+    LUNA_TRY(moving_work<D>(fv));
+    LUNA_TRY(moving_work1<D>(fv));
+    const auto m = fv->mesh_dev<D>();
+    const unsigned int cb = blocks(fv->n, 128);
+    luna::mvd::k_mv_prims<D><<<cb, 128, 0, fv->stream>>>(m, fv->q.ptr, dq, dV, fv->gas, fv->mv_W.ptr, fv->mv_dW.ptr);
+    luna::mvd::k_mv_velocity<D><<<cb, 128, 0, fv->stream>>>(m, fv->mv_W.ptr, fv->mv_dW.ptr, dx, dc, dA, fv->mv_w.ptr, fv->mv_dw.ptr,
+                                                            fv->mv_angle_f.ptr);
+    launch_mv1_cells<D>(fv, dt, fv->mv_dW.ptr, dx, dc, dA, dxf);
+    if (fv->mv_steps_fixed) LUNA_CUDA(cudaMemsetAsync(fv->mv_dw.ptr, 0, static_cast<size_t>(fv->n) * D * sizeof(double), fv->stream));
+    launch_mv1_pass_tangent<D, false>(fv, dt, dq, dx, dc, dA, dxf);
+    luna::mvd::k_mv1_drift_tangent<D><<<cb, 128, 0, fv->stream>>>(static_cast<int>(fv->n), fv->mv_dw.ptr, dt, dx);
+    LUNA_CUDA(cudaGetLastError());
+    fv->mv_stage = 1;
+    return LUNA_OK;
+}
+
+template <int D>
+luna_status run_moving_tangent1_end(luna_fv* fv, double dt, double* dq, const double* dx, const double* dc, const double* dA, const double* dxf) {
+    launch_mv1_pass_tangent<D, true>(fv, dt, dq, dx, dc, dA, dxf);
+    LUNA_CUDA(cudaGetLastError());
+    fv->mv_stage = 0;
+    return LUNA_OK;
+}
+
+// Order 1 adjoint (step_moving_adjoint_1, :2987-3155), in three parts around the caller's step and restore: begin at t^n
+// (W, g, w-hat, c^n kept; the bars zeroed), the second pass on the mesh of t^n+1, then the rest on the mesh of t^n.
+template <int D>
+luna_status run_moving_adjoint1_begin(luna_fv* fv, double dt) {
+    constexpr int V = D + 2;
+    LUNA_TRY(moving_work<D>(fv));
+    LUNA_TRY(moving_work1<D>(fv));
+    const auto m = fv->mesh_dev<D>();
+    const unsigned int cb = blocks(fv->n, 128);
+    const size_t N = static_cast<size_t>(fv->n);
+    luna::mvd::k_mv_prims<D><<<cb, 128, 0, fv->stream>>>(m, fv->q.ptr, nullptr, nullptr, fv->gas, fv->mv_W.ptr, nullptr);
+    luna::mvd::k_mv_velocity<D><<<cb, 128, 0, fv->stream>>>(m, fv->mv_W.ptr, nullptr, nullptr, nullptr, nullptr, fv->mv_w.ptr, nullptr,
+                                                            fv->mv_angle_f.ptr);
+    launch_mv1_cells<D>(fv, dt, nullptr, nullptr, nullptr, nullptr, nullptr);
+    LUNA_CUDA(cudaMemsetAsync(fv->mv_Wb.ptr, 0, N * V * sizeof(double), fv->stream));
+    LUNA_CUDA(cudaMemsetAsync(fv->mv_gb.ptr, 0, N * V * D * sizeof(double), fv->stream));
+    LUNA_CUDA(cudaMemsetAsync(fv->mv_whb.ptr, 0, N * D * sizeof(double), fv->stream));
+    LUNA_CUDA(cudaMemsetAsync(fv->mv_cb.ptr, 0, N * D * sizeof(double), fv->stream));
+    LUNA_CUDA(cudaGetLastError());
+    fv->mv_stage = 2;
+    return LUNA_OK;
+}
+
+template <int D, bool Second>
+void launch_mv1_pass_adjoint(luna_fv* fv, double dt, const double* qbar, double* Abar, double* xfbar) {
+    const auto m = fv->mesh_dev<D>();
+    const unsigned int cb = blocks(fv->n, 128), fb = blocks(fv->f > 0 ? fv->f : 1, 128);
+    if (fv->f > 0) {
+        if (fv->riemann == LUNA_HLL)
+            luna::mvd::k_mv1_pass_faces_adjoint<D, 1, Second><<<fb, 128, 0, fv->stream>>>(m, fv->mv_W.ptr, fv->mv_g.ptr, fv->mv_wh.ptr, fv->mv_c0.ptr,
+                                                                                          qbar, dt, fv->gas, fv->mv_face.ptr, Abar, xfbar);
+        else
+            luna::mvd::k_mv1_pass_faces_adjoint<D, 0, Second><<<fb, 128, 0, fv->stream>>>(m, fv->mv_W.ptr, fv->mv_g.ptr, fv->mv_wh.ptr, fv->mv_c0.ptr,
+                                                                                          qbar, dt, fv->gas, fv->mv_face.ptr, Abar, xfbar);
+    }
+    luna::mvd::k_mv1_pass_gather<D, Second><<<cb, 128, 0, fv->stream>>>(m, fv->mv_W.ptr, fv->mv_g.ptr, fv->mv_wh.ptr, fv->mv_c0.ptr, fv->mv_face.ptr,
+                                                                        dt, fv->gas, fv->mv_Wb.ptr, fv->mv_gb.ptr, fv->mv_whb.ptr, fv->mv_cb.ptr,
+                                                                        fv->mv_xb.ptr);
+}
+
+template <int D>
+luna_status run_moving_adjoint1_new_mesh(luna_fv* fv, double dt, const double* qbar, const double* xbar, double* Abar, double* xfbar) {
+    LUNA_CUDA(cudaMemcpyAsync(fv->mv_xb.ptr, xbar, static_cast<size_t>(fv->n) * D * sizeof(double), cudaMemcpyDeviceToDevice, fv->stream));
+    launch_mv1_pass_adjoint<D, true>(fv, dt, qbar, Abar, xfbar);
+    LUNA_CUDA(cudaGetLastError());
+    fv->mv_stage = 3;
+    return LUNA_OK;
+}
+
+template <int D>
+luna_status run_moving_adjoint1_end(luna_fv* fv, double dt, double* qbar, const double* xbar, double* Vbar, double* cbar, double* Abar,
+                                    double* xfbar) {
+    const auto m = fv->mesh_dev<D>();
+    const unsigned int cb = blocks(fv->n, 128), fb = blocks(fv->f > 0 ? fv->f : 1, 128);
+    LUNA_CUDA(cudaMemcpyAsync(fv->mv_xb.ptr, xbar, static_cast<size_t>(fv->n) * D * sizeof(double), cudaMemcpyDeviceToDevice, fv->stream));
+    luna::mvd::k_mv1_drift_adjoint<D><<<cb, 128, 0, fv->stream>>>(static_cast<int>(fv->n), fv->mv_xb.ptr, dt, fv->mv_whb.ptr);
+    launch_mv1_pass_adjoint<D, false>(fv, dt, qbar, Abar, xfbar);
+    luna::mvd::k_mv1_cells_adjoint<D><<<cb, 128, 0, fv->stream>>>(m, fv->mv_W.ptr, fv->mv_gb.ptr, fv->mv_whb.ptr, fv->mv_angle_f.ptr,
+                                                                  fv->limiter == LUNA_LIMITER_FACE_CENTROID, fv->mv_steps_fixed, fv->gas, fv->mv_Wb.ptr,
+                                                                  fv->mv_cb.ptr,
+                                                                  fv->mv_entry.ptr, fv->mv_angle_Abar.ptr, fv->mv_angle_dbar.ptr);
+    luna::mvd::k_mv1_gather_adjoint<D><<<cb, 128, 0, fv->stream>>>(m, fv->q.ptr, fv->mv_Wb.ptr, fv->mv_cb.ptr, fv->mv_entry.ptr, fv->mv_angle_f.ptr,
+                                                                   fv->mv_angle_dbar.ptr, fv->gas, qbar, Vbar, cbar, fv->mv_xb.ptr);
+    if (fv->f > 0)
+        luna::mvd::k_mv1_faces_bar<D><<<fb, 128, 0, fv->stream>>>(m, fv->mv_entry.ptr, fv->mv_angle_f.ptr, fv->mv_angle_Abar.ptr, Abar, xfbar);
+    LUNA_CUDA(cudaGetLastError());
+    fv->mv_stage = 0;
     return LUNA_OK;
 }
 
@@ -1457,6 +1605,7 @@ LUNA_API luna_status luna_fv_step_moving_tangent(luna_fv* fv, double dt, double*
                                                  const double* dA, const double* dxf, int on_device) {
     if (!fv || !dq || !dx) return set_error(LUNA_EINVAL, "null argument");
     LUNA_TRY(check_moving_derivative(fv, dt, "step_moving_tangent"));
+    if (fv->mv_stage != 0) return set_error(LUNA_ESTATE, "step_moving_tangent: another moving derivative is open");
     const int D = fv->dim;
     const size_t N = static_cast<size_t>(fv->n), F = static_cast<size_t>(fv->f), nq = N * (D + 2), nx = N * D;
     const double *gV, *gc, *gA, *gxf, *gq, *gx;
@@ -1468,7 +1617,10 @@ LUNA_API luna_status luna_fv_step_moving_tangent(luna_fv* fv, double dt, double*
     LUNA_TRY(device_view(fv, 5, dxf, F * D, on_device, &gxf));
     double* q_dev = const_cast<double*>(gq);
     double* x_dev = const_cast<double*>(gx);
-    LUNA_TRY(D == 3 ? run_moving_tangent<3>(fv, dt, q_dev, x_dev, gV, gc, gA, gxf) : run_moving_tangent<2>(fv, dt, q_dev, x_dev, gV, gc, gA, gxf));
+    if (fv->order == 1)
+        LUNA_TRY(D == 3 ? run_moving_tangent1<3>(fv, dt, q_dev, x_dev, gV, gc, gA, gxf) : run_moving_tangent1<2>(fv, dt, q_dev, x_dev, gV, gc, gA, gxf));
+    else
+        LUNA_TRY(D == 3 ? run_moving_tangent<3>(fv, dt, q_dev, x_dev, gV, gc, gA, gxf) : run_moving_tangent<2>(fv, dt, q_dev, x_dev, gV, gc, gA, gxf));
     if (!on_device) {
         LUNA_CUDA(cudaMemcpyAsync(dq, q_dev, nq * sizeof(double), cudaMemcpyDeviceToHost, fv->stream));
         LUNA_CUDA(cudaMemcpyAsync(dx, x_dev, nx * sizeof(double), cudaMemcpyDeviceToHost, fv->stream));
@@ -1477,10 +1629,78 @@ LUNA_API luna_status luna_fv_step_moving_tangent(luna_fv* fv, double dt, double*
     return LUNA_OK;
 }
 
+LUNA_API luna_status luna_fv_step_moving_tangent_end(luna_fv* fv, double dt, double* dq, const double* dx, const double* dV, const double* dc,
+                                                     const double* dA, const double* dxf, int on_device) {
+    if (!fv || !dq || !dx) return set_error(LUNA_EINVAL, "null argument");
+    LUNA_TRY(check_moving_derivative(fv, dt, "step_moving_tangent"));
+    if (fv->order != 1 || fv->mv_stage != 1) return set_error(LUNA_ESTATE, "step_moving_tangent_end: after an order-1 step_moving_tangent and the step");
+    const int D = fv->dim;
+    const size_t N = static_cast<size_t>(fv->n), F = static_cast<size_t>(fv->f), nq = N * (D + 2), nx = N * D;
+    const double *gV, *gc, *gA, *gxf, *gq, *gx;
+    LUNA_TRY(device_view(fv, 0, dq, nq, on_device, &gq));
+    LUNA_TRY(device_view(fv, 1, dx, nx, on_device, &gx));
+    LUNA_TRY(device_view(fv, 2, dV, N, on_device, &gV));
+    LUNA_TRY(device_view(fv, 3, dc, nx, on_device, &gc));
+    LUNA_TRY(device_view(fv, 4, dA, F * D, on_device, &gA));
+    LUNA_TRY(device_view(fv, 5, dxf, F * D, on_device, &gxf));
+    double* q_dev = const_cast<double*>(gq);
+    LUNA_TRY(D == 3 ? run_moving_tangent1_end<3>(fv, dt, q_dev, gx, gc, gA, gxf) : run_moving_tangent1_end<2>(fv, dt, q_dev, gx, gc, gA, gxf));
+    if (!on_device) LUNA_CUDA(cudaMemcpyAsync(dq, q_dev, nq * sizeof(double), cudaMemcpyDeviceToHost, fv->stream));
+    LUNA_CUDA(cudaStreamSynchronize(fv->stream));
+    return LUNA_OK;
+}
+
+LUNA_API luna_status luna_fv_set_steps_fixed(luna_fv* fv, int held) {
+    if (!fv) return set_error(LUNA_EINVAL, "null argument");
+    fv->mv_steps_fixed = held != 0;
+    return LUNA_OK;
+}
+
+LUNA_API luna_status luna_fv_step_moving_adjoint_begin(luna_fv* fv, double dt) {
+    if (!fv) return set_error(LUNA_EINVAL, "null argument");
+    LUNA_TRY(check_moving_derivative(fv, dt, "step_moving_adjoint"));
+    if (fv->order != 1) return set_error(LUNA_EINVAL, "step_moving_adjoint_begin: order 1 (order 0 takes luna_fv_step_moving_adjoint alone)");
+    if (fv->mv_stage != 0) return set_error(LUNA_ESTATE, "step_moving_adjoint_begin: another moving derivative is open");
+    LUNA_TRY(fv->dim == 3 ? run_moving_adjoint1_begin<3>(fv, dt) : run_moving_adjoint1_begin<2>(fv, dt));
+    LUNA_CUDA(cudaStreamSynchronize(fv->stream));
+    return LUNA_OK;
+}
+
+LUNA_API luna_status luna_fv_step_moving_adjoint_new_mesh(luna_fv* fv, double dt, const double* qbar, double* xbar, double* Abar, double* xfbar,
+                                                          int on_device) {
+    if (!fv || !qbar || !xbar || !Abar || !xfbar) return set_error(LUNA_EINVAL, "null argument");
+    LUNA_TRY(check_moving_derivative(fv, dt, "step_moving_adjoint"));
+    if (fv->order != 1 || fv->mv_stage != 2) return set_error(LUNA_ESTATE, "step_moving_adjoint_new_mesh: after step_moving_adjoint_begin and the step");
+    const int D = fv->dim;
+    const size_t N = static_cast<size_t>(fv->n), F = static_cast<size_t>(fv->f), nq = N * (D + 2), nx = N * D;
+    const double *gq, *gx;
+    LUNA_TRY(device_view(fv, 0, qbar, nq, on_device, &gq));
+    LUNA_TRY(device_view(fv, 1, xbar, nx, on_device, &gx));
+    double* outs[2] = {Abar, xfbar};
+    double* dev_out[2];
+    for (int k = 0; k < 2; ++k) {
+        if (on_device) {
+            dev_out[k] = outs[k];
+        } else {
+            LUNA_TRY(fv->mv_in[2 + k].alloc(F * D > 0 ? F * D : 1, "moving derivative output"));
+            dev_out[k] = fv->mv_in[2 + k].ptr;
+        }
+    }
+    LUNA_TRY(D == 3 ? run_moving_adjoint1_new_mesh<3>(fv, dt, gq, gx, dev_out[0], dev_out[1]) : run_moving_adjoint1_new_mesh<2>(fv, dt, gq, gx, dev_out[0], dev_out[1]));
+    LUNA_CUDA(cudaMemcpyAsync(xbar, fv->mv_xb.ptr, nx * sizeof(double), on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, fv->stream));
+    if (!on_device)
+        for (int k = 0; k < 2; ++k)
+            if (F) LUNA_CUDA(cudaMemcpyAsync(outs[k], dev_out[k], F * D * sizeof(double), cudaMemcpyDeviceToHost, fv->stream));
+    LUNA_CUDA(cudaStreamSynchronize(fv->stream));
+    return LUNA_OK;
+}
+
 LUNA_API luna_status luna_fv_step_moving_adjoint(luna_fv* fv, double dt, double* qbar, double* xbar, double* Vbar, double* cbar, double* Abar,
                                                  double* xfbar, int on_device) {
     if (!fv || !qbar || !xbar || !Vbar || !cbar || !Abar || !xfbar) return set_error(LUNA_EINVAL, "null argument");
     LUNA_TRY(check_moving_derivative(fv, dt, "step_moving_adjoint"));
+    if (fv->order == 1 && fv->mv_stage != 3) return set_error(LUNA_ESTATE, "step_moving_adjoint (order 1): after begin, the step, new_mesh and the restore");
+    if (fv->order == 0 && fv->mv_stage != 0) return set_error(LUNA_ESTATE, "step_moving_adjoint: another moving derivative is open");
     const int D = fv->dim;
     const size_t N = static_cast<size_t>(fv->n), F = static_cast<size_t>(fv->f), nq = N * (D + 2), nx = N * D;
     const double *gq, *gx;
@@ -1499,8 +1719,14 @@ LUNA_API luna_status luna_fv_step_moving_adjoint(luna_fv* fv, double dt, double*
     }
     double* q_dev = const_cast<double*>(gq);
     double* x_dev = const_cast<double*>(gx);
-    LUNA_TRY(D == 3 ? run_moving_adjoint<3>(fv, dt, q_dev, x_dev, dev_out[0], dev_out[1], dev_out[2], dev_out[3])
-                    : run_moving_adjoint<2>(fv, dt, q_dev, x_dev, dev_out[0], dev_out[1], dev_out[2], dev_out[3]));
+    if (fv->order == 1) {
+        LUNA_TRY(D == 3 ? run_moving_adjoint1_end<3>(fv, dt, q_dev, x_dev, dev_out[0], dev_out[1], dev_out[2], dev_out[3])
+                        : run_moving_adjoint1_end<2>(fv, dt, q_dev, x_dev, dev_out[0], dev_out[1], dev_out[2], dev_out[3]));
+        LUNA_CUDA(cudaMemcpyAsync(x_dev, fv->mv_xb.ptr, nx * sizeof(double), cudaMemcpyDeviceToDevice, fv->stream));
+    } else {
+        LUNA_TRY(D == 3 ? run_moving_adjoint<3>(fv, dt, q_dev, x_dev, dev_out[0], dev_out[1], dev_out[2], dev_out[3])
+                        : run_moving_adjoint<2>(fv, dt, q_dev, x_dev, dev_out[0], dev_out[1], dev_out[2], dev_out[3]));
+    }
     if (!on_device) {
         LUNA_CUDA(cudaMemcpyAsync(qbar, q_dev, nq * sizeof(double), cudaMemcpyDeviceToHost, fv->stream));
         LUNA_CUDA(cudaMemcpyAsync(xbar, x_dev, nx * sizeof(double), cudaMemcpyDeviceToHost, fv->stream));
@@ -1619,6 +1845,8 @@ LUNA_API luna_status luna_fv_device_bytes(luna_fv* fv, int64_t* out) {
     b += fv->fz_xflux.bytes();
     b += fv->mv_W.bytes() + fv->mv_dW.bytes() + fv->mv_w.bytes() + fv->mv_dw.bytes() + fv->mv_face.bytes() + fv->mv_angle_Abar.bytes();
     b += fv->mv_angle_dbar.bytes() + fv->mv_angle_f.bytes();
+    b += fv->mv_g.bytes() + fv->mv_dg.bytes() + fv->mv_wh.bytes() + fv->mv_c0.bytes() + fv->mv_dc0.bytes() + fv->mv_Wb.bytes() + fv->mv_gb.bytes();
+    b += fv->mv_whb.bytes() + fv->mv_cb.bytes() + fv->mv_xb.bytes() + fv->mv_entry.bytes();
     for (const auto& a : fv->mv_in) b += a.bytes();
     *out = static_cast<int64_t>(b);
     return LUNA_OK;

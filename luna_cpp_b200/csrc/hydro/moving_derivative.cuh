@@ -499,5 +499,701 @@ __global__ void k_mv_separation_adjoint(MeshDev<D> m, const double* __restrict__
     for (int a = 0; a < D; ++a) xbar[D * i + a] += sum[a];
 }
 
+// ---- Order 1 (step_moving_tangent_1 / step_moving_adjoint_1, finite_volume.hpp:2626-3155): the MUSCL-Hancock moving
+// step's two passes (W + g r on the mesh of t^n; W a whole step on, to the face of t^n+1) with the limited gradients, the
+// grid-step point velocities w-hat (their quantisation taken as the identity: tangent dw) and the meshes of t^n and t^n+1.
+// The gradients are the reference's direct fit (an area-weighted least squares with intercept, its Cholesky solve and the
+// face-centroid clip in list order, limited_core :1008-1034), here on dual numbers so that it carries the derivative in
+// every input: W of the cell and its neighbours, the separations, the centroids, the areas and the face centroids.
+
+// The direction of the fit's inputs for one dual pass: the caller's tangents, one unit seed, or none.
+template <int D>
+struct FitDirection {
+    static constexpr int V = D + 2, R = V + 1;
+    const double *dW = nullptr, *dx = nullptr, *dc = nullptr, *dA = nullptr, *dxf = nullptr;  // tangents (null: zero)
+    int kind = -1, entry = -1, comp = -1;  // a unit seed: 0 W_i, 1 c_i, 2 W_j, 3 d (x_j - x_i), 4 c_j, 5 A, 6 x_f of an entry
+    __device__ double Wi(int i, int v) const { return kind >= 0 ? (kind == 0 && comp == v ? 1.0 : 0.0) : dW ? dW[R * i + v] : 0.0; }
+    __device__ double ci(int i, int a) const { return kind >= 0 ? (kind == 1 && comp == a ? 1.0 : 0.0) : dc ? dc[D * i + a] : 0.0; }
+    __device__ double Wj(int k, int j, int v) const {
+        return kind >= 0 ? (kind == 2 && entry == k && comp == v ? 1.0 : 0.0) : dW ? dW[R * j + v] : 0.0;
+    }
+    __device__ double d(int k, int i, int j, int a) const {
+        return kind >= 0 ? (kind == 3 && entry == k && comp == a ? 1.0 : 0.0) : dx ? dx[D * j + a] - dx[D * i + a] : 0.0;
+    }
+    __device__ double cj(int k, int j, int a) const { return kind >= 0 ? (kind == 4 && entry == k && comp == a ? 1.0 : 0.0) : dc ? dc[D * j + a] : 0.0; }
+    __device__ double A(int k, int f, int a) const { return kind >= 0 ? (kind == 5 && entry == k && comp == a ? 1.0 : 0.0) : dA ? dA[D * f + a] : 0.0; }
+    __device__ double xf(int k, int f, int a) const {
+        return kind >= 0 ? (kind == 6 && entry == k && comp == a ? 1.0 : 0.0) : dxf ? dxf[D * f + a] : 0.0;
+    }
+};
+
+// Cell i's limited gradient on dual numbers (the adjoint's k_sweep_fit arithmetic: Sweep with the fit, finite_volume.hpp:
+// 486-515, 591-615, the tiny-face rule and the face-centroid clip, :1008-1034). W: rows of V + 1 (W, c_s).
+template <int D>
+__device__ void fit_gradient_t(const MeshDev<D>& m, int i, const double* __restrict__ W, bool limit, const FitDirection<D>& dir,
+                               Dual (&g)[(D + 2) * D]) {
+    constexpr int V = D + 2, U = D + 1, R = V + 1;
+    Dual Wi[V], ci[D];
+#pragma unroll
+    for (int v = 0; v < V; ++v) Wi[v] = Dual(W[R * i + v], dir.Wi(i, v));
+#pragma unroll
+    for (int a = 0; a < D; ++a) ci[a] = Dual(m.cen[D * i + a], dir.ci(i, a));
+    const int first = m.start[i], end = m.start[i + 1];
+    double surface = 0, smallest = __longlong_as_double(0x7ff0000000000000ll);
+    Dual M[U][U], b[V][U], lo[V], hi[V];
+#pragma unroll
+    for (int p = 0; p < U; ++p)
+#pragma unroll
+        for (int s = 0; s < U; ++s) M[p][s] = Dual(0.0);
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        lo[v] = Dual(finite_max<double>());
+        hi[v] = Dual(-finite_max<double>());
+#pragma unroll
+        for (int p = 0; p < U; ++p) b[v][p] = Dual(0.0);
+    }
+    for (int k = first; k < end; ++k) {
+        const int32_t e = m.list[k];
+        const int f = list_face(e), j = e >= 0 ? m.neighbour[f] : m.owner[f], kk = k - first;
+        Dual A[D], d[D], X[U];
+        double sep[D];
+        m.separation(i, j, sep);
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+            A[a] = Dual(m.area[D * f + a], dir.A(kk, f, a));
+            d[a] = Dual(sep[a], dir.d(kk, i, j, a));
+        }
+        const Dual w = sqrt(dot<D>(A, A));
+        surface += w.v;
+        smallest = fmin(smallest, w.v);
+        X[0] = Dual(1.0);
+#pragma unroll
+        for (int p = 1; p < U; ++p) X[p] = d[p - 1] + Dual(m.cen[D * j + p - 1], dir.cj(kk, j, p - 1)) - ci[p - 1];
+#pragma unroll
+        for (int p = 0; p < U; ++p)
+#pragma unroll
+            for (int s = p; s < U; ++s) M[p][s] += w * X[p] * X[s];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const Dual Wj = Dual(W[R * j + v], dir.Wj(kk, j, v));
+            const Dual dW = Wj - Wi[v];
+#pragma unroll
+            for (int p = 0; p < U; ++p) b[v][p] += w * X[p] * dW;
+            if (Wj.v < lo[v].v) lo[v] = Wj;
+            if (Wj.v > hi[v].v) hi[v] = Wj;
+        }
+    }
+    const double tiny = 1e-6 * surface;
+    const bool any_tiny = smallest < tiny;
+    if (any_tiny) {  // the range without the tiny faces' neighbours
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            lo[v] = Dual(finite_max<double>());
+            hi[v] = Dual(-finite_max<double>());
+        }
+        for (int k = first; k < end; ++k) {
+            const int32_t e = m.list[k];
+            const int f = list_face(e), j = e >= 0 ? m.neighbour[f] : m.owner[f], kk = k - first;
+            if (m.mag[f] < tiny) continue;
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                const Dual Wj = Dual(W[R * j + v], dir.Wj(kk, j, v));
+                if (Wj.v < lo[v].v) lo[v] = Wj;
+                if (Wj.v > hi[v].v) hi[v] = Wj;
+            }
+        }
+    }
+    // M is symmetric: the solve reads its upper triangle
+    cholesky_solve<D, Dual>(M, b, g);
+    if (!limit) return;
+    for (int k = first; k < end; ++k) {
+        const int32_t e = m.list[k];
+        const int f = list_face(e), kk = k - first;
+        if (any_tiny && m.mag[f] < tiny) continue;
+        Dual o[D];
+        if (e >= 0) {
+#pragma unroll
+            for (int a = 0; a < D; ++a) o[a] = Dual(m.fcen[D * f + a], dir.xf(kk, f, a)) - ci[a];
+        } else {  // face_offset: the owner j's face centroid moved to i's generator, x_f + (x_j - x_i)
+            const int j = m.owner[f];
+            double sep[D];
+            m.separation(i, j, sep);
+#pragma unroll
+            for (int a = 0; a < D; ++a) o[a] = Dual(m.fcen[D * f + a], dir.xf(kk, f, a)) + Dual(sep[a], dir.d(kk, i, j, a)) - ci[a];
+        }
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            Dual* gv = g + D * v;
+            const Dual dp = dot<D>(gv, o);
+            if (dp.v > 0 && Wi[v].v + dp.v > hi[v].v) {
+                const Dual sc = hi[v].v > Wi[v].v ? (hi[v] - Wi[v]) / dp : Dual(0.0);
+#pragma unroll
+                for (int a = 0; a < D; ++a) gv[a] = gv[a] * sc;
+            } else if (dp.v < 0 && Wi[v].v + dp.v < lo[v].v) {
+                const Dual sc = lo[v].v < Wi[v].v ? (lo[v] - Wi[v]) / dp : Dual(0.0);
+#pragma unroll
+                for (int a = 0; a < D; ++a) gv[a] = gv[a] * sc;
+            }
+        }
+    }
+}
+
+// Per cell: the limited gradient g [N][V D] and (with the tangents) dg; c^n (the centroids the second pass starts from);
+// w-hat, the whole grid steps of x + dt w per dt (k_keep_centroids' rounding), and its tangent dw (0 with the steps held).
+template <int D>
+__global__ void k_mv1_cells(MeshDev<D> m, const double* __restrict__ W, const double* __restrict__ dW, const double* __restrict__ dx,
+                            const double* __restrict__ dc, const double* __restrict__ dA, const double* __restrict__ dxf,
+                            const double* __restrict__ x, const double* __restrict__ w, bool limit, double dt, double step, double per_step,
+                            long long p0, long long p1, long long p2, double* __restrict__ g, double* __restrict__ dg, double* __restrict__ wh,
+                            double* __restrict__ c0, double* __restrict__ dc0) {
+    constexpr int V = D + 2;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.n) return;
+    FitDirection<D> dir;
+    dir.dW = dW, dir.dx = dx, dir.dc = dc, dir.dA = dA, dir.dxf = dxf;
+    Dual gd[V * D];
+    fit_gradient_t<D>(m, i, W, limit, dir, gd);
+#pragma unroll
+    for (int c = 0; c < V * D; ++c) {
+        g[V * D * static_cast<int64_t>(i) + c] = gd[c].v;
+        if (dg) dg[V * D * static_cast<int64_t>(i) + c] = gd[c].d;
+    }
+    const long long period[3] = {p0, p1, p2};
+    const double unit = step / dt;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        const long long p = period[a];
+        long long k0 = llround(x[D * i + a] * per_step);
+        k0 = ((k0 % p) + p) % p;
+        long long k1 = llround((x[D * i + a] + dt * w[D * i + a]) * per_step);
+        k1 = ((k1 % p) + p) % p;
+        long long s = k1 - k0;
+        if (s > p / 2) s -= p;
+        if (s < -(p / 2)) s += p;
+        wh[D * i + a] = static_cast<double>(s) * unit;
+        c0[D * i + a] = m.cen[D * i + a];
+        if (dc0) dc0[D * i + a] = dc ? dc[D * i + a] : 0.0;
+    }
+}
+
+// One side of a pass: W + g r (pass 1), or W a whole step on (the half-step rate at 2 dt) plus g r (pass 2); the cell's W
+// where rho or P would not stay positive (FaceFlux::side_value, :1342-1347).
+template <int D, bool Second, class T>
+__device__ __forceinline__ void pass_side_t(const T* W, const T* g, const T* r, double dt, double gamma, T* Wf, bool& fallback) {
+    constexpr int V = D + 2;
+    if constexpr (Second) {
+        T A[V];
+        half_step_rate<D, T>(W, g, T(gamma), A);
+#pragma unroll
+        for (int v = 0; v < V; ++v) Wf[v] = W[v] - T(0.5 * (2 * dt)) * A[v];
+    } else {
+#pragma unroll
+        for (int v = 0; v < V; ++v) Wf[v] = W[v];
+    }
+#pragma unroll
+    for (int v = 0; v < V; ++v) Wf[v] += dot<D>(g + D * v, r);
+    fallback = !(Wf[0] > T(0) && Wf[D + 1] > T(0));
+    if (fallback)
+#pragma unroll
+        for (int v = 0; v < V; ++v) Wf[v] = W[v];
+}
+
+// The offset r of cell i's side of face f in a pass (pass_offset, :2876-2880): face_offset(f, i) on this mesh; pass 2 from the
+// old centroid to the new face plus dt w-hat. Values only.
+template <int D, bool Second>
+__device__ __forceinline__ void pass_offset(const MeshDev<D>& m, int f, int i, const double* wh, const double* c0, double dt, double* r) {
+    m.face_offset(f, i, r);
+    if constexpr (Second)
+#pragma unroll
+        for (int a = 0; a < D; ++a) r[a] = r[a] + m.cen[D * i + a] - c0[D * i + a] + wh[D * i + a] * (0.5 * (2 * dt));
+}
+
+// One pass's tangent per face (moving_pass_tangent, :2833-2865): both sides' tangents (W, g, the offset through x, c, x_f and
+// pass 2's c^n and w-hat), the face velocity's (w-hat, d, x_f) and the area's, through the flux.
+template <int D, int Riemann, bool Second>
+__global__ void k_mv1_pass_tangent(MeshDev<D> m, const double* __restrict__ W, const double* __restrict__ dW, const double* __restrict__ g,
+                                   const double* __restrict__ dg, const double* __restrict__ wh, const double* __restrict__ dw,
+                                   const double* __restrict__ c0, const double* __restrict__ dc0, const double* __restrict__ dx,
+                                   const double* __restrict__ dc, const double* __restrict__ dA, const double* __restrict__ dxf, double dt,
+                                   GasDev gas, double* __restrict__ dG) {
+    constexpr int V = D + 2, R = V + 1;
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.f) return;
+    const int o = m.owner[f], j = m.neighbour[f];
+    double a[D];
+    load_vec<D>(m.area, f, a);
+    if (dot<D>(a, a) == 0) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) dG[V * static_cast<int64_t>(f) + v] = 0;
+        return;
+    }
+    Dual side[2][V];
+    for (int s = 0; s < 2; ++s) {
+        const int i = s == 0 ? o : j;
+        Dual Wi[V], gi[V * D], r[D];
+#pragma unroll
+        for (int v = 0; v < V; ++v) Wi[v] = Dual(W[R * i + v], dW[R * i + v]);
+#pragma unroll
+        for (int c = 0; c < V * D; ++c) gi[c] = Dual(g[V * D * static_cast<int64_t>(i) + c], dg[V * D * static_cast<int64_t>(i) + c]);
+        double rv[D];
+        pass_offset<D, Second>(m, f, i, wh, c0, dt, rv);
+#pragma unroll
+        for (int q = 0; q < D; ++q) {  // offset_tangent (:2618-2621): dx_f - dc_i (+ dx_o - dx_i off the owner)
+            double dr = dxf[D * f + q] - dc[D * i + q] + (i != o ? dx[D * o + q] - dx[D * i + q] : 0.0);
+            if constexpr (Second) dr += dc[D * i + q] - dc0[D * i + q] + dw[D * i + q] * dt;
+            r[q] = Dual(rv[q], dr);
+        }
+        bool fallback;
+        pass_side_t<D, Second, Dual>(Wi, gi, r, dt, gas.gamma, side[s], fallback);
+    }
+    double sep[D];
+    m.separation(o, j, sep);
+    Dual d[D], xf[D], wL[D], wR[D], A[D], wf[D], G[V];
+#pragma unroll
+    for (int q = 0; q < D; ++q) {
+        d[q] = Dual(sep[q], dx[D * j + q] - dx[D * o + q]);
+        xf[q] = Dual(m.fcen[D * f + q], dxf[D * f + q]);
+        wL[q] = Dual(wh[D * o + q], dw[D * o + q]);
+        wR[q] = Dual(wh[D * j + q], dw[D * j + q]);
+        A[q] = Dual(a[q], dA[D * f + q]);
+    }
+    face_velocity_t<D, Dual>(d, xf, wL, wR, wf);
+    face_flux_t<D, Riemann, Dual>(side[0], side[1], A, wf, gas, G);
+#pragma unroll
+    for (int v = 0; v < V; ++v) dG[V * static_cast<int64_t>(f) + v] = G[v].d;
+}
+
+// dQ_i -= dt / 2 sum_k sign_k dG_k in list order (moving_pass_update_tangent, :2866-2875).
+template <int D>
+__global__ void k_mv1_pass_update_tangent(MeshDev<D> m, const double* __restrict__ dG, double dt, double* __restrict__ dq) {
+    constexpr int V = D + 2;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.n) return;
+    double sum[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) sum[v] = 0;
+    for (int k = m.start[i]; k < m.start[i + 1]; ++k) {
+        const int32_t e = m.list[k];
+        const double sign = e >= 0 ? 1.0 : -1.0;
+        const int64_t f = list_face(e);
+#pragma unroll
+        for (int v = 0; v < V; ++v) sum[v] += sign * dG[V * f + v];
+    }
+#pragma unroll
+    for (int v = 0; v < V; ++v) dq[V * i + v] -= 0.5 * dt * sum[v];
+}
+
+// x^n+1's tangent: dx += dt dw.
+template <int D>
+__global__ void k_mv1_drift_tangent(int n, const double* __restrict__ dw, double dt, double* __restrict__ dx) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+#pragma unroll
+    for (int a = 0; a < D; ++a) dx[D * i + a] += dt * dw[D * i + a];
+}
+
+// A pass's face rows in the adjoint: the two sides' bars, w-hat's two bars, d's bar, the neighbour side's offset bar.
+template <int D>
+__host__ __device__ constexpr int pass_width() {
+    return 2 * (D + 2) + 4 * D;
+}
+
+// One pass's adjoint per face (moving_pass_adjoint, :2882-2929): the flux's local Jacobian columns times G's bar -> the sides',
+// the area's and the face velocity's bars; the face velocity's -> d, x_f, w-hat; the sides' offsets' bars g^T S-bar (where
+// the side did not fall back) into x_f's bar and, for the neighbour's side (whose offset carries x_owner), the row.
+template <int D, int Riemann, bool Second>
+__global__ void k_mv1_pass_faces_adjoint(MeshDev<D> m, const double* __restrict__ W, const double* __restrict__ g, const double* __restrict__ wh,
+                                         const double* __restrict__ c0, const double* __restrict__ qbar, double dt, GasDev gas,
+                                         double* __restrict__ rows, double* __restrict__ Abar, double* __restrict__ xfbar) {
+    constexpr int V = D + 2, R = V + 1, B = pass_width<D>();
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.f) return;
+    double* row = rows + static_cast<int64_t>(B) * f;
+#pragma unroll
+    for (int s = 0; s < B; ++s) row[s] = 0;
+#pragma unroll
+    for (int q = 0; q < D; ++q) Abar[D * f + q] = xfbar[D * f + q] = 0;
+    const int o = m.owner[f], j = m.neighbour[f];
+    double a[D];
+    load_vec<D>(m.area, f, a);
+    if (dot<D>(a, a) == 0) return;
+    double side[2][V], Gbar[V];
+    bool fallback[2];
+    for (int s = 0; s < 2; ++s) {
+        const int i = s == 0 ? o : j;
+        double r[D];
+        pass_offset<D, Second>(m, f, i, wh, c0, dt, r);
+        pass_side_t<D, Second, double>(W + R * i, g + V * D * static_cast<int64_t>(i), r, dt, gas.gamma, side[s], fallback[s]);
+    }
+#pragma unroll
+    for (int v = 0; v < V; ++v) Gbar[v] = -0.5 * dt * (qbar[V * o + v] - qbar[V * j + v]);
+    double sep[D], xfv[D], wLv[D], wRv[D], wf[D];
+    m.separation(o, j, sep);
+    load_vec<D>(m.fcen, f, xfv);
+    load_vec<D>(wh, o, wLv);
+    load_vec<D>(wh, j, wRv);
+    face_velocity_t<D, double>(sep, xfv, wLv, wRv, wf);
+    double Sbar[2][V], wfbar[D];
+#pragma unroll
+    for (int q = 0; q < D; ++q) wfbar[q] = 0;
+    for (int s = 0; s < 2 * V + 2 * D; ++s) {
+        Dual L[V], Rs[V], A[D], wd[D], G[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            L[v] = Dual(side[0][v], s == v ? 1.0 : 0.0);
+            Rs[v] = Dual(side[1][v], s == V + v ? 1.0 : 0.0);
+        }
+#pragma unroll
+        for (int q = 0; q < D; ++q) {
+            A[q] = Dual(a[q], s == 2 * V + q ? 1.0 : 0.0);
+            wd[q] = Dual(wf[q], s == 2 * V + D + q ? 1.0 : 0.0);
+        }
+        face_flux_t<D, Riemann, Dual>(L, Rs, A, wd, gas, G);
+        double bar = 0;
+#pragma unroll
+        for (int v = 0; v < V; ++v) bar += Gbar[v] * G[v].d;
+        if (s < V)
+            Sbar[0][s] = bar;
+        else if (s < 2 * V)
+            Sbar[1][s - V] = bar;
+        else if (s < 2 * V + D)
+            Abar[D * f + (s - 2 * V)] = bar;
+        else
+            wfbar[s - 2 * V - D] = bar;
+    }
+    for (int s = 0; s < 4 * D; ++s) {
+        Dual d[D], xf[D], wL[D], wR[D], out[D];
+#pragma unroll
+        for (int q = 0; q < D; ++q) {
+            d[q] = Dual(sep[q], s == q ? 1.0 : 0.0);
+            xf[q] = Dual(xfv[q], s == D + q ? 1.0 : 0.0);
+            wL[q] = Dual(wLv[q], s == 2 * D + q ? 1.0 : 0.0);
+            wR[q] = Dual(wRv[q], s == 3 * D + q ? 1.0 : 0.0);
+        }
+        face_velocity_t<D, Dual>(d, xf, wL, wR, out);
+        double bar = 0;
+#pragma unroll
+        for (int q = 0; q < D; ++q) bar += wfbar[q] * out[q].d;
+        if (s < D)
+            row[2 * V + 2 * D + s] = bar;  // d
+        else if (s < 2 * D)
+            xfbar[D * f + (s - D)] += bar;
+        else
+            row[2 * V + (s - 2 * D)] = bar;  // w-hat of the owner, then of the neighbour
+    }
+    for (int s = 0; s < 2; ++s) {
+        const int i = s == 0 ? o : j;
+        double rbar[D];
+#pragma unroll
+        for (int q = 0; q < D; ++q) {
+            rbar[q] = 0;
+            if (!fallback[s])
+#pragma unroll
+                for (int v = 0; v < V; ++v) rbar[q] += g[V * D * static_cast<int64_t>(i) + D * v + q] * Sbar[s][v];
+            xfbar[D * f + q] += rbar[q];
+            if (s == 1) row[2 * V + 3 * D + q] = rbar[q];
+        }
+#pragma unroll
+        for (int v = 0; v < V; ++v) row[(s == 0 ? 0 : V) + v] = Sbar[s][v];
+    }
+}
+
+// Each cell's sides of one pass (moving_pass_gather, :2931-2985): the side's adjoint into W's and g's bars (the local
+// Jacobian's columns), its offset's bar into c^n's (and w-hat's on pass 2) and x's, its share of the face velocity's
+// adjoint into w-hat's and x's bars. Added to the running bars.
+template <int D, bool Second>
+__global__ void k_mv1_pass_gather(MeshDev<D> m, const double* __restrict__ W, const double* __restrict__ g, const double* __restrict__ wh,
+                                  const double* __restrict__ c0, const double* __restrict__ rows, double dt, GasDev gas, double* __restrict__ Wb,
+                                  double* __restrict__ gb, double* __restrict__ whb, double* __restrict__ cb, double* __restrict__ xb) {
+    constexpr int V = D + 2, R = V + 1, B = pass_width<D>();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.n) return;
+    double Wv[V], gv[V * D];
+#pragma unroll
+    for (int v = 0; v < V; ++v) Wv[v] = W[R * i + v];
+#pragma unroll
+    for (int c = 0; c < V * D; ++c) gv[c] = g[V * D * static_cast<int64_t>(i) + c];
+    double Wbar[V], gbar[V * D], whbar[D], cbar[D], xbar[D];
+#pragma unroll
+    for (int v = 0; v < V; ++v) Wbar[v] = 0;
+#pragma unroll
+    for (int c = 0; c < V * D; ++c) gbar[c] = 0;
+#pragma unroll
+    for (int q = 0; q < D; ++q) whbar[q] = cbar[q] = xbar[q] = 0;
+    for (int k = m.start[i]; k < m.start[i + 1]; ++k) {
+        const int32_t e = m.list[k];
+        const int f = list_face(e);
+        double a[D];
+        load_vec<D>(m.area, f, a);
+        if (dot<D>(a, a) == 0) continue;
+        const bool owned = e >= 0;
+        const double* row = rows + static_cast<int64_t>(B) * f;
+        double Sbar[V], r[D];
+#pragma unroll
+        for (int v = 0; v < V; ++v) Sbar[v] = row[(owned ? 0 : V) + v];
+        pass_offset<D, Second>(m, f, i, wh, c0, dt, r);
+        bool fallback = false;
+        for (int s = 0; s < V + V * D; ++s) {  // the side's columns in W and g
+            Dual Wd[V], gd[V * D], rd[D], out[V];
+#pragma unroll
+            for (int v = 0; v < V; ++v) Wd[v] = Dual(Wv[v], s == v ? 1.0 : 0.0);
+#pragma unroll
+            for (int c = 0; c < V * D; ++c) gd[c] = Dual(gv[c], s == V + c ? 1.0 : 0.0);
+#pragma unroll
+            for (int q = 0; q < D; ++q) rd[q] = Dual(r[q]);
+            pass_side_t<D, Second, Dual>(Wd, gd, rd, dt, gas.gamma, out, fallback);
+            double bar = 0;
+#pragma unroll
+            for (int v = 0; v < V; ++v) bar += Sbar[v] * out[v].d;
+            if (s < V)
+                Wbar[s] += bar;
+            else
+                gbar[s - V] += bar;
+        }
+        double rbar[D];
+#pragma unroll
+        for (int q = 0; q < D; ++q) {
+            rbar[q] = 0;
+            if (!fallback)
+#pragma unroll
+                for (int v = 0; v < V; ++v) rbar[q] += gv[D * v + q] * Sbar[v];
+            cbar[q] -= rbar[q];
+            if constexpr (Second) whbar[q] += rbar[q] * dt;
+            if (!owned) xbar[q] -= rbar[q];                     // own offset: + x_o - x_i
+            if (owned) xbar[q] += row[2 * V + 3 * D + q];      // the neighbour's offset carries x_i
+            whbar[q] += row[2 * V + (owned ? 0 : D) + q];      // the face velocity's share
+            xbar[q] += owned ? -row[2 * V + 2 * D + q] : row[2 * V + 2 * D + q];  // d = x_j - x_o
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < V; ++v) Wb[V * i + v] += Wbar[v];
+#pragma unroll
+    for (int c = 0; c < V * D; ++c) gb[V * D * static_cast<int64_t>(i) + c] += gbar[c];
+#pragma unroll
+    for (int q = 0; q < D; ++q) {
+        whb[D * i + q] += whbar[q];
+        cb[D * i + q] += cbar[q];
+        xb[D * i + q] += xbar[q];
+    }
+}
+
+// x^n+1 = x^n + dt w-hat: w-hat's bar takes dt x^n+1's; x^n's bar is x^n+1's (moving_drift_adjoint, :3034-3038).
+template <int D>
+__global__ void k_mv1_drift_adjoint(int n, const double* __restrict__ xb, double dt, double* __restrict__ whb) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+#pragma unroll
+    for (int a = 0; a < D; ++a) whb[D * i + a] += dt * xb[D * i + a];
+}
+
+// The fit's entry rows: per list entry, the bars of the neighbour's W, the separation, the neighbour's centroid, the area
+// and the face centroid (V + 4 D).
+template <int D>
+__host__ __device__ constexpr int entry_width() {
+    return (D + 2) + 4 * D;
+}
+
+// Per cell at t^n (moving_cells_adjoint_1, :3068-3105): w-hat's bar through the point velocity (W, c_s, c, the angle face's
+// A and d); c_s's bar into W's; g's bar through the fit: the cell's own W and c bars, and each entry's bars into the entry
+// rows. Wb and cb hold the passes' sums on entry and the cell's own totals on return.
+template <int D>
+__global__ void k_mv1_cells_adjoint(MeshDev<D> m, const double* __restrict__ W, const double* __restrict__ gb, const double* __restrict__ whb,
+                                    const int32_t* __restrict__ angle_f, bool limit, bool steps_fixed, GasDev gas, double* __restrict__ Wb,
+                                    double* __restrict__ cb, double* __restrict__ entry_bar, double* __restrict__ angle_Abar,
+                                    double* __restrict__ angle_dbar) {
+    constexpr int V = D + 2, R = V + 1, E = entry_width<D>();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.n) return;
+    double Wbar[V], cbar[D], wbar[D];
+#pragma unroll
+    for (int v = 0; v < V; ++v) Wbar[v] = Wb[V * i + v];
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        cbar[a] = cb[D * i + a];
+        wbar[a] = steps_fixed ? 0.0 : whb[D * i + a];
+        angle_Abar[D * i + a] = angle_dbar[D * i + a] = 0;
+    }
+    // the point velocity (as the order-0 adjoint's cells)
+    AngleFace<D> af;
+    af.f = angle_f[i];
+    double Wv[V], csv = W[R * i + V], cv[D], Av[D], dv[D];
+#pragma unroll
+    for (int v = 0; v < V; ++v) Wv[v] = W[R * i + v];
+    load_vec<D>(m.cen, i, cv);
+    if (af.f >= 0) {
+        const int32_t o = m.owner[af.f];
+        af.other = o == i ? m.neighbour[af.f] : o;
+        load_vec<D>(m.area, af.f, Av);
+        m.separation(i, af.other, dv);
+        af.amax = face_angle<D>(sqrt(dot<D>(Av, Av))) / (0.5 * sqrt(dot<D>(dv, dv)));
+    } else {
+#pragma unroll
+        for (int a = 0; a < D; ++a) Av[a] = 0, dv[a] = 1;
+    }
+    double csbar = 0;
+    for (int s = 0; s < V + 1 + 3 * D; ++s) {
+        Dual Wd[V], cs, c[D], A[D], d[D], out[D];
+#pragma unroll
+        for (int v = 0; v < V; ++v) Wd[v] = Dual(Wv[v], s == v ? 1.0 : 0.0);
+        cs = Dual(csv, s == V ? 1.0 : 0.0);
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+            c[a] = Dual(cv[a], s == V + 1 + a ? 1.0 : 0.0);
+            A[a] = Dual(Av[a], s == V + 1 + D + a ? 1.0 : 0.0);
+            d[a] = Dual(dv[a], s == V + 1 + 2 * D + a ? 1.0 : 0.0);
+        }
+        point_velocity_t<D, Dual>(af, Wd, cs, c, A, d, out);
+        double bar = 0;
+#pragma unroll
+        for (int a = 0; a < D; ++a) bar += wbar[a] * out[a].d;
+        if (s < V)
+            Wbar[s] += bar;
+        else if (s == V)
+            csbar = bar;
+        else if (s < V + 1 + D)
+            cbar[s - V - 1] += bar;
+        else if (s < V + 1 + 2 * D)
+            angle_Abar[D * i + (s - V - 1 - D)] = bar;
+        else
+            angle_dbar[D * i + (s - V - 1 - 2 * D)] = bar;
+    }
+    for (int s = 0; s < V; ++s) {
+        Dual Wd[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) Wd[v] = Dual(Wv[v], s == v ? 1.0 : 0.0);
+        Wbar[s] += csbar * sound_t<Dual>(Wd, D + 1, gas.gamma).d;
+    }
+    // the fit's columns: the cell's W and c, then every entry's W_j, d, c_j, A, x_f
+    double gbv[V * D];
+#pragma unroll
+    for (int c = 0; c < V * D; ++c) gbv[c] = gb[V * D * static_cast<int64_t>(i) + c];
+    const int first = m.start[i], count = m.start[i + 1] - first;
+    FitDirection<D> dir;
+    for (int s = 0; s < V + D; ++s) {
+        dir.kind = s < V ? 0 : 1;
+        dir.comp = s < V ? s : s - V;
+        Dual gd[V * D];
+        fit_gradient_t<D>(m, i, W, limit, dir, gd);
+        double bar = 0;
+#pragma unroll
+        for (int c = 0; c < V * D; ++c) bar += gbv[c] * gd[c].d;
+        if (s < V)
+            Wbar[s] += bar;
+        else
+            cbar[s - V] += bar;
+    }
+    for (int k = 0; k < count; ++k) {
+        double* row = entry_bar + static_cast<int64_t>(E) * (first + k);
+        for (int s = 0; s < E; ++s) {
+            dir.entry = k;
+            if (s < V) {
+                dir.kind = 2;
+                dir.comp = s;
+            } else {
+                dir.kind = 3 + (s - V) / D;
+                dir.comp = (s - V) % D;
+            }
+            Dual gd[V * D];
+            fit_gradient_t<D>(m, i, W, limit, dir, gd);
+            double bar = 0;
+#pragma unroll
+            for (int c = 0; c < V * D; ++c) bar += gbv[c] * gd[c].d;
+            row[s] = bar;
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < V; ++v) Wb[V * i + v] = Wbar[v];
+#pragma unroll
+    for (int a = 0; a < D; ++a) cb[D * i + a] = cbar[a];
+}
+
+// The list position of face f in cell i's list (entry_of, :2622-2626).
+template <int D>
+__device__ __forceinline__ int entry_of(const MeshDev<D>& m, int i, int f) {
+    for (int k = m.start[i]; k < m.start[i + 1]; ++k)
+        if (list_face(m.list[k]) == f) return k;
+    return -1;
+}
+
+// Per cell at t^n (moving_gather_adjoint_1, :3106-3140): the W bars the neighbours' fits hold for it, then the primitives'
+// adjoint into Q's bar (added) and V's bar (written); c's bar (written) and x's (added) from its own and its neighbours'
+// entries (the separations, the neighbours' centroids, the offsets off the owner) and the angle faces.
+template <int D>
+__global__ void k_mv1_gather_adjoint(MeshDev<D> m, const double* __restrict__ q, const double* __restrict__ Wb, const double* __restrict__ cb,
+                                     const double* __restrict__ entry_bar, const int32_t* __restrict__ angle_f,
+                                     const double* __restrict__ angle_dbar, GasDev gas, double* __restrict__ qbar, double* __restrict__ Vbar,
+                                     double* __restrict__ cbar_out, double* __restrict__ xb) {
+    constexpr int V = D + 2, E = entry_width<D>();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.n) return;
+    double Wbar[V], cbar[D], xsum[D];
+#pragma unroll
+    for (int v = 0; v < V; ++v) Wbar[v] = Wb[V * i + v];
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        cbar[a] = cb[D * i + a];
+        xsum[a] = -angle_dbar[D * i + a];
+    }
+    for (int k = m.start[i]; k < m.start[i + 1]; ++k) {
+        const int32_t e = m.list[k];
+        const int f = list_face(e), j = e >= 0 ? m.neighbour[f] : m.owner[f];
+        const int kj = entry_of<D>(m, j, f);
+        const double* own = entry_bar + static_cast<int64_t>(E) * k;
+        const double* mirror = entry_bar + static_cast<int64_t>(E) * kj;
+#pragma unroll
+        for (int v = 0; v < V; ++v) Wbar[v] += mirror[v];  // j's fit reads W_i
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+            xsum[a] += -own[V + a] + mirror[V + a];  // d = x_j - x_i here, x_i - x_j in j's fit
+            cbar[a] += mirror[V + D + a];           // j's fit reads c_i as its neighbour's centroid
+        }
+        if (angle_f[j] == f)
+#pragma unroll
+            for (int a = 0; a < D; ++a) xsum[a] += angle_dbar[D * j + a];
+    }
+    const double inv = 1.0 / m.vol[i];
+    double Uv[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) Uv[v] = q[V * i + v] * inv;
+    double vb = 0;
+    for (int s = 0; s < V; ++s) {
+        Dual U[V], Wd[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) U[v] = Dual(Uv[v], s == v ? 1.0 : 0.0);
+        primitive_t<D, Dual>(U, gas, Wd);
+        double bar = 0;
+#pragma unroll
+        for (int v = 0; v < V; ++v) bar += Wbar[v] * Wd[v].d;
+        qbar[V * i + s] += bar * inv;
+        vb -= bar * Uv[s] * inv;
+    }
+    Vbar[i] = vb;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        cbar_out[D * i + a] = cbar[a];
+        xb[D * i + a] += xsum[a];
+    }
+}
+
+// Per face at t^n (moving_faces_bar_1, :3141-3153): A's bar from both cells' fit entries and angle faces, x_f's from the fit
+// entries, added to the passes'.
+template <int D>
+__global__ void k_mv1_faces_bar(MeshDev<D> m, const double* __restrict__ entry_bar, const int32_t* __restrict__ angle_f,
+                                const double* __restrict__ angle_Abar, double* __restrict__ Abar, double* __restrict__ xfbar) {
+    constexpr int V = D + 2, E = entry_width<D>();
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.f) return;
+    const int o = m.owner[f], j = m.neighbour[f];
+    const int ko = entry_of<D>(m, o, f), kj = entry_of<D>(m, j, f);
+    const double* ro = entry_bar + static_cast<int64_t>(E) * ko;
+    const double* rj = entry_bar + static_cast<int64_t>(E) * kj;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        Abar[D * f + a] += ro[V + 2 * D + a] + rj[V + 2 * D + a] + (angle_f[o] == f ? angle_Abar[D * o + a] : 0.0) +
+                           (angle_f[j] == f ? angle_Abar[D * j + a] : 0.0);
+        xfbar[D * f + a] += ro[V + 3 * D + a] + rj[V + 3 * D + a];
+    }
+}
+
 }  // namespace mvd
 }  // namespace luna

@@ -81,6 +81,10 @@ SIGNATURES = {
     "luna_fv_fused_pass": ([P, P, P], I),
     "luna_fv_step_moving_tangent": ([P, D64, P, P, P, P, P, P, I], I),
     "luna_fv_step_moving_adjoint": ([P, D64, P, P, P, P, P, P, I], I),
+    "luna_fv_step_moving_tangent_end": ([P, D64, P, P, P, P, P, P, I], I),
+    "luna_fv_step_moving_adjoint_begin": ([P, D64], I),
+    "luna_fv_set_steps_fixed": ([P, I], I),
+    "luna_fv_step_moving_adjoint_new_mesh": ([P, D64, P, P, P, P, I], I),
     "luna_fv_set_timing": ([P, I], I),
     "luna_fv_step_adjoint": ([P, D64, P, I], I),
     "luna_fv_step_tangent": ([P, D64, P, I], I),
@@ -329,28 +333,68 @@ class FiniteVolume:
         check(lib().luna_fv_step_tangent(self._h, dt, a.ctypes.data, 0))
         return a
 
-    def step_moving_tangent(self, dt: float, dq, dx, geometry):
-        """The order-0 moving step's tangent at fixed topology (luna_fv_step_moving_tangent): (dq, dx) of (Q, x) at the
-        step's start -> after it; ``geometry`` is the current mesh's GeometryDerivative (``tangent(dx) -> dV, dc, dA,
-        dxf``, e.g. luna_cpp_b200.geometry_derivative.Geometry2D). Nothing steps. Returns (dq, dx) as new arrays."""
+    def set_steps_fixed(self, held: bool = True) -> None:
+        """The order-1 moving derivatives with the grid steps held (the reference's steps_fixed)."""
+        check(lib().luna_fv_set_steps_fixed(self._h, 1 if held else 0))
+
+    @staticmethod
+    def _geometry_of(geometry):
+        """A GeometryDerivative factory (mesh -> derivative) from a factory or class, or from one derivative object."""
+        if isinstance(geometry, type) or not hasattr(geometry, "tangent"):
+            return geometry
+        return lambda mesh: geometry
+
+    def step_moving_tangent(self, dt: float, dq, dx, geometry, remesh=None):
+        """The moving step's tangent at fixed topology (luna_fv_step_moving_tangent): (dq, dx) of (Q, x) at the step's
+        start -> after it. ``geometry``: a GeometryDerivative (``tangent(dx) -> dV, dc, dA, dxf``) of the current mesh,
+        or a factory of one from a mesh (e.g. luna_cpp_b200.geometry_derivative.Geometry2D). Order 0: nothing steps
+        unless ``remesh`` (positions -> Mesh) is given, then the step follows. Order 1: ``remesh`` is required and the
+        step runs between the two passes' tangents (the reference's step_moving_tangent steps too). Returns (dq, dx)."""
+        make = self._geometry_of(geometry)
         q = np.ascontiguousarray(dq, dtype=np.float64).copy()
         x = np.ascontiguousarray(dx, dtype=np.float64).copy()
-        dV, dc, dA, dxf = (np.ascontiguousarray(a, dtype=np.float64) for a in geometry.tangent(x))
+        dV, dc, dA, dxf = (np.ascontiguousarray(a, dtype=np.float64) for a in make(self.mesh).tangent(x))
         check(lib().luna_fv_step_moving_tangent(self._h, dt, q.ctypes.data, x.ctypes.data, dV.ctypes.data, dc.ctypes.data,
                                                 dA.ctypes.data, dxf.ctypes.data, 0))
+        if self.order == 1:
+            if remesh is None:
+                raise ValueError("the order-1 moving tangent needs remesh: its second pass is on the new mesh")
+            self.step_moving(dt, remesh)
+            dV, dc, dA, dxf = (np.ascontiguousarray(a, dtype=np.float64) for a in make(self.mesh).tangent(x))
+            check(lib().luna_fv_step_moving_tangent_end(self._h, dt, q.ctypes.data, x.ctypes.data, dV.ctypes.data,
+                                                        dc.ctypes.data, dA.ctypes.data, dxf.ctypes.data, 0))
+        elif remesh is not None:
+            self.step_moving(dt, remesh)
         return q, x
 
-    def step_moving_adjoint(self, dt: float, qbar, xbar, geometry):
-        """The order-0 moving step's adjoint (luna_fv_step_moving_adjoint), the geometry's part through ``geometry``'s
-        ``adjoint(Vbar, cbar, Abar, xfbar) -> xbar``: (qbar, xbar) after the step -> at its start. The state and the mesh
-        must be the step's start. Returns (qbar, xbar) as new arrays."""
+    def step_moving_adjoint(self, dt: float, qbar, xbar, geometry, remesh=None):
+        """The moving step's adjoint (luna_fv_step_moving_adjoint), the geometry's part through ``geometry``'s
+        ``adjoint(Vbar, cbar, Abar, xfbar) -> xbar`` (a derivative object or a factory from a mesh): (qbar, xbar) after
+        the step -> at its start. The state and the mesh must be the step's start. Order 1: ``remesh`` is required; the
+        step runs to the new mesh for the second pass and the start is restored after. Returns (qbar, xbar)."""
+        make = self._geometry_of(geometry)
         q = np.ascontiguousarray(qbar, dtype=np.float64).copy()
         x = np.ascontiguousarray(xbar, dtype=np.float64).copy()
-        N, F, D = self.n, int(self.mesh.n_faces), self.dim
+        N, D = self.n, self.dim
+        start_mesh = self.mesh
+        if self.order == 1:
+            if remesh is None:
+                raise ValueError("the order-1 moving adjoint needs remesh: its second pass is on the new mesh")
+            check(lib().luna_fv_step_moving_adjoint_begin(self._h, dt))
+            q_start = self.get_state()
+            self.step_moving(dt, remesh)
+            F2 = int(self.mesh.n_faces)
+            Ab2, xfb2 = np.empty((F2, D)), np.empty((F2, D))
+            check(lib().luna_fv_step_moving_adjoint_new_mesh(self._h, dt, q.ctypes.data, x.ctypes.data, Ab2.ctypes.data,
+                                                             xfb2.ctypes.data, 0))
+            x = x + make(self.mesh).adjoint(np.zeros(N), np.zeros((N, D)), Ab2, xfb2)
+            self.set_mesh(start_mesh)
+            self.set_state(q_start)
+        F = int(start_mesh.n_faces)
         Vb, cb, Ab, xfb = np.empty(N), np.empty((N, D)), np.empty((F, D)), np.empty((F, D))
         check(lib().luna_fv_step_moving_adjoint(self._h, dt, q.ctypes.data, x.ctypes.data, Vb.ctypes.data, cb.ctypes.data,
                                                 Ab.ctypes.data, xfb.ctypes.data, 0))
-        return q, x + geometry.adjoint(Vb, cb, Ab, xfb)
+        return q, x + make(start_mesh).adjoint(Vb, cb, Ab, xfb)
 
     def set_limiter(self, mode: str = "plain", params=None) -> None:
         """The slope limiter of the sweep: "plain" (the reference's), "learned" (the MLP with ``params``, a CUDA float32

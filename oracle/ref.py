@@ -73,8 +73,8 @@ def lib():
         "lr_fv_faces": ([P], I),
         "lr_fv_density_gradients": ([P, P], I),
         "lr_fv_set_positions": ([P, P], I),
-        "lr_fv_step_moving_tangent": ([P, D, P, P, _GEO_TANGENT, _GEO_ADJOINT, P], I),
-        "lr_fv_step_moving_adjoint": ([P, D, P, P, _GEO_TANGENT, _GEO_ADJOINT, P], I),
+        "lr_fv_step_moving_tangent": ([P, D, P, P, _GEO_TANGENT, _GEO_ADJOINT, P, I], I),
+        "lr_fv_step_moving_adjoint": ([P, D, P, P, _GEO_TANGENT, _GEO_ADJOINT, P, I], I),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -209,40 +209,43 @@ class ReferenceFV:
         _check(lib().lr_fv_set_positions(self._h, a.ctypes.data))
 
     def _geometry_callbacks(self, geometry):
-        """The caller's geometry derivative of the current mesh as the driver's two callbacks."""
+        """The caller's geometry derivative as the driver's two callbacks: one derivative object, or a factory (a class
+        or a function of the mesh) evaluated on the mesh as it is at each call (the order-1 derivatives ask before and
+        after their step)."""
         N, D = self.n, self.dim
+        make = geometry if (isinstance(geometry, type) or not hasattr(geometry, "tangent")) else (lambda mesh: geometry)
 
         def view(ptr, shape):
             return np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ctypes.c_double)), shape=shape)
 
         def tangent(user, dx, dV, dc, dA, dxf):
             F = self.mesh.n_faces
-            out = geometry.tangent(view(dx, (N, D)).copy())
+            out = make(self.mesh).tangent(view(dx, (N, D)).copy())
             for arr, ptr, shape in zip(out, (dV, dc, dA, dxf), ((N,), (N, D), (F, D), (F, D))):
                 view(ptr, shape)[...] = arr
 
         def adjoint(user, Vbar, cbar, Abar, xfbar, xbar):
             F = self.mesh.n_faces
-            add = geometry.adjoint(view(Vbar, (N,)).copy(), view(cbar, (N, D)).copy(), view(Abar, (F, D)).copy(),
-                                   view(xfbar, (F, D)).copy())
+            add = make(self.mesh).adjoint(view(Vbar, (N,)).copy(), view(cbar, (N, D)).copy(), view(Abar, (F, D)).copy(),
+                                          view(xfbar, (F, D)).copy())
             view(xbar, (N, D))[...] += add
 
         return _GEO_TANGENT(tangent), _GEO_ADJOINT(adjoint)
 
-    def step_moving_tangent(self, dt, dq, dx, geometry):
+    def step_moving_tangent(self, dt, dq, dx, geometry, steps_fixed=False):
         """step_moving_tangent(dt, dq, dx, geometry) (finite_volume.hpp:2431-2486): (dq, dx) -> after the step, and the
         step itself (the state advances, the mesh moves)."""
         q = np.ascontiguousarray(dq, dtype=np.float64).copy()
         x = np.ascontiguousarray(dx, dtype=np.float64).copy()
         t, a = self._geometry_callbacks(geometry)
-        _check(lib().lr_fv_step_moving_tangent(self._h, dt, q.ctypes.data, x.ctypes.data, t, a, None))
+        _check(lib().lr_fv_step_moving_tangent(self._h, dt, q.ctypes.data, x.ctypes.data, t, a, None, 1 if steps_fixed else 0))
         return q, x
 
-    def step_moving_adjoint(self, dt, qbar, xbar, geometry):
+    def step_moving_adjoint(self, dt, qbar, xbar, geometry, steps_fixed=False):
         """step_moving_adjoint(dt, qbar, xbar, geometry) (:2490-2604): the bars after the step -> at its start; the state
         and the mesh must be the step's start."""
         q = np.ascontiguousarray(qbar, dtype=np.float64).copy()
         x = np.ascontiguousarray(xbar, dtype=np.float64).copy()
         t, a = self._geometry_callbacks(geometry)
-        _check(lib().lr_fv_step_moving_adjoint(self._h, dt, q.ctypes.data, x.ctypes.data, t, a, None))
+        _check(lib().lr_fv_step_moving_adjoint(self._h, dt, q.ctypes.data, x.ctypes.data, t, a, None, 1 if steps_fixed else 0))
         return q, x

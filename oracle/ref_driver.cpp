@@ -37,8 +37,8 @@ struct Solver {
     virtual const double* point_velocities() = 0;
     virtual void density_gradients(double* out) = 0;
     virtual void set_positions(const double* x) = 0;
-    virtual void step_moving_tangent(double dt, double* dq, double* dx, GeoTangent t, GeoAdjoint a, void* user) = 0;
-    virtual void step_moving_adjoint(double dt, double* qbar, double* xbar, GeoTangent t, GeoAdjoint a, void* user) = 0;
+    virtual void step_moving_tangent(double dt, double* dq, double* dx, GeoTangent t, GeoAdjoint a, void* user, bool fixed) = 0;
+    virtual void step_moving_adjoint(double dt, double* qbar, double* xbar, GeoTangent t, GeoAdjoint a, void* user, bool fixed) = 0;
 };
 
 template <class Base>
@@ -114,22 +114,22 @@ struct SolverOf : Solver {
         mesh.update_cells();
         fv.mesh_moved();
     }
-    void step_moving_tangent(double dt, double* dq, double* dx, GeoTangent t, GeoAdjoint a, void* user) override {
+    void step_moving_tangent(double dt, double* dq, double* dx, GeoTangent t, GeoAdjoint a, void* user, bool fixed) override {
         if constexpr (std::is_same_v<typename Precision::flux, double> && std::is_same_v<typename Precision::riemann, double>) {
             typename FV::Cells q(dq, static_cast<std::size_t>(cells()));
             typename FV::Points x(dx, static_cast<std::size_t>(cells()));
             const CallbackGeometry<typename FV::Derivative> geometry(t, a, user);
-            fv.step_moving_tangent(dt, q, x, geometry);
+            fv.step_moving_tangent(dt, q, x, geometry, fixed);
         } else {
             throw std::logic_error("step_moving_tangent: double flux rows and Riemann solve only");
         }
     }
-    void step_moving_adjoint(double dt, double* qbar, double* xbar, GeoTangent t, GeoAdjoint a, void* user) override {
+    void step_moving_adjoint(double dt, double* qbar, double* xbar, GeoTangent t, GeoAdjoint a, void* user, bool fixed) override {
         if constexpr (std::is_same_v<typename Precision::flux, double> && std::is_same_v<typename Precision::riemann, double>) {
             typename FV::Cells q(qbar, static_cast<std::size_t>(cells()));
             typename FV::Points x(xbar, static_cast<std::size_t>(cells()));
             const CallbackGeometry<typename FV::Derivative> geometry(t, a, user);
-            fv.step_moving_adjoint(dt, q, x, geometry);
+            fv.step_moving_adjoint(dt, q, x, geometry, fixed);
         } else {
             throw std::logic_error("step_moving_adjoint: double flux rows and Riemann solve only");
         }
@@ -250,12 +250,13 @@ int lr_fv_density_gradients(void* h, double* out) {
 int lr_fv_set_positions(void* h, const double* x) {
     return guarded([&] { static_cast<Solver*>(h)->set_positions(x); });
 }
-// step_moving_tangent / step_moving_adjoint (finite_volume.hpp:2431-2604) with the caller's geometry derivative.
-int lr_fv_step_moving_tangent(void* h, double dt, double* dq, double* dx, lr::GeoTangent t, lr::GeoAdjoint a, void* user) {
-    return guarded([&] { static_cast<Solver*>(h)->step_moving_tangent(dt, dq, dx, t, a, user); });
+// step_moving_tangent / step_moving_adjoint (finite_volume.hpp:2431-3155) with the caller's geometry derivative; fixed: the
+// order-1 derivatives' steps_fixed (the grid steps held).
+int lr_fv_step_moving_tangent(void* h, double dt, double* dq, double* dx, lr::GeoTangent t, lr::GeoAdjoint a, void* user, int fixed) {
+    return guarded([&] { static_cast<Solver*>(h)->step_moving_tangent(dt, dq, dx, t, a, user, fixed != 0); });
 }
-int lr_fv_step_moving_adjoint(void* h, double dt, double* qbar, double* xbar, lr::GeoTangent t, lr::GeoAdjoint a, void* user) {
-    return guarded([&] { static_cast<Solver*>(h)->step_moving_adjoint(dt, qbar, xbar, t, a, user); });
+int lr_fv_step_moving_adjoint(void* h, double dt, double* qbar, double* xbar, lr::GeoTangent t, lr::GeoAdjoint a, void* user, int fixed) {
+    return guarded([&] { static_cast<Solver*>(h)->step_moving_adjoint(dt, qbar, xbar, t, a, user, fixed != 0); });
 }
 
 }  // extern "C"

@@ -1,5 +1,6 @@
-"""The order-0 moving step's derivatives at fixed topology (luna_fv_step_moving_tangent / luna_fv_step_moving_adjoint,
-the reference's step_moving_tangent / step_moving_adjoint, finite_volume.hpp:2431-2604) on 2D meshes, with the 2D
+"""The moving step's derivatives at fixed topology, orders 0 and 1 (luna_fv_step_moving_tangent[_end] /
+luna_fv_step_moving_adjoint[_begin, _new_mesh], the reference's step_moving_tangent / step_moving_adjoint,
+finite_volume.hpp:2431-3155) on 2D meshes, with the 2D
 geometry derivative of luna_cpp_b200/geometry_derivative.py: the adjoint is the tangent's transpose over several steps
 (the dot test), and the tangent equals central differences of the forward step (the same dt, the host remesh), as the
 reference's derivative tests check theirs (hydro_derivatives_test.cpp:592-716)."""
@@ -30,13 +31,16 @@ def shear_state(mesh, seed=4):
 
 
 class Run:
-    """Order-0 moving steps from (Q, x): the forward through the library with the host remesh; the tangent and the
-    adjoint with the 2D geometry derivative of each step's starting mesh."""
+    """Moving steps from (Q, x): the forward through the library with the host remesh; the tangent and the adjoint with
+    the 2D geometry derivative of each mesh they read (order 1: the step runs inside them, between their passes)."""
 
-    def __init__(self, mesh, riemann="hllc"):
+    def __init__(self, mesh, riemann="hllc", order=0):
         self.box = tuple(mesh.box[:2])
         self.riemann = riemann
-        self.fv = hydro.FiniteVolume(mesh, hydro.Gas(GAMMA), order=0, motion="moving", riemann=riemann)
+        self.fv = hydro.FiniteVolume(mesh, hydro.Gas(GAMMA), order=order, motion="moving", riemann=riemann)
+
+    def remesh(self, p):
+        return build_mesh(p, box=self.box)
 
     def start(self, q, x):
         self.fv.set_mesh(build_mesh(x, box=self.box))
@@ -55,15 +59,14 @@ class Run:
         self.start(q, x)
         for dt in dts:
             self.fv.time_step(0.3)
-            dq, dx = self.fv.step_moving_tangent(dt, dq, dx, Geometry2D(self.fv.mesh))
-            self.fv.step_moving(dt, lambda p: build_mesh(p, box=self.box))
+            dq, dx = self.fv.step_moving_tangent(dt, dq, dx, Geometry2D, self.remesh)  # the step runs inside
         return dq, dx
 
     def adjoint(self, path, qbar, xbar, dts):
         for (q, x), dt in zip(reversed(path), reversed(dts)):
             self.start(q, x)
             self.fv.time_step(0.3)
-            qbar, xbar = self.fv.step_moving_adjoint(dt, qbar, xbar, Geometry2D(self.fv.mesh))
+            qbar, xbar = self.fv.step_moving_adjoint(dt, qbar, xbar, Geometry2D, self.remesh)
         return qbar, xbar
 
 
@@ -72,12 +75,14 @@ def base(n=24, seed=2):
     return mesh, shear_state(mesh)
 
 
+@pytest.mark.parametrize("order", [0, 1])
 @pytest.mark.parametrize("riemann", ["hllc", "hll"])
-def test_moving_dot_test(cuda, riemann):
+def test_moving_dot_test(cuda, riemann, order):
     """<qbar, J dq> + <xbar, J dx> = <J^T qbar, dq> + <J^T xbar, dx> over 3 steps, relative to the sum of the products'
-    magnitudes: 1e-12 (the reference's C1, hydro_derivatives_test.cpp:595)."""
+    magnitudes: 1e-12 (the reference's C1, hydro_derivatives_test.cpp:595); order 0, and order 1 (two passes on the
+    meshes of t^n and t^n+1, the limited fit's derivative in W and in the geometry)."""
     mesh, q0 = base()
-    run = Run(mesh, riemann)
+    run = Run(mesh, riemann, order)
     x0 = mesh.positions.copy()
     run.start(q0, x0)
     dts = [0.5 * run.fv.time_step(0.3)] * 3
@@ -118,9 +123,45 @@ def test_moving_tangent_equals_central_differences(cuda):
     assert np.max(np.abs(Jx - fx)) <= 1e-6 * np.max(np.abs(fx))
 
 
-def test_moving_derivatives_need_order_0(cuda):
+def test_moving_tangent_order_1_equals_central_differences(cuda):
+    """Order 1 with the grid steps held (the reference's steps_fixed), one step along a Q direction of 1e-9 of each entry
+    (dx = 0), as the reference's order-1 check (hydro_derivatives_test.cpp:1598-1655): J dq equals the central difference
+    of the forward within 1e-5 of the largest entry, except next to a point whose grid step changed within +- h (the
+    tangent holds it; there one side matches), at most 8 cells per such point."""
+    mesh, q0 = base(seed=5)
+    run = Run(mesh, order=1)
+    run.fv.set_steps_fixed(True)
+    x0 = mesh.positions.copy()
+    run.start(q0, x0)
+    dts = [0.5 * run.fv.time_step(0.3)]
+    rng = np.random.default_rng(3)
+    dq = rng.normal(size=q0.shape) * np.abs(q0)
+    Jq, Jx = run.tangent(q0, x0, dq, np.zeros_like(x0), dts)
+    assert np.all(Jx == 0)
+    q_end = run.fv.get_state()  # the tangent's own forward
+    h = 1e-9
+    qp, xp, _ = run.forward(q0 + h * dq, x0, dts)
+    qm, xm, _ = run.forward(q0 - h * dq, x0, dts)
+    changed = int(np.sum(np.any(xp != xm, axis=1)))
+    scale = np.max(np.abs(qp - qm)) / (2 * h)
+    central = np.max(np.abs(Jq - (qp - qm) / (2 * h)), axis=1) / scale
+    one_sided = np.minimum(np.max(np.abs(Jq - (qp - q_end) / h), axis=1), np.max(np.abs(Jq - (q_end - qm) / h), axis=1)) / scale
+    off = central > 1e-5
+    assert int(off.sum()) <= 8 * changed, (int(off.sum()), changed)
+    assert np.all(one_sided[off] < 1e-5), float(np.max(one_sided[off]))
+
+
+def test_moving_adjoint_states(cuda):
+    """The last part of the order-1 adjoint refuses to run before its first two; the order-1 tangent needs a remesh."""
     mesh, q0 = base(8)
     fv = hydro.FiniteVolume(mesh, hydro.Gas(GAMMA), order=1, motion="moving")
     fv.set_state(q0)
-    with pytest.raises(hydro.LunaError):
-        fv.step_moving_tangent(1e-3, np.zeros_like(q0), np.zeros((mesh.n_cells, 2)), Geometry2D(mesh))
+    fv.time_step(0.3)
+    with pytest.raises(hydro.LunaError):  # the last part without begin and the new mesh
+        hydro.check(hydro.lib().luna_fv_step_moving_adjoint(fv.handle, 1e-3, np.zeros_like(q0).ctypes.data,
+                                                             np.zeros((mesh.n_cells, 2)).ctypes.data, np.zeros(mesh.n_cells).ctypes.data,
+                                                             np.zeros((mesh.n_cells, 2)).ctypes.data,
+                                                             np.zeros((mesh.n_faces, 2)).ctypes.data,
+                                                             np.zeros((mesh.n_faces, 2)).ctypes.data, 0))
+    with pytest.raises(ValueError):
+        fv.step_moving_tangent(1e-3, np.zeros_like(q0), np.zeros((mesh.n_cells, 2)), Geometry2D)

@@ -167,3 +167,45 @@ def test_moving_derivatives_order_0(reference, riemann):
     want = ref.step_moving_adjoint(dt, qb, xb, Geometry2D(ref.mesh))
     for a, b in zip(got, want):
         assert np.max(np.abs(a - b)) <= 1e-10 * np.max(np.abs(b))
+
+
+@pytest.mark.parametrize("steps_fixed", [False, True])
+@pytest.mark.parametrize("riemann", ["hllc", "hll"])
+def test_moving_derivatives_order_1(reference, riemann, steps_fixed):
+    """The GPU's order-1 moving tangent and adjoint (two passes around the step, the limited fit's derivative in W and in
+    the geometry of both meshes) against the reference's own step_moving_tangent / step_moving_adjoint
+    (finite_volume.hpp:2767-3155), with the grid steps' derivative (dw-hat = dw) and with them held (steps_fixed), on the
+    reference's own wave state (every field non-uniform: a uniform one leaves the limiter's scale to rounding), both with
+    this repository's 2D geometry derivative of each mesh: J (dq, dx) and J^T (qbar, xbar) within 1e-9 of the largest
+    entry."""
+    from conftest import wave_state_2d
+    from luna_cpp_b200.geometry_derivative import Geometry2D
+
+    mesh = jittered_mesh(24, dim=2, jitter=0.3, seed=2)
+    x0 = mesh.positions.copy()
+    q0 = wave_state_2d(mesh)
+    remesh = lambda p: build_mesh(p, box=(1.0, 1.0))  # noqa: E731
+    gpu = hydro.FiniteVolume(mesh, hydro.Gas(5.0 / 3.0), order=1, motion="moving", riemann=riemann)
+    gpu.set_steps_fixed(steps_fixed)
+    ref = R.ReferenceFV(mesh, gamma=5.0 / 3.0, order=1, moving=True, riemann=riemann, remesh=remesh)
+    gpu.set_state(q0)
+    ref.set_state(q0)
+    dt = 0.5 * ref.time_step(0.3)
+    gpu.time_step(0.3)
+    rng = np.random.default_rng(5)
+    dq, dx = rng.normal(size=q0.shape) * np.abs(q0), rng.normal(size=x0.shape) * 1e-3
+    got = gpu.step_moving_tangent(dt, dq, dx, Geometry2D, remesh)
+    want = ref.step_moving_tangent(dt, dq, dx, Geometry2D, steps_fixed=steps_fixed)
+    for a, b in zip(got, want):
+        assert np.max(np.abs(a - b)) <= 1e-9 * np.max(np.abs(b))
+    gpu.set_mesh(mesh)
+    gpu.set_state(q0)
+    gpu.time_step(0.3)
+    ref.set_positions(x0)
+    ref.set_state(q0)
+    ref.time_step(0.3)
+    qb, xb = rng.normal(size=q0.shape), rng.normal(size=x0.shape)
+    got = gpu.step_moving_adjoint(dt, qb, xb, Geometry2D, remesh)
+    want = ref.step_moving_adjoint(dt, qb, xb, Geometry2D, steps_fixed=steps_fixed)
+    for a, b in zip(got, want):
+        assert np.max(np.abs(a - b)) <= 1e-9 * np.max(np.abs(b))
