@@ -21,9 +21,9 @@ The fixed dt is checked against time_step(courant) of every step; the steps wher
 the forward keeps the positions' tape beside the states' and its final rows carry the moved generators and the final
 mesh's volumes; ``cfl`` and ``geometry`` start from the lattice's mesh. ``--order=0|1`` (default 1, as the reference's
 server): the scheme's order. The moving derivatives (rollout.cpp:170-271: step_moving_tangent / step_moving_adjoint,
-the final volumes' bars onto the positions through the geometry derivative) are served for order 0 in 2D, with the 2D
-geometry derivative of luna_cpp_b200.geometry_derivative; for order 1, or in 3D, ``adjoint`` and ``tangent`` answer an
-error line (the order-1 moving derivatives and a 3D geometry derivative are not in the library).
+the final volumes' bars onto the positions through the geometry derivative) are served for orders 0 and 1 in 2D, with
+the 2D geometry derivative of luna_cpp_b200.geometry_derivative; in 3D ``adjoint`` and ``tangent`` answer an error line
+(a 3D geometry derivative is not in the library).
 """
 from __future__ import annotations
 
@@ -116,9 +116,9 @@ class Server:
         return rows
 
     def _moving_derivatives(self, what):
-        if self.order != 0 or self.dim != 2:
-            raise NotImplementedError(f"the moving mesh's {what} is served for order 0 in 2D (the order-1 moving derivatives "
-                                      "and a 3D geometry derivative are not in libluna_b200)")
+        if self.dim != 2:
+            raise NotImplementedError(f"the moving mesh's {what} is served in 2D (a 3D geometry derivative is not in "
+                                      "libluna_b200)")
         from .geometry_derivative import Geometry2D
         from .mesh import build_mesh
 
@@ -149,20 +149,21 @@ class Server:
             self.fv.set_mesh(remesh(x))
             self.fv.set_state(self.tape[s])
             self.fv.time_step(self.courant)  # the point velocities of this state
-            qbar, xbar = self.fv.step_moving_adjoint(self.dt, qbar, xbar, Geometry2D(self.fv.mesh))
+            # order 1: the step runs again to the next mesh for the second pass, and the start is restored
+            qbar, xbar = self.fv.step_moving_adjoint(self.dt, qbar, xbar, Geometry2D, remesh)
         return qbar * self.V0[:, None]
 
     def _moving_tangent(self, U0: np.ndarray, dU0: np.ndarray) -> np.ndarray:
         """Rollout::tangent, moving (rollout.cpp:170-196): the positions' tangent starts at 0; each step's tangent with
-        the geometry derivative of its mesh, then the step (host remesh: the same mesh as the device remesh's)."""
+        the geometry derivative of its mesh (order 1: of both meshes), the step inside it (host remesh: the same mesh as
+        the device remesh's)."""
         Geometry2D, remesh = self._moving_derivatives("tangent")
         self.load(U0)
         dq = np.ascontiguousarray(dU0.reshape(self.n, self.V) * self.V0[:, None])
         dx = np.zeros((self.n, self.dim))
         for _ in range(self.steps):
             self.fv.time_step(self.courant)
-            dq, dx = self.fv.step_moving_tangent(self.dt, dq, dx, Geometry2D(self.fv.mesh))
-            self.fv.step_moving(self.dt, remesh)
+            dq, dx = self.fv.step_moving_tangent(self.dt, dq, dx, Geometry2D, remesh)
         return dq
 
     def tangent(self, U0: np.ndarray, dU0: np.ndarray) -> np.ndarray:
@@ -215,7 +216,6 @@ def serve(argv, stdin=sys.stdin, stdout=sys.stdout) -> int:
                 violations = srv.forward(U0)
                 ms = now_ms(torch) - t0
                 srv.final_rows().tofile(args[1])
-                srv.peak = max(srv.peak, srv.now())
                 answer(f"ok {ms:.17g} {violations}")
             elif cmd == "adjoint":
                 bars = np.fromfile(args[0], dtype=np.float64, count=N * w)
@@ -243,6 +243,7 @@ def serve(argv, stdin=sys.stdin, stdout=sys.stdout) -> int:
                 answer("error unknown command")
         except Exception as e:  # one answer a line, as the reference's server: the client raises on anything but ok
             answer(f"error {type(e).__name__}: {e}".replace("\n", " "))
+        srv.peak = max(srv.peak, srv.now())  # the derivatives' work arrays too
     return 0
 
 

@@ -107,8 +107,7 @@ def test_served_adjoint_matches_central_differences(cuda, tmp_path):
 def test_served_moving_forward(cuda, tmp_path):
     """--moving: a 2D shear layer on the 32^2 lattice, 10 moving steps remeshed on the device. The final rows carry the
     moved generators and the final mesh's volumes (which tile the box), mass and momentum are conserved, a second
-    forward from the same U0 restarts from the lattice's mesh (the same bits), and the derivatives answer an error
-    line (step_moving_adjoint / step_moving_tangent are not in the library)."""
+    forward from the same U0 restarts from the lattice's mesh (the same bits), and zero bars give a zero U0 bar."""
     c = Client(tmp_path, 2, 32, 10, 2e-3, moving=True)
     try:
         xc = (np.arange(32) + 0.5) / 32
@@ -130,7 +129,8 @@ def test_served_moving_forward(cuda, tmp_path):
         assert again.tobytes() == fin.tobytes()
         bars = np.zeros_like(fin)
         bars.tofile(tmp_path / "bars.bin")
-        assert c.ask(f"adjoint {tmp_path / 'bars.bin'} {tmp_path / 'ubar.bin'}")[0] == "error"
+        assert c.ask(f"adjoint {tmp_path / 'bars.bin'} {tmp_path / 'ubar.bin'}")[0] == "ok"
+        assert not np.any(np.fromfile(tmp_path / "ubar.bin"))
         out = c.ask("memory")
         assert out[0] == "ok" and int(out[1]) >= int(out[2]) > 0
     finally:
@@ -183,5 +183,58 @@ def test_served_moving_derivatives_order_0(cuda, tmp_path):
         dQ = np.fromfile(tmp_path / "dq.bin").reshape(-1, 4)
         lhs, rhs = float((dQ * bars[:, :4]).sum()), float((qbar_u * d).sum())
         assert abs(lhs - rhs) <= 1e-10 * abs(rhs)
+    finally:
+        c.close()
+
+
+@pytest.mark.gpu
+def test_served_moving_derivatives_order_1(cuda, tmp_path):
+    """--moving (order 1, the default) in 2D: the served tangent and adjoint (two passes a step, the geometry derivative
+    of both meshes, the grid steps' derivative taken as dw as in the reference's server) are each other's transpose (the
+    dot test, 1e-10), and the adjoint against central differences of the served forward of L = <bars, final rows>. The
+    forward moves the points by whole grid steps (2^-30), which the derivative takes as the identity: the difference
+    (h = 1e-2 along a direction of 1e-2 of U0, moving the points by about 60 grid steps a step) carries the
+    quantisation's error of a few per cent (the reference leaves this check ungated, hydro_derivatives_test.cpp:1693).
+    The precise check of these derivatives is the library's against the reference's own (test_gpu_reference)."""
+    c = Client(tmp_path, 2, 24, 4, 2e-3, moving=True, order=1)
+    try:
+        xc = (np.arange(24) + 0.5) / 24
+        X, Y = np.meshgrid(xc, xc, indexing="ij")
+        noise = np.random.default_rng(8).uniform(-1e-2, 1e-2, (4,) + X.shape)
+        k = 2 * np.pi
+        rho = 1 + 0.2 * np.sin(k * X) + noise[0]
+        vx = 0.3 * np.sin(k * Y) + noise[1]
+        vy = 0.2 * np.cos(k * X) + noise[2]
+        P = 1 + 0.2 * np.cos(k * (X + Y)) + noise[3]
+        U0 = np.stack([rho, rho * vx, rho * vy, P / (2 / 3) + 0.5 * rho * (vx * vx + vy * vy)], -1).reshape(-1, 4)
+        fin, violations = c.forward(U0)
+        assert violations == 0
+        rng = np.random.default_rng(4)
+        bars = rng.standard_normal(fin.shape)
+        bars[:, 4:6] *= 10.0
+        d = rng.standard_normal(U0.shape) * np.abs(U0) * 1e-2
+        h = 1e-2
+        plus, minus = c.forward(U0 + h * d)[0], c.forward(U0 - h * d)[0]
+        c.forward(U0)  # the adjoint's tape is the last forward's
+        bars.tofile(tmp_path / "bars.bin")
+        out = c.ask(f"adjoint {tmp_path / 'bars.bin'} {tmp_path / 'ubar.bin'}")
+        assert out[0] == "ok", out
+        ubar = np.fromfile(tmp_path / "ubar.bin").reshape(-1, 4)
+        fd = float(((plus - minus) * bars).sum()) / (2 * h)
+        print("served order-1 adjoint against central differences:", float((ubar * d).sum()), fd)
+        assert abs(float((ubar * d).sum()) - fd) <= 5e-2 * abs(fd), (float((ubar * d).sum()), fd)
+        U0.tofile(tmp_path / "u0.bin")
+        d.tofile(tmp_path / "du0.bin")
+        out = c.ask(f"tangent {tmp_path / 'u0.bin'} {tmp_path / 'du0.bin'} {tmp_path / 'dq.bin'}")
+        assert out[0] == "ok", out
+        dQ = np.fromfile(tmp_path / "dq.bin").reshape(-1, 4)
+        qbars = bars.copy()
+        qbars[:, 4:] = 0
+        qbars.tofile(tmp_path / "bars.bin")
+        c.forward(U0)
+        out = c.ask(f"adjoint {tmp_path / 'bars.bin'} {tmp_path / 'ubar.bin'}")
+        qbar_u = np.fromfile(tmp_path / "ubar.bin").reshape(-1, 4)
+        lhs, rhs = float((dQ * bars[:, :4]).sum()), float((qbar_u * d).sum())
+        assert abs(lhs - rhs) <= 1e-10 * abs(rhs), (lhs, rhs)
     finally:
         c.close()
