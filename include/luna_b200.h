@@ -259,10 +259,10 @@ LUNA_API luna_status luna_fv_fused_pass(luna_fv* fv, int* fused, int64_t* crossi
 
 /* ---- The 1D solver: hydro::FiniteVolume<1, Exec, Riemann, Precision<>> on a static line (src/hydro/finite_volume_1d.hpp).
  * A batch of `lines` independent lines sharing one geometry: n_cells generators at `positions` (any order) on [0, length],
- * snapped to voronoi-cpp's grid (step = length 2^-30), closed by two walls (LUNA_WALL_*, inflow: the primitives
+ * snapped to the 1D mesh's grid (step = length 2^-52), closed by two walls (LUNA_WALL_*, inflow: the primitives
  * rho, v, P of each inflow wall, [2][3]) or periodic. Q is [lines][n_cells][3] (rho, rho v, E, extensive) in the caller's
  * cell order. limiter: LUNA_LIMITER_FACE_CENTROID (LUNA's MC on a uniform line), NONE, MINMOD, VAN_LEER; riemann:
- * LUNA_HLLC or LUNA_HLL. The moving line (cells supplied by inflow walls) is not covered. */
+ * LUNA_HLLC or LUNA_HLL. The moving line is luna_mline_* below. */
 typedef struct luna_line luna_line;
 /* FiniteVolume(exec, mesh, gas, order, limiter, static_mesh, walls) (finite_volume_1d.hpp:41-56). */
 LUNA_API luna_status luna_line_create(int64_t n_cells, int lines, const double* positions, double length, int periodic, const int* walls,
@@ -286,6 +286,41 @@ LUNA_API luna_status luna_line_step_and_time_step(luna_line* ln, const double* d
  * line needs 5 cells or more (the 5-cell stencil must not wrap onto itself). Synchronises when x is in host memory. */
 LUNA_API luna_status luna_line_step_tangent(luna_line* ln, const double* dt, double* dq, int on_device);
 LUNA_API luna_status luna_line_step_adjoint(luna_line* ln, const double* dt, double* qbar, int on_device);
+
+/* ---- The 1D solver on a moving line: FiniteVolume<1> with Motion::moving (finite_volume_1d.hpp:41-56, the Moving
+ * branches of Kernel::body :552-660, time_step :332-384, supply_cells :421-470, run_fused :679-711). One line of n_cells
+ * generators at `positions` (the caller's cell order) on [0, length], snapped to the grid of step length 2^-52; the points
+ * move with the gas (AREPO-ng's regularisation when `regularise`), each step by whole grid steps, and each face's flux is
+ * the mean of those on the meshes of t^n and t^n+1 (order 1). Walls that do not reflect supply cells on a non-periodic
+ * line (spacing length / n_cells by default; 0 turns it off): a cell inserted next to a wall takes the overlapped share of
+ * its neighbour's Q, and is appended to the cell order (ids n_cells, n_cells + 1, ...). Q [cells][3] and x [cells] are in
+ * cell order; luna_mline_cells gives the current count. The slots re-sort when points cross (the count in stats). */
+typedef struct luna_mline luna_mline;
+LUNA_API luna_status luna_mline_create(int64_t n_cells, const double* positions, double length, int periodic, const int* walls,
+                                       const double* inflow, const luna_gas* gas, int order, int limiter, int riemann, int regularise,
+                                       luna_mline** out);
+LUNA_API luna_status luna_mline_destroy(luna_mline* ml);
+LUNA_API luna_status luna_mline_set_stream(luna_mline* ml, void* stream);
+LUNA_API luna_status luna_mline_cells(luna_mline* ml, int64_t* cells);
+LUNA_API luna_status luna_mline_set_state(luna_mline* ml, const double* q, int on_device);
+LUNA_API luna_status luna_mline_get_state(luna_mline* ml, double* q, int on_device);
+/* The points' positions (FiniteVolume<1>::positions), cell order. */
+LUNA_API luna_status luna_mline_positions(luna_mline* ml, double* x, int on_device);
+/* Per cell (cell order, host): the generator's grid position, the cell's length, its centroid's offset from the generator. */
+LUNA_API luna_status luna_mline_geometry(luna_mline* ml, double* generator, double* volume, double* centroid);
+/* set_inflow_spacing (:61-66). */
+LUNA_API luna_status luna_mline_set_inflow_spacing(luna_mline* ml, double spacing);
+/* supply_cells (:421-470): the cells the walls have room for now; *added (may be null) the count. Synchronises. */
+LUNA_API luna_status luna_mline_supply_cells(luna_mline* ml, int* added);
+/* time_step(courant, rule) (:332-384): rule 0 AREPO's, 1 LUNA's, with the point velocity's |w - v|. Synchronises. */
+LUNA_API luna_status luna_mline_time_step(luna_mline* ml, double courant, int rule, double* dt);
+/* step(dt) (:389-410): the moving step, the slots' order, the walls' cells when due. Synchronises. */
+LUNA_API luna_status luna_mline_step(luna_mline* ml, double dt);
+/* step_and_time_step(dt, courant) (:412-418, :679-711): the step and the next dt of LUNA's rule in one launch (afresh by
+ * time_step when the slots re-sorted or cells were added). Synchronises. */
+LUNA_API luna_status luna_mline_step_and_time_step(luna_mline* ml, double dt, double courant, double* dt_next);
+/* cells_added(), and the mesh's re-sorts and updates (MeshStats). Any pointer may be null. */
+LUNA_API luna_status luna_mline_stats(luna_mline* ml, int64_t* cells_added, int64_t* sorts, int64_t* updates);
 
 #ifdef __cplusplus
 }

@@ -71,6 +71,9 @@ def build_oracle(force=False):
     return target
 
 
+NO_CONTRACTION = {"moving_line.cu"}
+
+
 def build_hydro(force=False, extra=()):
     target = os.path.join(PKG, "libluna_b200.so")
     hydro = os.path.join(CSRC, "hydro")
@@ -96,9 +99,12 @@ def build_hydro(force=False, extra=()):
         for src in cu:
             obj = os.path.join(obj_dir, os.path.splitext(os.path.basename(src))[0] + ".o")
             objs.append(obj)
+            # the moving line's grid steps depend on the last bit of each point velocity: the reference's operation
+            # order, no contraction
+            exact = ["-fmad=false"] if os.path.basename(src) in NO_CONTRACTION else []
             jobs.append([_nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler",
-                         "-fPIC", "-Xcompiler", "-fvisibility=hidden", "-c", "-I", INCLUDE, "-I", hydro, *extra, "-o",
-                         obj, src])
+                         "-fPIC", "-Xcompiler", "-fvisibility=hidden", *exact, "-c", "-I", INCLUDE, "-I", hydro, *extra,
+                         "-o", obj, src])
         with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 1)) as pool:
             for _ in pool.map(_run, jobs):
                 pass

@@ -110,6 +110,20 @@ SIGNATURES = {
     "luna_line_step_and_time_step": ([P, P, D64, P], I),
     "luna_line_step_tangent": ([P, P, P, I], I),
     "luna_line_step_adjoint": ([P, P, P, I], I),
+    "luna_mline_create": ([I64, P, D64, I, P, P, P, I, I, I, I, P], I),
+    "luna_mline_destroy": ([P], I),
+    "luna_mline_set_stream": ([P, P], I),
+    "luna_mline_cells": ([P, P], I),
+    "luna_mline_set_state": ([P, P, I], I),
+    "luna_mline_get_state": ([P, P, I], I),
+    "luna_mline_positions": ([P, P, I], I),
+    "luna_mline_geometry": ([P, P, P, P], I),
+    "luna_mline_set_inflow_spacing": ([P, D64], I),
+    "luna_mline_supply_cells": ([P, P], I),
+    "luna_mline_time_step": ([P, D64, I, P], I),
+    "luna_mline_step": ([P, D64], I),
+    "luna_mline_step_and_time_step": ([P, D64, D64, P], I),
+    "luna_mline_stats": ([P, P, P, P], I),
     "luna_remesh_create": ([I, P, P], I),
     "luna_remesh_destroy": ([P], I),
     "luna_remesh_set_stream": ([P, P], I),

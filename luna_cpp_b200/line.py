@@ -1,6 +1,7 @@
-"""The 1D solver, luna-cpp's ``hydro::FiniteVolume<1>`` on a static line (src/hydro/finite_volume_1d.hpp), through the
-C ABI (``luna_line_*`` in include/luna_b200.h): a batch of independent lines sharing one geometry, all stepped by one
-launch.
+"""The 1D solver, luna-cpp's ``hydro::FiniteVolume<1>`` (src/hydro/finite_volume_1d.hpp), through the C ABI: on a static
+line (``Line``, ``luna_line_*`` in include/luna_b200.h), a batch of independent lines sharing one geometry, all stepped
+by one launch; on a moving line (``MovingLine``, ``luna_mline_*``), one line whose points move with the gas and whose
+open walls supply cells.
 
     ln = Line(positions, length, walls=("outflow", "outflow"), lines=1, gamma=1.4)
     ln.set_state(q)                      # [lines, n, 3] or [n, 3]: rho, rho v, E (extensive), caller's cell order
@@ -8,7 +9,8 @@ launch.
     W = ln.primitives()
 
 Mirrors the reference's interface: time_step(courant, rule) -> dt (per line), step(dt), step_and_time_step(dt, courant),
-step_tangent(dt, dq), step_adjoint(dt, qbar).
+step_tangent(dt, dq), step_adjoint(dt, qbar); the moving line's also positions(), cells(), cells_added(),
+supply_cells(), set_inflow_spacing(spacing).
 No CPU fallback: the library must be built (``python -m luna_cpp_b200.build``) and a GPU present.
 """
 from __future__ import annotations
@@ -94,6 +96,98 @@ class Line:
         x = np.ascontiguousarray(np.broadcast_to(np.asarray(qbar, dtype=np.float64), (self.lines, self.n, 3))).copy()
         check(lib().luna_line_step_adjoint(self._h, d.ctypes.data, x.ctypes.data, 0))
         return x
+
+
+class MovingLine:
+    """FiniteVolume<1> with Motion::moving (finite_volume_1d.hpp:41-56): n points at `positions` (cell order) on
+    [0, length]; the state Q [cells, 3] and the positions in cell order, cells from the walls appended."""
+
+    def __init__(self, positions, length: float, walls=("outflow", "outflow"), periodic=False, inflow=None, gamma: float = 1.4,
+                 order: int = 1, limiter: str = "face_centroid", riemann: str = "hllc", regularise: bool = True):
+        pos = np.ascontiguousarray(positions, dtype=np.float64)
+        self.lines, self.gamma = 1, float(gamma)
+        g = Gas(gamma)
+        self._gas = _Gas(g.gamma, g.smallr, g.smallc)
+        w = np.array([WALLS[walls[0]], WALLS[walls[1]]], dtype=np.int32)
+        inflow_arr = None if inflow is None else np.ascontiguousarray(inflow, dtype=np.float64).reshape(2, 3)
+        self._h = ctypes.c_void_p()
+        check(lib().luna_mline_create(int(pos.shape[0]), pos.ctypes.data, float(length), int(bool(periodic)), w.ctypes.data,
+                                      None if inflow_arr is None else inflow_arr.ctypes.data, ctypes.byref(self._gas), int(order),
+                                      LIMITERS[limiter], 0 if riemann == "hllc" else 1, 1 if regularise else 0, ctypes.byref(self._h)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().luna_mline_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    @property
+    def n(self) -> int:
+        out = ctypes.c_int64()
+        check(lib().luna_mline_cells(self._h, ctypes.byref(out)))
+        return int(out.value)
+
+    def cells(self) -> int:
+        return self.n
+
+    def set_state(self, q) -> None:
+        a = np.ascontiguousarray(q, dtype=np.float64).reshape(self.n, 3)
+        check(lib().luna_mline_set_state(self._h, a.ctypes.data, 0))
+
+    def get_state(self) -> np.ndarray:
+        out = np.empty((self.n, 3))
+        check(lib().luna_mline_get_state(self._h, out.ctypes.data, 0))
+        return out
+
+    def positions(self) -> np.ndarray:
+        out = np.empty(self.n)
+        check(lib().luna_mline_positions(self._h, out.ctypes.data, 0))
+        return out
+
+    def geometry(self):
+        """Per cell: the generator's grid position, the cell's length, its centroid's offset from the generator."""
+        n = self.n
+        g, v, c = np.empty(n), np.empty(n), np.empty(n)
+        check(lib().luna_mline_geometry(self._h, g.ctypes.data, v.ctypes.data, c.ctypes.data))
+        return g, v, c
+
+    def primitives(self) -> np.ndarray:
+        _, volume, _ = self.geometry()
+        U = self.get_state() / volume[:, None]
+        rho = U[:, 0]
+        v = U[:, 1] / rho
+        return np.stack([rho, v, (self.gamma - 1) * (U[:, 2] - 0.5 * rho * v * v)], axis=-1)
+
+    def stats(self) -> dict:
+        a, s, u = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        check(lib().luna_mline_stats(self._h, ctypes.byref(a), ctypes.byref(s), ctypes.byref(u)))
+        return {"cells_added": a.value, "sorts": s.value, "updates": u.value}
+
+    def cells_added(self) -> int:
+        return self.stats()["cells_added"]
+
+    def set_inflow_spacing(self, spacing: float) -> None:
+        check(lib().luna_mline_set_inflow_spacing(self._h, float(spacing)))
+
+    def supply_cells(self) -> int:
+        out = ctypes.c_int()
+        check(lib().luna_mline_supply_cells(self._h, ctypes.byref(out)))
+        return int(out.value)
+
+    def time_step(self, courant: float, rule: str = "arepo") -> np.ndarray:
+        out = ctypes.c_double()
+        check(lib().luna_mline_time_step(self._h, float(courant), RULES[rule], ctypes.byref(out)))
+        return np.array([out.value])
+
+    def step(self, dt) -> None:
+        check(lib().luna_mline_step(self._h, float(np.asarray(dt).reshape(-1)[0])))
+
+    def step_and_time_step(self, dt, courant: float) -> np.ndarray:
+        out = ctypes.c_double()
+        check(lib().luna_mline_step_and_time_step(self._h, float(np.asarray(dt).reshape(-1)[0]), float(courant), ctypes.byref(out)))
+        return np.array([out.value])
 
 
 def run_to(ln: Line, t_end, courant: float = 0.8, rule: str = "luna", fused: bool = False, max_steps: int = 10 ** 7):

@@ -145,8 +145,11 @@ def line_problem(name: str) -> dict:
         return {"L": 1.0, "origin": 0.0, "t_end": t_end, "gamma": 1.4, "walls": outflow,
                 "average": _tube(left, right, 0.5, 1.4)}
     if name == "shu-osher":
+        # moving_walls (:287-298): gas enters supersonically at the left, so on a moving line that wall holds its state
+        left = (3.857143, 2.629369, 10.33333)
         return {"L": 10.0, "origin": -5.0, "t_end": 1.8, "gamma": 1.4, "walls": outflow,
-                "average": _shock_into_wave((3.857143, 2.629369, 10.33333), -4.0, 0.2, 5.0, 1.4)}
+                "average": _shock_into_wave(left, -4.0, 0.2, 5.0, 1.4),
+                "moving_walls": ("inflow", "outflow"), "moving_inflow": (left, (0.0, 0.0, 0.0))}
     if name == "woodward-colella":
         return {"L": 1.0, "origin": 0.0, "t_end": 0.038, "gamma": 1.4, "walls": closed, "average": _woodward_colella}
     raise ValueError(f"unknown 1D problem {name!r}")
@@ -158,20 +161,20 @@ def line_tube(left, right, t_end: float, x0: float = 0.5, gamma: float = 1.4, wa
 
 
 def line_keys(positions, L: float):
-    """The generators of a line of length L on voronoi-cpp's snapping grid (step = L 2^-30, period 2^30 steps): sorted
+    """The generators of a line of length L on the 1D mesh's grid (step = L 2^-52, period 2^52 steps): sorted
     keys, the slot -> position order, the step and the period."""
     x = np.asarray(positions, dtype=np.float64)
-    step = np.ldexp(L, -30)
+    step = np.ldexp(L, -52)
     keys = np.rint(x / step).astype(np.int64)
     order = np.argsort(keys, kind="stable")
-    return keys[order], order, float(step), 1 << 30
+    return keys[order], order, float(step), 1 << 52
 
 
 def line_state(problem: dict, keys, step: float) -> np.ndarray:
     """Q [n, 3] in slot order: each cell's average of the problem over its extent (midway to its neighbours, to a wall at
     the ends), as hydro1d_test.cpp's set() fills it (:40-55)."""
     k = np.asarray(keys, dtype=np.float64)
-    gaps = np.concatenate([[2 * k[0]], np.diff(k), [2 * ((1 << 30) - k[-1])]])
+    gaps = np.concatenate([[2 * k[0]], np.diff(k), [2 * ((1 << 52) - k[-1])]])
     volume = (gaps[:-1] + gaps[1:]) * (0.5 * step)
     centroid = (gaps[1:] - gaps[:-1]) * (0.25 * step)
     x = k * step

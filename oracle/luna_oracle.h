@@ -94,6 +94,25 @@ const double* lo_line_centroids(const lo_line* ln);
 double lo_line_time_step(const lo_line* ln, double courant, int rule /* 0 AREPO's, 1 LUNA's */);
 void lo_line_step(lo_line* ln, double dt);
 
+/* FiniteVolume<1> on a moving line (oracle_mline.c; finite_volume_1d.hpp with Motion::moving): n generators at
+ * `positions` (cell order) on [0, length]; Q [cells][3] and x [cells] in cell order (cells supplied by a wall are
+ * appended); regularise: AREPO-ng's point-velocity regularisation. lo_mline_state / lo_mline_positions point at arrays
+ * that move with each step: fetch them again after one. */
+typedef struct lo_mline lo_mline;
+lo_mline* lo_mline_create(int n, const double* positions, double length, int periodic, const int* walls, const double* inflow,
+                          const lo_gas* gas, int order, int limiter, int riemann, int regularise);
+void lo_mline_destroy(lo_mline* ml);
+int lo_mline_cells(const lo_mline* ml);
+double* lo_mline_state(lo_mline* ml);
+double* lo_mline_positions(lo_mline* ml);
+void lo_mline_geometry(const lo_mline* ml, double* generator, double* volume, double* centroid);
+void lo_mline_stats(const lo_mline* ml, long long* added, long long* sorts, long long* updates);
+void lo_mline_set_inflow_spacing(lo_mline* ml, double spacing);
+int lo_mline_supply_cells(lo_mline* ml);
+double lo_mline_time_step(lo_mline* ml, double courant, int rule /* 0 AREPO's, 1 LUNA's */);
+void lo_mline_step(lo_mline* ml, double dt);
+double lo_mline_step_and_time_step(lo_mline* ml, double dt, double courant);
+
 #ifdef __cplusplus
 }
 #endif

@@ -77,6 +77,21 @@ def lib():
         "lo_line_time_step": ([P, D, I], D),
         "lo_line_step": ([P, D], V),
     }
+    LL = ctypes.c_longlong
+    line_sig.update({
+        "lo_mline_create": ([I, P, D, I, P, P, P, I, I, I, I], P),
+        "lo_mline_destroy": ([P], V),
+        "lo_mline_cells": ([P], I),
+        "lo_mline_state": ([P], P),
+        "lo_mline_positions": ([P], P),
+        "lo_mline_geometry": ([P, P, P, P], V),
+        "lo_mline_stats": ([P, ctypes.POINTER(LL), ctypes.POINTER(LL), ctypes.POINTER(LL)], V),
+        "lo_mline_set_inflow_spacing": ([P, D], V),
+        "lo_mline_supply_cells": ([P], I),
+        "lo_mline_time_step": ([P, D, I], D),
+        "lo_mline_step": ([P, D], V),
+        "lo_mline_step_and_time_step": ([P, D, D], D),
+    })
     for name, (args, res) in line_sig.items():
         fn = getattr(L, name)
         fn.argtypes = args
@@ -272,3 +287,67 @@ class OracleLine:
 
     def step(self, dt):
         lib().lo_line_step(self._h, dt)
+
+
+class OracleMovingLine:
+    """FiniteVolume<1> on a moving line (oracle_mline.c): n generators at `positions` (cell order) on [0, length]; Q and
+    x per cell in cell order, cells supplied by open walls appended."""
+
+    def __init__(self, positions, length, gamma=1.4, walls=("outflow", "outflow"), periodic=False, inflow=None, order=1,
+                 limiter="face_centroid", riemann="hllc", regularise=True):
+        x = np.ascontiguousarray(positions, dtype=np.float64)
+        self._gas = gas(gamma)
+        w = np.array([WALLS[walls[0]], WALLS[walls[1]]], dtype=np.int32)
+        inflow = np.zeros((2, 3)) if inflow is None else np.ascontiguousarray(inflow, dtype=np.float64)
+        self._keep = (w, inflow)
+        self._h = lib().lo_mline_create(len(x), _ptr(x), float(length), int(periodic), _ptr(w), _ptr(inflow),
+                                        ctypes.byref(self._gas), order, LIMITERS[limiter], 0 if riemann == "hllc" else 1,
+                                        1 if regularise else 0)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().lo_mline_destroy(self._h)
+            self._h = None
+
+    @property
+    def n(self):
+        return int(lib().lo_mline_cells(self._h))
+
+    def _view(self, ptr, shape):
+        buf = (ctypes.c_double * int(np.prod(shape))).from_address(ptr)
+        return np.frombuffer(buf, dtype=np.float64).reshape(shape)
+
+    def set_state(self, q):
+        self._view(lib().lo_mline_state(self._h), (self.n, 3))[:] = q
+
+    def get_state(self):
+        return self._view(lib().lo_mline_state(self._h), (self.n, 3)).copy()
+
+    def positions(self):
+        return self._view(lib().lo_mline_positions(self._h), (self.n,)).copy()
+
+    def geometry(self):
+        """Per cell: the generator's grid position, the cell's length, its centroid's offset."""
+        g, v, c = np.empty(self.n), np.empty(self.n), np.empty(self.n)
+        lib().lo_mline_geometry(self._h, _ptr(g), _ptr(v), _ptr(c))
+        return g, v, c
+
+    def stats(self):
+        a, s, u = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        lib().lo_mline_stats(self._h, ctypes.byref(a), ctypes.byref(s), ctypes.byref(u))
+        return {"cells_added": a.value, "sorts": s.value, "updates": u.value}
+
+    def set_inflow_spacing(self, spacing):
+        lib().lo_mline_set_inflow_spacing(self._h, float(spacing))
+
+    def supply_cells(self):
+        return int(lib().lo_mline_supply_cells(self._h))
+
+    def time_step(self, courant, rule="arepo"):
+        return float(lib().lo_mline_time_step(self._h, courant, RULES[rule]))
+
+    def step(self, dt):
+        lib().lo_mline_step(self._h, dt)
+
+    def step_and_time_step(self, dt, courant):
+        return float(lib().lo_mline_step_and_time_step(self._h, dt, courant))
