@@ -2,7 +2,9 @@
 //
 // Layout: the line's slots (its generators sorted along it) hold everything: Q [slots][3], the positions x, the grid
 // keys and each slot's cell id (the caller's cell order, cells from the walls appended); the slots' gaps, volumes and
-// centroid offsets follow from the keys after every step (k_mline_geometry). One thread per slot does what the
+// centroid offsets follow from the keys (the step writes the next ones beside its update; after a re-sort or new cells,
+// k_mline_geometry). A step is one launch and one pinned read of its counters (the next dt, the slots out of order, the
+// error word, the end slots' wishes), as the reference reads its dt and order check. One thread per slot does what the
 // reference's Kernel::body does for a moving line (:552-660): the five-cell stencil, the slopes and point velocities of
 // s - 1, s, s + 1, their new keys (each point moves by whole grid steps), the two faces' fluxes on the meshes of t^n and
 // t^n+1 in the frame of the face's move, the update and the slot's next position and key; the fused variant also reduces
@@ -49,6 +51,9 @@ struct MovingDev {
     const double* __restrict__ x;      // [slots]
     double* __restrict__ x_next;       // [slots]
     int64_t* __restrict__ keys_next;   // [slots]
+    double* __restrict__ gap_next;     // [slots + 1]: the next step's geometry, from the new keys
+    double* __restrict__ volume_next;  // [slots]
+    double* __restrict__ centroid_next;  // [slots]
     double length, spacing;
     int64_t period;
     int regularise, supply[2];
@@ -147,14 +152,29 @@ __device__ __forceinline__ void moving_flux(const LineDev& L, const double* Wl, 
         luna::hllc_flux<1, double>(Wl, Wr, n, wv, L.gas.gamma, L.gas.inverse_gm1, F, true);
 }
 
+// What one launch hands back, in one read: the next dt's bits (the Min reducer), the error word, the slots out of order
+// and the end slots' wishes for a cell. Two of them alternate: each launch zeroes the other for the next one.
+struct Counters {
+    unsigned long long dt_bits, error;
+    int descents, wants;
+};
+__device__ __forceinline__ void reset_spare(Counters* spare) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        spare->dt_bits = 0x7fefffffffffffffull;  // DBL_MAX, the Min reducer's identity
+        spare->error = 0;
+        spare->descents = 0;
+        spare->wants = 0;
+    }
+}
+
 // Kernel::body, moving (:552-660), one thread per slot. Writes the slot's next Q, position and key; counts the slots out of
 // order against their right neighbour; Fused: the next dt of LUNA's rule with the volume of the new keys and |w - v| of
 // t^n (:632-658) into dt_bits, and with `watching` the end slots' wishes for a cell (the line before the step).
 template <int Order, bool Fused>
 __global__ void __launch_bounds__(128) k_mline_step(LineDev L, MovingDev M, const double* __restrict__ q, double* __restrict__ next, double dt,
-                                                    double courant, int watching, unsigned long long* __restrict__ dt_bits,
-                                                    int* __restrict__ counts, unsigned long long* __restrict__ error) {
+                                                    double courant, int watching, Counters* __restrict__ use, Counters* __restrict__ spare) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    reset_spare(spare);
     double smallest = 1.0e300;
     if (s < L.n) {
         Cell1 cell[5];
@@ -210,7 +230,7 @@ __global__ void __launch_bounds__(128) k_mline_step(LineDev L, MovingDev M, cons
             next[3 * s + v] = U[v];
             finite = finite && isfinite(U[v]);
         }
-        if (!finite) atomicOr(error, 2ull);
+        if (!finite) atomicOr(&use->error, 2ull);
         M.x_next[s] = moved(L, M, M.x[s], point[2], dt);
         M.keys_next[s] = key[2];
         const int i = M.cell[s];
@@ -225,10 +245,15 @@ __global__ void __launch_bounds__(128) k_mline_step(LineDev L, MovingDev M, cons
             const int t = slot_at(L, s, 1);
             const int64_t d = key[3] - key[2];
             right = static_cast<double>(d < 0 && L.periodic ? d + M.period : d);
-            if (!before(key[2], i, key[3], M.cell[t])) atomicAdd(counts, 1);
+            if (!before(key[2], i, key[3], M.cell[t])) atomicAdd(&use->descents, 1);
         } else {
             right = static_cast<double>(2 * (M.period - key[2]));
         }
+        // the next step's geometry from the new keys (k_mline_geometry's, as long as the slots stay in order)
+        M.gap_next[s + 1] = right;
+        if (s == 0) M.gap_next[0] = left;
+        M.volume_next[s] = (left + right) * (0.5 * L.step);
+        M.centroid_next[s] = (right - left) * (0.25 * L.step);
         if constexpr (Fused) {
             const double volume = (left + right) * (0.5 * L.step), inv = 1.0 / volume;
             double Un[3], Wn[3];
@@ -237,14 +262,14 @@ __global__ void __launch_bounds__(128) k_mline_step(LineDev L, MovingDev M, cons
             luna::primitive<1>(Un, L.gas, Wn);
             const double relative = fabs(point[2] - cell[2].W[1]);
             smallest = courant * volume / (relative + sound1(L, Wn));
-            if (!(smallest == smallest)) atomicOr(error, 1ull);
+            if (!(smallest == smallest)) atomicOr(&use->error, 1ull);
             if (watching && (s == 0 || s == L.n - 1)) {
                 const int wants = wants_cell(L, M, s);
-                if (wants) atomicAdd(counts + 1, wants);
+                if (wants) atomicAdd(&use->wants, wants);
             }
         }
     }
-    if constexpr (Fused) luna::block_min_to(smallest, dt_bits);
+    if constexpr (Fused) luna::block_min_to(smallest, &use->dt_bits);
 }
 
 // time_step (:332-384), moving: per slot the point velocity's |w - v| (order 1: with the limited density slope) in place
@@ -252,9 +277,9 @@ __global__ void __launch_bounds__(128) k_mline_step(LineDev L, MovingDev M, cons
 // side, (distance + r) / vsig. With `watching`, the end slots' wishes for a cell.
 template <int Order, int Rule>
 __global__ void __launch_bounds__(128) k_mline_time_step(LineDev L, MovingDev M, const double* __restrict__ q, double courant, int watching,
-                                                         unsigned long long* __restrict__ dt_bits, int* __restrict__ counts,
-                                                         unsigned long long* __restrict__ error) {
+                                                         Counters* __restrict__ use, Counters* __restrict__ spare) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    reset_spare(spare);
     double smallest = 1.0e300;
     if (s < L.n) {
         Cell1 cell[5];
@@ -267,7 +292,7 @@ __global__ void __launch_bounds__(128) k_mline_time_step(LineDev L, MovingDev M,
         const double vi = fabs(point_velocity(L, M, cell + 2, gap[1], gap[2], g, volume));
         if (watching && (s == 0 || s == L.n - 1)) {
             const int wants = wants_cell(L, M, s);
-            if (wants) atomicAdd(counts + 1, wants);
+            if (wants) atomicAdd(&use->wants, wants);
         }
         if constexpr (Rule == 1) {
             smallest = courant * volume / (vi + ci);
@@ -288,9 +313,9 @@ __global__ void __launch_bounds__(128) k_mline_time_step(LineDev L, MovingDev M,
             }
             smallest = courant * step;
         }
-        if (!(smallest == smallest)) atomicOr(error, 1ull);
+        if (!(smallest == smallest)) atomicOr(&use->error, 1ull);
     }
-    luna::block_min_to(smallest, dt_bits);
+    luna::block_min_to(smallest, &use->dt_bits);
 }
 
 // Line::gap, volume, centroid from the keys (load_inner :163-176): between neighbours the key difference (a periodic
@@ -427,13 +452,6 @@ __global__ void k_mline_permute(int n, int width, const int* __restrict__ cell, 
     }
 }
 
-__global__ void k_mline_reset(unsigned long long* dt_bits, int* counts) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        *dt_bits = 0x7fefffffffffffffull;  // DBL_MAX, the Min reducer's identity
-        counts[0] = counts[1] = 0;
-    }
-}
-
 template <class T>
 struct DevBuffer {
     T* ptr = nullptr;
@@ -468,6 +486,9 @@ unsigned int blocks_of(int64_t n) { return static_cast<unsigned int>((std::max<i
 }  // namespace
 
 struct luna_mline {
+    ~luna_mline() {
+        if (host_counters) cudaFreeHost(host_counters);
+    }
     LineDev dev{};
     MovingDev mdev{};
     int n = 0, cap = 0, order = 1;
@@ -475,12 +496,14 @@ struct luna_mline {
     int64_t period = int64_t(1) << 52;  // the 1D mesh's grid: 2^52 steps (research_notes/stage1_1d_2026-11-04.md:35)
     cudaStream_t stream = nullptr;
     // slot arrays and their spares (the step's outputs, the sort's and the insertion's targets)
-    DevBuffer<double> q, q2, x, x2, gap, volume, centroid, staging;
+    DevBuffer<double> q, q2, x, x2, gap, volume, centroid, gap2, volume2, centroid2, staging;
     DevBuffer<int64_t> keys, keys2;
     DevBuffer<int> cell, cell2, slot, slot2;
-    DevBuffer<unsigned long long> composite, composite2, bits, error;
+    DevBuffer<unsigned long long> composite, composite2;
     DevBuffer<unsigned int> by_cell, by_cell2;
-    DevBuffer<int> counts;
+    DevBuffer<Counters> counters;  // two, alternating
+    Counters* host_counters = nullptr;  // pinned
+    int epoch = 0;
     DevBuffer<unsigned char> sort_temp;
     DevBuffer<Ends> ends;
     // supply_cells' bookkeeping (:924-1000)
@@ -499,6 +522,9 @@ struct luna_mline {
         mdev.x = x.ptr;
         mdev.x_next = x2.ptr;
         mdev.keys_next = keys2.ptr;
+        mdev.gap_next = gap2.ptr;
+        mdev.volume_next = volume2.ptr;
+        mdev.centroid_next = centroid2.ptr;
         mdev.spacing = spacing;
         mdev.supply[0] = supply[0];
         mdev.supply[1] = supply[1];
@@ -538,6 +564,8 @@ struct luna_mline {
         grow(cell2, 1, "moving line spare cells");
         grow(volume, 1, "moving line volumes");
         grow(centroid, 1, "moving line centroids");
+        grow(volume2, 1, "moving line next volumes");
+        grow(centroid2, 1, "moving line next centroids");
         grow(staging, 3, "moving line staging");
         grow(slot, 1, "moving line sort slots");
         grow(slot2, 1, "moving line sorted slots");
@@ -546,10 +574,12 @@ struct luna_mline {
         grow(by_cell, 1, "moving line sort cells");
         grow(by_cell2, 1, "moving line sorted cells");
         if (st != LUNA_OK) return st;
-        DevBuffer<double> g;
+        DevBuffer<double> g, g2;
         st = g.alloc(static_cast<size_t>(grown) + 1, "moving line gaps");
+        if (st == LUNA_OK) st = g2.alloc(static_cast<size_t>(grown) + 1, "moving line next gaps");
         if (st != LUNA_OK) return st;
         gap.swap(g);
+        gap2.swap(g2);
         cap = grown;
         size_t temp_keys = 0, temp_cells = 0;
         MLINE_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp_keys, composite.ptr, composite2.ptr, slot.ptr, slot2.ptr, cap, 0, 53, stream));
@@ -579,19 +609,19 @@ struct luna_mline {
         bind();
         return LUNA_OK;
     }
-    luna_status read_counts(int* out, double* dt_out) {
-        unsigned long long hb = 0, err = 0;
-        MLINE_CUDA(cudaMemcpyAsync(out, counts.ptr, sizeof(int) * 2, cudaMemcpyDeviceToHost, stream));
-        MLINE_CUDA(cudaMemcpyAsync(&hb, bits.ptr, sizeof(hb), cudaMemcpyDeviceToHost, stream));
-        MLINE_CUDA(cudaMemcpyAsync(&err, error.ptr, sizeof(err), cudaMemcpyDeviceToHost, stream));
+    // The launch's counters (one pinned read); the next launch uses the other pair.
+    luna_status read_counters(Counters* out, double* dt_out) {
+        MLINE_CUDA(cudaMemcpyAsync(host_counters, counters.ptr + epoch, sizeof(Counters), cudaMemcpyDeviceToHost, stream));
         MLINE_CUDA(cudaStreamSynchronize(stream));
-        if (err) {
-            MLINE_CUDA(cudaMemsetAsync(error.ptr, 0, sizeof(unsigned long long), stream));
-            return mfail(LUNA_ENONFINITE, err & 1ull ? "the moving line's time step is not finite" : "the moving line's state is not finite after the update");
-        }
-        if (dt_out) std::memcpy(dt_out, &hb, sizeof(double));
+        *out = *host_counters;
+        epoch ^= 1;
+        if (out->error)
+            return mfail(LUNA_ENONFINITE, out->error & 1ull ? "the moving line's time step is not finite" : "the moving line's state is not finite after the update");
+        if (dt_out) std::memcpy(dt_out, &out->dt_bits, sizeof(double));
         return LUNA_OK;
     }
+    Counters* use() { return counters.ptr + epoch; }
+    Counters* spare() { return counters.ptr + (epoch ^ 1); }
     // due() (:957-964).
     bool due() {
         if (!supply[0] && !supply[1]) return false;
@@ -602,18 +632,17 @@ struct luna_mline {
     }
     luna_status time_step(double courant, int rule, double* dt) {
         bind();
-        k_mline_reset<<<1, 1, 0, stream>>>(bits.ptr, counts.ptr);
         const int w = watching ? 1 : 0;
         if (order == 1)
-            (rule == 1 ? k_mline_time_step<1, 1> : k_mline_time_step<1, 0>)<<<blocks_of(n), 128, 0, stream>>>(dev, mdev, q.ptr, courant, w, bits.ptr, counts.ptr, error.ptr);
+            (rule == 1 ? k_mline_time_step<1, 1> : k_mline_time_step<1, 0>)<<<blocks_of(n), 128, 0, stream>>>(dev, mdev, q.ptr, courant, w, use(), spare());
         else
-            (rule == 1 ? k_mline_time_step<0, 1> : k_mline_time_step<0, 0>)<<<blocks_of(n), 128, 0, stream>>>(dev, mdev, q.ptr, courant, w, bits.ptr, counts.ptr, error.ptr);
+            (rule == 1 ? k_mline_time_step<0, 1> : k_mline_time_step<0, 0>)<<<blocks_of(n), 128, 0, stream>>>(dev, mdev, q.ptr, courant, w, use(), spare());
         MLINE_CUDA(cudaGetLastError());
-        int c[2];
-        const luna_status st = read_counts(c, dt);
+        Counters c;
+        const luna_status st = read_counters(&c, dt);
         if (st != LUNA_OK) return st;
         if (watching) {
-            wants = c[1];
+            wants = c.wants;
             looked = true;
         }
         return LUNA_OK;
@@ -681,35 +710,34 @@ struct luna_mline {
     luna_status advance(double dt, double courant, bool fused, double* smallest, bool* again) {
         if (!(dt > 0) || !std::isfinite(dt)) return mfail(LUNA_EINVAL, "dt must be finite and > 0");
         bind();
-        k_mline_reset<<<1, 1, 0, stream>>>(bits.ptr, counts.ptr);
         const int w = fused && watching ? 1 : 0;
         const dim3 grid(blocks_of(n));
         if (order == 1)
-            (fused ? k_mline_step<1, true> : k_mline_step<1, false>)<<<grid, 128, 0, stream>>>(dev, mdev, q.ptr, q2.ptr, dt, courant, w, bits.ptr,
-                                                                                              counts.ptr, error.ptr);
+            (fused ? k_mline_step<1, true> : k_mline_step<1, false>)<<<grid, 128, 0, stream>>>(dev, mdev, q.ptr, q2.ptr, dt, courant, w, use(), spare());
         else
-            (fused ? k_mline_step<0, true> : k_mline_step<0, false>)<<<grid, 128, 0, stream>>>(dev, mdev, q.ptr, q2.ptr, dt, courant, w, bits.ptr,
-                                                                                              counts.ptr, error.ptr);
+            (fused ? k_mline_step<0, true> : k_mline_step<0, false>)<<<grid, 128, 0, stream>>>(dev, mdev, q.ptr, q2.ptr, dt, courant, w, use(), spare());
         MLINE_CUDA(cudaGetLastError());
-        int c[2];
-        luna_status st = read_counts(c, smallest);
+        Counters c;
+        luna_status st = read_counters(&c, smallest);
         if (st != LUNA_OK) return st;
         q.swap(q2);
         x.swap(x2);
         keys.swap(keys2);
+        gap.swap(gap2);
+        volume.swap(volume2);
+        centroid.swap(centroid2);
         updates += 1;
         *again = false;
-        if (c[0] != (dev.periodic ? 1 : 0)) {
+        bind();
+        if (c.descents != (dev.periodic ? 1 : 0)) {
             st = sort();
+            if (st == LUNA_OK) st = geometry();
             if (st != LUNA_OK) return st;
             sorts += 1;
             *again = true;
         }
-        bind();
-        st = geometry();
-        if (st != LUNA_OK) return st;
         if (fused) {
-            wants = c[1];
+            wants = c.wants;
             looked = watching;
         }
         return LUNA_OK;
@@ -768,9 +796,12 @@ LUNA_API luna_status luna_mline_create(int64_t n_cells, const double* positions,
     }
     luna_status st = LUNA_OK;
     ml->n = 0;  // nothing to keep in reserve()
-    if (st == LUNA_OK) st = ml->bits.alloc(1, "moving line dt bits");
-    if (st == LUNA_OK) st = ml->error.alloc(1, "moving line error word");
-    if (st == LUNA_OK) st = ml->counts.alloc(2, "moving line counts");
+    if (st == LUNA_OK) st = ml->counters.alloc(2, "moving line counters");
+    if (st == LUNA_OK && cudaMallocHost(&ml->host_counters, sizeof(Counters)) != cudaSuccess) {
+        cudaGetLastError();
+        ml->host_counters = nullptr;
+        st = mfail(LUNA_ENOMEM, "luna_mline_create: pinned counters");
+    }
     if (st == LUNA_OK) st = ml->ends.alloc(1, "moving line ends");
     if (st == LUNA_OK) st = ml->reserve(static_cast<int>(n_cells));
     if (st != LUNA_OK) {
@@ -782,7 +813,11 @@ LUNA_API luna_status luna_mline_create(int64_t n_cells, const double* positions,
     if (e == cudaSuccess) e = cudaMemcpy(ml->cell.ptr, cells.data(), sizeof(int) * n_cells, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(ml->x.ptr, sx.data(), sizeof(double) * n_cells, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(ml->q.ptr, 0, sizeof(double) * 3 * n_cells);
-    if (e == cudaSuccess) e = cudaMemset(ml->error.ptr, 0, sizeof(unsigned long long));
+    if (e == cudaSuccess) {
+        Counters fresh[2];
+        for (Counters& f : fresh) f = Counters{0x7fefffffffffffffull, 0, 0, 0};
+        e = cudaMemcpy(ml->counters.ptr, fresh, sizeof(fresh), cudaMemcpyHostToDevice);
+    }
     if (e != cudaSuccess) {
         delete ml;
         return mfail(LUNA_ECUDA, std::string("luna_mline_create: ") + cudaGetErrorString(e));

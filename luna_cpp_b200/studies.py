@@ -557,9 +557,56 @@ def kernels(case="adjoint", nx=64, repeat=3, log=print) -> dict:
     return out
 
 
+def moving_line(nx=131072, steps=2000, courant=0.4, log=print) -> dict:
+    """The moving 1D line on Shu-Osher (the left wall holding the entering state and supplying cells, the reference's
+    moving pass table, research_notes/inflow_2026-11-06.md:51-64): `steps` steps from t = 0 at nx cells, timed by CUDA
+    events over the whole loop (each step reads its dt or its order check back, as the reference's driver does): time_step
+    (AREPO's rule) + step, and step_and_time_step (LUNA's rule, one launch a step). Cell updates: the cells of each step,
+    summed."""
+    import torch
+
+    from .line import MovingLine
+    from .problems import line_problem
+
+    pr = line_problem("shu-osher")
+    L, o = pr["L"], pr["origin"]
+    x = L * (np.arange(nx) + 0.5) / nx
+    out = {"config": {"problem": "shu-osher", "cells": nx, "steps": steps, "walls": "inflow (holding the state), outflow",
+                      "courant": courant}}
+    for path in ("time_step+step", "step_and_time_step"):
+        ml = MovingLine(x, L, walls=pr["moving_walls"], inflow=np.array(pr["moving_inflow"]), gamma=pr["gamma"])
+        g, V, c = ml.geometry()
+        a, b = g + c - 0.5 * V, g + c + 0.5 * V
+        ml.set_state(pr["average"](a + o, b + o) * (b - a)[:, None])
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        updates = 0
+        torch.cuda.synchronize()
+        start.record()
+        if path == "time_step+step":
+            for _ in range(steps):
+                updates += ml.n
+                ml.step(ml.time_step(courant, "arepo"))
+        else:
+            dt = ml.time_step(courant, "luna")
+            for _ in range(steps):
+                updates += ml.n
+                dt = ml.step_and_time_step(dt, courant)
+        end.record()
+        torch.cuda.synchronize()
+        ms = start.elapsed_time(end)
+        out[path] = {"device_ms_per_step": ms / steps, "cell_updates_per_s": updates / (ms * 1e-3), "cells_at_end": ml.n,
+                     "cells_added": ml.cells_added(), "sorts": ml.stats()["sorts"],
+                     "finite": bool(np.all(np.isfinite(ml.get_state())))}
+        log(f"{path}: {ms / steps * 1e3:.1f} us/step, {out[path]['cell_updates_per_s'] / 1e9:.2f} G cell-updates/s, "
+            f"{ml.n} cells")
+        ml.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("study", choices=["precision", "adjoint", "moving", "learned", "learned_moving", "lines", "kernels"])
+    ap.add_argument("study", choices=["precision", "adjoint", "moving", "learned", "learned_moving", "lines", "moving_line",
+                                      "kernels"])
     ap.add_argument("--case", default="adjoint", help="kernels: adjoint, tangent, mlp, line, tiles or moving")
     ap.add_argument("--nx", type=int)
     ap.add_argument("--steps", type=int)
@@ -581,7 +628,7 @@ def main():
         kw.pop("steps", None)
     if args.study == "learned_moving":
         kw.pop("threads", None)
-    if args.study == "lines":
+    if args.study in ("lines", "moving_line"):
         kw.pop("threads", None)
     if args.study == "kernels":
         kw.pop("threads", None)
@@ -589,7 +636,7 @@ def main():
         if args.steps:
             kw["repeat"] = kw.pop("steps")
     res = {"precision": precision, "adjoint": adjoint, "moving": moving, "learned": learned_blast,
-           "learned_moving": learned_moving, "lines": lines, "kernels": kernels}[args.study](**kw)
+           "learned_moving": learned_moving, "lines": lines, "moving_line": moving_line, "kernels": kernels}[args.study](**kw)
     text = json.dumps(res, indent=1)
     if args.out:
         with open(args.out, "w") as f:
