@@ -996,6 +996,278 @@ __host__ __device__ constexpr int entry_width() {
 // Per cell at t^n (moving_cells_adjoint_1, :3068-3105): w-hat's bar through the point velocity (W, c_s, c, the angle face's
 // A and d); c_s's bar into W's; g's bar through the fit: the cell's own W and c bars, and each entry's bars into the entry
 // rows. Wb and cb hold the passes' sums on entry and the cell's own totals on return.
+// The transpose of fit_gradient_t's Jacobian in reverse mode, for the bars gbar of cell i's limited gradient: the
+// forward fit again (M, b, the range and its entries, the clips in list order), then the last clip's scale
+// s = (bound - W_i) / (g0 . o) backwards onto g0, the bound's entry and the offset; M x = b once more for b's bars
+// (bbar = M^-1 xbar, M symmetric) and M's (-bbar x^T); and each entry's share through w = |A| and X = (1, d + c_j - c_i)
+// (the reference's moving_gradient_adjoint, finite_volume.hpp:2690-2760). Adds into Wibar, cibar; writes each entry's
+// row of entry_width: W_j, d, c_j, A, x_f.
+template <int D>
+__device__ void fit_gradient_adjoint(const MeshDev<D>& m, int i, const double* __restrict__ W, bool limit, const double* gbar,
+                                     double (&Wibar)[D + 2], double (&cibar)[D], double* __restrict__ rows) {
+    constexpr int V = D + 2, U = D + 1, R = V + 1, E = entry_width<D>();
+    double Wi[V], ci[D];
+#pragma unroll
+    for (int v = 0; v < V; ++v) Wi[v] = W[R * i + v];
+#pragma unroll
+    for (int a = 0; a < D; ++a) ci[a] = m.cen[D * i + a];
+    const int first = m.start[i], end = m.start[i + 1];
+    double surface = 0, smallest = __longlong_as_double(0x7ff0000000000000ll);
+    double M[U][U], b[V][U], lo[V], hi[V];
+    int lo_k[V], hi_k[V];
+#pragma unroll
+    for (int p = 0; p < U; ++p)
+#pragma unroll
+        for (int q = 0; q < U; ++q) M[p][q] = 0.0;
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        lo[v] = finite_max<double>();
+        hi[v] = -finite_max<double>();
+        lo_k[v] = hi_k[v] = -1;
+#pragma unroll
+        for (int p = 0; p < U; ++p) b[v][p] = 0.0;
+    }
+    // the entry k's face, neighbour, area vector, |A|, X and W_j
+    const auto entry = [&](int k, int& f, int& j, bool& owned, double (&A)[D], double& w, double (&X)[U]) {
+        const int32_t e = m.list[k];
+        f = list_face(e);
+        owned = e >= 0;
+        j = owned ? m.neighbour[f] : m.owner[f];
+        double sep[D];
+        m.separation(i, j, sep);
+#pragma unroll
+        for (int a = 0; a < D; ++a) A[a] = m.area[D * f + a];
+        w = sqrt(dot<D>(A, A));
+        X[0] = 1.0;
+#pragma unroll
+        for (int p = 1; p < U; ++p) X[p] = sep[p - 1] + m.cen[D * j + p - 1] - ci[p - 1];
+    };
+    for (int k = first; k < end; ++k) {
+        int f, j;
+        bool owned;
+        double A[D], w, X[U];
+        entry(k, f, j, owned, A, w, X);
+        surface += w;
+        smallest = fmin(smallest, w);
+#pragma unroll
+        for (int p = 0; p < U; ++p)
+#pragma unroll
+            for (int q = p; q < U; ++q) M[p][q] += w * X[p] * X[q];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const double Wj = W[R * j + v], dW = Wj - Wi[v];
+#pragma unroll
+            for (int p = 0; p < U; ++p) b[v][p] += w * X[p] * dW;
+            if (Wj < lo[v]) lo[v] = Wj, lo_k[v] = k - first;
+            if (Wj > hi[v]) hi[v] = Wj, hi_k[v] = k - first;
+        }
+    }
+    const double tiny = 1e-6 * surface;
+    const bool any_tiny = smallest < tiny;
+    if (any_tiny) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            lo[v] = finite_max<double>();
+            hi[v] = -finite_max<double>();
+            lo_k[v] = hi_k[v] = -1;
+        }
+        for (int k = first; k < end; ++k) {
+            const int32_t e = m.list[k];
+            const int f = list_face(e), j = e >= 0 ? m.neighbour[f] : m.owner[f];
+            if (m.mag[f] < tiny) continue;
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                const double Wj = W[R * j + v];
+                if (Wj < lo[v]) lo[v] = Wj, lo_k[v] = k - first;
+                if (Wj > hi[v]) hi[v] = Wj, hi_k[v] = k - first;
+            }
+        }
+    }
+    // Cholesky of M (its upper triangle) and the fit of every variable, as cholesky_solve
+    double L[U][U];
+#pragma unroll
+    for (int p = 0; p < U; ++p)
+#pragma unroll
+        for (int q = 0; q < U; ++q) L[p][q] = 0.0;
+#pragma unroll
+    for (int p = 0; p < U; ++p)
+#pragma unroll
+        for (int q = 0; q <= p; ++q) {
+            double sum = M[q][p];
+#pragma unroll
+            for (int k = 0; k < q; ++k) sum -= L[p][k] * L[q][k];
+            L[p][q] = p == q ? sqrt(sum) : sum / L[q][q];
+        }
+    const auto solve = [&](const double (&r)[U], double (&x)[U]) {
+        double z[U];
+#pragma unroll
+        for (int p = 0; p < U; ++p) {
+            double sum = r[p];
+#pragma unroll
+            for (int k = 0; k < p; ++k) sum -= L[p][k] * z[k];
+            z[p] = sum / L[p][p];
+        }
+#pragma unroll
+        for (int p = U - 1; p >= 0; --p) {
+            double sum = z[p];
+#pragma unroll
+            for (int k = p + 1; k < U; ++k) sum -= L[k][p] * x[k];
+            x[p] = sum / L[p][p];
+        }
+    };
+    double xs[V][U], g[V][D];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        solve(b[v], xs[v]);
+#pragma unroll
+        for (int a = 0; a < D; ++a) g[v][a] = xs[v][1 + a];
+    }
+    // the clips in list order: each variable's last one (entry, which bound, to zero or not, its face offset)
+    int last[V];
+    bool upper[V], zero[V], last_owned[V];
+    double offset[V][D];
+#pragma unroll
+    for (int v = 0; v < V; ++v) last[v] = -1, upper[v] = zero[v] = false, last_owned[v] = true;
+    if (limit)
+        for (int k = first; k < end; ++k) {
+            const int32_t e = m.list[k];
+            const int f = list_face(e);
+            if (any_tiny && m.mag[f] < tiny) continue;
+            double o[D];
+            if (e >= 0) {
+#pragma unroll
+                for (int a = 0; a < D; ++a) o[a] = m.fcen[D * f + a] - ci[a];
+            } else {
+                double sep[D];
+                m.separation(i, m.owner[f], sep);
+#pragma unroll
+                for (int a = 0; a < D; ++a) o[a] = m.fcen[D * f + a] + sep[a] - ci[a];
+            }
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                const double dp = dot<D>(g[v], o);
+                bool clip = false, up = false;
+                double sc = 0.0;
+                if (dp > 0 && Wi[v] + dp > hi[v]) {
+                    clip = up = true;
+                    sc = hi[v] > Wi[v] ? (hi[v] - Wi[v]) / dp : 0.0;
+                } else if (dp < 0 && Wi[v] + dp < lo[v]) {
+                    clip = true;
+                    sc = lo[v] < Wi[v] ? (lo[v] - Wi[v]) / dp : 0.0;
+                }
+                if (!clip) continue;
+#pragma unroll
+                for (int a = 0; a < D; ++a) g[v][a] = g[v][a] * sc;
+                last[v] = k - first;
+                upper[v] = up;
+                zero[v] = up ? !(hi[v] > Wi[v]) : !(lo[v] < Wi[v]);
+                last_owned[v] = e >= 0;
+#pragma unroll
+                for (int a = 0; a < D; ++a) offset[v][a] = o[a];
+            }
+        }
+    // backwards through the clip: g = g0 s, s = (bound - W_i) / (g0 . o)
+    double xbar[V][U], bound_bar[V], obar[V][D];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        const double* gb = gbar + D * v;
+        xbar[v][0] = 0.0;
+        bound_bar[v] = 0.0;
+#pragma unroll
+        for (int a = 0; a < D; ++a) obar[v][a] = 0.0;
+        if (last[v] < 0) {
+#pragma unroll
+            for (int a = 0; a < D; ++a) xbar[v][1 + a] = gb[a];
+        } else if (zero[v]) {
+#pragma unroll
+            for (int a = 0; a < D; ++a) xbar[v][1 + a] = 0.0;
+        } else {
+            double g0[D];
+#pragma unroll
+            for (int a = 0; a < D; ++a) g0[a] = xs[v][1 + a];
+            const double den = dot<D>(g0, offset[v]);
+            const double sc = ((upper[v] ? hi[v] : lo[v]) - Wi[v]) / den;
+            const double sbar = dot<D>(gb, g0);
+            bound_bar[v] = sbar / den;
+            Wibar[v] -= sbar / den;
+            const double denbar = -sbar * sc / den;
+#pragma unroll
+            for (int a = 0; a < D; ++a) {
+                xbar[v][1 + a] = sc * gb[a] + denbar * offset[v][a];
+                obar[v][a] = denbar * g0[a];
+            }
+        }
+    }
+    // x = M^-1 b: b's bars M^-1 xbar; M's -sum_v bbar x^T
+    double bbar[V][U], G[U][U];
+#pragma unroll
+    for (int v = 0; v < V; ++v) solve(xbar[v], bbar[v]);
+#pragma unroll
+    for (int p = 0; p < U; ++p)
+#pragma unroll
+        for (int q = 0; q < U; ++q) {
+            double sum = 0.0;
+#pragma unroll
+            for (int v = 0; v < V; ++v) sum -= bbar[v][p] * xs[v][q];
+            G[p][q] = sum;
+        }
+    // each entry's bars: M = sum w X X^T, b_v = sum w X (W_j - W_i), X = (1, d + c_j - c_i), w = |A|
+    for (int k = first; k < end; ++k) {
+        const int kk = k - first;
+        int f, j;
+        bool owned;
+        double A[D], w, X[U];
+        entry(k, f, j, owned, A, w, X);
+        double Xbar[U], wbar = 0.0;
+#pragma unroll
+        for (int p = 0; p < U; ++p) {
+            double sum = 0.0;
+#pragma unroll
+            for (int q = 0; q < U; ++q) {
+                wbar += G[p][q] * X[p] * X[q];
+                sum += (G[p][q] + G[q][p]) * X[q];
+            }
+            Xbar[p] = w * sum;
+        }
+        double* row = rows + static_cast<int64_t>(E) * kk;
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const double dW = W[R * j + v] - Wi[v], xb = dot<U>(X, bbar[v]);
+            wbar += xb * dW;
+#pragma unroll
+            for (int p = 0; p < U; ++p) Xbar[p] += w * bbar[v][p] * dW;
+            Wibar[v] -= w * xb;
+            double Wjbar = w * xb;
+            if (last[v] >= 0 && !zero[v] && (upper[v] ? hi_k[v] : lo_k[v]) == kk) Wjbar += bound_bar[v];
+            row[v] = Wjbar;
+        }
+        double dbar[D], xfbar[D];
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+            dbar[a] = Xbar[1 + a];
+            xfbar[a] = 0.0;
+            cibar[a] -= Xbar[1 + a];
+            row[V + D + a] = Xbar[1 + a];                                   // c_j
+            row[V + 2 * D + a] = w > 0 ? wbar * A[a] / w : 0.0;              // A
+        }
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            if (last[v] != kk || zero[v]) continue;
+#pragma unroll
+            for (int a = 0; a < D; ++a) {
+                xfbar[a] += obar[v][a];
+                cibar[a] -= obar[v][a];
+                if (!last_owned[v]) dbar[a] += obar[v][a];
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+            row[V + a] = dbar[a];               // d
+            row[V + 3 * D + a] = xfbar[a];      // x_f
+        }
+    }
+}
+
 template <int D>
 __global__ void k_mv1_cells_adjoint(MeshDev<D> m, const double* __restrict__ W, const double* __restrict__ gb, const double* __restrict__ whb,
                                     const int32_t* __restrict__ angle_f, bool limit, bool steps_fixed, GasDev gas, double* __restrict__ Wb,
@@ -1063,44 +1335,11 @@ __global__ void k_mv1_cells_adjoint(MeshDev<D> m, const double* __restrict__ W, 
         for (int v = 0; v < V; ++v) Wd[v] = Dual(Wv[v], s == v ? 1.0 : 0.0);
         Wbar[s] += csbar * sound_t<Dual>(Wd, D + 1, gas.gamma).d;
     }
-    // the fit's columns: the cell's W and c, then every entry's W_j, d, c_j, A, x_f
+    // the fit's transpose: the cell's W and c, and every entry's row (W_j, d, c_j, A, x_f)
     double gbv[V * D];
 #pragma unroll
     for (int c = 0; c < V * D; ++c) gbv[c] = gb[V * D * static_cast<int64_t>(i) + c];
-    const int first = m.start[i], count = m.start[i + 1] - first;
-    FitDirection<D> dir;
-    for (int s = 0; s < V + D; ++s) {
-        dir.kind = s < V ? 0 : 1;
-        dir.comp = s < V ? s : s - V;
-        Dual gd[V * D];
-        fit_gradient_t<D>(m, i, W, limit, dir, gd);
-        double bar = 0;
-#pragma unroll
-        for (int c = 0; c < V * D; ++c) bar += gbv[c] * gd[c].d;
-        if (s < V)
-            Wbar[s] += bar;
-        else
-            cbar[s - V] += bar;
-    }
-    for (int k = 0; k < count; ++k) {
-        double* row = entry_bar + static_cast<int64_t>(E) * (first + k);
-        for (int s = 0; s < E; ++s) {
-            dir.entry = k;
-            if (s < V) {
-                dir.kind = 2;
-                dir.comp = s;
-            } else {
-                dir.kind = 3 + (s - V) / D;
-                dir.comp = (s - V) % D;
-            }
-            Dual gd[V * D];
-            fit_gradient_t<D>(m, i, W, limit, dir, gd);
-            double bar = 0;
-#pragma unroll
-            for (int c = 0; c < V * D; ++c) bar += gbv[c] * gd[c].d;
-            row[s] = bar;
-        }
-    }
+    fit_gradient_adjoint<D>(m, i, W, limit, gbv, Wbar, cbar, entry_bar + static_cast<int64_t>(E) * m.start[i]);
 #pragma unroll
     for (int v = 0; v < V; ++v) Wb[V * i + v] = Wbar[v];
 #pragma unroll

@@ -603,10 +603,99 @@ def moving_line(nx=131072, steps=2000, courant=0.4, log=print) -> dict:
     return out
 
 
+def moving_derivatives(nx=1024, repeat=5, log=print) -> dict:
+    """The cost of the order-1 moving derivatives in 2D, as the reference's --cost-moving measures it
+    (hydro_derivatives_test.cpp:1853-1990): an nx^2 jittered periodic mesh on the 2^-30 grid, the reference's wave state,
+    medians of `repeat` calls after a warm-up, each from the same state (the reload not timed), CUDA events. The geometry's
+    derivative is a null one on the device (zeros), standing in for the mesh library's, as there. The forward step is
+    time_step + step with the device remesh; the tangent and the adjoint run that step inside (the adjoint's restore of
+    the t^n mesh and state included); every array on the device."""
+    import torch
+
+    lib = hydro.lib()
+    step = 2.0 ** -30
+    rng = np.random.default_rng(5)
+    ij = np.stack(np.meshgrid(np.arange(nx), np.arange(nx), indexing="ij"), -1).reshape(-1, 2)
+    pts = np.floor((ij + 0.5 + rng.uniform(-0.15, 0.15, ij.shape)) / nx / step) * step
+    start_remesh, remesher = Remesher(dim=2, box=(1.0, 1.0)), Remesher(dim=2, box=(1.0, 1.0))
+    start = start_remesh.build(pts)
+    cells = start.cells()
+    c = cells.positions + cells.centroid
+    k, gamma = 2 * np.pi, 5.0 / 3.0
+    rho = 1 + 0.2 * np.sin(k * c[:, 0]) + rng.uniform(-0.01, 0.01, len(c))
+    vx = 0.3 * np.sin(k * c[:, 1]) + rng.uniform(-0.01, 0.01, len(c))
+    vy = 0.2 * np.cos(k * c[:, 0]) + rng.uniform(-0.01, 0.01, len(c))
+    P = 1 + 0.2 * np.cos(k * (c[:, 0] + c[:, 1])) + rng.uniform(-0.01, 0.01, len(c))
+    q0 = np.stack([rho, rho * vx, rho * vy, P / (gamma - 1) + 0.5 * rho * (vx * vx + vy * vy)], -1) * cells.volume[:, None]
+    fv = hydro.FiniteVolume(start, hydro.Gas(gamma), order=1, motion="moving")
+    N = nx * nx
+    dev = dict(device="cuda", dtype=torch.float64)
+    q_start = torch.tensor(q0, **dev)
+    faces = 4 * N  # above either mesh's faces (about 3 a cell on a jittered 2D lattice)
+    zero_cells, zero_points, zero_faces = torch.zeros(N, **dev), torch.zeros(N, 2, **dev), torch.zeros(faces, 2, **dev)
+    bar_cells, bar_points, bar_faces, bar_faces2 = (torch.zeros(N, **dev), torch.zeros(N, 2, **dev), torch.zeros(faces, 2, **dev),
+                                                    torch.zeros(faces, 2, **dev))
+    ptr = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+
+    def load():
+        fv.set_mesh(start)
+        hydro.check(lib.luna_fv_set_state(fv.handle, ptr(q_start), 1))
+        torch.cuda.synchronize()
+
+    def forward(dt):
+        fv.time_step(0.3)
+        fv.step_moving_device(dt, remesher)
+
+    def tangent(dt, dq, dx):
+        fv.time_step(0.3)
+        hydro.check(lib.luna_fv_step_moving_tangent(fv.handle, dt, ptr(dq), ptr(dx), ptr(zero_cells), ptr(zero_points),
+                                                    ptr(zero_faces), ptr(zero_faces), 1))
+        fv.step_moving_device(dt, remesher)
+        hydro.check(lib.luna_fv_step_moving_tangent_end(fv.handle, dt, ptr(dq), ptr(dx), ptr(zero_cells), ptr(zero_points),
+                                                        ptr(zero_faces), ptr(zero_faces), 1))
+
+    def adjoint(dt, qbar, xbar):
+        fv.time_step(0.3)
+        hydro.check(lib.luna_fv_step_moving_adjoint_begin(fv.handle, dt))
+        fv.step_moving_device(dt, remesher)
+        hydro.check(lib.luna_fv_step_moving_adjoint_new_mesh(fv.handle, dt, ptr(qbar), ptr(xbar), ptr(bar_faces2), ptr(bar_faces2), 1))
+        fv.set_mesh(start)  # the t^n mesh and state back for the first pass
+        hydro.check(lib.luna_fv_set_state(fv.handle, ptr(q_start), 1))
+        hydro.check(lib.luna_fv_step_moving_adjoint(fv.handle, dt, ptr(qbar), ptr(xbar), ptr(bar_cells), ptr(bar_points),
+                                                    ptr(bar_faces), ptr(bar_faces), 1))
+
+    load()
+    dt = fv.time_step(0.3)
+    out = {"config": {"cells": N, "order": 1, "dim": 2, "repeat": repeat, "geometry_derivative": "null (zeros on the device)",
+                      "remesh": "device"}}
+    calls = {"forward": lambda a: forward(dt), "tangent": lambda a: tangent(dt, *a), "adjoint": lambda a: adjoint(dt, *a)}
+    inputs = {"forward": lambda: (), "tangent": lambda: (torch.full((N, 4), 1e-6, **dev), torch.zeros(N, 2, **dev)),
+              "adjoint": lambda: (torch.ones(N, 4, **dev), torch.ones(N, 2, **dev))}
+    for name, call in calls.items():
+        times = []
+        for r in range(repeat + 1):
+            load()
+            args = inputs[name]()  # filled before the timed region, as the reference fills dq, dx, qbar, xbar
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            call(args)
+            e1.record()
+            torch.cuda.synchronize()
+            if r > 0:
+                times.append(e0.elapsed_time(e1))
+        out[name] = {"ms": float(np.median(times)), "cell_steps_per_s": N / (float(np.median(times)) * 1e-3)}
+    for name in ("tangent", "adjoint"):
+        out[name]["x_forward"] = out[name]["ms"] / out["forward"]["ms"]
+    log(f"{nx}^2: forward {out['forward']['ms']:.2f} ms, tangent {out['tangent']['ms']:.2f} ms ({out['tangent']['x_forward']:.1f}x), "
+        f"adjoint {out['adjoint']['ms']:.2f} ms ({out['adjoint']['x_forward']:.1f}x)")
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("study", choices=["precision", "adjoint", "moving", "learned", "learned_moving", "lines", "moving_line",
-                                      "kernels"])
+                                      "moving_derivatives", "kernels"])
     ap.add_argument("--case", default="adjoint", help="kernels: adjoint, tangent, mlp, line, tiles or moving")
     ap.add_argument("--nx", type=int)
     ap.add_argument("--steps", type=int)
@@ -628,15 +717,18 @@ def main():
         kw.pop("steps", None)
     if args.study == "learned_moving":
         kw.pop("threads", None)
-    if args.study in ("lines", "moving_line"):
+    if args.study in ("lines", "moving_line", "moving_derivatives"):
         kw.pop("threads", None)
+    if args.study == "moving_derivatives" and args.steps:
+        kw["repeat"] = kw.pop("steps")
     if args.study == "kernels":
         kw.pop("threads", None)
         kw["case"] = args.case
         if args.steps:
             kw["repeat"] = kw.pop("steps")
     res = {"precision": precision, "adjoint": adjoint, "moving": moving, "learned": learned_blast,
-           "learned_moving": learned_moving, "lines": lines, "moving_line": moving_line, "kernels": kernels}[args.study](**kw)
+           "learned_moving": learned_moving, "lines": lines, "moving_line": moving_line,
+           "moving_derivatives": moving_derivatives, "kernels": kernels}[args.study](**kw)
     text = json.dumps(res, indent=1)
     if args.out:
         with open(args.out, "w") as f:
