@@ -7,8 +7,9 @@
 // error word, the end slots' wishes), as the reference reads its dt and order check. One thread per slot does what the
 // reference's Kernel::body does for a moving line (:552-660): the five-cell stencil, the slopes and point velocities of
 // s - 1, s, s + 1, their new keys (each point moves by whole grid steps), the two faces' fluxes on the meshes of t^n and
-// t^n+1 in the frame of the face's move, the update and the slot's next position and key; the fused variant also reduces
-// the next dt of LUNA's rule and counts the slots out of order. When points cross, the slots re-sort by (key, cell) (CUB's
+// t^n+1 in the frame of the face's move (each computed once, shared through the block), the update and the slot's next
+// position and key; the fused variant also reduces the next dt of LUNA's rule and counts the slots out of order. When
+// points cross, the slots re-sort by (key, cell) (CUB's
 // radix sort, then one gather of every slot array). Cells from the walls (supply_cells) are decided on the host from the
 // two end slots, as the reference does, and inserted by one kernel that shifts the slot arrays.
 //
@@ -167,60 +168,95 @@ __device__ __forceinline__ void reset_spare(Counters* spare) {
     }
 }
 
-// Kernel::body, moving (:552-660), one thread per slot. Writes the slot's next Q, position and key; counts the slots out of
+constexpr int kLineBlock = 128;
+
+// Kernel::body, moving (:552-660), one thread per slot, a block sharing what the reference computes per slot three times
+// (the slope, point velocity and new key of s - 1, s, s + 1) and twice (each face's flux): each thread computes them for
+// its own slot (the block's first and last slots also for their outer neighbours) and the flux of its right face (the
+// first slot also its left one), and reads the rest from shared memory; the same operations on the same operands, so
+// the same bits as the per-slot body. Writes the slot's next Q, position, key and geometry; counts the slots out of
 // order against their right neighbour; Fused: the next dt of LUNA's rule with the volume of the new keys and |w - v| of
 // t^n (:632-658) into dt_bits, and with `watching` the end slots' wishes for a cell (the line before the step).
 template <int Order, bool Fused>
-__global__ void __launch_bounds__(128) k_mline_step(LineDev L, MovingDev M, const double* __restrict__ q, double* __restrict__ next, double dt,
-                                                    double courant, int watching, Counters* __restrict__ use, Counters* __restrict__ spare) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kLineBlock) k_mline_step(LineDev L, MovingDev M, const double* __restrict__ q, double* __restrict__ next, double dt,
+                                                           double courant, int watching, Counters* __restrict__ use, Counters* __restrict__ spare) {
+    __shared__ double s_grad[kLineBlock][3], s_point[kLineBlock], s_moves[kLineBlock], s_F[kLineBlock][3];
+    __shared__ long long s_key[kLineBlock];
+    const int t = threadIdx.x, s = blockIdx.x * blockDim.x + t;
     reset_spare(spare);
+    const bool active = s < L.n;
+    const bool last = active && (t == blockDim.x - 1 || s == L.n - 1);
     double smallest = 1.0e300;
-    if (s < L.n) {
-        Cell1 cell[5];
-        double gap[4], grad[5][3], point[5] = {0, 0, 0, 0, 0}, moves[5] = {0, 0, 0, 0, 0};
-        int64_t key[5] = {0, 0, 0, 0, 0};
+    Cell1 cell[5];
+    double gap[4], grad[5][3], point[5] = {0, 0, 0, 0, 0}, moves[5] = {0, 0, 0, 0, 0};
+    int64_t key[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+#pragma unroll
+        for (int v = 0; v < 3; ++v) grad[k][v] = 0;
+    if (active) {
         load(L, q, s, cell, gap);
 #pragma unroll
         for (int k = 1; k <= 3; ++k) {
-#pragma unroll
-            for (int v = 0; v < 3; ++v) grad[k][v] = 0;
-            if (!cell[k].real) continue;
+            if (!(k == 2 || (k == 1 && t == 0) || (k == 3 && last)) || !cell[k].real) continue;
             if constexpr (Order == 1)
 #pragma unroll
                 for (int v = 0; v < 3; ++v) grad[k][v] = gradient(L, cell + k, gap[k - 1], gap[k], v);
             point[k] = cell[k].W[1] + point_velocity(L, M, cell + k, gap[k - 1], gap[k], grad[k][0], 0.5 * (gap[k - 1] + gap[k]));
-        }
-#pragma unroll
-        for (int k = 1; k <= 3; ++k) {
-            if (!cell[k].real) continue;
-            const int t = slot_at(L, s, k - 2);
-            key[k] = snap(L, M, moved(L, M, M.x[t], point[k], dt));
-            int64_t d = key[k] - M.keys[t];
+            const int u = slot_at(L, s, k - 2);
+            key[k] = snap(L, M, moved(L, M, M.x[u], point[k], dt));
+            int64_t d = key[k] - M.keys[u];
             if (L.periodic) d = d > M.period / 2 ? d - M.period : d < -M.period / 2 ? d + M.period : d;
             moves[k] = static_cast<double>(d);
         }
-        double F[2][3];
 #pragma unroll
-        for (int f = 0; f < 2; ++f) {
-            const int a = 1 + f, b = 2 + f;
-            // a wall's face is static; between cells the face moves by the mean of its generators' moves
-            const bool inside = cell[a].real && cell[b].real;
-            const double travel = inside ? 0.5 * (moves[a] + moves[b]) * L.step : 0.0;
-            const double w = travel / dt;
-            const double ra = 0.5 * gap[a] - cell[a].c, rb = -0.5 * gap[a] - cell[b].c;
-            double pass[2][3];
+        for (int v = 0; v < 3; ++v) s_grad[t][v] = grad[2][v];
+        s_point[t] = point[2];
+        s_moves[t] = moves[2];
+        s_key[t] = key[2];
+    }
+    __syncthreads();
+    // the flux through the face between stencil cells a and b = a + 1, positive along +x
+    const auto face = [&](int a, double (&F)[3]) {
+        const int b = a + 1;
+        // a wall's face is static; between cells the face moves by the mean of its generators' moves
+        const bool inside = cell[a].real && cell[b].real;
+        const double travel = inside ? 0.5 * (moves[a] + moves[b]) * L.step : 0.0;
+        const double w = travel / dt;
+        const double ra = 0.5 * gap[a] - cell[a].c, rb = -0.5 * gap[a] - cell[b].c;
+        double pass[2][3];
 #pragma unroll
-            for (int second = 0; second < (Order == 1 ? 2 : 1); ++second) {
-                double Wl[3] = {0, 0, 0}, Wr[3] = {0, 0, 0};
-                if (cell[a].real) extrapolated<Order>(L, cell[a].W, grad[a], ra + second * travel, second, dt, Wl);
-                if (cell[b].real) extrapolated<Order>(L, cell[b].W, grad[b], rb + second * travel, second, dt, Wr);
-                if (!cell[a].real) ghost_face(L, Wr, cell[b].W, true, Wl);
-                if (!cell[b].real) ghost_face(L, Wl, cell[a].W, false, Wr);
-                moving_flux(L, Wl, Wr, w, pass[second]);
-            }
+        for (int second = 0; second < (Order == 1 ? 2 : 1); ++second) {
+            double Wl[3] = {0, 0, 0}, Wr[3] = {0, 0, 0};
+            if (cell[a].real) extrapolated<Order>(L, cell[a].W, grad[a], ra + second * travel, second, dt, Wl);
+            if (cell[b].real) extrapolated<Order>(L, cell[b].W, grad[b], rb + second * travel, second, dt, Wr);
+            if (!cell[a].real) ghost_face(L, Wr, cell[b].W, true, Wl);
+            if (!cell[b].real) ghost_face(L, Wl, cell[a].W, false, Wr);
+            moving_flux(L, Wl, Wr, w, pass[second]);
+        }
 #pragma unroll
-            for (int v = 0; v < 3; ++v) F[f][v] = Order == 1 ? 0.5 * (pass[0][v] + pass[1][v]) : pass[0][v];
+        for (int v = 0; v < 3; ++v) F[v] = Order == 1 ? 0.5 * (pass[0][v] + pass[1][v]) : pass[0][v];
+    };
+    double F[2][3];
+    if (active) {
+        if (!last) {  // the right neighbour's from its thread
+#pragma unroll
+            for (int v = 0; v < 3; ++v) grad[3][v] = cell[3].real ? s_grad[t + 1][v] : 0.0;
+            point[3] = cell[3].real ? s_point[t + 1] : 0.0;
+            moves[3] = cell[3].real ? s_moves[t + 1] : 0.0;
+            key[3] = cell[3].real ? s_key[t + 1] : 0;
+        }
+        face(2, F[1]);
+#pragma unroll
+        for (int v = 0; v < 3; ++v) s_F[t][v] = F[1][v];
+        if (t == 0) face(1, F[0]);
+    }
+    __syncthreads();
+    if (active) {
+        if (t > 0) {
+#pragma unroll
+            for (int v = 0; v < 3; ++v) F[0][v] = s_F[t - 1][v];
+            key[1] = cell[1].real ? s_key[t - 1] : 0;
         }
         double U[3];
         bool finite = true;
@@ -242,10 +278,10 @@ __global__ void __launch_bounds__(128) k_mline_step(LineDev L, MovingDev M, cons
             left = static_cast<double>(2 * key[2]);
         }
         if (cell[3].real) {
-            const int t = slot_at(L, s, 1);
+            const int u = slot_at(L, s, 1);
             const int64_t d = key[3] - key[2];
             right = static_cast<double>(d < 0 && L.periodic ? d + M.period : d);
-            if (!before(key[2], i, key[3], M.cell[t])) atomicAdd(&use->descents, 1);
+            if (!before(key[2], i, key[3], M.cell[u])) atomicAdd(&use->descents, 1);
         } else {
             right = static_cast<double>(2 * (M.period - key[2]));
         }
@@ -713,9 +749,9 @@ struct luna_mline {
         const int w = fused && watching ? 1 : 0;
         const dim3 grid(blocks_of(n));
         if (order == 1)
-            (fused ? k_mline_step<1, true> : k_mline_step<1, false>)<<<grid, 128, 0, stream>>>(dev, mdev, q.ptr, q2.ptr, dt, courant, w, use(), spare());
+            (fused ? k_mline_step<1, true> : k_mline_step<1, false>)<<<grid, kLineBlock, 0, stream>>>(dev, mdev, q.ptr, q2.ptr, dt, courant, w, use(), spare());
         else
-            (fused ? k_mline_step<0, true> : k_mline_step<0, false>)<<<grid, 128, 0, stream>>>(dev, mdev, q.ptr, q2.ptr, dt, courant, w, use(), spare());
+            (fused ? k_mline_step<0, true> : k_mline_step<0, false>)<<<grid, kLineBlock, 0, stream>>>(dev, mdev, q.ptr, q2.ptr, dt, courant, w, use(), spare());
         MLINE_CUDA(cudaGetLastError());
         Counters c;
         luna_status st = read_counters(&c, smallest);
