@@ -275,8 +275,9 @@ def learned_section(mesh, q0, steps, warmup, stream, torch) -> dict:
 
 def moving_section(nx, steps, warmup) -> dict:
     """The moving-mesh configuration's step at nx^3 (the point blast on snapped jittered generators, generators moved with
-    the gas plus the roundness velocity, fluxes on the old and the new faces, FP32 face arithmetic with FP64 state:
-    riemann32), with the mesh rebuilt on the GPU every step: the hydro part's device time (CUDA events around the
+    the gas plus the roundness velocity, fluxes on the old and the new faces, FP32 fluxes with FP64 state: the
+    reference's Precision<double, float, float, float>, "single": face states, Riemann solve and flux rows in float),
+    with the mesh rebuilt on the GPU every step: the hydro part's device time (CUDA events around the
     hydro kernels, the geometry rows of the new mesh included; the remesh outside, as the reference's hydro part) and
     the whole step's wall time (remesh and taking the new mesh included), after ``warmup`` steps."""
     from luna_cpp_b200 import hydro
@@ -289,12 +290,13 @@ def moving_section(nx, steps, warmup) -> dict:
     pts = np.round(jittered_points((nx, nx, nx), jitter=0.1, seed=1) / grid) * grid
     remesher = Remesher(3, (1.0, 1.0, 1.0))
     mesh = remesher.build(pts)
-    fv = hydro.FiniteVolume(mesh, precision="fp32", motion="moving")
+    fv = hydro.FiniteVolume(mesh, precision="single", motion="moving")
     fv.set_state(point_blast(mesh.cells()))
     run_moving(fv, 1.0, max_steps=warmup, remesher=remesher)
     r = run_moving(fv, 1.0, max_steps=steps, remesher=remesher)
     N, n = mesh.n_cells, r["steps"]
-    out = {"workload": f"3D moving point blast {nx}^3 jittered (0.1), riemann32, CFL 0.3, remesh on the GPU every step",
+    out = {"workload": f"3D moving point blast {nx}^3 jittered (0.1), FP64 state / FP32 fluxes (single), CFL 0.3, remesh on "
+                       "the GPU every step",
            "steps": n, "warmup": warmup, "hydro_ms_per_step": r["hydro_device_ms"] / n,
            "hydro_cell_updates_per_s": N * n / (r["hydro_device_ms"] * 1e-3),
            "remesh_ms_per_step": 1e3 * r["remesh_s"] / n, "mesh_load_ms_per_step": 1e3 * r["mesh_load_s"] / n,

@@ -262,12 +262,12 @@ def test_moving_step_matches_oracle(cuda):
     assert abs((g[:, 4].sum() - before[4]) / before[4]) < 1e-14
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "single"])
 def test_moving_config_radial_profile_against_oracle(cuda, precision):
     """The moving-mesh configuration scaled down: the point blast on 16^3 snapped jittered generators, moving mesh, to
     t = 0.05, each side its own dt, positions and remesh; the radial density profile (32 shells) against the oracle's
-    run of the same policy: relative L1 <= 1e-8 (FP64) or 1e-4 (FP32 face arithmetic, riemann32). Also the steps
-    taken agree and mass and energy are conserved to round-off."""
+    run of the same policy: relative L1 <= 1e-8 (FP64) or 1e-4 (FP32 face arithmetic: riemann32, and single with its
+    float flux rows). Also the steps taken agree and mass and energy are conserved to round-off."""
     from luna_cpp_b200.mesh import build_mesh
     from luna_cpp_b200.studies import radial_profile, snapped_jittered_mesh
 

@@ -110,6 +110,27 @@ def test_moving_steps(reference):
     assert np.max(np.abs(got - want)) <= 1e-12 * np.max(np.abs(want))
 
 
+@pytest.mark.parametrize("precision,ref_precision", [("fp32", "riemann32"), ("single", "single")])
+def test_moving_step_float_policies(reference, precision, ref_precision):
+    """One moving step of the blast on 16^3 jittered generators in the float policies the moving configuration runs
+    (riemann32: the Riemann solve in float; single: the gradients, face states, solve and flux rows in float) against the
+    reference running the same policy: the same positions, Q within 1e-5 of the largest (float face arithmetic)."""
+    mesh = jittered_mesh(16)
+    q0 = point_blast(mesh, radius_cells=2.0)
+    box = tuple(mesh.box[:3])
+    gpu = hydro.FiniteVolume(mesh, motion="moving", precision=precision)
+    ref = R.ReferenceFV(mesh, moving=True, precision=ref_precision, remesh=lambda x: build_mesh(x, box=box))
+    gpu.set_state(q0)
+    ref.set_state(q0)
+    dg, dr = gpu.time_step(0.3), ref.time_step(0.3)
+    assert abs(dg - dr) <= 1e-6 * dr
+    gpu.step_moving(dr, lambda x: build_mesh(x, box=box))
+    ref.step(dr)
+    assert np.array_equal(gpu.positions(), ref.positions())
+    got, want = gpu.get_state(), ref.get_state()
+    assert np.max(np.abs(got - want)) <= 1e-5 * np.max(np.abs(want))
+
+
 @pytest.mark.parametrize("dim", [2, 3])
 def test_moving_steps_order_0(reference, dim):
     """The order-0 moving step (step(): FaceFlux<0, true> on the current mesh with the point velocities' face velocities,
