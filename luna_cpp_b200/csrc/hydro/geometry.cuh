@@ -940,6 +940,7 @@ __global__ void __launch_bounds__(128, sizeof(G) == sizeof(double) ? LUNA_FLUX_M
     constexpr int V = D + 2;
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     int count = 0;
+    if (x.dt_at) x.dt = *x.dt_at;  // launched behind the sweep before the host has read the dt
     if (f < m.f) {
         FaceRow<G> r;
         load_face_row<G>(geo.faces + f, r);

@@ -294,6 +294,7 @@ struct FluxArgs {
     const double* __restrict__ w = nullptr;            // order-0 moving step: the point velocities [N][D]
     const uint16_t* __restrict__ grad16 = nullptr;    // Grad16: binary16 rows [N][16] instead of grad (G = float)
     const uint32_t* __restrict__ exponents = nullptr;  // Grad16: the three int8 group exponents of each row
+    const double* __restrict__ dt_at = nullptr;        // set: dt read from device memory (the sweep's reduction)
 };
 
 // The group (0 rho, 1 the velocity, 2 P) of gradient component c = D v + a: each has its own exponent in a Grad16 row.

@@ -152,6 +152,11 @@ struct luna_fv {
     int64_t phase_launches[5] = {0, 0, 0, 0, 0};
 
     bool prims_ready = false, swept = false, moving_pending = false;
+    // The static per-face step's flux pass, launched by time_step behind the sweep with the dt of the sweep's reduction
+    // read on the device (no idle gap while the host reads dt); step(dt) with that dt, bit for bit, then only updates.
+    bool flux_ready = false;
+    unsigned long long flux_dt_bits = 0;
+    cudaEvent_t counters_read = nullptr;
     double pending_dt = 0;
     double grid_step = 0, per_step = 0;
     long long period[3] = {1, 1, 1};
@@ -171,6 +176,7 @@ struct luna_fv {
     ~luna_fv() {
         if (tiler) luna::device_tiler_destroy(tiler);
         if (host_counters) cudaFreeHost(host_counters);
+        if (counters_read) cudaEventDestroy(counters_read);
         for (auto& e : event_pool) {
             cudaEventDestroy(e.first);
             cudaEventDestroy(e.second);
@@ -823,10 +829,46 @@ luna_status run_apply(luna_fv* fv, const G* grad, double dt) {
     return LUNA_OK;
 }
 
+// Whether time_step may launch the step's flux pass itself: a static mesh stepped per face by the two-kernel pass.
+template <int D>
+luna_status flux_ahead(luna_fv* fv, bool* ahead) {
+    *ahead = false;
+    if (fv->motion == LUNA_MOVING || fv->update != LUNA_UPDATE_PER_FACE) return LUNA_OK;
+    if (fv->precision == LUNA_FP64 && fv->order == 1 && fv->grads_in_wg) {
+        if (fv->fused == 0) LUNA_TRY(plan_fused<D>(fv));
+        if (fv->fused == 1) return LUNA_OK;
+    }
+    *ahead = true;
+    return LUNA_OK;
+}
+
+// The flux pass of the static step with the dt of the sweep's reduction (read on the device).
+template <int D, class G>
+luna_status launch_flux_ahead(luna_fv* fv, const G* grad) {
+    auto x = flux_args<D, G>(fv, grad, 0.0);
+    x.dt_at = reinterpret_cast<const double*>(&fv->counters.ptr->dt_bits);
+    if (fv->order == 0) return dispatch_flux_rows<D, 0, G>(fv, x);
+    return dispatch_flux_rows<D, 1, G>(fv, x);
+}
+
 template <int D>
 luna_status step_static(luna_fv* fv, double dt) {
+    unsigned long long bits;
+    std::memcpy(&bits, &dt, sizeof(bits));
+    const bool ahead = fv->swept && fv->flux_ready && bits == fv->flux_dt_bits;
+    fv->flux_ready = false;
     if (!fv->swept) LUNA_TRY(prepare_sweep<D>(fv, 1.0));
     fv->swept = false;
+    if (ahead) {  // time_step launched this dt's flux pass: the update alone
+        {
+            const long timed_ = fv->open_timed(3);
+            launch_update<D, true>(fv, dt);
+            fv->close_timed(timed_);
+        }
+        LUNA_CUDA(cudaGetLastError());
+        fv->prims_ready = true;  // the update wrote the next primitive rows
+        return LUNA_OK;
+    }
     LUNA_CUDA(cudaMemsetAsync(&fv->counters.ptr->fallbacks[0], 0, 2 * sizeof(unsigned long long), fv->stream));
     if (fv->precision != LUNA_FP64) return run_apply<D, float>(fv, fv->grad32.ptr, dt);
     return run_apply<D, double>(fv, fv->grad64.ptr, dt);
@@ -1437,7 +1479,28 @@ LUNA_API luna_status luna_fv_time_step(luna_fv* fv, double courant, double* dt_o
     if (!fv || !dt_out) return set_error(LUNA_EINVAL, "null argument");
     if (fv->moving_pending) return set_error(LUNA_ESTATE, "time_step inside a moving step (call luna_fv_step_moving_end first)");
     LUNA_TRY(fv->dim == 3 ? prepare_sweep<3>(fv, courant) : prepare_sweep<2>(fv, courant));
-    LUNA_TRY(read_counters(fv));
+    fv->flux_ready = false;
+    bool ahead = false;
+    LUNA_TRY(fv->dim == 3 ? flux_ahead<3>(fv, &ahead) : flux_ahead<2>(fv, &ahead));
+    if (ahead) {
+        // the counters (dt, error word) read behind the sweep; the step's flux pass queued behind that read with the
+        // reduced dt read on the device, so it runs while the host takes dt
+        if (!fv->counters_read) LUNA_CUDA(cudaEventCreateWithFlags(&fv->counters_read, cudaEventDisableTiming));
+        LUNA_CUDA(cudaMemsetAsync(&fv->counters.ptr->fallbacks[0], 0, 2 * sizeof(unsigned long long), fv->stream));
+        LUNA_CUDA(cudaMemcpyAsync(fv->host_counters, fv->counters.ptr, sizeof(luna::Counters), cudaMemcpyDeviceToHost, fv->stream));
+        LUNA_CUDA(cudaEventRecord(fv->counters_read, fv->stream));
+        luna_status st;
+        if (fv->precision != LUNA_FP64)
+            st = fv->dim == 3 ? launch_flux_ahead<3, float>(fv, fv->grad32.ptr) : launch_flux_ahead<2, float>(fv, fv->grad32.ptr);
+        else
+            st = fv->dim == 3 ? launch_flux_ahead<3, double>(fv, fv->grad64.ptr) : launch_flux_ahead<2, double>(fv, fv->grad64.ptr);
+        LUNA_TRY(st);
+        LUNA_CUDA(cudaEventSynchronize(fv->counters_read));
+        std::memcpy(&fv->flux_dt_bits, &fv->host_counters->dt_bits, sizeof(fv->flux_dt_bits));
+        fv->flux_ready = (fv->host_counters->error & 17ull) == 0;
+    } else {
+        LUNA_TRY(read_counters(fv));
+    }
     fv->swept = true;
     double dt;
     std::memcpy(&dt, &fv->host_counters->dt_bits, sizeof(dt));
