@@ -664,6 +664,9 @@ __device__ __forceinline__ void update_cell(const MeshDev<D>& m, double* __restr
 #ifndef LUNA_UPDATE_MIN_BLOCKS_F
 #define LUNA_UPDATE_MIN_BLOCKS_F LUNA_UPDATE_MIN_BLOCKS  // single's float flux rows
 #endif
+#ifndef LUNA_UPDATE_BATCH_F
+#define LUNA_UPDATE_BATCH_F LUNA_UPDATE_BATCH  // single's float flux rows (32-B rows, half the registers a row)
+#endif
 // FS = float: the rows of store_flux_row, one aligned vector load each, widened to double before the sum (the
 // reference's static_cast<double>(F(f, v)), finite_volume.hpp:1607).
 template <int D, bool NextPrims, bool Windowed = false, class FS = double>
@@ -678,7 +681,7 @@ __global__ void __launch_bounds__(256, Windowed ? (sizeof(FS) == sizeof(float) ?
     const int first = m.start[i], end = m.start[i + 1];
     // kBatch entries at a time: their list words, then their flux rows, are all requested before any is used (the
     // gathers of a list are independent); the sums stay in list order.
-    constexpr int kBatch = Windowed ? LUNA_UPDATE_BATCH : 4;
+    constexpr int kBatch = Windowed ? (sizeof(FS) == sizeof(float) ? LUNA_UPDATE_BATCH_F : LUNA_UPDATE_BATCH) : 4;
     for (int k0 = first; k0 < end; k0 += kBatch) {
         int32_t e[kBatch];
 #pragma unroll
