@@ -275,6 +275,78 @@ __host__ __device__ constexpr int bar_width() {
 
 // Per face: G's bar from both cells' Q bars, then through the flux and the face velocity to the bars of W_L, W_R, A,
 // d, x_f, w_L, w_R (moving_faces_adjoint, :2510-2540), from the local Jacobians' columns.
+// The transpose of face_flux_t in reverse mode (MovingFace::adjoint, euler.hpp:883-916): G = |A| to_lab(F, w), F the
+// static solve of the face-frame states L - w, R - w along n = A / |A|. The solve's adjoint in its states
+// (hllc_flux_adjoint / hll_flux_adjoint), to_lab's in F and w, and n's bar from the solve's invariance under rotations:
+// for dn orthogonal to n, <Fbar, dF/dn dn> = dn . (turn(Fbar, F) - turn(Lbar, L') - turn(Rbar, R')) on the velocity parts,
+// turn(a, b) = a (n . b) - b (n . a). Adds into Lbar, Rbar, Abar, wbar.
+template <int D, int Riemann>
+__device__ void moving_face_adjoint(const double* L, const double* R, const double* A, const double* w, const GasDev& gas,
+                                    const double* Gbar, double* Lbar, double* Rbar, double* Abar, double* wbar) {
+    constexpr int V = D + 2, P = D + 1;
+    const double mag = sqrt(dot<D>(A, A)), inv = 1.0 / mag;
+    double n[D];
+#pragma unroll
+    for (int a = 0; a < D; ++a) n[a] = A[a] * inv;
+    double Lr[V], Rr[V], F[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) Lr[v] = L[v], Rr[v] = R[v];
+#pragma unroll
+    for (int k = 0; k < D; ++k) Lr[1 + k] -= w[k], Rr[1 + k] -= w[k];
+    const double zero[D] = {};
+    if constexpr (Riemann == 1)
+        hll_flux<D>(Lr, Rr, n, zero, gas, F, false);
+    else
+        hllc_flux<D, double>(Lr, Rr, n, zero, gas.gamma, gas.inverse_gm1, F, false);
+    double lab[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) lab[v] = F[v];
+    to_lab<D, double>(lab, w);
+    // G = |A| lab
+    double magbar = 0, labbar[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        magbar += Gbar[v] * lab[v];
+        labbar[v] = mag * Gbar[v];
+    }
+    // lab = to_lab(F, w): momentum += w F_0, energy += w . F_mom + |w|^2 / 2 F_0
+    double Fbar[V];
+    Fbar[0] = labbar[0] + 0.5 * dot<D>(w, w) * labbar[P];
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        Fbar[0] += w[k] * labbar[1 + k];
+        Fbar[1 + k] = labbar[1 + k] + w[k] * labbar[P];
+        wbar[k] += labbar[1 + k] * F[0] + labbar[P] * (F[1 + k] + w[k] * F[0]);
+    }
+    Fbar[P] = labbar[P];
+    double Lrb[V], Rrb[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) Lrb[v] = Rrb[v] = 0;
+    if constexpr (Riemann == 1)
+        hll_flux_adjoint<D>(Lr, Rr, n, gas, Fbar, Lrb, Rrb);
+    else
+        hllc_flux_adjoint<D>(Lr, Rr, n, gas, Fbar, Lrb, Rrb);
+    const auto turn = [&](const double* a, const double* b, double* out, double sign) {
+        const double nb = dot<D>(n, b), na = dot<D>(n, a);
+#pragma unroll
+        for (int k = 0; k < D; ++k) out[k] += sign * (a[k] * nb - b[k] * na);
+    };
+    double nbar[D] = {};
+    turn(Fbar + 1, F + 1, nbar, 1.0);
+    turn(Lrb + 1, Lr + 1, nbar, -1.0);
+    turn(Rrb + 1, Rr + 1, nbar, -1.0);
+    const double nn = dot<D>(n, nbar);
+#pragma unroll
+    for (int a = 0; a < D; ++a) Abar[a] += magbar * n[a] + (nbar[a] - n[a] * nn) * inv;
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        Lbar[v] += Lrb[v];
+        Rbar[v] += Rrb[v];
+    }
+#pragma unroll
+    for (int k = 0; k < D; ++k) wbar[k] -= Lrb[1 + k] + Rrb[1 + k];
+}
+
 template <int D, int Riemann>
 __global__ void k_mv_faces_adjoint(MeshDev<D> m, const double* __restrict__ W, const double* __restrict__ w, const double* __restrict__ qbar,
                                    double dt, GasDev gas, double* __restrict__ face_bar, double* __restrict__ xfbar) {
@@ -308,33 +380,20 @@ __global__ void k_mv_faces_adjoint(MeshDev<D> m, const double* __restrict__ W, c
 #pragma unroll
         for (int q = 0; q < D; ++q) wf[q] = tmp[q];
     }
-    // the flux's inputs: W_L (V), W_R (V), A (D), w_f (D)
-    double wfbar[D];
+    // the flux's inputs, W_L (V), W_R (V), A (D), w_f (D), by the face's reverse mode
+    double wfbar[D], Lbar[V], Rbar[V], Ab[D];
 #pragma unroll
-    for (int q = 0; q < D; ++q) wfbar[q] = 0;
-    for (int s = 0; s < 2 * V + 2 * D; ++s) {
-        Dual L[V], R[V], A[D], wd[D], G[V];
+    for (int q = 0; q < D; ++q) wfbar[q] = Ab[q] = 0;
 #pragma unroll
-        for (int v = 0; v < V; ++v) {
-            L[v] = Dual(Lv[v], s == v ? 1.0 : 0.0);
-            R[v] = Dual(Rv[v], s == V + v ? 1.0 : 0.0);
-        }
+    for (int v = 0; v < V; ++v) Lbar[v] = Rbar[v] = 0;
+    moving_face_adjoint<D, Riemann>(Lv, Rv, a, wf, gas, Gbar, Lbar, Rbar, Ab, wfbar);
 #pragma unroll
-        for (int q = 0; q < D; ++q) {
-            A[q] = Dual(a[q], s == 2 * V + q ? 1.0 : 0.0);
-            wd[q] = Dual(wf[q], s == 2 * V + D + q ? 1.0 : 0.0);
-        }
-        face_flux_t<D, Riemann, Dual>(L, R, A, wd, gas, G);
-        double bar = 0;
-#pragma unroll
-        for (int v = 0; v < V; ++v) bar += Gbar[v] * G[v].d;
-        if (s < 2 * V)
-            row[s] = bar;  // W_L then W_R
-        else if (s < 2 * V + D)
-            row[2 * V + 3 * D + (s - 2 * V)] = bar;  // A
-        else
-            wfbar[s - 2 * V - D] = bar;
+    for (int v = 0; v < V; ++v) {
+        row[v] = Lbar[v];  // W_L then W_R
+        row[V + v] = Rbar[v];
     }
+#pragma unroll
+    for (int q = 0; q < D; ++q) row[2 * V + 3 * D + q] = Ab[q];  // A
     // the face velocity's inputs: d (D), x_f (D), w_L (D), w_R (D)
     for (int s = 0; s < 4 * D; ++s) {
         Dual d[D], xf[D], wL[D], wR[D], out[D];
@@ -802,78 +861,6 @@ __host__ __device__ constexpr int pass_width() {
 // One pass's adjoint per face (moving_pass_adjoint, :2882-2929): the flux's local Jacobian columns times G's bar -> the sides',
 // the area's and the face velocity's bars; the face velocity's -> d, x_f, w-hat; the sides' offsets' bars g^T S-bar (where
 // the side did not fall back) into x_f's bar and, for the neighbour's side (whose offset carries x_owner), the row.
-// The transpose of face_flux_t in reverse mode (MovingFace::adjoint, euler.hpp:883-916): G = |A| to_lab(F, w), F the
-// static solve of the face-frame states L - w, R - w along n = A / |A|. The solve's adjoint in its states
-// (hllc_flux_adjoint / hll_flux_adjoint), to_lab's in F and w, and n's bar from the solve's invariance under rotations:
-// for dn orthogonal to n, <Fbar, dF/dn dn> = dn . (turn(Fbar, F) - turn(Lbar, L') - turn(Rbar, R')) on the velocity parts,
-// turn(a, b) = a (n . b) - b (n . a). Adds into Lbar, Rbar, Abar, wbar.
-template <int D, int Riemann>
-__device__ void moving_face_adjoint(const double* L, const double* R, const double* A, const double* w, const GasDev& gas,
-                                    const double* Gbar, double* Lbar, double* Rbar, double* Abar, double* wbar) {
-    constexpr int V = D + 2, P = D + 1;
-    const double mag = sqrt(dot<D>(A, A)), inv = 1.0 / mag;
-    double n[D];
-#pragma unroll
-    for (int a = 0; a < D; ++a) n[a] = A[a] * inv;
-    double Lr[V], Rr[V], F[V];
-#pragma unroll
-    for (int v = 0; v < V; ++v) Lr[v] = L[v], Rr[v] = R[v];
-#pragma unroll
-    for (int k = 0; k < D; ++k) Lr[1 + k] -= w[k], Rr[1 + k] -= w[k];
-    const double zero[D] = {};
-    if constexpr (Riemann == 1)
-        hll_flux<D>(Lr, Rr, n, zero, gas, F, false);
-    else
-        hllc_flux<D, double>(Lr, Rr, n, zero, gas.gamma, gas.inverse_gm1, F, false);
-    double lab[V];
-#pragma unroll
-    for (int v = 0; v < V; ++v) lab[v] = F[v];
-    to_lab<D, double>(lab, w);
-    // G = |A| lab
-    double magbar = 0, labbar[V];
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-        magbar += Gbar[v] * lab[v];
-        labbar[v] = mag * Gbar[v];
-    }
-    // lab = to_lab(F, w): momentum += w F_0, energy += w . F_mom + |w|^2 / 2 F_0
-    double Fbar[V];
-    Fbar[0] = labbar[0] + 0.5 * dot<D>(w, w) * labbar[P];
-#pragma unroll
-    for (int k = 0; k < D; ++k) {
-        Fbar[0] += w[k] * labbar[1 + k];
-        Fbar[1 + k] = labbar[1 + k] + w[k] * labbar[P];
-        wbar[k] += labbar[1 + k] * F[0] + labbar[P] * (F[1 + k] + w[k] * F[0]);
-    }
-    Fbar[P] = labbar[P];
-    double Lrb[V], Rrb[V];
-#pragma unroll
-    for (int v = 0; v < V; ++v) Lrb[v] = Rrb[v] = 0;
-    if constexpr (Riemann == 1)
-        hll_flux_adjoint<D>(Lr, Rr, n, gas, Fbar, Lrb, Rrb);
-    else
-        hllc_flux_adjoint<D>(Lr, Rr, n, gas, Fbar, Lrb, Rrb);
-    const auto turn = [&](const double* a, const double* b, double* out, double sign) {
-        const double nb = dot<D>(n, b), na = dot<D>(n, a);
-#pragma unroll
-        for (int k = 0; k < D; ++k) out[k] += sign * (a[k] * nb - b[k] * na);
-    };
-    double nbar[D] = {};
-    turn(Fbar + 1, F + 1, nbar, 1.0);
-    turn(Lrb + 1, Lr + 1, nbar, -1.0);
-    turn(Rrb + 1, Rr + 1, nbar, -1.0);
-    const double nn = dot<D>(n, nbar);
-#pragma unroll
-    for (int a = 0; a < D; ++a) Abar[a] += magbar * n[a] + (nbar[a] - n[a] * nn) * inv;
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-        Lbar[v] += Lrb[v];
-        Rbar[v] += Rrb[v];
-    }
-#pragma unroll
-    for (int k = 0; k < D; ++k) wbar[k] -= Lrb[1 + k] + Rrb[1 + k];
-}
-
 template <int D, int Riemann, bool Second>
 __global__ void k_mv1_pass_faces_adjoint(MeshDev<D> m, const double* __restrict__ W, const double* __restrict__ g, const double* __restrict__ wh,
                                          const double* __restrict__ c0, const double* __restrict__ qbar, double dt, GasDev gas,
