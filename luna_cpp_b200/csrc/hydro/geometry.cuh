@@ -878,7 +878,7 @@ __global__ void k_apply_factors(int rows, const int* __restrict__ cells, const u
 // The static flux pass over the face rows (FaceFlux::operator(), finite_volume.hpp:1415-1434): one streamed row per
 // face, then the two cells' primitive and gradient rows.
 // Resident blocks per SM the flux pass's registers are cut for; measured at 128^3 FP64 (fluxes ms): unbounded (96
-// registers, 5 blocks) 0.80-0.84, 6 blocks 0.77, 8 blocks 1.03 (spills).
+// registers, 5 blocks) 0.80-0.84, 6 blocks 0.77 (0.699 with the later rows), 7 blocks 0.767, 8 blocks 1.03 (spills).
 #ifndef LUNA_FLUX_MIN_BLOCKS
 #define LUNA_FLUX_MIN_BLOCKS 6
 #endif
