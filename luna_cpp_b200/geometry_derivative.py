@@ -203,3 +203,20 @@ class Geometry2D:
         b = np.concatenate([np.asarray(Vbar, np.float64).reshape(-1), np.asarray(cbar, np.float64).reshape(-1),
                             np.asarray(Abar, np.float64).reshape(-1), np.asarray(xfbar, np.float64).reshape(-1)])
         return (self.J.T @ b).reshape(N, 2)
+
+
+class NullGeometry:
+    """A geometry derivative that is zero: the mesh's V, c, A and x_f held fixed as the generators move (the reference's
+    cost test stands one in for the mesh library's, hydro_derivatives_test.cpp:1853-1857). Any dimension. The moving
+    step's derivatives then hold every term but the geometry's own (the separations, the face velocity and the drift
+    still take dx)."""
+
+    def __init__(self, mesh):
+        self.n, self.f, self.dim = int(mesh.n_cells), int(mesh.n_faces), int(mesh.dim)
+
+    def tangent(self, dx):
+        D = self.dim
+        return np.zeros(self.n), np.zeros((self.n, D)), np.zeros((self.f, D)), np.zeros((self.f, D))
+
+    def adjoint(self, Vbar, cbar, Abar, xfbar):
+        return np.zeros((self.n, self.dim))

@@ -22,6 +22,25 @@ def jittered_mesh(nx: int, dim: int = 3, jitter: float = 0.1, seed: int = 1):
     return build_mesh(jittered_points(cells, jitter=jitter, seed=seed), box=(1.0,) * dim)
 
 
+def wave_state_3d(mesh, seed: int = 3, noise: float = 0.01, gamma: float = 5.0 / 3.0):
+    """The reference's 3D moving-step derivative state (hydro_derivatives_test.cpp:1513-1516), extensive: waves in every
+    primitive at the cell centroids plus uniform noise of +- noise."""
+    rng = np.random.default_rng(seed)
+    c = mesh.positions + mesh.centroid
+    n, k = len(c), 2 * np.pi
+
+    def jitter():
+        return noise * rng.uniform(-1, 1, n)
+
+    rho = 1 + 0.2 * np.sin(k * c[:, 0]) + jitter()
+    vx = 0.3 * np.sin(k * c[:, 1]) + jitter()
+    vy = 0.2 * np.cos(k * c[:, 2]) + jitter()
+    vz = 0.25 * np.sin(k * (c[:, 0] + c[:, 2])) + jitter()
+    P = 1 + 0.2 * np.cos(k * (c[:, 0] + c[:, 1] + c[:, 2])) + jitter()
+    U = np.stack([rho, rho * vx, rho * vy, rho * vz, P / (gamma - 1) + 0.5 * rho * (vx * vx + vy * vy + vz * vz)], -1)
+    return U * mesh.volume[:, None]
+
+
 def wave_state_2d(mesh, seed: int = 3, noise: float = 0.01, gamma: float = 5.0 / 3.0):
     """The reference's moving-step derivative state (hydro_derivatives_test.cpp:1505-1516), extensive: smooth waves in
     every primitive at the cell centroids plus uniform noise of +- noise in each, so no two neighbours tie and no field is

@@ -99,6 +99,50 @@ def test_moving_dot_test(cuda, riemann, order):
     assert abs(lhs - rhs) < 1e-12 * size, (lhs, rhs, size)
 
 
+@pytest.mark.parametrize("order", [0, 1])
+def test_moving_dot_test_3d(cuda, order):
+    """The 3D kernels: the dot test over two steps on 8^3 jittered generators with the reference's 3D wave state and a
+    null geometry derivative (the same linear map on both sides), 1e-12 of the products' magnitudes."""
+    from conftest import wave_state_3d
+    from luna_cpp_b200.geometry_derivative import NullGeometry
+
+    mesh = jittered_mesh(8, dim=3, jitter=0.15, seed=4)
+    q0 = wave_state_3d(mesh)
+    box = tuple(mesh.box[:3])
+    fv = hydro.FiniteVolume(mesh, hydro.Gas(GAMMA), order=order, motion="moving")
+    remesh = lambda p: build_mesh(p, box=box)  # noqa: E731
+    x0 = mesh.positions.copy()
+
+    def start(q, x):
+        fv.set_mesh(build_mesh(x, box=box))
+        fv.set_state(q)
+
+    start(q0, x0)
+    dts = [0.5 * fv.time_step(0.3)] * 2
+    path = []
+    for dt in dts:
+        path.append((fv.get_state(), fv.positions()))
+        fv.time_step(0.3)
+        fv.step_moving(dt, remesh)
+    rng = np.random.default_rng(8)
+    dq0, dx0 = rng.normal(size=q0.shape) * np.abs(q0), rng.normal(size=x0.shape) * 1e-3
+    start(q0, x0)
+    dq, dx = dq0, dx0
+    for dt in dts:
+        fv.time_step(0.3)
+        dq, dx = fv.step_moving_tangent(dt, dq, dx, NullGeometry, remesh)
+    qbar, xbar = rng.normal(size=q0.shape), rng.normal(size=x0.shape)
+    Tq, Tx = qbar, xbar
+    for (q, x), dt in zip(reversed(path), reversed(dts)):
+        start(q, x)
+        fv.time_step(0.3)
+        Tq, Tx = fv.step_moving_adjoint(dt, Tq, Tx, NullGeometry, remesh)
+    lhs = float(np.sum(qbar * dq) + np.sum(xbar * dx))
+    rhs = float(np.sum(Tq * dq0) + np.sum(Tx * dx0))
+    size = float(np.sum(np.abs(qbar * dq)) + np.sum(np.abs(xbar * dx)) + np.sum(np.abs(Tq * dq0)) + np.sum(np.abs(Tx * dx0)))
+    assert abs(lhs - rhs) < 1e-12 * size, (lhs, rhs, size)
+
+
 def test_moving_tangent_equals_central_differences(cuda):
     """J (dq, dx) over 2 steps against central differences of the forward (the same dt, each side its own host remesh,
     the starting meshes' topology fixed within +- h): within 1e-6 of each block's largest entry at h = 1e-6 (dq relative

@@ -230,3 +230,42 @@ def test_moving_derivatives_order_1(reference, riemann, steps_fixed):
     want = ref.step_moving_adjoint(dt, qb, xb, Geometry2D, steps_fixed=steps_fixed)
     for a, b in zip(got, want):
         assert np.max(np.abs(a - b)) <= 1e-9 * np.max(np.abs(b))
+
+
+@pytest.mark.parametrize("order", [0, 1])
+def test_moving_derivatives_3d_null_geometry(reference, order):
+    """The moving derivatives' kernels in 3D (dimension-generic; no 3D geometry derivative here, voronoi-cpp's
+    MeshDerivative being absent): with a null geometry derivative on both sides (V, c, A, x_f held; the reference's cost
+    test does the same), the GPU's tangent and adjoint of one moving step against the reference's own on 8^3 jittered
+    generators and the reference's 3D wave state (hydro_derivatives_test.cpp:1513-1516): within 1e-9 of the largest
+    entry, orders 0 and 1."""
+    from conftest import wave_state_3d
+    from luna_cpp_b200.geometry_derivative import NullGeometry
+
+    mesh = jittered_mesh(8, dim=3, jitter=0.15, seed=4)
+    x0 = mesh.positions.copy()
+    q0 = wave_state_3d(mesh)
+    remesh = lambda p: build_mesh(p, box=(1.0, 1.0, 1.0))  # noqa: E731
+    gpu = hydro.FiniteVolume(mesh, hydro.Gas(5.0 / 3.0), order=order, motion="moving")
+    ref = R.ReferenceFV(mesh, gamma=5.0 / 3.0, order=order, moving=True, remesh=remesh)
+    gpu.set_state(q0)
+    ref.set_state(q0)
+    dt = 0.5 * ref.time_step(0.3)
+    gpu.time_step(0.3)
+    rng = np.random.default_rng(6)
+    dq, dx = rng.normal(size=q0.shape) * np.abs(q0), rng.normal(size=x0.shape) * 1e-3
+    got = gpu.step_moving_tangent(dt, dq, dx, NullGeometry, remesh if order == 1 else None)
+    want = ref.step_moving_tangent(dt, dq, dx, NullGeometry)
+    for a, b in zip(got, want):
+        assert np.max(np.abs(a - b)) <= 1e-9 * np.max(np.abs(b))
+    gpu.set_mesh(mesh)
+    gpu.set_state(q0)
+    gpu.time_step(0.3)
+    ref.set_positions(x0)
+    ref.set_state(q0)
+    ref.time_step(0.3)
+    qb, xb = rng.normal(size=q0.shape), rng.normal(size=x0.shape)
+    got = gpu.step_moving_adjoint(dt, qb, xb, NullGeometry, remesh if order == 1 else None)
+    want = ref.step_moving_adjoint(dt, qb, xb, NullGeometry)
+    for a, b in zip(got, want):
+        assert np.max(np.abs(a - b)) <= 1e-9 * np.max(np.abs(b))
