@@ -355,7 +355,8 @@ __device__ __forceinline__ bool side_value(const double* W, const double* g, con
 
 // Resident blocks an SM the adjoint's register-heavy kernels are cut for, and the list entries the gather requests
 // together. Measured at 128^3 (step_adjoint, FP64): no cap (128-164 registers) 9.66 ms, 4 blocks (128 registers, a few
-// spills) 8.32 ms; a gather batch of 4 changed nothing (9.68 / 8.34 ms).
+// spills) 8.32 ms; a gather batch of 4 changed nothing (9.68 / 8.34 ms); 3 blocks 8.65 ms, and the fit's entry loop
+// unrolled by 2 8.54 ms (8.28 for the default).
 #ifndef LUNA_ADJ_MIN_BLOCKS
 #define LUNA_ADJ_MIN_BLOCKS 4
 #endif
