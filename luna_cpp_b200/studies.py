@@ -544,7 +544,7 @@ def kernels(case="adjoint", nx=64, repeat=3, log=print) -> dict:
                 fv = hydro.FiniteVolume(mesh)
                 fv.close()
         else:
-            fv = hydro.FiniteVolume(mesh, precision="fp32", motion="moving")
+            fv = hydro.FiniteVolume(mesh, precision="single", motion="moving")
             fv.set_state(point_blast(mesh.cells()))
             r = run_moving(fv, 1.0, max_steps=repeat + 1, remesher=remesher, log=lambda s: None)
             out["hydro_device_ms_per_step"] = r["hydro_device_ms"] / r["steps"]
