@@ -354,19 +354,51 @@ struct CandidatesT {
     int n;
 };
 
+// Whether the bucket at offset o from the cell's bucket bi can hold an image with lo2 < d2 <= hi2 from the cell's
+// generator xi: the distance from xi to the bucket's box, per axis, against hi2, and to its far corner against lo2. A
+// point in bucket b lies within [b w, (b + 1) w) up to the rounding of floor(x / w) and of b w, which the margin of a
+// millionth of a bucket covers, so a bucket it skips holds no image of the shell and the batch is the same without it.
+template <int D>
+LUNA_VC_HD bool bucket_reaches(const double* xi, const int* bi, const int32_t* o, const Grid& grid, double lo2, double hi2) {
+    double near2 = 0, far2 = 0;
+    for (int a = 0; a < D; ++a) {
+        const double w = grid.w[a], m = 1e-6 * w;
+        const double lo = static_cast<double>(bi[a] + o[a]) * w - xi[a];  // the bucket's low face from xi
+        const double hi = lo + w;
+        double near = 0;
+        if (lo > 0)
+            near = lo - m;
+        else if (hi < 0)
+            near = -hi - m;
+        near = near > 0 ? near : 0;
+        const double far = (-lo > hi ? -lo : hi) + m;
+        near2 += near * near;
+        far2 += far * far;
+    }
+    return near2 <= hi2 && far2 > lo2;
+}
+
 // Appends to the batch the images in the bucket at offset o from the cell's bucket bi with lo2 < d2 <= hi2 from its
-// generator xi. Returns false when the batch outgrows the storage.
+// generator xi (nothing from a bucket that cannot hold one). Returns false when the batch outgrows the storage.
 template <int D, class Cand>
 LUNA_VC_HD bool gather_bucket(const double* xi, const int* bi, const int32_t* o, const double* pos, const double* side, const Grid& grid,
                               double lo2, double hi2, Cand& cand) {
     constexpr int kMax = sizeof(cand.j) / sizeof(cand.j[0]);
+    if (!bucket_reaches<D>(xi, bi, o, grid, lo2, hi2)) return true;
     int64_t b = 0;
     double shift[3] = {0, 0, 0};
     for (int a = 0; a < D; ++a) {
-        const int t = bi[a] + o[a];
-        const int tw = ((t % grid.nb[a]) + grid.nb[a]) % grid.nb[a];
-        shift[a] = static_cast<double>((t - tw) / grid.nb[a]) * side[a];
-        b = b * grid.nb[a] + tw;
+        int t = bi[a] + o[a], wraps = 0;  // t = wraps nb + tw with 0 <= tw < nb, without an integer division
+        while (t < 0) {
+            t += grid.nb[a];
+            --wraps;
+        }
+        while (t >= grid.nb[a]) {
+            t -= grid.nb[a];
+            ++wraps;
+        }
+        shift[a] = static_cast<double>(wraps) * side[a];
+        b = b * grid.nb[a] + t;
     }
     for (int64_t q = grid.start[b]; q < grid.start[b + 1]; ++q) {
         const int32_t j = grid.items[q];
