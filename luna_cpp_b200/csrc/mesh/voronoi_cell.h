@@ -652,6 +652,7 @@ struct DualT {
     int nt;
     double eps;
     bool full;
+    double rmax2;  // after a cut: the largest squared vertex radius (max_radius2())
 
     LUNA_VC_HD void vertex(int t) {  // the meeting point of the triangle's three planes (Cramer's rule)
         const double* a = pn[tri[t][0]];
@@ -735,12 +736,15 @@ struct DualT {
                 ++nb;
             }
         int w = 0;
+        double r = 0;  // the largest squared vertex radius left, as max_radius2() gives it
         for (int t = 0; t < nt; ++t)
             if (!out[t]) {
                 if (w != t) {
                     for (int k = 0; k < 3; ++k) tri[w][k] = tri[t][k];
                     for (int k = 0; k < 3; ++k) tv[w][k] = tv[t][k];
                 }
+                const double d = dot3(tv[w], tv[w]);
+                r = d > r ? d : r;
                 ++w;
             }
         nt = w;
@@ -753,8 +757,11 @@ struct DualT {
             tri[nt][1] = ev[e];
             tri[nt][2] = static_cast<uint8_t>(q);
             vertex(nt);
+            const double d = dot3(tv[nt], tv[nt]);
+            r = d > r ? d : r;
             ++nt;
         }
+        rmax2 = r;
         return true;
     }
     // The faces (one per plane still holding vertices), volume and first moment, as cell_faces3: each face's vertices
@@ -763,11 +770,24 @@ struct DualT {
     template <class Faces>
     LUNA_VC_HD int finish(int64_t i, Faces& faces, double& volume, double* cm) {
         int loop[kMaxTris];
+        // each plane's triangles in increasing index (a counting sort of the corners): a face's walk looks only at the
+        // triangles of its plane, in the order a scan over all triangles meets them, so it makes the same loop
+        int start[kMaxPlanes + 1], at[kMaxPlanes];
+        int16_t inc[3 * kMaxTris];
+        for (int p = 0; p <= np; ++p) start[p] = 0;
+        for (int t = 0; t < nt; ++t)
+            for (int k = 0; k < 3; ++k) ++start[tri[t][k] + 1];
         for (int p = 0; p < np; ++p) {
-            int t0 = -1, m = 0;
-            for (int t = 0; t < nt && t0 < 0; ++t)
-                if (tri[t][0] == p || tri[t][1] == p || tri[t][2] == p) t0 = t;
-            if (t0 < 0) continue;
+            start[p + 1] += start[p];
+            at[p] = start[p];
+        }
+        for (int t = 0; t < nt; ++t)
+            for (int k = 0; k < 3; ++k) inc[at[tri[t][k]]++] = static_cast<int16_t>(t);
+        for (int p = 0; p < np; ++p) {
+            const int s0 = start[p], s1 = start[p + 1];
+            if (s0 == s1) continue;
+            const int t0 = inc[s0];
+            int m = 0;
             if (ptag[p] < 0) return kReachesBox;
             if (ptag[p] == i) return kTouchesSelf;
             int cur = t0;
@@ -777,8 +797,8 @@ struct DualT {
                 if (m >= kMaxTris) return kCapacity;
                 loop[m++] = cur;
                 int next = -1;  // the triangle with p followed by b
-                for (int t = 0; t < nt && next < 0; ++t)
-                    for (int k = 0; k < 3; ++k)
+                for (int s = s0; s < s1 && next < 0; ++s)
+                    for (int k = 0, t = inc[s]; k < 3; ++k)
                         if (tri[t][k] == p && tri[t][(k + 1) % 3] == b) {
                             next = t;
                             b = tri[t][(k + 2) % 3];
@@ -861,7 +881,7 @@ LUNA_VC_HD int build_cell_dual(int64_t i, const double* pos, const double* side,
             }
             const double inv = 1.0 / sqrt(d2);
             const double nrm[3] = {cand.d[e][0] * inv, cand.d[e][1] * inv, cand.d[e][2] * inv};
-            if (poly.clip(nrm, 0.5 * d2 * inv, cand.j[e])) rmax2 = poly.max_radius2();
+            if (poly.clip(nrm, 0.5 * d2 * inv, cand.j[e])) rmax2 = poly.rmax2;
             if (poly.full) return kCapacity;
         }
         if (done || 4.0 * rmax2 <= hi2) break;
