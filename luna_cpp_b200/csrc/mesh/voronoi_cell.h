@@ -647,8 +647,7 @@ struct DualT {
     uint8_t tri[kMaxTris][3];
     double tv[kMaxTris][3];
     bool out[kMaxTris];
-    uint8_t eu[3 * kMaxTris], ev[3 * kMaxTris];
-    bool boundary[3 * kMaxTris];
+    uint16_t ek[3 * kMaxTris], eb[3 * kMaxTris];
     int nt;
     double eps;
     bool full;
@@ -715,26 +714,17 @@ struct DualT {
         for (int a = 0; a < 3; ++a) pn[q][a] = nrm[a];
         pc[q] = c;
         ptag[q] = tag;
-        int ne = 0;
+        int ne = 0;  // the dropped triangles' edges, each as (from plane) << 8 | (to plane)
         for (int t = 0; t < nt; ++t)
             if (out[t])
-                for (int k = 0; k < 3; ++k) {
-                    eu[ne] = tri[t][k];
-                    ev[ne] = tri[t][(k + 1) % 3];
-                    ++ne;
-                }
-        for (int e = 0; e < ne; ++e) {  // the boundary edges: those whose reverse is not a dropped triangle's edge
+                for (int k = 0; k < 3; ++k) ek[ne++] = static_cast<uint16_t>(tri[t][k] << 8 | tri[t][(k + 1) % 3]);
+        int nb = 0;  // the boundary edges: those whose reverse is not a dropped triangle's edge, compacted in order
+        for (int e = 0; e < ne; ++e) {
+            const uint16_t rev = static_cast<uint16_t>((ek[e] & 0xff) << 8 | ek[e] >> 8);
             bool paired = false;
-            for (int f = 0; f < ne && !paired; ++f) paired = eu[f] == ev[e] && ev[f] == eu[e];
-            boundary[e] = !paired;
+            for (int f = 0; f < ne && !paired; ++f) paired = ek[f] == rev;
+            if (!paired) eb[nb++] = ek[e];
         }
-        int nb = 0;  // compacted in place, after every pairing is known
-        for (int e = 0; e < ne; ++e)
-            if (boundary[e]) {
-                eu[nb] = eu[e];
-                ev[nb] = ev[e];
-                ++nb;
-            }
         int w = 0;
         double r = 0;  // the largest squared vertex radius left, as max_radius2() gives it
         for (int t = 0; t < nt; ++t)
@@ -753,8 +743,8 @@ struct DualT {
             return false;
         }
         for (int e = 0; e < nb; ++e) {
-            tri[nt][0] = eu[e];
-            tri[nt][1] = ev[e];
+            tri[nt][0] = static_cast<uint8_t>(eb[e] >> 8);
+            tri[nt][1] = static_cast<uint8_t>(eb[e] & 0xff);
             tri[nt][2] = static_cast<uint8_t>(q);
             vertex(nt);
             const double d = dot3(tv[nt], tv[nt]);
