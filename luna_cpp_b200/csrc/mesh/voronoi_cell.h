@@ -343,14 +343,17 @@ struct CellFacesT {
     int n;
 };
 
-// The generator images a cell is clipped by, one batch at a time: offset from the cell's generator, squared distance,
-// index; in clipping order.
+// The generator images a cell is clipped by, one batch at a time: the image's periodic wraps, squared distance,
+// index; in clipping order. The clip recomputes an image's offset from its generator, its wraps and the cell's generator
+// in the gather's own operations, so the offset is the gathered one bit for bit, and the store keeps 4 bytes an image
+// instead of 24.
 template <int kMax>
 struct CandidatesT {
-    double d[kMax][3];
+    uint32_t w[kMax];  // the image's wraps per axis, each + 128 in a byte
     double d2[kMax];
     int32_t j[kMax];
     int order[kMax];
+    double key[kMax];  // d2 in clipping order
     int n;
 };
 
@@ -386,6 +389,7 @@ LUNA_VC_HD bool gather_bucket(const double* xi, const int* bi, const int32_t* o,
     constexpr int kMax = sizeof(cand.j) / sizeof(cand.j[0]);
     if (!bucket_reaches<D>(xi, bi, o, grid, lo2, hi2)) return true;
     int64_t b = 0;
+    uint32_t packed = 0;
     double shift[3] = {0, 0, 0};
     for (int a = 0; a < D; ++a) {
         int t = bi[a] + o[a], wraps = 0;  // t = wraps nb + tw with 0 <= tw < nb, without an integer division
@@ -398,6 +402,7 @@ LUNA_VC_HD bool gather_bucket(const double* xi, const int* bi, const int32_t* o,
             ++wraps;
         }
         shift[a] = static_cast<double>(wraps) * side[a];
+        packed |= static_cast<uint32_t>(wraps + 128) << (8 * a);
         b = b * grid.nb[a] + t;
     }
     for (int64_t q = grid.start[b]; q < grid.start[b + 1]; ++q) {
@@ -411,7 +416,7 @@ LUNA_VC_HD bool gather_bucket(const double* xi, const int* bi, const int32_t* o,
         if (!(d2 > lo2 && d2 <= hi2)) continue;
         if (cand.n >= kMax) return false;
         const int e = cand.n++;
-        for (int a = 0; a < 3; ++a) cand.d[e][a] = d[a];
+        cand.w[e] = packed;
         cand.d2[e] = d2;
         cand.j[e] = j;
     }
@@ -454,13 +459,17 @@ LUNA_VC_HD bool gather(const double* xi, const int* bi, const double* pos, const
     } else if (!gather_cube<D>(xi, bi, pos, side, grid, lo2, hi2, cand)) {
         return false;
     }
-    for (int k = 0; k < cand.n; ++k) {  // insertion sort by (d2, j), stable
-        int x = k, m = k - 1;
-        while (m >= 0 && (cand.d2[cand.order[m]] > cand.d2[x] || (cand.d2[cand.order[m]] == cand.d2[x] && cand.j[cand.order[m]] > cand.j[x]))) {
+    for (int k = 0; k < cand.n; ++k) {  // insertion sort by (d2, j), stable; the sorted d2 kept beside the order
+        const double dk = cand.d2[k];
+        const int32_t jk = cand.j[k];
+        int m = k - 1;
+        while (m >= 0 && (cand.key[m] > dk || (cand.key[m] == dk && cand.j[cand.order[m]] > jk))) {
+            cand.key[m + 1] = cand.key[m];
             cand.order[m + 1] = cand.order[m];
             --m;
         }
-        cand.order[m + 1] = x;
+        cand.key[m + 1] = dk;
+        cand.order[m + 1] = k;
     }
     return true;
 }
@@ -585,13 +594,17 @@ LUNA_VC_HD int build_cell(int64_t i, const double* pos, const double* side, cons
         bool done = false;
         for (int k = 0; k < cand.n; ++k) {
             const int e = cand.order[k];
-            const double d2 = cand.d2[e];
+            const double d2 = cand.key[k];
             if (d2 > 4.0 * rmax2) {
                 done = true;
                 break;
             }
             const double inv = 1.0 / sqrt(d2);
-            const double nrm[3] = {cand.d[e][0] * inv, cand.d[e][1] * inv, cand.d[e][2] * inv};
+            double dv[3] = {0, 0, 0};
+            const int32_t je = cand.j[e];
+            for (int a = 0; a < D; ++a)
+                dv[a] = pos[D * je + a] + static_cast<double>(static_cast<int>((cand.w[e] >> (8 * a)) & 0xff) - 128) * side[a] - xi[a];
+            const double nrm[3] = {dv[0] * inv, dv[1] * inv, dv[2] * inv};
             if (poly.clip(nrm, 0.5 * d2 * inv, cand.j[e])) rmax2 = poly.max_radius2();
             if (poly.full) return kCapacity;
         }
@@ -864,13 +877,17 @@ LUNA_VC_HD int build_cell_dual(int64_t i, const double* pos, const double* side,
         bool done = false;
         for (int k = 0; k < cand.n; ++k) {
             const int e = cand.order[k];
-            const double d2 = cand.d2[e];
+            const double d2 = cand.key[k];
             if (d2 > 4.0 * rmax2) {
                 done = true;
                 break;
             }
             const double inv = 1.0 / sqrt(d2);
-            const double nrm[3] = {cand.d[e][0] * inv, cand.d[e][1] * inv, cand.d[e][2] * inv};
+            double dv[3] = {0, 0, 0};
+            const int32_t je = cand.j[e];
+            for (int a = 0; a < D; ++a)
+                dv[a] = pos[D * je + a] + static_cast<double>(static_cast<int>((cand.w[e] >> (8 * a)) & 0xff) - 128) * side[a] - xi[a];
+            const double nrm[3] = {dv[0] * inv, dv[1] * inv, dv[2] * inv};
             if (poly.clip(nrm, 0.5 * d2 * inv, cand.j[e])) rmax2 = poly.rmax2;
             if (poly.full) return kCapacity;
         }
