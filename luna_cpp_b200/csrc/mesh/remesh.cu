@@ -152,10 +152,12 @@ struct CellOut {
 
 // The cells (all of them, or those of the list), each built by one thread. Without Far, a cell whose search would
 // pass the grid's sorted offsets or fill the candidate store is put on the retry list for the Far pass (the same cell
-// either way, voronoi_cell.h), which keeps the common cell's code small. Eight blocks an SM (64 registers, a few
-// spilled): 57.5 ms for the 128^3 jittered remesh against 62 ms at 80 registers, 58.6 ms at seven blocks and 58 ms at ten.
+// either way, voronoi_cell.h), which keeps the common cell's code small. 1,024 threads an SM (64 registers, a few
+// spilled): 57.5 ms for the 128^3 jittered remesh against 62 ms at 80 registers, 58.6 ms at 896 threads and 58 ms at
+// 1,280; in 64-thread blocks (16 an SM) about 1 % faster than in 128-thread blocks, and no faster with the L1 carveout
+// preferred.
 template <int D, bool Far>
-__global__ void __launch_bounds__(128, 8) k_cells(int64_t n, const int32_t* __restrict__ list, const double* __restrict__ pos, Box box, Grid g,
+__global__ void __launch_bounds__(64, 16) k_cells(int64_t n, const int32_t* __restrict__ list, const double* __restrict__ pos, Box box, Grid g,
                                                CellOut out, Counters* c, int32_t* __restrict__ retry) {
     const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (k >= n) return;
@@ -476,12 +478,12 @@ luna_status luna_remesh::build(int64_t n, const double* points, bool on_device, 
         RM_TRY(fc.reserve(capacity * D, "face records"));
         if (attempt > 0) RM_CUDA(cudaMemsetAsync(counters.ptr, 0, sizeof(Counters), stream));
         const CellOut out{volume.ptr, centroid.ptr, first.ptr, count.ptr, fj.ptr, fa.ptr, fc.ptr, capacity};
-        k_cells<D, false><<<grid_blocks(n, 128), 128, 0, stream>>>(n, nullptr, pos.ptr, box, g, out, counters.ptr, retry.ptr);
+        k_cells<D, false><<<grid_blocks(n, 64), 64, 0, stream>>>(n, nullptr, pos.ptr, box, g, out, counters.ptr, retry.ptr);
         RM_CUDA(cudaGetLastError());
         RM_CUDA(cudaMemcpyAsync(&h, counters.ptr, sizeof(Counters), cudaMemcpyDeviceToHost, stream));
         RM_CUDA(cudaStreamSynchronize(stream));
         if (h.retry > 0 && !h.error && !h.nonfinite) {  // the far search for the cells the fast path handed on
-            k_cells<D, true><<<grid_blocks(h.retry, 128), 128, 0, stream>>>(h.retry, retry.ptr, pos.ptr, box, g, out, counters.ptr, nullptr);
+            k_cells<D, true><<<grid_blocks(h.retry, 64), 64, 0, stream>>>(h.retry, retry.ptr, pos.ptr, box, g, out, counters.ptr, nullptr);
             RM_CUDA(cudaGetLastError());
             RM_CUDA(cudaMemcpyAsync(&h, counters.ptr, sizeof(Counters), cudaMemcpyDeviceToHost, stream));
             RM_CUDA(cudaStreamSynchronize(stream));
